@@ -1,0 +1,408 @@
+"""Benchmark of the dense Helmholtz BEM hot path (frequency-solves per second).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload c2|c1]
+
+A step is one batched sweep of the workload's frequencies through
+corrected assembly -> LU -> solve -> exterior field -> tag reductions.
+
+* ``value``: whole-job freq-solves/s with inputs resident in HBM (CUDA events,
+  barrier + synchronize around the K timed steps, max over ranks).
+* ``e2e``: the same metric through the reference-facing batch call
+  ``NativeSession.assemble_solve_evaluate_standard_neumann_batch`` with host
+  numpy inputs and outputs (host<->device copies inside the timed region).
+* ``roofline``: the dominant kernel (regular pair assembly, ``k_regular``)
+  timed by CUDA events on its launch stream inside the timed region.
+* ``cpu_baseline``: the CPU oracle (C restatement of the reference's CPU
+  path, all host threads) + LAPACK cgesv on a bounded sample of the workload.
+* ``--impl reference``: the reference's own algorithm on the host cores (the
+  oracle port; the reference itself needs Apple Metal/Accelerate), same
+  metric and config, rank 0 only.
+
+Multi-GPU (torchrun): replicas only -- every rank sweeps its own copy of the
+workload (frequencies are independent); no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+FLOPS_PER_SAMPLE = 36.0     # algorithmic FP32 flops (FMA = 2) per kernel sample, incl. accumulation
+SFU_PER_SAMPLE = 3.0        # rsqrt, sin, cos
+FP32_LANES_PER_SM = 128
+SFU_LANES_PER_SM = 16
+N_SM = 148
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", choices=["c2", "c1"], default="c2")
+    ap.add_argument("--precision", choices=["plain", "mixed"], default="plain")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------------- workload
+def workload(name: str):
+    """C2: seeded yz+xz quarter exponential horn, ~1k P1 dofs, 40 log freqs 0.5-20 kHz, 3 x 37 obs at 2 m.
+    C1: icosphere level 3 (642 dofs), 8 log freqs 0.2-5 kHz, 1 x 37 obs."""
+    import hornlab_metal_bem_b200 as hb
+    from hornlab_metal_bem_b200 import generators as G
+    from hornlab_metal_bem_b200.bie import build_source_face_scale
+    from hornlab_metal_bem_b200.geometry import build_geometry_buffers
+    from hornlab_metal_bem_b200.mesh import make_pure_function_spaces
+    from hornlab_metal_bem_b200.observation import build_observation_points
+    from hornlab_metal_bem_b200.sweep import build_frequency_grid, field_points_3xn, k_values, neumann_rows
+
+    if name == "c2":
+        spec = G.horn_spec_from_seed(0, edge=0.007)
+        mesh = G.horn(spec, quarter=True)
+        cfg = hb.native_config(
+            freq_min_hz=500.0, freq_max_hz=20000.0, freq_count=40, source_motion="axial",
+            native_symmetry_plane="yz+xz", native_check_open_edges=False,
+            observation=hb.ObservationConfig(planes=["horizontal", "vertical", "diagonal"], angle_count=37),
+        )
+        desc = (f"C2 yz+xz quarter exponential horn (seed 0: flare {spec.flare:.2f} 1/m, lip {spec.lip * 1e3:.2f} mm), "
+                "40 log freqs 0.5-20 kHz, 3x37 obs @ 2 m")
+    else:
+        mesh = G.icosphere(3, 0.1)
+        cfg = hb.native_config(freq_min_hz=200.0, freq_max_hz=5000.0, freq_count=8, velocity_mode="velocity",
+                               air_density=1.205,
+                               observation=hb.ObservationConfig(planes=["horizontal"], angle_count=37))
+        desc = "C1 pulsating icosphere L3, 8 log freqs 0.2-5 kHz, 1x37 obs @ 2 m"
+    frame = hb._resolve_frame(mesh, cfg)
+    obs, _ = build_observation_points(frame, cfg.observation)
+    p1, dp0 = make_pure_function_spaces(mesh.grid)
+    buf = build_geometry_buffers(mesh.grid, mesh.physical_tags, p1, dp0)
+    freqs = build_frequency_grid(cfg)
+    k_re, k_im = k_values(freqs, cfg)
+    scale = build_source_face_scale(mesh.grid, mesh.physical_tags, cfg, frame.axis, frame.source_center)
+    q = neumann_rows(buf.n_triangles, mesh.physical_tags, freqs, cfg, scale)
+    sym = {None: 0, "yz+xz": 3}[cfg.native_symmetry_plane]
+    return dict(name=name, desc=desc, mesh=mesh, cfg=cfg, buf=buf, freqs=freqs, k_re=k_re, k_im=k_im, q=q,
+                obs=field_points_3xn(obs), tags=sorted(cfg.velocity_sources), sym=sym)
+
+
+# --------------------------------------------------------------------------- helpers
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_uuid: str | None):
+        self.uuid = device_uuid
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+            if self.uuid:
+                cmd.insert(1, f"--id={self.uuid}")
+            self.proc = subprocess.Popen(cmd, stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        pw = [float(r[2]) for r in rows if r[2].replace(".", "", 1).isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i].lower().startswith("active")})
+        loaded = [s for s, p in zip(sm, pw) if p >= 0.5 * max(pw)] if pw else sm
+        return {"sm_mhz": statistics.median(loaded or sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows), "power_w_max": max(pw) if pw else None}
+
+
+def measured_peaks() -> dict:
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        d["source"] = "measured (MEASURED_PEAKS.json)"
+        return d
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0, "source": "fallback"}
+
+
+def profile_traffic(kernel: str, workload: str) -> float | None:
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+    f = REPO / "profiles" / f"{kernel}_{workload}.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def cpu_baseline(w, n_freq_sample: int = 1) -> dict:
+    """Oracle port (f32, OpenMP on all host threads) + LAPACK cgesv on a bounded sample."""
+    from oracle.oracle import Oracle, dense_solve
+
+    threads = len(os.sched_getaffinity(0))
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", str(threads))
+    o = Oracle(w["buf"], w["sym"], "f32", threads=threads)
+    F = len(w["freqs"])
+    picks = np.linspace(0, F - 1, n_freq_sample + 2)[1:-1].round().astype(int) if n_freq_sample < F else np.arange(F)
+    t0 = time.perf_counter()
+    for f in picks:
+        A, b = o.corrected(float(w["k_re"][f]), w["q"][f])
+        p = dense_solve(A, b, "f32")
+        o.field(float(w["k_re"][f]), p, w["q"][f], w["obs"])
+        for t in w["tags"]:
+            o.tag_average(p, t)
+    dt = time.perf_counter() - t0
+    return {"value": len(picks) / dt, "unit": "freq-solves/s", "cores": threads, "kind": "port",
+            "sample": f"{len(picks)} of {F} frequencies (index {picks.tolist()}) of the same workload, "
+                      f"{dt:.1f} s: corrected assembly + cgesv + field + tag averages"}
+
+
+# --------------------------------------------------------------------------- arms
+def run_reference(args, w):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    warm = max(1, args.warmup)
+    from oracle.oracle import Oracle  # noqa: F401  (import timing outside the region)
+
+    for _ in range(warm):
+        cpu_baseline(w, 1)
+    vals = [cpu_baseline(w, 1) for _ in range(args.steps)]
+    secs = [1.0 / v["value"] for v in vals]
+    total = sum(secs)
+    value = args.steps / total
+    line = {
+        "impl": "reference", "metric": "freq-solves/s", "value": value, "unit": "freq-solves/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": warm, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64 (f32)",
+        "data": "synthetic", "config": {"workload": w["desc"], "n_dof": w["buf"].p1_dof_count,
+                                         "n_triangles": w["buf"].n_triangles, "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": "freq-solves/s", "cores": vals[0]["cores"], "kind": "port",
+                         "sample": "each step: 1 middle frequency of the workload (corrected assembly, cgesv, field, "
+                                   "tag averages); the reference's own Swift/Metal/Accelerate path cannot run here"},
+        "e2e": {"value": value, "unit": "freq-solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args, w):
+    import torch
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from hornlab_metal_bem_b200.native import (
+        HBEM_ASM_DUFFY, HBEM_ASM_REGULAR, NativeSession, ResidentSweep, _np_ptr, _stream_ptr, _t_ptr, check,
+        load_library,
+    )
+
+    lib = load_library()
+    buf = w["buf"]
+    F = len(w["freqs"])
+    sess = NativeSession(buf, symmetry_plane=w["cfg"].native_symmetry_plane, check_open_edges=False)
+    rs = ResidentSweep(sess, w["k_re"], w["k_im"], w["q"], w["obs"], w["tags"], precision=args.precision)
+    n = rs.n
+    stream = torch.cuda.current_stream()
+
+    def assemble_split(ev0=None, ev1=None):
+        # zero, regular (timed), Duffy: three ABI calls on one stream
+        rs.A_re.zero_(); rs.A_im.zero_(); rs.b_re.zero_(); rs.b_im.zero_()
+        if ev0 is not None:
+            ev0.record(stream)
+        check(lib.hbem_assemble(sess.handle, F, _np_ptr(rs.k_re), _np_ptr(rs.k_im), _t_ptr(rs.q_re),
+                                _t_ptr(rs.q_im), rs.q_re.stride(0), None, None, _t_ptr(rs.A_re), _t_ptr(rs.A_im), n,
+                                n * n, _t_ptr(rs.b_re), _t_ptr(rs.b_im), n, HBEM_ASM_REGULAR, _stream_ptr()),
+              "hbem_assemble", lib)
+        if ev1 is not None:
+            ev1.record(stream)
+        check(lib.hbem_assemble(sess.handle, F, _np_ptr(rs.k_re), _np_ptr(rs.k_im), _t_ptr(rs.q_re),
+                                _t_ptr(rs.q_im), rs.q_re.stride(0), None, None, _t_ptr(rs.A_re), _t_ptr(rs.A_im), n,
+                                n * n, _t_ptr(rs.b_re), _t_ptr(rs.b_im), n, HBEM_ASM_DUFFY, _stream_ptr()),
+              "hbem_assemble", lib)
+
+    def step(evs=None):
+        if evs is None:
+            assemble_split()
+        else:
+            assemble_split(evs[0], evs[1])
+        if evs is not None:
+            evs[2].record(stream)
+        rs.factor_solve()
+        if evs is not None:
+            evs[3].record(stream)
+        rs.field()
+        if evs is not None:
+            evs[4].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if int(rs.info.abs().sum()) != 0:
+        raise RuntimeError("zero pivot in the benchmark workload")
+
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    clocks = Clocks(uuid)
+    stage_evs = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(args.steps)]
+    launches0 = lib.hbem_launch_count()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for i in range(args.steps):
+        step(stage_evs[i])
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clk = clocks.stop()
+    launches = lib.hbem_launch_count() - launches0
+    ms = t_start.elapsed_time(t_end)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    stage = {"regular_ms": [], "duffy_ms": [], "lu_solve_ms": [], "field_ms": []}
+    for e in stage_evs:
+        stage["regular_ms"].append(e[0].elapsed_time(e[1]))
+        stage["duffy_ms"].append(e[1].elapsed_time(e[2]))
+        stage["lu_solve_ms"].append(e[2].elapsed_time(e[3]))
+        stage["field_ms"].append(e[3].elapsed_time(e[4]))
+    stage = {k: statistics.median(v) for k, v in stage.items()}
+    value = world * F * args.steps / (ms * 1e-3)
+
+    # ---- e2e through the reference-facing batch call with host buffers
+    q = w["q"]
+    e2e_kw = dict(k_imag_f32=w["k_im"], source_tags=w["tags"], impedance_source_tag=min(w["tags"]),
+                  precision=args.precision)
+    for _ in range(max(1, args.warmup)):
+        sess.assemble_solve_evaluate_standard_neumann_batch(w["freqs"], w["k_re"], q, w["obs"], **e2e_kw)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        res = sess.assemble_solve_evaluate_standard_neumann_batch(w["freqs"], w["k_re"], q, w["obs"], **e2e_kw)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    assert all(r.lapack_info == 0 for r in res)
+    n_obs = w["obs"].shape[1]
+    ntag = len(w["tags"])
+    h2d = F * buf.n_triangles * 8 + F * 8 + 3 * n_obs * 4 + ntag * 4
+    d2h = F * n_obs * 8 + F * ntag * 16 + F * 4 + F * 12
+
+    # ---- roofline of the dominant kernel
+    peaks = measured_peaks()
+    m_img = {0: 1, 1: 2, 2: 2, 3: 4, 4: 2}[w["sym"]]
+    T = buf.n_triangles
+    samples = F * T * T * 36 * m_img
+    clk_mhz = peaks.get("sm_max_mhz", 1965.0)
+    fp32_peak = N_SM * FP32_LANES_PER_SM * 2 * clk_mhz * 1e6 / 1e12
+    achieved = samples * FLOPS_PER_SAMPLE / (stage["regular_ms"] * 1e-3) / 1e12
+    sfu_peak = N_SM * SFU_LANES_PER_SM * clk_mhz * 1e6 / SFU_PER_SAMPLE
+    sfu_achieved = samples / (stage["regular_ms"] * 1e-3)
+    roofline = {
+        "kernel": "k_regular (regular pair assembly, %d launch/step)" % ((F + 63) // 64),
+        "bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+        "traffic": profile_traffic("k_regular", w["name"]),
+        "algorithmic": f"{samples:.3e} kernel samples/launch x {FLOPS_PER_SAMPLE:.0f} FP32 flops",
+        "peak_source": f"148 SM x 128 FP32 lanes x 2 x {clk_mhz:.0f} MHz (sm_max_mhz, {peaks['source']})",
+        "sfu": {"achieved_gsamples_s": sfu_achieved / 1e9, "peak_gsamples_s": sfu_peak / 1e9,
+                "frac": sfu_achieved / sfu_peak, "per_sample": "rsqrt + sin + cos (3 MUFU), 16 MUFU/clk/SM"},
+    }
+    line = {
+        "metric": "freq-solves/s", "value": value, "unit": "freq-solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64 (f32 planar)", "data": "synthetic",
+        "config": {"workload": w["desc"], "n_dof": buf.p1_dof_count, "n_triangles": T, "n_freq": F,
+                   "n_obs": n_obs, "precision": args.precision, "parallelism": f"replicas x{world} (frequency-parallel)",
+                   "l2": f"working set {2 * F * n * n * 4 / 1e6:.0f} MB of dense matrices > 126 MB L2"},
+        "e2e": {"value": world * F * args.steps / (e2e_ms * 1e-3), "unit": "freq-solves/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(launches),
+        "stages_ms_per_step": stage,
+        "clocks": clk,
+        "roofline": roofline,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(w, 1)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sess.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    w = workload(args.workload)
+    if args.impl == "reference":
+        run_reference(args, w)
+    else:
+        run_b200(args, w)
+
+
+if __name__ == "__main__":
+    main()

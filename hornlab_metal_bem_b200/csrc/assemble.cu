@@ -1,0 +1,578 @@
+// Dense P1 Galerkin assembly of the Helmholtz double-layer system and the
+// single-layer right-hand side on sm_100a.
+//
+//   A_ij = w_sym * sum_{tau ∋ i, sigma ∋ j} sum_images  ∫∫ phi_i phi_j dG/dn_y
+//          - 1/2 w_sym * M_ij                      (reference main.swift:3993-4133)
+//   b_i  = w_sym * sum_{tau ∋ i} sum_sigma ∫∫ phi_i G  q_sigma   (main.swift:3698-3736)
+//   + Robin coupling -1/3 (i k beta_sigma) ∫∫ phi_i G on every (i, j)  (main.swift:4103-4110)
+//   + Duffy corrections (singular - regular) on touching pairs (main.swift:4246-4431),
+//     folded into A and b on the device (the reference folds them on the CPU,
+//     main.swift:6498-6561).
+//
+// Kernel design (regular part).  A CTA owns a tile of 32 test triangles
+// (one per lane) x 64 trial triangles (eight per warp, warp-uniform).  The
+// trial tile's quadrature points are staged once in shared memory and read
+// as broadcasts; the test points live in registers.  Each lane evaluates
+// 36 x (1 + images) kernel samples per pair with one rsqrt and one sincos
+// (phase reduced in turns before the fast sine/cosine), factorises the 3x3
+// basis products (inner sum over trial points first) and adds the pair block
+// into a shared-memory accumulator indexed by the tile's distinct dofs.  The
+// tile is flushed once with red.global.add, which cuts global atomics by the
+// ~25x dof sharing inside a spatially compact (Morton ordered) tile.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "hbem_internal.h"
+
+namespace hbem {
+
+namespace {
+
+constexpr int kMaxFreqPerLaunch = 64;
+
+struct AsmArgs {
+    const float4 *qp;
+    const float4 *nrm;
+    const int4 *tri;
+    const uchar4 *test_slot;
+    const uchar4 *trial_slot;
+    const int *row_off;
+    const int *rows;
+    const int *col_off;
+    const int *cols;
+    const float *q_re;
+    const float *q_im;
+    const float *beta_re;
+    const float *beta_im;
+    float *a_re;
+    float *a_im;
+    float *b_re;
+    float *b_im;
+    long long q_stride, lda, a_stride, b_stride;
+    int T;
+    float rw;
+    float k[kMaxFreqPerLaunch];
+    float kt[kMaxFreqPerLaunch];  // k / (2 pi): phase in turns per metre
+    float ki[kMaxFreqPerLaunch];
+};
+
+__device__ __forceinline__ float qx(int q) {
+    return q == 0 ? HBEM_QX0 : q == 1 ? HBEM_QX1 : q == 2 ? HBEM_QX2 : q == 3 ? HBEM_QX3 : q == 4 ? HBEM_QX4 : HBEM_QX5;
+}
+__device__ __forceinline__ float qy(int q) {
+    return q == 0 ? HBEM_QY0 : q == 1 ? HBEM_QY1 : q == 2 ? HBEM_QY2 : q == 3 ? HBEM_QY3 : q == 4 ? HBEM_QY4 : HBEM_QY5;
+}
+__device__ __forceinline__ float qw(int q) { return (q == 0 || q == 2 || q == 3) ? HBEM_QWA : HBEM_QWB; }
+__device__ __forceinline__ float bas(int q, int i) {
+    return i == 0 ? 1.0f - qx(q) - qy(q) : (i == 1 ? qx(q) : qy(q));
+}
+
+// One kernel sample: adds dG/dn_y (D) and, when NEED_G, G to the running
+// sums.  The 1/(4 pi) factor is applied once per pair block.  r^2 <= 1e-14
+// is treated as the singular point and contributes nothing (main.swift:3443-3480).
+template <bool CK, bool NEED_G>
+__device__ __forceinline__ void sample(float dx, float dy, float dz, float nx, float ny, float nz, float k,
+                                       float kt, float ki, float &dre, float &dim, float &gre, float &gim) {
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    float rinv = rsqrtf(r2);
+    rinv = r2 > 1.0e-14f ? rinv : 0.0f;
+    const float r = r2 * rinv;
+    float t = r * kt;
+    t -= rintf(t);
+    float s, c;
+    __sincosf(t * 6.28318530717958647692f, &s, &c);
+    float g = rinv;
+    float fre = -rinv;
+    if (CK) {
+        g *= __expf(-ki * r);
+        fre -= ki;
+    }
+    const float gc = g * c, gs = g * s;
+    const float proj = fmaf(dx, nx, fmaf(dy, ny, dz * nz)) * rinv;
+    dre = fmaf(fmaf(gc, fre, -gs * k), proj, dre);
+    dim = fmaf(fmaf(gc, k, gs * fre), proj, dim);
+    if (NEED_G) {
+        gre += gc;
+        gim += gs;
+    }
+}
+
+template <int SYM, bool CK, bool NEED_G>
+__device__ __forceinline__ void pair_block(const float (&tx)[6], const float (&ty)[6], const float (&tz)[6],
+                                           const float4 *__restrict__ sp, float nx, float ny, float nz,
+                                           bool self, float k, float kt, float ki, float (&are)[9],
+                                           float (&aim)[9], float (&sre)[3], float (&sim)[3]) {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) are[i] = aim[i] = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) sre[i] = sim[i] = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 6; ++a) {
+        float ere[3] = {0, 0, 0}, eim[3] = {0, 0, 0};
+        float hre = 0, him = 0;
+#pragma unroll
+        for (int b = 0; b < 6; ++b) {
+            const float4 y = sp[b];
+            float dre = 0, dim = 0, gre = 0, gim = 0;
+            if (!(self && a == b))
+                sample<CK, NEED_G>(y.x - tx[a], y.y - ty[a], y.z - tz[a], nx, ny, nz, k, kt, ki, dre, dim, gre, gim);
+            if (SYM == 1 || SYM == 3)
+                sample<CK, NEED_G>(-y.x - tx[a], y.y - ty[a], y.z - tz[a], -nx, ny, nz, k, kt, ki, dre, dim, gre, gim);
+            if (SYM == 2 || SYM == 3)
+                sample<CK, NEED_G>(y.x - tx[a], -y.y - ty[a], y.z - tz[a], nx, -ny, nz, k, kt, ki, dre, dim, gre, gim);
+            if (SYM == 3)
+                sample<CK, NEED_G>(-y.x - tx[a], -y.y - ty[a], y.z - tz[a], -nx, -ny, nz, k, kt, ki, dre, dim, gre, gim);
+            if (SYM == 4)
+                sample<CK, NEED_G>(y.x - tx[a], y.y - ty[a], -y.z - tz[a], nx, ny, -nz, k, kt, ki, dre, dim, gre, gim);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const float wb = qw(b) * bas(b, j);
+                ere[j] = fmaf(dre, wb, ere[j]);
+                eim[j] = fmaf(dim, wb, eim[j]);
+            }
+            if (NEED_G) {
+                hre = fmaf(gre, qw(b), hre);
+                him = fmaf(gim, qw(b), him);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const float wa = qw(a) * bas(a, i);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                are[i * 3 + j] = fmaf(wa, ere[j], are[i * 3 + j]);
+                aim[i * 3 + j] = fmaf(wa, eim[j], aim[i * 3 + j]);
+            }
+            if (NEED_G) {
+                sre[i] = fmaf(wa, hre, sre[i]);
+                sim[i] = fmaf(wa, him, sim[i]);
+            }
+        }
+    }
+}
+
+template <int SYM, bool CK>
+__global__ void __launch_bounds__(kAsmThreads, 2) k_regular(const __grid_constant__ AsmArgs p) {
+    extern __shared__ float2 s_acc[];
+    __shared__ float4 s_qp[kTrialTile * 6];
+    __shared__ float4 s_nrm[kTrialTile];
+    __shared__ uchar4 s_cs[kTrialTile];
+    __shared__ float4 s_qb[kTrialTile];
+    __shared__ int s_flag[kTrialTile];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int f = blockIdx.z;
+    const int test_tile = blockIdx.y, trial_tile = blockIdx.x;
+    const int T = p.T;
+    const int r0 = p.row_off[test_tile], nrows = p.row_off[test_tile + 1] - r0;
+    const int c0 = p.col_off[trial_tile], ncols = p.col_off[trial_tile + 1] - c0;
+    const int tbase = trial_tile * kTrialTile;
+    const int ntrial = min(kTrialTile, T - tbase);
+    float2 *s_rhs = s_acc + nrows * ncols;
+
+    for (int i = tid; i < nrows * ncols + nrows; i += kAsmThreads) s_acc[i] = make_float2(0.f, 0.f);
+    for (int i = tid; i < ntrial * 6; i += kAsmThreads) s_qp[i] = p.qp[(size_t)tbase * 6 + i];
+    for (int i = tid; i < ntrial; i += kAsmThreads) {
+        s_nrm[i] = p.nrm[tbase + i];
+        s_cs[i] = p.trial_slot[tbase + i];
+        const int orig = p.tri[tbase + i].w;
+        float4 qb = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (p.q_re) {
+            qb.x = p.q_re[(size_t)f * p.q_stride + orig];
+            qb.y = p.q_im[(size_t)f * p.q_stride + orig];
+        }
+        if (p.beta_re) {
+            qb.z = p.beta_re[orig];
+            qb.w = p.beta_im[orig];
+        }
+        s_qb[i] = qb;
+        s_flag[i] = (qb.x != 0.f || qb.y != 0.f || qb.z != 0.f || qb.w != 0.f) ? 1 : 0;
+    }
+    __syncthreads();
+
+    const float k = p.k[f], kt = p.kt[f], ki = p.ki[f];
+    const int test = test_tile * kTestTile + lane;
+    if (test < T) {
+        float tx[6], ty[6], tz[6];
+#pragma unroll
+        for (int a = 0; a < 6; ++a) {
+            const float4 v = p.qp[(size_t)test * 6 + a];
+            tx[a] = v.x;
+            ty[a] = v.y;
+            tz[a] = v.z;
+        }
+        const float tjac = p.nrm[test].w;
+        const uchar4 rs = p.test_slot[test];
+        const int rslot[3] = {rs.x, rs.y, rs.z};
+        for (int jj = warp; jj < ntrial; jj += kAsmThreads / 32) {
+            const float4 nj = s_nrm[jj];
+            const bool self = (tbase + jj) == test;
+            float are[9], aim[9], sre[3], sim[3];
+            if (s_flag[jj])
+                pair_block<SYM, CK, true>(tx, ty, tz, &s_qp[jj * 6], nj.x, nj.y, nj.z, self, k, kt, ki, are, aim, sre, sim);
+            else
+                pair_block<SYM, CK, false>(tx, ty, tz, &s_qp[jj * 6], nj.x, nj.y, nj.z, self, k, kt, ki, are, aim, sre, sim);
+            const float scale = HBEM_INV4PI * tjac * nj.w;
+            const float4 qb = s_qb[jj];
+            const uchar4 cs = s_cs[jj];
+            const int cslot[3] = {cs.x, cs.y, cs.z};
+            float rob_re = 0.f, rob_im = 0.f;  // -(1/3) i k beta
+            if (qb.z != 0.f || qb.w != 0.f) {
+                // i k beta with k = k + i ki: (-ki + i k)(br + i bi)
+                const float ikb_re = -ki * qb.z - k * qb.w;
+                const float ikb_im = -ki * qb.w + k * qb.z;
+                rob_re = -ikb_re * (1.0f / 3.0f);
+                rob_im = -ikb_im * (1.0f / 3.0f);
+            }
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const float s_re = sre[i] * scale, s_im = sim[i] * scale;
+                const float radd_re = rob_re * s_re - rob_im * s_im;
+                const float radd_im = rob_re * s_im + rob_im * s_re;
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    float vre = are[i * 3 + j] * scale + radd_re;
+                    float vim = aim[i * 3 + j] * scale + radd_im;
+                    if (self) vre -= 0.25f * tjac * (i == j ? (1.0f / 6.0f) : (1.0f / 12.0f));
+                    float2 *dst = &s_acc[rslot[i] * ncols + cslot[j]];
+                    atomicAdd(&dst->x, vre * p.rw);
+                    atomicAdd(&dst->y, vim * p.rw);
+                }
+                if (qb.x != 0.f || qb.y != 0.f) {
+                    atomicAdd(&s_rhs[rslot[i]].x, (s_re * qb.x - s_im * qb.y) * p.rw);
+                    atomicAdd(&s_rhs[rslot[i]].y, (s_re * qb.y + s_im * qb.x) * p.rw);
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    float *are_g = p.a_re + (size_t)f * p.a_stride;
+    float *aim_g = p.a_im + (size_t)f * p.a_stride;
+    for (int e = tid; e < nrows * ncols; e += kAsmThreads) {
+        const int r = e / ncols, c = e - r * ncols;
+        const size_t off = (size_t)p.rows[r0 + r] * p.lda + p.cols[c0 + c];
+        const float2 v = s_acc[e];
+        atomicAdd(are_g + off, v.x);
+        atomicAdd(aim_g + off, v.y);
+    }
+    if (p.q_re && trial_tile >= 0) {
+        for (int r = tid; r < nrows; r += kAsmThreads) {
+            const float2 v = s_rhs[r];
+            if (v.x != 0.f || v.y != 0.f) {
+                const size_t off = (size_t)f * p.b_stride + p.rows[r0 + r];
+                atomicAdd(p.b_re + off, v.x);
+                atomicAdd(p.b_im + off, v.y);
+            }
+        }
+    }
+}
+
+template <int SYM, bool CK>
+cudaError_t launch_regular_t(const AsmArgs &a, dim3 grid, size_t smem, cudaStream_t st) {
+    auto kern = k_regular<SYM, CK>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kern<<<grid, kAsmThreads, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <bool CK>
+cudaError_t dispatch_sym(int sym, const AsmArgs &a, dim3 grid, size_t smem, cudaStream_t st) {
+    switch (sym) {
+        case 0: return launch_regular_t<0, CK>(a, grid, smem, st);
+        case 1: return launch_regular_t<1, CK>(a, grid, smem, st);
+        case 2: return launch_regular_t<2, CK>(a, grid, smem, st);
+        case 3: return launch_regular_t<3, CK>(a, grid, smem, st);
+        default: return launch_regular_t<4, CK>(a, grid, smem, st);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Duffy corrections: one warp per singular pair.  Lanes stride over the
+// pair's Duffy points (+ the 36 regular points, subtracted), each computing
+// the image point geometry, one kernel sample and the 3 SLP + 9 DLP basis
+// products.  Per-lane partial sums and the warp reduction are FP64, so the
+// singular - regular difference is formed in double before the single
+// rounding into A and b.
+// ---------------------------------------------------------------------------
+struct DuffyArgs {
+    const DuffyPair *pairs;
+    const float4 *rule;
+    const float *rule_w;
+    const float *verts;
+    const int *tris;
+    const int *l2g;
+    const float *areas;
+    const float *normals;
+    const float *q_re, *q_im, *beta_re, *beta_im;
+    float *a_re, *a_im, *b_re, *b_im;
+    long long q_stride, lda, a_stride, b_stride;
+    int V, T, n_pairs;
+    int rule_off[3], rule_cnt[3];
+    float k[kMaxFreqPerLaunch];
+    float kt[kMaxFreqPerLaunch];
+    float ki[kMaxFreqPerLaunch];
+};
+
+__device__ __forceinline__ float refx(int l) { return l == 1 ? 1.f : 0.f; }
+__device__ __forceinline__ float refy(int l) { return l == 2 ? 1.f : 0.f; }
+
+// Map a Duffy point onto the shared edge / vertex of the image triangle
+// (main.swift:4213-4231).
+__device__ __forceinline__ void remap(float x, float y, int kind, int l1, int l2, float &ox, float &oy) {
+    if (kind == 2) {
+        const int vc = 3 - l1 - l2;
+        const float ax = refx(l1), ay = refy(l1);
+        ox = ax + x * (refx(l2) - ax) + y * (refx(vc) - ax);
+        oy = ay + x * (refy(l2) - ay) + y * (refy(vc) - ay);
+    } else if (kind == 3 && l1 == 1) {
+        ox = 1.f - x - y;
+        oy = y;
+    } else if (kind == 3 && l1 == 2) {
+        ox = x;
+        oy = 1.f - x - y;
+    } else {
+        ox = x;
+        oy = y;
+    }
+}
+
+template <bool CK>
+__global__ void __launch_bounds__(256) k_duffy(const __grid_constant__ DuffyArgs p) {
+    const int lane = threadIdx.x & 31;
+    const int pi = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (pi >= p.n_pairs) return;
+    const int f = blockIdx.y;
+    const DuffyPair pr = p.pairs[pi];
+    const int V = p.V, T = p.T;
+    float P[3][3], S[3][3];
+#pragma unroll
+    for (int l = 0; l < 3; ++l) {
+        const int vt = p.tris[l * T + pr.test], vs = p.tris[l * T + pr.trial];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            P[l][c] = p.verts[c * V + vt];
+            S[l][c] = p.verts[c * V + vs];
+        }
+    }
+    const float tsx = (pr.test_mask & 1) ? -1.f : 1.f, tsy = (pr.test_mask & 2) ? -1.f : 1.f,
+                tsz = (pr.test_mask & 4) ? -1.f : 1.f;
+    const float ssx = (pr.trial_mask & 1) ? -1.f : 1.f, ssy = (pr.trial_mask & 2) ? -1.f : 1.f,
+                ssz = (pr.trial_mask & 4) ? -1.f : 1.f;
+    const bool tswap = __popc(pr.test_mask) & 1, sswap = __popc(pr.trial_mask) & 1;
+    const float nx = ssx * p.normals[pr.trial], ny = ssy * p.normals[T + pr.trial], nz = ssz * p.normals[2 * T + pr.trial];
+    const float jac = (2.f * p.areas[pr.test]) * (2.f * p.areas[pr.trial]);
+    const float k = p.k[f], kt = p.kt[f], ki = p.ki[f];
+
+    double acc[24];
+#pragma unroll
+    for (int e = 0; e < 24; ++e) acc[e] = 0.0;
+
+    auto accumulate = [&](float txi, float teta, float sxi, float seta, float w) {
+        if (tswap) { const float t = txi; txi = teta; teta = t; }
+        if (sswap) { const float t = sxi; sxi = seta; seta = t; }
+        const float tb[3] = {1.f - txi - teta, txi, teta};
+        const float sb[3] = {1.f - sxi - seta, sxi, seta};
+        float x[3], y[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            x[c] = tb[0] * P[0][c] + tb[1] * P[1][c] + tb[2] * P[2][c];
+            y[c] = sb[0] * S[0][c] + sb[1] * S[1][c] + sb[2] * S[2][c];
+        }
+        float dre = 0, dim = 0, gre = 0, gim = 0;
+        sample<CK, true>(ssx * y[0] - tsx * x[0], ssy * y[1] - tsy * x[1], ssz * y[2] - tsz * x[2], nx, ny, nz, k, kt,
+                         ki, dre, dim, gre, gim);
+        gre *= w; gim *= w; dre *= w; dim *= w;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            acc[2 * i] += (double)(gre * tb[i]);
+            acc[2 * i + 1] += (double)(gim * tb[i]);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const float bb = tb[i] * sb[j];
+                acc[6 + 2 * (i * 3 + j)] += (double)(dre * bb);
+                acc[7 + 2 * (i * 3 + j)] += (double)(dim * bb);
+            }
+        }
+    };
+
+    // regular 6x6 rule, subtracted; the coincident self-point is excluded by
+    // index exactly as in the regular assembly (main.swift:4323-4336)
+    for (int q = lane; q < 36; q += 32) {
+        const int a = q / 6, b = q - 6 * (q / 6);
+        if (pr.test == pr.trial && pr.test_mask == pr.trial_mask && a == b) continue;
+        accumulate(qx(a), qy(a), qx(b), qy(b), -qw(a) * qw(b));
+    }
+    const int ri = pr.kind - 1;
+    const int off = p.rule_off[ri], cnt = p.rule_cnt[ri];
+    for (int q = lane; q < cnt; q += 32) {
+        const float4 r = __ldg(&p.rule[off + q]);
+        const float w = __ldg(&p.rule_w[off + q]);
+        float tx_, ty_, sx_, sy_;
+        remap(r.x, r.y, pr.kind, pr.tl1, pr.tl2, tx_, ty_);
+        remap(r.z, r.w, pr.kind, pr.sl1, pr.sl2, sx_, sy_);
+        accumulate(tx_, ty_, sx_, sy_, w);
+    }
+#pragma unroll
+    for (int e = 0; e < 24; ++e) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc[e] += __shfl_xor_sync(0xffffffffu, acc[e], o);
+    }
+    const double scale = (double)HBEM_INV4PI * (double)jac;
+    // lane e < 9 owns DLP entry e; lanes 9..11 own the SLP rows
+    double sr = 0, si = 0, dr = 0, di = 0;
+#pragma unroll
+    for (int e = 0; e < 9; ++e)
+        if (lane == e) { dr = acc[6 + 2 * e]; di = acc[7 + 2 * e]; }
+    const int i_row = lane < 9 ? lane / 3 : lane - 9;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        if (i_row == i) { sr = acc[2 * i]; si = acc[2 * i + 1]; }
+    sr *= scale; si *= scale; dr *= scale; di *= scale;
+    const float br = p.beta_re ? p.beta_re[pr.trial] : 0.f, bi = p.beta_im ? p.beta_im[pr.trial] : 0.f;
+    if (lane < 9) {
+        const int j = lane - 3 * (lane / 3);
+        if (br != 0.f || bi != 0.f) {
+            const double ikb_re = -(double)ki * br - (double)k * bi, ikb_im = -(double)ki * bi + (double)k * br;
+            dr -= (sr * ikb_re - si * ikb_im) / 3.0;
+            di -= (sr * ikb_im + si * ikb_re) / 3.0;
+        }
+        const size_t o = (size_t)f * p.a_stride + (size_t)p.l2g[pr.test * 3 + i_row] * p.lda + p.l2g[pr.trial * 3 + j];
+        atomicAdd(p.a_re + o, (float)dr);
+        atomicAdd(p.a_im + o, (float)di);
+    } else if (lane < 12 && p.q_re) {
+        const float qr = p.q_re[(size_t)f * p.q_stride + pr.trial], qi = p.q_im[(size_t)f * p.q_stride + pr.trial];
+        if (qr != 0.f || qi != 0.f) {
+            const size_t o = (size_t)f * p.b_stride + p.l2g[pr.test * 3 + i_row];
+            atomicAdd(p.b_re + o, (float)(sr * qr - si * qi));
+            atomicAdd(p.b_im + o, (float)(sr * qi + si * qr));
+        }
+    }
+}
+
+void fill_k(float *k, float *kt, float *ki, const float *k_re, const float *k_im, int n) {
+    for (int f = 0; f < n; ++f) {
+        k[f] = k_re[f];
+        kt[f] = (float)((double)k_re[f] / (2.0 * 3.14159265358979323846));
+        ki[f] = k_im ? k_im[f] : 0.f;
+    }
+}
+
+}  // namespace
+
+int launch_regular(Session &s, int n_freq, const float *k_re, const float *k_im, const float *q_re,
+                   const float *q_im, long long q_stride, const float *beta_re, const float *beta_im, float *a_re,
+                   float *a_im, long long lda, long long a_stride, float *b_re, float *b_im, long long b_stride,
+                   cudaStream_t st) {
+    const size_t smem = (size_t)(s.max_rows * s.max_cols + s.max_rows) * sizeof(float2);
+    if (smem > 180 * 1024)
+        return fail(HBEM_ERR_ARG, "assembly tile needs too much shared memory (mesh ordering too scattered)");
+    for (int f0 = 0; f0 < n_freq; f0 += kMaxFreqPerLaunch) {
+        const int nf = std::min(kMaxFreqPerLaunch, n_freq - f0);
+        AsmArgs a{};
+        a.qp = s.d_qp; a.nrm = s.d_nrm; a.tri = s.d_tri; a.test_slot = s.d_test_slot; a.trial_slot = s.d_trial_slot;
+        a.row_off = s.d_row_off; a.rows = s.d_rows; a.col_off = s.d_col_off; a.cols = s.d_cols;
+        a.q_re = q_re ? q_re + (size_t)f0 * q_stride : nullptr;
+        a.q_im = q_im ? q_im + (size_t)f0 * q_stride : nullptr;
+        a.beta_re = beta_re; a.beta_im = beta_im;
+        a.a_re = a_re + (size_t)f0 * a_stride; a.a_im = a_im + (size_t)f0 * a_stride;
+        a.b_re = b_re ? b_re + (size_t)f0 * b_stride : nullptr;
+        a.b_im = b_im ? b_im + (size_t)f0 * b_stride : nullptr;
+        a.q_stride = q_stride; a.lda = lda; a.a_stride = a_stride; a.b_stride = b_stride;
+        a.T = s.n_triangles;
+        a.rw = (float)(1 << ((s.sym & 1) + ((s.sym >> 1) & 1) + ((s.sym >> 2) & 1)));
+        bool ck = false;
+        fill_k(a.k, a.kt, a.ki, k_re + f0, k_im ? k_im + f0 : nullptr, nf);
+        for (int f = 0; f < nf; ++f) ck |= a.ki[f] != 0.f;
+        if (!a.b_re) a.q_re = a.q_im = nullptr;
+        dim3 grid(s.n_trial_tiles, s.n_test_tiles, nf);
+        cudaError_t e = ck ? dispatch_sym<true>(s.sym, a, grid, smem, st) : dispatch_sym<false>(s.sym, a, grid, smem, st);
+        if (e != cudaSuccess) return cuda_fail(e, "k_regular launch");
+        count_launch();
+        ++s.launches;
+    }
+    return HBEM_OK;
+}
+
+int launch_duffy(Session &s, int n_freq, const float *k_re, const float *k_im, const float *q_re, const float *q_im,
+                 long long q_stride, const float *beta_re, const float *beta_im, float *a_re, float *a_im,
+                 long long lda, long long a_stride, float *b_re, float *b_im, long long b_stride, cudaStream_t st) {
+    if (s.n_pairs == 0) return HBEM_OK;
+    for (int f0 = 0; f0 < n_freq; f0 += kMaxFreqPerLaunch) {
+        const int nf = std::min(kMaxFreqPerLaunch, n_freq - f0);
+        DuffyArgs a{};
+        a.pairs = s.d_pairs; a.rule = s.d_rule; a.rule_w = s.d_rule_w;
+        a.verts = s.d_verts; a.tris = s.d_tris; a.l2g = s.d_l2g; a.areas = s.d_areas; a.normals = s.d_normals;
+        a.q_re = (q_re && b_re) ? q_re + (size_t)f0 * q_stride : nullptr;
+        a.q_im = (q_im && b_re) ? q_im + (size_t)f0 * q_stride : nullptr;
+        a.beta_re = beta_re; a.beta_im = beta_im;
+        a.a_re = a_re + (size_t)f0 * a_stride; a.a_im = a_im + (size_t)f0 * a_stride;
+        a.b_re = b_re ? b_re + (size_t)f0 * b_stride : nullptr;
+        a.b_im = b_im ? b_im + (size_t)f0 * b_stride : nullptr;
+        a.q_stride = q_stride; a.lda = lda; a.a_stride = a_stride; a.b_stride = b_stride;
+        a.V = s.n_vertices; a.T = s.n_triangles; a.n_pairs = s.n_pairs;
+        for (int r = 0; r < 3; ++r) { a.rule_off[r] = s.rule_off[r]; a.rule_cnt[r] = s.rule_cnt[r]; }
+        fill_k(a.k, a.kt, a.ki, k_re + f0, k_im ? k_im + f0 : nullptr, nf);
+        bool ck = false;
+        for (int f = 0; f < nf; ++f) ck |= a.ki[f] != 0.f;
+        dim3 grid((s.n_pairs + 7) / 8, nf);
+        if (ck) k_duffy<true><<<grid, 256, 0, st>>>(a);
+        else k_duffy<false><<<grid, 256, 0, st>>>(a);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(e, "k_duffy launch");
+        count_launch();
+        ++s.launches;
+    }
+    return HBEM_OK;
+}
+
+}  // namespace hbem
+
+using namespace hbem;
+
+extern "C" int hbem_assemble(hbem_session *h, int n_freq, const float *k_re, const float *k_im, const float *q_re,
+                             const float *q_im, long long q_stride, const float *beta_re, const float *beta_im,
+                             float *a_re, float *a_im, long long lda, long long a_stride, float *b_re, float *b_im,
+                             long long b_stride, int flags, void *stream) {
+    Session *s = reinterpret_cast<Session *>(h);
+    if (!s) return fail(HBEM_ERR_ARG, "hbem_assemble: NULL session");
+    if (n_freq <= 0) return HBEM_OK;
+    if (!k_re || !a_re || !a_im) return fail(HBEM_ERR_ARG, "hbem_assemble: NULL k or A pointer");
+    if (lda < s->n_dof || a_stride < lda * s->n_dof) return fail(HBEM_ERR_ARG, "hbem_assemble: lda/a_stride too small");
+    if ((q_re == nullptr) != (q_im == nullptr) || (b_re == nullptr) != (b_im == nullptr))
+        return fail(HBEM_ERR_ARG, "hbem_assemble: real/imag pointers must be given together");
+    if (q_re && q_stride < s->n_triangles) return fail(HBEM_ERR_ARG, "hbem_assemble: q_stride < n_triangles");
+    if (b_re && b_stride < s->n_dof) return fail(HBEM_ERR_ARG, "hbem_assemble: b_stride < n_dof");
+    if ((beta_re == nullptr) != (beta_im == nullptr)) return fail(HBEM_ERR_ARG, "hbem_assemble: beta pointers");
+    for (int f = 0; f < n_freq; ++f)
+        if (!std::isfinite(k_re[f]) || (k_im && !std::isfinite(k_im[f])))
+            return fail(HBEM_ERR_ARG, "hbem_assemble: non-finite wavenumber");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    HBEM_CUDA(cudaSetDevice(s->device));
+    if (flags & HBEM_ASM_ZERO) {
+        if (lda == s->n_dof && a_stride == lda * s->n_dof) {
+            HBEM_CUDA(cudaMemsetAsync(a_re, 0, sizeof(float) * (size_t)a_stride * n_freq, st));
+            HBEM_CUDA(cudaMemsetAsync(a_im, 0, sizeof(float) * (size_t)a_stride * n_freq, st));
+        } else {
+            for (int f = 0; f < n_freq; ++f) {
+                HBEM_CUDA(cudaMemset2DAsync(a_re + (size_t)f * a_stride, lda * sizeof(float), 0, s->n_dof * sizeof(float), s->n_dof, st));
+                HBEM_CUDA(cudaMemset2DAsync(a_im + (size_t)f * a_stride, lda * sizeof(float), 0, s->n_dof * sizeof(float), s->n_dof, st));
+            }
+        }
+        if (b_re) {
+            HBEM_CUDA(cudaMemset2DAsync(b_re, b_stride * sizeof(float), 0, s->n_dof * sizeof(float), n_freq, st));
+            HBEM_CUDA(cudaMemset2DAsync(b_im, b_stride * sizeof(float), 0, s->n_dof * sizeof(float), n_freq, st));
+        }
+    }
+    int rc = HBEM_OK;
+    if (flags & HBEM_ASM_REGULAR)
+        rc = launch_regular(*s, n_freq, k_re, k_im, q_re, q_im, q_stride, beta_re, beta_im, a_re, a_im, lda, a_stride,
+                            b_re, b_im, b_stride, st);
+    if (rc == HBEM_OK && (flags & HBEM_ASM_DUFFY))
+        rc = launch_duffy(*s, n_freq, k_re, k_im, q_re, q_im, q_stride, beta_re, beta_im, a_re, a_im, lda, a_stride,
+                          b_re, b_im, b_stride, st);
+    return rc;
+}

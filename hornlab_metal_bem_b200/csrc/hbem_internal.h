@@ -1,0 +1,135 @@
+// Internal declarations shared by the libhbem.so translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/hbem.h"
+
+namespace hbem {
+
+// ---- error plumbing ------------------------------------------------------
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+void count_launch(long long n = 1);
+
+#define HBEM_CUDA(call)                                        \
+    do {                                                       \
+        cudaError_t _e = (call);                               \
+        if (_e != cudaSuccess) return ::hbem::cuda_fail(_e, #call); \
+    } while (0)
+
+#define HBEM_LAUNCH_CHECK(name)                                \
+    do {                                                       \
+        cudaError_t _e = cudaGetLastError();                   \
+        if (_e != cudaSuccess) return ::hbem::cuda_fail(_e, name); \
+        ::hbem::count_launch();                                \
+    } while (0)
+
+// ---- assembly tiling constants -------------------------------------------
+constexpr int kTestTile = 32;    // test triangles per CTA (one per lane)
+constexpr int kTrialTile = 64;   // trial triangles per CTA (split over 8 warps)
+constexpr int kAsmThreads = 256;
+
+// Duffy pair record (device), 3 x int4.
+struct DuffyPair {
+    int test, trial, test_mask, trial_mask;   // original triangle ids, image masks
+    int kind, tl1, tl2, sl1;                  // 1 coincident, 2 edge, 3 vertex; image-local ids
+    int sl2, row_base, col_base, pad;         // row_base/col_base unused (reserved)
+};
+
+struct Session {
+    int device = 0;
+    int n_vertices = 0, n_triangles = 0, n_dof = 0, sym = 0;
+    // host copies (original order)
+    std::vector<float> verts;      // (3, V)
+    std::vector<int> tris;         // (3, T)
+    std::vector<int> l2g;          // (T, 3)
+    std::vector<int> tags;         // (T,)
+    std::vector<float> areas;      // (T,)
+    std::vector<float> normals;    // (3, T)
+
+    // spatial order used by the tiled assembly: sorted position -> original id
+    std::vector<int> order;
+    int n_test_tiles = 0, n_trial_tiles = 0;
+    int max_rows = 0, max_cols = 0;  // distinct dofs per test / trial tile
+
+    // device geometry, sorted order
+    float4 *d_qp = nullptr;         // (T, 6) quadrature points (x, y, z, 0)
+    float4 *d_nrm = nullptr;        // (T) normal xyz + jacobian 2*area
+    int4 *d_tri = nullptr;          // (T) dof0, dof1, dof2, original id
+    uchar4 *d_test_slot = nullptr;  // (T) slot of each local dof within its test tile
+    uchar4 *d_trial_slot = nullptr; // (T) slot within its trial tile
+    int *d_row_off = nullptr;       // (n_test_tiles + 1)
+    int *d_rows = nullptr;          // concatenated dof lists of test tiles
+    int *d_col_off = nullptr;       // (n_trial_tiles + 1)
+    int *d_cols = nullptr;
+
+    // device geometry, original order (Duffy, field, reductions)
+    float *d_verts = nullptr;       // (3, V)
+    int *d_tris = nullptr;          // (3, T)
+    int *d_l2g = nullptr;           // (T, 3)
+    int *d_tags = nullptr;          // (T)
+    float *d_areas = nullptr;       // (T)
+    float *d_normals = nullptr;     // (3, T)
+    float4 *d_fqp = nullptr;        // (T, 6) quadrature points, original order
+    float4 *d_fnrm = nullptr;       // (T) normal + jac, original order
+
+    // Duffy pairs (sorted by kind) + rule tables
+    int n_pairs = 0;
+    long long n_coincident = 0, n_edge = 0, n_vertex = 0, n_image_pairs = 0, n_unique_triplets = 0;
+    int kind_begin[4] = {0, 0, 0, 0};
+    DuffyPair *d_pairs = nullptr;
+    float4 *d_rule = nullptr;       // test(x,y), trial(x,y) for kinds 1,2,3 concatenated
+    float *d_rule_w = nullptr;
+    int rule_off[3] = {0, 0, 0}, rule_cnt[3] = {0, 0, 0};
+
+    int *d_status = nullptr;        // device-side status word (bounds / wait failures)
+
+    // sweep workspace (grown on demand)
+    void *ws = nullptr;
+    size_t ws_bytes = 0;
+    void *pinned = nullptr;
+    size_t pinned_bytes = 0;
+
+    long long launches = 0;
+};
+
+// ---- pieces implemented in separate translation units ---------------------
+int build_duffy_pairs(Session &s, std::vector<DuffyPair> &pairs);
+void duffy_rule_table(int kind, std::vector<float> &rec);  // 5 floats per point
+
+int launch_regular(Session &s, int n_freq, const float *k_re, const float *k_im,
+                   const float *q_re, const float *q_im, long long q_stride,
+                   const float *beta_re, const float *beta_im,
+                   float *a_re, float *a_im, long long lda, long long a_stride,
+                   float *b_re, float *b_im, long long b_stride, cudaStream_t st);
+int launch_duffy(Session &s, int n_freq, const float *k_re, const float *k_im,
+                 const float *q_re, const float *q_im, long long q_stride,
+                 const float *beta_re, const float *beta_im,
+                 float *a_re, float *a_im, long long lda, long long a_stride,
+                 float *b_re, float *b_im, long long b_stride, cudaStream_t st);
+
+}  // namespace hbem
+
+// Dunavant 6-point degree-4 rule on the reference triangle (xi, eta), weights
+// summing to 1/2 (reference main.swift:1472-1489).
+#define HBEM_QX0 0.4459484909159651f
+#define HBEM_QX1 0.0915762135097710f
+#define HBEM_QX2 0.1081030181680700f
+#define HBEM_QX3 0.4459484909159651f
+#define HBEM_QX4 0.8168475729804590f
+#define HBEM_QX5 0.0915762135097710f
+#define HBEM_QY0 0.4459484909159651f
+#define HBEM_QY1 0.0915762135097700f
+#define HBEM_QY2 0.4459484909159651f
+#define HBEM_QY3 0.1081030181680700f
+#define HBEM_QY4 0.0915762135097700f
+#define HBEM_QY5 0.8168475729804580f
+#define HBEM_QWA 0.1116907948390055f
+#define HBEM_QWB 0.0549758718276610f
+#define HBEM_INV4PI 0.07957747154594767f

@@ -1,0 +1,219 @@
+// One-call batched sweep over host buffers (hbem_solve_batch): the drop-in
+// for the reference's assemble_solve_evaluate_standard_neumann_batch
+// (hornlab_metal_bem/metal/native.py:737-1203, helper main.swift:8869-9878).
+//
+// Frequencies are processed in chunks whose dense matrices fit the device
+// memory budget; within a chunk every stage is one batched launch set on one
+// stream: corrected assembly -> LU -> solve (-> FP64-residual refinement) ->
+// field -> tag reductions.  Nothing round-trips to the host between stages.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "hbem_internal.h"
+
+namespace hbem {
+int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long long a_stride, int *piv,
+              long long piv_stride, int *info, int precision, cudaStream_t st);
+int lu_solve(int n, int nrhs, int batch, const float *lu_re, const float *lu_im, long long lda, long long a_stride,
+             const int *piv, long long piv_stride, float *b_re, float *b_im, long long ldb, long long b_stride,
+             int trans, cudaStream_t st);
+int refine(int n, int batch, const float *a_re, const float *a_im, long long lda, long long a_stride,
+           const float *lu_re, const float *lu_im, long long lu_stride, const int *piv, long long piv_stride,
+           const float *b_re, const float *b_im, long long b_stride, float *x_re, float *x_im, long long x_stride,
+           double tol, int max_iter, int *iters, double *resid, cudaStream_t st);
+int launch_field(Session &s, int n_freq, const float *k_re, const float *p_re, const float *p_im, long long p_stride,
+                 const float *q_re, const float *q_im, long long q_stride, const float *obs, int n_obs, float *out_re,
+                 float *out_im, long long out_stride, cudaStream_t st);
+int launch_tag_avg(Session &s, int n_freq, const float *p_re, const float *p_im, long long p_stride,
+                   const int *d_want, int n_tags, double *out, cudaStream_t st);
+
+namespace {
+
+size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
+
+struct Layout {
+    size_t q, a, a0, x, b, piv, info, obs, fld, tag, want, iters, resid, total;
+};
+
+Layout layout(const Session &s, int nf, int n_obs, int n_tags, bool keep_a) {
+    const size_t n = s.n_dof, T = s.n_triangles;
+    Layout L{};
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off += align_up(bytes); return o; };
+    L.q = take(2 * sizeof(float) * nf * T);
+    L.a = take(2 * sizeof(float) * nf * n * n);
+    L.a0 = keep_a ? take(2 * sizeof(float) * nf * n * n) : 0;
+    L.x = take(2 * sizeof(float) * nf * n);
+    L.b = take(2 * sizeof(float) * nf * n);
+    L.piv = take(sizeof(int) * nf * n);
+    L.info = take(sizeof(int) * nf);
+    L.obs = take(3 * sizeof(float) * std::max(1, n_obs));
+    L.fld = take(2 * sizeof(float) * nf * std::max(1, n_obs));
+    L.tag = take(2 * sizeof(double) * nf * std::max(1, n_tags));
+    L.want = take(sizeof(int) * std::max(1, n_tags));
+    L.iters = take(sizeof(int) * nf);
+    L.resid = take(sizeof(double) * nf);
+    L.total = off;
+    return L;
+}
+
+int ensure_ws(Session &s, size_t bytes) {
+    if (s.ws_bytes >= bytes) return HBEM_OK;
+    if (s.ws) cudaFree(s.ws);
+    s.ws = nullptr;
+    s.ws_bytes = 0;
+    HBEM_CUDA(cudaMalloc(&s.ws, bytes));
+    s.ws_bytes = bytes;
+    return HBEM_OK;
+}
+
+}  // namespace
+}  // namespace hbem
+
+using namespace hbem;
+
+extern "C" int hbem_solve_batch(hbem_session *h, int n_freq, const float *k_re, const float *k_im, const float *q_re,
+                                const float *q_im, const float *obs_3xn, int n_obs, const int *tags, int n_tags,
+                                int precision, double refine_tol, int refine_max_iter, float *field_re,
+                                float *field_im, double *tag_avg, float *surface_re, float *surface_im, int *info,
+                                int *refine_iters, double *refine_resid, float *timings_ms, void *stream) {
+    Session *s = reinterpret_cast<Session *>(h);
+    if (!s) return fail(HBEM_ERR_ARG, "hbem_solve_batch: NULL session");
+    if (n_freq <= 0) return HBEM_OK;
+    if (!k_re || !q_re || !q_im || !info) return fail(HBEM_ERR_ARG, "hbem_solve_batch: NULL input");
+    if (n_obs > 0 && (!obs_3xn || !field_re || !field_im)) return fail(HBEM_ERR_ARG, "hbem_solve_batch: NULL field buffers");
+    if (n_tags > 0 && (!tags || !tag_avg)) return fail(HBEM_ERR_ARG, "hbem_solve_batch: NULL tag buffers");
+    if (n_tags > 64) return fail(HBEM_ERR_ARG, "hbem_solve_batch: at most 64 tags");
+    if ((surface_re == nullptr) != (surface_im == nullptr)) return fail(HBEM_ERR_ARG, "hbem_solve_batch: surface pointers");
+    if (precision != HBEM_PREC_PLAIN && precision != HBEM_PREC_MIXED)
+        return fail(HBEM_ERR_ARG, "hbem_solve_batch: bad precision");
+    for (int f = 0; f < n_freq; ++f)
+        if (!std::isfinite(k_re[f]) || (k_im && !std::isfinite(k_im[f])))
+            return fail(HBEM_ERR_ARG, "hbem_solve_batch: non-finite wavenumber");
+    HBEM_CUDA(cudaSetDevice(s->device));
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const bool do_refine = (precision == HBEM_PREC_MIXED) || refine_max_iter > 0;
+    const int max_iter = precision == HBEM_PREC_MIXED ? std::max(1, refine_max_iter) : refine_max_iter;
+    const double tol = refine_tol > 0 ? refine_tol : 1e-6;
+    const size_t n = s->n_dof, T = s->n_triangles;
+
+    // chunk size: dense matrices within ~60 % of free memory
+    size_t free_b = 0, total_b = 0;
+    HBEM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    free_b += s->ws_bytes;
+    int chunk = n_freq;
+    while (chunk > 1 && layout(*s, chunk, n_obs, n_tags, do_refine).total > free_b * 6 / 10) chunk = (chunk + 1) / 2;
+    const Layout L = layout(*s, chunk, n_obs, n_tags, do_refine);
+    int rc = ensure_ws(*s, L.total);
+    if (rc != HBEM_OK) return rc;
+    char *ws = static_cast<char *>(s->ws);
+    float *dq = reinterpret_cast<float *>(ws + L.q);
+    float *da = reinterpret_cast<float *>(ws + L.a);
+    float *da0 = do_refine ? reinterpret_cast<float *>(ws + L.a0) : nullptr;
+    float *dx = reinterpret_cast<float *>(ws + L.x);
+    float *db = reinterpret_cast<float *>(ws + L.b);
+    int *dpiv = reinterpret_cast<int *>(ws + L.piv);
+    int *dinfo = reinterpret_cast<int *>(ws + L.info);
+    float *dobs = reinterpret_cast<float *>(ws + L.obs);
+    float *dfld = reinterpret_cast<float *>(ws + L.fld);
+    double *dtag = reinterpret_cast<double *>(ws + L.tag);
+    int *dwant = reinterpret_cast<int *>(ws + L.want);
+    int *diters = reinterpret_cast<int *>(ws + L.iters);
+    double *dres = reinterpret_cast<double *>(ws + L.resid);
+
+    cudaEvent_t ev[5];
+    for (auto &e : ev) HBEM_CUDA(cudaEventCreate(&e));
+    float t_asm = 0, t_solve = 0, t_field = 0, t_total = 0;
+    HBEM_CUDA(cudaEventRecord(ev[4], st));
+    if (n_obs > 0) HBEM_CUDA(cudaMemcpyAsync(dobs, obs_3xn, 3 * sizeof(float) * n_obs, cudaMemcpyHostToDevice, st));
+    if (n_tags > 0) HBEM_CUDA(cudaMemcpyAsync(dwant, tags, sizeof(int) * n_tags, cudaMemcpyHostToDevice, st));
+
+    for (int f0 = 0; f0 < n_freq && rc == HBEM_OK; f0 += chunk) {
+        const int nf = std::min(chunk, n_freq - f0);
+        float *qr = dq, *qi = dq + (size_t)nf * T;
+        HBEM_CUDA(cudaMemcpyAsync(qr, q_re + (size_t)f0 * T, sizeof(float) * nf * T, cudaMemcpyHostToDevice, st));
+        HBEM_CUDA(cudaMemcpyAsync(qi, q_im + (size_t)f0 * T, sizeof(float) * nf * T, cudaMemcpyHostToDevice, st));
+        float *ar = da, *ai = da + (size_t)nf * n * n;
+        float *br = db, *bi = db + (size_t)nf * n;
+        float *xr = dx, *xi = dx + (size_t)nf * n;
+        HBEM_CUDA(cudaEventRecord(ev[0], st));
+        rc = hbem_assemble(h, nf, k_re + f0, k_im ? k_im + f0 : nullptr, qr, qi, (long long)T, nullptr, nullptr, ar, ai,
+                           (long long)n, (long long)(n * n), br, bi, (long long)n, HBEM_ASM_CORRECTED, st);
+        if (rc != HBEM_OK) break;
+        HBEM_CUDA(cudaEventRecord(ev[1], st));
+        HBEM_CUDA(cudaMemcpyAsync(xr, br, sizeof(float) * nf * n, cudaMemcpyDeviceToDevice, st));
+        HBEM_CUDA(cudaMemcpyAsync(xi, bi, sizeof(float) * nf * n, cudaMemcpyDeviceToDevice, st));
+        float *a0r = nullptr, *a0i = nullptr;
+        if (do_refine) {
+            a0r = da0;
+            a0i = da0 + (size_t)nf * n * n;
+            HBEM_CUDA(cudaMemcpyAsync(a0r, ar, sizeof(float) * nf * n * n, cudaMemcpyDeviceToDevice, st));
+            HBEM_CUDA(cudaMemcpyAsync(a0i, ai, sizeof(float) * nf * n * n, cudaMemcpyDeviceToDevice, st));
+        }
+        rc = lu_factor((int)n, nf, ar, ai, (long long)n, (long long)(n * n), dpiv, (long long)n, dinfo, precision, st);
+        if (rc != HBEM_OK) break;
+        rc = lu_solve((int)n, 1, nf, ar, ai, (long long)n, (long long)(n * n), dpiv, (long long)n, xr, xi, 1,
+                      (long long)n, HBEM_TRANS_N, st);
+        if (rc != HBEM_OK) break;
+        if (do_refine) {
+            rc = refine((int)n, nf, a0r, a0i, (long long)n, (long long)(n * n), ar, ai, (long long)(n * n), dpiv,
+                        (long long)n, br, bi, (long long)n, xr, xi, (long long)n, tol, max_iter, diters, dres, st);
+            if (rc != HBEM_OK) break;
+        }
+        HBEM_CUDA(cudaEventRecord(ev[2], st));
+        float *fr = dfld, *fi = dfld + (size_t)nf * std::max(1, n_obs);
+        if (n_obs > 0) {
+            rc = launch_field(*s, nf, k_re + f0, xr, xi, (long long)n, qr, qi, (long long)T, dobs, n_obs, fr, fi,
+                              (long long)n_obs, st);
+            if (rc != HBEM_OK) break;
+        }
+        if (n_tags > 0) {
+            rc = launch_tag_avg(*s, nf, xr, xi, (long long)n, dwant, n_tags, dtag, st);
+            if (rc != HBEM_OK) break;
+        }
+        HBEM_CUDA(cudaEventRecord(ev[3], st));
+        if (n_obs > 0) {
+            HBEM_CUDA(cudaMemcpyAsync(field_re + (size_t)f0 * n_obs, fr, sizeof(float) * nf * n_obs, cudaMemcpyDeviceToHost, st));
+            HBEM_CUDA(cudaMemcpyAsync(field_im + (size_t)f0 * n_obs, fi, sizeof(float) * nf * n_obs, cudaMemcpyDeviceToHost, st));
+        }
+        if (n_tags > 0)
+            HBEM_CUDA(cudaMemcpyAsync(tag_avg + (size_t)f0 * n_tags * 2, dtag, 2 * sizeof(double) * nf * n_tags,
+                                      cudaMemcpyDeviceToHost, st));
+        if (surface_re) {
+            HBEM_CUDA(cudaMemcpyAsync(surface_re + (size_t)f0 * n, xr, sizeof(float) * nf * n, cudaMemcpyDeviceToHost, st));
+            HBEM_CUDA(cudaMemcpyAsync(surface_im + (size_t)f0 * n, xi, sizeof(float) * nf * n, cudaMemcpyDeviceToHost, st));
+        }
+        HBEM_CUDA(cudaMemcpyAsync(info + f0, dinfo, sizeof(int) * nf, cudaMemcpyDeviceToHost, st));
+        if (do_refine && refine_iters)
+            HBEM_CUDA(cudaMemcpyAsync(refine_iters + f0, diters, sizeof(int) * nf, cudaMemcpyDeviceToHost, st));
+        if (do_refine && refine_resid)
+            HBEM_CUDA(cudaMemcpyAsync(refine_resid + f0, dres, sizeof(double) * nf, cudaMemcpyDeviceToHost, st));
+        HBEM_CUDA(cudaStreamSynchronize(st));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ev[0], ev[1]); t_asm += ms;
+        cudaEventElapsedTime(&ms, ev[1], ev[2]); t_solve += ms;
+        cudaEventElapsedTime(&ms, ev[2], ev[3]); t_field += ms;
+    }
+    if (rc == HBEM_OK) {
+        cudaEventRecord(ev[0], st);
+        cudaStreamSynchronize(st);
+        cudaEventElapsedTime(&t_total, ev[4], ev[0]);
+        if (!do_refine) {
+            if (refine_iters) std::memset(refine_iters, 0, sizeof(int) * n_freq);
+            if (refine_resid) std::memset(refine_resid, 0, sizeof(double) * n_freq);
+        }
+        if (timings_ms) {
+            timings_ms[0] = t_asm;
+            timings_ms[1] = t_solve;
+            timings_ms[2] = t_field;
+            timings_ms[3] = t_total;
+        }
+    } else {
+        cudaStreamSynchronize(st);
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    return rc;
+}

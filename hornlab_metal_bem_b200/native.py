@@ -1,0 +1,453 @@
+"""ctypes binding of ``libhbem.so`` and the session object of the B200 path.
+
+``NativeSession`` stands where the reference's ``MetalNativeStandardSession``
+stands (``hornlab_metal_bem/metal/native.py:233-1203``): it owns one mesh's
+resident geometry on the GPU and runs the batched
+assemble -> LU -> solve -> field -> reductions operation.  Instead of a helper
+subprocess with JSON manifests and float32 files, every call goes through the
+C ABI declared in ``include/hbem.h``.
+
+There is no CPU fallback: if the library is missing or no CUDA device is
+visible, construction raises ``BackendUnavailable``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import time
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Any
+
+import numpy as np
+
+from .config import SYMMETRY_CODES
+from .geometry import (
+    GeometryBuffers,
+    validate_native_infinite_baffle_aperture,
+    validate_native_symmetry_plane,
+)
+
+LIB_PATH = Path(__file__).resolve().parent / "libhbem.so"
+
+HBEM_OK = 0
+HBEM_ASM_REGULAR = 1
+HBEM_ASM_DUFFY = 2
+HBEM_ASM_ZERO = 4
+HBEM_ASM_CORRECTED = 7
+HBEM_PREC_PLAIN = 0
+HBEM_PREC_MIXED = 1
+HBEM_TRANS_N, HBEM_TRANS_T, HBEM_TRANS_C = 0, 1, 2
+QUERY_KEYS = {
+    "n_dof": 0, "n_triangles": 1, "n_pairs": 2, "coincident": 3, "edge": 4, "vertex": 5,
+    "image_pairs": 6, "unique_triplets": 7, "symmetry": 8, "kernel_launches": 9,
+    "regular_evals": 10, "duffy_evals": 11,
+}
+
+
+class BackendUnavailable(RuntimeError):
+    """The CUDA library or device needed by the B200 path is not available."""
+
+
+# Drop-in alias for the reference's exception name (hornlab_metal_bem/backends.py).
+AssemblyBackendUnavailable = BackendUnavailable
+
+_c_int, _c_ll, _c_d, _vp = ctypes.c_int, ctypes.c_longlong, ctypes.c_double, ctypes.c_void_p
+_SIGNATURES = {
+    "hbem_version": ([], _c_int),
+    "hbem_last_error": ([ctypes.c_char_p, ctypes.c_size_t], _c_int),
+    "hbem_launch_count": ([], _c_ll),
+    "hbem_session_create": ([_vp, _c_int, _vp, _c_int, _vp, _c_int, _vp, _vp, _vp, _c_int, _c_int,
+                             ctypes.POINTER(_vp)], _c_int),
+    "hbem_session_destroy": ([_vp], _c_int),
+    "hbem_session_query": ([_vp, _c_int, ctypes.POINTER(_c_ll)], _c_int),
+    "hbem_assemble": ([_vp, _c_int, _vp, _vp, _vp, _vp, _c_ll, _vp, _vp, _vp, _vp, _c_ll, _c_ll, _vp, _vp, _c_ll,
+                       _c_int, _vp], _c_int),
+    "hbem_lu_factor": ([_c_int, _c_int, _vp, _vp, _c_ll, _c_ll, _vp, _c_ll, _vp, _c_int, _vp], _c_int),
+    "hbem_lu_solve": ([_c_int, _c_int, _c_int, _vp, _vp, _c_ll, _c_ll, _vp, _c_ll, _vp, _vp, _c_ll, _c_ll, _c_int,
+                       _vp], _c_int),
+    "hbem_refine": ([_c_int, _c_int, _vp, _vp, _c_ll, _c_ll, _vp, _vp, _c_ll, _vp, _c_ll, _vp, _vp, _c_ll, _vp, _vp,
+                     _c_ll, _c_d, _c_int, _vp, _vp, _vp], _c_int),
+    "hbem_field": ([_vp, _c_int, _vp, _vp, _vp, _c_ll, _vp, _vp, _c_ll, _vp, _c_int, _vp, _vp, _c_ll, _vp], _c_int),
+    "hbem_reduce_tag_avg": ([_vp, _c_int, _vp, _vp, _c_ll, _vp, _c_int, _vp, _vp], _c_int),
+    "hbem_solve_batch": ([_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _c_int, _vp, _c_int, _c_int, _c_d, _c_int, _vp, _vp,
+                          _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _c_int),
+}
+
+_LIB: ctypes.CDLL | None = None
+
+
+def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
+    """Load ``libhbem.so`` (built in-tree) and declare every exported signature."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    p = Path(path) if path is not None else LIB_PATH
+    if not p.exists():
+        raise BackendUnavailable(
+            f"{p} is not built; run `python -m hornlab_metal_bem_b200.csrc.build` (nvcc, sm_100a)"
+        )
+    lib = ctypes.CDLL(str(p))
+    for name, (args, res) in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    if path is None:
+        _LIB = lib
+    return lib
+
+
+def last_error(lib: ctypes.CDLL | None = None) -> str:
+    lib = lib or load_library()
+    buf = ctypes.create_string_buffer(2048)
+    lib.hbem_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(status: int, what: str, lib: ctypes.CDLL | None = None) -> int:
+    if status < 0:
+        raise RuntimeError(f"{what} failed ({status}): {last_error(lib)}")
+    return status
+
+
+def _np_ptr(a: np.ndarray | None):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def _t_ptr(t):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def _stream_ptr(stream=None):
+    import torch
+
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def require_cuda():
+    import torch
+
+    if not torch.cuda.is_available():
+        raise BackendUnavailable("no CUDA device is visible; the B200 path has no CPU fallback")
+    return torch
+
+
+@dataclass
+class CaseResult:
+    """One solved frequency (the reference's ``DenseSolveFieldResult``, in memory)."""
+
+    frequency_hz: float
+    field: np.ndarray                      # (N_obs,) complex64
+    impedance: complex | None
+    surface_pressure_avg: dict[int, complex] | None
+    surface_pressure: np.ndarray | None    # (n_dof,) complex64
+    assembly_s: float
+    dense_solve_s: float
+    field_s: float
+    lapack_info: int
+    diagnostics: dict[str, Any] = field(default_factory=dict)
+
+
+class NativeSession:
+    """One mesh resident on one GPU (``hbem_session``)."""
+
+    def __init__(self, geometry_buffers: GeometryBuffers, *, symmetry_plane: str | None = None,
+                 aperture_tag: int | None = None, velocity_source_tags=None, check_open_edges: bool = True,
+                 device: int | None = None):
+        torch = require_cuda()
+        self.lib = load_library()
+        self.buffers = geometry_buffers
+        self.symmetry_plane = validate_native_symmetry_plane(
+            geometry_buffers, symmetry_plane, check_open_edges=check_open_edges
+        )
+        self.aperture_tag = validate_native_infinite_baffle_aperture(
+            geometry_buffers, aperture_tag, velocity_source_tags=velocity_source_tags,
+            symmetry_plane=self.symmetry_plane,
+        )
+        self.sym_code = SYMMETRY_CODES[self.symmetry_plane]
+        self.device = torch.cuda.current_device() if device is None else int(device)
+        b = geometry_buffers
+        self._host = [
+            np.ascontiguousarray(b.vertices_3xn_f32, dtype=np.float32),
+            np.ascontiguousarray(b.triangles_3xm_i32, dtype=np.int32),
+            np.ascontiguousarray(b.p1_local2global_i32, dtype=np.int32),
+            np.ascontiguousarray(b.physical_tags_i32, dtype=np.int32),
+            np.ascontiguousarray(b.triangle_areas_f32, dtype=np.float32),
+            np.ascontiguousarray(b.triangle_normals_3xm_f32, dtype=np.float32),
+        ]
+        v, t, l2g, tags, areas, normals = self._host
+        handle = ctypes.c_void_p()
+        t0 = time.perf_counter()
+        check(self.lib.hbem_session_create(
+            _np_ptr(v), v.shape[1], _np_ptr(t), t.shape[1], _np_ptr(l2g), int(b.p1_dof_count), _np_ptr(tags),
+            _np_ptr(areas), _np_ptr(normals), self.sym_code, self.device, ctypes.byref(handle)),
+            "hbem_session_create", self.lib)
+        self.setup_s = time.perf_counter() - t0
+        self.handle = handle
+        self.n_dof = int(b.p1_dof_count)
+        self.n_triangles = int(t.shape[1])
+
+    # -- lifecycle -------------------------------------------------------------
+    @classmethod
+    def create_session(cls, *, geometry_buffers, symmetry_plane=None, aperture_tag=None, velocity_source_tags=None,
+                       check_open_edges=True, device=None, **_ignored) -> "NativeSession":
+        return cls(geometry_buffers, symmetry_plane=symmetry_plane, aperture_tag=aperture_tag,
+                   velocity_source_tags=velocity_source_tags, check_open_edges=check_open_edges, device=device)
+
+    def close(self) -> None:
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            self.lib.hbem_session_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown ordering
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def query(self, key: str) -> int:
+        out = ctypes.c_longlong()
+        check(self.lib.hbem_session_query(self.handle, QUERY_KEYS[key], ctypes.byref(out)), "hbem_session_query")
+        return int(out.value)
+
+    def pair_plan(self) -> dict[str, int]:
+        c, e, v = self.query("coincident"), self.query("edge"), self.query("vertex")
+        return {"coincident": c, "edge": e, "vertex": v, "total": c + e + v}
+
+    # -- device primitives (torch tensors in, torch tensors out) ---------------
+    def assemble(self, k_re, q, *, k_imag=None, beta=None, flags: int = HBEM_ASM_CORRECTED, stream=None):
+        """Return ``(A_re, A_im, b_re, b_im)`` float32 CUDA tensors of shape (F, n, n) / (F, n)."""
+        torch = require_cuda()
+        k_re = np.ascontiguousarray(np.atleast_1d(k_re), dtype=np.float32)
+        F = k_re.shape[0]
+        k_im = None if k_imag is None else np.ascontiguousarray(np.atleast_1d(k_imag), dtype=np.float32)
+        dev = torch.device("cuda", self.device)
+        qr, qi = self._split_device(q, (F, self.n_triangles), dev)
+        br_, bi_ = (None, None) if beta is None else self._split_device(beta, (self.n_triangles,), dev)
+        n = self.n_dof
+        Ar = torch.empty((F, n, n), dtype=torch.float32, device=dev)
+        Ai = torch.empty_like(Ar)
+        b_re = torch.empty((F, n), dtype=torch.float32, device=dev)
+        b_im = torch.empty_like(b_re)
+        check(self.lib.hbem_assemble(
+            self.handle, F, _np_ptr(k_re), _np_ptr(k_im), _t_ptr(qr), _t_ptr(qi), self.n_triangles, _t_ptr(br_),
+            _t_ptr(bi_), _t_ptr(Ar), _t_ptr(Ai), n, n * n, _t_ptr(b_re), _t_ptr(b_im), n, flags | HBEM_ASM_ZERO,
+            _stream_ptr(stream)), "hbem_assemble", self.lib)
+        return Ar, Ai, b_re, b_im
+
+    @staticmethod
+    def _split_device(z, shape, dev):
+        import torch
+
+        if isinstance(z, tuple):
+            return z
+        arr = np.asarray(z).reshape(shape)
+        re = torch.from_numpy(np.ascontiguousarray(arr.real, dtype=np.float32)).to(dev)
+        im = torch.from_numpy(np.ascontiguousarray(arr.imag, dtype=np.float32)).to(dev)
+        return re, im
+
+    def field(self, k_re, p_re, p_im, q, obs_3xn, stream=None):
+        torch = require_cuda()
+        k_re = np.ascontiguousarray(np.atleast_1d(k_re), dtype=np.float32)
+        F = k_re.shape[0]
+        dev = p_re.device
+        qr, qi = self._split_device(q, (F, self.n_triangles), dev)
+        obs = torch.as_tensor(np.ascontiguousarray(obs_3xn, dtype=np.float32), device=dev)
+        N = obs.shape[1]
+        out_re = torch.empty((F, N), dtype=torch.float32, device=dev)
+        out_im = torch.empty_like(out_re)
+        check(self.lib.hbem_field(
+            self.handle, F, _np_ptr(k_re), _t_ptr(p_re), _t_ptr(p_im), p_re.stride(0), _t_ptr(qr), _t_ptr(qi),
+            qr.stride(0), _t_ptr(obs), N, _t_ptr(out_re), _t_ptr(out_im), N, _stream_ptr(stream)), "hbem_field", self.lib)
+        return out_re, out_im
+
+    def tag_average(self, p_re, p_im, tags, stream=None):
+        torch = require_cuda()
+        tags = np.ascontiguousarray(tags, dtype=np.int32)
+        F = p_re.shape[0]
+        out = torch.empty((F, tags.shape[0], 2), dtype=torch.float64, device=p_re.device)
+        check(self.lib.hbem_reduce_tag_avg(
+            self.handle, F, _t_ptr(p_re), _t_ptr(p_im), p_re.stride(0), _np_ptr(tags), tags.shape[0], _t_ptr(out),
+            _stream_ptr(stream)), "hbem_reduce_tag_avg", self.lib)
+        return out
+
+    # -- the reference-facing batched operation -------------------------------
+    def assemble_solve_evaluate_standard_neumann_batch(
+        self,
+        frequency_hz,
+        k_real_f32,
+        neumann_dp0,
+        observation_points,
+        *,
+        k_imag_f32=None,
+        source_tags=None,
+        impedance_source_tag=None,
+        write_surface_pressure: bool = False,
+        dense_solve_dtype: str = "float32",
+        precision: str = "plain",
+        refine_tolerance: float = 1e-6,
+        refine_max_iterations: int = 10,
+        timings_out: dict | None = None,
+        **_ignored,
+    ) -> list[CaseResult]:
+        """Assemble, factor, solve and evaluate every frequency in one native call.
+
+        Same argument meaning as the reference (``native.py:737-764``):
+        ``frequency_hz`` (F,), ``k_real_f32`` (F,) float32 wavenumbers,
+        ``neumann_dp0`` (F, T) complex DP0 Neumann data, ``observation_points``
+        (3, N) or (N, 3).  ``dense_solve_dtype="float64"`` keeps the FP32 LU and
+        refines the solution with FP64 residuals to 1e-7 (the GPU analogue of
+        the reference's complex128 zgesv path).
+        """
+        freqs = np.ascontiguousarray(np.atleast_1d(frequency_hz), dtype=np.float64)
+        F = freqs.shape[0]
+        k_re = np.ascontiguousarray(np.atleast_1d(k_real_f32), dtype=np.float32)
+        if k_re.shape != (F,):
+            raise ValueError("k_real_f32 must have one value per frequency")
+        k_im = None if k_imag_f32 is None else np.ascontiguousarray(np.atleast_1d(k_imag_f32), dtype=np.float32)
+        q = np.asarray(neumann_dp0)
+        if q.shape != (F, self.n_triangles):
+            raise ValueError(f"neumann_dp0 must have shape {(F, self.n_triangles)}, got {q.shape}")
+        if not np.all(np.isfinite(q)):
+            raise ValueError("neumann_dp0 must be finite")
+        obs = np.asarray(observation_points, dtype=np.float64)
+        if obs.ndim != 2 or 3 not in obs.shape:
+            raise ValueError("observation_points must have shape (3, N) or (N, 3)")
+        if obs.shape[0] != 3:
+            obs = obs.T
+        obs = np.ascontiguousarray(obs, dtype=np.float32)
+        N = obs.shape[1]
+        tags = list(source_tags or [])
+        imp_tag = impedance_source_tag
+        want = list(tags) + ([imp_tag] if imp_tag is not None and imp_tag not in tags else [])
+        want_arr = np.ascontiguousarray(want, dtype=np.int32) if want else np.zeros(1, np.int32)
+        qr = np.ascontiguousarray(q.real, dtype=np.float32)
+        qi = np.ascontiguousarray(q.imag, dtype=np.float32)
+        fr = np.zeros((F, N), np.float32)
+        fi = np.zeros((F, N), np.float32)
+        tavg = np.zeros((F, max(1, len(want)), 2), np.float64)
+        sr = np.zeros((F, self.n_dof), np.float32) if write_surface_pressure else None
+        si = np.zeros((F, self.n_dof), np.float32) if write_surface_pressure else None
+        info = np.zeros(F, np.int32)
+        iters = np.zeros(F, np.int32)
+        resid = np.zeros(F, np.float64)
+        tms = np.zeros(4, np.float32)
+        prec = HBEM_PREC_MIXED if precision == "mixed" else HBEM_PREC_PLAIN
+        max_it = int(refine_max_iterations) if (prec == HBEM_PREC_MIXED or dense_solve_dtype == "float64") else 0
+        tol = 1e-7 if (dense_solve_dtype == "float64" and prec == HBEM_PREC_PLAIN) else float(refine_tolerance)
+        t0 = time.perf_counter()
+        check(self.lib.hbem_solve_batch(
+            self.handle, F, _np_ptr(k_re), _np_ptr(k_im), _np_ptr(qr), _np_ptr(qi), _np_ptr(obs), N,
+            _np_ptr(want_arr), len(want), prec, tol, max_it, _np_ptr(fr), _np_ptr(fi), _np_ptr(tavg), _np_ptr(sr),
+            _np_ptr(si), _np_ptr(info), _np_ptr(iters), _np_ptr(resid), _np_ptr(tms), None), "hbem_solve_batch", self.lib)
+        wall = time.perf_counter() - t0
+        if timings_out is not None:
+            timings_out.update(assembly_ms=float(tms[0]), solve_ms=float(tms[1]), field_ms=float(tms[2]),
+                               total_ms=float(tms[3]), wall_s=wall)
+        per = 1.0 / F
+        results = []
+        for f in range(F):
+            avgs = {int(t): complex(tavg[f, j, 0], tavg[f, j, 1]) for j, t in enumerate(want)}
+            diag = {
+                "dense_solve_impl": "hbem_blocked_lu_" + ("bf16x3_refined" if prec else "fp32"),
+                "dense_solve_dtype": dense_solve_dtype,
+                "precision": precision,
+                "refine_iterations": int(iters[f]),
+                "refine_residual_rel": float(resid[f]) if max_it > 0 else None,
+                "dense_solve_rcond": None,
+                "assembly_mode": "corrected",
+                "duffy_pairs": None,
+            }
+            results.append(CaseResult(
+                frequency_hz=float(freqs[f]),
+                field=(fr[f] + 1j * fi[f]).astype(np.complex64),
+                impedance=avgs.get(int(imp_tag)) if imp_tag is not None else None,
+                surface_pressure_avg={int(t): avgs[int(t)] for t in tags} if tags else None,
+                surface_pressure=None if sr is None else (sr[f] + 1j * si[f]).astype(np.complex64),
+                assembly_s=float(tms[0]) * 1e-3 * per,
+                dense_solve_s=float(tms[1]) * 1e-3 * per,
+                field_s=float(tms[2]) * 1e-3 * per,
+                lapack_info=int(info[f]),
+                diagnostics=diag,
+            ))
+        return results
+
+
+# Drop-in alias for the reference's session class name.
+MetalNativeStandardSession = NativeSession
+
+
+class ResidentSweep:
+    """Device-resident batched sweep: inputs and outputs stay in HBM.
+
+    Pre-allocates, for ``F`` frequencies on one session, the dense matrices,
+    right-hand sides, pivots and field buffers, then ``run()`` issues the same
+    launch sequence as ``hbem_solve_batch`` on the current stream without any
+    host transfer: corrected assembly -> LU -> solve -> field -> tag averages.
+    """
+
+    def __init__(self, session: NativeSession, k_re, k_im, q, obs_3xn, tags, precision: str = "plain"):
+        torch = require_cuda()
+        self.s = session
+        self.lib = session.lib
+        dev = torch.device("cuda", session.device)
+        self.k_re = np.ascontiguousarray(np.atleast_1d(k_re), dtype=np.float32)
+        self.k_im = None if k_im is None else np.ascontiguousarray(np.atleast_1d(k_im), dtype=np.float32)
+        F, n, T = self.k_re.shape[0], session.n_dof, session.n_triangles
+        self.F, self.n = F, n
+        self.q_re, self.q_im = NativeSession._split_device(q, (F, T), dev)
+        self.obs = torch.as_tensor(np.ascontiguousarray(obs_3xn, dtype=np.float32), device=dev)
+        self.n_obs = int(self.obs.shape[1])
+        self.tags = np.ascontiguousarray(tags, dtype=np.int32)
+        self.A_re = torch.empty((F, n, n), dtype=torch.float32, device=dev)
+        self.A_im = torch.empty_like(self.A_re)
+        self.b_re = torch.empty((F, n), dtype=torch.float32, device=dev)
+        self.b_im = torch.empty_like(self.b_re)
+        self.x_re = torch.empty_like(self.b_re)
+        self.x_im = torch.empty_like(self.b_re)
+        self.piv = torch.empty((F, n), dtype=torch.int32, device=dev)
+        self.info = torch.empty(F, dtype=torch.int32, device=dev)
+        self.f_re = torch.empty((F, self.n_obs), dtype=torch.float32, device=dev)
+        self.f_im = torch.empty_like(self.f_re)
+        self.tag_out = torch.empty((F, max(1, self.tags.shape[0]), 2), dtype=torch.float64, device=dev)
+        self.precision = HBEM_PREC_MIXED if precision == "mixed" else HBEM_PREC_PLAIN
+
+    def assemble(self, stream=None):
+        n = self.n
+        check(self.lib.hbem_assemble(
+            self.s.handle, self.F, _np_ptr(self.k_re), _np_ptr(self.k_im), _t_ptr(self.q_re), _t_ptr(self.q_im),
+            self.q_re.stride(0), None, None, _t_ptr(self.A_re), _t_ptr(self.A_im), n, n * n, _t_ptr(self.b_re),
+            _t_ptr(self.b_im), n, HBEM_ASM_CORRECTED, _stream_ptr(stream)), "hbem_assemble", self.lib)
+
+    def factor_solve(self, stream=None):
+        n, st = self.n, _stream_ptr(stream)
+        self.x_re.copy_(self.b_re)
+        self.x_im.copy_(self.b_im)
+        check(self.lib.hbem_lu_factor(n, self.F, _t_ptr(self.A_re), _t_ptr(self.A_im), n, n * n, _t_ptr(self.piv), n,
+                                      _t_ptr(self.info), self.precision, st), "hbem_lu_factor", self.lib)
+        check(self.lib.hbem_lu_solve(n, 1, self.F, _t_ptr(self.A_re), _t_ptr(self.A_im), n, n * n, _t_ptr(self.piv), n,
+                                     _t_ptr(self.x_re), _t_ptr(self.x_im), 1, n, HBEM_TRANS_N, st), "hbem_lu_solve",
+              self.lib)
+
+    def field(self, stream=None):
+        st = _stream_ptr(stream)
+        check(self.lib.hbem_field(
+            self.s.handle, self.F, _np_ptr(self.k_re), _t_ptr(self.x_re), _t_ptr(self.x_im), self.n,
+            _t_ptr(self.q_re), _t_ptr(self.q_im), self.q_re.stride(0), _t_ptr(self.obs), self.n_obs,
+            _t_ptr(self.f_re), _t_ptr(self.f_im), self.n_obs, st), "hbem_field", self.lib)
+        if self.tags.shape[0]:
+            check(self.lib.hbem_reduce_tag_avg(
+                self.s.handle, self.F, _t_ptr(self.x_re), _t_ptr(self.x_im), self.n, _np_ptr(self.tags),
+                self.tags.shape[0], _t_ptr(self.tag_out), st), "hbem_reduce_tag_avg", self.lib)
+
+    def run(self, stream=None):
+        self.assemble(stream)
+        self.factor_solve(stream)
+        self.field(stream)

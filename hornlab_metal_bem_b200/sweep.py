@@ -1,0 +1,261 @@
+"""Frequency sweep driver of the B200 path.
+
+Mirrors ``hornlab_metal_bem/sweep.py`` of the reference: frequency grid
+(``sweep.py:63-66``), float32 wavenumbers with the optional complex-k shift
+(``:150-161``), per-frequency Neumann rows (``:238-285``), field points
+(``:288-312``), directivity (``:523-532``), rcond / mesh-resolution policies
+(``:383-440``) and ``SolveResult`` assembly (``:535-926``).  The solve itself
+is one ``NativeSession.assemble_solve_evaluate_standard_neumann_batch`` call
+per chunk of frequencies (all of them unless a streaming callback is set).
+"""
+from __future__ import annotations
+
+import logging
+import math
+import time
+from dataclasses import replace
+
+import numpy as np
+
+from ._constants import REFERENCE_PRESSURE, SPEED_OF_SOUND
+from .bie import build_driver_neumann, build_source_face_scale
+from .config import BIEFormulation, NATIVE_SYMMETRY_PLANES, SolveConfig
+from .geometry import build_geometry_buffers
+from .mesh import LoadedMesh, make_pure_function_spaces
+from .native import BackendUnavailable, NativeSession
+from .observation import ObservationFrame, build_observation_points
+from .result import SolveResult
+
+logger = logging.getLogger(__name__)
+
+
+def build_frequency_grid(config: SolveConfig) -> np.ndarray:
+    if config.freq_spacing == "log":
+        return np.geomspace(config.freq_min_hz, config.freq_max_hz, config.freq_count)
+    return np.linspace(config.freq_min_hz, config.freq_max_hz, config.freq_count)
+
+
+def should_route_native(config: SolveConfig) -> bool:
+    if config.native_symmetry_plane is not None and config.native_symmetry_plane not in NATIVE_SYMMETRY_PLANES:
+        raise BackendUnavailable(
+            "native_symmetry_plane must be None or one of " + ", ".join(repr(p) for p in NATIVE_SYMMETRY_PLANES)
+        )
+    if config.chief_points is not None:
+        raise BackendUnavailable("chief_points (CHIEF least squares) is not supported by the B200 path")
+    if config.aperture_tag is not None:
+        raise BackendUnavailable("aperture_tag (coupled infinite baffle) is not supported by the B200 path yet")
+    if config.impedance_sources or config.impedance_source_callback is not None:
+        raise BackendUnavailable("impedance_sources (Robin) are not routed by the B200 sweep yet")
+    return True
+
+
+def k_values(frequencies, config: SolveConfig) -> tuple[np.ndarray, np.ndarray]:
+    """``k = float32(2 pi f / c)``; complex-k adds ``i * shift * k`` (``sweep.py:150-161``)."""
+    k_re = (2.0 * np.pi * np.asarray(frequencies, dtype=np.float64) / SPEED_OF_SOUND).astype(np.float32)
+    if config.formulation == BIEFormulation.COMPLEX_K:
+        k_im = (k_re.astype(np.float64) * config.complex_k_shift).astype(np.float32)
+    else:
+        k_im = np.zeros_like(k_re)
+    return k_re, k_im
+
+
+def neumann_rows(n_faces: int, physical_tags, frequencies, config: SolveConfig, source_face_scale=None) -> np.ndarray:
+    tags_robin = set(config.impedance_sources.keys())
+    return np.stack([
+        build_driver_neumann(n_faces, physical_tags, 2.0 * np.pi * float(f), config, np.complex64,
+                             impedance_tags=tags_robin, source_face_scale=source_face_scale)
+        for f in frequencies
+    ])
+
+
+def field_points_3xn(obs_points: np.ndarray) -> np.ndarray:
+    p, n, _ = obs_points.shape
+    return np.ascontiguousarray(obs_points.reshape(p * n, 3).T, dtype=np.float32)
+
+
+def directivity_from_pressure(pressure: np.ndarray, on_axis_idx: int) -> np.ndarray:
+    """SPL re 20 uPa, floored at -120 dB SPL, minus the on-axis value per plane."""
+    floor = REFERENCE_PRESSURE * 10.0 ** (-120.0 / 20.0)
+    spl = 20.0 * np.log10(np.maximum(np.abs(pressure), floor) / REFERENCE_PRESSURE)
+    return spl - spl[:, on_axis_idx][:, None]
+
+
+def mesh_max_edge(mesh: LoadedMesh) -> float:
+    v = np.asarray(mesh.grid.vertices, dtype=np.float64).T
+    f = np.asarray(mesh.grid.elements).T
+    if f.size == 0:
+        return 0.0
+    e = [np.linalg.norm(v[f[:, (i + 1) % 3]] - v[f[:, i]], axis=1).max() for i in range(3)]
+    return float(max(e))
+
+
+def apply_dense_solve_policy(diag: dict, threshold: float) -> None:
+    diag["dense_solve_rcond_warning_threshold"] = float(threshold)
+    diag["dense_solve_suspect"] = False
+    if threshold <= 0.0:
+        return
+    rcond = diag.get("dense_solve_rcond")
+    if rcond is None:
+        diag["dense_solve_policy_available"] = False
+        return
+    diag["dense_solve_policy_available"] = True
+    if math.isfinite(float(rcond)) and float(rcond) < threshold:
+        diag["dense_solve_suspect"] = True
+        diag["dense_solve_recommendation"] = (
+            "Treat this frequency as suspect; nudge or densify the frequency grid around the resonance "
+            "and compare against nearby points. This flag detects dense-solve conditioning only."
+        )
+
+
+def apply_mesh_resolution_policy(diag: dict, frequency_hz: float, max_edge: float, epw_min: float) -> None:
+    diag["mesh_max_edge_m"] = float(max_edge)
+    diag["mesh_elements_per_wavelength_min"] = float(epw_min)
+    if max_edge <= 0.0:
+        diag["mesh_elements_per_wavelength"] = math.inf
+        diag["mesh_max_valid_frequency_hz"] = math.inf
+        diag["mesh_resolution_suspect"] = False
+        return
+    epw = (SPEED_OF_SOUND / float(frequency_hz)) / max_edge
+    diag["mesh_elements_per_wavelength"] = float(epw)
+    diag["mesh_max_valid_frequency_hz"] = float(SPEED_OF_SOUND / (epw_min * max_edge))
+    diag["mesh_resolution_suspect"] = bool(epw < epw_min)
+
+
+def run_sweep(mesh: LoadedMesh, frequencies, frame: ObservationFrame, config: SolveConfig,
+              *, session: NativeSession | None = None) -> SolveResult:
+    """Standard-Neumann sweep on the GPU (the reference's ``run_sweep_native_metal``)."""
+    should_route_native(config)
+    freqs = np.asarray(frequencies, dtype=np.float64)
+    if freqs.size == 0:
+        raise ValueError("frequencies must contain at least one value")
+    mesh_tags = {int(t) for t in np.unique(mesh.physical_tags)}
+    missing = sorted(set(config.velocity_sources) - mesh_tags)
+    if missing:
+        raise ValueError(
+            f"velocity_sources tags {missing} are not present in the mesh; available physical tags: {sorted(mesh_tags)}"
+        )
+    t_total = time.time()
+    obs_points, angles = build_observation_points(frame, config.observation)
+    p1, dp0 = make_pure_function_spaces(mesh.grid)
+    buffers = build_geometry_buffers(mesh.grid, mesh.physical_tags, p1, dp0)
+    max_edge = mesh_max_edge(mesh)
+    source_tags = list(config.velocity_sources.keys())
+    scale = build_source_face_scale(mesh.grid, mesh.physical_tags, config, frame.axis, frame.source_center)
+    on_axis = int(np.argmin(np.abs(angles)))
+    imp_tag = min(config.velocity_sources.keys(), default=2)
+    n_planes, n_angles, _ = obs_points.shape
+    pts = field_points_3xn(obs_points)
+    n_sphere = 0
+    if config.observation.sphere_points is not None:
+        sp = np.ascontiguousarray(np.asarray(config.observation.sphere_points, dtype=np.float64).T, dtype=np.float32)
+        n_sphere = sp.shape[1]
+        pts = np.concatenate([pts, sp], axis=1)
+    k_re, k_im = k_values(freqs, config)
+    q = neumann_rows(buffers.n_triangles, mesh.physical_tags, freqs, config, scale)
+
+    own = session is None
+    if own:
+        session = NativeSession(buffers, symmetry_plane=config.native_symmetry_plane,
+                                aperture_tag=config.aperture_tag, velocity_source_tags=source_tags,
+                                check_open_edges=config.native_check_open_edges)
+    pressure_rows, spl_rows, imp_rows, surf_rows, diag_rows, log = [], [], [], [], [], []
+    pavg: dict[int, list[complex]] = {t: [] for t in source_tags}
+    done: list[float] = []
+    try:
+        chunk = freqs.size if config.on_frequency_result is None else 1
+        stop = False
+        for f0 in range(0, freqs.size, chunk):
+            sl = slice(f0, f0 + chunk)
+            results = session.assemble_solve_evaluate_standard_neumann_batch(
+                freqs[sl], k_re[sl], q[sl], pts, k_imag_f32=k_im[sl], source_tags=source_tags,
+                impedance_source_tag=imp_tag, write_surface_pressure=config.return_surface_pressure,
+                dense_solve_dtype=config.dense_solve_dtype, precision=config.precision,
+                refine_tolerance=config.refine_tolerance, refine_max_iterations=config.refine_max_iterations,
+            )
+            for j, res in enumerate(results):
+                i = f0 + j
+                if res.lapack_info != 0:
+                    raise RuntimeError(f"dense LU failed at {res.frequency_hz:.3f} Hz: zero pivot {res.lapack_info}")
+                flat = res.field.astype(np.complex128)
+                arc = flat[: n_planes * n_angles].reshape(n_planes, n_angles)
+                sphere = flat[n_planes * n_angles:] if n_sphere else None
+                spl = directivity_from_pressure(arc, on_axis)
+                diag = dict(res.diagnostics)
+                apply_dense_solve_policy(diag, config.dense_solve_rcond_warning_threshold)
+                apply_mesh_resolution_policy(diag, res.frequency_hz, max_edge, config.mesh_elements_per_wavelength_min)
+                for t in source_tags:
+                    pavg[t].append(res.surface_pressure_avg[int(t)])
+                entry = {
+                    "frequency_hz": res.frequency_hz,
+                    "iterations": None,
+                    "timing_s": res.assembly_s + res.dense_solve_s + res.field_s,
+                    "backend": "hbem_b200_batch" if chunk > 1 else "hbem_b200_streamed",
+                    "assembly_s": res.assembly_s,
+                    "dense_solve_s": res.dense_solve_s,
+                    "field_s": res.field_s,
+                    "lapack_info": res.lapack_info,
+                    "impedance": res.impedance,
+                    "native_diagnostics": diag,
+                    "observation_sphere_pressure_complex": sphere,
+                }
+                done.append(res.frequency_hz)
+                pressure_rows.append(arc)
+                spl_rows.append(spl)
+                imp_rows.append(res.impedance)
+                if config.return_surface_pressure:
+                    surf_rows.append(res.surface_pressure.astype(np.complex128))
+                diag_rows.append(diag)
+                log.append(entry)
+                if config.progress_callback is not None:
+                    config.progress_callback(i, freqs.size, res.frequency_hz)
+                if config.on_frequency_result is not None:
+                    cb = {**entry, "observation_pressure_complex": arc, "observation_directivity_db": spl,
+                          "observation_angles_deg": angles, "observation_planes": config.observation.planes}
+                    if config.on_frequency_result(i, res.frequency_hz, cb) is False:
+                        logger.info("Early stop requested after %.1f Hz", res.frequency_hz)
+                        stop = True
+                        break
+            if stop:
+                break
+    finally:
+        if own:
+            session.close()
+    timings = {
+        "solve_s": sum(e["timing_s"] for e in log),
+        "assembly_s": sum(e["assembly_s"] for e in log),
+        "dense_solve_s": sum(e["dense_solve_s"] for e in log),
+        "directivity_s": sum(e["field_s"] for e in log),
+        "total_s": time.time() - t_total,
+    }
+    return SolveResult(
+        frequencies_hz=np.array(done, dtype=np.float64),
+        pressure_complex=np.stack(pressure_rows, axis=0),
+        directivity_db=np.stack(spl_rows, axis=0),
+        impedance=np.array(imp_rows, dtype=np.complex128),
+        observation_angles_deg=angles,
+        observation_points=obs_points,
+        observation_planes=config.observation.planes,
+        config=config,
+        mesh_info=mesh.info,
+        timings=timings,
+        solver_log=log,
+        surface_pressure_avg={t: np.array(v, dtype=np.complex128) for t, v in pavg.items()} or None,
+        surface_pressure_complex=np.stack(surf_rows, axis=0) if config.return_surface_pressure else None,
+        native_diagnostics=diag_rows,
+    )
+
+
+def run_sweep_multi_source(mesh: LoadedMesh, frequencies, frame: ObservationFrame, config: SolveConfig,
+                           sources: list[dict[int, complex]]) -> list[SolveResult]:
+    """One result per velocity-source dict (the reference's ``run_sweep_native_metal_multi_source``).
+
+    Each source is an independent sweep on one resident session; the
+    factorisation is recomputed per source.
+    """
+    p1, dp0 = make_pure_function_spaces(mesh.grid)
+    buffers = build_geometry_buffers(mesh.grid, mesh.physical_tags, p1, dp0)
+    all_tags = sorted({int(t) for s in sources for t in s})
+    with NativeSession(buffers, symmetry_plane=config.native_symmetry_plane, aperture_tag=config.aperture_tag,
+                       velocity_source_tags=all_tags, check_open_edges=config.native_check_open_edges) as session:
+        return [run_sweep(mesh, frequencies, frame, replace(config, velocity_sources=dict(src)), session=session)
+                for src in sources]

@@ -1,0 +1,207 @@
+/*
+ * hbem.h — C ABI of libhbem.so, the B200 (sm_100a) dense Helmholtz BEM hot path.
+ *
+ * Conventions
+ *   - Every entry point returns an int status: HBEM_OK (0) on success, a
+ *     negative HBEM_ERR_* code on failure (message via hbem_last_error), or a
+ *     positive value for a numerical condition (singular pivot).
+ *   - No C++ exception crosses this ABI; no torch type appears in it.
+ *   - Complex arrays are planar: separate real and imaginary float32 arrays
+ *     (the reference's IPC layout, docs/native-ipc.md "real_f32"/"imag_f32").
+ *   - Dense matrices are row-major with a leading dimension `lda` (>= n) and a
+ *     batch stride between consecutive matrices, all in elements.
+ *   - "device" pointers are caller-owned CUDA device memory on the session's
+ *     device; "host" pointers are ordinary host memory.  `stream` is a
+ *     cudaStream_t passed as void* (NULL = legacy default stream).
+ *   - A session is not thread-safe: use it from one host thread and one stream
+ *     at a time.  Distinct sessions are independent.
+ *
+ * The reference (m3gnus/hornlab-metal-bem) crosses this boundary as a
+ * subprocess with JSON manifests and planar float32 files
+ * (hornlab_metal_bem/metal/native.py:252-377, 737-1203;
+ *  hornlab_metal_bem/metal/session.py:21-389).  Each entry point below names
+ * the reference operation it replaces.
+ */
+#ifndef HBEM_H
+#define HBEM_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HBEM_OK 0
+#define HBEM_ERR_ARG (-1)      /* invalid argument / shape / index */
+#define HBEM_ERR_CUDA (-2)     /* CUDA runtime or launch failure */
+#define HBEM_ERR_NOMEM (-3)    /* device or host allocation failed */
+#define HBEM_ERR_STATE (-4)    /* session misuse or device-side status flag set */
+#define HBEM_SINGULAR 1        /* LU hit an exactly zero pivot (info > 0) */
+
+/* Assembly flags */
+#define HBEM_ASM_REGULAR 1     /* 6x6 Dunavant regular quadrature, all pairs */
+#define HBEM_ASM_DUFFY 2       /* Duffy singular corrections (coincident/edge/vertex pairs) */
+#define HBEM_ASM_ZERO 4        /* zero A and b before accumulating */
+#define HBEM_ASM_CORRECTED (HBEM_ASM_REGULAR | HBEM_ASM_DUFFY | HBEM_ASM_ZERO)
+
+/* LU precision */
+#define HBEM_PREC_PLAIN 0      /* FP32-accurate trailing updates (complex64 cgesv semantics) */
+#define HBEM_PREC_MIXED 1      /* BF16x3 tensor-core trailing updates; pair with hbem_refine */
+
+/* Solve transposition */
+#define HBEM_TRANS_N 0
+#define HBEM_TRANS_T 1
+#define HBEM_TRANS_C 2
+
+/* hbem_session_query keys */
+#define HBEM_Q_N_DOF 0
+#define HBEM_Q_N_TRIANGLES 1
+#define HBEM_Q_N_PAIRS 2
+#define HBEM_Q_PAIRS_COINCIDENT 3
+#define HBEM_Q_PAIRS_EDGE 4
+#define HBEM_Q_PAIRS_VERTEX 5
+#define HBEM_Q_IMAGE_PAIRS 6
+#define HBEM_Q_UNIQUE_TRIPLETS 7
+#define HBEM_Q_SYMMETRY 8
+#define HBEM_Q_KERNEL_LAUNCHES 9   /* cumulative launches of this library's kernels on the session */
+#define HBEM_Q_REGULAR_EVALS 10    /* kernel evaluations per frequency, regular part */
+#define HBEM_Q_DUFFY_EVALS 11      /* kernel evaluations per frequency, Duffy part */
+
+typedef struct hbem_session hbem_session;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int hbem_version(void);
+
+/* Copy the calling thread's last error message into buf (always NUL-terminated).
+   Returns the message length. */
+int hbem_last_error(char *buf, size_t len);
+
+/* Number of kernel launches this library issued in the calling process. */
+long long hbem_launch_count(void);
+
+/*
+ * Create a session on `device` from host geometry buffers.
+ * Replaces: MetalNativeStandardSession.create_session
+ *   (hornlab_metal_bem/metal/native.py:252-377) and the helper's
+ *   ResidentMetalContext set-up (main.swift:5370-5507: P1 incidence, Duffy
+ *   pair list, reduction plan, rules, geometry upload).
+ * Inputs (host): vertices (3, n_vertices) f32; triangles (3, n_triangles) i32;
+ *   p1_local2global (n_triangles, 3) i32 with values < n_dof; tags (n_triangles,);
+ *   areas (n_triangles,) f32; normals (3, n_triangles) f32;
+ *   sym_code 0 none, 1 yz, 2 xz, 3 yz+xz, 4 xy (main.swift:703-717).
+ */
+int hbem_session_create(const float *vertices_3xv, int n_vertices,
+                        const int *triangles_3xt, int n_triangles,
+                        const int *p1_local2global_tx3, int n_dof,
+                        const int *tags, const float *areas, const float *normals_3xt,
+                        int sym_code, int device, hbem_session **out);
+
+/* Release a session and its device memory. */
+int hbem_session_destroy(hbem_session *s);
+
+/* Read one HBEM_Q_* property. */
+int hbem_session_query(const hbem_session *s, int key, long long *value);
+
+/*
+ * Assemble A (P1 x P1 Galerkin, DLP - 1/2 mass, image method, Robin) and the
+ * right-hand side b = SLP q for `n_freq` wavenumbers in one launch set.
+ * Replaces: assemble_standard_neumann[_batch] ops
+ *   (main.swift:3993-4133 pair kernel, 3698-3736 RHS kernel, 4246-4431 Duffy
+ *   kernel, 6498-6561 CPU delta reduction).
+ * k_re/k_im: host (n_freq,).  q_re/q_im: device (n_freq, n_triangles), row
+ * stride q_stride.  beta_re/beta_im: device (n_triangles,) Robin admittance or
+ * NULL.  A: device, frequency f at A + f*a_stride, row-major with lda.
+ * b: device, frequency f at b + f*b_stride.
+ */
+int hbem_assemble(hbem_session *s, int n_freq, const float *k_re, const float *k_im,
+                  const float *q_re, const float *q_im, long long q_stride,
+                  const float *beta_re, const float *beta_im,
+                  float *a_re, float *a_im, long long lda, long long a_stride,
+                  float *b_re, float *b_im, long long b_stride,
+                  int flags, void *stream);
+
+/*
+ * Batched in-place complex LU with partial pivoting (LAPACK getrf semantics:
+ * unit-lower L and U overwrite A; piv[i] = 0-based row swapped with row i).
+ * Replaces: cgesv_/cgetrf_ in solveDenseAccelerateCgesvMulti
+ *   (main.swift:7834-7941, 8015-8020).
+ * info: device int per matrix; 0 or the 1-based index of the first zero pivot.
+ * Returns HBEM_OK even when a pivot is zero (read info).
+ */
+int hbem_lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long long a_stride,
+                   int *piv, long long piv_stride, int *info, int precision, void *stream);
+
+/*
+ * Solve op(A) X = B with the factors of hbem_lu_factor; B (n, nrhs) row-major
+ * with leading dimension ldb, overwritten by X.  trans = HBEM_TRANS_N/T/C.
+ * Replaces: cgetrs_ / the back-substitution inside cgesv_.
+ */
+int hbem_lu_solve(int n, int nrhs, int batch, const float *lu_re, const float *lu_im, long long lda,
+                  long long a_stride, const int *piv, long long piv_stride,
+                  float *b_re, float *b_im, long long ldb, long long b_stride, int trans, void *stream);
+
+/*
+ * FP64-residual iterative refinement of X for A X = B (nrhs = 1 per matrix):
+ * r = b - A x in FP64 from the ORIGINAL matrix, d = LU \ r, x += d, until
+ * ||r|| / ||b|| <= tol or max_iter passes.  iters/resid: device per matrix.
+ * Replaces: refineDenseSolveSolution (main.swift:6964-7070).
+ */
+int hbem_refine(int n, int batch, const float *a_re, const float *a_im, long long lda, long long a_stride,
+                const float *lu_re, const float *lu_im, long long lu_stride,
+                const int *piv, long long piv_stride,
+                const float *b_re, const float *b_im, long long b_stride,
+                float *x_re, float *x_im, long long x_stride,
+                double tol, int max_iter, int *iters, double *resid, void *stream);
+
+/*
+ * Exterior field p(x_o) = sum_tri sum_q w [dG/dn_y p(y_q) - G q_tri] (+ images)
+ * for n_freq cases at once.  Replaces: evaluate_field_regular / evaluateExterior
+ *   (main.swift:4135-4203, 8312-8424; Python forces the GPU field,
+ *   hornlab_metal_bem/sweep.py:114-115).
+ * p: device (n_freq, n_dof) with stride p_stride; q: device (n_freq, n_triangles).
+ * obs: device (3, n_obs).  out: device (n_freq, n_obs) with stride out_stride.
+ */
+int hbem_field(hbem_session *s, int n_freq, const float *k_re,
+               const float *p_re, const float *p_im, long long p_stride,
+               const float *q_re, const float *q_im, long long q_stride,
+               const float *obs_3xn, int n_obs,
+               float *out_re, float *out_im, long long out_stride, void *stream);
+
+/*
+ * Area-weighted average of the P1 surface pressure over the faces of each tag,
+ * FP64 sums.  out: device (n_freq, n_tags, 2) double (re, im).
+ * Replaces: averageSurfacePressureForTag / nativePressureReductionPayload
+ *   (main.swift:807-871).
+ */
+int hbem_reduce_tag_avg(hbem_session *s, int n_freq, const float *p_re, const float *p_im, long long p_stride,
+                        const int *tags_host, int n_tags, double *out, void *stream);
+
+/*
+ * One-call batched sweep over host buffers: host->device copies, assembly,
+ * LU, solve, optional refinement, field and tag reductions, device->host
+ * copies.  Replaces: MetalNativeStandardSession.
+ *   assemble_solve_evaluate_standard_neumann_batch
+ *   (hornlab_metal_bem/metal/native.py:737-1203; helper op
+ *    main.swift:8869-9878).
+ * Host inputs: k_re, k_im (n_freq,); q_re, q_im (n_freq, n_triangles);
+ *   obs (3, n_obs); tags (n_tags,).
+ * Host outputs: field (n_freq, n_obs) planar; tag_avg (n_freq, n_tags, 2)
+ *   double; surface (n_freq, n_dof) planar or NULL; info (n_freq,);
+ *   refine_iters (n_freq,) or NULL; refine_resid (n_freq,) or NULL;
+ *   timings_ms (4,) = assembly, solve, field, total (device event times) or NULL.
+ */
+int hbem_solve_batch(hbem_session *s, int n_freq, const float *k_re, const float *k_im,
+                     const float *q_re, const float *q_im,
+                     const float *obs_3xn, int n_obs,
+                     const int *tags, int n_tags,
+                     int precision, double refine_tol, int refine_max_iter,
+                     float *field_re, float *field_im, double *tag_avg,
+                     float *surface_re, float *surface_im,
+                     int *info, int *refine_iters, double *refine_resid,
+                     float *timings_ms, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HBEM_H */

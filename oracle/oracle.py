@@ -1,0 +1,193 @@
+"""TEST INFRASTRUCTURE — Python face of the CPU oracle (``hbem_oracle.c``).
+
+Only tests/, ``__graft_entry__.smoke()`` and ``bench.py`` (its cpu_baseline and
+``--impl reference`` arms) import this module, as the checker or as the timed
+CPU baseline.  The product path never does.
+
+It wraps the C restatement of the reference's CPU path (see the header of
+``hbem_oracle.c`` for the file:line map) and adds the dense solve the
+reference delegates to Apple Accelerate ``cgesv`` (``main.swift:7834-7941``);
+the stand-in here is LAPACK ``cgesv``/``zgesv`` from SciPy (OpenBLAS).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+BUILD = HERE / "_build"
+
+
+class _Geom(ctypes.Structure):
+    _fields_ = [
+        ("n_vertices", ctypes.c_int),
+        ("n_triangles", ctypes.c_int),
+        ("n_dof", ctypes.c_int),
+        ("sym", ctypes.c_int),
+        ("verts", ctypes.c_void_p),
+        ("tris", ctypes.c_void_p),
+        ("l2g", ctypes.c_void_p),
+        ("areas", ctypes.c_void_p),
+        ("normals", ctypes.c_void_p),
+    ]
+
+
+def build() -> None:
+    """Compile the oracle libraries (gcc + OpenMP) into ``oracle/_build``."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+def _lib(precision: str):
+    name = {"f32": "libhbem_oracle_f32.so", "f64": "libhbem_oracle_f64.so"}[precision]
+    path = BUILD / name
+    if not path.exists():
+        build()
+    return ctypes.CDLL(str(path))
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Oracle:
+    """CPU oracle bound to one geometry (``GeometryBuffers``-like object)."""
+
+    def __init__(self, buffers, symmetry_code: int = 0, precision: str = "f64", threads: int | None = None):
+        self.precision = precision
+        self.lib = _lib(precision)
+        self.pre = "og32_" if precision == "f32" else "og64_"
+        self.real = np.float32 if precision == "f32" else np.float64
+        self._ct = ctypes.c_float if precision == "f32" else ctypes.c_double
+        self._keep = [
+            np.ascontiguousarray(buffers.vertices_3xn_f32, dtype=np.float32),
+            np.ascontiguousarray(buffers.triangles_3xm_i32, dtype=np.int32),
+            np.ascontiguousarray(buffers.p1_local2global_i32, dtype=np.int32),
+            np.ascontiguousarray(buffers.triangle_areas_f32, dtype=np.float32),
+            np.ascontiguousarray(buffers.triangle_normals_3xm_f32, dtype=np.float32),
+        ]
+        self.tags = np.ascontiguousarray(buffers.physical_tags_i32, dtype=np.int32)
+        self.n = int(buffers.p1_dof_count)
+        self.T = int(buffers.triangles_3xm_i32.shape[1])
+        self.geom = _Geom(
+            int(buffers.vertices_3xn_f32.shape[1]), self.T, self.n, int(symmetry_code),
+            *[_ptr(a) for a in self._keep],
+        )
+        self.set_threads(threads if threads is not None else len(os.sched_getaffinity(0)))
+
+    def _fn(self, name):
+        return getattr(self.lib, self.pre + name)
+
+    def set_threads(self, n: int) -> int:
+        return int(self._fn("set_threads")(ctypes.c_int(int(n))))
+
+    # -- assembly -----------------------------------------------------------
+    def _split(self, z, n):
+        if z is None:
+            return None, None
+        z = np.asarray(z, dtype=np.complex128).reshape(n)
+        return (np.ascontiguousarray(z.real, dtype=np.float32), np.ascontiguousarray(z.imag, dtype=np.float32))
+
+    def regular(self, k: float, q=None, k_imag: float = 0.0, beta=None):
+        n = self.n
+        Are = np.zeros((n, n), self.real); Aim = np.zeros((n, n), self.real)
+        bre = np.zeros(n, self.real); bim = np.zeros(n, self.real)
+        qre, qim = self._split(q, self.T)
+        brr, bri = self._split(beta, self.T)
+        self._fn("regular_assemble")(
+            ctypes.byref(self.geom), self._ct(k), self._ct(k_imag), _ptr(qre), _ptr(qim), _ptr(brr), _ptr(bri),
+            _ptr(Are), _ptr(Aim), _ptr(bre), _ptr(bim),
+        )
+        return Are + 1j * Aim, bre + 1j * bim
+
+    def duffy_correct(self, A, b, k: float, q=None, k_imag: float = 0.0, beta=None) -> int:
+        """Add the Duffy singular corrections to ``A``/``b`` in place; returns unique triplets."""
+        Are = np.ascontiguousarray(A.real, dtype=self.real); Aim = np.ascontiguousarray(A.imag, dtype=self.real)
+        bre = np.ascontiguousarray(b.real, dtype=self.real); bim = np.ascontiguousarray(b.imag, dtype=self.real)
+        qre, qim = self._split(q, self.T)
+        brr, bri = self._split(beta, self.T)
+        u = self._fn("duffy_correct")(
+            ctypes.byref(self.geom), self._ct(k), self._ct(k_imag), _ptr(qre), _ptr(qim), _ptr(brr), _ptr(bri),
+            _ptr(Are), _ptr(Aim), _ptr(bre), _ptr(bim),
+        )
+        A[...] = Are + 1j * Aim
+        b[...] = bre + 1j * bim
+        return int(u)
+
+    def corrected(self, k: float, q=None, k_imag: float = 0.0, beta=None):
+        """Regular 6x6 assembly plus Duffy corrections: the reference's 'corrected' mode."""
+        A, b = self.regular(k, q, k_imag, beta)
+        self.duffy_correct(A, b, k, q, k_imag, beta)
+        return A, b
+
+    def duffy_pairs(self):
+        counts = (ctypes.c_int * 3)()
+        np_ = self._fn("duffy_pairs")(ctypes.byref(self.geom), None, 0, counts)
+        pairs = np.zeros((max(np_, 1), 9), dtype=np.int32)
+        self._fn("duffy_pairs")(ctypes.byref(self.geom), _ptr(pairs), ctypes.c_int(np_), counts)
+        return pairs[:np_], {"coincident": counts[0], "edge": counts[1], "vertex": counts[2]}
+
+    def unique_triplets(self, pairs) -> int:
+        pairs = np.ascontiguousarray(pairs, dtype=np.int32)
+        return int(self._fn("duffy_unique_triplets")(ctypes.byref(self.geom), _ptr(pairs), ctypes.c_int(pairs.shape[0])))
+
+    def pair_blocks(self, test, trial, test_mask=0, trial_mask=0, mode=0, kind=0, locals_=None, level=0, k=1.0, k_imag=0.0):
+        out = np.zeros(24, self.real)
+        loc = None if locals_ is None else np.ascontiguousarray(locals_, dtype=np.int32)
+        self._fn("pair_blocks")(
+            ctypes.byref(self.geom), test, trial, test_mask, trial_mask, mode, kind, _ptr(loc), level,
+            self._ct(k), self._ct(k_imag), _ptr(out),
+        )
+        slp = out[0:6:2] + 1j * out[1:6:2]
+        dlp = (out[6::2] + 1j * out[7::2]).reshape(3, 3)
+        return slp, dlp
+
+    def rule(self, kind: int):
+        rec = np.zeros((1536, 5), self.real)
+        n = self._fn("duffy_rule_table")(ctypes.c_int(kind), _ptr(rec))
+        return rec[:n]
+
+    # -- field / reductions -------------------------------------------------
+    def field(self, k: float, p, q, obs_3xn):
+        obs = np.ascontiguousarray(obs_3xn, dtype=np.float32)
+        nobs = obs.shape[1]
+        p = np.asarray(p).reshape(self.n); q = np.asarray(q).reshape(self.T)
+        pre = np.ascontiguousarray(p.real, self.real); pim = np.ascontiguousarray(p.imag, self.real)
+        qre = np.ascontiguousarray(q.real, self.real); qim = np.ascontiguousarray(q.imag, self.real)
+        ore = np.zeros(nobs, self.real); oim = np.zeros(nobs, self.real)
+        self._fn("field")(
+            ctypes.byref(self.geom), self._ct(k), _ptr(pre), _ptr(pim), _ptr(qre), _ptr(qim), _ptr(obs),
+            ctypes.c_int(nobs), _ptr(ore), _ptr(oim),
+        )
+        return ore + 1j * oim
+
+    def tag_average(self, p, tag: int) -> complex:
+        p = np.asarray(p).reshape(self.n)
+        pre = np.ascontiguousarray(p.real, self.real); pim = np.ascontiguousarray(p.imag, self.real)
+        out = np.zeros(3, np.float64)
+        self._fn("tag_average")(ctypes.byref(self.geom), _ptr(self.tags), _ptr(pre), _ptr(pim), ctypes.c_int(int(tag)), _ptr(out))
+        return complex(out[0], out[1])
+
+
+def dense_solve(A, b, precision: str = "f32"):
+    """LAPACK ``cgesv`` (complex64) or ``zgesv`` (complex128): the Accelerate stand-in."""
+    from scipy.linalg import lapack
+
+    if precision == "f32":
+        lu, piv, x, info = lapack.cgesv(np.asarray(A, np.complex64), np.asarray(b, np.complex64))
+    else:
+        lu, piv, x, info = lapack.zgesv(np.asarray(A, np.complex128), np.asarray(b, np.complex128))
+    if info != 0:
+        raise RuntimeError(f"LAPACK gesv info={info}")
+    return x
+
+
+def solve_case(oracle: Oracle, k: float, q, obs_3xn, precision: str = "f32"):
+    """One frequency of the reference's corrected path: assemble, solve, field."""
+    A, b = oracle.corrected(k, q)
+    p = dense_solve(A, b, precision)
+    field = oracle.field(k, p, q, obs_3xn)
+    return A, b, p, field

@@ -1,0 +1,250 @@
+"""GPU parity: every CUDA stage through the C ABI against the CPU oracle.
+
+Tolerances: assembled matrix and RHS within 1e-4
+relative L2 of the reference method (here the FP64 oracle, which is pinned to
+the reference's known answers in test_oracle_pins.py); LU solutions within
+1e-5 of LAPACK; field within 1e-4 relative; directivity within 0.01 dB.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden_buffers
+
+from oracle.oracle import Oracle, dense_solve
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover - CPU containers
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+from hornlab_metal_bem_b200 import generators as G  # noqa: E402
+from hornlab_metal_bem_b200.geometry import build_geometry_buffers  # noqa: E402
+from hornlab_metal_bem_b200.mesh import make_pure_function_spaces  # noqa: E402
+from hornlab_metal_bem_b200.native import (  # noqa: E402
+    HBEM_ASM_CORRECTED, HBEM_ASM_REGULAR, HBEM_ASM_ZERO, NativeSession, load_library,
+)
+
+SYM = {"tiny": 0, "near": 0, "ico2": 0, "horn_quarter": 3, "yzxz_quarter": 3, "yzxz_full": 0, "yz_half": 1,
+       "xy_half": 4, "ib_box": 0, "yz_full": 0}
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))
+
+
+def _session(name):
+    return NativeSession(golden_buffers(name), symmetry_plane={0: None, 1: "yz", 3: "yz+xz", 4: "xy"}[SYM[name]],
+                         check_open_edges=False)
+
+
+def _q(T, seed=0):
+    rng = np.random.default_rng(seed)
+    return (rng.normal(size=T) + 1j * rng.normal(size=T)).astype(np.complex64)
+
+
+def _host(t_re, t_im):
+    return t_re.cpu().numpy().astype(np.float64) + 1j * t_im.cpu().numpy().astype(np.float64)
+
+
+@pytest.mark.parametrize("name", ["tiny", "near", "ico2", "horn_quarter", "yzxz_quarter", "yz_half", "xy_half"])
+@pytest.mark.parametrize("k", [1.8318326, 18.3, 91.6])
+def test_corrected_assembly_matches_oracle(name, k):
+    b = golden_buffers(name)
+    o = Oracle(b, SYM[name], "f64")
+    q = _q(b.n_triangles)
+    A_ref, b_ref = o.corrected(k, q)
+    with _session(name) as s:
+        Ar, Ai, br, bi = s.assemble([k], q[None, :])
+        A, rhs = _host(Ar, Ai)[0], _host(br, bi)[0]
+    assert rel(A, A_ref) < 1e-4
+    assert rel(rhs, b_ref) < 1e-4
+
+
+@pytest.mark.parametrize("name", ["ico2", "horn_quarter"])
+def test_regular_only_assembly_matches_oracle(name):
+    b = golden_buffers(name)
+    o = Oracle(b, SYM[name], "f64")
+    q = _q(b.n_triangles, 3)
+    A_ref, b_ref = o.regular(40.0, q)
+    with _session(name) as s:
+        Ar, Ai, br, bi = s.assemble([40.0], q[None, :], flags=HBEM_ASM_REGULAR | HBEM_ASM_ZERO)
+    assert rel(_host(Ar, Ai)[0], A_ref) < 1e-4
+    assert rel(_host(br, bi)[0], b_ref) < 1e-4
+
+
+def test_complex_k_and_robin_assembly_match_oracle():
+    b = golden_buffers("ico2")
+    o = Oracle(b, 0, "f64")
+    q = _q(b.n_triangles, 5)
+    rng = np.random.default_rng(9)
+    beta = np.where(rng.random(b.n_triangles) < 0.3, 0.4 + 0.2j, 0.0).astype(np.complex64)
+    A_ref, b_ref = o.corrected(25.0, q, k_imag=0.125, beta=beta)
+    with _session("ico2") as s:
+        Ar, Ai, br, bi = s.assemble([25.0], q[None, :], k_imag=[0.125], beta=beta)
+    assert rel(_host(Ar, Ai)[0], A_ref) < 1e-4
+    assert rel(_host(br, bi)[0], b_ref) < 1e-4
+
+
+def test_multi_frequency_batch_equals_single_frequency():
+    b = golden_buffers("horn_quarter")
+    ks = [3.0, 20.0, 75.0]
+    q = np.stack([_q(b.n_triangles, i) for i in range(3)])
+    with _session("horn_quarter") as s:
+        Ar, Ai, br, bi = s.assemble(ks, q)
+        for f, k in enumerate(ks):
+            Ar1, Ai1, br1, bi1 = s.assemble([k], q[f][None, :])
+            assert rel(_host(Ar, Ai)[f], _host(Ar1, Ai1)[0]) < 1e-6
+            assert rel(_host(br, bi)[f], _host(br1, bi1)[0]) < 1e-6
+
+
+@pytest.mark.parametrize("name", ["tiny", "ico2", "horn_quarter", "yzxz_quarter"])
+def test_pair_plan_matches_oracle(name):
+    b = golden_buffers(name)
+    o = Oracle(b, SYM[name], "f64")
+    pairs, counts = o.duffy_pairs()
+    with _session(name) as s:
+        plan = s.pair_plan()
+        assert {k: plan[k] for k in counts} == counts
+        assert s.query("unique_triplets") == o.unique_triplets(pairs)
+        assert s.query("image_pairs") == int(np.sum((pairs[:, 2] != 0) | (pairs[:, 3] != 0)))
+
+
+def test_quarter_equals_orbit_reduced_full_on_gpu():
+    with _session("yzxz_full") as sf, _session("yzxz_quarter") as sq:
+        Af = _host(*sf.assemble([1.8318326], np.ones((1, 4), np.complex64))[:2])[0]
+        bf = _host(*sf.assemble([1.8318326], np.ones((1, 4), np.complex64))[2:])[0]
+        Aq_r, Aq_i, bq_r, bq_i = sq.assemble([1.8318326], np.ones((1, 1), np.complex64))
+    orbits = [np.array([0]), np.array([1, 3]), np.array([2, 4])]
+    R = np.array([[Af[np.ix_(r, c)].sum() for c in orbits] for r in orbits])
+    rb = np.array([bf[r].sum() for r in orbits])
+    assert rel(_host(Aq_r, Aq_i)[0], R) < 1e-6
+    assert rel(_host(bq_r, bq_i)[0], rb) < 1e-6
+
+
+# ---------------------------------------------------------------------------- LU
+def _lu_case(n, batch, seed):
+    rng = np.random.default_rng(seed)
+    A = rng.normal(size=(batch, n, n)) + 1j * rng.normal(size=(batch, n, n))
+    A += np.eye(n)[None] * (2.0 * np.sqrt(n))
+    b = rng.normal(size=(batch, n)) + 1j * rng.normal(size=(batch, n))
+    return A.astype(np.complex64), b.astype(np.complex64)
+
+
+def _dev(z):
+    return (torch.from_numpy(np.ascontiguousarray(z.real, np.float32)).cuda(),
+            torch.from_numpy(np.ascontiguousarray(z.imag, np.float32)).cuda())
+
+
+def _factor(Ar, Ai, n, batch, precision=0):
+    import ctypes
+
+    lib = load_library()
+    piv = torch.zeros((batch, n), dtype=torch.int32, device="cuda")
+    info = torch.zeros(batch, dtype=torch.int32, device="cuda")
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rc = lib.hbem_lu_factor(n, batch, ctypes.c_void_p(Ar.data_ptr()), ctypes.c_void_p(Ai.data_ptr()), n, n * n,
+                            ctypes.c_void_p(piv.data_ptr()), n, ctypes.c_void_p(info.data_ptr()), precision, st)
+    assert rc == 0
+    return piv, info
+
+
+def _solve(Ar, Ai, piv, Br, Bi, n, nrhs, batch, trans=0):
+    import ctypes
+
+    lib = load_library()
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rc = lib.hbem_lu_solve(n, nrhs, batch, ctypes.c_void_p(Ar.data_ptr()), ctypes.c_void_p(Ai.data_ptr()), n, n * n,
+                           ctypes.c_void_p(piv.data_ptr()), n, ctypes.c_void_p(Br.data_ptr()),
+                           ctypes.c_void_p(Bi.data_ptr()), nrhs, n * nrhs, trans, st)
+    assert rc == 0
+
+
+@pytest.mark.parametrize("n", [1, 2, 5, 31, 33, 100, 257, 700, 1059])
+def test_lu_solve_matches_lapack(n):
+    batch = 3
+    A, b = _lu_case(n, batch, n)
+    Ar, Ai = _dev(A)
+    piv, info = _factor(Ar, Ai, n, batch)
+    assert int(info.abs().sum()) == 0
+    Br, Bi = _dev(b[:, :, None])
+    _solve(Ar, Ai, piv, Br, Bi, n, 1, batch)
+    x = _host(Br, Bi)[:, :, 0]
+    for m in range(batch):
+        ref = np.linalg.solve(A[m].astype(np.complex128), b[m].astype(np.complex128))
+        assert rel(x[m], ref) < 1e-5
+
+
+@pytest.mark.parametrize("trans", [1, 2])
+def test_transposed_solves(trans):
+    n, batch, nrhs = 130, 2, 3
+    A, _ = _lu_case(n, batch, 11)
+    rng = np.random.default_rng(2)
+    B = (rng.normal(size=(batch, n, nrhs)) + 1j * rng.normal(size=(batch, n, nrhs))).astype(np.complex64)
+    Ar, Ai = _dev(A)
+    piv, info = _factor(Ar, Ai, n, batch)
+    Br, Bi = _dev(B)
+    _solve(Ar, Ai, piv, Br, Bi, n, nrhs, batch, trans)
+    X = _host(Br, Bi)
+    for m in range(batch):
+        op = A[m].T if trans == 1 else A[m].conj().T
+        ref = np.linalg.solve(op.astype(np.complex128), B[m].astype(np.complex128))
+        assert rel(X[m], ref) < 1e-5
+
+
+def test_singular_pivot_reports_info():
+    n = 8
+    A = np.eye(n, dtype=np.complex64)
+    A[3, 3] = 0.0
+    A[3, :] = 0.0
+    Ar, Ai = _dev(A[None])
+    piv, info = _factor(Ar, Ai, n, 1)
+    assert int(info[0]) == 4
+
+
+def test_bem_matrix_solve_matches_lapack():
+    b = golden_buffers("horn_quarter")
+    q = _q(b.n_triangles, 1)
+    with _session("horn_quarter") as s:
+        Ar, Ai, br, bi = s.assemble([30.0], q[None, :])
+        A = _host(Ar, Ai)[0]
+        rhs = _host(br, bi)[0]
+        n = s.n_dof
+        piv, info = _factor(Ar, Ai, n, 1)
+        Br, Bi = br[:, :, None].contiguous(), bi[:, :, None].contiguous()
+        _solve(Ar, Ai, piv, Br, Bi, n, 1, 1)
+    x = _host(Br, Bi)[0, :, 0]
+    ref = dense_solve(A, rhs, "f64")
+    assert rel(x, ref) < 1e-5
+
+
+# ------------------------------------------------------------------ field / tags
+@pytest.mark.parametrize("name", ["ico2", "horn_quarter", "yz_half", "xy_half"])
+def test_field_matches_oracle(name):
+    b = golden_buffers(name)
+    o = Oracle(b, SYM[name], "f64")
+    rng = np.random.default_rng(4)
+    p = (rng.normal(size=b.p1_dof_count) + 1j * rng.normal(size=b.p1_dof_count)).astype(np.complex64)
+    q = _q(b.n_triangles, 6)
+    obs = rng.normal(size=(3, 29)) * 1.5 + np.array([[0.3], [0.2], [1.0]])
+    ref = o.field(33.0, p, q, obs)
+    with _session(name) as s:
+        pr, pi = _dev(p[None])
+        fr, fi = s.field([33.0], pr, pi, q[None], obs)
+    assert rel(_host(fr, fi)[0], ref) < 1e-4
+
+
+def test_tag_average_matches_oracle():
+    b = golden_buffers("horn_quarter")
+    o = Oracle(b, 3, "f64")
+    rng = np.random.default_rng(8)
+    p = (rng.normal(size=(2, b.p1_dof_count)) + 1j * rng.normal(size=(2, b.p1_dof_count))).astype(np.complex64)
+    with _session("horn_quarter") as s:
+        pr, pi = _dev(p)
+        out = s.tag_average(pr, pi, [1, 2, 99]).cpu().numpy()
+    for f in range(2):
+        for j, tag in enumerate([1, 2, 99]):
+            want = o.tag_average(p[f], tag)
+            assert abs(complex(out[f, j, 0], out[f, j, 1]) - want) <= 1e-12 + 1e-9 * abs(want)

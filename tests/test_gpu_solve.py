@@ -1,0 +1,118 @@
+"""End-to-end ``solve()`` on the GPU against the oracle's corrected path and the
+analytic pulsating sphere (surface pressure within 1e-4
+relative, directivity within 0.01 dB)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle, dense_solve
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import hornlab_metal_bem_b200 as hb  # noqa: E402
+from hornlab_metal_bem_b200 import generators as G  # noqa: E402
+from hornlab_metal_bem_b200.geometry import build_geometry_buffers  # noqa: E402
+from hornlab_metal_bem_b200.mesh import make_pure_function_spaces  # noqa: E402
+from hornlab_metal_bem_b200.sweep import directivity_from_pressure, field_points_3xn  # noqa: E402
+
+
+def _oracle_sweep(mesh, res, config, sym=0):
+    p1, dp0 = make_pure_function_spaces(mesh.grid)
+    buf = build_geometry_buffers(mesh.grid, mesh.physical_tags, p1, dp0)
+    o = Oracle(buf, sym, "f64")
+    from hornlab_metal_bem_b200.sweep import k_values, neumann_rows
+    from hornlab_metal_bem_b200.bie import build_source_face_scale
+    from hornlab_metal_bem_b200.observation import infer_frame
+
+    frame = infer_frame(mesh.grid, mesh.physical_tags, source_tag=min(config.velocity_sources), symmetry_plane=config.native_symmetry_plane)
+    scale = build_source_face_scale(mesh.grid, mesh.physical_tags, config, frame.axis, frame.source_center)
+    k_re, _ = k_values(res.frequencies_hz, config)
+    q = neumann_rows(buf.n_triangles, mesh.physical_tags, res.frequencies_hz, config, scale)
+    pts = field_points_3xn(res.observation_points)
+    out_p, out_f = [], []
+    for f in range(len(res.frequencies_hz)):
+        A, b = o.corrected(float(k_re[f]), q[f])
+        p = dense_solve(A, b, "f64")
+        out_p.append(p)
+        out_f.append(o.field(float(k_re[f]), p, q[f], pts))
+    return np.array(out_p), np.array(out_f)
+
+
+def test_pulsating_sphere_solve_matches_oracle_and_analytic():
+    mesh = G.icosphere(3, 0.1)
+    cfg = hb.native_config(
+        freq_min_hz=200.0, freq_max_hz=5000.0, freq_count=8, velocity_mode="velocity", air_density=1.205,
+        observation=hb.ObservationConfig(planes=["horizontal"], angle_count=37, distance_m=2.0),
+        return_surface_pressure=True,
+    )
+    res = hb.solve(mesh, cfg)
+    assert res.pressure_complex.shape == (8, 1, 37)
+    p_ref, f_ref = _oracle_sweep(mesh, res, cfg)
+    for f in range(8):
+        sp = res.surface_pressure_complex[f]
+        assert np.linalg.norm(sp - p_ref[f]) / np.linalg.norm(p_ref[f]) < 1e-4
+        fld = res.pressure_complex[f].reshape(-1)
+        assert np.linalg.norm(fld - f_ref[f]) / np.linalg.norm(f_ref[f]) < 1e-4
+        d_ref = directivity_from_pressure(f_ref[f].reshape(1, -1), int(np.argmin(np.abs(res.observation_angles_deg))))
+        assert np.max(np.abs(res.directivity_db[f] - d_ref)) < 0.01
+    # analytic pulsating sphere: Z/(rho c) = ika / (ika - 1) on the surface
+    rho, c, a = 1.205, 343.0, 0.1
+    k = (2 * np.pi * res.frequencies_hz / c).astype(np.float32).astype(np.float64)
+    za = rho * c * (1j * k * a) / (1j * k * a - 1)
+    rel = np.abs(res.impedance - za) / np.abs(za)
+    assert np.all(rel < 5e-3), rel
+    assert np.all(np.isfinite(res.directivity_db))
+
+
+def test_quarter_horn_solve_matches_oracle():
+    mesh = G.horn(G.HornSpec(edge=0.014), quarter=True)
+    cfg = hb.native_config(
+        freq_min_hz=500.0, freq_max_hz=8000.0, freq_count=3, source_motion="axial",
+        native_symmetry_plane="yz+xz", native_check_open_edges=False,
+        observation=hb.ObservationConfig(planes=["horizontal", "vertical", "diagonal"], angle_count=13),
+        return_surface_pressure=True,
+    )
+    res = hb.solve(mesh, cfg)
+    p_ref, f_ref = _oracle_sweep(mesh, res, cfg, sym=3)
+    for f in range(3):
+        assert np.linalg.norm(res.surface_pressure_complex[f] - p_ref[f]) / np.linalg.norm(p_ref[f]) < 1e-4
+        fld = res.pressure_complex[f].reshape(-1)
+        assert np.linalg.norm(fld - f_ref[f]) / np.linalg.norm(f_ref[f]) < 1e-4
+        d_ref = directivity_from_pressure(f_ref[f].reshape(3, 13), 0)
+        assert np.max(np.abs(res.directivity_db[f] - d_ref)) < 0.01
+    assert set(res.surface_pressure_avg) == {2}
+    assert res.native_diagnostics[0]["mesh_max_edge_m"] > 0
+
+
+def test_streaming_callback_early_stop_and_progress():
+    mesh = G.icosphere(2, 0.1)
+    seen, progress = [], []
+
+    def on_result(i, f, entry):
+        seen.append((i, f, entry["observation_directivity_db"].shape))
+        return False if i == 1 else None
+
+    cfg = hb.native_config(freq_min_hz=300.0, freq_max_hz=3000.0, freq_count=5, on_frequency_result=on_result,
+                           progress_callback=lambda i, n, f: progress.append(i))
+    res = hb.solve(mesh, cfg)
+    assert [s[0] for s in seen] == [0, 1]
+    assert res.frequencies_hz.shape == (2,)
+    assert progress == [0, 1]
+
+
+def test_mixed_precision_refines_to_plain_solution():
+    mesh = G.icosphere(3, 0.1)
+    base = dict(freq_min_hz=1000.0, freq_max_hz=4000.0, freq_count=3, velocity_mode="velocity",
+                return_surface_pressure=True)
+    plain = hb.solve(mesh, hb.native_config(**base))
+    mixed = hb.solve(mesh, hb.native_config(precision="mixed", refine_tolerance=1e-6, **base))
+    for f in range(3):
+        a, b = mixed.surface_pressure_complex[f], plain.surface_pressure_complex[f]
+        assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-4
+        assert mixed.native_diagnostics[f]["refine_residual_rel"] <= 1e-6
+    assert np.max(np.abs(mixed.directivity_db - plain.directivity_db)) < 0.01

@@ -1,0 +1,109 @@
+"""Pins of the CPU oracle (test infrastructure) before it is trusted as the checker.
+
+* Duffy pair plans / unique triplets / image-pair counts: the reference tests'
+  known answers (tests/test_metal_native.py:1544-1550, 1809-1816, 1731, 2351).
+* Mirror-symmetry: the yz+xz quarter assembly equals the even-orbit reduction
+  of the full mesh (reference tests :1652-1732, tolerance 1e-6).
+* Pair blocks: FP64 level-4 subdivided quadrature of the reference test helper
+  (:230-350) reproduced exactly, and approached by the regular rule off contact.
+* Pulsating sphere: surface pressure vs the analytic Z/(rho c) = ika/(ika-1).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden, golden_buffers, known_answers
+
+from oracle.oracle import Oracle, dense_solve
+
+K_TINY = 1.8318326
+
+
+def test_tiny_mesh_pair_plan_matches_reference_known_answer():
+    want = known_answers()["tiny_pair_plan"]
+    for prec in ("f32", "f64"):
+        o = Oracle(golden_buffers("tiny"), 0, prec)
+        pairs, counts = o.duffy_pairs()
+        assert counts == {k: want[k] for k in ("coincident", "edge", "vertex")}
+        assert o.unique_triplets(pairs) == want["unique_triplets"]
+
+
+def test_quarter_image_adjacent_pairs_match_reference_known_answer():
+    o = Oracle(golden_buffers("yzxz_quarter"), 3, "f64")
+    pairs, _ = o.duffy_pairs()
+    image_pairs = int(np.sum((pairs[:, 2] != 0) | (pairs[:, 3] != 0)))
+    assert image_pairs == known_answers()["yzxz_quarter_image_adjacent_pairs"]
+
+
+def _orbit_reduce(A, b, orbits):
+    R = np.array([[A[np.ix_(r, c)].sum() for c in orbits] for r in orbits])
+    return R, np.array([b[r].sum() for r in orbits])
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_quarter_equals_orbit_reduced_full_domain(prec):
+    full = Oracle(golden_buffers("yzxz_full"), 0, prec)
+    quarter = Oracle(golden_buffers("yzxz_quarter"), 3, prec)
+    Af, bf = full.corrected(K_TINY, np.ones(4))
+    Aq, bq = quarter.corrected(K_TINY, np.ones(1))
+    Ar, br = _orbit_reduce(Af, bf, [np.array([0]), np.array([1, 3]), np.array([2, 4])])
+    tol = 1e-6 if prec == "f32" else 1e-12
+    assert np.linalg.norm(Aq - Ar) / np.linalg.norm(Ar) < tol
+    assert np.linalg.norm(bq - br) / np.linalg.norm(br) < tol
+
+
+def test_subdivided_pair_blocks_match_reference_fp64_helper():
+    pb = golden("pair_blocks.npz")
+    for i, (name, test, trial, k) in enumerate(known_answers()["pair_block_cases"]):
+        o = Oracle(golden_buffers(name), 0, "f64")
+        slp, dlp = o.pair_blocks(test, trial, mode=2, level=4, k=k)
+        np.testing.assert_allclose(slp, pb[f"{i}__slp"], rtol=1e-10, atol=1e-14)
+        np.testing.assert_allclose(dlp, pb[f"{i}__dlp"], rtol=1e-10, atol=1e-14)
+        if name == "ico2":
+            # well-separated pairs: the regular 6x6 rule already matches the subdivided reference
+            rs, rd = o.pair_blocks(test, trial, mode=0, k=k)
+            assert np.linalg.norm(rs - pb[f"{i}__slp"]) / np.linalg.norm(pb[f"{i}__slp"]) < 1e-3
+            assert np.linalg.norm(rd - pb[f"{i}__dlp"]) / np.linalg.norm(pb[f"{i}__dlp"]) < 1e-2
+
+
+def test_duffy_rule_integrates_constants():
+    o = Oracle(golden_buffers("tiny"), 0, "f64")
+    for kind in (1, 2, 3):
+        r = o.rule(kind)
+        assert r.shape[0] == {1: 1536, 2: 1280, 3: 512}[kind]
+        # weights integrate 1 over the 4-d domain T x T with area 1/4
+        assert abs(r[:, 4].sum() - 0.25) < 1e-12
+        assert np.all(r[:, 0] >= -1e-12) and np.all(r[:, 0] + r[:, 1] <= 1 + 1e-12)
+
+
+@pytest.mark.parametrize("freq", [200.0, 1000.0])
+def test_pulsating_sphere_matches_analytic(freq):
+    from hornlab_metal_bem_b200 import generators as G
+    from hornlab_metal_bem_b200.geometry import build_geometry_buffers
+    from hornlab_metal_bem_b200.mesh import make_pure_function_spaces
+
+    m = G.icosphere(2, 0.1)
+    p1, dp0 = make_pure_function_spaces(m.grid)
+    buf = build_geometry_buffers(m.grid, m.physical_tags, p1, dp0)
+    rho, c, a = 1.205, 343.0, 0.1
+    k = float(np.float32(2 * np.pi * freq / c))
+    q = np.full(buf.n_triangles, 1j * rho * 2 * np.pi * freq, np.complex64)
+    o = Oracle(buf, 0, "f64")
+    A, b = o.corrected(k, q)
+    p = dense_solve(A, b, "f64")
+    pa = rho * c * (1j * k * a) / (1j * k * a - 1)
+    assert abs(np.mean(p) - pa) / abs(pa) < 1e-2
+    fld = o.field(k, p, q, np.array([[0.0], [0.0], [2.0]]))
+    pr = pa * (a / 2.0) * np.exp(1j * k * (2.0 - a))
+    assert abs(fld[0] - pr) / abs(pr) < 2e-2
+
+
+def test_f32_oracle_tracks_f64_oracle():
+    o32 = Oracle(golden_buffers("ico2"), 0, "f32")
+    o64 = Oracle(golden_buffers("ico2"), 0, "f64")
+    q = np.full(o32.T, 1j * 7.5, np.complex64)
+    A32, b32 = o32.corrected(18.3, q)
+    A64, b64 = o64.corrected(18.3, q)
+    assert np.linalg.norm(A32 - A64) / np.linalg.norm(A64) < 1e-5
+    assert np.linalg.norm(b32 - b64) / np.linalg.norm(b64) < 1e-5
