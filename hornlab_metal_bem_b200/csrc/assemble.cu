@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 #include "hbem_internal.h"
 
@@ -31,6 +32,7 @@ namespace hbem {
 namespace {
 
 constexpr int kMaxFreqPerLaunch = 64;
+constexpr int kAsmFreqs = 2;  // wavenumbers per geometric sample in the pair kernel
 
 struct AsmArgs {
     const float4 *qp;
@@ -51,7 +53,7 @@ struct AsmArgs {
     float *b_re;
     float *b_im;
     long long q_stride, lda, a_stride, b_stride;
-    int T;
+    int T, nf;
     float rw;
     float k[kMaxFreqPerLaunch];
     float kt[kMaxFreqPerLaunch];  // k / (2 pi): phase in turns per metre
@@ -69,6 +71,13 @@ __device__ __forceinline__ float bas(int q, int i) {
     return i == 0 ? 1.0f - qx(q) - qy(q) : (i == 1 ? qx(q) : qy(q));
 }
 
+// Round to nearest integer on the FMA pipe (|t| < 2^22): adding and removing
+// 1.5 * 2^23 leaves the rounded value.
+__device__ __forceinline__ float round_fma(float t) {
+    const float big = 12582912.0f;
+    return __fsub_rn(__fadd_rn(t, big), big);
+}
+
 // One kernel sample: adds dG/dn_y (D) and, when NEED_G, G to the running
 // sums.  The 1/(4 pi) factor is applied once per pair block.  r^2 <= 1e-14
 // is treated as the singular point and contributes nothing (main.swift:3443-3480).
@@ -80,7 +89,7 @@ __device__ __forceinline__ void sample(float dx, float dy, float dz, float nx, f
     rinv = r2 > 1.0e-14f ? rinv : 0.0f;
     const float r = r2 * rinv;
     float t = r * kt;
-    t -= rintf(t);
+    t -= round_fma(t);
     float s, c;
     __sincosf(t * 6.28318530717958647692f, &s, &c);
     float g = rinv;
@@ -99,195 +108,304 @@ __device__ __forceinline__ void sample(float dx, float dy, float dz, float nx, f
     }
 }
 
-template <int SYM, bool CK, bool NEED_G>
-__device__ __forceinline__ void pair_block(const float (&tx)[6], const float (&ty)[6], const float (&tz)[6],
-                                           const float4 *__restrict__ sp, float nx, float ny, float nz,
-                                           bool self, float k, float kt, float ki, float (&are)[9],
-                                           float (&aim)[9], float (&sre)[3], float (&sim)[3]) {
+// Per test quadrature point a: wa[a][i] = w_a * phi_i(x_a) (uniform across the
+// warp, served from the constant cache).
+__constant__ float c_wa[6][3];
+__constant__ float c_wb[6][3];   // w_b * phi_j(y_b)
+__constant__ float c_w[6];       // w_b
+
+// One geometric sample y - x shared by NF wavenumbers.  Frequency-independent
+// part once (distance, 1/r, (y-x).n / r^3); per wavenumber the phase in turns
+// reduced to [-1/2, 1/2], one sincos, and the dG/dn_y update
+//   D = (c + i s)(-1/r + i k) (y-x).n / r^2     (times 1/(4 pi) later)
+// and, when NEED_G, G = (c + i s) / r.
+template <int NF, bool CK, bool NEED_G>
+__device__ __forceinline__ void sample_nf(float dx, float dy, float dz, float nx, float ny, float nz,
+                                          const float (&k)[NF], const float (&kt)[NF], const float (&ki)[NF],
+                                          float (&dre)[NF], float (&dim)[NF], float (&gre)[NF], float (&gim)[NF]) {
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    float u = rsqrtf(r2);
+    u = r2 > 1.0e-14f ? u : 0.0f;
+    const float r = r2 * u;
+    const float dn = fmaf(dx, nx, fmaf(dy, ny, dz * nz));
+    const float h = dn * (u * u);
 #pragma unroll
-    for (int i = 0; i < 9; ++i) are[i] = aim[i] = 0.0f;
+    for (int f = 0; f < NF; ++f) {
+        float t = r * kt[f];
+        t -= round_fma(t);
+        float sn, cs;
+        __sincosf(t * 6.28318530717958647692f, &sn, &cs);
+        float hh = h, uu = u, fre = u;
+        if (CK) {
+            const float damp = __expf(-ki[f] * r);
+            hh *= damp;
+            uu *= damp;
+            fre += ki[f];
+        }
+        // D = hh (c + i s)(-fre + i k)
+        dre[f] = fmaf(-hh, fmaf(cs, fre, sn * k[f]), dre[f]);
+        dim[f] = fmaf(hh, fmaf(cs, k[f], -sn * fre), dim[f]);
+        if (NEED_G) {
+            gre[f] = fmaf(uu, cs, gre[f]);
+            gim[f] = fmaf(uu, sn, gim[f]);
+        }
+    }
+}
+
+template <int SYM, int NF, bool CK, bool NEED_G>
+__device__ __forceinline__ void pair_block(const float4 *__restrict__ tq, const float4 *__restrict__ sp, float nx,
+                                           float ny, float nz, bool self, const float (&k)[NF],
+                                           const float (&kt)[NF], const float (&ki)[NF], float (&are)[NF][9],
+                                           float (&aim)[NF][9], float (&sre)[NF][3], float (&sim)[NF][3]) {
 #pragma unroll
-    for (int i = 0; i < 3; ++i) sre[i] = sim[i] = 0.0f;
+    for (int f = 0; f < NF; ++f) {
 #pragma unroll
+        for (int i = 0; i < 9; ++i) are[f][i] = aim[f][i] = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) sre[f][i] = sim[f][i] = 0.0f;
+    }
+    // The test-point loop stays rolled (test point from shared memory, weights
+    // from constant memory) so the kernel body fits the instruction cache;
+    // the trial-point loop is unrolled with the image samples.
+#pragma unroll 1
     for (int a = 0; a < 6; ++a) {
-        float ere[3] = {0, 0, 0}, eim[3] = {0, 0, 0};
-        float hre = 0, him = 0;
+        const float4 x = tq[a * kTestTile];
+        float ere[NF][3], eim[NF][3], hre[NF], him[NF];
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+            hre[f] = him[f] = 0.f;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) ere[f][j] = eim[f][j] = 0.f;
+        }
 #pragma unroll
         for (int b = 0; b < 6; ++b) {
             const float4 y = sp[b];
-            float dre = 0, dim = 0, gre = 0, gim = 0;
-            if (!(self && a == b))
-                sample<CK, NEED_G>(y.x - tx[a], y.y - ty[a], y.z - tz[a], nx, ny, nz, k, kt, ki, dre, dim, gre, gim);
-            if (SYM == 1 || SYM == 3)
-                sample<CK, NEED_G>(-y.x - tx[a], y.y - ty[a], y.z - tz[a], -nx, ny, nz, k, kt, ki, dre, dim, gre, gim);
-            if (SYM == 2 || SYM == 3)
-                sample<CK, NEED_G>(y.x - tx[a], -y.y - ty[a], y.z - tz[a], nx, -ny, nz, k, kt, ki, dre, dim, gre, gim);
-            if (SYM == 3)
-                sample<CK, NEED_G>(-y.x - tx[a], -y.y - ty[a], y.z - tz[a], -nx, -ny, nz, k, kt, ki, dre, dim, gre, gim);
-            if (SYM == 4)
-                sample<CK, NEED_G>(y.x - tx[a], y.y - ty[a], -y.z - tz[a], nx, ny, -nz, k, kt, ki, dre, dim, gre, gim);
+            float dre[NF], dim[NF], gre[NF], gim[NF];
 #pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                const float wb = qw(b) * bas(b, j);
-                ere[j] = fmaf(dre, wb, ere[j]);
-                eim[j] = fmaf(dim, wb, eim[j]);
-            }
-            if (NEED_G) {
-                hre = fmaf(gre, qw(b), hre);
-                him = fmaf(gim, qw(b), him);
+            for (int f = 0; f < NF; ++f) dre[f] = dim[f] = gre[f] = gim[f] = 0.f;
+            if (!(self && a == b))
+                sample_nf<NF, CK, NEED_G>(y.x - x.x, y.y - x.y, y.z - x.z, nx, ny, nz, k, kt, ki, dre, dim, gre, gim);
+            if (SYM == 1 || SYM == 3)
+                sample_nf<NF, CK, NEED_G>(-y.x - x.x, y.y - x.y, y.z - x.z, -nx, ny, nz, k, kt, ki, dre, dim, gre, gim);
+            if (SYM == 2 || SYM == 3)
+                sample_nf<NF, CK, NEED_G>(y.x - x.x, -y.y - x.y, y.z - x.z, nx, -ny, nz, k, kt, ki, dre, dim, gre, gim);
+            if (SYM == 3)
+                sample_nf<NF, CK, NEED_G>(-y.x - x.x, -y.y - x.y, y.z - x.z, -nx, -ny, nz, k, kt, ki, dre, dim, gre,
+                                          gim);
+            if (SYM == 4)
+                sample_nf<NF, CK, NEED_G>(y.x - x.x, y.y - x.y, -y.z - x.z, nx, ny, -nz, k, kt, ki, dre, dim, gre, gim);
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const float wb = qw(b) * bas(b, j);
+                    ere[f][j] = fmaf(dre[f], wb, ere[f][j]);
+                    eim[f][j] = fmaf(dim[f], wb, eim[f][j]);
+                }
+                if (NEED_G) {
+                    hre[f] = fmaf(gre[f], qw(b), hre[f]);
+                    him[f] = fmaf(gim[f], qw(b), him[f]);
+                }
             }
         }
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
-            const float wa = qw(a) * bas(a, i);
+            const float wa = c_wa[a][i];
 #pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                are[i * 3 + j] = fmaf(wa, ere[j], are[i * 3 + j]);
-                aim[i * 3 + j] = fmaf(wa, eim[j], aim[i * 3 + j]);
-            }
-            if (NEED_G) {
-                sre[i] = fmaf(wa, hre, sre[i]);
-                sim[i] = fmaf(wa, him, sim[i]);
+            for (int f = 0; f < NF; ++f) {
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    are[f][i * 3 + j] = fmaf(wa, ere[f][j], are[f][i * 3 + j]);
+                    aim[f][i * 3 + j] = fmaf(wa, eim[f][j], aim[f][i * 3 + j]);
+                }
+                if (NEED_G) {
+                    sre[f][i] = fmaf(wa, hre[f], sre[f][i]);
+                    sim[f][i] = fmaf(wa, him[f], sim[f][i]);
+                }
             }
         }
     }
 }
 
-template <int SYM, bool CK>
-__global__ void __launch_bounds__(kAsmThreads, 2) k_regular(const __grid_constant__ AsmArgs p) {
+// blockIdx.z selects a group of NF consecutive frequencies; a missing last
+// member (odd count) is computed on a repeated wavenumber and not flushed.
+template <int SYM, bool CK, int MINB>
+__global__ void __launch_bounds__(kAsmThreads, MINB) k_regular(const __grid_constant__ AsmArgs p) {
+    constexpr int NF = kAsmFreqs;
     extern __shared__ float2 s_acc[];
     __shared__ float4 s_qp[kTrialTile * 6];
+    __shared__ float4 s_tq[6 * kTestTile];   // test points, [a][lane]
     __shared__ float4 s_nrm[kTrialTile];
     __shared__ uchar4 s_cs[kTrialTile];
-    __shared__ float4 s_qb[kTrialTile];
+    __shared__ float4 s_qb[NF][kTrialTile];
     __shared__ int s_flag[kTrialTile];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int f = blockIdx.z;
+    const int f0 = blockIdx.z * NF;
+    const int nfv = min(NF, p.nf - f0);
     const int test_tile = blockIdx.y, trial_tile = blockIdx.x;
     const int T = p.T;
     const int r0 = p.row_off[test_tile], nrows = p.row_off[test_tile + 1] - r0;
     const int c0 = p.col_off[trial_tile], ncols = p.col_off[trial_tile + 1] - c0;
+    const int ldc = ncols | 1;  // odd row pitch spreads same-column rows over banks
+    const int plane = nrows * ldc + nrows;
     const int tbase = trial_tile * kTrialTile;
     const int ntrial = min(kTrialTile, T - tbase);
-    float2 *s_rhs = s_acc + nrows * ncols;
+    const int test0 = test_tile * kTestTile;
+    const int ntest = min(kTestTile, T - test0);
 
-    for (int i = tid; i < nrows * ncols + nrows; i += kAsmThreads) s_acc[i] = make_float2(0.f, 0.f);
+    for (int i = tid; i < NF * plane; i += kAsmThreads) s_acc[i] = make_float2(0.f, 0.f);
     for (int i = tid; i < ntrial * 6; i += kAsmThreads) s_qp[i] = p.qp[(size_t)tbase * 6 + i];
+    for (int i = tid; i < ntest * 6; i += kAsmThreads) {
+        const int t = i / 6, a = i - 6 * t;
+        s_tq[a * kTestTile + t] = p.qp[(size_t)(test0 + t) * 6 + a];
+    }
     for (int i = tid; i < ntrial; i += kAsmThreads) {
         s_nrm[i] = p.nrm[tbase + i];
         s_cs[i] = p.trial_slot[tbase + i];
         const int orig = p.tri[tbase + i].w;
-        float4 qb = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (p.q_re) {
-            qb.x = p.q_re[(size_t)f * p.q_stride + orig];
-            qb.y = p.q_im[(size_t)f * p.q_stride + orig];
+        int flag = 0;
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+            float4 qb = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (p.q_re && f < nfv) {
+                qb.x = p.q_re[(size_t)(f0 + f) * p.q_stride + orig];
+                qb.y = p.q_im[(size_t)(f0 + f) * p.q_stride + orig];
+            }
+            if (p.beta_re) {
+                qb.z = p.beta_re[orig];
+                qb.w = p.beta_im[orig];
+            }
+            s_qb[f][i] = qb;
+            flag |= (qb.x != 0.f || qb.y != 0.f || qb.z != 0.f || qb.w != 0.f) ? 1 : 0;
         }
-        if (p.beta_re) {
-            qb.z = p.beta_re[orig];
-            qb.w = p.beta_im[orig];
-        }
-        s_qb[i] = qb;
-        s_flag[i] = (qb.x != 0.f || qb.y != 0.f || qb.z != 0.f || qb.w != 0.f) ? 1 : 0;
+        s_flag[i] = flag;
     }
     __syncthreads();
 
-    const float k = p.k[f], kt = p.kt[f], ki = p.ki[f];
-    const int test = test_tile * kTestTile + lane;
-    if (test < T) {
-        float tx[6], ty[6], tz[6];
+    float k[NF], kt[NF], ki[NF];
 #pragma unroll
-        for (int a = 0; a < 6; ++a) {
-            const float4 v = p.qp[(size_t)test * 6 + a];
-            tx[a] = v.x;
-            ty[a] = v.y;
-            tz[a] = v.z;
-        }
+    for (int f = 0; f < NF; ++f) {
+        const int ff = f0 + min(f, nfv - 1);
+        k[f] = p.k[ff];
+        kt[f] = p.kt[ff];
+        ki[f] = p.ki[ff];
+    }
+    const int test = test0 + lane;
+    if (lane < ntest) {
         const float tjac = p.nrm[test].w;
         const uchar4 rs = p.test_slot[test];
         const int rslot[3] = {rs.x, rs.y, rs.z};
+        const float4 *tq = &s_tq[lane];
         for (int jj = warp; jj < ntrial; jj += kAsmThreads / 32) {
             const float4 nj = s_nrm[jj];
             const bool self = (tbase + jj) == test;
-            float are[9], aim[9], sre[3], sim[3];
+            float are[NF][9], aim[NF][9], sre[NF][3], sim[NF][3];
             if (s_flag[jj])
-                pair_block<SYM, CK, true>(tx, ty, tz, &s_qp[jj * 6], nj.x, nj.y, nj.z, self, k, kt, ki, are, aim, sre, sim);
+                pair_block<SYM, NF, CK, true>(tq, &s_qp[jj * 6], nj.x, nj.y, nj.z, self, k, kt, ki, are, aim, sre, sim);
             else
-                pair_block<SYM, CK, false>(tx, ty, tz, &s_qp[jj * 6], nj.x, nj.y, nj.z, self, k, kt, ki, are, aim, sre, sim);
+                pair_block<SYM, NF, CK, false>(tq, &s_qp[jj * 6], nj.x, nj.y, nj.z, self, k, kt, ki, are, aim, sre,
+                                               sim);
             const float scale = HBEM_INV4PI * tjac * nj.w;
-            const float4 qb = s_qb[jj];
             const uchar4 cs = s_cs[jj];
             const int cslot[3] = {cs.x, cs.y, cs.z};
-            float rob_re = 0.f, rob_im = 0.f;  // -(1/3) i k beta
-            if (qb.z != 0.f || qb.w != 0.f) {
-                // i k beta with k = k + i ki: (-ki + i k)(br + i bi)
-                const float ikb_re = -ki * qb.z - k * qb.w;
-                const float ikb_im = -ki * qb.w + k * qb.z;
-                rob_re = -ikb_re * (1.0f / 3.0f);
-                rob_im = -ikb_im * (1.0f / 3.0f);
-            }
 #pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                const float s_re = sre[i] * scale, s_im = sim[i] * scale;
-                const float radd_re = rob_re * s_re - rob_im * s_im;
-                const float radd_im = rob_re * s_im + rob_im * s_re;
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    float vre = are[i * 3 + j] * scale + radd_re;
-                    float vim = aim[i * 3 + j] * scale + radd_im;
-                    if (self) vre -= 0.25f * tjac * (i == j ? (1.0f / 6.0f) : (1.0f / 12.0f));
-                    float2 *dst = &s_acc[rslot[i] * ncols + cslot[j]];
-                    atomicAdd(&dst->x, vre * p.rw);
-                    atomicAdd(&dst->y, vim * p.rw);
+            for (int f = 0; f < NF; ++f) {
+                const float4 qb = s_qb[f][jj];
+                float2 *acc = s_acc + f * plane;
+                float2 *rhs = acc + nrows * ldc;
+                float rob_re = 0.f, rob_im = 0.f;  // -(1/3) i k beta
+                if (qb.z != 0.f || qb.w != 0.f) {
+                    // i k beta with k = k + i ki: (-ki + i k)(br + i bi)
+                    const float ikb_re = -ki[f] * qb.z - k[f] * qb.w;
+                    const float ikb_im = -ki[f] * qb.w + k[f] * qb.z;
+                    rob_re = -ikb_re * (1.0f / 3.0f);
+                    rob_im = -ikb_im * (1.0f / 3.0f);
                 }
-                if (qb.x != 0.f || qb.y != 0.f) {
-                    atomicAdd(&s_rhs[rslot[i]].x, (s_re * qb.x - s_im * qb.y) * p.rw);
-                    atomicAdd(&s_rhs[rslot[i]].y, (s_re * qb.y + s_im * qb.x) * p.rw);
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    const float s_re = sre[f][i] * scale, s_im = sim[f][i] * scale;
+                    const float radd_re = rob_re * s_re - rob_im * s_im;
+                    const float radd_im = rob_re * s_im + rob_im * s_re;
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        float vre = are[f][i * 3 + j] * scale + radd_re;
+                        float vim = aim[f][i * 3 + j] * scale + radd_im;
+                        if (self) vre -= 0.25f * tjac * (i == j ? (1.0f / 6.0f) : (1.0f / 12.0f));
+                        float2 *dst = &acc[rslot[i] * ldc + cslot[j]];
+                        atomicAdd(&dst->x, vre * p.rw);
+                        atomicAdd(&dst->y, vim * p.rw);
+                    }
+                    if (qb.x != 0.f || qb.y != 0.f) {
+                        atomicAdd(&rhs[rslot[i]].x, (s_re * qb.x - s_im * qb.y) * p.rw);
+                        atomicAdd(&rhs[rslot[i]].y, (s_re * qb.y + s_im * qb.x) * p.rw);
+                    }
                 }
             }
         }
     }
     __syncthreads();
 
-    float *are_g = p.a_re + (size_t)f * p.a_stride;
-    float *aim_g = p.a_im + (size_t)f * p.a_stride;
-    for (int e = tid; e < nrows * ncols; e += kAsmThreads) {
-        const int r = e / ncols, c = e - r * ncols;
-        const size_t off = (size_t)p.rows[r0 + r] * p.lda + p.cols[c0 + c];
-        const float2 v = s_acc[e];
-        atomicAdd(are_g + off, v.x);
-        atomicAdd(aim_g + off, v.y);
-    }
-    if (p.q_re && trial_tile >= 0) {
-        for (int r = tid; r < nrows; r += kAsmThreads) {
-            const float2 v = s_rhs[r];
-            if (v.x != 0.f || v.y != 0.f) {
-                const size_t off = (size_t)f * p.b_stride + p.rows[r0 + r];
-                atomicAdd(p.b_re + off, v.x);
-                atomicAdd(p.b_im + off, v.y);
+    for (int f = 0; f < nfv; ++f) {
+        const float2 *acc = s_acc + f * plane;
+        float *are_g = p.a_re + (size_t)(f0 + f) * p.a_stride;
+        float *aim_g = p.a_im + (size_t)(f0 + f) * p.a_stride;
+        for (int e = tid; e < nrows * ncols; e += kAsmThreads) {
+            const int r = e / ncols, c = e - r * ncols;
+            const size_t off = (size_t)p.rows[r0 + r] * p.lda + p.cols[c0 + c];
+            const float2 v = acc[r * ldc + c];
+            atomicAdd(are_g + off, v.x);
+            atomicAdd(aim_g + off, v.y);
+        }
+        if (p.q_re) {
+            const float2 *rhs = acc + nrows * ldc;
+            for (int r = tid; r < nrows; r += kAsmThreads) {
+                const float2 v = rhs[r];
+                if (v.x != 0.f || v.y != 0.f) {
+                    const size_t off = (size_t)(f0 + f) * p.b_stride + p.rows[r0 + r];
+                    atomicAdd(p.b_re + off, v.x);
+                    atomicAdd(p.b_im + off, v.y);
+                }
             }
         }
     }
 }
 
-template <int SYM, bool CK>
+template <int SYM, bool CK, int MINB>
 cudaError_t launch_regular_t(const AsmArgs &a, dim3 grid, size_t smem, cudaStream_t st) {
-    auto kern = k_regular<SYM, CK>;
+    auto kern = k_regular<SYM, CK, MINB>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     kern<<<grid, kAsmThreads, smem, st>>>(a);
     return cudaGetLastError();
 }
 
+// Resident CTAs per SM for the pair kernel: 2 (128 registers, no spills) or 3
+// (80 registers).  HBEM_ASM_MINBLOCKS overrides the default for tuning.
+int regular_min_blocks() {
+    static int v = [] {
+        const char *e = getenv("HBEM_ASM_MINBLOCKS");
+        int m = e ? atoi(e) : 2;
+        return (m == 3) ? 3 : 2;
+    }();
+    return v;
+}
+
+template <bool CK, int MINB>
+cudaError_t dispatch_sym_m(int sym, const AsmArgs &a, dim3 grid, size_t smem, cudaStream_t st) {
+    switch (sym) {
+        case 0: return launch_regular_t<0, CK, MINB>(a, grid, smem, st);
+        case 1: return launch_regular_t<1, CK, MINB>(a, grid, smem, st);
+        case 2: return launch_regular_t<2, CK, MINB>(a, grid, smem, st);
+        case 3: return launch_regular_t<3, CK, MINB>(a, grid, smem, st);
+        default: return launch_regular_t<4, CK, MINB>(a, grid, smem, st);
+    }
+}
+
 template <bool CK>
 cudaError_t dispatch_sym(int sym, const AsmArgs &a, dim3 grid, size_t smem, cudaStream_t st) {
-    switch (sym) {
-        case 0: return launch_regular_t<0, CK>(a, grid, smem, st);
-        case 1: return launch_regular_t<1, CK>(a, grid, smem, st);
-        case 2: return launch_regular_t<2, CK>(a, grid, smem, st);
-        case 3: return launch_regular_t<3, CK>(a, grid, smem, st);
-        default: return launch_regular_t<4, CK>(a, grid, smem, st);
-    }
+    return regular_min_blocks() == 3 ? dispatch_sym_m<CK, 3>(sym, a, grid, smem, st)
+                                     : dispatch_sym_m<CK, 2>(sym, a, grid, smem, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -367,11 +485,14 @@ __global__ void __launch_bounds__(256) k_duffy(const __grid_constant__ DuffyArgs
     const float jac = (2.f * p.areas[pr.test]) * (2.f * p.areas[pr.trial]);
     const float k = p.k[f], kt = p.kt[f], ki = p.ki[f];
 
-    double acc[24];
+    // Per-lane partial sums over this lane's <= 48 points stay in FP32 (separate
+    // singular and regular sets, so their difference is never formed in FP32);
+    // the cross-lane reduction and the singular - regular difference are FP64.
+    float accs[24], accr[24];
 #pragma unroll
-    for (int e = 0; e < 24; ++e) acc[e] = 0.0;
+    for (int e = 0; e < 24; ++e) accs[e] = accr[e] = 0.0f;
 
-    auto accumulate = [&](float txi, float teta, float sxi, float seta, float w) {
+    auto accumulate = [&](float (&acc)[24], float txi, float teta, float sxi, float seta, float w) {
         if (tswap) { const float t = txi; txi = teta; teta = t; }
         if (sswap) { const float t = sxi; sxi = seta; seta = t; }
         const float tb[3] = {1.f - txi - teta, txi, teta};
@@ -388,13 +509,13 @@ __global__ void __launch_bounds__(256) k_duffy(const __grid_constant__ DuffyArgs
         gre *= w; gim *= w; dre *= w; dim *= w;
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
-            acc[2 * i] += (double)(gre * tb[i]);
-            acc[2 * i + 1] += (double)(gim * tb[i]);
+            acc[2 * i] = fmaf(gre, tb[i], acc[2 * i]);
+            acc[2 * i + 1] = fmaf(gim, tb[i], acc[2 * i + 1]);
+            const float dti_re = dre * tb[i], dti_im = dim * tb[i];
 #pragma unroll
             for (int j = 0; j < 3; ++j) {
-                const float bb = tb[i] * sb[j];
-                acc[6 + 2 * (i * 3 + j)] += (double)(dre * bb);
-                acc[7 + 2 * (i * 3 + j)] += (double)(dim * bb);
+                acc[6 + 2 * (i * 3 + j)] = fmaf(dti_re, sb[j], acc[6 + 2 * (i * 3 + j)]);
+                acc[7 + 2 * (i * 3 + j)] = fmaf(dti_im, sb[j], acc[7 + 2 * (i * 3 + j)]);
             }
         }
     };
@@ -404,7 +525,7 @@ __global__ void __launch_bounds__(256) k_duffy(const __grid_constant__ DuffyArgs
     for (int q = lane; q < 36; q += 32) {
         const int a = q / 6, b = q - 6 * (q / 6);
         if (pr.test == pr.trial && pr.test_mask == pr.trial_mask && a == b) continue;
-        accumulate(qx(a), qy(a), qx(b), qy(b), -qw(a) * qw(b));
+        accumulate(accr, qx(a), qy(a), qx(b), qy(b), qw(a) * qw(b));
     }
     const int ri = pr.kind - 1;
     const int off = p.rule_off[ri], cnt = p.rule_cnt[ri];
@@ -414,14 +535,17 @@ __global__ void __launch_bounds__(256) k_duffy(const __grid_constant__ DuffyArgs
         float tx_, ty_, sx_, sy_;
         remap(r.x, r.y, pr.kind, pr.tl1, pr.tl2, tx_, ty_);
         remap(r.z, r.w, pr.kind, pr.sl1, pr.sl2, sx_, sy_);
-        accumulate(tx_, ty_, sx_, sy_, w);
+        accumulate(accs, tx_, ty_, sx_, sy_, w);
     }
+    double acc[24];
 #pragma unroll
     for (int e = 0; e < 24; ++e) {
+        double v = (double)accs[e] - (double)accr[e];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc[e] += __shfl_xor_sync(0xffffffffu, acc[e], o);
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        acc[e] = v;
     }
-    const double scale = (double)HBEM_INV4PI * (double)jac;
+    const double scale = (double)HBEM_INV4PI * (double)jac * (double)pr.weight;
     // lane e < 9 owns DLP entry e; lanes 9..11 own the SLP rows
     double sr = 0, si = 0, dr = 0, di = 0;
 #pragma unroll
@@ -467,7 +591,26 @@ int launch_regular(Session &s, int n_freq, const float *k_re, const float *k_im,
                    const float *q_im, long long q_stride, const float *beta_re, const float *beta_im, float *a_re,
                    float *a_im, long long lda, long long a_stride, float *b_re, float *b_im, long long b_stride,
                    cudaStream_t st) {
-    const size_t smem = (size_t)(s.max_rows * s.max_cols + s.max_rows) * sizeof(float2);
+    const size_t smem = (size_t)kAsmFreqs * (s.max_rows * (s.max_cols | 1) + s.max_rows) * sizeof(float2);
+    static bool consts_ready[64] = {false};
+    if (s.device >= 0 && s.device < 64 && !consts_ready[s.device]) {
+        const double QX[6] = {0.4459484909159651, 0.0915762135097710, 0.1081030181680700,
+                              0.4459484909159651, 0.8168475729804590, 0.0915762135097710};
+        const double QY[6] = {0.4459484909159651, 0.0915762135097700, 0.4459484909159651,
+                              0.1081030181680700, 0.0915762135097700, 0.8168475729804580};
+        const float QW[6] = {HBEM_QWA, HBEM_QWB, HBEM_QWA, HBEM_QWA, HBEM_QWB, HBEM_QWB};
+        float wa[6][3], w[6];
+        for (int q = 0; q < 6; ++q) {
+            const float x = (float)QX[q], y = (float)QY[q];
+            const float b[3] = {1.0f - x - y, x, y};
+            for (int i = 0; i < 3; ++i) wa[q][i] = QW[q] * b[i];
+            w[q] = QW[q];
+        }
+        HBEM_CUDA(cudaMemcpyToSymbol(c_wa, wa, sizeof(wa)));
+        HBEM_CUDA(cudaMemcpyToSymbol(c_wb, wa, sizeof(wa)));
+        HBEM_CUDA(cudaMemcpyToSymbol(c_w, w, sizeof(w)));
+        consts_ready[s.device] = true;
+    }
     if (smem > 180 * 1024)
         return fail(HBEM_ERR_ARG, "assembly tile needs too much shared memory (mesh ordering too scattered)");
     for (int f0 = 0; f0 < n_freq; f0 += kMaxFreqPerLaunch) {
@@ -488,7 +631,8 @@ int launch_regular(Session &s, int n_freq, const float *k_re, const float *k_im,
         fill_k(a.k, a.kt, a.ki, k_re + f0, k_im ? k_im + f0 : nullptr, nf);
         for (int f = 0; f < nf; ++f) ck |= a.ki[f] != 0.f;
         if (!a.b_re) a.q_re = a.q_im = nullptr;
-        dim3 grid(s.n_trial_tiles, s.n_test_tiles, nf);
+        a.nf = nf;
+        dim3 grid(s.n_trial_tiles, s.n_test_tiles, (nf + kAsmFreqs - 1) / kAsmFreqs);
         cudaError_t e = ck ? dispatch_sym<true>(s.sym, a, grid, smem, st) : dispatch_sym<false>(s.sym, a, grid, smem, st);
         if (e != cudaSuccess) return cuda_fail(e, "k_regular launch");
         count_launch();

@@ -39,7 +39,7 @@ constexpr int kAsmThreads = 256;
 struct DuffyPair {
     int test, trial, test_mask, trial_mask;   // original triangle ids, image masks
     int kind, tl1, tl2, sl1;                  // 1 coincident, 2 edge, 3 vertex; image-local ids
-    int sl2, row_base, col_base, pad;         // row_base/col_base unused (reserved)
+    int sl2, weight, col_base, pad;           // weight: exact image twins folded into one pair
 };
 
 struct Session {

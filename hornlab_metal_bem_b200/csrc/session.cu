@@ -383,21 +383,17 @@ extern "C" int hbem_session_create(const float *vertices_3xv, int n_vertices, co
     // Duffy pairs, sorted by kind (coincident, edge, vertex)
     std::vector<DuffyPair> pairs;
     build_duffy_pairs(*s, pairs);
-    std::stable_sort(pairs.begin(), pairs.end(), [](const DuffyPair &a, const DuffyPair &b) { return a.kind < b.kind; });
-    s->n_pairs = (int)pairs.size();
     for (auto &p : pairs) {
         if (p.kind == 1) ++s->n_coincident;
         else if (p.kind == 2) ++s->n_edge;
         else ++s->n_vertex;
         if (p.test_mask || p.trial_mask) ++s->n_image_pairs;
+        p.weight = 1;
     }
-    s->kind_begin[0] = 0;
-    s->kind_begin[1] = (int)s->n_coincident;
-    s->kind_begin[2] = (int)(s->n_coincident + s->n_edge);
-    s->kind_begin[3] = s->n_pairs;
     {
+        // unique (row, col) triplets of the full enumeration (main.swift:2560-2613)
         std::vector<long long> keys;
-        keys.reserve((size_t)s->n_pairs * 9);
+        keys.reserve((size_t)pairs.size() * 9);
         for (auto &p : pairs)
             for (int i = 0; i < 3; ++i)
                 for (int j = 0; j < 3; ++j)
@@ -405,6 +401,24 @@ extern "C" int hbem_session_create(const float *vertices_3xv, int n_vertices, co
         std::sort(keys.begin(), keys.end());
         s->n_unique_triplets = (long long)(std::unique(keys.begin(), keys.end()) - keys.begin());
     }
+    if (sym_code == 3) {
+        // With both yz and xz planes, mirroring a (test image, trial image) pair
+        // by the even mask 3 (a rotation by pi about z) maps it onto the pair
+        // (test_mask ^ 3, trial_mask ^ 3) with identical local numbering and
+        // bitwise-identical kernel samples (sign flips are exact).  The pair
+        // list holds both twins; keep one with weight 2.
+        std::vector<DuffyPair> kept;
+        kept.reserve(pairs.size() / 2 + 1);
+        for (auto &p : pairs)
+            if (p.test_mask == 0 || p.test_mask == 1) {
+                p.weight = 2;
+                kept.push_back(p);
+            }
+        pairs.swap(kept);
+    }
+    std::stable_sort(pairs.begin(), pairs.end(), [](const DuffyPair &a, const DuffyPair &b) { return a.kind < b.kind; });
+    s->n_pairs = (int)pairs.size();
+
     std::vector<float4> rule;
     std::vector<float> rule_w;
     for (int kind = 1; kind <= 3; ++kind) {
@@ -476,9 +490,12 @@ extern "C" int hbem_session_query(const hbem_session *h, int key, long long *val
         case HBEM_Q_SYMMETRY: *value = s->sym; break;
         case HBEM_Q_KERNEL_LAUNCHES: *value = s->launches; break;
         case HBEM_Q_REGULAR_EVALS: *value = T * T * 36 * M; break;
-        case HBEM_Q_DUFFY_EVALS:
-            *value = s->n_coincident * (1536 + 36) + s->n_edge * (1280 + 36) + s->n_vertex * (512 + 36);
+        case HBEM_Q_DUFFY_EVALS: {
+            // evaluated after exact twin folding
+            const long long fold = s->sym == 3 ? 2 : 1;
+            *value = (s->n_coincident * (1536 + 36) + s->n_edge * (1280 + 36) + s->n_vertex * (512 + 36)) / fold;
             break;
+        }
         default: return fail(HBEM_ERR_ARG, "hbem_session_query: unknown key");
     }
     return HBEM_OK;

@@ -249,8 +249,8 @@ class NativeSession:
         if isinstance(z, tuple):
             return z
         arr = np.asarray(z).reshape(shape)
-        re = torch.from_numpy(np.ascontiguousarray(arr.real, dtype=np.float32)).to(dev)
-        im = torch.from_numpy(np.ascontiguousarray(arr.imag, dtype=np.float32)).to(dev)
+        re = torch.tensor(np.ascontiguousarray(arr.real, dtype=np.float32), device=dev).contiguous()
+        im = torch.tensor(np.ascontiguousarray(arr.imag, dtype=np.float32), device=dev).contiguous()
         return re, im
 
     def field(self, k_re, p_re, p_im, q, obs_3xn, stream=None):
@@ -259,22 +259,25 @@ class NativeSession:
         F = k_re.shape[0]
         dev = p_re.device
         qr, qi = self._split_device(q, (F, self.n_triangles), dev)
-        obs = torch.as_tensor(np.ascontiguousarray(obs_3xn, dtype=np.float32), device=dev)
+        p_re, p_im = p_re.reshape(F, self.n_dof).contiguous(), p_im.reshape(F, self.n_dof).contiguous()
+        obs = torch.as_tensor(np.ascontiguousarray(obs_3xn, dtype=np.float32), device=dev).contiguous()
         N = obs.shape[1]
         out_re = torch.empty((F, N), dtype=torch.float32, device=dev)
         out_im = torch.empty_like(out_re)
         check(self.lib.hbem_field(
-            self.handle, F, _np_ptr(k_re), _t_ptr(p_re), _t_ptr(p_im), p_re.stride(0), _t_ptr(qr), _t_ptr(qi),
-            qr.stride(0), _t_ptr(obs), N, _t_ptr(out_re), _t_ptr(out_im), N, _stream_ptr(stream)), "hbem_field", self.lib)
+            self.handle, F, _np_ptr(k_re), _t_ptr(p_re), _t_ptr(p_im), self.n_dof, _t_ptr(qr), _t_ptr(qi),
+            self.n_triangles, _t_ptr(obs), N, _t_ptr(out_re), _t_ptr(out_im), N, _stream_ptr(stream)), "hbem_field",
+            self.lib)
         return out_re, out_im
 
     def tag_average(self, p_re, p_im, tags, stream=None):
         torch = require_cuda()
         tags = np.ascontiguousarray(tags, dtype=np.int32)
         F = p_re.shape[0]
+        p_re, p_im = p_re.reshape(F, self.n_dof).contiguous(), p_im.reshape(F, self.n_dof).contiguous()
         out = torch.empty((F, tags.shape[0], 2), dtype=torch.float64, device=p_re.device)
         check(self.lib.hbem_reduce_tag_avg(
-            self.handle, F, _t_ptr(p_re), _t_ptr(p_im), p_re.stride(0), _np_ptr(tags), tags.shape[0], _t_ptr(out),
+            self.handle, F, _t_ptr(p_re), _t_ptr(p_im), self.n_dof, _np_ptr(tags), tags.shape[0], _t_ptr(out),
             _stream_ptr(stream)), "hbem_reduce_tag_avg", self.lib)
         return out
 
@@ -423,7 +426,7 @@ class ResidentSweep:
         n = self.n
         check(self.lib.hbem_assemble(
             self.s.handle, self.F, _np_ptr(self.k_re), _np_ptr(self.k_im), _t_ptr(self.q_re), _t_ptr(self.q_im),
-            self.q_re.stride(0), None, None, _t_ptr(self.A_re), _t_ptr(self.A_im), n, n * n, _t_ptr(self.b_re),
+            self.s.n_triangles, None, None, _t_ptr(self.A_re), _t_ptr(self.A_im), n, n * n, _t_ptr(self.b_re),
             _t_ptr(self.b_im), n, HBEM_ASM_CORRECTED, _stream_ptr(stream)), "hbem_assemble", self.lib)
 
     def factor_solve(self, stream=None):
@@ -440,7 +443,7 @@ class ResidentSweep:
         st = _stream_ptr(stream)
         check(self.lib.hbem_field(
             self.s.handle, self.F, _np_ptr(self.k_re), _t_ptr(self.x_re), _t_ptr(self.x_im), self.n,
-            _t_ptr(self.q_re), _t_ptr(self.q_im), self.q_re.stride(0), _t_ptr(self.obs), self.n_obs,
+            _t_ptr(self.q_re), _t_ptr(self.q_im), self.s.n_triangles, _t_ptr(self.obs), self.n_obs,
             _t_ptr(self.f_re), _t_ptr(self.f_im), self.n_obs, st), "hbem_field", self.lib)
         if self.tags.shape[0]:
             check(self.lib.hbem_reduce_tag_avg(
