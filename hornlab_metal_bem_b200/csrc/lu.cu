@@ -2,14 +2,17 @@
 // replacing LAPACK cgesv/cgetrf/cgetrs (reference main.swift:7834-7941,
 // 8015-8020).  Matrices are planar (re, im) float32, row-major.
 //
-// Right-looking blocked factorisation, one matrix per CTA column of the grid:
-//   1. k_panel        : factor the nb-wide panel (rows k0..n) with partial
-//                        pivoting (pivot = first max |re|+|im|, as LAPACK's
-//                        icamax); the panel is staged in shared memory when
-//                        n*nb*8 bytes fit, else worked in place in L2.
-//   2. k_swap_trsm    : apply the panel's row swaps to every other column and
-//                        solve L11 U12 = A12 for the columns right of it.
-//   3. trailing update: A22 -= L21 U12 (complex GEMM, K = nb).
+// Two-level right-looking blocked factorisation, batched over matrices:
+//   for each 64-column block b0:
+//     for each inner sub-panel c (32 or 16 columns):
+//       k_panel      : factor rows c..n of the sub-panel with partial pivoting
+//                      (pivot = first max |re|+|im|, as LAPACK's icamax),
+//                      staged in shared memory when it fits, else in L2;
+//       k_swap_trsm  : swap + forward-solve the other columns of the block;
+//       trailing     : update the block's remaining columns (K = 16/32);
+//     k_swap_trsm    : the block's 64 swaps on all other columns and the
+//                      64-row TRSM U12 = L11^-1 A12;
+//     trailing       : A22 -= L21 U12 with K = 64.
 // The solve applies the pivots then runs blocked forward / backward
 // substitution (op(A) = A, A^T or A^H).
 #include <cuda_runtime.h>
@@ -21,8 +24,9 @@
 
 namespace hbem {
 
-int launch_trailing_update(int n, int batch, int k0, int nb, float *a_re, float *a_im, long long lda,
-                           long long a_stride, int precision, cudaStream_t st);
+// A[start:n, start:col_end] -= A[start:n, k0:k0+kw] * A[k0:k0+kw, start:col_end]
+int launch_trailing_update(int n, int batch, int k0, int kw, int start, int col_end, float *a_re, float *a_im,
+                           long long lda, long long a_stride, int precision, cudaStream_t st);
 
 namespace {
 
@@ -147,28 +151,32 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(float *a_re, float *a_i
     if (threadIdx.x == 0 && first_zero && info[b] == 0) info[b] = first_zero;
 }
 
-// Row swaps for all non-panel columns + forward substitution with the unit
-// lower L11 for the columns right of the panel.  One thread per column.
-template <int NB>
-__global__ void __launch_bounds__(128) k_swap_trsm(float *a_re, float *a_im, long long lda, long long a_stride, int n,
-                                                   int k0, int nb, const int *piv, long long piv_stride) {
-    __shared__ float Lr[NB][NB + 1], Li[NB][NB + 1];
-    __shared__ int s_piv[NB];
+// Row swaps + forward substitution for a column range.  One thread per
+// column of [col_lo, col_hi) minus the panel [ex_lo, ex_lo + np): apply the
+// pivots of rows k0 .. k0+np-1 in order; columns >= trsm_lo then solve
+// L11 x = a with the unit-lower L11 = A[k0:k0+np, k0:k0+np] (np <= 64), in
+// 16-row register chunks whose updates of the remaining rows go through L2.
+__global__ void __launch_bounds__(128) k_swap_trsm(float *a_re, float *a_im, long long lda, long long a_stride,
+                                                   int k0, int np, int col_lo, int col_hi, int ex_lo,
+                                                   int trsm_lo, const int *piv, long long piv_stride) {
+    __shared__ float Lr[64][65], Li[64][65];
+    __shared__ int s_piv[64];
     const int b = blockIdx.y;
     float *are = a_re + (size_t)b * a_stride, *aim = a_im + (size_t)b * a_stride;
     const int *pv = piv + (size_t)b * piv_stride;
-    for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-        const int r = e / nb, c = e - r * nb;
-        Lr[r][c] = are[(size_t)(k0 + r) * lda + k0 + c];
-        Li[r][c] = aim[(size_t)(k0 + r) * lda + k0 + c];
-    }
-    for (int e = threadIdx.x; e < nb; e += blockDim.x) s_piv[e] = pv[k0 + e];
+    const bool any_trsm = trsm_lo < col_hi;
+    if (any_trsm)
+        for (int e = threadIdx.x; e < np * np; e += blockDim.x) {
+            const int r = e / np, c = e - r * np;
+            Lr[r][c] = are[(size_t)(k0 + r) * lda + k0 + c];
+            Li[r][c] = aim[(size_t)(k0 + r) * lda + k0 + c];
+        }
+    for (int e = threadIdx.x; e < np; e += blockDim.x) s_piv[e] = pv[k0 + e];
     __syncthreads();
-    int col = blockIdx.x * blockDim.x + threadIdx.x;
-    // skip over the panel columns
-    if (col >= k0) col += nb;
-    if (col >= n) return;
-    for (int j = 0; j < nb; ++j) {
+    int col = col_lo + blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ex_lo) col += np;
+    if (col >= col_hi) return;
+    for (int j = 0; j < np; ++j) {
         const int p = s_piv[j];
         if (p != k0 + j) {
             const size_t o1 = (size_t)(k0 + j) * lda + col, o2 = (size_t)p * lda + col;
@@ -179,33 +187,46 @@ __global__ void __launch_bounds__(128) k_swap_trsm(float *a_re, float *a_im, lon
             aim[o2] = ti;
         }
     }
-    if (col < k0) return;
-    float xr[NB], xi[NB];
+    if (col < trsm_lo) return;
+    for (int q0 = 0; q0 < np; q0 += 16) {
+        const int qn = min(16, np - q0);
+        float xr[16], xi[16];
 #pragma unroll
-    for (int i = 0; i < NB; ++i) {
-        if (i < nb) {
-            xr[i] = are[(size_t)(k0 + i) * lda + col];
-            xi[i] = aim[(size_t)(k0 + i) * lda + col];
-        }
-    }
-#pragma unroll
-    for (int i = 1; i < NB; ++i) {
-        if (i < nb) {
-            float sr = xr[i], si = xi[i];
-#pragma unroll
-            for (int j = 0; j < i; ++j) {
-                sr -= Lr[i][j] * xr[j] - Li[i][j] * xi[j];
-                si -= Lr[i][j] * xi[j] + Li[i][j] * xr[j];
+        for (int i = 0; i < 16; ++i)
+            if (i < qn) {
+                xr[i] = are[(size_t)(k0 + q0 + i) * lda + col];
+                xi[i] = aim[(size_t)(k0 + q0 + i) * lda + col];
             }
-            xr[i] = sr;
-            xi[i] = si;
-        }
-    }
 #pragma unroll
-    for (int i = 0; i < NB; ++i) {
-        if (i < nb) {
-            are[(size_t)(k0 + i) * lda + col] = xr[i];
-            aim[(size_t)(k0 + i) * lda + col] = xi[i];
+        for (int i = 1; i < 16; ++i)
+            if (i < qn) {
+                float sr = xr[i], si = xi[i];
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                    if (j < i) {
+                        sr -= Lr[q0 + i][q0 + j] * xr[j] - Li[q0 + i][q0 + j] * xi[j];
+                        si -= Lr[q0 + i][q0 + j] * xi[j] + Li[q0 + i][q0 + j] * xr[j];
+                    }
+                xr[i] = sr;
+                xi[i] = si;
+            }
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+            if (i < qn) {
+                are[(size_t)(k0 + q0 + i) * lda + col] = xr[i];
+                aim[(size_t)(k0 + q0 + i) * lda + col] = xi[i];
+            }
+        // rows below this chunk inside L11's range
+        for (int r = q0 + qn; r < np; ++r) {
+            float sr = are[(size_t)(k0 + r) * lda + col], si = aim[(size_t)(k0 + r) * lda + col];
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+                if (j < qn) {
+                    sr -= Lr[r][q0 + j] * xr[j] - Li[r][q0 + j] * xi[j];
+                    si -= Lr[r][q0 + j] * xi[j] + Li[r][q0 + j] * xr[j];
+                }
+            are[(size_t)(k0 + r) * lda + col] = sr;
+            aim[(size_t)(k0 + r) * lda + col] = si;
         }
     }
 }
@@ -467,29 +488,44 @@ __global__ void k_axpy_active(int n, float *x_re, float *x_im, long long x_strid
 
 int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long long a_stride, int *piv,
               long long piv_stride, int *info, int precision, cudaStream_t st) {
+    // Two-level blocking: 64-column blocks whose (n - b0) x 64 panel is
+    // factored by inner sub-panels (32 wide when the sub-panel fits shared
+    // memory, else 16) with updates confined to the block's columns; then one
+    // row-swap pass, a 64-row TRSM and a K = 64 trailing update per block.
     const size_t smem_cap = 200 * 1024;
-    int nb = 32;
-    if ((size_t)n * 32 * 8 > smem_cap && (size_t)n * 16 * 8 <= smem_cap) nb = 16;
+    constexpr int NB = 64;
     HBEM_CUDA(cudaMemsetAsync(info, 0, sizeof(int) * batch, st));
-    for (int k0 = 0; k0 < n; k0 += nb) {
-        const int w = std::min(nb, n - k0);
-        const size_t psmem = (size_t)(n - k0) * w * 8;
-        if (psmem <= smem_cap) {
-            HBEM_CUDA(cudaFuncSetAttribute(k_panel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
-            k_panel<true><<<batch, kPanelThreads, psmem, st>>>(a_re, a_im, lda, a_stride, n, k0, w, piv, piv_stride, info);
-        } else {
-            k_panel<false><<<batch, kPanelThreads, 0, st>>>(a_re, a_im, lda, a_stride, n, k0, w, piv, piv_stride, info);
+    HBEM_CUDA(cudaFuncSetAttribute(k_panel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+    for (int b0 = 0; b0 < n; b0 += NB) {
+        const int bw = std::min(NB, n - b0);
+        const int nbi = ((size_t)(n - b0) * 32 * 8 <= smem_cap) ? 32 : 16;
+        for (int c = b0; c < b0 + bw; c += nbi) {
+            const int w = std::min(nbi, b0 + bw - c);
+            const size_t psmem = (size_t)(n - c) * w * 8;
+            if (psmem <= smem_cap)
+                k_panel<true><<<batch, kPanelThreads, psmem, st>>>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info);
+            else
+                k_panel<false><<<batch, kPanelThreads, 0, st>>>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info);
+            HBEM_LAUNCH_CHECK("k_panel");
+            const int other = bw - w;  // block columns outside this sub-panel
+            if (other > 0) {
+                dim3 grid((other + 127) / 128, batch);
+                k_swap_trsm<<<grid, 128, 0, st>>>(a_re, a_im, lda, a_stride, c, w, b0, b0 + bw, c, c + w, piv, piv_stride);
+                HBEM_LAUNCH_CHECK("k_swap_trsm");
+            }
+            if (c + w < b0 + bw) {
+                int rc = launch_trailing_update(n, batch, c, w, c + w, b0 + bw, a_re, a_im, lda, a_stride, precision, st);
+                if (rc != HBEM_OK) return rc;
+            }
         }
-        HBEM_LAUNCH_CHECK("k_panel");
-        const int other = n - w;
-        if (other > 0) {
-            dim3 grid((other + 127) / 128, batch);
-            if (nb == 32) k_swap_trsm<32><<<grid, 128, 0, st>>>(a_re, a_im, lda, a_stride, n, k0, w, piv, piv_stride);
-            else k_swap_trsm<16><<<grid, 128, 0, st>>>(a_re, a_im, lda, a_stride, n, k0, w, piv, piv_stride);
+        const int outside = n - bw;
+        if (outside > 0) {
+            dim3 grid((outside + 127) / 128, batch);
+            k_swap_trsm<<<grid, 128, 0, st>>>(a_re, a_im, lda, a_stride, b0, bw, 0, n, b0, b0 + bw, piv, piv_stride);
             HBEM_LAUNCH_CHECK("k_swap_trsm");
         }
-        if (k0 + w < n) {
-            int rc = launch_trailing_update(n, batch, k0, w, a_re, a_im, lda, a_stride, precision, st);
+        if (b0 + bw < n) {
+            int rc = launch_trailing_update(n, batch, b0, bw, b0 + bw, n, a_re, a_im, lda, a_stride, precision, st);
             if (rc != HBEM_OK) return rc;
         }
     }
