@@ -61,172 +61,265 @@ __device__ void block_argmax(float &v, int &idx, float *s_v, int *s_i) {
     __syncthreads();
 }
 
-// Panel factorisation.  SMEM: panel rows k0..n-1 x nb columns staged in
-// shared memory (planar), written back at the end.
+// Panel factorisation of rows k0..n-1 x nb columns (nb <= 32).
+// SMEM: the panel is staged in shared memory with an odd row pitch (nb + 1),
+// so column reads across rows are bank-conflict free; otherwise it is worked
+// in place through L2.  Per column j, three barrier-separated phases:
+//   R (threads over rows)    : scale column j-1 by 1/pivot, local argmax of
+//                              |re| + |im| in column j (first index on ties);
+//   P (nb threads)           : pick the pivot, swap rows j <-> p, publish the
+//                              pivot row;
+//   E (threads over elements): A[r][c] -= (A[r][j] / pivot) * A[j][c], r, c > j.
 template <bool SMEM>
 __global__ void __launch_bounds__(kPanelThreads) k_panel(float *a_re, float *a_im, long long lda, long long a_stride,
                                                          int n, int k0, int nb, int *piv, long long piv_stride,
                                                          int *info) {
     extern __shared__ float s_panel[];
-    __shared__ float s_v[32];
-    __shared__ int s_i[32];
-    __shared__ float s_prow[2][64];
+    __shared__ float s_v[kPanelThreads / 32];
+    __shared__ int s_i[kPanelThreads / 32];
+    __shared__ float s_pr[32], s_pi[32];
     const int b = blockIdx.x;
-    float *are = a_re + (size_t)b * a_stride, *aim = a_im + (size_t)b * a_stride;
     int *pv = piv + (size_t)b * piv_stride;
     const int m = n - k0;  // panel rows
-    float *pre = s_panel, *pim = s_panel + (size_t)m * nb;
-    // element (row r in [0,m), col j in [0,nb)) of the panel
-    auto RE = [&](int r, int j) -> float & { return SMEM ? pre[(size_t)r * nb + j] : are[(size_t)(k0 + r) * lda + k0 + j]; };
-    auto IM = [&](int r, int j) -> float & { return SMEM ? pim[(size_t)r * nb + j] : aim[(size_t)(k0 + r) * lda + k0 + j]; };
+    // element (r, c) of the panel: smem pitch P, or global pitch lda
+    const int P = SMEM ? nb + 1 : (int)lda;
+    float *pre, *pim;
     if (SMEM) {
-        for (int e = threadIdx.x; e < m * nb; e += blockDim.x) {
+        pre = s_panel;
+        pim = s_panel + m * P;
+    } else {
+        pre = a_re + (size_t)b * a_stride + (size_t)k0 * lda + k0;
+        pim = a_im + (size_t)b * a_stride + (size_t)k0 * lda + k0;
+    }
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    if (SMEM) {
+        const float *gre = a_re + (size_t)b * a_stride + (size_t)k0 * lda + k0;
+        const float *gim = a_im + (size_t)b * a_stride + (size_t)k0 * lda + k0;
+        for (int e = tid; e < m * nb; e += blockDim.x) {
             const int r = e / nb, j = e - r * nb;
-            pre[e] = are[(size_t)(k0 + r) * lda + k0 + j];
-            pim[e] = aim[(size_t)(k0 + r) * lda + k0 + j];
+            pre[r * P + j] = gre[(size_t)r * lda + j];
+            pim[r * P + j] = gim[(size_t)r * lda + j];
         }
         __syncthreads();
     }
+    // element-phase mapping: LPR lanes per row, RPW rows per warp instruction
+    const int LPR = nb > 16 ? 32 : 16;
+    const int c_off = lane & (LPR - 1);
+    const int r_sub = lane / LPR;
+    const int r_step = nw * (32 / LPR);
     int first_zero = 0;
-    for (int j = 0; j < nb; ++j) {
+    float ir = 0.f, ii = 0.f;  // 1 / pivot of the previous column
+    for (int j = 0; j <= nb; ++j) {
+        // ---- phase R
         float v = -1.f;
         int idx = 0x7fffffff;
-        for (int r = j + threadIdx.x; r < m; r += blockDim.x) {
-            const float c = cabs1(RE(r, j), IM(r, j));
-            if (c > v) { v = c; idx = r; }
-        }
-        block_argmax(v, idx, s_v, s_i);
-        const int p = idx;
-        if (threadIdx.x == 0) pv[k0 + j] = k0 + p;
-        if (p != j) {
-            for (int c = threadIdx.x; c < nb; c += blockDim.x) {
-                const float tr = RE(j, c), ti = IM(j, c);
-                RE(j, c) = RE(p, c);
-                IM(j, c) = IM(p, c);
-                RE(p, c) = tr;
-                IM(p, c) = ti;
+        for (int r = j + tid; r < m; r += blockDim.x) {
+            const int o = r * P;
+            if (j > 0) {
+                const float xr = pre[o + j - 1], xi = pim[o + j - 1];
+                pre[o + j - 1] = xr * ir - xi * ii;
+                pim[o + j - 1] = xr * ii + xi * ir;
+            }
+            if (j < nb) {
+                const float c = cabs1(pre[o + j], pim[o + j]);
+                if (c > v) { v = c; idx = r; }
             }
         }
+        if (j == nb) break;
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ov = __shfl_xor_sync(0xffffffffu, v, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+            if (ov > v || (ov == v && oi < idx)) { v = ov; idx = oi; }
+        }
+        if (lane == 0) { s_v[warp] = v; s_i[warp] = idx; }
         __syncthreads();
-        const float dr = RE(j, j), di = IM(j, j);
-        const bool zero = (dr == 0.f && di == 0.f);
-        if (zero && first_zero == 0) first_zero = k0 + j + 1;
-        for (int c = threadIdx.x; c < nb; c += blockDim.x) {
-            s_prow[0][c] = RE(j, c);
-            s_prow[1][c] = IM(j, c);
+        // ---- phase P
+        if (tid < nb) {
+            float bv = s_v[0];
+            int p = s_i[0];
+            for (int w = 1; w < nw; ++w) {
+                const float ov = s_v[w];
+                const int oi = s_i[w];
+                if (ov > bv || (ov == bv && oi < p)) { bv = ov; p = oi; }
+            }
+            const int c = tid;
+            const float jr = pre[j * P + c], ji = pim[j * P + c];
+            const float pr = pre[p * P + c], pi = pim[p * P + c];
+            s_pr[c] = pr;
+            s_pi[c] = pi;
+            pre[j * P + c] = pr;
+            pim[j * P + c] = pi;
+            if (p != j) {
+                pre[p * P + c] = jr;
+                pim[p * P + c] = ji;
+            }
+            if (c == 0) pv[k0 + j] = k0 + p;
         }
         __syncthreads();
-        if (!zero) {
-            // 1 / pivot
+        const float dr = s_pr[j], di = s_pi[j];
+        const bool zero = (dr == 0.f && di == 0.f);
+        if (zero) {
+            if (first_zero == 0) first_zero = k0 + j + 1;
+            ir = 0.f;
+            ii = 0.f;
+        } else {
             const float den = 1.0f / (dr * dr + di * di);
-            const float ir = dr * den, ii = -di * den;
-            // scale column j below the diagonal and update the panel's trailing columns
-            const int cols = nb - j - 1;
-            const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-            for (int r = j + 1 + warp; r < m; r += nw) {
-                const float xr = RE(r, j), xi = IM(r, j);
+            ir = dr * den;
+            ii = -di * den;
+        }
+        // ---- phase E
+        const int c = j + 1 + c_off;
+        if (c < nb && !zero) {
+            const float ur = s_pr[c], ui = s_pi[c];
+            for (int r = j + 1 + warp * (32 / LPR) + r_sub; r < m; r += r_step) {
+                const int o = r * P;
+                const float xr = pre[o + j], xi = pim[o + j];
                 const float lr = xr * ir - xi * ii, li = xr * ii + xi * ir;
-                for (int c = lane; c < cols; c += 32) {
-                    const int cc = j + 1 + c;
-                    const float ur = s_prow[0][cc], ui = s_prow[1][cc];
-                    RE(r, cc) -= lr * ur - li * ui;
-                    IM(r, cc) -= lr * ui + li * ur;
-                }
-                __syncwarp();
-                if (lane == 0) {
-                    RE(r, j) = lr;
-                    IM(r, j) = li;
-                }
+                pre[o + c] -= lr * ur - li * ui;
+                pim[o + c] -= lr * ui + li * ur;
             }
         }
         __syncthreads();
     }
     if (SMEM) {
-        for (int e = threadIdx.x; e < m * nb; e += blockDim.x) {
+        float *gre = a_re + (size_t)b * a_stride + (size_t)k0 * lda + k0;
+        float *gim = a_im + (size_t)b * a_stride + (size_t)k0 * lda + k0;
+        for (int e = tid; e < m * nb; e += blockDim.x) {
             const int r = e / nb, j = e - r * nb;
-            are[(size_t)(k0 + r) * lda + k0 + j] = pre[e];
-            aim[(size_t)(k0 + r) * lda + k0 + j] = pim[e];
+            gre[(size_t)r * lda + j] = pre[r * P + j];
+            gim[(size_t)r * lda + j] = pim[r * P + j];
         }
     }
-    if (threadIdx.x == 0 && first_zero && info[b] == 0) info[b] = first_zero;
+    if (tid == 0 && first_zero && info[b] == 0) info[b] = first_zero;
 }
 
-// Row swaps + forward substitution for a column range.  One thread per
-// column of [col_lo, col_hi) minus the panel [ex_lo, ex_lo + np): apply the
-// pivots of rows k0 .. k0+np-1 in order; columns >= trsm_lo then solve
-// L11 x = a with the unit-lower L11 = A[k0:k0+np, k0:k0+np] (np <= 64), in
-// 16-row register chunks whose updates of the remaining rows go through L2.
-__global__ void __launch_bounds__(128) k_swap_trsm(float *a_re, float *a_im, long long lda, long long a_stride,
-                                                   int k0, int np, int col_lo, int col_hi, int ex_lo,
-                                                   int trsm_lo, const int *piv, long long piv_stride) {
-    __shared__ float Lr[64][65], Li[64][65];
-    __shared__ int s_piv[64];
+// Row swaps + forward substitution for a column range, staged in shared
+// memory.  A CTA owns up to kSwapCols consecutive columns of
+// [col_lo, col_hi) minus the panel [ex_lo, ex_lo + np).  The rows touched by
+// the pivots of rows k0 .. k0+np-1 (the np block rows and at most np distinct
+// rows below) are loaded once with coalesced reads, the swap sequence is
+// replayed in shared memory, columns >= trsm_lo are solved with the unit-lower
+// L11 = A[k0:k0+np, k0:k0+np] (np <= 64) in 16-row register chunks, and the
+// touched rows are written back.
+constexpr int kSwapCols = 64;
+constexpr int kSwapThreads = 256;
+constexpr size_t kSwapSmem = (size_t)(2 * 128 * (kSwapCols + 1) + 2 * 64 * 65) * sizeof(float);
+
+__global__ void __launch_bounds__(kSwapThreads) k_swap_trsm(float *a_re, float *a_im, long long lda,
+                                                            long long a_stride, int k0, int np, int col_lo,
+                                                            int col_hi, int ex_lo, int trsm_lo, const int *piv,
+                                                            long long piv_stride) {
+    extern __shared__ float s_dyn[];
+    constexpr int XP = kSwapCols + 1;
+    float *Xr = s_dyn, *Xi = Xr + 128 * XP;           // [slot][col]
+    float *Lr = Xi + 128 * XP, *Li = Lr + 64 * 65;     // [row][col] of L11
+    __shared__ int s_slot[64];   // smem slot holding the partner row of pivot j
+    __shared__ int s_row[128];   // global row of each slot (-1: unused)
+    __shared__ int s_col[kSwapCols];
     const int b = blockIdx.y;
     float *are = a_re + (size_t)b * a_stride, *aim = a_im + (size_t)b * a_stride;
     const int *pv = piv + (size_t)b * piv_stride;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int ncols_total = col_hi - col_lo - np;
+    const int c_first = blockIdx.x * kSwapCols;
+    const int ncols = min(kSwapCols, ncols_total - c_first);
+    if (tid < kSwapCols) {
+        int col = col_lo + c_first + tid;
+        if (col >= ex_lo) col += np;
+        s_col[tid] = tid < ncols ? col : -1;
+    }
+    if (tid < 128) s_row[tid] = tid < np ? k0 + tid : -1;
+    __syncthreads();
+    if (tid < np) {
+        const int p = pv[k0 + tid];
+        int slot;
+        if (p < k0 + np) {
+            slot = p - k0;
+        } else {
+            int first = tid;
+            for (int j = 0; j < tid; ++j)
+                if (pv[k0 + j] == p) { first = j; break; }
+            slot = np + first;
+            if (first == tid) s_row[slot] = p;
+        }
+        s_slot[tid] = slot;
+    }
     const bool any_trsm = trsm_lo < col_hi;
     if (any_trsm)
-        for (int e = threadIdx.x; e < np * np; e += blockDim.x) {
+        for (int e = tid; e < np * np; e += blockDim.x) {
             const int r = e / np, c = e - r * np;
-            Lr[r][c] = are[(size_t)(k0 + r) * lda + k0 + c];
-            Li[r][c] = aim[(size_t)(k0 + r) * lda + k0 + c];
+            Lr[r * 65 + c] = are[(size_t)(k0 + r) * lda + k0 + c];
+            Li[r * 65 + c] = aim[(size_t)(k0 + r) * lda + k0 + c];
         }
-    for (int e = threadIdx.x; e < np; e += blockDim.x) s_piv[e] = pv[k0 + e];
     __syncthreads();
-    int col = col_lo + blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= ex_lo) col += np;
-    if (col >= col_hi) return;
-    for (int j = 0; j < np; ++j) {
-        const int p = s_piv[j];
-        if (p != k0 + j) {
-            const size_t o1 = (size_t)(k0 + j) * lda + col, o2 = (size_t)p * lda + col;
-            const float tr = are[o1], ti = aim[o1];
-            are[o1] = are[o2];
-            aim[o1] = aim[o2];
-            are[o2] = tr;
-            aim[o2] = ti;
+    // load touched rows: warps over slots, lanes over columns
+    for (int sl = warp; sl < 128; sl += kSwapThreads / 32) {
+        const int row = s_row[sl];
+        if (row < 0) continue;
+        for (int c = lane; c < ncols; c += 32) {
+            Xr[sl * XP + c] = are[(size_t)row * lda + s_col[c]];
+            Xi[sl * XP + c] = aim[(size_t)row * lda + s_col[c]];
         }
     }
-    if (col < trsm_lo) return;
-    for (int q0 = 0; q0 < np; q0 += 16) {
-        const int qn = min(16, np - q0);
-        float xr[16], xi[16];
-#pragma unroll
-        for (int i = 0; i < 16; ++i)
-            if (i < qn) {
-                xr[i] = are[(size_t)(k0 + q0 + i) * lda + col];
-                xi[i] = aim[(size_t)(k0 + q0 + i) * lda + col];
+    __syncthreads();
+    if (tid < ncols) {
+        const int c = tid;
+        for (int j = 0; j < np; ++j) {
+            const int sl = s_slot[j];
+            if (sl != j) {
+                const float tr = Xr[j * XP + c], ti = Xi[j * XP + c];
+                Xr[j * XP + c] = Xr[sl * XP + c];
+                Xi[j * XP + c] = Xi[sl * XP + c];
+                Xr[sl * XP + c] = tr;
+                Xi[sl * XP + c] = ti;
             }
+        }
+        if (s_col[c] >= trsm_lo) {
+            for (int q0 = 0; q0 < np; q0 += 16) {
+                const int qn = min(16, np - q0);
+                float xr[16], xi[16];
 #pragma unroll
-        for (int i = 1; i < 16; ++i)
-            if (i < qn) {
-                float sr = xr[i], si = xi[i];
+                for (int i = 0; i < 16; ++i)
+                    if (i < qn) { xr[i] = Xr[(q0 + i) * XP + c]; xi[i] = Xi[(q0 + i) * XP + c]; }
 #pragma unroll
-                for (int j = 0; j < 16; ++j)
-                    if (j < i) {
-                        sr -= Lr[q0 + i][q0 + j] * xr[j] - Li[q0 + i][q0 + j] * xi[j];
-                        si -= Lr[q0 + i][q0 + j] * xi[j] + Li[q0 + i][q0 + j] * xr[j];
+                for (int i = 1; i < 16; ++i)
+                    if (i < qn) {
+                        float sr = xr[i], si = xi[i];
+#pragma unroll
+                        for (int j = 0; j < 16; ++j)
+                            if (j < i) {
+                                const float lr = Lr[(q0 + i) * 65 + q0 + j], li = Li[(q0 + i) * 65 + q0 + j];
+                                sr -= lr * xr[j] - li * xi[j];
+                                si -= lr * xi[j] + li * xr[j];
+                            }
+                        xr[i] = sr;
+                        xi[i] = si;
                     }
-                xr[i] = sr;
-                xi[i] = si;
-            }
 #pragma unroll
-        for (int i = 0; i < 16; ++i)
-            if (i < qn) {
-                are[(size_t)(k0 + q0 + i) * lda + col] = xr[i];
-                aim[(size_t)(k0 + q0 + i) * lda + col] = xi[i];
-            }
-        // rows below this chunk inside L11's range
-        for (int r = q0 + qn; r < np; ++r) {
-            float sr = are[(size_t)(k0 + r) * lda + col], si = aim[(size_t)(k0 + r) * lda + col];
+                for (int i = 0; i < 16; ++i)
+                    if (i < qn) { Xr[(q0 + i) * XP + c] = xr[i]; Xi[(q0 + i) * XP + c] = xi[i]; }
+                for (int r = q0 + qn; r < np; ++r) {
+                    float sr = Xr[r * XP + c], si = Xi[r * XP + c];
 #pragma unroll
-            for (int j = 0; j < 16; ++j)
-                if (j < qn) {
-                    sr -= Lr[r][q0 + j] * xr[j] - Li[r][q0 + j] * xi[j];
-                    si -= Lr[r][q0 + j] * xi[j] + Li[r][q0 + j] * xr[j];
+                    for (int j = 0; j < 16; ++j)
+                        if (j < qn) {
+                            const float lr = Lr[r * 65 + q0 + j], li = Li[r * 65 + q0 + j];
+                            sr -= lr * xr[j] - li * xi[j];
+                            si -= lr * xi[j] + li * xr[j];
+                        }
+                    Xr[r * XP + c] = sr;
+                    Xi[r * XP + c] = si;
                 }
-            are[(size_t)(k0 + r) * lda + col] = sr;
-            aim[(size_t)(k0 + r) * lda + col] = si;
+            }
+        }
+    }
+    __syncthreads();
+    for (int sl = warp; sl < 128; sl += kSwapThreads / 32) {
+        const int row = s_row[sl];
+        if (row < 0) continue;
+        for (int c = lane; c < ncols; c += 32) {
+            are[(size_t)row * lda + s_col[c]] = Xr[sl * XP + c];
+            aim[(size_t)row * lda + s_col[c]] = Xi[sl * XP + c];
         }
     }
 }
@@ -287,18 +380,18 @@ __global__ void __launch_bounds__(512) k_getrs(int n, const float *lu_re, const 
                 }
             }
             __syncthreads();
-            for (int i = j0 + jb + warp; i < n; i += nw) {
+            // rows below the block: one thread per row, independent loads
+            for (int i = j0 + jb + tid; i < n; i += blockDim.x) {
+                const float *lr_row = Ar + (size_t)i * lda + j0, *li_row = Ai + (size_t)i * lda + j0;
                 float pr = 0, pi = 0;
-                if (lane < jb) {
-                    const float lr = Ar[(size_t)i * lda + j0 + lane], li = Ai[(size_t)i * lda + j0 + lane];
-                    pr = lr * xr[j0 + lane] - li * xi[j0 + lane];
-                    pi = lr * xi[j0 + lane] + li * xr[j0 + lane];
+#pragma unroll 8
+                for (int c = 0; c < jb; ++c) {
+                    const float lr = lr_row[c], li = li_row[c];
+                    pr += lr * xr[j0 + c] - li * xi[j0 + c];
+                    pi += lr * xi[j0 + c] + li * xr[j0 + c];
                 }
-                for (int o = 16; o > 0; o >>= 1) {
-                    pr += __shfl_xor_sync(0xffffffffu, pr, o);
-                    pi += __shfl_xor_sync(0xffffffffu, pi, o);
-                }
-                if (lane == 0) { xr[i] -= pr; xi[i] -= pi; }
+                xr[i] -= pr;
+                xi[i] -= pi;
             }
             __syncthreads();
         }
@@ -328,18 +421,17 @@ __global__ void __launch_bounds__(512) k_getrs(int n, const float *lu_re, const 
                 }
             }
             __syncthreads();
-            for (int i = warp; i < j0; i += nw) {
+            for (int i = tid; i < j0; i += blockDim.x) {
+                const float *ur_row = Ar + (size_t)i * lda + j0, *ui_row = Ai + (size_t)i * lda + j0;
                 float pr = 0, pi = 0;
-                if (lane < jb) {
-                    const float ur = Ar[(size_t)i * lda + j0 + lane], ui = Ai[(size_t)i * lda + j0 + lane];
-                    pr = ur * xr[j0 + lane] - ui * xi[j0 + lane];
-                    pi = ur * xi[j0 + lane] + ui * xr[j0 + lane];
+#pragma unroll 8
+                for (int c = 0; c < jb; ++c) {
+                    const float ur = ur_row[c], ui = ui_row[c];
+                    pr += ur * xr[j0 + c] - ui * xi[j0 + c];
+                    pi += ur * xi[j0 + c] + ui * xr[j0 + c];
                 }
-                for (int o = 16; o > 0; o >>= 1) {
-                    pr += __shfl_xor_sync(0xffffffffu, pr, o);
-                    pi += __shfl_xor_sync(0xffffffffu, pi, o);
-                }
-                if (lane == 0) { xr[i] -= pr; xi[i] -= pi; }
+                xr[i] -= pr;
+                xi[i] -= pi;
             }
             __syncthreads();
         }
@@ -496,12 +588,13 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
     constexpr int NB = 64;
     HBEM_CUDA(cudaMemsetAsync(info, 0, sizeof(int) * batch, st));
     HBEM_CUDA(cudaFuncSetAttribute(k_panel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+    HBEM_CUDA(cudaFuncSetAttribute(k_swap_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSwapSmem));
     for (int b0 = 0; b0 < n; b0 += NB) {
         const int bw = std::min(NB, n - b0);
-        const int nbi = ((size_t)(n - b0) * 32 * 8 <= smem_cap) ? 32 : 16;
+        const int nbi = ((size_t)(n - b0) * 33 * 8 <= smem_cap) ? 32 : 16;
         for (int c = b0; c < b0 + bw; c += nbi) {
             const int w = std::min(nbi, b0 + bw - c);
-            const size_t psmem = (size_t)(n - c) * w * 8;
+            const size_t psmem = (size_t)(n - c) * (w + 1) * 8;
             if (psmem <= smem_cap)
                 k_panel<true><<<batch, kPanelThreads, psmem, st>>>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info);
             else
@@ -509,8 +602,9 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
             HBEM_LAUNCH_CHECK("k_panel");
             const int other = bw - w;  // block columns outside this sub-panel
             if (other > 0) {
-                dim3 grid((other + 127) / 128, batch);
-                k_swap_trsm<<<grid, 128, 0, st>>>(a_re, a_im, lda, a_stride, c, w, b0, b0 + bw, c, c + w, piv, piv_stride);
+                dim3 grid((other + kSwapCols - 1) / kSwapCols, batch);
+                k_swap_trsm<<<grid, kSwapThreads, kSwapSmem, st>>>(a_re, a_im, lda, a_stride, c, w, b0, b0 + bw, c,
+                                                                   c + w, piv, piv_stride);
                 HBEM_LAUNCH_CHECK("k_swap_trsm");
             }
             if (c + w < b0 + bw) {
@@ -520,8 +614,9 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
         }
         const int outside = n - bw;
         if (outside > 0) {
-            dim3 grid((outside + 127) / 128, batch);
-            k_swap_trsm<<<grid, 128, 0, st>>>(a_re, a_im, lda, a_stride, b0, bw, 0, n, b0, b0 + bw, piv, piv_stride);
+            dim3 grid((outside + kSwapCols - 1) / kSwapCols, batch);
+            k_swap_trsm<<<grid, kSwapThreads, kSwapSmem, st>>>(a_re, a_im, lda, a_stride, b0, bw, 0, n, b0, b0 + bw,
+                                                               piv, piv_stride);
             HBEM_LAUNCH_CHECK("k_swap_trsm");
         }
         if (b0 + bw < n) {
