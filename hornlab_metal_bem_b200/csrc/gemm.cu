@@ -6,9 +6,12 @@
 // complex outputs per thread, L and U tiles staged in shared memory with
 // 128-bit broadcast reads; FP32 FMA gives the exact-FP32 products of
 // LAPACK cgemm-based cgetrf.
+#include <cuda.h>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <string>
 
 #include "hbem_internal.h"
 
@@ -102,16 +105,340 @@ __global__ void __launch_bounds__(256) k_trailing_simt(float *a_re, float *a_im,
 
 }  // namespace
 
+int launch_trailing_tc(int n, int batch, int k0, int start, int col_end, float *a_re, float *a_im, long long lda,
+                       long long a_stride, int *status, cudaStream_t st);
+
 int launch_trailing_update(int n, int batch, int k0, int kw, int start, int col_end, float *a_re, float *a_im,
-                           long long lda, long long a_stride, int precision, cudaStream_t st) {
-    (void)precision;
+                           long long lda, long long a_stride, int precision, int *status, cudaStream_t st) {
     const int m = n - start, w = col_end - start;
     if (m <= 0 || w <= 0) return HBEM_OK;
     if (kw % 16) return fail(HBEM_ERR_ARG, "trailing update: K must be a multiple of 16");
+    if (precision == HBEM_PREC_MIXED && kw == 64 && status)
+        return launch_trailing_tc(n, batch, k0, start, col_end, a_re, a_im, lda, a_stride, status, st);
     dim3 grid((w + 63) / 64, (m + 63) / 64, batch);
     k_trailing_simt<<<grid, 256, 0, st>>>(a_re, a_im, lda, a_stride, n, k0, kw, start, col_end);
     HBEM_LAUNCH_CHECK("k_trailing_simt");
     return HBEM_OK;
+}
+
+}  // namespace hbem
+
+// ===========================================================================
+// Tensor-core trailing update (tcgen05, BF16x3 split products, FP32 TMEM
+// accumulation) for the mixed-precision LU.
+//
+// The complex update C -= L U is one real GEMM: for a tile of 64 complex rows
+// the 128 MMA rows are [Lr, -Li] (real part) and [Li, Lr] (imaginary part)
+// against B = [Ur; Ui].  Each FP32 operand x is split into hi = bf16(x) and
+// lo = bf16(x - hi); A B ~ Ah Bh + Ah Bl + Al Bh is a single K = 3 * 2 * 64
+// = 384 contraction over the packed operands A3 = [Ah | Ah | Al] and
+// B3^T = [Bh | Bl | Bh] (both K-major, written by k_pack_*).  TMA loads the
+// six 64-wide K-blocks of both operands (128-byte swizzle) into shared memory
+// up front; one thread issues 4 tcgen05.mma (K = 16) per block into a
+// 128 x 128 FP32 TMEM accumulator; the four warps read their 32 TMEM lanes
+// back with tcgen05.ld and subtract from C in global memory.
+// Every mbarrier wait is bounded; a timeout sets the status word and the CTA
+// returns after releasing its TMEM.
+// ===========================================================================
+namespace hbem {
+namespace {
+
+constexpr int kTcM = 128;          // MMA rows per CTA (64 complex rows)
+constexpr int kTcN = 128;          // columns per CTA
+constexpr int kTcKBlk = 64;        // bf16 elements per K-block (128 bytes)
+constexpr int kTcK3 = 384;         // 3 x 2 x 64
+constexpr int kTcStages = kTcK3 / kTcKBlk;
+constexpr int kTcStageBytes = (kTcM + kTcN) * kTcKBlk * 2;
+constexpr size_t kTcSmem = (size_t)kTcStages * kTcStageBytes + 1024 + 256;
+constexpr long long kSpinLimit = 1LL << 24;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (long long it = 0; it < kSpinLimit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// K-major, 128-byte swizzle UMMA shared-memory descriptor: rows of 128 bytes
+// in 8-row groups of 1024 bytes (stride byte offset 1024).
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);          // start address
+    d |= (uint64_t)1 << 16;                           // leading byte offset (unused for SW128 K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;                 // stride byte offset
+    d |= (uint64_t)1 << 46;                           // descriptor version (sm100)
+    d |= (uint64_t)2 << 61;                           // layout: SWIZZLE_128B
+    return d;
+}
+
+// kind::f16 instruction descriptor: BF16 A/B, FP32 accumulate, K-major A/B.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int m, int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+__global__ void __launch_bounds__(128, 1) k_trailing_tc(const __grid_constant__ CUtensorMap tmA,
+                                                         const __grid_constant__ CUtensorMap tmB, float *a_re,
+                                                         float *a_im, long long lda, long long a_stride, int n,
+                                                         int start, int col_end, int rows3, int cols_pad,
+                                                         int *status) {
+    extern __shared__ uint8_t s_raw[];
+    __shared__ uint64_t s_full[kTcStages];
+    __shared__ uint64_t s_done;
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_fail;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int mat = blockIdx.z;
+    const int tile_m = blockIdx.y, tile_n = blockIdx.x;
+    uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(s_raw) + 1023) & ~(uintptr_t)1023);
+    if (tid == 0) {
+        s_fail = 0;
+        for (int s = 0; s < kTcStages; ++s)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_full[s])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_done)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(kTcN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+
+    const int row_a = mat * rows3 + tile_m * kTcM;      // A3 row of this tile
+    const int row_b = mat * cols_pad + tile_n * kTcN;   // B3^T row of this tile
+    if (tid == 0) {
+        for (int s = 0; s < kTcStages; ++s) {
+            uint8_t *sa = base + (size_t)s * kTcStageBytes;
+            uint8_t *sb = sa + kTcM * kTcKBlk * 2;
+            const uint32_t bar = smem_u32(&s_full[s]);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kTcStageBytes)
+                         : "memory");
+            asm volatile(
+                "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                ::"r"(smem_u32(sa)), "l"(reinterpret_cast<uint64_t>(&tmA)), "r"(s * kTcKBlk), "r"(row_a), "r"(bar)
+                : "memory");
+            asm volatile(
+                "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                ::"r"(smem_u32(sb)), "l"(reinterpret_cast<uint64_t>(&tmB)), "r"(s * kTcKBlk), "r"(row_b), "r"(bar)
+                : "memory");
+        }
+        constexpr uint32_t idesc = umma_idesc_bf16(kTcM, kTcN);
+        bool ok = true;
+        for (int s = 0; s < kTcStages && ok; ++s) {
+            if (!mbar_wait(smem_u32(&s_full[s]), 0)) { ok = false; break; }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t sa = smem_u32(base + (size_t)s * kTcStageBytes);
+            const uint32_t sb = sa + kTcM * kTcKBlk * 2;
+#pragma unroll
+            for (int kk = 0; kk < kTcKBlk / 16; ++kk) {
+                const uint64_t da = umma_desc_sw128(sa + kk * 32);
+                const uint64_t db = umma_desc_sw128(sb + kk * 32);
+                const uint32_t acc = (s > 0 || kk > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                    ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc)
+                    : "memory");
+            }
+        }
+        if (ok) {
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&s_done))
+                         : "memory");
+        } else {
+            s_fail = 1;
+            atomicExch(status, 1);
+            // let outstanding TMA copies land before the CTA exits
+            for (int s = 0; s < kTcStages; ++s) mbar_wait(smem_u32(&s_full[s]), 0);
+        }
+    }
+    __syncthreads();
+    bool ok = s_fail == 0;
+    if (ok && !mbar_wait(smem_u32(&s_done), 0)) {
+        ok = false;
+        atomicExch(status, 2);
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok) {
+        // TMEM lane = MMA row: warp w owns lanes 32w .. 32w+31
+        const int rr = warp * 32 + lane;
+        const int crow = start + tile_m * 64 + (rr & 63);
+        float *dst = ((rr < 64) ? a_re : a_im) + (size_t)mat * a_stride + (size_t)crow * lda;
+        for (int c0 = 0; c0 < kTcN; c0 += 32) {
+            uint32_t v[32];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+                "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                  "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                  "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+                  "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (crow < n) {
+                const int gc0 = start + tile_n * kTcN + c0;
+#pragma unroll
+                for (int c = 0; c < 32; ++c)
+                    if (gc0 + c < col_end) dst[gc0 + c] -= __uint_as_float(v[c]);
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcN));
+}
+
+// Pack L21 (rows start..n, cols k0..k0+64) into A3 (K-major, bf16 hi/lo).
+__global__ void k_pack_a(const float *a_re, const float *a_im, long long lda, long long a_stride, int n, int start,
+                         int k0, int rows3, __nv_bfloat16 *A3) {
+    const int mat = blockIdx.z;
+    const int i = blockIdx.x * blockDim.y + threadIdx.y;  // complex row offset
+    const int k = threadIdx.x;                            // 0..63
+    const int m = n - start;
+    const int rows_alloc = rows3 / 2;                     // complex rows incl. padding
+    if (i >= rows_alloc) return;
+    float lr = 0.f, li = 0.f;
+    if (i < m) {
+        lr = a_re[(size_t)mat * a_stride + (size_t)(start + i) * lda + k0 + k];
+        li = a_im[(size_t)mat * a_stride + (size_t)(start + i) * lda + k0 + k];
+    }
+    const int t = i >> 6, rl = i & 63;
+    __nv_bfloat16 *re_row = A3 + ((size_t)mat * rows3 + (size_t)t * 128 + rl) * kTcK3;
+    __nv_bfloat16 *im_row = re_row + (size_t)64 * kTcK3;
+    auto put = [](__nv_bfloat16 *row, int k2, float x) {
+        const __nv_bfloat16 h = __float2bfloat16_rn(x);
+        const __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
+        row[k2] = h;
+        row[128 + k2] = h;
+        row[256 + k2] = l;
+    };
+    put(re_row, k, lr);
+    put(re_row, 64 + k, -li);
+    put(im_row, k, li);
+    put(im_row, 64 + k, lr);
+}
+
+// Pack U12 (rows k0..k0+64, cols start..col_end) into B3^T (K-major).
+__global__ void k_pack_b(const float *a_re, const float *a_im, long long lda, long long a_stride, int start,
+                         int col_end, int k0, int cols_pad, __nv_bfloat16 *B3) {
+    const int mat = blockIdx.z;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;  // column offset
+    const int k = blockIdx.y;                             // 0..63
+    if (j >= cols_pad) return;
+    float ur = 0.f, ui = 0.f;
+    if (start + j < col_end) {
+        ur = a_re[(size_t)mat * a_stride + (size_t)(k0 + k) * lda + start + j];
+        ui = a_im[(size_t)mat * a_stride + (size_t)(k0 + k) * lda + start + j];
+    }
+    __nv_bfloat16 *row = B3 + ((size_t)mat * cols_pad + j) * kTcK3;
+    auto put = [&](int k2, float x) {
+        const __nv_bfloat16 h = __float2bfloat16_rn(x);
+        const __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
+        row[k2] = h;
+        row[128 + k2] = l;
+        row[256 + k2] = h;
+    };
+    put(k, ur);
+    put(64 + k, ui);
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+int make_map(CUtensorMap *map, void *ptr, long long rows, int box_rows) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return fail(HBEM_ERR_CUDA, "cuTensorMapEncodeTiled entry point unavailable");
+    const cuuint64_t dims[2] = {(cuuint64_t)kTcK3, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)kTcK3 * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)kTcKBlk, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, ptr, dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(HBEM_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+    return HBEM_OK;
+}
+
+}  // namespace
+
+// Mixed-precision trailing update with K = 64 (one LU block).  Workspace is
+// allocated on the stream; status receives 1/2 if a barrier wait timed out.
+int launch_trailing_tc(int n, int batch, int k0, int start, int col_end, float *a_re, float *a_im, long long lda,
+                       long long a_stride, int *status, cudaStream_t st) {
+    const int m = n - start, w = col_end - start;
+    if (m <= 0 || w <= 0) return HBEM_OK;
+    const int tiles_m = (m + 63) / 64, tiles_n = (w + kTcN - 1) / kTcN;
+    const int rows3 = tiles_m * kTcM, cols_pad = tiles_n * kTcN;
+    __nv_bfloat16 *A3 = nullptr, *B3 = nullptr;
+    const size_t bytes_a = (size_t)batch * rows3 * kTcK3 * 2, bytes_b = (size_t)batch * cols_pad * kTcK3 * 2;
+    HBEM_CUDA(cudaMallocAsync((void **)&A3, bytes_a, st));
+    HBEM_CUDA(cudaMallocAsync((void **)&B3, bytes_b, st));
+    int rc = HBEM_OK;
+    {
+        dim3 blk(64, 4), grd((rows3 / 2 + 3) / 4, 1, batch);
+        k_pack_a<<<grd, blk, 0, st>>>(a_re, a_im, lda, a_stride, n, start, k0, rows3, A3);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = cuda_fail(e, "k_pack_a");
+        else count_launch();
+    }
+    if (rc == HBEM_OK) {
+        dim3 grd((cols_pad + 127) / 128, 64, batch);
+        k_pack_b<<<grd, 128, 0, st>>>(a_re, a_im, lda, a_stride, start, col_end, k0, cols_pad, B3);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = cuda_fail(e, "k_pack_b");
+        else count_launch();
+    }
+    CUtensorMap ma, mb;
+    if (rc == HBEM_OK) rc = make_map(&ma, A3, (long long)batch * rows3, kTcM);
+    if (rc == HBEM_OK) rc = make_map(&mb, B3, (long long)batch * cols_pad, kTcN);
+    if (rc == HBEM_OK) {
+        cudaError_t e = cudaFuncSetAttribute(k_trailing_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+        if (e == cudaSuccess) {
+            dim3 grd(tiles_n, tiles_m, batch);
+            k_trailing_tc<<<grd, 128, kTcSmem, st>>>(ma, mb, a_re, a_im, lda, a_stride, n, start, col_end, rows3,
+                                                    cols_pad, status);
+            e = cudaGetLastError();
+        }
+        if (e != cudaSuccess) rc = cuda_fail(e, "k_trailing_tc");
+        else count_launch();
+    }
+    cudaFreeAsync(A3, st);
+    cudaFreeAsync(B3, st);
+    return rc;
 }
 
 }  // namespace hbem

@@ -19,6 +19,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <string>
 
 #include "hbem_internal.h"
 
@@ -26,7 +27,7 @@ namespace hbem {
 
 // A[start:n, start:col_end] -= A[start:n, k0:k0+kw] * A[k0:k0+kw, start:col_end]
 int launch_trailing_update(int n, int batch, int k0, int kw, int start, int col_end, float *a_re, float *a_im,
-                           long long lda, long long a_stride, int precision, cudaStream_t st);
+                           long long lda, long long a_stride, int precision, int *status, cudaStream_t st);
 
 namespace {
 
@@ -587,6 +588,27 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
     const size_t smem_cap = 200 * 1024;
     constexpr int NB = 64;
     HBEM_CUDA(cudaMemsetAsync(info, 0, sizeof(int) * batch, st));
+    // mixed precision: K = 64 block updates run on the tensor cores; their
+    // barrier waits report through this status word
+    int *status = nullptr;
+    if (precision == HBEM_PREC_MIXED) {
+        HBEM_CUDA(cudaMallocAsync((void **)&status, sizeof(int), st));
+        HBEM_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
+    }
+    auto finish = [&](int rc) -> int {
+        if (status) {
+            int h = 0;
+            if (rc == HBEM_OK) {
+                cudaError_t e = cudaMemcpyAsync(&h, status, sizeof(int), cudaMemcpyDeviceToHost, st);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+                if (e != cudaSuccess) rc = cuda_fail(e, "lu status");
+            }
+            cudaFreeAsync(status, st);
+            if (rc == HBEM_OK && h != 0)
+                rc = fail(HBEM_ERR_STATE, "tensor-core trailing update: barrier wait timed out (status " + std::to_string(h) + ")");
+        }
+        return rc;
+    };
     HBEM_CUDA(cudaFuncSetAttribute(k_panel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
     HBEM_CUDA(cudaFuncSetAttribute(k_swap_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSwapSmem));
     for (int b0 = 0; b0 < n; b0 += NB) {
@@ -608,8 +630,9 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
                 HBEM_LAUNCH_CHECK("k_swap_trsm");
             }
             if (c + w < b0 + bw) {
-                int rc = launch_trailing_update(n, batch, c, w, c + w, b0 + bw, a_re, a_im, lda, a_stride, precision, st);
-                if (rc != HBEM_OK) return rc;
+                int rc = launch_trailing_update(n, batch, c, w, c + w, b0 + bw, a_re, a_im, lda, a_stride, precision,
+                                                nullptr, st);
+                if (rc != HBEM_OK) return finish(rc);
             }
         }
         const int outside = n - bw;
@@ -620,11 +643,12 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
             HBEM_LAUNCH_CHECK("k_swap_trsm");
         }
         if (b0 + bw < n) {
-            int rc = launch_trailing_update(n, batch, b0, bw, b0 + bw, n, a_re, a_im, lda, a_stride, precision, st);
-            if (rc != HBEM_OK) return rc;
+            int rc = launch_trailing_update(n, batch, b0, bw, b0 + bw, n, a_re, a_im, lda, a_stride, precision, status,
+                                            st);
+            if (rc != HBEM_OK) return finish(rc);
         }
     }
-    return HBEM_OK;
+    return finish(HBEM_OK);
 }
 
 int lu_solve(int n, int nrhs, int batch, const float *lu_re, const float *lu_im, long long lda, long long a_stride,

@@ -248,3 +248,40 @@ def test_tag_average_matches_oracle():
         for j, tag in enumerate([1, 2, 99]):
             want = o.tag_average(p[f], tag)
             assert abs(complex(out[f, j, 0], out[f, j, 1]) - want) <= 1e-12 + 1e-9 * abs(want)
+
+
+def _refine(A0r, A0i, LUr, LUi, piv, Br, Bi, Xr, Xi, n, batch, tol, max_iter):
+    import ctypes
+
+    lib = load_library()
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    iters = torch.zeros(batch, dtype=torch.int32, device="cuda")
+    resid = torch.zeros(batch, dtype=torch.float64, device="cuda")
+    P = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    rc = lib.hbem_refine(n, batch, P(A0r), P(A0i), n, n * n, P(LUr), P(LUi), n * n, P(piv), n, P(Br), P(Bi), n,
+                         P(Xr), P(Xi), n, tol, max_iter, P(iters), P(resid), st)
+    assert rc == 0
+    return iters.cpu().numpy(), resid.cpu().numpy()
+
+
+@pytest.mark.parametrize("n", [130, 700])
+def test_mixed_precision_lu_with_refinement(n):
+    """BF16x3 tensor-core trailing updates, then FP64-residual refinement to 1e-6."""
+    batch = 2
+    A, b = _lu_case(n, batch, 100 + n)
+    A0r, A0i = _dev(A)
+    LUr, LUi = A0r.clone(), A0i.clone()
+    piv, info = _factor(LUr, LUi, n, batch, precision=1)
+    assert int(info.abs().sum()) == 0
+    Xr, Xi = _dev(b[:, :, None])
+    _solve(LUr, LUi, piv, Xr, Xi, n, 1, batch)
+    x0 = _host(Xr, Xi)[:, :, 0]
+    Br, Bi = _dev(b)
+    Xr2, Xi2 = Xr[:, :, 0].contiguous(), Xi[:, :, 0].contiguous()
+    iters, resid = _refine(A0r, A0i, LUr, LUi, piv, Br, Bi, Xr2, Xi2, n, batch, 1e-6, 10)
+    x = _host(Xr2, Xi2)
+    for m in range(batch):
+        ref = np.linalg.solve(A[m].astype(np.complex128), b[m].astype(np.complex128))
+        assert rel(x0[m], ref) < 1e-3          # unrefined BF16x3 factors
+        assert resid[m] <= 1e-6
+        assert rel(x[m], ref) < 1e-5           # refined
