@@ -430,6 +430,12 @@ struct DuffyArgs {
     long long q_stride, lda, a_stride, b_stride;
     int V, T, n_pairs;
     int rule_off[3], rule_cnt[3];
+    // coupled-baffle projections: ap_local[t] = aperture index or -1.
+    // mode 0: A/b (when a_re) and S_ia (when sia); mode 1: S_aa only.
+    const int *ap_local;
+    float *sia_re, *sia_im, *saa_re, *saa_im;
+    long long sia_stride, saa_stride;
+    int m_ap, mode;
     float k[kMaxFreqPerLaunch];
     float kt[kMaxFreqPerLaunch];
     float ki[kMaxFreqPerLaunch];
@@ -466,6 +472,10 @@ __global__ void __launch_bounds__(256) k_duffy(const __grid_constant__ DuffyArgs
     const int f = blockIdx.y;
     const DuffyPair pr = p.pairs[pi];
     const int V = p.V, T = p.T;
+    // pairs without an aperture trial (and, for S_aa, an unmirrored aperture
+    // test) contribute nothing to the projection-only passes
+    if (p.mode == 1 && (pr.test_mask != 0 || p.ap_local[pr.test] < 0 || p.ap_local[pr.trial] < 0)) return;
+    if (p.mode == 0 && !p.a_re && (!p.ap_local || p.ap_local[pr.trial] < 0)) return;
     float P[3][3], S[3][3];
 #pragma unroll
     for (int l = 0; l < 3; ++l) {
@@ -556,6 +566,27 @@ __global__ void __launch_bounds__(256) k_duffy(const __grid_constant__ DuffyArgs
     for (int i = 0; i < 3; ++i)
         if (i_row == i) { sr = acc[2 * i]; si = acc[2 * i + 1]; }
     sr *= scale; si *= scale; dr *= scale; di *= scale;
+    if (p.mode == 1) {
+        // S_aa: sum_i delta_slp_i / area(test), one contribution per unmirrored pair
+        if (lane == 0) {
+            const double s_re = (acc[0] + acc[2] + acc[4]) * (double)HBEM_INV4PI * (double)jac;
+            const double s_im = (acc[1] + acc[3] + acc[5]) * (double)HBEM_INV4PI * (double)jac;
+            const double inv = 1.0 / fmax((double)p.areas[pr.test], 1e-38);
+            const size_t o = (size_t)f * p.saa_stride + (size_t)p.ap_local[pr.test] * p.m_ap + p.ap_local[pr.trial];
+            atomicAdd(p.saa_re + o, (float)(s_re * inv));
+            atomicAdd(p.saa_im + o, (float)(s_im * inv));
+        }
+        return;
+    }
+    if (p.sia_re && lane >= 9 && lane < 12) {
+        const int t = p.ap_local[pr.trial];
+        if (t >= 0) {
+            const size_t o = (size_t)f * p.sia_stride + (size_t)p.l2g[pr.test * 3 + i_row] * p.m_ap + t;
+            atomicAdd(p.sia_re + o, (float)sr);
+            atomicAdd(p.sia_im + o, (float)si);
+        }
+    }
+    if (!p.a_re) return;
     const float br = p.beta_re ? p.beta_re[pr.trial] : 0.f, bi = p.beta_im ? p.beta_im[pr.trial] : 0.f;
     if (lane < 9) {
         const int j = lane - 3 * (lane / 3);
@@ -643,7 +674,8 @@ int launch_regular(Session &s, int n_freq, const float *k_re, const float *k_im,
 
 int launch_duffy(Session &s, int n_freq, const float *k_re, const float *k_im, const float *q_re, const float *q_im,
                  long long q_stride, const float *beta_re, const float *beta_im, float *a_re, float *a_im,
-                 long long lda, long long a_stride, float *b_re, float *b_im, long long b_stride, cudaStream_t st) {
+                 long long lda, long long a_stride, float *b_re, float *b_im, long long b_stride, cudaStream_t st,
+                 const ApertureOut *ap) {
     if (s.n_pairs == 0) return HBEM_OK;
     for (int f0 = 0; f0 < n_freq; f0 += kMaxFreqPerLaunch) {
         const int nf = std::min(kMaxFreqPerLaunch, n_freq - f0);
@@ -660,6 +692,17 @@ int launch_duffy(Session &s, int n_freq, const float *k_re, const float *k_im, c
         a.V = s.n_vertices; a.T = s.n_triangles; a.n_pairs = s.n_pairs;
         for (int r = 0; r < 3; ++r) { a.rule_off[r] = s.rule_off[r]; a.rule_cnt[r] = s.rule_cnt[r]; }
         fill_k(a.k, a.kt, a.ki, k_re + f0, k_im ? k_im + f0 : nullptr, nf);
+        if (ap) {
+            a.ap_local = s.d_ap_local;
+            a.m_ap = s.m_ap;
+            a.mode = ap->mode;
+            a.sia_re = ap->sia_re ? ap->sia_re + (size_t)f0 * ap->sia_stride : nullptr;
+            a.sia_im = ap->sia_im ? ap->sia_im + (size_t)f0 * ap->sia_stride : nullptr;
+            a.saa_re = ap->saa_re ? ap->saa_re + (size_t)f0 * ap->saa_stride : nullptr;
+            a.saa_im = ap->saa_im ? ap->saa_im + (size_t)f0 * ap->saa_stride : nullptr;
+            a.sia_stride = ap->sia_stride;
+            a.saa_stride = ap->saa_stride;
+        }
         bool ck = false;
         for (int f = 0; f < nf; ++f) ck |= a.ki[f] != 0.f;
         dim3 grid((s.n_pairs + 7) / 8, nf);
@@ -717,6 +760,6 @@ extern "C" int hbem_assemble(hbem_session *h, int n_freq, const float *k_re, con
                             b_re, b_im, b_stride, st);
     if (rc == HBEM_OK && (flags & HBEM_ASM_DUFFY))
         rc = launch_duffy(*s, n_freq, k_re, k_im, q_re, q_im, q_stride, beta_re, beta_im, a_re, a_im, lda, a_stride,
-                          b_re, b_im, b_stride, st);
+                          b_re, b_im, b_stride, st, nullptr);
     return rc;
 }

@@ -16,6 +16,7 @@
 #include "hbem_internal.h"
 
 namespace hbem {
+struct TcWorkspace;
 namespace {
 
 // C[start:n, start:col_end] -= L[start:n, k0:k0+kw] * U[k0:k0+kw, start:col_end]
@@ -105,16 +106,16 @@ __global__ void __launch_bounds__(256) k_trailing_simt(float *a_re, float *a_im,
 
 }  // namespace
 
-int launch_trailing_tc(int n, int batch, int k0, int start, int col_end, float *a_re, float *a_im, long long lda,
-                       long long a_stride, int *status, cudaStream_t st);
+int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int col_end, float *a_re, float *a_im,
+                       long long lda, long long a_stride, int *status, cudaStream_t st);
 
 int launch_trailing_update(int n, int batch, int k0, int kw, int start, int col_end, float *a_re, float *a_im,
-                           long long lda, long long a_stride, int precision, int *status, cudaStream_t st) {
+                           long long lda, long long a_stride, TcWorkspace *tc, int *status, cudaStream_t st) {
     const int m = n - start, w = col_end - start;
     if (m <= 0 || w <= 0) return HBEM_OK;
     if (kw % 16) return fail(HBEM_ERR_ARG, "trailing update: K must be a multiple of 16");
-    if (precision == HBEM_PREC_MIXED && kw == 64 && status)
-        return launch_trailing_tc(n, batch, k0, start, col_end, a_re, a_im, lda, a_stride, status, st);
+    if (tc && kw == 64 && status)
+        return launch_trailing_tc(tc, n, batch, k0, start, col_end, a_re, a_im, lda, a_stride, status, st);
     dim3 grid((w + 63) / 64, (m + 63) / 64, batch);
     k_trailing_simt<<<grid, 256, 0, st>>>(a_re, a_im, lda, a_stride, n, k0, kw, start, col_end);
     HBEM_LAUNCH_CHECK("k_trailing_simt");
@@ -309,13 +310,12 @@ __global__ void __launch_bounds__(128, 1) k_trailing_tc(const __grid_constant__ 
 
 // Pack L21 (rows start..n, cols k0..k0+64) into A3 (K-major, bf16 hi/lo).
 __global__ void k_pack_a(const float *a_re, const float *a_im, long long lda, long long a_stride, int n, int start,
-                         int k0, int rows3, __nv_bfloat16 *A3) {
+                         int k0, int rows3, int rows_used, __nv_bfloat16 *A3) {
     const int mat = blockIdx.z;
     const int i = blockIdx.x * blockDim.y + threadIdx.y;  // complex row offset
     const int k = threadIdx.x;                            // 0..63
     const int m = n - start;
-    const int rows_alloc = rows3 / 2;                     // complex rows incl. padding
-    if (i >= rows_alloc) return;
+    if (i >= rows_used) return;                           // complex rows incl. tile padding
     float lr = 0.f, li = 0.f;
     if (i < m) {
         lr = a_re[(size_t)mat * a_stride + (size_t)(start + i) * lda + k0 + k];
@@ -339,11 +339,11 @@ __global__ void k_pack_a(const float *a_re, const float *a_im, long long lda, lo
 
 // Pack U12 (rows k0..k0+64, cols start..col_end) into B3^T (K-major).
 __global__ void k_pack_b(const float *a_re, const float *a_im, long long lda, long long a_stride, int start,
-                         int col_end, int k0, int cols_pad, __nv_bfloat16 *B3) {
+                         int col_end, int k0, int cols_pad, int cols_used, __nv_bfloat16 *B3) {
     const int mat = blockIdx.z;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;  // column offset
     const int k = blockIdx.y;                             // 0..63
-    if (j >= cols_pad) return;
+    if (j >= cols_used) return;
     float ur = 0.f, ui = 0.f;
     if (start + j < col_end) {
         ur = a_re[(size_t)mat * a_stride + (size_t)(k0 + k) * lda + start + j];
@@ -395,50 +395,70 @@ int make_map(CUtensorMap *map, void *ptr, long long rows, int box_rows) {
 
 }  // namespace
 
-// Mixed-precision trailing update with K = 64 (one LU block).  Workspace is
-// allocated on the stream; status receives 1/2 if a barrier wait timed out.
-int launch_trailing_tc(int n, int batch, int k0, int start, int col_end, float *a_re, float *a_im, long long lda,
-                       long long a_stride, int *status, cudaStream_t st) {
-    const int m = n - start, w = col_end - start;
-    if (m <= 0 || w <= 0) return HBEM_OK;
-    const int tiles_m = (m + 63) / 64, tiles_n = (w + kTcN - 1) / kTcN;
-    const int rows3 = tiles_m * kTcM, cols_pad = tiles_n * kTcN;
+// Packed-operand workspace and tensor maps for one factorisation: sized for
+// the first (largest) trailing update and reused by the later, smaller ones.
+struct TcWorkspace {
     __nv_bfloat16 *A3 = nullptr, *B3 = nullptr;
-    const size_t bytes_a = (size_t)batch * rows3 * kTcK3 * 2, bytes_b = (size_t)batch * cols_pad * kTcK3 * 2;
-    HBEM_CUDA(cudaMallocAsync((void **)&A3, bytes_a, st));
-    HBEM_CUDA(cudaMallocAsync((void **)&B3, bytes_b, st));
-    int rc = HBEM_OK;
-    {
-        dim3 blk(64, 4), grd((rows3 / 2 + 3) / 4, 1, batch);
-        k_pack_a<<<grd, blk, 0, st>>>(a_re, a_im, lda, a_stride, n, start, k0, rows3, A3);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) rc = cuda_fail(e, "k_pack_a");
-        else count_launch();
-    }
-    if (rc == HBEM_OK) {
-        dim3 grd((cols_pad + 127) / 128, 64, batch);
-        k_pack_b<<<grd, 128, 0, st>>>(a_re, a_im, lda, a_stride, start, col_end, k0, cols_pad, B3);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) rc = cuda_fail(e, "k_pack_b");
-        else count_launch();
-    }
+    int rows3 = 0, cols_pad = 0, batch = 0;
     CUtensorMap ma, mb;
-    if (rc == HBEM_OK) rc = make_map(&ma, A3, (long long)batch * rows3, kTcM);
-    if (rc == HBEM_OK) rc = make_map(&mb, B3, (long long)batch * cols_pad, kTcN);
-    if (rc == HBEM_OK) {
-        cudaError_t e = cudaFuncSetAttribute(k_trailing_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
-        if (e == cudaSuccess) {
-            dim3 grd(tiles_n, tiles_m, batch);
-            k_trailing_tc<<<grd, 128, kTcSmem, st>>>(ma, mb, a_re, a_im, lda, a_stride, n, start, col_end, rows3,
-                                                    cols_pad, status);
-            e = cudaGetLastError();
-        }
-        if (e != cudaSuccess) rc = cuda_fail(e, "k_trailing_tc");
-        else count_launch();
+};
+
+int tc_workspace_create(int n, int batch, TcWorkspace **out, cudaStream_t st) {
+    *out = nullptr;
+    auto *w = new TcWorkspace();
+    w->rows3 = ((n + 63) / 64) * kTcM;
+    w->cols_pad = ((n + kTcN - 1) / kTcN) * kTcN;
+    w->batch = batch;
+    cudaError_t e = cudaMallocAsync((void **)&w->A3, (size_t)batch * w->rows3 * kTcK3 * 2, st);
+    if (e == cudaSuccess) e = cudaMallocAsync((void **)&w->B3, (size_t)batch * w->cols_pad * kTcK3 * 2, st);
+    if (e != cudaSuccess) {
+        if (w->A3) cudaFreeAsync(w->A3, st);
+        delete w;
+        return cuda_fail(e, "tensor-core workspace");
     }
-    cudaFreeAsync(A3, st);
-    cudaFreeAsync(B3, st);
-    return rc;
+    int rc = make_map(&w->ma, w->A3, (long long)batch * w->rows3, kTcM);
+    if (rc == HBEM_OK) rc = make_map(&w->mb, w->B3, (long long)batch * w->cols_pad, kTcN);
+    if (rc != HBEM_OK) {
+        cudaFreeAsync(w->A3, st);
+        cudaFreeAsync(w->B3, st);
+        delete w;
+        return rc;
+    }
+    *out = w;
+    return HBEM_OK;
+}
+
+void tc_workspace_destroy(TcWorkspace *w, cudaStream_t st) {
+    if (!w) return;
+    cudaFreeAsync(w->A3, st);
+    cudaFreeAsync(w->B3, st);
+    delete w;
+}
+
+// Mixed-precision trailing update with K = 64 (one LU block); status
+// receives 1/2 if a barrier wait timed out.
+int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int col_end, float *a_re, float *a_im,
+                       long long lda, long long a_stride, int *status, cudaStream_t st) {
+    const int m = n - start, wd = col_end - start;
+    if (m <= 0 || wd <= 0) return HBEM_OK;
+    const int tiles_m = (m + 63) / 64, tiles_n = (wd + kTcN - 1) / kTcN;
+    // packed rows use the workspace's fixed per-matrix pitch (rows3 / cols_pad)
+    {
+        dim3 blk(64, 4), grd((tiles_m * 64 + 3) / 4, 1, batch);
+        k_pack_a<<<grd, blk, 0, st>>>(a_re, a_im, lda, a_stride, n, start, k0, w->rows3, tiles_m * 64, w->A3);
+        HBEM_LAUNCH_CHECK("k_pack_a");
+    }
+    {
+        dim3 grd((tiles_n * kTcN + 127) / 128, 64, batch);
+        k_pack_b<<<grd, 128, 0, st>>>(a_re, a_im, lda, a_stride, start, col_end, k0, w->cols_pad, tiles_n * kTcN, w->B3);
+        HBEM_LAUNCH_CHECK("k_pack_b");
+    }
+    HBEM_CUDA(cudaFuncSetAttribute(k_trailing_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+    dim3 grd(tiles_n, tiles_m, batch);
+    k_trailing_tc<<<grd, 128, kTcSmem, st>>>(w->ma, w->mb, a_re, a_im, lda, a_stride, n, start, col_end, w->rows3,
+                                            w->cols_pad, status);
+    HBEM_LAUNCH_CHECK("k_trailing_tc");
+    return HBEM_OK;
 }
 
 }  // namespace hbem

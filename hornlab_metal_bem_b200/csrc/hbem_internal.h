@@ -90,6 +90,13 @@ struct Session {
 
     int *d_status = nullptr;        // device-side status word (bounds / wait failures)
 
+    // coupled infinite baffle: aperture triangles (ascending ids) and their
+    // local index per triangle (-1 elsewhere)
+    int aperture_tag = 0, m_ap = 0;
+    std::vector<int> ap_tris;
+    int *d_ap_tris = nullptr;
+    int *d_ap_local = nullptr;
+
     // sweep workspace (grown on demand)
     void *ws = nullptr;
     size_t ws_bytes = 0;
@@ -108,11 +115,17 @@ int launch_regular(Session &s, int n_freq, const float *k_re, const float *k_im,
                    const float *beta_re, const float *beta_im,
                    float *a_re, float *a_im, long long lda, long long a_stride,
                    float *b_re, float *b_im, long long b_stride, cudaStream_t st);
+struct ApertureOut {
+    int mode;                        // 0: S_ia (with or without A/b), 1: S_aa
+    float *sia_re, *sia_im, *saa_re, *saa_im;
+    long long sia_stride, saa_stride;
+};
 int launch_duffy(Session &s, int n_freq, const float *k_re, const float *k_im,
                  const float *q_re, const float *q_im, long long q_stride,
                  const float *beta_re, const float *beta_im,
                  float *a_re, float *a_im, long long lda, long long a_stride,
-                 float *b_re, float *b_im, long long b_stride, cudaStream_t st);
+                 float *b_re, float *b_im, long long b_stride, cudaStream_t st,
+                 const ApertureOut *ap);
 
 }  // namespace hbem
 

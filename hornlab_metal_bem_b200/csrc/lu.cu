@@ -26,8 +26,11 @@
 namespace hbem {
 
 // A[start:n, start:col_end] -= A[start:n, k0:k0+kw] * A[k0:k0+kw, start:col_end]
+struct TcWorkspace;
+int tc_workspace_create(int n, int batch, TcWorkspace **out, cudaStream_t st);
+void tc_workspace_destroy(TcWorkspace *w, cudaStream_t st);
 int launch_trailing_update(int n, int batch, int k0, int kw, int start, int col_end, float *a_re, float *a_im,
-                           long long lda, long long a_stride, int precision, int *status, cudaStream_t st);
+                           long long lda, long long a_stride, TcWorkspace *tc, int *status, cudaStream_t st);
 
 namespace {
 
@@ -591,11 +594,18 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
     // mixed precision: K = 64 block updates run on the tensor cores; their
     // barrier waits report through this status word
     int *status = nullptr;
-    if (precision == HBEM_PREC_MIXED) {
+    TcWorkspace *tc = nullptr;
+    if (precision == HBEM_PREC_MIXED && n > 64) {
         HBEM_CUDA(cudaMallocAsync((void **)&status, sizeof(int), st));
         HBEM_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
+        int rc = tc_workspace_create(n, batch, &tc, st);
+        if (rc != HBEM_OK) {
+            cudaFreeAsync(status, st);
+            return rc;
+        }
     }
     auto finish = [&](int rc) -> int {
+        tc_workspace_destroy(tc, st);
         if (status) {
             int h = 0;
             if (rc == HBEM_OK) {
@@ -630,7 +640,7 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
                 HBEM_LAUNCH_CHECK("k_swap_trsm");
             }
             if (c + w < b0 + bw) {
-                int rc = launch_trailing_update(n, batch, c, w, c + w, b0 + bw, a_re, a_im, lda, a_stride, precision,
+                int rc = launch_trailing_update(n, batch, c, w, c + w, b0 + bw, a_re, a_im, lda, a_stride, nullptr,
                                                 nullptr, st);
                 if (rc != HBEM_OK) return finish(rc);
             }
@@ -643,8 +653,7 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
             HBEM_LAUNCH_CHECK("k_swap_trsm");
         }
         if (b0 + bw < n) {
-            int rc = launch_trailing_update(n, batch, b0, bw, b0 + bw, n, a_re, a_im, lda, a_stride, precision, status,
-                                            st);
+            int rc = launch_trailing_update(n, batch, b0, bw, b0 + bw, n, a_re, a_im, lda, a_stride, tc, status, st);
             if (rc != HBEM_OK) return finish(rc);
         }
     }

@@ -230,7 +230,8 @@ void free_session(Session *s) {
     cudaSetDevice(s->device);
     void *ptrs[] = {s->d_qp, s->d_nrm, s->d_tri, s->d_test_slot, s->d_trial_slot, s->d_row_off, s->d_rows,
                     s->d_col_off, s->d_cols, s->d_verts, s->d_tris, s->d_l2g, s->d_tags, s->d_areas,
-                    s->d_normals, s->d_fqp, s->d_fnrm, s->d_pairs, s->d_rule, s->d_rule_w, s->d_status, s->ws};
+                    s->d_normals, s->d_fqp, s->d_fnrm, s->d_pairs, s->d_rule, s->d_rule_w, s->d_status, s->ws,
+                    s->d_ap_tris, s->d_ap_local};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (s->pinned) cudaFreeHost(s->pinned);
@@ -488,6 +489,7 @@ extern "C" int hbem_session_query(const hbem_session *h, int key, long long *val
         case HBEM_Q_IMAGE_PAIRS: *value = s->n_image_pairs; break;
         case HBEM_Q_UNIQUE_TRIPLETS: *value = s->n_unique_triplets; break;
         case HBEM_Q_SYMMETRY: *value = s->sym; break;
+        case HBEM_Q_APERTURE_TRIANGLES: *value = s->m_ap; break;
         case HBEM_Q_KERNEL_LAUNCHES: *value = s->launches; break;
         case HBEM_Q_REGULAR_EVALS: *value = T * T * 36 * M; break;
         case HBEM_Q_DUFFY_EVALS: {

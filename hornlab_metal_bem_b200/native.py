@@ -41,7 +41,7 @@ HBEM_TRANS_N, HBEM_TRANS_T, HBEM_TRANS_C = 0, 1, 2
 QUERY_KEYS = {
     "n_dof": 0, "n_triangles": 1, "n_pairs": 2, "coincident": 3, "edge": 4, "vertex": 5,
     "image_pairs": 6, "unique_triplets": 7, "symmetry": 8, "kernel_launches": 9,
-    "regular_evals": 10, "duffy_evals": 11,
+    "regular_evals": 10, "duffy_evals": 11, "aperture_triangles": 12,
 }
 
 
@@ -72,6 +72,10 @@ _SIGNATURES = {
     "hbem_reduce_tag_avg": ([_vp, _c_int, _vp, _vp, _c_ll, _vp, _c_int, _vp, _vp], _c_int),
     "hbem_solve_batch": ([_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _c_int, _vp, _c_int, _c_int, _c_d, _c_int, _vp, _vp,
                           _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _c_int),
+    "hbem_session_set_aperture": ([_vp, _c_int], _c_int),
+    "hbem_aperture_assemble": ([_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _c_int),
+    "hbem_coupled_ib_schur": ([_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _c_int),
+    "hbem_coupled_ib_field": ([_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _vp, _vp], _c_int),
 }
 
 _LIB: ctypes.CDLL | None = None
@@ -187,6 +191,11 @@ class NativeSession:
         self.handle = handle
         self.n_dof = int(b.p1_dof_count)
         self.n_triangles = int(t.shape[1])
+        self.m_aperture = 0
+        if self.aperture_tag is not None:
+            check(self.lib.hbem_session_set_aperture(self.handle, int(self.aperture_tag)),
+                  "hbem_session_set_aperture", self.lib)
+            self.m_aperture = self.query("aperture_triangles")
 
     # -- lifecycle -------------------------------------------------------------
     @classmethod
@@ -381,6 +390,102 @@ class NativeSession:
                 diagnostics=diag,
             ))
         return results
+
+
+    # -- coupled infinite baffle ---------------------------------------------
+    def coupled_ib_batch(self, frequency_hz, k_real_f32, neumann_dp0, observation_points, *, k_imag_f32=None,
+                         field_k_f32=None, source_tags=None, impedance_source_tag=None,
+                         write_surface_pressure=False, precision="plain", refine_tolerance=1e-6,
+                         refine_max_iterations=10, timings_out=None, **_ignored) -> list[CaseResult]:
+        """Coupled interior BIE + Rayleigh half-space solve (the reference's aperture_tag path).
+
+        A - S_ia (2 S_aa)^-1 P_avg is factored per frequency; the field is the
+        Rayleigh integral of q_a = (2 S_aa)^-1 P_avg p (main.swift:1397-1444,
+        7597-7789).
+        """
+        torch = require_cuda()
+        if self.m_aperture <= 0:
+            raise ValueError("session has no aperture_tag")
+        dev = torch.device("cuda", self.device)
+        freqs = np.ascontiguousarray(np.atleast_1d(frequency_hz), dtype=np.float64)
+        F, n, m, T = freqs.shape[0], self.n_dof, self.m_aperture, self.n_triangles
+        k_re = np.ascontiguousarray(np.atleast_1d(k_real_f32), dtype=np.float32)
+        k_im = None if k_imag_f32 is None else np.ascontiguousarray(np.atleast_1d(k_imag_f32), dtype=np.float32)
+        kf = k_re if field_k_f32 is None else np.ascontiguousarray(np.atleast_1d(field_k_f32), dtype=np.float32)
+        obs = np.asarray(observation_points, dtype=np.float64)
+        if obs.shape[0] != 3:
+            obs = obs.T
+        obs_t = torch.tensor(np.ascontiguousarray(obs, dtype=np.float32), device=dev)
+        N = obs_t.shape[1]
+        st = _stream_ptr()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record()
+        Ar, Ai, br, bi = self.assemble(k_re, np.asarray(neumann_dp0).reshape(F, T), k_imag=k_im)
+        sia_r = torch.empty((F, n, m), dtype=torch.float32, device=dev); sia_i = torch.empty_like(sia_r)
+        saa_r = torch.empty((F, m, m), dtype=torch.float32, device=dev); saa_i = torch.empty_like(saa_r)
+        check(self.lib.hbem_aperture_assemble(self.handle, F, _np_ptr(k_re), _np_ptr(k_im), _np_ptr(kf), _t_ptr(sia_r),
+                                              _t_ptr(sia_i), _t_ptr(saa_r), _t_ptr(saa_i), st),
+              "hbem_aperture_assemble", self.lib)
+        minv_r = torch.empty_like(saa_r); minv_i = torch.empty_like(saa_r)
+        info_ap = torch.zeros(F, dtype=torch.int32, device=dev)
+        check(self.lib.hbem_coupled_ib_schur(self.handle, F, _t_ptr(Ar), _t_ptr(Ai), _t_ptr(sia_r), _t_ptr(sia_i),
+                                             _t_ptr(saa_r), _t_ptr(saa_i), _t_ptr(minv_r), _t_ptr(minv_i),
+                                             _t_ptr(info_ap), st), "hbem_coupled_ib_schur", self.lib)
+        ev[1].record()
+        prec = HBEM_PREC_MIXED if precision == "mixed" else HBEM_PREC_PLAIN
+        A0r = A0i = None
+        if prec == HBEM_PREC_MIXED:
+            A0r, A0i = Ar.clone(), Ai.clone()
+        piv = torch.empty((F, n), dtype=torch.int32, device=dev)
+        info = torch.empty(F, dtype=torch.int32, device=dev)
+        xr, xi = br.clone(), bi.clone()
+        check(self.lib.hbem_lu_factor(n, F, _t_ptr(Ar), _t_ptr(Ai), n, n * n, _t_ptr(piv), n, _t_ptr(info), prec, st),
+              "hbem_lu_factor", self.lib)
+        check(self.lib.hbem_lu_solve(n, 1, F, _t_ptr(Ar), _t_ptr(Ai), n, n * n, _t_ptr(piv), n, _t_ptr(xr), _t_ptr(xi),
+                                     1, n, HBEM_TRANS_N, st), "hbem_lu_solve", self.lib)
+        iters = torch.zeros(F, dtype=torch.int32, device=dev)
+        resid = torch.zeros(F, dtype=torch.float64, device=dev)
+        if prec == HBEM_PREC_MIXED:
+            check(self.lib.hbem_refine(n, F, _t_ptr(A0r), _t_ptr(A0i), n, n * n, _t_ptr(Ar), _t_ptr(Ai), n * n,
+                                       _t_ptr(piv), n, _t_ptr(br), _t_ptr(bi), n, _t_ptr(xr), _t_ptr(xi), n,
+                                       float(refine_tolerance), int(refine_max_iterations), _t_ptr(iters),
+                                       _t_ptr(resid), st), "hbem_refine", self.lib)
+        ev[2].record()
+        qa_r = torch.empty((F, m), dtype=torch.float32, device=dev); qa_i = torch.empty_like(qa_r)
+        fr = torch.empty((F, N), dtype=torch.float32, device=dev); fi = torch.empty_like(fr)
+        check(self.lib.hbem_coupled_ib_field(self.handle, F, _np_ptr(kf), _t_ptr(xr), _t_ptr(xi), _t_ptr(minv_r),
+                                             _t_ptr(minv_i), _t_ptr(obs_t), N, _t_ptr(qa_r), _t_ptr(qa_i), _t_ptr(fr),
+                                             _t_ptr(fi), st), "hbem_coupled_ib_field", self.lib)
+        tags = list(source_tags or [])
+        want = tags + ([impedance_source_tag] if impedance_source_tag is not None and impedance_source_tag not in tags else [])
+        tavg = self.tag_average(xr, xi, want).cpu().numpy() if want else None
+        ev[3].record()
+        torch.cuda.synchronize()
+        t_asm, t_solve, t_field = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2]), ev[2].elapsed_time(ev[3])
+        if timings_out is not None:
+            timings_out.update(assembly_ms=t_asm, solve_ms=t_solve, field_ms=t_field)
+        f_h = (fr.cpu().numpy() + 1j * fi.cpu().numpy()).astype(np.complex64)
+        x_h = (xr.cpu().numpy() + 1j * xi.cpu().numpy()).astype(np.complex64)
+        qa_h = (qa_r.cpu().numpy() + 1j * qa_i.cpu().numpy()).astype(np.complex64)
+        info_h, info_ap_h = info.cpu().numpy(), info_ap.cpu().numpy()
+        it_h, res_h = iters.cpu().numpy(), resid.cpu().numpy()
+        out = []
+        for f in range(F):
+            avgs = {int(t): complex(tavg[f, j, 0], tavg[f, j, 1]) for j, t in enumerate(want)} if want else {}
+            out.append(CaseResult(
+                frequency_hz=float(freqs[f]), field=f_h[f],
+                impedance=avgs.get(int(impedance_source_tag)) if impedance_source_tag is not None else None,
+                surface_pressure_avg={int(t): avgs[int(t)] for t in tags} if tags else None,
+                surface_pressure=x_h[f] if write_surface_pressure else None,
+                assembly_s=t_asm * 1e-3 / F, dense_solve_s=t_solve * 1e-3 / F, field_s=t_field * 1e-3 / F,
+                lapack_info=int(info_h[f] or info_ap_h[f]),
+                diagnostics={"coupled_ib": True, "aperture_triangles": m, "aperture_neumann": qa_h[f],
+                             "aperture_lapack_info": int(info_ap_h[f]), "precision": precision,
+                             "refine_iterations": int(it_h[f]),
+                             "refine_residual_rel": float(res_h[f]) if prec == HBEM_PREC_MIXED else None,
+                             "dense_solve_rcond": None, "assembly_mode": "corrected"},
+            ))
+        return out
 
 
 # Drop-in alias for the reference's session class name.

@@ -42,8 +42,6 @@ def should_route_native(config: SolveConfig) -> bool:
         )
     if config.chief_points is not None:
         raise BackendUnavailable("chief_points (CHIEF least squares) is not supported by the B200 path")
-    if config.aperture_tag is not None:
-        raise BackendUnavailable("aperture_tag (coupled infinite baffle) is not supported by the B200 path yet")
     if config.impedance_sources or config.impedance_source_callback is not None:
         raise BackendUnavailable("impedance_sources (Robin) are not routed by the B200 sweep yet")
     return True
@@ -166,7 +164,9 @@ def run_sweep(mesh: LoadedMesh, frequencies, frame: ObservationFrame, config: So
         stop = False
         for f0 in range(0, freqs.size, chunk):
             sl = slice(f0, f0 + chunk)
-            results = session.assemble_solve_evaluate_standard_neumann_batch(
+            batch_fn = (session.coupled_ib_batch if config.aperture_tag is not None
+                        else session.assemble_solve_evaluate_standard_neumann_batch)
+            results = batch_fn(
                 freqs[sl], k_re[sl], q[sl], pts, k_imag_f32=k_im[sl], source_tags=source_tags,
                 impedance_source_tag=imp_tag, write_surface_pressure=config.return_surface_pressure,
                 dense_solve_dtype=config.dense_solve_dtype, precision=config.precision,

@@ -66,6 +66,7 @@ extern "C" {
 #define HBEM_Q_KERNEL_LAUNCHES 9   /* cumulative launches of this library's kernels on the session */
 #define HBEM_Q_REGULAR_EVALS 10    /* kernel evaluations per frequency, regular part */
 #define HBEM_Q_DUFFY_EVALS 11      /* kernel evaluations per frequency, Duffy part */
+#define HBEM_Q_APERTURE_TRIANGLES 12  /* m: aperture triangles of the coupled baffle (0 when unset) */
 
 typedef struct hbem_session hbem_session;
 
@@ -199,6 +200,34 @@ int hbem_solve_batch(hbem_session *s, int n_freq, const float *k_re, const float
                      float *surface_re, float *surface_im,
                      int *info, int *refine_iters, double *refine_resid,
                      float *timings_ms, void *stream);
+
+/*
+ * Coupled infinite baffle (interior BIE + Rayleigh half-space through the
+ * aperture at z = 0).  Replaces: buildApertureGeometry / buildCoupledIBCoupling
+ * / solveCoupledIBDenseMultiSchur / evaluateCoupledIBRayleighReference
+ * (main.swift:915-964, 1295-1385, 7597-7789, 1397-1444).
+ *
+ * hbem_session_set_aperture: select the aperture faces (physical tag); m is
+ *   then readable with HBEM_Q_APERTURE_TRIANGLES.
+ * hbem_aperture_assemble: S_ia (n_freq, n, m) = P1-test x DP0-aperture-trial
+ *   single layer at k (images, 2^planes row weight, Duffy deltas), and
+ *   S_aa (n_freq, m, m) = aperture-averaged single layer at the real field
+ *   wavenumber kf (Duffy deltas of unmirrored test triangles), both device.
+ * hbem_coupled_ib_schur: A <- A - S_ia (2 S_aa)^-1 P_avg in place (P_avg: 1/3
+ *   on the three dofs of each aperture triangle); writes M = (2 S_aa)^-1
+ *   (n_freq, m, m).  S_aa is overwritten by its LU factors.
+ * hbem_coupled_ib_field: q_a = M (P_avg p) (n_freq, m) and the Rayleigh field
+ *   -2 sum G(y, x') q_a with x' = (x, y, max(z, 0)) for z >= -1e-5, 0 below.
+ */
+int hbem_session_set_aperture(hbem_session *s, int aperture_tag);
+int hbem_aperture_assemble(hbem_session *s, int n_freq, const float *k_re, const float *k_im, const float *kf_re,
+                           float *sia_re, float *sia_im, float *saa_re, float *saa_im, void *stream);
+int hbem_coupled_ib_schur(hbem_session *s, int n_freq, float *a_re, float *a_im, const float *sia_re,
+                          const float *sia_im, float *saa_re, float *saa_im, float *minv_re, float *minv_im,
+                          int *info, void *stream);
+int hbem_coupled_ib_field(hbem_session *s, int n_freq, const float *kf_re, const float *p_re, const float *p_im,
+                          const float *minv_re, const float *minv_im, const float *obs_3xn, int n_obs,
+                          float *qa_re, float *qa_im, float *out_re, float *out_im, void *stream);
 
 #ifdef __cplusplus
 }

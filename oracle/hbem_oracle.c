@@ -717,3 +717,143 @@ int OGP(set_threads)(int n) {
     return 1;
 #endif
 }
+
+/* ---- coupled infinite baffle (main.swift:873-1470, 7504-7595) ---------- */
+/* S_ia (n x m): interior SLP projection onto aperture triangles: regular part
+   with trial images and the 2^planes row weight (main.swift:1178-1235), plus
+   the Duffy SLP deltas of every singular pair whose trial is an aperture
+   triangle, at weight 1 (main.swift:1011-1049). */
+int OGP(aperture_slp)(const og_geom *g, const int *ap, int m, REAL kr, REAL ki, REAL *S_re, REAL *S_im) {
+    int T = g->n_triangles;
+    int masks[4] = {0, 0, 0, 0};
+    int nm = 1 + mirror_masks(g->sym, masks + 1);
+    REAL rw = row_weight(g->sym);
+#pragma omp parallel for schedule(dynamic, 8)
+    for (int test = 0; test < T; ++test) {
+        for (int t = 0; t < m; ++t) {
+            cplx slp[3] = {{0, 0}, {0, 0}, {0, 0}};
+            for (int mi = 0; mi < nm; ++mi) {
+                cplx s[3], d[9];
+                pair_blocks(g, test, ap[t], 0, masks[mi], 0, 0, NULL, 0, NULL, 0, kr, ki, s, d);
+                for (int i = 0; i < 3; ++i) slp[i] = cadd(slp[i], s[i]);
+            }
+            for (int i = 0; i < 3; ++i) {
+                int row = dof(g, test, i);
+                atomic_add(&S_re[(size_t)row * m + t], slp[i].re * rw);
+                atomic_add(&S_im[(size_t)row * m + t], slp[i].im * rw);
+            }
+        }
+    }
+    int counts[3];
+    int np = OGP(duffy_pairs)(g, NULL, 0, counts);
+    int *pairs = malloc((size_t)(np ? np : 1) * PAIR_INTS * sizeof(int));
+    OGP(duffy_pairs)(g, pairs, np, counts);
+    int *loc = malloc((size_t)T * sizeof(int));
+    for (int i = 0; i < T; ++i) loc[i] = -1;
+    for (int t = 0; t < m; ++t) loc[ap[t]] = t;
+    REAL *rules[3];
+    int nr[3];
+    for (int k = 0; k < 3; ++k) { rules[k] = malloc(1536 * 5 * sizeof(REAL)); nr[k] = duffy_rule(k + 1, rules[k]); }
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int p = 0; p < np; ++p) {
+        const int *r = pairs + (size_t)p * PAIR_INTS;
+        int t = loc[r[1]];
+        if (t < 0) continue;
+        cplx rs[3], rd[9], ss[3], sd[9];
+        pair_blocks(g, r[0], r[1], r[2], r[3], 0, 0, r + 5, 0, NULL, 0, kr, ki, rs, rd);
+        pair_blocks(g, r[0], r[1], r[2], r[3], 1, r[4], r + 5, 0, rules[r[4] - 1], nr[r[4] - 1], kr, ki, ss, sd);
+        for (int i = 0; i < 3; ++i) {
+            int row = dof(g, r[0], i);
+            cplx dlt = csub(ss[i], rs[i]);
+            atomic_add(&S_re[(size_t)row * m + t], dlt.re);
+            atomic_add(&S_im[(size_t)row * m + t], dlt.im);
+        }
+    }
+    free(pairs); free(loc);
+    for (int k = 0; k < 3; ++k) free(rules[k]);
+    return 0;
+}
+
+/* S_aa (m x m): aperture-averaged SLP at the real field wavenumber, divided
+   by the test triangle area (main.swift:1237-1290); Duffy deltas of aperture
+   pairs with an unmirrored test triangle (main.swift:1051-1087). */
+int OGP(aperture_avg)(const og_geom *g, const int *ap, int m, REAL kr, REAL *S_re, REAL *S_im) {
+    int T = g->n_triangles;
+    int masks[4] = {0, 0, 0, 0};
+    int nm = 1 + mirror_masks(g->sym, masks + 1);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int r = 0; r < m; ++r) {
+        REAL inv = (REAL)1 / (g->areas[ap[r]] > 0 ? (REAL)g->areas[ap[r]] : (REAL)1e-38);
+        for (int c = 0; c < m; ++c) {
+            cplx acc = {0, 0};
+            for (int mi = 0; mi < nm; ++mi) {
+                cplx s[3], d[9];
+                pair_blocks(g, ap[r], ap[c], 0, masks[mi], 0, 0, NULL, 0, NULL, 0, kr, 0, s, d);
+                for (int i = 0; i < 3; ++i) acc = cadd(acc, s[i]);
+            }
+            S_re[(size_t)r * m + c] += acc.re * inv;
+            S_im[(size_t)r * m + c] += acc.im * inv;
+        }
+    }
+    int counts[3];
+    int np = OGP(duffy_pairs)(g, NULL, 0, counts);
+    int *pairs = malloc((size_t)(np ? np : 1) * PAIR_INTS * sizeof(int));
+    OGP(duffy_pairs)(g, pairs, np, counts);
+    int *loc = malloc((size_t)T * sizeof(int));
+    for (int i = 0; i < T; ++i) loc[i] = -1;
+    for (int t = 0; t < m; ++t) loc[ap[t]] = t;
+    REAL *rules[3];
+    int nr[3];
+    for (int k = 0; k < 3; ++k) { rules[k] = malloc(1536 * 5 * sizeof(REAL)); nr[k] = duffy_rule(k + 1, rules[k]); }
+    for (int p = 0; p < np; ++p) {
+        const int *q = pairs + (size_t)p * PAIR_INTS;
+        if (q[2] != 0 || loc[q[0]] < 0 || loc[q[1]] < 0) continue;
+        cplx rs[3], rd[9], ss[3], sd[9];
+        pair_blocks(g, q[0], q[1], q[2], q[3], 0, 0, q + 5, 0, NULL, 0, kr, 0, rs, rd);
+        pair_blocks(g, q[0], q[1], q[2], q[3], 1, q[4], q + 5, 0, rules[q[4] - 1], nr[q[4] - 1], kr, 0, ss, sd);
+        cplx dlt = {0, 0};
+        for (int i = 0; i < 3; ++i) dlt = cadd(dlt, csub(ss[i], rs[i]));
+        REAL inv = (REAL)1 / (g->areas[q[0]] > 0 ? (REAL)g->areas[q[0]] : (REAL)1e-38);
+        S_re[(size_t)loc[q[0]] * m + loc[q[1]]] += dlt.re * inv;
+        S_im[(size_t)loc[q[0]] * m + loc[q[1]]] += dlt.im * inv;
+    }
+    free(pairs); free(loc);
+    for (int k = 0; k < 3; ++k) free(rules[k]);
+    return 0;
+}
+
+/* Rayleigh half-space field of the aperture Neumann data (main.swift:1397-1444):
+   p(x) = -2 sum_t q_t sum_q w 2|t| sum_images G(y, x') with x' = (x, y, max(z, 0))
+   for z >= -1e-5, zero below the baffle. */
+int OGP(rayleigh)(const og_geom *g, const int *ap, int m, REAL kr, const REAL *qa_re, const REAL *qa_im,
+                  const float *obs3xN, int nobs, REAL *out_re, REAL *out_im) {
+    int masks[3];
+    int nm = mirror_masks(g->sym, masks);
+#pragma omp parallel for schedule(static)
+    for (int o = 0; o < nobs; ++o) {
+        REAL ox = obs3xN[o], oy = obs3xN[nobs + o], oz = obs3xN[2 * nobs + o];
+        out_re[o] = 0; out_im[o] = 0;
+        if (oz < (REAL)-1e-5) continue;
+        REAL ez = oz < 0 ? 0 : oz;
+        cplx acc = {0, 0};
+        for (int t = 0; t < m; ++t) {
+            cplx qv = {qa_re[t], qa_im[t]};
+            if (qv.re == 0 && qv.im == 0) continue;
+            REAL jac = (REAL)2 * (REAL)g->areas[ap[t]];
+            for (int a = 0; a < 6; ++a) {
+                REAL sp[3];
+                point_on(g, ap[t], (REAL)QX[a], (REAL)QY[a], sp);
+                REAL w = (REAL)QW[a] * jac;
+                acc = cadd(acc, cscale(cmul(green(sp[0] - ox, sp[1] - oy, sp[2] - ez, kr, 0), qv), w));
+                for (int mi = 0; mi < nm; ++mi) {
+                    REAL ip[3] = {sp[0], sp[1], sp[2]};
+                    mirror(ip, masks[mi]);
+                    acc = cadd(acc, cscale(cmul(green(ip[0] - ox, ip[1] - oy, ip[2] - ez, kr, 0), qv), w));
+                }
+            }
+        }
+        out_re[o] = acc.re * (REAL)-2;
+        out_im[o] = acc.im * (REAL)-2;
+    }
+    return 0;
+}

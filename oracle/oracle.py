@@ -172,6 +172,55 @@ class Oracle:
         return complex(out[0], out[1])
 
 
+    # -- coupled infinite baffle ---------------------------------------------
+    def aperture_triangles(self, tag: int):
+        return np.flatnonzero(self.tags == int(tag)).astype(np.int32)
+
+    def aperture_slp(self, ap, k: float, k_imag: float = 0.0):
+        ap = np.ascontiguousarray(ap, dtype=np.int32)
+        m = ap.shape[0]
+        Sre = np.zeros((self.n, m), self.real); Sim = np.zeros((self.n, m), self.real)
+        self._fn("aperture_slp")(ctypes.byref(self.geom), _ptr(ap), ctypes.c_int(m), self._ct(k), self._ct(k_imag),
+                                 _ptr(Sre), _ptr(Sim))
+        return Sre + 1j * Sim
+
+    def aperture_avg(self, ap, k: float):
+        ap = np.ascontiguousarray(ap, dtype=np.int32)
+        m = ap.shape[0]
+        Sre = np.zeros((m, m), self.real); Sim = np.zeros((m, m), self.real)
+        self._fn("aperture_avg")(ctypes.byref(self.geom), _ptr(ap), ctypes.c_int(m), self._ct(k), _ptr(Sre), _ptr(Sim))
+        return Sre + 1j * Sim
+
+    def rayleigh(self, ap, k: float, qa, obs_3xn):
+        ap = np.ascontiguousarray(ap, dtype=np.int32)
+        obs = np.ascontiguousarray(obs_3xn, dtype=np.float32)
+        qa = np.asarray(qa)
+        qre = np.ascontiguousarray(qa.real, self.real); qim = np.ascontiguousarray(qa.imag, self.real)
+        ore = np.zeros(obs.shape[1], self.real); oim = np.zeros(obs.shape[1], self.real)
+        self._fn("rayleigh")(ctypes.byref(self.geom), _ptr(ap), ctypes.c_int(ap.shape[0]), self._ct(k), _ptr(qre),
+                             _ptr(qim), _ptr(obs), ctypes.c_int(obs.shape[1]), _ptr(ore), _ptr(oim))
+        return ore + 1j * oim
+
+    def coupled_ib_solve(self, A, b, ap, k: float, field_k: float, k_imag: float = 0.0, precision: str = "f64"):
+        """Augmented system [[A, -S_ia], [P_avg, -2 S_aa]] [p; q_a] = [b; 0] (main.swift:7504-7595)."""
+        S_ia = self.aperture_slp(ap, k, k_imag)
+        S_aa = self.aperture_avg(ap, field_k)
+        n, m = self.n, len(ap)
+        l2g = np.asarray(self._keep[2])
+        P = np.zeros((m, n))
+        for r, t in enumerate(ap):
+            for d in l2g[t]:
+                P[r, d] += 1.0 / 3.0
+        Aug = np.zeros((n + m, n + m), np.complex128)
+        Aug[:n, :n] = A
+        Aug[:n, n:] = -S_ia
+        Aug[n:, :n] = P
+        Aug[n:, n:] = -2.0 * S_aa
+        rhs = np.concatenate([np.asarray(b, np.complex128), np.zeros(m)])
+        x = dense_solve(Aug, rhs, precision)
+        return x[:n], x[n:], S_ia, S_aa
+
+
 def dense_solve(A, b, precision: str = "f32"):
     """LAPACK ``cgesv`` (complex64) or ``zgesv`` (complex128): the Accelerate stand-in."""
     from scipy.linalg import lapack
