@@ -246,3 +246,62 @@ def horn(spec: HornSpec = HornSpec(), quarter: bool = True) -> LoadedMesh:
     else:
         f = _orient_outward(v, f)
     return mesh_from_arrays(v, f, tags, physical_groups={1: "wall", 2: "throat"})
+
+
+def baffled_horn(spec: HornSpec = HornSpec(), quarter: bool = False, aperture_tag: int = 12) -> LoadedMesh:
+    """Interior-domain horn for the coupled infinite baffle.
+
+    The cavity is the horn's air volume: throat disc (tag 2) at z = -L, flared
+    wall (tag 1) and the flush mouth aperture (``aperture_tag``) at z = 0.
+    Normals point into the cavity (aperture normals -Z), so the signed-volume
+    indicator is negative, as the reference requires for coupled meshes
+    (``mesh.py:411-484``).
+    """
+    h = spec.edge
+    L, rt, rm, m = spec.length, spec.throat_radius, spec.mouth_radius, spec.flare
+
+    def flare_r(z):
+        return rt + (rm - rt) * (np.expm1(m * (z + L)) / np.expm1(m * L))
+
+    pts: list[tuple[float, float]] = []
+    tags: list[int] = []
+
+    def extend(points, tag):
+        start = 1 if pts else 0
+        for p in points[start:]:
+            if pts:
+                tags.append(tag)
+            pts.append((float(p[0]), float(p[1])))
+
+    def seg(p0, p1):
+        n = max(1, int(math.ceil(math.dist(p0, p1) / h)))
+        return [(p0[0] + (p1[0] - p0[0]) * t, p0[1] + (p1[1] - p0[1]) * t) for t in np.linspace(0, 1, n + 1)]
+
+    zs = np.linspace(-L, 0.0, 4000)
+    rs = flare_r(zs)
+    ds = np.concatenate([[0.0], np.cumsum(np.hypot(np.diff(rs), np.diff(zs)))])
+    nseg = max(1, int(math.ceil(ds[-1] / h)))
+    sgrid = np.linspace(0, ds[-1], nseg + 1)
+    wall = list(zip(np.interp(sgrid, ds, rs), np.interp(sgrid, ds, zs)))
+    extend(seg((0.0, -L), (rt, -L)), 2)
+    extend(wall, 1)
+    extend(seg((rm, 0.0), (0.0, 0.0)), aperture_tag)
+    v, f, t = revolve(np.asarray(pts), np.asarray(tags, dtype=np.int32), h, quarter)
+    keys = np.round(v / 1e-9).astype(np.int64)
+    _, first, inv = np.unique(keys, axis=0, return_index=True, return_inverse=True)
+    inv = np.asarray(inv).reshape(-1)
+    order = np.argsort(first)
+    remap = np.empty_like(order)
+    remap[order] = np.arange(order.size)
+    v = v[first[order]]
+    f = remap[inv[f]].astype(np.int32)
+    keep = ~((f[:, 0] == f[:, 1]) | (f[:, 1] == f[:, 2]) | (f[:, 0] == f[:, 2]))
+    f, t = f[keep], t[keep]
+    # orient so the aperture normals point -Z (into the cavity)
+    ap = t == aperture_tag
+    p0, p1, p2 = v[f[:, 0]], v[f[:, 1]], v[f[:, 2]]
+    nz = np.cross(p1 - p0, p2 - p0)[:, 2]
+    if float(np.mean(nz[ap])) > 0:
+        f = f[:, [0, 2, 1]]
+    return mesh_from_arrays(v, np.ascontiguousarray(f), t,
+                            physical_groups={1: "wall", 2: "throat", aperture_tag: "mouth_aperture"})
