@@ -7,14 +7,18 @@
 //     for each inner sub-panel c (32 or 16 columns):
 //       k_panel      : factor rows c..n of the sub-panel with partial pivoting
 //                      (pivot = first max |re|+|im|, as LAPACK's icamax),
-//                      staged in shared memory when it fits, else in L2;
+//                      staged in one CTA's shared memory when it fits, else
+//                      spread over a 2/4/8-CTA cluster's shared memory
+//                      (k_panel_cluster), else in L2;
 //       k_swap_trsm  : swap + forward-solve the other columns of the block;
 //       trailing     : update the block's remaining columns (K = 16/32);
 //     k_swap_trsm    : the block's 64 swaps on all other columns and the
 //                      64-row TRSM U12 = L11^-1 A12;
 //     trailing       : A22 -= L21 U12 with K = 64.
 // The solve applies the pivots then runs blocked forward / backward
-// substitution (op(A) = A, A^T or A^H).
+// substitution: op(A) = A with n > 128 in 128-row block steps over many CTAs
+// (k_trsv_*), A^T / A^H and small n in one CTA per right-hand side (k_getrs).
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -37,33 +41,6 @@ namespace {
 constexpr int kPanelThreads = 512;
 
 __device__ __forceinline__ float cabs1(float r, float i) { return fabsf(r) + fabsf(i); }
-
-// Block-wide argmax of (value, index), ties to the smallest index.
-__device__ void block_argmax(float &v, int &idx, float *s_v, int *s_i) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int o = 16; o > 0; o >>= 1) {
-        const float ov = __shfl_xor_sync(0xffffffffu, v, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
-        if (ov > v || (ov == v && oi < idx)) { v = ov; idx = oi; }
-    }
-    if (lane == 0) { s_v[warp] = v; s_i[warp] = idx; }
-    __syncthreads();
-    if (warp == 0) {
-        const int nw = blockDim.x >> 5;
-        v = lane < nw ? s_v[lane] : -1.f;
-        idx = lane < nw ? s_i[lane] : 0x7fffffff;
-        for (int o = 16; o > 0; o >>= 1) {
-            const float ov = __shfl_xor_sync(0xffffffffu, v, o);
-            const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
-            if (ov > v || (ov == v && oi < idx)) { v = ov; idx = oi; }
-        }
-        if (lane == 0) { s_v[0] = v; s_i[0] = idx; }
-    }
-    __syncthreads();
-    v = s_v[0];
-    idx = s_i[0];
-    __syncthreads();
-}
 
 // Panel factorisation of rows k0..n-1 x nb columns (nb <= 32).
 // SMEM: the panel is staged in shared memory with an odd row pitch (nb + 1),
@@ -146,6 +123,7 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(float *a_re, float *a_i
                 const int oi = s_i[w];
                 if (ov > bv || (ov == bv && oi < p)) { bv = ov; p = oi; }
             }
+            if (p >= m) p = j;  // column of NaNs: keep the diagonal, as icamax does
             const int c = tid;
             const float jr = pre[j * P + c], ji = pim[j * P + c];
             const float pr = pre[p * P + c], pi = pim[p * P + c];
@@ -195,6 +173,162 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(float *a_re, float *a_i
         }
     }
     if (tid == 0 && first_zero && info[b] == 0) info[b] = first_zero;
+}
+
+// Panel factorisation across a thread-block cluster, for panels too tall for
+// one CTA's shared memory.  CTA q of the cluster owns panel rows
+// [q R, (q+1) R) in its shared memory (pitch nb + 1).  Per column j:
+//   R: every CTA scales its rows of column j-1 and finds its local argmax of
+//      column j;                                           -> cluster barrier
+//   P: every CTA reduces the CS candidates (same order everywhere), copies the
+//      pivot row from its owner's shared memory (DSMEM), the owner of the
+//      pivot row copies the old row j;                     -> cluster barrier
+//      row j := pivot row, pivot row := old row j (owners write locally);
+//   E: every CTA updates its own rows below j.
+// Both barriers are executed by every CTA on every column.
+template <int CS>
+__global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(kPanelThreads)
+    k_panel_cluster(float *a_re, float *a_im, long long lda, long long a_stride, int n, int k0, int nb, int R,
+                    int *piv, long long piv_stride, int *info) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    extern __shared__ float s_panel[];
+    __shared__ float s_v[kPanelThreads / 32];
+    __shared__ int s_i[kPanelThreads / 32];
+    __shared__ float s_cv;   // this CTA's candidate
+    __shared__ int s_ci;
+    __shared__ float s_pr[32], s_pi[32];   // pivot row
+    __shared__ float s_or[32], s_oi[32];   // old row j (used by the pivot row's owner)
+    const int q = (int)cluster.block_rank();
+    const int b = blockIdx.y;
+    int *pv = piv + (size_t)b * piv_stride;
+    const int m = n - k0;
+    const int P = nb + 1;
+    const int r0 = q * R, r1 = min(m, r0 + R);  // own panel rows
+    const int nr = max(0, r1 - r0);
+    float *pre = s_panel, *pim = s_panel + R * P;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    {
+        const float *gre = a_re + (size_t)b * a_stride + (size_t)(k0 + r0) * lda + k0;
+        const float *gim = a_im + (size_t)b * a_stride + (size_t)(k0 + r0) * lda + k0;
+        for (int e = tid; e < nr * nb; e += blockDim.x) {
+            const int r = e / nb, j = e - r * nb;
+            pre[r * P + j] = gre[(size_t)r * lda + j];
+            pim[r * P + j] = gim[(size_t)r * lda + j];
+        }
+    }
+    __syncthreads();
+    const int LPR = nb > 16 ? 32 : 16;
+    const int c_off = lane & (LPR - 1), r_sub = lane / LPR, r_step = nw * (32 / LPR);
+    int first_zero = 0;
+    float ir = 0.f, ii = 0.f;
+    for (int j = 0; j <= nb; ++j) {
+        // ---- R (local rows r >= j, global panel index r0 + lr)
+        float v = -1.f;
+        int idx = 0x7fffffff;
+        const int lr0 = max(0, j - r0);
+        for (int lr = lr0 + tid; lr < nr; lr += blockDim.x) {
+            const int o = lr * P;
+            if (j > 0) {
+                const float xr = pre[o + j - 1], xi = pim[o + j - 1];
+                pre[o + j - 1] = xr * ir - xi * ii;
+                pim[o + j - 1] = xr * ii + xi * ir;
+            }
+            if (j < nb) {
+                const float c = cabs1(pre[o + j], pim[o + j]);
+                if (c > v) { v = c; idx = r0 + lr; }
+            }
+        }
+        if (j == nb) break;
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ov = __shfl_xor_sync(0xffffffffu, v, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+            if (ov > v || (ov == v && oi < idx)) { v = ov; idx = oi; }
+        }
+        if (lane == 0) { s_v[warp] = v; s_i[warp] = idx; }
+        __syncthreads();
+        if (tid == 0) {
+            float bv = s_v[0];
+            int bi = s_i[0];
+            for (int w = 1; w < nw; ++w)
+                if (s_v[w] > bv || (s_v[w] == bv && s_i[w] < bi)) { bv = s_v[w]; bi = s_i[w]; }
+            s_cv = bv;
+            s_ci = bi;
+        }
+        cluster.sync();
+        // ---- P
+        float bv = -1.f;
+        int p = 0x7fffffff;
+        for (int c = 0; c < CS; ++c) {
+            const float ov = *cluster.map_shared_rank(&s_cv, c);
+            const int oi = *cluster.map_shared_rank(&s_ci, c);
+            if (ov > bv || (ov == bv && oi < p)) { bv = ov; p = oi; }
+        }
+        if (p >= m) p = j;  // column of NaNs: keep the diagonal, as icamax does
+        const int owner_p = p / R, owner_j = j / R;
+        if (tid < nb) {
+            const float *rre = cluster.map_shared_rank(pre, owner_p);
+            const float *rim = cluster.map_shared_rank(pim, owner_p);
+            s_pr[tid] = rre[(p - owner_p * R) * P + tid];
+            s_pi[tid] = rim[(p - owner_p * R) * P + tid];
+            if (q == owner_p && p != j) {
+                const float *jre = cluster.map_shared_rank(pre, owner_j);
+                const float *jim = cluster.map_shared_rank(pim, owner_j);
+                s_or[tid] = jre[(j - owner_j * R) * P + tid];
+                s_oi[tid] = jim[(j - owner_j * R) * P + tid];
+            }
+        }
+        cluster.sync();
+        if (tid < nb) {
+            if (q == owner_j) {
+                pre[(j - r0) * P + tid] = s_pr[tid];
+                pim[(j - r0) * P + tid] = s_pi[tid];
+            }
+            if (q == owner_p && p != j) {
+                pre[(p - r0) * P + tid] = s_or[tid];
+                pim[(p - r0) * P + tid] = s_oi[tid];
+            }
+        }
+        if (q == 0 && tid == 0) pv[k0 + j] = k0 + p;
+        __syncthreads();
+        const float dr = s_pr[j], di = s_pi[j];
+        const bool zero = (dr == 0.f && di == 0.f);
+        if (zero) {
+            if (first_zero == 0) first_zero = k0 + j + 1;
+            ir = 0.f;
+            ii = 0.f;
+        } else {
+            const float den = 1.0f / (dr * dr + di * di);
+            ir = dr * den;
+            ii = -di * den;
+        }
+        // ---- E (own rows below j)
+        const int c = j + 1 + c_off;
+        if (c < nb && !zero) {
+            const float ur = s_pr[c], ui = s_pi[c];
+            const int lstart = max(0, j + 1 - r0);
+            for (int lr = lstart + warp * (32 / LPR) + r_sub; lr < nr; lr += r_step) {
+                const int o = lr * P;
+                const float xr = pre[o + j], xi = pim[o + j];
+                const float lr_ = xr * ir - xi * ii, li_ = xr * ii + xi * ir;
+                pre[o + c] -= lr_ * ur - li_ * ui;
+                pim[o + c] -= lr_ * ui + li_ * ur;
+            }
+        }
+        __syncthreads();
+    }
+    {
+        float *gre = a_re + (size_t)b * a_stride + (size_t)(k0 + r0) * lda + k0;
+        float *gim = a_im + (size_t)b * a_stride + (size_t)(k0 + r0) * lda + k0;
+        for (int e = tid; e < nr * nb; e += blockDim.x) {
+            const int r = e / nb, j = e - r * nb;
+            gre[(size_t)r * lda + j] = pre[r * P + j];
+            gim[(size_t)r * lda + j] = pim[r * P + j];
+        }
+    }
+    if (q == 0 && tid == 0 && first_zero && info[b] == 0) info[b] = first_zero;
+    // no CTA may exit while another can still read its shared memory
+    cluster.sync();
 }
 
 // Row swaps + forward substitution for a column range, staged in shared
@@ -344,7 +478,7 @@ __global__ void __launch_bounds__(512) k_getrs(int n, const float *lu_re, const 
     const float *Ar = lu_re + (size_t)mat * a_stride, *Ai = lu_im + (size_t)mat * a_stride;
     const int *pv = piv + (size_t)mat * piv_stride;
     float *br = b_re + (size_t)mat * b_stride, *bi = b_im + (size_t)mat * b_stride;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const float cs = TRANS == 2 ? -1.f : 1.f;  // conjugation sign on the imaginary part
     for (int i = tid; i < n; i += blockDim.x) {
         xr[i] = br[(size_t)i * ldb + rhs];
@@ -537,6 +671,251 @@ __global__ void __launch_bounds__(512) k_getrs(int n, const float *lu_re, const 
     }
 }
 
+// ---------------------------------------------------------------------------
+// Blocked no-transpose solve for many CTAs per right-hand side.  The rows are
+// cut into kTB-row blocks.  One launch per block step: CTA 0 of each
+// (rhs, matrix) applies the final block's x to the next block's rows and then
+// solves that block's diagonal triangle; the other CTAs apply the final
+// block's x to all later rows (warp per row, coalesced row reads).  A
+// prologue CTA per (rhs, matrix) applies the row interchanges (forward only)
+// and solves the first block.  x lives in b throughout.
+// ---------------------------------------------------------------------------
+constexpr int kTB = 128;          // rows per block step
+constexpr int kTrsvThreads = 256;
+constexpr int kTrsvRows = 64;     // rows per update CTA (8 warps x 8 rows)
+
+// Solve the diagonal triangle of rows [g0, g1) in place (x in global), unit
+// lower (UPPER = false, 32-row sub-blocks from the top) or non-unit upper
+// (UPPER = true, from the bottom).  All kTrsvThreads threads take part.
+template <bool UPPER>
+__device__ void trsv_diag(const float *Ar, const float *Ai, long long lda, float *xr, float *xi, long long ldb,
+                          int g0, int g1, float *s_tr, float *s_ti, float *s_xr, float *s_xi) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    const int gb = g1 - g0;
+    const int nsub = (gb + 31) / 32;
+    for (int q = 0; q < nsub; ++q) {
+        const int sb = UPPER ? nsub - 1 - q : q;
+        const int s0 = g0 + sb * 32, s1 = min(g1, s0 + 32), sw = s1 - s0;
+        // stage the 32 x 32 diagonal tile (pitch 33) and the sub-block's x
+        for (int e = tid; e < 32 * 32; e += blockDim.x) {
+            const int r = e >> 5, c = e & 31;
+            float tr = 0.f, ti = 0.f;
+            if (r < sw && c < sw) {
+                tr = Ar[(size_t)(s0 + r) * lda + s0 + c];
+                ti = Ai[(size_t)(s0 + r) * lda + s0 + c];
+            }
+            s_tr[r * 33 + c] = tr;
+            s_ti[r * 33 + c] = ti;
+        }
+        if (tid < 32) {
+            s_xr[tid] = tid < sw ? xr[(size_t)(s0 + tid) * ldb] : 0.f;
+            s_xi[tid] = tid < sw ? xi[(size_t)(s0 + tid) * ldb] : 0.f;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            // column sweep: lane i holds x_i; step j finalises x_j and
+            // removes its contribution from the remaining rows
+            float vr = s_xr[lane], vi = s_xi[lane];
+            if (!UPPER) {
+                for (int j = 0; j < sw; ++j) {
+                    const float jr = __shfl_sync(0xffffffffu, vr, j), ji = __shfl_sync(0xffffffffu, vi, j);
+                    if (lane > j) {
+                        const float lr = s_tr[lane * 33 + j], li = s_ti[lane * 33 + j];
+                        vr -= lr * jr - li * ji;
+                        vi -= lr * ji + li * jr;
+                    }
+                }
+            } else {
+                for (int j = sw - 1; j >= 0; --j) {
+                    if (lane == j) {
+                        const float dr = s_tr[j * 33 + j], di = s_ti[j * 33 + j];
+                        const float den = 1.0f / (dr * dr + di * di);
+                        const float yr = vr, yi = vi;
+                        vr = (yr * dr + yi * di) * den;
+                        vi = (yi * dr - yr * di) * den;
+                    }
+                    const float jr = __shfl_sync(0xffffffffu, vr, j), ji = __shfl_sync(0xffffffffu, vi, j);
+                    if (lane < j) {
+                        const float ur = s_tr[lane * 33 + j], ui = s_ti[lane * 33 + j];
+                        vr -= ur * jr - ui * ji;
+                        vi -= ur * ji + ui * jr;
+                    }
+                }
+            }
+            s_xr[lane] = vr;
+            s_xi[lane] = vi;
+            if (lane < sw) {
+                xr[(size_t)(s0 + lane) * ldb] = vr;
+                xi[(size_t)(s0 + lane) * ldb] = vi;
+            }
+        }
+        __syncthreads();
+        // remaining rows of this diagonal block: below (lower) or above (upper)
+        const int u0 = UPPER ? g0 : s1, u1 = UPPER ? s0 : g1;
+        for (int i = u0 + warp; i < u1; i += nw) {
+            float pr = 0.f, pi = 0.f;
+            if (lane < sw) {
+                const float ar = Ar[(size_t)i * lda + s0 + lane], ai = Ai[(size_t)i * lda + s0 + lane];
+                pr = ar * s_xr[lane] - ai * s_xi[lane];
+                pi = ar * s_xi[lane] + ai * s_xr[lane];
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                pr += __shfl_xor_sync(0xffffffffu, pr, o);
+                pi += __shfl_xor_sync(0xffffffffu, pi, o);
+            }
+            if (lane == 0) {
+                xr[(size_t)i * ldb] -= pr;
+                xi[(size_t)i * ldb] -= pi;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// rows [r0, r1): x_i -= A[i, f0:f1] x[f0:f1], with x[f0:f1] staged in s_x*
+__device__ __forceinline__ void trsv_apply(const float *Ar, const float *Ai, long long lda, float *xr, float *xi,
+                                           long long ldb, int f0, int fw, int r0, int r1, const float *s_xr,
+                                           const float *s_xi) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int i = r0 + warp; i < r1; i += nw) {
+        const float *rr = Ar + (size_t)i * lda + f0, *ri = Ai + (size_t)i * lda + f0;
+        float pr = 0.f, pi = 0.f;
+#pragma unroll
+        for (int c0 = 0; c0 < kTB; c0 += 32) {
+            const int c = c0 + lane;
+            if (c < fw) {
+                const float ar = rr[c], ai = ri[c];
+                pr += ar * s_xr[c] - ai * s_xi[c];
+                pi += ar * s_xi[c] + ai * s_xr[c];
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            pr += __shfl_xor_sync(0xffffffffu, pr, o);
+            pi += __shfl_xor_sync(0xffffffffu, pi, o);
+        }
+        if (lane == 0) {
+            xr[(size_t)i * ldb] -= pr;
+            xi[(size_t)i * ldb] -= pi;
+        }
+    }
+}
+
+// Prologue: one CTA per (rhs, matrix).  Forward: apply the interchanges to
+// the whole vector in shared memory, then solve block 0.  Backward: solve
+// the last block.
+template <bool UPPER>
+__global__ void __launch_bounds__(kTrsvThreads) k_trsv_first(int n, const float *lu_re, const float *lu_im,
+                                                             long long lda, long long a_stride, const int *piv,
+                                                             long long piv_stride, float *b_re, float *b_im,
+                                                             long long ldb, long long b_stride) {
+    extern __shared__ float s_x[];
+    __shared__ float s_tr[32 * 33], s_ti[32 * 33], s_xr[32], s_xi[32];
+    const int mat = blockIdx.y, rhs = blockIdx.x;
+    const float *Ar = lu_re + (size_t)mat * a_stride, *Ai = lu_im + (size_t)mat * a_stride;
+    float *xr = b_re + (size_t)mat * b_stride + rhs, *xi = b_im + (size_t)mat * b_stride + rhs;
+    if (!UPPER) {
+        const int *pv = piv + (size_t)mat * piv_stride;
+        float *vr = s_x, *vi = s_x + n;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            vr[i] = xr[(size_t)i * ldb];
+            vi[i] = xi[(size_t)i * ldb];
+        }
+        __shared__ int s_pv[1024];
+        for (int base = 0; base < n; base += 1024) {
+            const int cnt = min(1024, n - base);
+            __syncthreads();
+            for (int i = threadIdx.x; i < cnt; i += blockDim.x) s_pv[i] = pv[base + i];
+            __syncthreads();
+            if (threadIdx.x == 0)
+                for (int i = 0; i < cnt; ++i) {
+                    const int p = s_pv[i], r = base + i;
+                    if (p != r && p >= 0 && p < n) {
+                        float t = vr[r]; vr[r] = vr[p]; vr[p] = t;
+                        t = vi[r]; vi[r] = vi[p]; vi[p] = t;
+                    }
+                }
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            xr[(size_t)i * ldb] = vr[i];
+            xi[(size_t)i * ldb] = vi[i];
+        }
+        __syncthreads();
+        trsv_diag<false>(Ar, Ai, lda, xr, xi, ldb, 0, min(n, kTB), s_tr, s_ti, s_xr, s_xi);
+    } else {
+        const int last = (n - 1) / kTB;
+        trsv_diag<true>(Ar, Ai, lda, xr, xi, ldb, last * kTB, n, s_tr, s_ti, s_xr, s_xi);
+    }
+}
+
+// Block step: x of block `blk` is final.  Lower: CTA 0 updates and solves
+// block blk+1, CTAs >= 1 update rows from block blk+2 on.  Upper: CTA 0
+// updates and solves block blk-1, CTAs >= 1 update rows before block blk-1.
+template <bool UPPER>
+__global__ void __launch_bounds__(kTrsvThreads) k_trsv_step(int n, const float *lu_re, const float *lu_im,
+                                                            long long lda, long long a_stride, float *b_re,
+                                                            float *b_im, long long ldb, long long b_stride, int blk) {
+    __shared__ float s_fr[kTB], s_fi[kTB];
+    __shared__ float s_tr[32 * 33], s_ti[32 * 33], s_xr[32], s_xi[32];
+    const int mat = blockIdx.z, rhs = blockIdx.y;
+    const float *Ar = lu_re + (size_t)mat * a_stride, *Ai = lu_im + (size_t)mat * a_stride;
+    float *xr = b_re + (size_t)mat * b_stride + rhs, *xi = b_im + (size_t)mat * b_stride + rhs;
+    const int f0 = blk * kTB, f1 = min(n, f0 + kTB), fw = f1 - f0;
+    for (int c = threadIdx.x; c < kTB; c += blockDim.x) {
+        s_fr[c] = c < fw ? xr[(size_t)(f0 + c) * ldb] : 0.f;
+        s_fi[c] = c < fw ? xi[(size_t)(f0 + c) * ldb] : 0.f;
+    }
+    __syncthreads();
+    int g0, g1, o0, o1;  // next diagonal block, other rows
+    if (!UPPER) {
+        g0 = f1; g1 = min(n, g0 + kTB); o0 = g1; o1 = n;
+    } else {
+        g1 = f0; g0 = max(0, g1 - kTB); o0 = 0; o1 = g0;
+    }
+    if (blockIdx.x == 0) {
+        trsv_apply(Ar, Ai, lda, xr, xi, ldb, f0, fw, g0, g1, s_fr, s_fi);
+        __syncthreads();
+        trsv_diag<UPPER>(Ar, Ai, lda, xr, xi, ldb, g0, g1, s_tr, s_ti, s_xr, s_xi);
+    } else {
+        const int r0 = o0 + (blockIdx.x - 1) * kTrsvRows;
+        const int r1 = min(o1, r0 + kTrsvRows);
+        if (r0 < r1) trsv_apply(Ar, Ai, lda, xr, xi, ldb, f0, fw, r0, r1, s_fr, s_fi);
+    }
+}
+
+int lu_solve_blocked(int n, int nrhs, int batch, const float *lu_re, const float *lu_im, long long lda,
+                     long long a_stride, const int *piv, long long piv_stride, float *b_re, float *b_im,
+                     long long ldb, long long b_stride, cudaStream_t st) {
+    const size_t smem = (size_t)n * 2 * sizeof(float);
+    static bool attr = false;
+    if (!attr) {
+        HBEM_CUDA(cudaFuncSetAttribute(k_trsv_first<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        attr = true;
+    }
+    const int nblk = (n + kTB - 1) / kTB;
+    k_trsv_first<false><<<dim3(nrhs, batch), kTrsvThreads, smem, st>>>(n, lu_re, lu_im, lda, a_stride, piv, piv_stride,
+                                                                       b_re, b_im, ldb, b_stride);
+    HBEM_LAUNCH_CHECK("k_trsv_first");
+    for (int blk = 0; blk + 1 < nblk; ++blk) {
+        const int rest = std::max(0, n - (blk + 2) * kTB);
+        const int ctas = 1 + (rest + kTrsvRows - 1) / kTrsvRows;
+        k_trsv_step<false><<<dim3(ctas, nrhs, batch), kTrsvThreads, 0, st>>>(n, lu_re, lu_im, lda, a_stride, b_re, b_im,
+                                                                            ldb, b_stride, blk);
+        HBEM_LAUNCH_CHECK("k_trsv_step");
+    }
+    k_trsv_first<true><<<dim3(nrhs, batch), kTrsvThreads, 0, st>>>(n, lu_re, lu_im, lda, a_stride, piv, piv_stride,
+                                                                   b_re, b_im, ldb, b_stride);
+    HBEM_LAUNCH_CHECK("k_trsv_first");
+    for (int blk = nblk - 1; blk > 0; --blk) {
+        const int rest = std::max(0, (blk - 1) * kTB);
+        const int ctas = 1 + (rest + kTrsvRows - 1) / kTrsvRows;
+        k_trsv_step<true><<<dim3(ctas, nrhs, batch), kTrsvThreads, 0, st>>>(n, lu_re, lu_im, lda, a_stride, b_re, b_im,
+                                                                           ldb, b_stride, blk);
+        HBEM_LAUNCH_CHECK("k_trsv_step");
+    }
+    return HBEM_OK;
+}
+
 // FP64 residual r = b - A x (one warp per row), and per-matrix norms.
 __global__ void __launch_bounds__(256) k_residual(int n, const float *a_re, const float *a_im, long long lda,
                                                   long long a_stride, const float *b_re, const float *b_im,
@@ -582,6 +961,35 @@ __global__ void k_axpy_active(int n, float *x_re, float *x_im, long long x_strid
 
 }  // namespace
 
+template <int CS>
+int launch_panel_cluster_t(float *a_re, float *a_im, long long lda, long long a_stride, int n, int c, int w, int *piv,
+                           long long piv_stride, int *info, int batch, int R, size_t smem, cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+        HBEM_CUDA(cudaFuncSetAttribute(k_panel_cluster<CS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(200 * 1024)));
+        attr = true;
+    }
+    k_panel_cluster<CS><<<dim3(CS, batch), kPanelThreads, smem, st>>>(a_re, a_im, lda, a_stride, n, c, w, R, piv,
+                                                                      piv_stride, info);
+    HBEM_LAUNCH_CHECK("k_panel_cluster");
+    return HBEM_OK;
+}
+
+int launch_panel_cluster(float *a_re, float *a_im, long long lda, long long a_stride, int n, int c, int w, int *piv,
+                         long long piv_stride, int *info, int batch, size_t smem_cap, cudaStream_t st) {
+    const int m = n - c;
+    const size_t row_bytes = (size_t)(w + 1) * 8;
+    const int rows_cap = (int)(smem_cap / row_bytes);
+    int cs = 2;
+    while (cs < 8 && (long long)cs * rows_cap < m) cs *= 2;
+    int R = (m + cs - 1) / cs;
+    if (R < 32) R = 32;  // row j (< 32) always lives in CTA 0
+    const size_t smem = (size_t)R * row_bytes;
+    if (cs == 2) return launch_panel_cluster_t<2>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info, batch, R, smem, st);
+    if (cs == 4) return launch_panel_cluster_t<4>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info, batch, R, smem, st);
+    return launch_panel_cluster_t<8>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info, batch, R, smem, st);
+}
+
 int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long long a_stride, int *piv,
               long long piv_stride, int *info, int precision, cudaStream_t st) {
     // Two-level blocking: 64-column blocks whose (n - b0) x 64 panel is
@@ -623,15 +1031,21 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
     HBEM_CUDA(cudaFuncSetAttribute(k_swap_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSwapSmem));
     for (int b0 = 0; b0 < n; b0 += NB) {
         const int bw = std::min(NB, n - b0);
-        const int nbi = ((size_t)(n - b0) * 33 * 8 <= smem_cap) ? 32 : 16;
+        // inner width 32 while an 8-CTA cluster can hold the panel, else 16
+        const int nbi = ((size_t)(n - b0) <= 8 * (smem_cap / (33 * 8))) ? 32 : 16;
         for (int c = b0; c < b0 + bw; c += nbi) {
             const int w = std::min(nbi, b0 + bw - c);
             const size_t psmem = (size_t)(n - c) * (w + 1) * 8;
-            if (psmem <= smem_cap)
+            if (psmem <= smem_cap) {
                 k_panel<true><<<batch, kPanelThreads, psmem, st>>>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info);
-            else
+                HBEM_LAUNCH_CHECK("k_panel");
+            } else if ((size_t)(n - c) <= 8 * (smem_cap / ((size_t)(w + 1) * 8))) {
+                int rc = launch_panel_cluster(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info, batch, smem_cap, st);
+                if (rc != HBEM_OK) return finish(rc);
+            } else {
                 k_panel<false><<<batch, kPanelThreads, 0, st>>>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info);
-            HBEM_LAUNCH_CHECK("k_panel");
+                HBEM_LAUNCH_CHECK("k_panel");
+            }
             const int other = bw - w;  // block columns outside this sub-panel
             if (other > 0) {
                 dim3 grid((other + kSwapCols - 1) / kSwapCols, batch);
@@ -666,6 +1080,8 @@ int lu_solve(int n, int nrhs, int batch, const float *lu_re, const float *lu_im,
     const size_t smem = (size_t)n * 2 * sizeof(float);
     if (smem > 200 * 1024) return fail(HBEM_ERR_ARG, "hbem_lu_solve: n too large for the staged solve");
     dim3 grid(nrhs, batch);
+    if (trans == HBEM_TRANS_N && n > kTB)
+        return lu_solve_blocked(n, nrhs, batch, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re, b_im, ldb, b_stride, st);
     if (trans == HBEM_TRANS_N) {
         HBEM_CUDA(cudaFuncSetAttribute(k_getrs<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_getrs<0><<<grid, 512, smem, st>>>(n, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re, b_im, ldb, b_stride, nrhs);
@@ -774,3 +1190,4 @@ extern "C" int hbem_refine(int n, int batch, const float *a_re, const float *a_i
     return refine(n, batch, a_re, a_im, lda, a_stride, lu_re, lu_im, lu_stride, piv, piv_stride, b_re, b_im, b_stride,
                   x_re, x_im, x_stride, tol, max_iter, iters, resid, reinterpret_cast<cudaStream_t>(stream));
 }
+
