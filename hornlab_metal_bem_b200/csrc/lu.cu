@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <cmath>
 #include <string>
 
@@ -1151,6 +1152,111 @@ int refine(int n, int batch, const float *a_re, const float *a_im, long long lda
     return rc;
 }
 
+// ---------------------------------------------------------------------------
+// Refinement without allocation.  The scratch of hbem_refine (correction
+// vectors, FP64 norm accumulators, active flags) lives in one fixed
+// module-scope device array instead of stream-ordered allocations, for
+// callers that may not allocate device memory: a process whose memory is
+// held by another caching allocator (a cudaMallocAsync from the default pool
+// can then fail although the host framework has room cached), or a hot loop
+// that must never enter an allocator.  Sizes: batch <= kNoAllocMaxBatch and
+// batch * x_stride <= kNoAllocMaxElems complex elements (4 MiB of vectors).
+// Every call, on any stream or thread, shares this one array per device, so
+// calls must not overlap; the array keeps the last call's contents, and the
+// norms are cleared by each pass before they accumulate.
+// ---------------------------------------------------------------------------
+constexpr long long kNoAllocMaxElems = 1LL << 19;
+constexpr int kNoAllocMaxBatch = 256;
+constexpr size_t kNoAllocVecBytes = sizeof(float) * (size_t)kNoAllocMaxElems;  // one of re / im
+constexpr size_t kNoAllocNormOff = 2 * kNoAllocVecBytes;
+constexpr size_t kNoAllocActiveOff = kNoAllocNormOff + sizeof(double) * 2 * kNoAllocMaxBatch;
+constexpr size_t kNoAllocBytes = kNoAllocActiveOff + sizeof(int) * kNoAllocMaxBatch;
+
+static __device__ __align__(256) unsigned char g_refine_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+static std::mutex g_noalloc_mu;
+static unsigned char *g_noalloc_ptr[kNoAllocMaxDevices];
+
+// Device address of the scratch array on the current device.  The first call
+// on a device looks the symbol up (which may load the module there).
+static int noalloc_scratch(unsigned char **out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "hbem_refine_noalloc: cudaGetDevice");
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(HBEM_ERR_ARG, "hbem_refine_noalloc: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_refine_scratch);
+        if (e != cudaSuccess || !p) return cuda_fail(e, "hbem_refine_noalloc: cudaGetSymbolAddress");
+        g_noalloc_ptr[dev] = static_cast<unsigned char *>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return HBEM_OK;
+}
+
+int refine_noalloc(int n, int batch, const float *a_re, const float *a_im, long long lda, long long a_stride,
+                   const float *lu_re, const float *lu_im, long long lu_stride, const int *piv, long long piv_stride,
+                   const float *b_re, const float *b_im, long long b_stride, float *x_re, float *x_im,
+                   long long x_stride, double tol, int max_iter, int *iters, double *resid, cudaStream_t st) {
+    if (batch > kNoAllocMaxBatch)
+        return fail(HBEM_ERR_ARG, "hbem_refine_noalloc: batch exceeds the fixed scratch limit of 256 matrices");
+    if ((long long)batch * x_stride > kNoAllocMaxElems)
+        return fail(HBEM_ERR_ARG,
+                    "hbem_refine_noalloc: batch * x_stride exceeds the fixed scratch limit of 524288 complex elements");
+    unsigned char *base = nullptr;
+    int rc = noalloc_scratch(&base);
+    if (rc != HBEM_OK) return rc;
+    float *dr = reinterpret_cast<float *>(base);
+    float *di = reinterpret_cast<float *>(base + kNoAllocVecBytes);
+    double *norms = reinterpret_cast<double *>(base + kNoAllocNormOff);
+    int *active = reinterpret_cast<int *>(base + kNoAllocActiveOff);
+    double h_norms[2 * kNoAllocMaxBatch];
+    int h_active[kNoAllocMaxBatch], h_iters[kNoAllocMaxBatch];
+    double h_res[kNoAllocMaxBatch];
+    for (int m = 0; m < batch; ++m) {
+        h_active[m] = 1;
+        h_iters[m] = 0;
+        h_res[m] = 0.0;
+    }
+    for (int it = 0; it <= max_iter && rc == HBEM_OK; ++it) {
+        cudaError_t e = cudaMemsetAsync(norms, 0, sizeof(double) * 2 * batch, st);
+        if (e != cudaSuccess) { rc = cuda_fail(e, "hbem_refine_noalloc: memset"); break; }
+        dim3 g((n * 32 + 255) / 256, batch);
+        k_residual<<<g, 256, 0, st>>>(n, a_re, a_im, lda, a_stride, b_re, b_im, b_stride, x_re, x_im, x_stride, dr, di, norms);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) { rc = cuda_fail(e, "k_residual"); break; }
+        count_launch();
+        e = cudaMemcpyAsync(h_norms, norms, sizeof(double) * 2 * batch, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) { rc = cuda_fail(e, "hbem_refine_noalloc: sync"); break; }
+        bool any = false;
+        for (int m = 0; m < batch; ++m) {
+            const double rel = h_norms[2 * m + 1] > 0 ? std::sqrt(h_norms[2 * m] / h_norms[2 * m + 1]) : 0.0;
+            h_res[m] = rel;
+            h_active[m] = (h_active[m] && rel > tol && it < max_iter) ? 1 : 0;
+            if (h_active[m]) { ++h_iters[m]; any = true; }
+        }
+        if (!any) break;
+        e = cudaMemcpyAsync(active, h_active, sizeof(int) * batch, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) { rc = cuda_fail(e, "hbem_refine_noalloc: copy"); break; }
+        rc = lu_solve(n, 1, batch, lu_re, lu_im, lda, lu_stride, piv, piv_stride, dr, di, 1, x_stride, HBEM_TRANS_N, st);
+        if (rc != HBEM_OK) break;
+        k_axpy_active<<<dim3((n + 255) / 256, batch), 256, 0, st>>>(n, x_re, x_im, x_stride, dr, di, active);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) { rc = cuda_fail(e, "k_axpy_active"); break; }
+        count_launch();
+    }
+    if (rc == HBEM_OK && iters) {
+        cudaError_t e = cudaMemcpyAsync(iters, h_iters, sizeof(int) * batch, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess && resid) e = cudaMemcpyAsync(resid, h_res, sizeof(double) * batch, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) rc = cuda_fail(e, "hbem_refine_noalloc: results");
+    }
+    return rc;
+}
+
 }  // namespace hbem
 
 using namespace hbem;
@@ -1191,3 +1297,17 @@ extern "C" int hbem_refine(int n, int batch, const float *a_re, const float *a_i
                   x_re, x_im, x_stride, tol, max_iter, iters, resid, reinterpret_cast<cudaStream_t>(stream));
 }
 
+extern "C" int hbem_refine_noalloc(int n, int batch, const float *a_re, const float *a_im, long long lda,
+                                   long long a_stride, const float *lu_re, const float *lu_im, long long lu_stride,
+                                   const int *piv, long long piv_stride, const float *b_re, const float *b_im,
+                                   long long b_stride, float *x_re, float *x_im, long long x_stride, double tol,
+                                   int max_iter, int *iters, double *resid, void *stream) {
+    if (n <= 0 || batch <= 0) return HBEM_OK;
+    if (!a_re || !a_im || !lu_re || !lu_im || !piv || !b_re || !b_im || !x_re || !x_im)
+        return fail(HBEM_ERR_ARG, "hbem_refine_noalloc: NULL pointer");
+    if (x_stride < n || b_stride < n || max_iter < 0 || !(tol > 0))
+        return fail(HBEM_ERR_ARG, "hbem_refine_noalloc: bad arguments");
+    return refine_noalloc(n, batch, a_re, a_im, lda, a_stride, lu_re, lu_im, lu_stride, piv, piv_stride, b_re, b_im,
+                          b_stride, x_re, x_im, x_stride, tol, max_iter, iters, resid,
+                          reinterpret_cast<cudaStream_t>(stream));
+}

@@ -155,6 +155,28 @@ int hbem_refine(int n, int batch, const float *a_re, const float *a_im, long lon
                 double tol, int max_iter, int *iters, double *resid, void *stream);
 
 /*
+ * hbem_refine without any device allocation: same arguments, same results.
+ * No counterpart in the reference, which allocates nothing on a device.
+ * For callers that may not allocate device memory, such as a process whose
+ * device memory is held by another caching allocator (a stream-ordered
+ * allocation inside hbem_refine can then fail), or a loop that must never
+ * enter an allocator.  Its scratch is one fixed device array of 4 MiB per
+ * device, in this library's module.  Limits: batch <= 256 and
+ * batch * x_stride <= 524288 complex elements; larger calls return
+ * HBEM_ERR_ARG.  The first call on each device looks the array up (and may
+ * load the module there), so make it before any stream capture.  Every call
+ * shares the array, which keeps the last call's contents: calls on different
+ * streams or threads that overlap in time race and give wrong results;
+ * serialise them.
+ */
+int hbem_refine_noalloc(int n, int batch, const float *a_re, const float *a_im, long long lda, long long a_stride,
+                        const float *lu_re, const float *lu_im, long long lu_stride,
+                        const int *piv, long long piv_stride,
+                        const float *b_re, const float *b_im, long long b_stride,
+                        float *x_re, float *x_im, long long x_stride,
+                        double tol, int max_iter, int *iters, double *resid, void *stream);
+
+/*
  * Exterior field p(x_o) = sum_tri sum_q w [dG/dn_y p(y_q) - G q_tri] (+ images)
  * for n_freq cases at once.  Replaces: evaluate_field_regular / evaluateExterior
  *   (main.swift:4135-4203, 8312-8424; Python forces the GPU field,
