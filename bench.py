@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=["c2", "c1"], default="c2")
+    ap.add_argument("--workload", choices=["c2", "c1", "c4"], default="c2")
     ap.add_argument("--precision", choices=["plain", "mixed"], default="plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -79,6 +79,15 @@ def workload(name: str):
         )
         desc = (f"C2 yz+xz quarter exponential horn (seed 0: flare {spec.flare:.2f} 1/m, lip {spec.lip * 1e3:.2f} mm), "
                 "40 log freqs 0.5-20 kHz, 3x37 obs @ 2 m")
+    elif name == "c4":
+        spec = G.horn_spec_from_seed(0, edge=0.004)
+        mesh = G.baffled_horn(spec, aperture_tag=12)
+        cfg = hb.native_config(
+            freq_min_hz=1000.0, freq_max_hz=20000.0, freq_count=20, source_motion="axial", aperture_tag=12,
+            observation=hb.ObservationConfig(planes=["horizontal", "vertical", "diagonal"], angle_count=37),
+        )
+        desc = (f"C4 coupled infinite-baffle horn, full (no symmetry), edge 4 mm (seed 0: flare {spec.flare:.2f} 1/m), "
+                "aperture tag 12 at z=0, 20 log freqs 1-20 kHz, 3x37 obs @ 2 m")
     else:
         mesh = G.icosphere(3, 0.1)
         cfg = hb.native_config(freq_min_hz=200.0, freq_max_hz=5000.0, freq_count=8, velocity_mode="velocity",
@@ -94,8 +103,9 @@ def workload(name: str):
     scale = build_source_face_scale(mesh.grid, mesh.physical_tags, cfg, frame.axis, frame.source_center)
     q = neumann_rows(buf.n_triangles, mesh.physical_tags, freqs, cfg, scale)
     sym = {None: 0, "yz+xz": 3}[cfg.native_symmetry_plane]
+    q_kf = k_re.copy() if cfg.aperture_tag is not None else None  # Rayleigh field at the real wavenumber
     return dict(name=name, desc=desc, mesh=mesh, cfg=cfg, buf=buf, freqs=freqs, k_re=k_re, k_im=k_im, q=q,
-                obs=field_points_3xn(obs), tags=sorted(cfg.velocity_sources), sym=sym)
+                obs=field_points_3xn(obs), tags=sorted(cfg.velocity_sources), sym=sym, kf=q_kf)
 
 
 # --------------------------------------------------------------------------- helpers
@@ -395,11 +405,158 @@ def run_b200(args, w):
         dist.destroy_process_group()
 
 
+def run_b200_c4(args, w):
+    """Coupled infinite-baffle sweep (augmented system, N = n + m unknowns) through
+    ``NativeSession.coupled_ib_batch``; accuracy against an FP64 GPU solve of the
+    same assembled system on two of the frequencies."""
+    import torch
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from hornlab_metal_bem_b200.native import NativeSession, _np_ptr, _stream_ptr, _t_ptr, check, load_library
+    from hornlab_metal_bem_b200.sweep import directivity_from_pressure
+
+    lib = load_library()
+    buf, cfg = w["buf"], w["cfg"]
+    F = len(w["freqs"])
+    sess = NativeSession(buf, aperture_tag=cfg.aperture_tag, velocity_source_tags=w["tags"])
+    n, m = sess.n_dof, sess.m_aperture
+    N = n + m
+    kw = dict(source_tags=w["tags"], impedance_source_tag=min(w["tags"]), precision=args.precision,
+              refine_tolerance=1e-6, field_k_f32=w["kf"], write_surface_pressure=True)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        t = {}
+        res = sess.coupled_ib_batch(w["freqs"], w["k_re"], w["q"], w["obs"], k_imag_f32=w["k_im"], timings_out=t, **kw)
+        return res, t
+
+    for _ in range(args.warmup):
+        res, _t = step()
+    torch.cuda.synchronize()
+    if any(r.lapack_info != 0 for r in res):
+        raise RuntimeError("zero pivot in the coupled benchmark workload")
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    clocks = Clocks(uuid)
+    launches0 = lib.hbem_launch_count()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    stages = []
+    for _ in range(args.steps):
+        res, t = step()
+        stages.append(t)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clk = clocks.stop()
+    launches = lib.hbem_launch_count() - launches0
+    e2e_ms = e0.elapsed_time(e1)
+    dev_ms = sum(t["assembly_ms"] + t["solve_ms"] + t["field_ms"] for t in stages)
+    if dist is not None:
+        tt = torch.tensor([e2e_ms, dev_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms, dev_ms = (float(v) for v in tt.tolist())
+    stage = {k: statistics.median(t[k] for t in stages) for k in ("assembly_ms", "solve_ms", "field_ms")}
+
+    # ---- accuracy against an FP64 GPU solve of the same FP32-assembled system
+    picks = [0, F - 1]
+    Kr, Ki, rr, ri, alpha = sess.coupled_ib_system(w["k_re"][picks], None if w["k_im"] is None else w["k_im"][picks],
+                                            w["kf"][picks], w["q"][picks])
+    K = torch.complex(Kr.double(), Ki.double())
+    del Kr, Ki
+    x64 = torch.linalg.solve(K, torch.complex(rr.double(), ri.double()).unsqueeze(-1)).squeeze(-1)
+    del K
+    qa = (x64[:, :m] * alpha.double()[:, None]).to(torch.complex64).contiguous()
+    qa_r, qa_i = qa.real.contiguous(), qa.imag.contiguous()
+    obs_t = torch.tensor(np.ascontiguousarray(w["obs"], dtype=np.float32), device="cuda")
+    n_obs = obs_t.shape[1]
+    fr = torch.empty((len(picks), n_obs), dtype=torch.float32, device="cuda")
+    fi = torch.empty_like(fr)
+    kf_p = np.ascontiguousarray(w["kf"][picks], dtype=np.float32)
+    check(lib.hbem_coupled_ib_field(sess.handle, len(picks), _np_ptr(kf_p), None, None, None, None, _t_ptr(obs_t),
+                                    n_obs, _t_ptr(qa_r), _t_ptr(qa_i), _t_ptr(fr), _t_ptr(fi), _stream_ptr()),
+          "hbem_coupled_ib_field", lib)
+    p64 = x64[:, m:].cpu().numpy()
+    f64 = (fr.cpu().numpy() + 1j * fi.cpu().numpy())
+    n_planes = len(cfg.observation.planes)
+    oc = cfg.observation
+    angles = np.linspace(oc.angle_min_deg, oc.angle_max_deg, oc.angle_count)
+    axis_idx = int(np.argmin(np.abs(angles)))
+    errs = []
+    for j, f in enumerate(picks):
+        ps = res[f].surface_pressure
+        rel = float(np.linalg.norm(ps - p64[j]) / np.linalg.norm(p64[j]))
+        d_ref = directivity_from_pressure(f64[j].reshape(n_planes, -1), axis_idx)
+        d_got = directivity_from_pressure(np.asarray(res[f].field).reshape(n_planes, -1), axis_idx)
+        front = angles <= 90.0
+        ddb = float(np.max(np.abs(d_got[:, front] - d_ref[:, front])))
+        errs.append({"frequency_hz": float(w["freqs"][f]), "surface_pressure_rel_l2": rel,
+                     "directivity_db_max_abs_0_90deg": ddb})
+
+    # ---- roofline of the dominant stage: the LU of the N x N systems
+    peaks = measured_peaks()
+    clk_mhz = peaks.get("sm_max_mhz", 1965.0)
+    lu_flops = F * (8.0 / 3.0) * N ** 3
+    achieved = lu_flops / (stage["solve_ms"] * 1e-3) / 1e12
+    if args.precision == "mixed":
+        peak, pk_src = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops", 1590.0))), \
+            f"cuBLAS bf16 dense, sustained ({peaks['source']}); BF16x3 issues 3 bf16 products per FP32 product"
+    else:
+        peak = N_SM * FP32_LANES_PER_SM * 2 * clk_mhz * 1e6 / 1e12
+        pk_src = f"148 SM x 128 FP32 lanes x 2 x {clk_mhz:.0f} MHz"
+    line = {
+        "metric": "freq-solves/s", "value": world * F * args.steps / (dev_ms * 1e-3), "unit": "freq-solves/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64 (f32 planar)",
+        "data": "synthetic",
+        "config": {"workload": w["desc"], "n_dof": n, "n_triangles": buf.n_triangles, "aperture_triangles": m,
+                   "unknowns": N, "n_freq": F, "n_obs": n_obs, "precision": args.precision,
+                   "coupled_solve": res[0].diagnostics["ib_coupled_solve"],
+                   "parallelism": f"replicas x{world} (frequency-parallel)",
+                   "l2": f"working set {F * N * N * 8 / 1e9:.1f} GB of dense matrices > 126 MB L2"},
+        "e2e": {"value": world * F * args.steps / (e2e_ms * 1e-3), "unit": "freq-solves/s",
+                "h2d_bytes_per_step": F * buf.n_triangles * 8 + 3 * n_obs * 4 + F * 8,
+                "d2h_bytes_per_step": F * (n_obs * 8 + n * 8 + m * 8) + F * 16},
+        "gpu_launches": int(launches),
+        "stages_ms_per_step": stage,
+        "refine_iterations": [int(r.diagnostics["refine_iterations"]) for r in res],
+        "accuracy_vs_fp64_gpu_solve": errs,
+        "clocks": clk,
+        "roofline": {"kernel": "batched LU + solve of the augmented systems", "bound": "tensor" if args.precision == "mixed" else "fp32",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                     "algorithmic": f"(8/3) N^3 real flops per system, N = {N}, {F} systems", "peak_source": pk_src},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sess.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     w = workload(args.workload)
     if args.impl == "reference":
         run_reference(args, w)
+    elif args.workload == "c4":
+        run_b200_c4(args, w)
     else:
         run_b200(args, w)
 

@@ -7,7 +7,11 @@
 // (an n x n x m product).  Here P_avg is applied as a sparse scatter instead:
 // X = S_ia (2 S_aa)^-1 (n x m x m), then A[:, d] -= X[:, r] / 3 for the three
 // dofs d of every aperture face r -- the same matrix with n/m times fewer
-// flops.
+// flops.  For large apertures (m comparable to n, where forming (2 S_aa)^-1
+// costs more than the solve) the reference's augmented twin
+// (main.swift:7504-7595) is used instead: one (m + n) system
+//   [[-2 S_aa, P_avg], [-S_ia, A]] [q_a; p] = [0; b]
+// built by k_ib_augment and factored by the batched LU.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -223,6 +227,84 @@ __global__ void k_ib_scatter(float *a_re, float *a_im, long long a_stride, const
     }
 }
 
+// Per-frequency max |re|, |im| of the three blocks that set the scaling of the
+// augmented system: mx[3 f + 0] = A block of K, + 1 = S_ia, + 2 = S_aa
+// (non-negative floats order like their bit patterns, so atomicMax on the
+// bits is exact).
+__global__ void k_ib_block_max(const float *k_re, const float *k_im, long long ldk, long long k_stride,
+                               const float *sia_re, const float *sia_im, const float *saa_re, const float *saa_im,
+                               int n, int m, unsigned *mx) {
+    const int f = blockIdx.z, which = blockIdx.y;
+    float v = 0.f;
+    if (which == 0) {
+        const long long tot = (long long)n * n;
+        for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot; e += (long long)gridDim.x * blockDim.x) {
+            const long long r = e / n, c = e - r * n;
+            const size_t o = (size_t)f * k_stride + (size_t)(m + r) * ldk + (m + c);
+            v = fmaxf(v, fmaxf(fabsf(k_re[o]), fabsf(k_im[o])));
+        }
+    } else {
+        const long long tot = which == 1 ? (long long)n * m : (long long)m * m;
+        const float *xr = which == 1 ? sia_re + (size_t)f * tot : saa_re + (size_t)f * tot;
+        const float *xi = which == 1 ? sia_im + (size_t)f * tot : saa_im + (size_t)f * tot;
+        for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot; e += (long long)gridDim.x * blockDim.x)
+            v = fmaxf(v, fmaxf(fabsf(xr[e]), fabsf(xi[e])));
+    }
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0 && v > 0.f) atomicMax(mx + 3 * f + which, __float_as_uint(v));
+}
+
+// Block scaling of the augmented system: q_a = alpha q~ (columns < m times
+// alpha) and the aperture rows times beta, with alpha = max|A| / max|S_ia|,
+// beta = max|A| / (alpha max|2 S_aa|): the unscaled system mixes entries
+// ~1e-4 (S_aa), 1/3 (P_avg), ~1e-6 (A) and ~1e-8 (S_ia), which inflates its
+// condition number by orders of magnitude over the Schur complement's.
+__device__ __forceinline__ void ib_scales(const unsigned *mx, int f, float &alpha, float &beta) {
+    const float a = __uint_as_float(mx[3 * f]), sia = __uint_as_float(mx[3 * f + 1]), saa = __uint_as_float(mx[3 * f + 2]);
+    alpha = (a > 0.f && sia > 0.f) ? a / sia : 1.f;
+    beta = (a > 0.f && saa > 0.f) ? a / (2.f * alpha * saa) : 1.f;
+}
+
+// Augmented coupled matrix K (N = m + n, row-major, ldk): rows r < m are
+// beta [-2 alpha S_aa[r, :] | P_avg[r, :]] (P_avg: 1/3 on the three dofs of
+// aperture face r), rows m + i take -alpha S_ia[i, :] in columns < m; the A
+// block (columns >= m) is assembled in place by hbem_assemble.
+__global__ void k_ib_augment(const float *sia_re, const float *sia_im, const float *saa_re, const float *saa_im,
+                             float *k_re, float *k_im, long long ldk, long long k_stride, const int *ap,
+                             const int *l2g, int n, int m, const unsigned *mx, float *alpha_out) {
+    const int f = blockIdx.z, row = blockIdx.y;
+    const long long N = (long long)n + m;
+    float alpha, beta;
+    ib_scales(mx, f, alpha, beta);
+    if (row == 0 && blockIdx.x == 0 && threadIdx.x == 0) alpha_out[f] = alpha;
+    float *kr = k_re + (size_t)f * k_stride + (size_t)row * ldk, *ki = k_im + (size_t)f * k_stride + (size_t)row * ldk;
+    if (row < m) {
+        const float *sr = saa_re + (size_t)f * m * m + (size_t)row * m, *si = saa_im + (size_t)f * m * m + (size_t)row * m;
+        const int t = ap[row];
+        const int d0 = l2g[3 * t], d1 = l2g[3 * t + 1], d2 = l2g[3 * t + 2];
+        const float s_aa = -2.f * alpha * beta, s_p = beta * (1.0f / 3.0f);
+        for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N; c += (long long)gridDim.x * blockDim.x) {
+            float vr, vi = 0.f;
+            if (c < m) {
+                vr = s_aa * sr[c];
+                vi = s_aa * si[c];
+            } else {
+                const int d = (int)(c - m);
+                vr = (d == d0 || d == d1 || d == d2) ? s_p : 0.f;
+            }
+            kr[c] = vr;
+            ki[c] = vi;
+        }
+    } else {
+        const int i = row - m;
+        const float *sr = sia_re + (size_t)f * n * m + (size_t)i * m, *si = sia_im + (size_t)f * n * m + (size_t)i * m;
+        for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < m; c += gridDim.x * blockDim.x) {
+            kr[c] = -alpha * sr[c];
+            ki[c] = -alpha * si[c];
+        }
+    }
+}
+
 // q_a = M (P_avg p): one warp per aperture row
 __global__ void k_ib_qa(const float *p_re, const float *p_im, int n, const float *m_re, const float *m_im, int m,
                         const int *ap, const int *l2g, float *qa_re, float *qa_im) {
@@ -423,14 +505,18 @@ extern "C" int hbem_coupled_ib_field(hbem_session *h, int n_freq, const float *k
     if (!s) return fail(HBEM_ERR_ARG, "hbem_coupled_ib_field: NULL session");
     if (s->m_ap <= 0) return fail(HBEM_ERR_STATE, "hbem_coupled_ib_field: no aperture set");
     if (n_freq <= 0) return HBEM_OK;
-    if (!kf_re || !p_re || !p_im || !minv_re || !minv_im || !qa_re || !qa_im || (n_obs > 0 && (!obs_3xn || !out_re || !out_im)))
+    const bool qa_given = !minv_re && !minv_im;
+    if (!kf_re || !qa_re || !qa_im || (!qa_given && (!p_re || !p_im || !minv_re || !minv_im)) ||
+        (n_obs > 0 && (!obs_3xn || !out_re || !out_im)))
         return fail(HBEM_ERR_ARG, "hbem_coupled_ib_field: NULL pointer");
     HBEM_CUDA(cudaSetDevice(s->device));
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     const int m = s->m_ap;
-    k_ib_qa<<<dim3((m + 7) / 8, n_freq), 256, 0, st>>>(p_re, p_im, s->n_dof, minv_re, minv_im, m, s->d_ap_tris,
-                                                       s->d_l2g, qa_re, qa_im);
-    HBEM_LAUNCH_CHECK("k_ib_qa");
+    if (!qa_given) {
+        k_ib_qa<<<dim3((m + 7) / 8, n_freq), 256, 0, st>>>(p_re, p_im, s->n_dof, minv_re, minv_im, m, s->d_ap_tris,
+                                                           s->d_l2g, qa_re, qa_im);
+        HBEM_LAUNCH_CHECK("k_ib_qa");
+    }
     if (n_obs <= 0) return HBEM_OK;
     for (int f0 = 0; f0 < n_freq; f0 += 64) {
         const int nf = std::min(64, n_freq - f0);
@@ -441,4 +527,42 @@ extern "C" int hbem_coupled_ib_field(hbem_session *h, int n_freq, const float *k
         HBEM_LAUNCH_CHECK("k_rayleigh");
     }
     return HBEM_OK;
+}
+
+extern "C" int hbem_coupled_ib_augment(hbem_session *h, int n_freq, const float *sia_re, const float *sia_im,
+                                       const float *saa_re, const float *saa_im, float *k_re, float *k_im,
+                                       long long ldk, long long k_stride, float *alpha, void *stream) {
+    Session *s = reinterpret_cast<Session *>(h);
+    if (!s) return fail(HBEM_ERR_ARG, "hbem_coupled_ib_augment: NULL session");
+    if (s->m_ap <= 0) return fail(HBEM_ERR_STATE, "hbem_coupled_ib_augment: no aperture set");
+    if (n_freq <= 0) return HBEM_OK;
+    if (!sia_re || !sia_im || !saa_re || !saa_im || !k_re || !k_im || !alpha)
+        return fail(HBEM_ERR_ARG, "hbem_coupled_ib_augment: NULL pointer");
+    const long long n = s->n_dof, m = s->m_ap, N = n + m;
+    if (ldk < N || k_stride < ldk * N) return fail(HBEM_ERR_ARG, "hbem_coupled_ib_augment: bad strides");
+    HBEM_CUDA(cudaSetDevice(s->device));
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    unsigned *mx = nullptr;
+    HBEM_CUDA(cudaMallocAsync((void **)&mx, sizeof(unsigned) * 3 * n_freq, st));
+    int rc = HBEM_OK;
+    cudaError_t e = cudaMemsetAsync(mx, 0, sizeof(unsigned) * 3 * n_freq, st);
+    if (e != cudaSuccess) rc = cuda_fail(e, "hbem_coupled_ib_augment: memset");
+    if (rc == HBEM_OK) {
+        k_ib_block_max<<<dim3(256, 3, n_freq), 256, 0, st>>>(k_re, k_im, ldk, k_stride, sia_re, sia_im, saa_re, saa_im,
+                                                            (int)n, (int)m, mx);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) rc = cuda_fail(e, "k_ib_block_max");
+        else count_launch();
+    }
+    if (rc == HBEM_OK) {
+        const unsigned gx = (unsigned)std::min<long long>(16, (N + 255) / 256);
+        k_ib_augment<<<dim3(gx, (unsigned)N, n_freq), 256, 0, st>>>(sia_re, sia_im, saa_re, saa_im, k_re, k_im, ldk,
+                                                                   k_stride, s->d_ap_tris, s->d_l2g, (int)n, (int)m,
+                                                                   mx, alpha);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) rc = cuda_fail(e, "k_ib_augment");
+        else count_launch();
+    }
+    cudaFreeAsync(mx, st);
+    return rc;
 }

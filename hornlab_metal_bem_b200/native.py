@@ -38,6 +38,8 @@ HBEM_ASM_CORRECTED = 7
 HBEM_PREC_PLAIN = 0
 HBEM_PREC_MIXED = 1
 HBEM_TRANS_N, HBEM_TRANS_T, HBEM_TRANS_C = 0, 1, 2
+# aperture faces from which the coupled solve uses the augmented (m + n) system
+AUGMENTED_MIN_APERTURE = 512
 QUERY_KEYS = {
     "n_dof": 0, "n_triangles": 1, "n_pairs": 2, "coincident": 3, "edge": 4, "vertex": 5,
     "image_pairs": 6, "unique_triplets": 7, "symmetry": 8, "kernel_launches": 9,
@@ -75,6 +77,7 @@ _SIGNATURES = {
     "hbem_solve_batch": ([_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _c_int, _vp, _c_int, _c_int, _c_d, _c_int, _vp, _vp,
                           _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _c_int),
     "hbem_session_set_aperture": ([_vp, _c_int], _c_int),
+    "hbem_coupled_ib_augment": ([_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _c_ll, _c_ll, _vp, _vp], _c_int),
     "hbem_aperture_assemble": ([_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _c_int),
     "hbem_coupled_ib_schur": ([_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _c_int),
     "hbem_coupled_ib_field": ([_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _vp, _vp], _c_int),
@@ -398,31 +401,118 @@ class NativeSession:
     def coupled_ib_batch(self, frequency_hz, k_real_f32, neumann_dp0, observation_points, *, k_imag_f32=None,
                          field_k_f32=None, source_tags=None, impedance_source_tag=None,
                          write_surface_pressure=False, precision="plain", refine_tolerance=1e-6,
-                         refine_max_iterations=10, timings_out=None, **_ignored) -> list[CaseResult]:
+                         refine_max_iterations=10, timings_out=None, coupled_method="auto",
+                         max_chunk_bytes=None, **_ignored) -> list[CaseResult]:
         """Coupled interior BIE + Rayleigh half-space solve (the reference's aperture_tag path).
 
-        A - S_ia (2 S_aa)^-1 P_avg is factored per frequency; the field is the
-        Rayleigh integral of q_a = (2 S_aa)^-1 P_avg p (main.swift:1397-1444,
-        7597-7789).
+        ``coupled_method="schur"``: A - S_ia (2 S_aa)^-1 P_avg is factored per
+        frequency and the field is the Rayleigh integral of
+        q_a = (2 S_aa)^-1 P_avg p (main.swift:1397-1444, 7597-7789).
+        ``"augmented"``: the reference's augmented twin (main.swift:7504-7595),
+        one (m + n) LU giving p and q_a together; cheaper once the aperture
+        has more than a few hundred faces.  ``"auto"`` picks augmented for
+        m >= AUGMENTED_MIN_APERTURE.  Frequencies are processed in chunks that
+        fit ``max_chunk_bytes`` (default: half the free device memory).
         """
         torch = require_cuda()
         if self.m_aperture <= 0:
             raise ValueError("session has no aperture_tag")
+        if coupled_method not in ("auto", "schur", "augmented"):
+            raise ValueError("coupled_method must be 'auto', 'schur' or 'augmented'")
+        method = coupled_method
+        if method == "auto":
+            env = os.environ.get("HORNLAB_METAL_BEM_NATIVE_COUPLED_IB_SOLVE", "").strip().lower()
+            if env in ("schur", "augmented"):
+                method = env
+            else:
+                method = "augmented" if self.m_aperture >= AUGMENTED_MIN_APERTURE else "schur"
         dev = torch.device("cuda", self.device)
         freqs = np.ascontiguousarray(np.atleast_1d(frequency_hz), dtype=np.float64)
         F, n, m, T = freqs.shape[0], self.n_dof, self.m_aperture, self.n_triangles
         k_re = np.ascontiguousarray(np.atleast_1d(k_real_f32), dtype=np.float32)
         k_im = None if k_imag_f32 is None else np.ascontiguousarray(np.atleast_1d(k_imag_f32), dtype=np.float32)
         kf = k_re if field_k_f32 is None else np.ascontiguousarray(np.atleast_1d(field_k_f32), dtype=np.float32)
+        q_all = np.asarray(neumann_dp0).reshape(F, T)
         obs = np.asarray(observation_points, dtype=np.float64)
         if obs.shape[0] != 3:
             obs = obs.T
         obs_t = torch.tensor(np.ascontiguousarray(obs, dtype=np.float32), device=dev)
-        N = obs_t.shape[1]
-        st = _stream_ptr()
+        mixed = precision == "mixed"
+        N = n + m
+        if method == "augmented":
+            per_freq = 8 * (N * N * (2 if mixed else 1) + n * m + m * m + 4 * N)
+        else:
+            per_freq = 8 * (n * n * (2 if mixed else 1) + 2 * n * m + 2 * m * m + 4 * n)
+        if max_chunk_bytes is None:
+            free, _ = torch.cuda.mem_get_info(dev)
+            max_chunk_bytes = free // 2
+        chunk = int(max(1, min(F, max_chunk_bytes // per_freq)))
+        tags = list(source_tags or [])
+        want = tags + ([impedance_source_tag] if impedance_source_tag is not None and impedance_source_tag not in tags else [])
+        parts = []
+        times = np.zeros(3)
+        for f0 in range(0, F, chunk):
+            sl = slice(f0, min(F, f0 + chunk))
+            run = self._coupled_chunk_augmented if method == "augmented" else self._coupled_chunk_schur
+            parts.append(run(k_re[sl], None if k_im is None else k_im[sl], kf[sl], q_all[sl], obs_t, want,
+                             mixed, refine_tolerance, refine_max_iterations, times))
+        if timings_out is not None:
+            timings_out.update(assembly_ms=times[0], solve_ms=times[1], field_ms=times[2], coupled_method=method,
+                               frequency_chunk=chunk)
+        cat = {key: np.concatenate([pt[key] for pt in parts]) for key in parts[0] if parts[0][key] is not None}
+        out = []
+        t_asm, t_solve, t_field = times
+        for f in range(F):
+            avgs = {int(t): complex(cat["tavg"][f, j, 0], cat["tavg"][f, j, 1]) for j, t in enumerate(want)} if want else {}
+            out.append(CaseResult(
+                frequency_hz=float(freqs[f]), field=cat["field"][f],
+                impedance=avgs.get(int(impedance_source_tag)) if impedance_source_tag is not None else None,
+                surface_pressure_avg={int(t): avgs[int(t)] for t in tags} if tags else None,
+                surface_pressure=cat["p"][f] if write_surface_pressure else None,
+                assembly_s=t_asm * 1e-3 / F, dense_solve_s=t_solve * 1e-3 / F, field_s=t_field * 1e-3 / F,
+                lapack_info=int(cat["info"][f] or cat["info_ap"][f]),
+                diagnostics={"coupled_ib": True, "ib_coupled_solve": method, "aperture_triangles": m,
+                             "aperture_neumann": cat["qa"][f], "aperture_lapack_info": int(cat["info_ap"][f]),
+                             "precision": precision, "refine_iterations": int(cat["iters"][f]),
+                             "refine_residual_rel": float(cat["resid"][f]) if mixed else None,
+                             "dense_solve_rcond": None, "assembly_mode": "corrected"},
+            ))
+        return out
+
+    def _factor_solve_refine(self, Kr, Ki, br, bi, N, F, mixed, tol, max_iter):
+        """LU (+ BF16x3 refinement) of F systems of order N; returns x, info, iters, resid."""
+        import torch
+
+        dev, st = Kr.device, _stream_ptr()
+        K0r = K0i = None
+        if mixed:
+            K0r, K0i = Kr.clone(), Ki.clone()
+        piv = torch.empty((F, N), dtype=torch.int32, device=dev)
+        info = torch.empty(F, dtype=torch.int32, device=dev)
+        xr, xi = br.clone(), bi.clone()
+        prec = HBEM_PREC_MIXED if mixed else HBEM_PREC_PLAIN
+        check(self.lib.hbem_lu_factor(N, F, _t_ptr(Kr), _t_ptr(Ki), N, N * N, _t_ptr(piv), N, _t_ptr(info), prec, st),
+              "hbem_lu_factor", self.lib)
+        check(self.lib.hbem_lu_solve(N, 1, F, _t_ptr(Kr), _t_ptr(Ki), N, N * N, _t_ptr(piv), N, _t_ptr(xr), _t_ptr(xi),
+                                     1, N, HBEM_TRANS_N, st), "hbem_lu_solve", self.lib)
+        iters = torch.zeros(F, dtype=torch.int32, device=dev)
+        resid = torch.zeros(F, dtype=torch.float64, device=dev)
+        if mixed:
+            check(self.lib.hbem_refine(N, F, _t_ptr(K0r), _t_ptr(K0i), N, N * N, _t_ptr(Kr), _t_ptr(Ki), N * N,
+                                       _t_ptr(piv), N, _t_ptr(br), _t_ptr(bi), N, _t_ptr(xr), _t_ptr(xi), N,
+                                       float(tol), int(max_iter), _t_ptr(iters), _t_ptr(resid), st),
+                  "hbem_refine", self.lib)
+            del K0r, K0i
+        return xr, xi, info, iters, resid
+
+    def _coupled_chunk_schur(self, k_re, k_im, kf, q, obs_t, want, mixed, tol, max_iter, times):
+        import torch
+
+        dev, st = obs_t.device, _stream_ptr()
+        F, n, m, N_obs = k_re.shape[0], self.n_dof, self.m_aperture, obs_t.shape[1]
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         ev[0].record()
-        Ar, Ai, br, bi = self.assemble(k_re, np.asarray(neumann_dp0).reshape(F, T), k_imag=k_im)
+        Ar, Ai, br, bi = self.assemble(k_re, q, k_imag=k_im)
         sia_r = torch.empty((F, n, m), dtype=torch.float32, device=dev); sia_i = torch.empty_like(sia_r)
         saa_r = torch.empty((F, m, m), dtype=torch.float32, device=dev); saa_i = torch.empty_like(saa_r)
         check(self.lib.hbem_aperture_assemble(self.handle, F, _np_ptr(k_re), _np_ptr(k_im), _np_ptr(kf), _t_ptr(sia_r),
@@ -433,61 +523,84 @@ class NativeSession:
         check(self.lib.hbem_coupled_ib_schur(self.handle, F, _t_ptr(Ar), _t_ptr(Ai), _t_ptr(sia_r), _t_ptr(sia_i),
                                              _t_ptr(saa_r), _t_ptr(saa_i), _t_ptr(minv_r), _t_ptr(minv_i),
                                              _t_ptr(info_ap), st), "hbem_coupled_ib_schur", self.lib)
+        del sia_r, sia_i, saa_r, saa_i
         ev[1].record()
-        prec = HBEM_PREC_MIXED if precision == "mixed" else HBEM_PREC_PLAIN
-        A0r = A0i = None
-        if prec == HBEM_PREC_MIXED:
-            A0r, A0i = Ar.clone(), Ai.clone()
-        piv = torch.empty((F, n), dtype=torch.int32, device=dev)
-        info = torch.empty(F, dtype=torch.int32, device=dev)
-        xr, xi = br.clone(), bi.clone()
-        check(self.lib.hbem_lu_factor(n, F, _t_ptr(Ar), _t_ptr(Ai), n, n * n, _t_ptr(piv), n, _t_ptr(info), prec, st),
-              "hbem_lu_factor", self.lib)
-        check(self.lib.hbem_lu_solve(n, 1, F, _t_ptr(Ar), _t_ptr(Ai), n, n * n, _t_ptr(piv), n, _t_ptr(xr), _t_ptr(xi),
-                                     1, n, HBEM_TRANS_N, st), "hbem_lu_solve", self.lib)
-        iters = torch.zeros(F, dtype=torch.int32, device=dev)
-        resid = torch.zeros(F, dtype=torch.float64, device=dev)
-        if prec == HBEM_PREC_MIXED:
-            check(self.lib.hbem_refine(n, F, _t_ptr(A0r), _t_ptr(A0i), n, n * n, _t_ptr(Ar), _t_ptr(Ai), n * n,
-                                       _t_ptr(piv), n, _t_ptr(br), _t_ptr(bi), n, _t_ptr(xr), _t_ptr(xi), n,
-                                       float(refine_tolerance), int(refine_max_iterations), _t_ptr(iters),
-                                       _t_ptr(resid), st), "hbem_refine", self.lib)
+        xr, xi, info, iters, resid = self._factor_solve_refine(Ar, Ai, br, bi, n, F, mixed, tol, max_iter)
+        del Ar, Ai
         ev[2].record()
         qa_r = torch.empty((F, m), dtype=torch.float32, device=dev); qa_i = torch.empty_like(qa_r)
-        fr = torch.empty((F, N), dtype=torch.float32, device=dev); fi = torch.empty_like(fr)
+        fr = torch.empty((F, N_obs), dtype=torch.float32, device=dev); fi = torch.empty_like(fr)
         check(self.lib.hbem_coupled_ib_field(self.handle, F, _np_ptr(kf), _t_ptr(xr), _t_ptr(xi), _t_ptr(minv_r),
-                                             _t_ptr(minv_i), _t_ptr(obs_t), N, _t_ptr(qa_r), _t_ptr(qa_i), _t_ptr(fr),
+                                             _t_ptr(minv_i), _t_ptr(obs_t), N_obs, _t_ptr(qa_r), _t_ptr(qa_i), _t_ptr(fr),
                                              _t_ptr(fi), st), "hbem_coupled_ib_field", self.lib)
-        tags = list(source_tags or [])
-        want = tags + ([impedance_source_tag] if impedance_source_tag is not None and impedance_source_tag not in tags else [])
         tavg = self.tag_average(xr, xi, want).cpu().numpy() if want else None
         ev[3].record()
+        return self._chunk_out(ev, times, xr, xi, qa_r, qa_i, fr, fi, info, info_ap, iters, resid, tavg)
+
+    def coupled_ib_system(self, k_re, k_im, kf, q):
+        """The augmented coupled system on the device: K (F, N, N), [0; b] (F, N), N = m + n, and the
+        per-frequency scale alpha of the aperture unknowns (q_a = alpha * x[:m])."""
+        torch = require_cuda()
+        dev, st = torch.device("cuda", self.device), _stream_ptr()
+        k_re = np.ascontiguousarray(np.atleast_1d(k_re), dtype=np.float32)
+        k_im = None if k_im is None else np.ascontiguousarray(np.atleast_1d(k_im), dtype=np.float32)
+        kf = np.ascontiguousarray(np.atleast_1d(kf), dtype=np.float32)
+        F, n, m, T = k_re.shape[0], self.n_dof, self.m_aperture, self.n_triangles
+        N = n + m
+        Kr = torch.empty((F, N, N), dtype=torch.float32, device=dev); Ki = torch.empty_like(Kr)
+        rr = torch.zeros((F, N), dtype=torch.float32, device=dev); ri = torch.zeros_like(rr)
+        qr, qi = self._split_device(q, (F, T), dev)
+        off_a, off_b = m * N + m, m
+        check(self.lib.hbem_assemble(
+            self.handle, F, _np_ptr(k_re), _np_ptr(k_im), _t_ptr(qr), _t_ptr(qi), T, None, None,
+            ctypes.c_void_p(Kr.data_ptr() + 4 * off_a), ctypes.c_void_p(Ki.data_ptr() + 4 * off_a), N, N * N,
+            ctypes.c_void_p(rr.data_ptr() + 4 * off_b), ctypes.c_void_p(ri.data_ptr() + 4 * off_b), N,
+            HBEM_ASM_CORRECTED, st), "hbem_assemble", self.lib)
+        sia_r = torch.empty((F, n, m), dtype=torch.float32, device=dev); sia_i = torch.empty_like(sia_r)
+        saa_r = torch.empty((F, m, m), dtype=torch.float32, device=dev); saa_i = torch.empty_like(saa_r)
+        check(self.lib.hbem_aperture_assemble(self.handle, F, _np_ptr(k_re), _np_ptr(k_im), _np_ptr(kf), _t_ptr(sia_r),
+                                              _t_ptr(sia_i), _t_ptr(saa_r), _t_ptr(saa_i), st),
+              "hbem_aperture_assemble", self.lib)
+        alpha = torch.empty(F, dtype=torch.float32, device=dev)
+        check(self.lib.hbem_coupled_ib_augment(self.handle, F, _t_ptr(sia_r), _t_ptr(sia_i), _t_ptr(saa_r),
+                                               _t_ptr(saa_i), _t_ptr(Kr), _t_ptr(Ki), N, N * N, _t_ptr(alpha), st),
+              "hbem_coupled_ib_augment", self.lib)
+        return Kr, Ki, rr, ri, alpha
+
+    def _coupled_chunk_augmented(self, k_re, k_im, kf, q, obs_t, want, mixed, tol, max_iter, times):
+        import torch
+
+        dev, st = obs_t.device, _stream_ptr()
+        F, n, m, N_obs = k_re.shape[0], self.n_dof, self.m_aperture, obs_t.shape[1]
+        N = n + m
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record()
+        Kr, Ki, rr, ri, alpha = self.coupled_ib_system(k_re, k_im, kf, q)
+        ev[1].record()
+        xr, xi, info, iters, resid = self._factor_solve_refine(Kr, Ki, rr, ri, N, F, mixed, tol, max_iter)
+        del Kr, Ki
+        ev[2].record()
+        qa_r, qa_i = (xr[:, :m] * alpha[:, None]).contiguous(), (xi[:, :m] * alpha[:, None]).contiguous()
+        pr, pi = xr[:, m:].contiguous(), xi[:, m:].contiguous()
+        fr = torch.empty((F, N_obs), dtype=torch.float32, device=dev); fi = torch.empty_like(fr)
+        check(self.lib.hbem_coupled_ib_field(self.handle, F, _np_ptr(kf), None, None, None, None, _t_ptr(obs_t), N_obs,
+                                             _t_ptr(qa_r), _t_ptr(qa_i), _t_ptr(fr), _t_ptr(fi), st),
+              "hbem_coupled_ib_field", self.lib)
+        tavg = self.tag_average(pr, pi, want).cpu().numpy() if want else None
+        ev[3].record()
+        info_ap = torch.zeros(F, dtype=torch.int32, device=dev)
+        return self._chunk_out(ev, times, pr, pi, qa_r, qa_i, fr, fi, info, info_ap, iters, resid, tavg)
+
+    @staticmethod
+    def _chunk_out(ev, times, pr, pi, qa_r, qa_i, fr, fi, info, info_ap, iters, resid, tavg):
+        import torch
+
         torch.cuda.synchronize()
-        t_asm, t_solve, t_field = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2]), ev[2].elapsed_time(ev[3])
-        if timings_out is not None:
-            timings_out.update(assembly_ms=t_asm, solve_ms=t_solve, field_ms=t_field)
-        f_h = (fr.cpu().numpy() + 1j * fi.cpu().numpy()).astype(np.complex64)
-        x_h = (xr.cpu().numpy() + 1j * xi.cpu().numpy()).astype(np.complex64)
-        qa_h = (qa_r.cpu().numpy() + 1j * qa_i.cpu().numpy()).astype(np.complex64)
-        info_h, info_ap_h = info.cpu().numpy(), info_ap.cpu().numpy()
-        it_h, res_h = iters.cpu().numpy(), resid.cpu().numpy()
-        out = []
-        for f in range(F):
-            avgs = {int(t): complex(tavg[f, j, 0], tavg[f, j, 1]) for j, t in enumerate(want)} if want else {}
-            out.append(CaseResult(
-                frequency_hz=float(freqs[f]), field=f_h[f],
-                impedance=avgs.get(int(impedance_source_tag)) if impedance_source_tag is not None else None,
-                surface_pressure_avg={int(t): avgs[int(t)] for t in tags} if tags else None,
-                surface_pressure=x_h[f] if write_surface_pressure else None,
-                assembly_s=t_asm * 1e-3 / F, dense_solve_s=t_solve * 1e-3 / F, field_s=t_field * 1e-3 / F,
-                lapack_info=int(info_h[f] or info_ap_h[f]),
-                diagnostics={"coupled_ib": True, "aperture_triangles": m, "aperture_neumann": qa_h[f],
-                             "aperture_lapack_info": int(info_ap_h[f]), "precision": precision,
-                             "refine_iterations": int(it_h[f]),
-                             "refine_residual_rel": float(res_h[f]) if prec == HBEM_PREC_MIXED else None,
-                             "dense_solve_rcond": None, "assembly_mode": "corrected"},
-            ))
-        return out
+        times += [ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2]), ev[2].elapsed_time(ev[3])]
+        cplx = lambda a, b: (a.cpu().numpy() + 1j * b.cpu().numpy()).astype(np.complex64)  # noqa: E731
+        return {"field": cplx(fr, fi), "p": cplx(pr, pi), "qa": cplx(qa_r, qa_i), "info": info.cpu().numpy(),
+                "info_ap": info_ap.cpu().numpy(), "iters": iters.cpu().numpy(), "resid": resid.cpu().numpy(),
+                "tavg": tavg}
 
 
 # Drop-in alias for the reference's session class name.

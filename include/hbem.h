@@ -240,6 +240,14 @@ int hbem_solve_batch(hbem_session *s, int n_freq, const float *k_re, const float
  *   (n_freq, m, m).  S_aa is overwritten by its LU factors.
  * hbem_coupled_ib_field: q_a = M (P_avg p) (n_freq, m) and the Rayleigh field
  *   -2 sum G(y, x') q_a with x' = (x, y, max(z, 0)) for z >= -1e-5, 0 below.
+ *   With minv_re = minv_im = NULL, q_a is an input (p is not read).
+ * hbem_coupled_ib_augment: the augmented twin (main.swift:7504-7595) for
+ *   large apertures: K (n_freq, N, N), N = m + n, rows beta [-2 alpha S_aa |
+ *   P_avg] then [-alpha S_ia | A], with per-frequency block scales alpha =
+ *   max|A| / max|S_ia| and beta = max|A| / (2 alpha max|S_aa|) written to
+ *   alpha (device, n_freq).  Call it after hbem_assemble has written the A
+ *   block in place (a = K + m * ldk + m, lda = ldk); it fills every other
+ *   entry.  K [q~; p] = [0; b] gives the Schur solution p and q_a = alpha q~.
  */
 int hbem_session_set_aperture(hbem_session *s, int aperture_tag);
 int hbem_aperture_assemble(hbem_session *s, int n_freq, const float *k_re, const float *k_im, const float *kf_re,
@@ -250,6 +258,9 @@ int hbem_coupled_ib_schur(hbem_session *s, int n_freq, float *a_re, float *a_im,
 int hbem_coupled_ib_field(hbem_session *s, int n_freq, const float *kf_re, const float *p_re, const float *p_im,
                           const float *minv_re, const float *minv_im, const float *obs_3xn, int n_obs,
                           float *qa_re, float *qa_im, float *out_re, float *out_im, void *stream);
+int hbem_coupled_ib_augment(hbem_session *s, int n_freq, const float *sia_re, const float *sia_im,
+                            const float *saa_re, const float *saa_im, float *k_re, float *k_im, long long ldk,
+                            long long k_stride, float *alpha, void *stream);
 
 #ifdef __cplusplus
 }
