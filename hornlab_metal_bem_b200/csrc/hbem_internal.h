@@ -89,6 +89,7 @@ struct Session {
     int rule_off[3] = {0, 0, 0}, rule_cnt[3] = {0, 0, 0};
 
     int *d_status = nullptr;        // device-side status word (bounds / wait failures)
+    unsigned *d_sing_bits = nullptr; // T x T bitmap of touching pairs (shape gradients, built on first use)
 
     // coupled infinite baffle: aperture triangles (ascending ids) and their
     // local index per triangle (-1 elsewhere)

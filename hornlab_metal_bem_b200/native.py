@@ -77,6 +77,12 @@ _SIGNATURES = {
     "hbem_solve_batch": ([_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _c_int, _vp, _c_int, _c_int, _c_d, _c_int, _vp, _vp,
                           _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _c_int),
     "hbem_session_set_aperture": ([_vp, _c_int], _c_int),
+    "hbem_session_set_vertices": ([_vp, _vp, _vp, _vp], _c_int),
+    "hbem_field_adjoint": ([_vp, _c_int, _vp, _vp, _c_int, _vp, _vp, _c_ll, _vp, _vp, _c_ll, _vp], _c_int),
+    "hbem_field_backward": ([_vp, _c_int, _vp, _vp, _c_int, _vp, _vp, _c_ll, _vp, _vp, _c_ll, _vp, _vp, _c_ll, _vp,
+                             _vp], _c_int),
+    "hbem_assemble_backward": ([_vp, _c_int, _vp, _vp, _vp, _vp, _c_ll, _vp, _vp, _c_ll, _vp, _vp, _c_ll, _vp, _vp],
+                               _c_int),
     "hbem_coupled_ib_augment": ([_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _c_ll, _c_ll, _vp, _vp], _c_int),
     "hbem_aperture_assemble": ([_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _c_int),
     "hbem_coupled_ib_schur": ([_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _c_int),

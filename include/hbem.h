@@ -262,6 +262,39 @@ int hbem_coupled_ib_augment(hbem_session *s, int n_freq, const float *sia_re, co
                             const float *saa_re, const float *saa_im, float *k_re, float *k_im, long long ldk,
                             long long k_stride, float *alpha, void *stream);
 
+/*
+ * Shape gradients (adjoint of the forward map vertices -> A, b -> p -> field),
+ * sessions without symmetry planes, real wavenumbers.  With g (n_freq, n_obs)
+ * = dL/dRe F + i dL/dIm F of a real objective L of the field F:
+ *   hbem_field_adjoint:    g_p = Fp^H g (n_freq, n_dof), F = Fp p + Fq q;
+ *   then lambda = A^-H g_p with hbem_lu_solve(..., HBEM_TRANS_C) on the
+ *   forward's factors;
+ *   hbem_field_backward:   grad += d/dX Re g^H F at fixed p;
+ *   hbem_assemble_backward: grad += -Re lambda^H (dA/dX) p + Re lambda^H (db/dX),
+ *   recomputing the forward's quadrature (regular 6x6 on far pairs, the Duffy
+ *   rules on touching pairs, the mass term) pair by pair.
+ * grad_3xv: device float64 (3, n_vertices), accumulated (zero it first).
+ * No dA/dX is stored.  hbem_session_set_vertices moves the vertices of a
+ * session in place (same topology), with areas and unit normals as at
+ * creation.  No counterpart in the reference, which has no adjoint; the
+ * forward they differentiate is main.swift:3443-3480, 4090-4120, 4246-4431,
+ * 4135-4203.
+ */
+int hbem_session_set_vertices(hbem_session *s, const float *vertices_3xv, const float *areas,
+                              const float *normals_3xt);
+int hbem_field_adjoint(hbem_session *s, int n_freq, const float *k_re, const float *obs_3xn, int n_obs,
+                       const float *g_re, const float *g_im, long long g_stride, float *gp_re, float *gp_im,
+                       long long gp_stride, void *stream);
+int hbem_field_backward(hbem_session *s, int n_freq, const float *k_re, const float *obs_3xn, int n_obs,
+                        const float *g_re, const float *g_im, long long g_stride, const float *p_re,
+                        const float *p_im, long long p_stride, const float *q_re, const float *q_im,
+                        long long q_stride, double *grad_3xv, void *stream);
+int hbem_assemble_backward(hbem_session *s, int n_freq, const float *k_re, const float *k_im,
+                           const float *lam_re, const float *lam_im, long long lam_stride,
+                           const float *p_re, const float *p_im, long long p_stride,
+                           const float *q_re, const float *q_im, long long q_stride,
+                           double *grad_3xv, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

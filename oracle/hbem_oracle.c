@@ -22,8 +22,10 @@
  *   - tag-average surface pressure                       main.swift:807-841
  *
  * REAL is float (oracle "f32": same arithmetic type as the reference) or
- * double (oracle "f64": the accuracy oracle).  Functions carry an og32_/og64_
- * prefix chosen by the build.  Parallel loops use OpenMP so the same code is
+ * double (oracle "f64": the accuracy oracle).  GREAL, the type of the
+ * vertex / area / normal inputs, is float (the reference's geometry buffers)
+ * or double (the "g64" build, for FP64 finite differences of the geometry).
+ * Functions carry an og32_/og64_/og64g_ prefix chosen by the build.  Parallel loops use OpenMP so the same code is
  * the timed multi-core CPU baseline.
  *
  * Parity pin: geometry/front-end inputs come from the reference's own Python
@@ -33,6 +35,10 @@
  */
 #include <math.h>
 #include <stdint.h>
+
+#ifndef GREAL
+#define GREAL float
+#endif
 #include <stdlib.h>
 #include <string.h>
 #ifdef _OPENMP
@@ -56,11 +62,11 @@ static inline cplx cscale(cplx a, REAL s) { cplx r = {a.re * s, a.im * s}; retur
 /* Geometry exactly as the session buffers carry it (f32 inputs). */
 typedef struct {
     int n_vertices, n_triangles, n_dof, sym;
-    const float *verts;    /* (3, V) */
+    const GREAL *verts;    /* (3, V) */
     const int *tris;       /* (3, T) */
     const int *l2g;        /* (T, 3) */
-    const float *areas;    /* (T,)   */
-    const float *normals;  /* (3, T) */
+    const GREAL *areas;    /* (T,)   */
+    const GREAL *normals;  /* (3, T) */
 } og_geom;
 
 /* ---- quadrature ------------------------------------------------------- */

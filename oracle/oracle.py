@@ -42,7 +42,7 @@ def build() -> None:
 
 
 def _lib(precision: str):
-    name = {"f32": "libhbem_oracle_f32.so", "f64": "libhbem_oracle_f64.so"}[precision]
+    name = {"f32": "libhbem_oracle_f32.so", "f64": "libhbem_oracle_f64.so", "g64": "libhbem_oracle_g64.so"}[precision]
     path = BUILD / name
     if not path.exists():
         build()
@@ -56,19 +56,29 @@ def _ptr(a):
 class Oracle:
     """CPU oracle bound to one geometry (``GeometryBuffers``-like object)."""
 
-    def __init__(self, buffers, symmetry_code: int = 0, precision: str = "f64", threads: int | None = None):
+    def __init__(self, buffers, symmetry_code: int = 0, precision: str = "f64", threads: int | None = None,
+                 vertices_3xv=None):
+        """precision: "f32" (the reference's arithmetic), "f64", or "g64" (f64 with float64 geometry:
+        ``vertices_3xv`` (3, V) float64 replaces the buffers' vertices, areas and normals are rebuilt
+        in float64 -- the finite-difference reference for shape gradients)."""
         self.precision = precision
         self.lib = _lib(precision)
-        self.pre = "og32_" if precision == "f32" else "og64_"
+        self.pre = {"f32": "og32_", "f64": "og64_", "g64": "og64g_"}[precision]
         self.real = np.float32 if precision == "f32" else np.float64
         self._ct = ctypes.c_float if precision == "f32" else ctypes.c_double
-        self._keep = [
-            np.ascontiguousarray(buffers.vertices_3xn_f32, dtype=np.float32),
-            np.ascontiguousarray(buffers.triangles_3xm_i32, dtype=np.int32),
-            np.ascontiguousarray(buffers.p1_local2global_i32, dtype=np.int32),
-            np.ascontiguousarray(buffers.triangle_areas_f32, dtype=np.float32),
-            np.ascontiguousarray(buffers.triangle_normals_3xm_f32, dtype=np.float32),
-        ]
+        tris = np.ascontiguousarray(buffers.triangles_3xm_i32, dtype=np.int32)
+        if precision == "g64":
+            v = np.asarray(buffers.vertices_3xn_f32 if vertices_3xv is None else vertices_3xv, dtype=np.float64)
+            p0, p1, p2 = (v[:, tris[i]].T for i in range(3))
+            cross = np.cross(p1 - p0, p2 - p0)
+            twice = np.linalg.norm(cross, axis=1)
+            geo = [np.ascontiguousarray(v), np.ascontiguousarray(0.5 * twice),
+                   np.ascontiguousarray((cross / twice[:, None]).T)]
+        else:
+            geo = [np.ascontiguousarray(buffers.vertices_3xn_f32, dtype=np.float32),
+                   np.ascontiguousarray(buffers.triangle_areas_f32, dtype=np.float32),
+                   np.ascontiguousarray(buffers.triangle_normals_3xm_f32, dtype=np.float32)]
+        self._keep = [geo[0], tris, np.ascontiguousarray(buffers.p1_local2global_i32, dtype=np.int32), geo[1], geo[2]]
         self.tags = np.ascontiguousarray(buffers.physical_tags_i32, dtype=np.int32)
         self.n = int(buffers.p1_dof_count)
         self.T = int(buffers.triangles_3xm_i32.shape[1])
