@@ -51,7 +51,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=["c2", "c1", "c4"], default="c2")
+    ap.add_argument("--workload", choices=["c2", "c1", "c3", "c4", "c5"], default="c2")
+    ap.add_argument("--streams", type=int, default=4, help="c3: concurrent streams")
     ap.add_argument("--precision", choices=["plain", "mixed"], default="plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -550,8 +551,226 @@ def run_b200_c4(args, w):
         dist.destroy_process_group()
 
 
+def c3_cases():
+    """64 seeded half (yz) waveguide variants: flare ~ U[10, 40] 1/m, mouth radius ~ U[80, 200] mm, edge
+    lambda(8 kHz) / 6 = 7.15 mm; 40 log freqs 0.5-20 kHz; throat disc axial piston; 3 x 37 obs at 2 m."""
+    import hornlab_metal_bem_b200 as hb
+    from hornlab_metal_bem_b200 import generators as G
+    from hornlab_metal_bem_b200.batch import SweepCase
+    from hornlab_metal_bem_b200.bie import build_source_face_scale
+    from hornlab_metal_bem_b200.geometry import build_geometry_buffers
+    from hornlab_metal_bem_b200.mesh import make_pure_function_spaces
+    from hornlab_metal_bem_b200.observation import build_observation_points
+    from hornlab_metal_bem_b200.sweep import build_frequency_grid, field_points_3xn, k_values, neumann_rows
+
+    cfg = hb.native_config(freq_min_hz=500.0, freq_max_hz=20000.0, freq_count=40, source_motion="axial",
+                           native_symmetry_plane="yz", native_check_open_edges=False,
+                           observation=hb.ObservationConfig(planes=["horizontal", "vertical", "diagonal"],
+                                                            angle_count=37))
+    freqs = build_frequency_grid(cfg)
+    k_re, k_im = k_values(freqs, cfg)
+    cases = []
+    for seed in range(64):
+        spec = G.horn_spec_from_seed(seed, edge=343.0 / 8000.0 / 6.0, flare_range=(10.0, 40.0),
+                                     mouth_range=(0.080, 0.200))
+        mesh = G.horn(spec, quarter=False, half=True)
+        frame = hb._resolve_frame(mesh, cfg)
+        obs, _ = build_observation_points(frame, cfg.observation)
+        p1, dp0 = make_pure_function_spaces(mesh.grid)
+        buf = build_geometry_buffers(mesh.grid, mesh.physical_tags, p1, dp0)
+        scale = build_source_face_scale(mesh.grid, mesh.physical_tags, cfg, frame.axis, frame.source_center)
+        q = neumann_rows(buf.n_triangles, mesh.physical_tags, freqs, cfg, scale)
+        cases.append(SweepCase(buf, k_re, q, field_points_3xn(obs), sorted(cfg.velocity_sources), "yz"))
+    return cases
+
+
+def run_b200_c3(args):
+    """All 2560 solves of the 64-mesh batch as graph replays on concurrent streams, autotuned variants."""
+    import torch
+
+    from hornlab_metal_bem_b200.batch import BatchedSweeps
+    from hornlab_metal_bem_b200.native import load_library
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    lib = load_library()
+    t0 = time.perf_counter()
+    cases = c3_cases()
+    t_mesh = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    bs = BatchedSweeps(cases, n_streams=args.streams, tuning="auto")
+    torch.cuda.synchronize()
+    t_setup = time.perf_counter() - t0
+    n_solves = sum(len(c.k_re) for c in cases)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        bs.run()
+    torch.cuda.synchronize()
+    outs = bs.outputs()
+    if any(int(np.abs(o.lapack_info).sum()) for o in outs):
+        raise RuntimeError("zero pivot in the batched workload")
+    clocks = Clocks(None)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        bs.run()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    # e2e: new Neumann data from host memory, the batch, and every result back to the host
+    qs = [c.q for c in cases]
+    h2d = d2h = 0
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        h2d = bs.set_neumann(qs)
+        bs.run()
+        outs = bs.outputs()
+        d2h = sum(o.field.nbytes + o.tag_average.nbytes + o.lapack_info.nbytes for o in outs)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e2.elapsed_time(e3)
+    ns = np.array([c.n for c in cases])
+    variants = {}
+    for i, c in enumerate(cases):
+        variants.setdefault(str(bs.variants[i]), 0)
+        variants[str(bs.variants[i])] += 1
+    line = {
+        "metric": "freq-solves/s", "value": n_solves * args.steps / (ms * 1e-3), "unit": "freq-solves/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64 (f32 planar)",
+        "data": "synthetic",
+        "config": {"workload": "C3 64 seeded half (yz) waveguide variants, flare U[10,40] 1/m, mouth U[80,200] mm, "
+                               "edge 7.15 mm, 40 log freqs 0.5-20 kHz, 3x37 obs @ 2 m",
+                   "meshes": len(cases), "solves": n_solves, "n_dof_min": int(ns.min()), "n_dof_max": int(ns.max()),
+                   "n_dof_median": int(np.median(ns)), "streams": len(bs.slots),
+                   "parallelism": "graph per mesh, meshes on concurrent streams (LPT by cost)",
+                   "l2": "per-mesh matrices 0.2-2.8 GB > 126 MB L2"},
+        "autotune": {"table": bs.autotuner.table if bs.autotuner else None,
+                     "measurements": bs.autotuner.measurements if bs.autotuner else None,
+                     "variant_use": variants},
+        "setup_s": {"meshing": t_mesh, "sessions_tuning_capture": t_setup},
+        "e2e": {"value": n_solves * args.steps / (e2e_ms * 1e-3), "unit": "freq-solves/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(bs.kernels_per_run() * args.steps),
+        "graph_launches": len(cases) * args.steps,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    bs.close()
+
+
+def run_b200_c5(args):
+    """Adjoint shape gradient of the directivity objective: 2082-dof full round horn, 24 radial-profile
+    spline control points, 20 log frequencies 2-16 kHz, 6 angles x 2 planes at 2 m.  The metric is the
+    time of one gradient (backward pass) over one forward solve; the gradient is checked against
+    central differences of the same GPU forward."""
+    import torch
+
+    from hornlab_metal_bem_b200 import generators as G
+    from hornlab_metal_bem_b200.adjoint import (
+        ShapeProblem, boundary_field, directivity_objective, directivity_points, spline_horn,
+    )
+    from hornlab_metal_bem_b200.geometry import build_geometry_buffers
+    from hornlab_metal_bem_b200.mesh import make_pure_function_spaces
+    from hornlab_metal_bem_b200.native import load_library
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    lib = load_library()
+    angles = [10, 20, 30, 40, 50, 60]
+    spec = G.horn_spec_from_seed(0, edge=0.0095)
+    mesh, sh = spline_horn(spec, 24)
+    p1, dp0 = make_pure_function_spaces(mesh.grid)
+    buf = build_geometry_buffers(mesh.grid, mesh.physical_tags, p1, dp0)
+    freqs = np.geomspace(2000.0, 16000.0, 20)
+    k = (2 * np.pi * freqs / 343.0).astype(np.float32)
+    q = np.zeros((len(freqs), buf.triangles_3xm_i32.shape[1]), np.complex64)
+    q[:, buf.physical_tags_i32 == 2] = 1.2041
+    obs = directivity_points(spec.length, angles).astype(np.float32)
+    prob = ShapeProblem(buf, k, q, obs)
+    c0 = np.random.default_rng(0).normal(0.0, 0.002, 24)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        c = torch.tensor(c0, dtype=torch.float64, requires_grad=True)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record(stream)
+        J = directivity_objective(boundary_field(sh.vertices(c), prob), angles)
+        e[1].record(stream)
+        J.backward()
+        e[2].record(stream)
+        return J, c.grad, e
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks = Clocks(None)
+    launches0 = lib.hbem_launch_count()
+    clocks.start()
+    evs = []
+    for _ in range(args.steps):
+        J, grad, e = step()
+        evs.append(e)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = lib.hbem_launch_count() - launches0
+    fwd = statistics.median(e[0].elapsed_time(e[1]) for e in evs)
+    bwd = statistics.median(e[1].elapsed_time(e[2]) for e in evs)
+    g = grad.numpy()
+    # central differences of the GPU forward on the four largest components
+    h = 1e-5
+    picks = [int(i) for i in np.argsort(-np.abs(g))[:4]]
+    fd = []
+    with torch.no_grad():
+        for i in picks:
+            vals = []
+            for sgn in (1.0, -1.0):
+                c = c0.copy()
+                c[i] += sgn * h
+                vals.append(float(directivity_objective(boundary_field(sh.vertices(torch.tensor(c)), prob), angles)))
+            fd.append((vals[0] - vals[1]) / (2 * h))
+    fd = np.asarray(fd)
+    line = {
+        "metric": "adjoint gradient time / forward solve time", "value": bwd / fwd, "unit": "ratio",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": fwd + bwd, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64 (f32 planar), f64 gradient accumulation",
+        "data": "synthetic",
+        "config": {"workload": "C5 full round horn (seed 0), edge 9.5 mm, 24 radial spline control points "
+                               "(seeded N(0, 2 mm)), 20 log freqs 2-16 kHz, 6 angles x 2 planes @ 2 m",
+                   "n_dof": prob.n, "n_triangles": prob.T, "n_freq": len(freqs), "n_obs": prob.n_obs},
+        "forward_ms": fwd, "gradient_ms": bwd, "objective": float(J.detach()),
+        "forward_freq_solves_per_s": len(freqs) / (fwd * 1e-3),
+        "gradient_check_gpu_central_fd": {"step_m": h, "components": picks, "adjoint": g[picks].tolist(),
+                                          "fd": fd.tolist(),
+                                          "rel_err": float(np.linalg.norm(g[picks] - fd) / np.linalg.norm(fd))},
+        "e2e": {"value": (fwd + bwd) * 1e-3, "unit": "s per objective + gradient", "h2d_bytes_per_step":
+                prob.V * 3 * 4 + prob.T * 8, "d2h_bytes_per_step": len(freqs) * prob.n_obs * 8 + prob.V * 24},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    prob.close()
+
+
 def main():
     args = parse()
+    if args.workload in ("c3", "c4", "c5") and args.impl == "reference":
+        if dist_env()[1] == 0:
+            why = {"c3": "2560 host-core solves of 800-3000 dofs take hours, beyond the bounded benchmark sample",
+                   "c4": "the host-core CPU path needs minutes per frequency for 18749-unknown dense systems, beyond "
+                         "the bounded benchmark sample",
+                   "c5": "the reference has no adjoint or gradient path"}[args.workload]
+            print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
+        return
+    if args.workload == "c5":
+        run_b200_c5(args)
+        return
+    if args.workload == "c3" and args.impl != "reference":
+        run_b200_c3(args)
+        return
     w = workload(args.workload)
     if args.impl == "reference":
         run_reference(args, w)

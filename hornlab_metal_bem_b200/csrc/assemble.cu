@@ -381,8 +381,11 @@ cudaError_t launch_regular_t(const AsmArgs &a, dim3 grid, size_t smem, cudaStrea
 }
 
 // Resident CTAs per SM for the pair kernel: 2 (128 registers, no spills) or 3
-// (80 registers).  HBEM_ASM_MINBLOCKS overrides the default for tuning.
+// (80 registers).  HBEM_TUNE_ASM_MINBLOCKS (or the HBEM_ASM_MINBLOCKS
+// environment variable) overrides the default.
 int regular_min_blocks() {
+    const int t = tuning(HBEM_TUNE_ASM_MINBLOCKS);
+    if (t == 2 || t == 3) return t;
     static int v = [] {
         const char *e = getenv("HBEM_ASM_MINBLOCKS");
         int m = e ? atoi(e) : 2;

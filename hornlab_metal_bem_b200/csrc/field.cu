@@ -246,3 +246,15 @@ extern "C" int hbem_reduce_tag_avg(hbem_session *h, int n_freq, const float *p_r
     cudaFreeAsync(d_want, st);
     return rc;
 }
+
+extern "C" int hbem_reduce_tag_avg_device(hbem_session *h, int n_freq, const float *p_re, const float *p_im,
+                                          long long p_stride, const int *tags_device, int n_tags, double *out,
+                                          void *stream) {
+    Session *s = reinterpret_cast<Session *>(h);
+    if (!s) return fail(HBEM_ERR_ARG, "hbem_reduce_tag_avg_device: NULL session");
+    if (n_freq <= 0 || n_tags <= 0) return HBEM_OK;
+    if (!p_re || !p_im || !tags_device || !out) return fail(HBEM_ERR_ARG, "hbem_reduce_tag_avg_device: NULL pointer");
+    if (n_tags > 64) return fail(HBEM_ERR_ARG, "hbem_reduce_tag_avg_device: at most 64 tags per call");
+    HBEM_CUDA(cudaSetDevice(s->device));
+    return launch_tag_avg(*s, n_freq, p_re, p_im, p_stride, tags_device, n_tags, out, reinterpret_cast<cudaStream_t>(stream));
+}

@@ -16,6 +16,7 @@ void set_error(const std::string &msg);
 int fail(int code, const std::string &msg);
 int cuda_fail(cudaError_t e, const char *what);
 void count_launch(long long n = 1);
+int tuning(int key);   // HBEM_TUNE_* value, 0 = built-in choice
 
 #define HBEM_CUDA(call)                                        \
     do {                                                       \

@@ -1033,7 +1033,9 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
     for (int b0 = 0; b0 < n; b0 += NB) {
         const int bw = std::min(NB, n - b0);
         // inner width 32 while an 8-CTA cluster can hold the panel, else 16
-        const int nbi = ((size_t)(n - b0) <= 8 * (smem_cap / (33 * 8))) ? 32 : 16;
+        const int fits32 = (size_t)(n - b0) <= 8 * (smem_cap / (33 * 8));
+        const int want = tuning(HBEM_TUNE_LU_PANEL);
+        const int nbi = (want == 16 || !fits32) ? 16 : 32;
         for (int c = b0; c < b0 + bw; c += nbi) {
             const int w = std::min(nbi, b0 + bw - c);
             const size_t psmem = (size_t)(n - c) * (w + 1) * 8;
@@ -1081,7 +1083,8 @@ int lu_solve(int n, int nrhs, int batch, const float *lu_re, const float *lu_im,
     const size_t smem = (size_t)n * 2 * sizeof(float);
     if (smem > 200 * 1024) return fail(HBEM_ERR_ARG, "hbem_lu_solve: n too large for the staged solve");
     dim3 grid(nrhs, batch);
-    if (trans == HBEM_TRANS_N && n > kTB)
+    const int solve_mode = tuning(HBEM_TUNE_LU_SOLVE);
+    if (trans == HBEM_TRANS_N && (solve_mode == 2 || (solve_mode == 0 && n > kTB)))
         return lu_solve_blocked(n, nrhs, batch, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re, b_im, ldb, b_stride, st);
     if (trans == HBEM_TRANS_N) {
         HBEM_CUDA(cudaFuncSetAttribute(k_getrs<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -36,6 +36,10 @@ int cuda_fail(cudaError_t e, const char *what) {
 
 void count_launch(long long n) { g_launches += n; }
 
+// Tuning knobs (HBEM_TUNE_*), process-wide; 0 = the built-in choice.
+static std::atomic<int> g_tuning[HBEM_TUNE_COUNT];
+int tuning(int key) { return (key >= 0 && key < HBEM_TUNE_COUNT) ? g_tuning[key].load() : 0; }
+
 // ---------------------------------------------------------------------------
 // Duffy rules: 4-point Gauss-Legendre on [0,1] in each of four Duffy
 // coordinates; 6 / 5 / 2 sub-regions for coincident / edge / vertex pairs.
@@ -285,6 +289,26 @@ extern "C" int hbem_last_error(char *buf, size_t len) {
 }
 
 extern "C" long long hbem_launch_count(void) { return g_launches.load(); }
+
+extern "C" int hbem_set_tuning(int key, int value) {
+    switch (key) {
+        case HBEM_TUNE_ASM_MINBLOCKS:
+            if (value != 0 && value != 2 && value != 3) return fail(HBEM_ERR_ARG, "HBEM_TUNE_ASM_MINBLOCKS: 0, 2 or 3");
+            break;
+        case HBEM_TUNE_LU_PANEL:
+            if (value != 0 && value != 16 && value != 32) return fail(HBEM_ERR_ARG, "HBEM_TUNE_LU_PANEL: 0, 16 or 32");
+            break;
+        case HBEM_TUNE_LU_SOLVE:
+            if (value < 0 || value > 2) return fail(HBEM_ERR_ARG, "HBEM_TUNE_LU_SOLVE: 0, 1 or 2");
+            break;
+        default:
+            return fail(HBEM_ERR_ARG, "hbem_set_tuning: unknown key " + std::to_string(key));
+    }
+    g_tuning[key].store(value);
+    return HBEM_OK;
+}
+
+extern "C" int hbem_get_tuning(int key) { return tuning(key); }
 
 extern "C" int hbem_session_create(const float *vertices_3xv, int n_vertices, const int *triangles_3xt,
                                    int n_triangles, const int *l2g, int n_dof, const int *tags,

@@ -77,7 +77,7 @@ def _ring_angles(r: float, h: float, phi_max: float) -> np.ndarray:
     return np.linspace(0.0, phi_max, n + 1)
 
 
-def revolve(profile_rz, tags_seg, h: float, quarter: bool) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+def revolve(profile_rz, tags_seg, h: float, quarter: bool, half: bool = False) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
     """Mesh the surface swept by a meridian polyline ``(r, z)`` around the z axis.
 
     ``tags_seg[i]`` tags the strip between profile nodes ``i`` and ``i + 1``.
@@ -86,20 +86,25 @@ def revolve(profile_rz, tags_seg, h: float, quarter: bool) -> tuple[np.ndarray, 
     travel along the profile in the (r, z) half-plane, i.e. consistently for
     a profile that runs clockwise around the body's meridian section.
     """
-    phi_max = 0.5 * math.pi if quarter else 2.0 * math.pi
-    closed = not quarter
+    # sector: quarter x, y >= 0 (yz + xz planes); half x >= 0 (yz plane), swept
+    # from -pi/2 to pi/2; else the full revolution
+    phi_max = 0.5 * math.pi if quarter else (math.pi if half else 2.0 * math.pi)
+    phi0 = -0.5 * math.pi if (half and not quarter) else 0.0
+    closed = not (quarter or half)
     verts: list[tuple[float, float, float]] = []
     rings: list[tuple[np.ndarray, list[int]]] = []
     for r, z in profile_rz:
         ang = _ring_angles(float(r), h, phi_max)
         ids = []
         for a in ang:
-            x, y = float(r) * math.cos(a), float(r) * math.sin(a)
+            x, y = float(r) * math.cos(a + phi0), float(r) * math.sin(a + phi0)
             if quarter:
                 if abs(a - phi_max) < 1e-12:
                     x = 0.0
                 if a == 0.0:
                     y = 0.0
+            elif half and (a == 0.0 or abs(a - phi_max) < 1e-12):
+                x = 0.0
             ids.append(len(verts))
             verts.append((x, y, float(z)))
         rings.append((ang, ids))
@@ -218,9 +223,10 @@ def horn_profile(spec: HornSpec) -> tuple[np.ndarray, np.ndarray]:
     return np.asarray(pts), np.asarray(tags, dtype=np.int32)
 
 
-def horn(spec: HornSpec = HornSpec(), quarter: bool = True) -> LoadedMesh:
+def horn(spec: HornSpec = HornSpec(), quarter: bool = True, half: bool = False) -> LoadedMesh:
+    """Closed round horn: quarter (x, y >= 0; yz + xz planes), half (x >= 0; yz plane) or full."""
     prof, seg_tags = horn_profile(spec)
-    v, f, tags = revolve(prof, seg_tags, spec.edge, quarter)
+    v, f, tags = revolve(prof, seg_tags, spec.edge, quarter, half and not quarter)
     # merge duplicate vertices created where the profile revisits a radius
     keys = np.round(v / 1e-9).astype(np.int64)
     _, first, inv = np.unique(keys, axis=0, return_index=True, return_inverse=True)
@@ -232,7 +238,7 @@ def horn(spec: HornSpec = HornSpec(), quarter: bool = True) -> LoadedMesh:
     f = remap[inv[f]].astype(np.int32)
     keep = ~((f[:, 0] == f[:, 1]) | (f[:, 1] == f[:, 2]) | (f[:, 0] == f[:, 2]))
     f, tags = f[keep], tags[keep]
-    if quarter:
+    if quarter or half:
         p0, p1, p2 = v[f[:, 0]], v[f[:, 1]], v[f[:, 2]]
         n = np.cross(p1 - p0, p2 - p0)
         c = (p0 + p1 + p2) / 3.0

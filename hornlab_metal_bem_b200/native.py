@@ -77,6 +77,9 @@ _SIGNATURES = {
     "hbem_solve_batch": ([_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _c_int, _vp, _c_int, _c_int, _c_d, _c_int, _vp, _vp,
                           _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _c_int),
     "hbem_session_set_aperture": ([_vp, _c_int], _c_int),
+    "hbem_set_tuning": ([_c_int, _c_int], _c_int),
+    "hbem_get_tuning": ([_c_int], _c_int),
+    "hbem_reduce_tag_avg_device": ([_vp, _c_int, _vp, _vp, _c_ll, _vp, _c_int, _vp, _vp], _c_int),
     "hbem_session_set_vertices": ([_vp, _vp, _vp, _vp], _c_int),
     "hbem_field_adjoint": ([_vp, _c_int, _vp, _vp, _c_int, _vp, _vp, _c_ll, _vp, _vp, _c_ll, _vp], _c_int),
     "hbem_field_backward": ([_vp, _c_int, _vp, _vp, _c_int, _vp, _vp, _c_ll, _vp, _vp, _c_ll, _vp, _vp, _c_ll, _vp,

@@ -81,6 +81,24 @@ int hbem_last_error(char *buf, size_t len);
 long long hbem_launch_count(void);
 
 /*
+ * Process-wide tuning knobs, read at launch time (so a CUDA graph captured
+ * after a change keeps the variant it captured).  0 restores the built-in
+ * choice.  Used by the autotuner of batched sweeps; no counterpart in the
+ * reference.
+ *   HBEM_TUNE_ASM_MINBLOCKS: resident CTAs per SM of the pair-assembly kernel
+ *                            (2: 128 registers, 3: 80 registers)
+ *   HBEM_TUNE_LU_PANEL:      inner sub-panel width of the LU (16 or 32)
+ *   HBEM_TUNE_LU_SOLVE:      no-transpose solve (1: one CTA per right-hand
+ *                            side, 2: blocked multi-CTA steps)
+ */
+#define HBEM_TUNE_ASM_MINBLOCKS 0
+#define HBEM_TUNE_LU_PANEL 1
+#define HBEM_TUNE_LU_SOLVE 2
+#define HBEM_TUNE_COUNT 3
+int hbem_set_tuning(int key, int value);
+int hbem_get_tuning(int key);
+
+/*
  * Create a session on `device` from host geometry buffers.
  * Replaces: MetalNativeStandardSession.create_session
  *   (hornlab_metal_bem/metal/native.py:252-377) and the helper's
@@ -198,6 +216,10 @@ int hbem_field(hbem_session *s, int n_freq, const float *k_re,
  */
 int hbem_reduce_tag_avg(hbem_session *s, int n_freq, const float *p_re, const float *p_im, long long p_stride,
                         const int *tags_host, int n_tags, double *out, void *stream);
+/* hbem_reduce_tag_avg with the tag list in device memory (n_tags ints): no
+ * host copy or allocation, so it can be captured in a CUDA graph. */
+int hbem_reduce_tag_avg_device(hbem_session *s, int n_freq, const float *p_re, const float *p_im, long long p_stride,
+                               const int *tags_device, int n_tags, double *out, void *stream);
 
 /*
  * One-call batched sweep over host buffers: host->device copies, assembly,
