@@ -51,7 +51,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=["c2", "c1", "c3", "c4", "c5"], default="c2")
+    ap.add_argument("--workload", choices=["c2", "c1", "c3", "c4", "c5", "lu"], default="c2")
+    ap.add_argument("--n", type=int, default=10000, help="lu: matrix order")
+    ap.add_argument("--batch", type=int, default=2, help="lu: matrices per launch")
     ap.add_argument("--streams", type=int, default=4, help="c3: concurrent streams")
     ap.add_argument("--precision", choices=["plain", "mixed"], default="plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -480,7 +482,7 @@ def run_b200_c4(args, w):
     picks = [0, F - 1]
     Kr, Ki, rr, ri, alpha = sess.coupled_ib_system(w["k_re"][picks], None if w["k_im"] is None else w["k_im"][picks],
                                             w["kf"][picks], w["q"][picks])
-    K = torch.complex(Kr.double(), Ki.double())
+    K = torch.complex(Kr[:, :, :N].double(), Ki[:, :, :N].double())
     del Kr, Ki
     x64 = torch.linalg.solve(K, torch.complex(rr.double(), ri.double()).unsqueeze(-1)).squeeze(-1)
     del K
@@ -662,6 +664,54 @@ def run_b200_c3(args):
     bs.close()
 
 
+def run_lu(args):
+    """Batched complex LU + solve microbenchmark (diagonally dominant random matrices, seeded)."""
+    import torch
+
+    from hornlab_metal_bem_b200.native import HBEM_TRANS_N, _stream_ptr, _t_ptr, check, load_library
+
+    lib = load_library()
+    n, F = args.n, args.batch
+    prec = 1 if args.precision == "mixed" else 0
+    g = torch.Generator(device="cuda").manual_seed(0)
+    A0r = torch.randn((F, n, n), device="cuda", generator=g)
+    A0r += 2 * n ** 0.5 * torch.eye(n, device="cuda")
+    A0i = torch.randn((F, n, n), device="cuda", generator=g)
+    br = torch.randn((F, n), device="cuda", generator=g)
+    bi = torch.randn((F, n), device="cuda", generator=g)
+    Ar, Ai = torch.empty_like(A0r), torch.empty_like(A0i)
+    piv = torch.empty((F, n), dtype=torch.int32, device="cuda")
+    info = torch.empty(F, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+    times = []
+    for it in range(args.warmup + args.steps):
+        Ar.copy_(A0r)
+        Ai.copy_(A0i)
+        xr, xi = br.clone(), bi.clone()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record(stream)
+        check(lib.hbem_lu_factor(n, F, _t_ptr(Ar), _t_ptr(Ai), n, n * n, _t_ptr(piv), n, _t_ptr(info), prec,
+                                 _stream_ptr()), "hbem_lu_factor", lib)
+        e[1].record(stream)
+        check(lib.hbem_lu_solve(n, 1, F, _t_ptr(Ar), _t_ptr(Ai), n, n * n, _t_ptr(piv), n, _t_ptr(xr), _t_ptr(xi), 1,
+                                n, HBEM_TRANS_N, _stream_ptr()), "hbem_lu_solve", lib)
+        e[2].record(stream)
+        torch.cuda.synchronize()
+        if it >= args.warmup:
+            times.append((e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])))
+    fac = statistics.median(t[0] for t in times)
+    sol = statistics.median(t[1] for t in times)
+    A = torch.complex(A0r[0].double(), A0i[0].double())
+    x = torch.complex(xr[0].double(), xi[0].double())
+    b = torch.complex(br[0].double(), bi[0].double())
+    resid = float(torch.linalg.norm(A @ x - b) / torch.linalg.norm(b))
+    flops = F * (8.0 / 3.0) * n ** 3
+    print(json.dumps({"metric": "complex LU factor TFLOP/s (8/3 n^3 per matrix)", "value": flops / (fac * 1e-3) / 1e12,
+                      "unit": "TFLOP/s", "n": n, "batch": F, "precision": args.precision, "factor_ms": fac,
+                      "solve_ms": sol, "steps": args.steps, "warmup": args.warmup, "residual_rel": resid,
+                      "info": int(info.abs().sum())}), flush=True)
+
+
 def run_b200_c5(args):
     """Adjoint shape gradient of the directivity objective: 2082-dof full round horn, 24 radial-profile
     spline control points, 20 log frequencies 2-16 kHz, 6 angles x 2 planes at 2 m.  The metric is the
@@ -764,6 +814,10 @@ def main():
                          "the bounded benchmark sample",
                    "c5": "the reference has no adjoint or gradient path"}[args.workload]
             print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
+        return
+    if args.workload == "lu":
+        if args.impl != "reference":
+            run_lu(args)
         return
     if args.workload == "c5":
         run_b200_c5(args)

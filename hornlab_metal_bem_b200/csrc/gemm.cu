@@ -133,31 +133,37 @@ int launch_trailing_update(int n, int batch, int k0, int kw, int start, int col_
 // against B = [Ur; Ui].  Each FP32 operand x is split into hi = bf16(x) and
 // lo = bf16(x - hi); A B ~ Ah Bh + Ah Bl + Al Bh is a single K = 3 * 2 * 64
 // = 384 contraction over the packed operands A3 = [Ah | Ah | Al] and
-// B3^T = [Bh | Bl | Bh] (both K-major, written by k_pack_*).  TMA loads the
-// six 64-wide K-blocks of both operands (128-byte swizzle) into shared memory
-// up front; one thread issues 4 tcgen05.mma (K = 16) per block into a
-// 128 x 128 FP32 TMEM accumulator; the four warps read their 32 TMEM lanes
-// back with tcgen05.ld and subtract from C in global memory.
+// B3^T = [Bh | Bl | Bh] (both K-major, written by k_pack_*), tiles of 64
+// complex rows x 64 columns (k_trailing_tc: TMA ring, single-thread MMA
+// issue into a 128 x 64 FP32 TMEM accumulator, C staged through shared
+// memory by the epilogue warps).
 // Every mbarrier wait is bounded; a timeout sets the status word and the CTA
 // returns after releasing its TMEM.
 // ===========================================================================
 namespace hbem {
 namespace {
 
-constexpr int kTcM = 128;          // MMA rows per CTA (64 complex rows)
-constexpr int kTcN = 128;          // columns per CTA
+constexpr int kTcM = 128;          // MMA rows per tile (64 complex rows: real and imaginary parts)
+constexpr int kTcN = 64;           // columns per tile
 constexpr int kTcKBlk = 64;        // bf16 elements per K-block (128 bytes)
 constexpr int kTcK3 = 384;         // 3 x 2 x 64
-constexpr int kTcStages = kTcK3 / kTcKBlk;
-constexpr int kTcStageBytes = (kTcM + kTcN) * kTcKBlk * 2;
-constexpr size_t kTcSmem = (size_t)kTcStages * kTcStageBytes + 1024 + 256;
+constexpr int kTcKBlocks = kTcK3 / kTcKBlk;
+constexpr int kTcStages = 4;       // operand ring
+constexpr int kTcABytes = kTcM * kTcKBlk * 2;
+constexpr int kTcBBytes = kTcN * kTcKBlk * 2;
+constexpr int kTcStageBytes = kTcABytes + kTcBBytes;
+constexpr int kTcCBytes = kTcM * kTcN * 4;   // one C tile staged in shared memory
+constexpr int kTcThreads = 320;    // warp 0: MMA issuer, warp 1: TMA producer, warps 2-9: C tiles
+constexpr size_t kTcSmem = (size_t)kTcStages * kTcStageBytes + 2 * kTcCBytes + 1024;
 constexpr long long kSpinLimit = 1LL << 24;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// Bounded wait on an mbarrier phase; false after kSpinLimit polls or when
+// another role has flagged a failure.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *fail = nullptr) {
     for (long long it = 0; it < kSpinLimit; ++it) {
         uint32_t done;
         asm volatile(
@@ -168,6 +174,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
             : "r"(bar), "r"(parity)
             : "memory");
         if (done) return true;
+        if (fail && (it & 1023) == 1023 && *fail) return false;
     }
     return false;
 }
@@ -189,123 +196,303 @@ __host__ __device__ constexpr uint32_t umma_idesc_bf16(int m, int n) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
 }
 
-__global__ void __launch_bounds__(128, 1) k_trailing_tc(const __grid_constant__ CUtensorMap tmA,
-                                                         const __grid_constant__ CUtensorMap tmB, float *a_re,
-                                                         float *a_im, long long lda, long long a_stride, int n,
-                                                         int start, int col_end, int rows3, int cols_pad,
-                                                         int *status) {
+__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+
+// Barrier of the four C-tile warps that also ORs a predicate across them, so
+// every warp takes the same branch afterwards.
+__device__ __forceinline__ bool epi_bar_or(bool pred) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, 1, 256, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)pred)
+        : "memory");
+    return r != 0;
+}
+
+struct TcTile {
+    int mat, tm, tn;
+};
+__device__ __forceinline__ TcTile tc_tile(int t, int tiles_m, int tiles_n) {
+    const int per = tiles_m * tiles_n;
+    const int mat = t / per, rem = t - mat * per;
+    return {mat, rem / tiles_n, rem - (rem / tiles_n) * tiles_n};
+}
+
+// Persistent trailing update: each CTA walks tiles b, b + G, b + 2G, ... of
+// 64 complex rows x 64 columns (columns fastest, so consecutive tiles share
+// their L panel in L2).
+//   warp 1 (TMA producer): streams the six 64-wide K-blocks of A3 / B3 of
+//     every tile through a 4-stage ring, running ahead across tiles;
+//   warp 0 (MMA issuer): 4 x tcgen05.mma (M = 128, N = 64, K = 16) per block
+//     into one of two TMEM accumulators, releases ring slots with
+//     tcgen05.commit and signals "accumulator full";
+//   warps 2-5 (C tiles): prefetch the next tile's C (real rows, then
+//     imaginary rows) into one of two shared buffers with cp.async, drain the
+//     finished accumulator into the current buffer (C - L U), hand the
+//     accumulator back, and write the tile out with coalesced stores.
+// Shared C layout: row r holds 16 groups of 4 columns, group g at position
+// g ^ (r & 7) (aligned 16-byte copies, conflict-free float4 drain).  Every
+// wait is bounded; a timeout sets *status and the roles stop, drain their
+// copies, free TMEM and return.
+__global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_constant__ CUtensorMap tmA,
+                                                                const __grid_constant__ CUtensorMap tmB, float *a_re,
+                                                                float *a_im, long long lda, long long a_stride, int n,
+                                                                int start, int col_end, int rows3, int cols_pad,
+                                                                int tiles_m, int tiles_n, int n_tiles, int *status) {
     extern __shared__ uint8_t s_raw[];
-    __shared__ uint64_t s_full[kTcStages];
+    __shared__ uint64_t s_full[kTcStages], s_empty[kTcStages];
+    __shared__ uint64_t s_acc_full[2], s_acc_empty[2];
     __shared__ uint64_t s_done;
     __shared__ uint32_t s_tmem;
-    __shared__ int s_fail;
+    __shared__ volatile int s_fail;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int mat = blockIdx.z;
-    const int tile_m = blockIdx.y, tile_n = blockIdx.x;
     uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(s_raw) + 1023) & ~(uintptr_t)1023);
+    float *sC0 = reinterpret_cast<float *>(base + (size_t)kTcStages * kTcStageBytes);
     if (tid == 0) {
         s_fail = 0;
-        for (int s = 0; s < kTcStages; ++s)
+        for (int s = 0; s < kTcStages; ++s) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_full[s])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_empty[s])));
+        }
+        for (int b = 0; b < 2; ++b) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_acc_full[b])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 8;" ::"r"(smem_u32(&s_acc_empty[b])));
+        }
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_done)));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
-                     "r"(kTcN));
+                     "r"(2 * kTcN));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
+    const int G = gridDim.x;
+    const int my_tiles = blockIdx.x < n_tiles ? (n_tiles - 1 - blockIdx.x) / G + 1 : 0;
 
-    const int row_a = mat * rows3 + tile_m * kTcM;      // A3 row of this tile
-    const int row_b = mat * cols_pad + tile_n * kTcN;   // B3^T row of this tile
-    if (tid == 0) {
-        for (int s = 0; s < kTcStages; ++s) {
-            uint8_t *sa = base + (size_t)s * kTcStageBytes;
-            uint8_t *sb = sa + kTcM * kTcKBlk * 2;
-            const uint32_t bar = smem_u32(&s_full[s]);
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kTcStageBytes)
-                         : "memory");
-            asm volatile(
-                "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
-                ::"r"(smem_u32(sa)), "l"(reinterpret_cast<uint64_t>(&tmA)), "r"(s * kTcKBlk), "r"(row_a), "r"(bar)
-                : "memory");
-            asm volatile(
-                "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
-                ::"r"(smem_u32(sb)), "l"(reinterpret_cast<uint64_t>(&tmB)), "r"(s * kTcKBlk), "r"(row_b), "r"(bar)
-                : "memory");
-        }
-        constexpr uint32_t idesc = umma_idesc_bf16(kTcM, kTcN);
-        bool ok = true;
-        for (int s = 0; s < kTcStages && ok; ++s) {
-            if (!mbar_wait(smem_u32(&s_full[s]), 0)) { ok = false; break; }
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t sa = smem_u32(base + (size_t)s * kTcStageBytes);
-            const uint32_t sb = sa + kTcM * kTcKBlk * 2;
-#pragma unroll
-            for (int kk = 0; kk < kTcKBlk / 16; ++kk) {
-                const uint64_t da = umma_desc_sw128(sa + kk * 32);
-                const uint64_t db = umma_desc_sw128(sb + kk * 32);
-                const uint32_t acc = (s > 0 || kk > 0) ? 1u : 0u;
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\t"
-                    "setp.ne.b32 p, %4, 0;\n\t"
-                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-                    ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc)
-                    : "memory");
+    if (warp == 1) {
+        // ---- TMA producer
+        if (lane == 0) {
+            int last_use[kTcStages];
+            for (int s = 0; s < kTcStages; ++s) last_use[s] = -1;
+            bool ok = true;
+            long long g = 0;   // ring position
+            for (int i = 0; i < my_tiles && ok; ++i) {
+                const TcTile tt = tc_tile(blockIdx.x + i * G, tiles_m, tiles_n);
+                const int row_a = tt.mat * rows3 + tt.tm * kTcM;
+                const int row_b = tt.mat * cols_pad + tt.tn * kTcN;
+                for (int kb = 0; kb < kTcKBlocks; ++kb, ++g) {
+                    const int s = (int)(g % kTcStages);
+                    const int u = (int)(g / kTcStages);
+                    if (u > 0 && !mbar_wait(smem_u32(&s_empty[s]), (u - 1) & 1, &s_fail)) { ok = false; break; }
+                    uint8_t *sa = base + (size_t)s * kTcStageBytes;
+                    uint8_t *sb = sa + kTcABytes;
+                    const uint32_t bar = smem_u32(&s_full[s]);
+                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                                 "r"(kTcStageBytes)
+                                 : "memory");
+                    asm volatile(
+                        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                        ::"r"(smem_u32(sa)), "l"(reinterpret_cast<uint64_t>(&tmA)), "r"(kb * kTcKBlk), "r"(row_a),
+                          "r"(bar)
+                        : "memory");
+                    asm volatile(
+                        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                        ::"r"(smem_u32(sb)), "l"(reinterpret_cast<uint64_t>(&tmB)), "r"(kb * kTcKBlk), "r"(row_b),
+                          "r"(bar)
+                        : "memory");
+                    last_use[s] = u;
+                }
             }
+            if (!ok) {
+                s_fail = 1;
+                atomicExch(status, 3);
+            }
+            // every issued copy must land before the CTA may exit
+            for (int s = 0; s < kTcStages; ++s)
+                if (last_use[s] >= 0) mbar_wait(smem_u32(&s_full[s]), last_use[s] & 1);
         }
-        if (ok) {
+    } else if (warp == 0) {
+        // ---- MMA issuer
+        if (lane == 0) {
+            constexpr uint32_t idesc = umma_idesc_bf16(kTcM, kTcN);
+            bool ok = true;
+            long long g = 0;
+            for (int i = 0; i < my_tiles && ok; ++i) {
+                const int b = i & 1;
+                // the epilogue must have drained this accumulator (tile i - 2)
+                if (i >= 2 && !mbar_wait(smem_u32(&s_acc_empty[b]), ((i >> 1) - 1) & 1, &s_fail)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t acc_addr = tmem + (uint32_t)(b * kTcN);
+                for (int kb = 0; kb < kTcKBlocks; ++kb, ++g) {
+                    const int s = (int)(g % kTcStages);
+                    const int u = (int)(g / kTcStages);
+                    if (!mbar_wait(smem_u32(&s_full[s]), u & 1, &s_fail)) { ok = false; break; }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t sa = smem_u32(base + (size_t)s * kTcStageBytes);
+                    const uint32_t sb = sa + kTcABytes;
+#pragma unroll
+                    for (int kk = 0; kk < kTcKBlk / 16; ++kk) {
+                        const uint64_t da = umma_desc_sw128(sa + kk * 32);
+                        const uint64_t db = umma_desc_sw128(sb + kk * 32);
+                        const uint32_t acc = (kb > 0 || kk > 0) ? 1u : 0u;
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\t"
+                            "setp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                            ::"r"(acc_addr), "l"(da), "l"(db), "r"(idesc), "r"(acc)
+                            : "memory");
+                    }
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                     smem_u32(&s_empty[s]))
+                                 : "memory");
+                }
+                if (!ok) break;
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_u32(&s_acc_full[b]))
+                             : "memory");
+            }
+            if (!ok) {
+                s_fail = 1;
+                atomicExch(status, 1);
+            }
+            // completion of everything issued, before TMEM may be freed
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                              smem_u32(&s_done))
                          : "memory");
-        } else {
-            s_fail = 1;
-            atomicExch(status, 1);
-            // let outstanding TMA copies land before the CTA exits
-            for (int s = 0; s < kTcStages; ++s) mbar_wait(smem_u32(&s_full[s]), 0);
+            mbar_wait(smem_u32(&s_done), 0);
         }
-    }
-    __syncthreads();
-    bool ok = s_fail == 0;
-    if (ok && !mbar_wait(smem_u32(&s_done), 0)) {
-        ok = false;
-        atomicExch(status, 2);
-    }
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (ok) {
-        // TMEM lane = MMA row: warp w owns lanes 32w .. 32w+31
-        const int rr = warp * 32 + lane;
-        const int crow = start + tile_m * 64 + (rr & 63);
-        float *dst = ((rr < 64) ? a_re : a_im) + (size_t)mat * a_stride + (size_t)crow * lda;
-        for (int c0 = 0; c0 < kTcN; c0 += 32) {
-            uint32_t v[32];
-            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-                "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
-                  "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
-                  "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
-                  "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-                : "r"(taddr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (crow < n) {
-                const int gc0 = start + tile_n * kTcN + c0;
-#pragma unroll
-                for (int c = 0; c < 32; ++c)
-                    if (gc0 + c < col_end) dst[gc0 + c] -= __uint_as_float(v[c]);
+    } else {
+        // ---- C tiles: 8 warps; thread et owns column group gq = et & 15 of
+        // rows (et >> 4) + 16 it; warp pair (w, w + 4) shares TMEM lane
+        // quarter w & 3 and drains columns [32 h, 32 h + 32), h = (w - 2) >> 2.
+        const int et = tid - 64;   // 0..255
+        const int q = warp & 3;
+        const int h = (warp - 2) >> 2;
+        const int gq = et & 15, r_first = et >> 4;
+        auto sidx = [](int r, int c) { return r * kTcN + ((((c >> 2) ^ (r & 7)) << 2) | (c & 3)); };
+        auto prefetch = [&](int t, float *sC) {
+            const TcTile tt = tc_tile(t, tiles_m, tiles_n);
+            const int row_c0 = start + tt.tm * 64, gcol = start + tt.tn * kTcN + 4 * gq;
+            if (gcol >= col_end) {
+                asm volatile("cp.async.commit_group;" ::: "memory");
+                return;
             }
+            const bool full4 = gcol + 3 < col_end;
+            const float *mre = a_re + (size_t)tt.mat * a_stride + gcol, *mim = a_im + (size_t)tt.mat * a_stride + gcol;
+#pragma unroll
+            for (int it = 0; it < kTcM / 16; ++it) {
+                const int r = r_first + 16 * it;
+                const int grow = row_c0 + (r & 63);
+                if (grow >= n) continue;
+                const float *src = ((r < 64) ? mre : mim) + (size_t)grow * lda;
+                const uint32_t dst = smem_u32(sC + sidx(r, 4 * gq));
+                if (full4 && (reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+                } else {
+                    for (int j = 0; j < 4; ++j)
+                        if (gcol + j < col_end)
+                            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                                             smem_u32(sC + sidx(r, 4 * gq + j))),
+                                         "l"(src + j)
+                                         : "memory");
+                }
+            }
+            asm volatile("cp.async.commit_group;" ::: "memory");
+        };
+        if (my_tiles > 0) prefetch(blockIdx.x, sC0);
+        for (int i = 0; i < my_tiles; ++i) {
+            const int b = i & 1;
+            float *sC = sC0 + (size_t)b * (kTcM * kTcN);
+            if (i + 1 < my_tiles) {
+                prefetch(blockIdx.x + (i + 1) * G, sC0 + (size_t)(b ^ 1) * (kTcM * kTcN));
+                asm volatile("cp.async.wait_group 1;" ::: "memory");
+            } else {
+                asm volatile("cp.async.wait_group 0;" ::: "memory");
+            }
+            bool ok = true;
+            if (!mbar_wait(smem_u32(&s_acc_full[b]), (i >> 1) & 1, &s_fail)) {
+                ok = false;
+                atomicExch(status, 2);
+                s_fail = 1;
+            }
+            // the C tile's copies from every thread have landed; stop together on any failure
+            if (epi_bar_or(!ok || s_fail != 0)) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            {
+                const int r = q * 32 + lane;
+                const int c0 = 32 * h;
+                uint32_t v[32];
+                const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * kTcN + c0);
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                    "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+                    "[%32];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                      "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                      "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+                      "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                    : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int jj = 0; jj < 8; ++jj) {
+                    float4 *p4 = reinterpret_cast<float4 *>(sC + sidx(r, c0 + 4 * jj));
+                    float4 cv = *p4;
+                    cv.x -= __uint_as_float(v[4 * jj]);
+                    cv.y -= __uint_as_float(v[4 * jj + 1]);
+                    cv.z -= __uint_as_float(v[4 * jj + 2]);
+                    cv.w -= __uint_as_float(v[4 * jj + 3]);
+                    *p4 = cv;
+                }
+            }
+            // hand the accumulator back (one arrival per warp)
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&s_acc_empty[b])) : "memory");
+            epi_bar();   // the whole tile is drained
+            {
+                const TcTile tt = tc_tile(blockIdx.x + i * G, tiles_m, tiles_n);
+                const int row_c0 = start + tt.tm * 64, gcol = start + tt.tn * kTcN + 4 * gq;
+                if (gcol < col_end) {
+                    const bool full4 = gcol + 3 < col_end;
+                    float *mre = a_re + (size_t)tt.mat * a_stride + gcol, *mim = a_im + (size_t)tt.mat * a_stride + gcol;
+#pragma unroll
+                    for (int it = 0; it < kTcM / 16; ++it) {
+                        const int r = r_first + 16 * it;
+                        const int grow = row_c0 + (r & 63);
+                        if (grow >= n) continue;
+                        float *dst = ((r < 64) ? mre : mim) + (size_t)grow * lda;
+                        const float4 cv = *reinterpret_cast<const float4 *>(sC + sidx(r, 4 * gq));
+                        if (full4 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+                            *reinterpret_cast<float4 *>(dst) = cv;
+                        } else {
+                            const float e4[4] = {cv.x, cv.y, cv.z, cv.w};
+                            for (int j = 0; j < 4; ++j)
+                                if (gcol + j < col_end) dst[j] = e4[j];
+                        }
+                    }
+                }
+            }
+            epi_bar();   // buffer b may be refilled by the prefetch of tile i + 2
         }
+        asm volatile("cp.async.wait_all;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcN));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kTcN));
 }
 
 // Pack L21 (rows start..n, cols k0..k0+64) into A3 (K-major, bf16 hi/lo).
@@ -453,10 +640,18 @@ int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int 
         k_pack_b<<<grd, 128, 0, st>>>(a_re, a_im, lda, a_stride, start, col_end, k0, w->cols_pad, tiles_n * kTcN, w->B3);
         HBEM_LAUNCH_CHECK("k_pack_b");
     }
-    HBEM_CUDA(cudaFuncSetAttribute(k_trailing_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
-    dim3 grd(tiles_n, tiles_m, batch);
-    k_trailing_tc<<<grd, 128, kTcSmem, st>>>(w->ma, w->mb, a_re, a_im, lda, a_stride, n, start, col_end, w->rows3,
-                                            w->cols_pad, status);
+    static int n_sm = 0;
+    if (!n_sm) {
+        int dev = 0;
+        HBEM_CUDA(cudaGetDevice(&dev));
+        HBEM_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+        HBEM_CUDA(cudaFuncSetAttribute(k_trailing_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+    }
+    const long long total = (long long)tiles_m * tiles_n * batch;
+    if (total > 0x7fffffffLL) return fail(HBEM_ERR_ARG, "trailing update: too many tiles");
+    const int grid = (int)std::min<long long>(total, n_sm);
+    k_trailing_tc<<<grid, kTcThreads, kTcSmem, st>>>(w->ma, w->mb, a_re, a_im, lda, a_stride, n, start, col_end,
+                                                    w->rows3, w->cols_pad, tiles_m, tiles_n, (int)total, status);
     HBEM_LAUNCH_CHECK("k_trailing_tc");
     return HBEM_OK;
 }

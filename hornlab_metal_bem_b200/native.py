@@ -489,10 +489,11 @@ class NativeSession:
         return out
 
     def _factor_solve_refine(self, Kr, Ki, br, bi, N, F, mixed, tol, max_iter):
-        """LU (+ BF16x3 refinement) of F systems of order N; returns x, info, iters, resid."""
+        """LU (+ BF16x3 refinement) of F systems of order N stored (F, N, lda); returns x, info, iters, resid."""
         import torch
 
         dev, st = Kr.device, _stream_ptr()
+        lda = int(Kr.shape[2])
         K0r = K0i = None
         if mixed:
             K0r, K0i = Kr.clone(), Ki.clone()
@@ -500,14 +501,14 @@ class NativeSession:
         info = torch.empty(F, dtype=torch.int32, device=dev)
         xr, xi = br.clone(), bi.clone()
         prec = HBEM_PREC_MIXED if mixed else HBEM_PREC_PLAIN
-        check(self.lib.hbem_lu_factor(N, F, _t_ptr(Kr), _t_ptr(Ki), N, N * N, _t_ptr(piv), N, _t_ptr(info), prec, st),
-              "hbem_lu_factor", self.lib)
-        check(self.lib.hbem_lu_solve(N, 1, F, _t_ptr(Kr), _t_ptr(Ki), N, N * N, _t_ptr(piv), N, _t_ptr(xr), _t_ptr(xi),
-                                     1, N, HBEM_TRANS_N, st), "hbem_lu_solve", self.lib)
+        check(self.lib.hbem_lu_factor(N, F, _t_ptr(Kr), _t_ptr(Ki), lda, N * lda, _t_ptr(piv), N, _t_ptr(info), prec,
+                                      st), "hbem_lu_factor", self.lib)
+        check(self.lib.hbem_lu_solve(N, 1, F, _t_ptr(Kr), _t_ptr(Ki), lda, N * lda, _t_ptr(piv), N, _t_ptr(xr),
+                                     _t_ptr(xi), 1, N, HBEM_TRANS_N, st), "hbem_lu_solve", self.lib)
         iters = torch.zeros(F, dtype=torch.int32, device=dev)
         resid = torch.zeros(F, dtype=torch.float64, device=dev)
         if mixed:
-            check(self.lib.hbem_refine(N, F, _t_ptr(K0r), _t_ptr(K0i), N, N * N, _t_ptr(Kr), _t_ptr(Ki), N * N,
+            check(self.lib.hbem_refine(N, F, _t_ptr(K0r), _t_ptr(K0i), lda, N * lda, _t_ptr(Kr), _t_ptr(Ki), N * lda,
                                        _t_ptr(piv), N, _t_ptr(br), _t_ptr(bi), N, _t_ptr(xr), _t_ptr(xi), N,
                                        float(tol), int(max_iter), _t_ptr(iters), _t_ptr(resid), st),
                   "hbem_refine", self.lib)
@@ -547,8 +548,9 @@ class NativeSession:
         return self._chunk_out(ev, times, xr, xi, qa_r, qa_i, fr, fi, info, info_ap, iters, resid, tavg)
 
     def coupled_ib_system(self, k_re, k_im, kf, q):
-        """The augmented coupled system on the device: K (F, N, N), [0; b] (F, N), N = m + n, and the
-        per-frequency scale alpha of the aperture unknowns (q_a = alpha * x[:m])."""
+        """The augmented coupled system on the device: K (F, N, L) with row stride L = N rounded up to a
+        multiple of 4, [0; b] (F, N), N = m + n, and the per-frequency scale alpha of the aperture
+        unknowns (q_a = alpha * x[:m])."""
         torch = require_cuda()
         dev, st = torch.device("cuda", self.device), _stream_ptr()
         k_re = np.ascontiguousarray(np.atleast_1d(k_re), dtype=np.float32)
@@ -556,13 +558,14 @@ class NativeSession:
         kf = np.ascontiguousarray(np.atleast_1d(kf), dtype=np.float32)
         F, n, m, T = k_re.shape[0], self.n_dof, self.m_aperture, self.n_triangles
         N = n + m
-        Kr = torch.empty((F, N, N), dtype=torch.float32, device=dev); Ki = torch.empty_like(Kr)
+        L = (N + 3) // 4 * 4   # row stride: 16-byte aligned rows for the LU's vector paths
+        Kr = torch.empty((F, N, L), dtype=torch.float32, device=dev); Ki = torch.empty_like(Kr)
         rr = torch.zeros((F, N), dtype=torch.float32, device=dev); ri = torch.zeros_like(rr)
         qr, qi = self._split_device(q, (F, T), dev)
-        off_a, off_b = m * N + m, m
+        off_a, off_b = m * L + m, m
         check(self.lib.hbem_assemble(
             self.handle, F, _np_ptr(k_re), _np_ptr(k_im), _t_ptr(qr), _t_ptr(qi), T, None, None,
-            ctypes.c_void_p(Kr.data_ptr() + 4 * off_a), ctypes.c_void_p(Ki.data_ptr() + 4 * off_a), N, N * N,
+            ctypes.c_void_p(Kr.data_ptr() + 4 * off_a), ctypes.c_void_p(Ki.data_ptr() + 4 * off_a), L, N * L,
             ctypes.c_void_p(rr.data_ptr() + 4 * off_b), ctypes.c_void_p(ri.data_ptr() + 4 * off_b), N,
             HBEM_ASM_CORRECTED, st), "hbem_assemble", self.lib)
         sia_r = torch.empty((F, n, m), dtype=torch.float32, device=dev); sia_i = torch.empty_like(sia_r)
@@ -572,7 +575,7 @@ class NativeSession:
               "hbem_aperture_assemble", self.lib)
         alpha = torch.empty(F, dtype=torch.float32, device=dev)
         check(self.lib.hbem_coupled_ib_augment(self.handle, F, _t_ptr(sia_r), _t_ptr(sia_i), _t_ptr(saa_r),
-                                               _t_ptr(saa_i), _t_ptr(Kr), _t_ptr(Ki), N, N * N, _t_ptr(alpha), st),
+                                               _t_ptr(saa_i), _t_ptr(Kr), _t_ptr(Ki), L, N * L, _t_ptr(alpha), st),
               "hbem_coupled_ib_augment", self.lib)
         return Kr, Ki, rr, ri, alpha
 
