@@ -262,7 +262,9 @@ def run_b200(args, w):
     buf = w["buf"]
     F = len(w["freqs"])
     sess = NativeSession(buf, symmetry_plane=w["cfg"].native_symmetry_plane, check_open_edges=False)
-    rs = ResidentSweep(sess, w["k_re"], w["k_im"], w["q"], w["obs"], w["tags"], precision=args.precision)
+    want_rcond = w["cfg"].dense_solve_rcond_warning_threshold > 0   # the reference's per-case cgecon
+    rs = ResidentSweep(sess, w["k_re"], w["k_im"], w["q"], w["obs"], w["tags"], precision=args.precision,
+                       rcond=want_rcond)
     n = rs.n
     stream = torch.cuda.current_stream()
 
@@ -342,7 +344,7 @@ def run_b200(args, w):
     # ---- e2e through the reference-facing batch call with host buffers
     q = w["q"]
     e2e_kw = dict(k_imag_f32=w["k_im"], source_tags=w["tags"], impedance_source_tag=min(w["tags"]),
-                  precision=args.precision)
+                  precision=args.precision, compute_rcond=want_rcond)
     for _ in range(max(1, args.warmup)):
         sess.assemble_solve_evaluate_standard_neumann_batch(w["freqs"], w["k_re"], q, w["obs"], **e2e_kw)
     torch.cuda.synchronize()
@@ -390,7 +392,8 @@ def run_b200(args, w):
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c64 (f32 planar)", "data": "synthetic",
         "config": {"workload": w["desc"], "n_dof": buf.p1_dof_count, "n_triangles": T, "n_freq": F,
-                   "n_obs": n_obs, "precision": args.precision, "parallelism": f"replicas x{world} (frequency-parallel)",
+                   "n_obs": n_obs, "precision": args.precision, "rcond_estimate": bool(want_rcond),
+                   "parallelism": f"replicas x{world} (frequency-parallel)",
                    "l2": f"working set {2 * F * n * n * 4 / 1e6:.0f} MB of dense matrices > 126 MB L2"},
         "e2e": {"value": world * F * args.steps / (e2e_ms * 1e-3), "unit": "freq-solves/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

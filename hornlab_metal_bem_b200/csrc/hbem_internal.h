@@ -17,6 +17,7 @@ int fail(int code, const std::string &msg);
 int cuda_fail(cudaError_t e, const char *what);
 void count_launch(long long n = 1);
 int tuning(int key);   // HBEM_TUNE_* value, 0 = built-in choice
+void keep_pool_memory();   // cache freed stream-ordered allocations of the current device
 
 #define HBEM_CUDA(call)                                        \
     do {                                                       \

@@ -464,247 +464,197 @@ __global__ void __launch_bounds__(kSwapThreads) k_swap_trsm(float *a_re, float *
 }
 
 // ---------------------------------------------------------------------------
-// Triangular solves.  One CTA per (matrix, right-hand side); x staged in
-// shared memory; 32-row diagonal blocks solved by warp 0, off-diagonal
-// updates by all warps with coalesced row reads.
-// TRANS: 0 = A, 1 = A^T, 2 = A^H.
+// Triangular solves, one CTA per (matrix, right-hand side): x staged in
+// shared memory; 32-row diagonal blocks staged as a tile and solved by a
+// register column sweep in warp 0; the block's contribution to every later
+// row applied by one thread per row (op = A: the row's 32 contiguous factor
+// entries; op = A^T / A^H: consecutive threads read consecutive columns of
+// the block's factor rows).  Best when many matrices / right-hand sides
+// fill the GPU; TR: 0 = A, 1 = A^T, 2 = A^H.
 // ---------------------------------------------------------------------------
-template <int TRANS>
-__global__ void __launch_bounds__(512) k_getrs(int n, const float *lu_re, const float *lu_im, long long lda,
-                                               long long a_stride, const int *piv, long long piv_stride, float *b_re,
-                                               float *b_im, long long ldb, long long b_stride, int nrhs) {
+constexpr int kGetrsThreads = 512;
+
+template <int TR>
+__device__ __forceinline__ void op_at(const float *Ar, const float *Ai, long long lda, int i, int j, float &re,
+                                      float &im) {
+    if (TR == 0) {
+        re = Ar[(size_t)i * lda + j];
+        im = Ai[(size_t)i * lda + j];
+    } else {
+        re = Ar[(size_t)j * lda + i];
+        im = TR == 2 ? -Ai[(size_t)j * lda + i] : Ai[(size_t)j * lda + i];
+    }
+}
+
+// One triangular phase on x in shared memory: lower (blocks from the top) or
+// upper (from the bottom), unit or non-unit diagonal.
+template <bool LOWER, bool UNIT, int TR>
+__device__ void getrs_phase(int n, const float *Ar, const float *Ai, long long lda, float *xr, float *xi, float *t_r,
+                            float *t_i) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nblk = (n + 31) / 32;
+    for (int q = 0; q < nblk; ++q) {
+        const int b = LOWER ? q : nblk - 1 - q;
+        const int j0 = b * 32, jb = min(32, n - j0);
+        for (int e = tid; e < 32 * 32; e += blockDim.x) {
+            const int r = e >> 5, c = e & 31;
+            float tr = 0.f, ti = 0.f;
+            if (r < jb && c < jb && (LOWER ? c <= r : c >= r)) op_at<TR>(Ar, Ai, lda, j0 + r, j0 + c, tr, ti);
+            t_r[r * 33 + c] = tr;
+            t_i[r * 33 + c] = ti;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            float vr = lane < jb ? xr[j0 + lane] : 0.f, vi = lane < jb ? xi[j0 + lane] : 0.f;
+            for (int t = 0; t < jb; ++t) {
+                const int j = LOWER ? t : jb - 1 - t;
+                if (!UNIT && lane == j) {
+                    const float dr = t_r[j * 33 + j], di = t_i[j * 33 + j];
+                    const float den = 1.0f / (dr * dr + di * di);
+                    const float yr = vr, yi = vi;
+                    vr = (yr * dr + yi * di) * den;
+                    vi = (yi * dr - yr * di) * den;
+                }
+                const float jr = __shfl_sync(0xffffffffu, vr, j), ji = __shfl_sync(0xffffffffu, vi, j);
+                if (LOWER ? lane > j : lane < j) {
+                    const float lr = t_r[lane * 33 + j], li = t_i[lane * 33 + j];
+                    vr -= lr * jr - li * ji;
+                    vi -= lr * ji + li * jr;
+                }
+            }
+            if (lane < jb) { xr[j0 + lane] = vr; xi[j0 + lane] = vi; }
+        }
+        __syncthreads();
+        // later rows: below the block (lower) or above it (upper)
+        const int r0 = LOWER ? j0 + jb : 0, r1 = LOWER ? n : j0;
+        const float cs = TR == 2 ? -1.f : 1.f;
+        for (int i = r0 + tid; i < r1; i += blockDim.x) {
+            float pr = 0.f, pi = 0.f;
+            if (TR == 0) {
+                const float *rr = Ar + (size_t)i * lda + j0, *ri = Ai + (size_t)i * lda + j0;
+#pragma unroll 8
+                for (int c = 0; c < jb; ++c) {
+                    const float ar = rr[c], ai = ri[c];
+                    pr += ar * xr[j0 + c] - ai * xi[j0 + c];
+                    pi += ar * xi[j0 + c] + ai * xr[j0 + c];
+                }
+            } else {
+#pragma unroll 8
+                for (int c = 0; c < jb; ++c) {
+                    const float ar = Ar[(size_t)(j0 + c) * lda + i], ai = cs * Ai[(size_t)(j0 + c) * lda + i];
+                    pr += ar * xr[j0 + c] - ai * xi[j0 + c];
+                    pi += ar * xi[j0 + c] + ai * xr[j0 + c];
+                }
+            }
+            xr[i] -= pr;
+            xi[i] -= pi;
+        }
+        __syncthreads();
+    }
+}
+
+template <int TR>
+__global__ void __launch_bounds__(kGetrsThreads) k_getrs(int n, const float *lu_re, const float *lu_im, long long lda,
+                                                         long long a_stride, const int *piv, long long piv_stride,
+                                                         float *b_re, float *b_im, long long ldb, long long b_stride) {
     extern __shared__ float s_x[];
+    __shared__ float t_r[32 * 33], t_i[32 * 33];
+    __shared__ int s_pv[1024];
     float *xr = s_x, *xi = s_x + n;
     const int mat = blockIdx.y, rhs = blockIdx.x;
     const float *Ar = lu_re + (size_t)mat * a_stride, *Ai = lu_im + (size_t)mat * a_stride;
-    const int *pv = piv + (size_t)mat * piv_stride;
-    float *br = b_re + (size_t)mat * b_stride, *bi = b_im + (size_t)mat * b_stride;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const float cs = TRANS == 2 ? -1.f : 1.f;  // conjugation sign on the imaginary part
-    for (int i = tid; i < n; i += blockDim.x) {
-        xr[i] = br[(size_t)i * ldb + rhs];
-        xi[i] = bi[(size_t)i * ldb + rhs];
+    float *br = b_re + (size_t)mat * b_stride + rhs, *bi = b_im + (size_t)mat * b_stride + rhs;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        xr[i] = br[(size_t)i * ldb];
+        xi[i] = bi[(size_t)i * ldb];
     }
+    const int *pv = piv ? piv + (size_t)mat * piv_stride : nullptr;
+    auto permute = [&](bool reverse) {
+        const int nchunk = (n + 1023) / 1024;
+        for (int qq = 0; qq < nchunk; ++qq) {
+            const int base = (reverse ? nchunk - 1 - qq : qq) * 1024;
+            const int cnt = min(1024, n - base);
+            __syncthreads();
+            for (int i = threadIdx.x; i < cnt; i += blockDim.x) s_pv[i] = pv[base + i];
+            __syncthreads();
+            if (threadIdx.x == 0)
+                for (int t = 0; t < cnt; ++t) {
+                    const int k = reverse ? cnt - 1 - t : t;
+                    const int p = s_pv[k], r = base + k;
+                    if (p != r && p >= 0 && p < n) {
+                        float tmp = xr[r]; xr[r] = xr[p]; xr[p] = tmp;
+                        tmp = xi[r]; xi[r] = xi[p]; xi[p] = tmp;
+                    }
+                }
+        }
+    };
+    if (TR == 0 && pv) permute(false);
     __syncthreads();
-    // element accessors of op(L) / op(U)
-    auto Lr_ = [&](int r, int c) { return TRANS ? Ar[(size_t)c * lda + r] : Ar[(size_t)r * lda + c]; };
-    auto Li_ = [&](int r, int c) { return TRANS ? cs * Ai[(size_t)c * lda + r] : Ai[(size_t)r * lda + c]; };
-    if (TRANS == 0) {
-        if (tid == 0)
-            for (int i = 0; i < n; ++i) {
-                const int p = pv[i];
-                if (p != i) {
-                    float t = xr[i]; xr[i] = xr[p]; xr[p] = t;
-                    t = xi[i]; xi[i] = xi[p]; xi[p] = t;
-                }
-            }
-        __syncthreads();
-        // forward: L unit lower (rows i, cols < i)
-        for (int j0 = 0; j0 < n; j0 += 32) {
-            const int jb = min(32, n - j0);
-            if (warp == 0) {
-                for (int i = 1; i < jb; ++i) {
-                    float pr = 0, pi = 0;
-                    if (lane < i) {
-                        const float lr = Ar[(size_t)(j0 + i) * lda + j0 + lane], li = Ai[(size_t)(j0 + i) * lda + j0 + lane];
-                        pr = lr * xr[j0 + lane] - li * xi[j0 + lane];
-                        pi = lr * xi[j0 + lane] + li * xr[j0 + lane];
-                    }
-                    for (int o = 16; o > 0; o >>= 1) {
-                        pr += __shfl_xor_sync(0xffffffffu, pr, o);
-                        pi += __shfl_xor_sync(0xffffffffu, pi, o);
-                    }
-                    if (lane == 0) { xr[j0 + i] -= pr; xi[j0 + i] -= pi; }
-                    __syncwarp();
-                }
-            }
-            __syncthreads();
-            // rows below the block: one thread per row, independent loads
-            for (int i = j0 + jb + tid; i < n; i += blockDim.x) {
-                const float *lr_row = Ar + (size_t)i * lda + j0, *li_row = Ai + (size_t)i * lda + j0;
-                float pr = 0, pi = 0;
-#pragma unroll 8
-                for (int c = 0; c < jb; ++c) {
-                    const float lr = lr_row[c], li = li_row[c];
-                    pr += lr * xr[j0 + c] - li * xi[j0 + c];
-                    pi += lr * xi[j0 + c] + li * xr[j0 + c];
-                }
-                xr[i] -= pr;
-                xi[i] -= pi;
-            }
-            __syncthreads();
-        }
-        // backward: U upper (non-unit)
-        for (int j1 = n; j1 > 0; j1 -= 32) {
-            const int j0 = max(0, j1 - 32), jb = j1 - j0;
-            if (warp == 0) {
-                for (int i = jb - 1; i >= 0; --i) {
-                    float pr = 0, pi = 0;
-                    if (lane > i && lane < jb) {
-                        const float ur = Ar[(size_t)(j0 + i) * lda + j0 + lane], ui = Ai[(size_t)(j0 + i) * lda + j0 + lane];
-                        pr = ur * xr[j0 + lane] - ui * xi[j0 + lane];
-                        pi = ur * xi[j0 + lane] + ui * xr[j0 + lane];
-                    }
-                    for (int o = 16; o > 0; o >>= 1) {
-                        pr += __shfl_xor_sync(0xffffffffu, pr, o);
-                        pi += __shfl_xor_sync(0xffffffffu, pi, o);
-                    }
-                    if (lane == 0) {
-                        const float dr = Ar[(size_t)(j0 + i) * lda + j0 + i], di = Ai[(size_t)(j0 + i) * lda + j0 + i];
-                        const float yr = xr[j0 + i] - pr, yi = xi[j0 + i] - pi;
-                        const float den = 1.0f / (dr * dr + di * di);
-                        xr[j0 + i] = (yr * dr + yi * di) * den;
-                        xi[j0 + i] = (yi * dr - yr * di) * den;
-                    }
-                    __syncwarp();
-                }
-            }
-            __syncthreads();
-            for (int i = tid; i < j0; i += blockDim.x) {
-                const float *ur_row = Ar + (size_t)i * lda + j0, *ui_row = Ai + (size_t)i * lda + j0;
-                float pr = 0, pi = 0;
-#pragma unroll 8
-                for (int c = 0; c < jb; ++c) {
-                    const float ur = ur_row[c], ui = ui_row[c];
-                    pr += ur * xr[j0 + c] - ui * xi[j0 + c];
-                    pi += ur * xi[j0 + c] + ui * xr[j0 + c];
-                }
-                xr[i] -= pr;
-                xi[i] -= pi;
-            }
-            __syncthreads();
-        }
+    if (TR == 0) {
+        getrs_phase<true, true, 0>(n, Ar, Ai, lda, xr, xi, t_r, t_i);
+        getrs_phase<false, false, 0>(n, Ar, Ai, lda, xr, xi, t_r, t_i);
     } else {
-        // op(A) = U^op L^op P ; solve U^op z = b (forward, U^op lower, non-unit),
-        // then L^op w = z (backward, unit upper), then x = P^T w.
-        for (int j0 = 0; j0 < n; j0 += 32) {
-            const int jb = min(32, n - j0);
-            if (warp == 0) {
-                for (int i = 0; i < jb; ++i) {
-                    float pr = 0, pi = 0;
-                    if (lane < i) {
-                        // (U^op)[r][c] = op(U[c][r]), r = j0+i, c = j0+lane
-                        const float ur = Ar[(size_t)(j0 + lane) * lda + j0 + i];
-                        const float ui = cs * Ai[(size_t)(j0 + lane) * lda + j0 + i];
-                        pr = ur * xr[j0 + lane] - ui * xi[j0 + lane];
-                        pi = ur * xi[j0 + lane] + ui * xr[j0 + lane];
-                    }
-                    for (int o = 16; o > 0; o >>= 1) {
-                        pr += __shfl_xor_sync(0xffffffffu, pr, o);
-                        pi += __shfl_xor_sync(0xffffffffu, pi, o);
-                    }
-                    if (lane == 0) {
-                        const float dr = Ar[(size_t)(j0 + i) * lda + j0 + i], di = cs * Ai[(size_t)(j0 + i) * lda + j0 + i];
-                        const float yr = xr[j0 + i] - pr, yi = xi[j0 + i] - pi;
-                        const float den = 1.0f / (dr * dr + di * di);
-                        xr[j0 + i] = (yr * dr + yi * di) * den;
-                        xi[j0 + i] = (yi * dr - yr * di) * den;
-                    }
-                    __syncwarp();
-                }
-            }
-            __syncthreads();
-            // rows i >= j0+jb: x_i -= sum_{c in block} op(U[c][i]) x_c.  Column i of
-            // U^op is row i of U: read U[c][i] with lanes over i for coalescing.
-            for (int i0 = j0 + jb; i0 < n; i0 += blockDim.x) {
-                const int i = i0 + tid;
-                if (i < n) {
-                    float pr = 0, pi = 0;
-                    for (int c = 0; c < jb; ++c) {
-                        const float ur = Ar[(size_t)(j0 + c) * lda + i], ui = cs * Ai[(size_t)(j0 + c) * lda + i];
-                        pr += ur * xr[j0 + c] - ui * xi[j0 + c];
-                        pi += ur * xi[j0 + c] + ui * xr[j0 + c];
-                    }
-                    xr[i] -= pr;
-                    xi[i] -= pi;
-                }
-            }
-            __syncthreads();
-        }
-        for (int j1 = n; j1 > 0; j1 -= 32) {
-            const int j0 = max(0, j1 - 32), jb = j1 - j0;
-            if (warp == 0) {
-                for (int i = jb - 1; i >= 0; --i) {
-                    float pr = 0, pi = 0;
-                    if (lane > i && lane < jb) {
-                        // (L^op)[r][c] = op(L[c][r]), r = j0+i, c = j0+lane > r
-                        const float lr = Lr_(j0 + i, j0 + lane), li = Li_(j0 + i, j0 + lane);
-                        pr = lr * xr[j0 + lane] - li * xi[j0 + lane];
-                        pi = lr * xi[j0 + lane] + li * xr[j0 + lane];
-                    }
-                    for (int o = 16; o > 0; o >>= 1) {
-                        pr += __shfl_xor_sync(0xffffffffu, pr, o);
-                        pi += __shfl_xor_sync(0xffffffffu, pi, o);
-                    }
-                    if (lane == 0) { xr[j0 + i] -= pr; xi[j0 + i] -= pi; }
-                    __syncwarp();
-                }
-            }
-            __syncthreads();
-            for (int i0 = 0; i0 < j0; i0 += blockDim.x) {
-                const int i = i0 + tid;
-                if (i < j0) {
-                    float pr = 0, pi = 0;
-                    for (int c = 0; c < jb; ++c) {
-                        const float lr = Ar[(size_t)(j0 + c) * lda + i], li = cs * Ai[(size_t)(j0 + c) * lda + i];
-                        pr += lr * xr[j0 + c] - li * xi[j0 + c];
-                        pi += lr * xi[j0 + c] + li * xr[j0 + c];
-                    }
-                    xr[i] -= pr;
-                    xi[i] -= pi;
-                }
-            }
-            __syncthreads();
-        }
-        if (tid == 0)
-            for (int i = n - 1; i >= 0; --i) {
-                const int p = pv[i];
-                if (p != i) {
-                    float t = xr[i]; xr[i] = xr[p]; xr[p] = t;
-                    t = xi[i]; xi[i] = xi[p]; xi[p] = t;
-                }
-            }
-        __syncthreads();
+        getrs_phase<true, false, TR>(n, Ar, Ai, lda, xr, xi, t_r, t_i);
+        getrs_phase<false, true, TR>(n, Ar, Ai, lda, xr, xi, t_r, t_i);
     }
-    for (int i = tid; i < n; i += blockDim.x) {
-        br[(size_t)i * ldb + rhs] = xr[i];
-        bi[(size_t)i * ldb + rhs] = xi[i];
+    if (TR != 0 && pv) permute(true);
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        br[(size_t)i * ldb] = xr[i];
+        bi[(size_t)i * ldb] = xi[i];
     }
 }
 
 // ---------------------------------------------------------------------------
-// Blocked no-transpose solve for many CTAs per right-hand side.  The rows are
-// cut into kTB-row blocks.  One launch per block step: CTA 0 of each
-// (rhs, matrix) applies the final block's x to the next block's rows and then
-// solves that block's diagonal triangle; the other CTAs apply the final
-// block's x to all later rows (warp per row, coalesced row reads).  A
-// prologue CTA per (rhs, matrix) applies the row interchanges (forward only)
-// and solves the first block.  x lives in b throughout.
+// Blocked solves for many CTAs per right-hand side, op(A) = A, A^T or A^H
+// (TR = 0, 1, 2).  With P A = L U:
+//   op = A:    x = U^-1 L^-1 P b       (L unit lower, then U upper)
+//   op = A^T:  x = P^T L^-T U^-T b     (U^T lower non-unit, then L^T upper unit)
+//   op = A^H:  the same with conjugates.
+// The rows are cut into kTB-row blocks.  One launch per block step: CTA 0
+// of each (rhs, matrix) applies the finished block's x to the next block's
+// rows and solves that block's diagonal triangle; the other CTAs apply the
+// finished block to all later rows (op = A: warp per row over the row's
+// contiguous segment; op = A^T / A^H: thread per row over the block's
+// contiguous rows of the factor).  A prologue CTA per (rhs, matrix) applies
+// the interchanges (op = A) and solves the first block; an epilogue CTA
+// applies the reverse interchanges (op = A^T / A^H).  x lives in b.
 // ---------------------------------------------------------------------------
 constexpr int kTB = 128;          // rows per block step
 constexpr int kTrsvThreads = 256;
-constexpr int kTrsvRows = 64;     // rows per update CTA (8 warps x 8 rows)
+constexpr int kTrsvRows = 64;     // rows per update CTA, op = A (8 warps x 8 rows)
+constexpr int kTrsvRowsT = 256;   // rows per update CTA, op = A^T / A^H (thread per row)
 
-// Solve the diagonal triangle of rows [g0, g1) in place (x in global), unit
-// lower (UPPER = false, 32-row sub-blocks from the top) or non-unit upper
-// (UPPER = true, from the bottom).  All kTrsvThreads threads take part.
-template <bool UPPER>
+// element (i, j) of op(A) from the stored factors
+template <int TR>
+__device__ __forceinline__ void op_elem(const float *Ar, const float *Ai, long long lda, int i, int j, float &re,
+                                        float &im) {
+    if (TR == 0) {
+        re = Ar[(size_t)i * lda + j];
+        im = Ai[(size_t)i * lda + j];
+    } else {
+        re = Ar[(size_t)j * lda + i];
+        im = TR == 2 ? -Ai[(size_t)j * lda + i] : Ai[(size_t)j * lda + i];
+    }
+}
+
+// Solve the diagonal triangle of op-rows [g0, g1) in place (x in global):
+// lower (sub-blocks from the top) or upper (from the bottom), unit or
+// non-unit diagonal.  All kTrsvThreads threads take part.
+template <bool LOWER, bool UNIT, int TR>
 __device__ void trsv_diag(const float *Ar, const float *Ai, long long lda, float *xr, float *xi, long long ldb,
                           int g0, int g1, float *s_tr, float *s_ti, float *s_xr, float *s_xi) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
     const int gb = g1 - g0;
     const int nsub = (gb + 31) / 32;
     for (int q = 0; q < nsub; ++q) {
-        const int sb = UPPER ? nsub - 1 - q : q;
+        const int sb = LOWER ? q : nsub - 1 - q;
         const int s0 = g0 + sb * 32, s1 = min(g1, s0 + 32), sw = s1 - s0;
-        // stage the 32 x 32 diagonal tile (pitch 33) and the sub-block's x
+        // stage the 32 x 32 diagonal tile of op(A) (pitch 33) and the sub-block's x
         for (int e = tid; e < 32 * 32; e += blockDim.x) {
             const int r = e >> 5, c = e & 31;
             float tr = 0.f, ti = 0.f;
-            if (r < sw && c < sw) {
-                tr = Ar[(size_t)(s0 + r) * lda + s0 + c];
-                ti = Ai[(size_t)(s0 + r) * lda + s0 + c];
-            }
+            if (r < sw && c < sw) op_elem<TR>(Ar, Ai, lda, s0 + r, s0 + c, tr, ti);
             s_tr[r * 33 + c] = tr;
             s_ti[r * 33 + c] = ti;
         }
@@ -714,33 +664,23 @@ __device__ void trsv_diag(const float *Ar, const float *Ai, long long lda, float
         }
         __syncthreads();
         if (warp == 0) {
-            // column sweep: lane i holds x_i; step j finalises x_j and
-            // removes its contribution from the remaining rows
+            // column sweep: lane i holds x_i; step j finalises x_j and removes
+            // its contribution from the remaining rows
             float vr = s_xr[lane], vi = s_xi[lane];
-            if (!UPPER) {
-                for (int j = 0; j < sw; ++j) {
-                    const float jr = __shfl_sync(0xffffffffu, vr, j), ji = __shfl_sync(0xffffffffu, vi, j);
-                    if (lane > j) {
-                        const float lr = s_tr[lane * 33 + j], li = s_ti[lane * 33 + j];
-                        vr -= lr * jr - li * ji;
-                        vi -= lr * ji + li * jr;
-                    }
+            for (int t = 0; t < sw; ++t) {
+                const int j = LOWER ? t : sw - 1 - t;
+                if (!UNIT && lane == j) {
+                    const float dr = s_tr[j * 33 + j], di = s_ti[j * 33 + j];
+                    const float den = 1.0f / (dr * dr + di * di);
+                    const float yr = vr, yi = vi;
+                    vr = (yr * dr + yi * di) * den;
+                    vi = (yi * dr - yr * di) * den;
                 }
-            } else {
-                for (int j = sw - 1; j >= 0; --j) {
-                    if (lane == j) {
-                        const float dr = s_tr[j * 33 + j], di = s_ti[j * 33 + j];
-                        const float den = 1.0f / (dr * dr + di * di);
-                        const float yr = vr, yi = vi;
-                        vr = (yr * dr + yi * di) * den;
-                        vi = (yi * dr - yr * di) * den;
-                    }
-                    const float jr = __shfl_sync(0xffffffffu, vr, j), ji = __shfl_sync(0xffffffffu, vi, j);
-                    if (lane < j) {
-                        const float ur = s_tr[lane * 33 + j], ui = s_ti[lane * 33 + j];
-                        vr -= ur * jr - ui * ji;
-                        vi -= ur * ji + ui * jr;
-                    }
+                const float jr = __shfl_sync(0xffffffffu, vr, j), ji = __shfl_sync(0xffffffffu, vi, j);
+                if (LOWER ? lane > j : lane < j) {
+                    const float lr = s_tr[lane * 33 + j], li = s_ti[lane * 33 + j];
+                    vr -= lr * jr - li * ji;
+                    vi -= lr * ji + li * jr;
                 }
             }
             s_xr[lane] = vr;
@@ -752,11 +692,12 @@ __device__ void trsv_diag(const float *Ar, const float *Ai, long long lda, float
         }
         __syncthreads();
         // remaining rows of this diagonal block: below (lower) or above (upper)
-        const int u0 = UPPER ? g0 : s1, u1 = UPPER ? s0 : g1;
+        const int u0 = LOWER ? s1 : g0, u1 = LOWER ? g1 : s0;
         for (int i = u0 + warp; i < u1; i += nw) {
             float pr = 0.f, pi = 0.f;
             if (lane < sw) {
-                const float ar = Ar[(size_t)i * lda + s0 + lane], ai = Ai[(size_t)i * lda + s0 + lane];
+                float ar, ai;
+                op_elem<TR>(Ar, Ai, lda, i, s0 + lane, ar, ai);
                 pr = ar * s_xr[lane] - ai * s_xi[lane];
                 pi = ar * s_xi[lane] + ai * s_xr[lane];
             }
@@ -773,38 +714,89 @@ __device__ void trsv_diag(const float *Ar, const float *Ai, long long lda, float
     }
 }
 
-// rows [r0, r1): x_i -= A[i, f0:f1] x[f0:f1], with x[f0:f1] staged in s_x*
+// op-rows [r0, r1): x_i -= op(A)[i, f0:f0+fw] x[f0:f0+fw], x of the block staged in s_x*
+template <int TR>
 __device__ __forceinline__ void trsv_apply(const float *Ar, const float *Ai, long long lda, float *xr, float *xi,
                                            long long ldb, int f0, int fw, int r0, int r1, const float *s_xr,
                                            const float *s_xi) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int i = r0 + warp; i < r1; i += nw) {
-        const float *rr = Ar + (size_t)i * lda + f0, *ri = Ai + (size_t)i * lda + f0;
-        float pr = 0.f, pi = 0.f;
+    if (TR == 0) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        for (int i = r0 + warp; i < r1; i += nw) {
+            const float *rr = Ar + (size_t)i * lda + f0, *ri = Ai + (size_t)i * lda + f0;
+            float pr = 0.f, pi = 0.f;
 #pragma unroll
-        for (int c0 = 0; c0 < kTB; c0 += 32) {
-            const int c = c0 + lane;
-            if (c < fw) {
-                const float ar = rr[c], ai = ri[c];
+            for (int c0 = 0; c0 < kTB; c0 += 32) {
+                const int c = c0 + lane;
+                if (c < fw) {
+                    const float ar = rr[c], ai = ri[c];
+                    pr += ar * s_xr[c] - ai * s_xi[c];
+                    pi += ar * s_xi[c] + ai * s_xr[c];
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                pr += __shfl_xor_sync(0xffffffffu, pr, o);
+                pi += __shfl_xor_sync(0xffffffffu, pi, o);
+            }
+            if (lane == 0) {
+                xr[(size_t)i * ldb] -= pr;
+                xi[(size_t)i * ldb] -= pi;
+            }
+        }
+    } else {
+        // op(A)[i, c] = A[c, i] (conjugated for A^H): threads over i read rows c coalesced
+        const float cs = TR == 2 ? -1.f : 1.f;
+        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+            float pr = 0.f, pi = 0.f;
+#pragma unroll 8
+            for (int c = 0; c < fw; ++c) {
+                const float ar = Ar[(size_t)(f0 + c) * lda + i], ai = cs * Ai[(size_t)(f0 + c) * lda + i];
                 pr += ar * s_xr[c] - ai * s_xi[c];
                 pi += ar * s_xi[c] + ai * s_xr[c];
             }
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            pr += __shfl_xor_sync(0xffffffffu, pr, o);
-            pi += __shfl_xor_sync(0xffffffffu, pi, o);
-        }
-        if (lane == 0) {
             xr[(size_t)i * ldb] -= pr;
             xi[(size_t)i * ldb] -= pi;
         }
     }
 }
 
-// Prologue: one CTA per (rhs, matrix).  Forward: apply the interchanges to
-// the whole vector in shared memory, then solve block 0.  Backward: solve
-// the last block.
-template <bool UPPER>
+// Apply the interchanges to the whole vector in shared memory: forward order
+// (P b, op = A) or reverse order (P^T v, op = A^T / A^H).
+template <bool REVERSE>
+__device__ void trsv_permute(int n, const int *pv, float *xr, float *xi, long long ldb, float *vr, float *vi) {
+    __shared__ int s_pv[1024];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        vr[i] = xr[(size_t)i * ldb];
+        vi[i] = xi[(size_t)i * ldb];
+    }
+    const int nchunk = (n + 1023) / 1024;
+    for (int q = 0; q < nchunk; ++q) {
+        const int base = (REVERSE ? nchunk - 1 - q : q) * 1024;
+        const int cnt = min(1024, n - base);
+        __syncthreads();
+        for (int i = threadIdx.x; i < cnt; i += blockDim.x) s_pv[i] = pv[base + i];
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (int t = 0; t < cnt; ++t) {
+                const int k = REVERSE ? cnt - 1 - t : t;
+                const int p = s_pv[k], r = base + k;
+                if (p != r && p >= 0 && p < n) {
+                    float tmp = vr[r]; vr[r] = vr[p]; vr[p] = tmp;
+                    tmp = vi[r]; vi[r] = vi[p]; vi[p] = tmp;
+                }
+            }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        xr[(size_t)i * ldb] = vr[i];
+        xi[(size_t)i * ldb] = vi[i];
+    }
+    __syncthreads();
+}
+
+// Prologue: one CTA per (rhs, matrix).  First phase (lower operator): the
+// interchanges for op = A, then the first block; second phase (upper
+// operator): the last block.
+template <bool LOWER, bool UNIT, int TR>
 __global__ void __launch_bounds__(kTrsvThreads) k_trsv_first(int n, const float *lu_re, const float *lu_im,
                                                              long long lda, long long a_stride, const int *piv,
                                                              long long piv_stride, float *b_re, float *b_im,
@@ -814,50 +806,35 @@ __global__ void __launch_bounds__(kTrsvThreads) k_trsv_first(int n, const float 
     const int mat = blockIdx.y, rhs = blockIdx.x;
     const float *Ar = lu_re + (size_t)mat * a_stride, *Ai = lu_im + (size_t)mat * a_stride;
     float *xr = b_re + (size_t)mat * b_stride + rhs, *xi = b_im + (size_t)mat * b_stride + rhs;
-    if (!UPPER) {
-        const int *pv = piv + (size_t)mat * piv_stride;
-        float *vr = s_x, *vi = s_x + n;
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            vr[i] = xr[(size_t)i * ldb];
-            vi[i] = xi[(size_t)i * ldb];
-        }
-        __shared__ int s_pv[1024];
-        for (int base = 0; base < n; base += 1024) {
-            const int cnt = min(1024, n - base);
-            __syncthreads();
-            for (int i = threadIdx.x; i < cnt; i += blockDim.x) s_pv[i] = pv[base + i];
-            __syncthreads();
-            if (threadIdx.x == 0)
-                for (int i = 0; i < cnt; ++i) {
-                    const int p = s_pv[i], r = base + i;
-                    if (p != r && p >= 0 && p < n) {
-                        float t = vr[r]; vr[r] = vr[p]; vr[p] = t;
-                        t = vi[r]; vi[r] = vi[p]; vi[p] = t;
-                    }
-                }
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            xr[(size_t)i * ldb] = vr[i];
-            xi[(size_t)i * ldb] = vi[i];
-        }
-        __syncthreads();
-        trsv_diag<false>(Ar, Ai, lda, xr, xi, ldb, 0, min(n, kTB), s_tr, s_ti, s_xr, s_xi);
+    if (LOWER) {
+        if (TR == 0 && piv) trsv_permute<false>(n, piv + (size_t)mat * piv_stride, xr, xi, ldb, s_x, s_x + n);
+        trsv_diag<true, UNIT, TR>(Ar, Ai, lda, xr, xi, ldb, 0, min(n, kTB), s_tr, s_ti, s_xr, s_xi);
     } else {
         const int last = (n - 1) / kTB;
-        trsv_diag<true>(Ar, Ai, lda, xr, xi, ldb, last * kTB, n, s_tr, s_ti, s_xr, s_xi);
+        trsv_diag<false, UNIT, TR>(Ar, Ai, lda, xr, xi, ldb, last * kTB, n, s_tr, s_ti, s_xr, s_xi);
     }
+}
+
+// Epilogue for op = A^T / A^H: x = P^T v.
+__global__ void __launch_bounds__(kTrsvThreads) k_trsv_unpermute(int n, const int *piv, long long piv_stride,
+                                                                 float *b_re, float *b_im, long long ldb,
+                                                                 long long b_stride) {
+    extern __shared__ float s_x[];
+    const int mat = blockIdx.y, rhs = blockIdx.x;
+    float *xr = b_re + (size_t)mat * b_stride + rhs, *xi = b_im + (size_t)mat * b_stride + rhs;
+    trsv_permute<true>(n, piv + (size_t)mat * piv_stride, xr, xi, ldb, s_x, s_x + n);
 }
 
 // Block step: x of block `blk` is final.  Lower: CTA 0 updates and solves
 // block blk+1, CTAs >= 1 update rows from block blk+2 on.  Upper: CTA 0
 // updates and solves block blk-1, CTAs >= 1 update rows before block blk-1.
-template <bool UPPER>
+template <bool LOWER, bool UNIT, int TR>
 __global__ void __launch_bounds__(kTrsvThreads) k_trsv_step(int n, const float *lu_re, const float *lu_im,
                                                             long long lda, long long a_stride, float *b_re,
                                                             float *b_im, long long ldb, long long b_stride, int blk) {
     __shared__ float s_fr[kTB], s_fi[kTB];
     __shared__ float s_tr[32 * 33], s_ti[32 * 33], s_xr[32], s_xi[32];
+    constexpr int RPC = TR == 0 ? kTrsvRows : kTrsvRowsT;
     const int mat = blockIdx.z, rhs = blockIdx.y;
     const float *Ar = lu_re + (size_t)mat * a_stride, *Ai = lu_im + (size_t)mat * a_stride;
     float *xr = b_re + (size_t)mat * b_stride + rhs, *xi = b_im + (size_t)mat * b_stride + rhs;
@@ -868,53 +845,282 @@ __global__ void __launch_bounds__(kTrsvThreads) k_trsv_step(int n, const float *
     }
     __syncthreads();
     int g0, g1, o0, o1;  // next diagonal block, other rows
-    if (!UPPER) {
+    if (LOWER) {
         g0 = f1; g1 = min(n, g0 + kTB); o0 = g1; o1 = n;
     } else {
         g1 = f0; g0 = max(0, g1 - kTB); o0 = 0; o1 = g0;
     }
     if (blockIdx.x == 0) {
-        trsv_apply(Ar, Ai, lda, xr, xi, ldb, f0, fw, g0, g1, s_fr, s_fi);
+        trsv_apply<TR>(Ar, Ai, lda, xr, xi, ldb, f0, fw, g0, g1, s_fr, s_fi);
         __syncthreads();
-        trsv_diag<UPPER>(Ar, Ai, lda, xr, xi, ldb, g0, g1, s_tr, s_ti, s_xr, s_xi);
+        trsv_diag<LOWER, UNIT, TR>(Ar, Ai, lda, xr, xi, ldb, g0, g1, s_tr, s_ti, s_xr, s_xi);
     } else {
-        const int r0 = o0 + (blockIdx.x - 1) * kTrsvRows;
-        const int r1 = min(o1, r0 + kTrsvRows);
-        if (r0 < r1) trsv_apply(Ar, Ai, lda, xr, xi, ldb, f0, fw, r0, r1, s_fr, s_fi);
+        const int r0 = o0 + (blockIdx.x - 1) * RPC;
+        const int r1 = min(o1, r0 + RPC);
+        if (r0 < r1) trsv_apply<TR>(Ar, Ai, lda, xr, xi, ldb, f0, fw, r0, r1, s_fr, s_fi);
     }
 }
 
-int lu_solve_blocked(int n, int nrhs, int batch, const float *lu_re, const float *lu_im, long long lda,
-                     long long a_stride, const int *piv, long long piv_stride, float *b_re, float *b_im,
-                     long long ldb, long long b_stride, cudaStream_t st) {
-    const size_t smem = (size_t)n * 2 * sizeof(float);
+// One triangular phase: the prologue block and the block steps.
+template <bool LOWER, bool UNIT, int TR>
+int trsv_phase(int n, int nrhs, int batch, const float *lu_re, const float *lu_im, long long lda, long long a_stride,
+               const int *piv, long long piv_stride, float *b_re, float *b_im, long long ldb, long long b_stride,
+               cudaStream_t st) {
     static bool attr = false;
     if (!attr) {
-        HBEM_CUDA(cudaFuncSetAttribute(k_trsv_first<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        HBEM_CUDA(cudaFuncSetAttribute(k_trsv_first<LOWER, UNIT, TR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       200 * 1024));
         attr = true;
     }
+    constexpr int RPC = TR == 0 ? kTrsvRows : kTrsvRowsT;
     const int nblk = (n + kTB - 1) / kTB;
-    k_trsv_first<false><<<dim3(nrhs, batch), kTrsvThreads, smem, st>>>(n, lu_re, lu_im, lda, a_stride, piv, piv_stride,
-                                                                       b_re, b_im, ldb, b_stride);
+    const size_t smem = (LOWER && TR == 0 && piv) ? (size_t)n * 2 * sizeof(float) : 0;
+    k_trsv_first<LOWER, UNIT, TR><<<dim3(nrhs, batch), kTrsvThreads, smem, st>>>(n, lu_re, lu_im, lda, a_stride, piv,
+                                                                               piv_stride, b_re, b_im, ldb, b_stride);
     HBEM_LAUNCH_CHECK("k_trsv_first");
-    for (int blk = 0; blk + 1 < nblk; ++blk) {
-        const int rest = std::max(0, n - (blk + 2) * kTB);
-        const int ctas = 1 + (rest + kTrsvRows - 1) / kTrsvRows;
-        k_trsv_step<false><<<dim3(ctas, nrhs, batch), kTrsvThreads, 0, st>>>(n, lu_re, lu_im, lda, a_stride, b_re, b_im,
-                                                                            ldb, b_stride, blk);
-        HBEM_LAUNCH_CHECK("k_trsv_step");
-    }
-    k_trsv_first<true><<<dim3(nrhs, batch), kTrsvThreads, 0, st>>>(n, lu_re, lu_im, lda, a_stride, piv, piv_stride,
-                                                                   b_re, b_im, ldb, b_stride);
-    HBEM_LAUNCH_CHECK("k_trsv_first");
-    for (int blk = nblk - 1; blk > 0; --blk) {
-        const int rest = std::max(0, (blk - 1) * kTB);
-        const int ctas = 1 + (rest + kTrsvRows - 1) / kTrsvRows;
-        k_trsv_step<true><<<dim3(ctas, nrhs, batch), kTrsvThreads, 0, st>>>(n, lu_re, lu_im, lda, a_stride, b_re, b_im,
-                                                                           ldb, b_stride, blk);
-        HBEM_LAUNCH_CHECK("k_trsv_step");
+    if (LOWER) {
+        for (int blk = 0; blk + 1 < nblk; ++blk) {
+            const int rest = std::max(0, n - (blk + 2) * kTB);
+            const int ctas = 1 + (rest + RPC - 1) / RPC;
+            k_trsv_step<LOWER, UNIT, TR><<<dim3(ctas, nrhs, batch), kTrsvThreads, 0, st>>>(
+                n, lu_re, lu_im, lda, a_stride, b_re, b_im, ldb, b_stride, blk);
+            HBEM_LAUNCH_CHECK("k_trsv_step");
+        }
+    } else {
+        for (int blk = nblk - 1; blk > 0; --blk) {
+            const int rest = std::max(0, (blk - 1) * kTB);
+            const int ctas = 1 + (rest + RPC - 1) / RPC;
+            k_trsv_step<LOWER, UNIT, TR><<<dim3(ctas, nrhs, batch), kTrsvThreads, 0, st>>>(
+                n, lu_re, lu_im, lda, a_stride, b_re, b_im, ldb, b_stride, blk);
+            HBEM_LAUNCH_CHECK("k_trsv_step");
+        }
     }
     return HBEM_OK;
+}
+
+// piv == nullptr: no interchanges (a solve with the factors L U themselves).
+int lu_solve_blocked(int n, int nrhs, int batch, const float *lu_re, const float *lu_im, long long lda,
+                     long long a_stride, const int *piv, long long piv_stride, float *b_re, float *b_im,
+                     long long ldb, long long b_stride, int trans, cudaStream_t st) {
+    int rc;
+    if (trans == HBEM_TRANS_N) {
+        rc = trsv_phase<true, true, 0>(n, nrhs, batch, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re, b_im, ldb,
+                                       b_stride, st);
+        if (rc == HBEM_OK)
+            rc = trsv_phase<false, false, 0>(n, nrhs, batch, lu_re, lu_im, lda, a_stride, nullptr, piv_stride, b_re,
+                                             b_im, ldb, b_stride, st);
+        return rc;
+    }
+    if (trans == HBEM_TRANS_T) {
+        rc = trsv_phase<true, false, 1>(n, nrhs, batch, lu_re, lu_im, lda, a_stride, nullptr, piv_stride, b_re, b_im,
+                                        ldb, b_stride, st);
+        if (rc == HBEM_OK)
+            rc = trsv_phase<false, true, 1>(n, nrhs, batch, lu_re, lu_im, lda, a_stride, nullptr, piv_stride, b_re,
+                                            b_im, ldb, b_stride, st);
+    } else {
+        rc = trsv_phase<true, false, 2>(n, nrhs, batch, lu_re, lu_im, lda, a_stride, nullptr, piv_stride, b_re, b_im,
+                                        ldb, b_stride, st);
+        if (rc == HBEM_OK)
+            rc = trsv_phase<false, true, 2>(n, nrhs, batch, lu_re, lu_im, lda, a_stride, nullptr, piv_stride, b_re,
+                                            b_im, ldb, b_stride, st);
+    }
+    if (rc == HBEM_OK && piv) {
+        static bool attr = false;
+        if (!attr) {
+            HBEM_CUDA(cudaFuncSetAttribute(k_trsv_unpermute, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+            attr = true;
+        }
+        k_trsv_unpermute<<<dim3(nrhs, batch), kTrsvThreads, (size_t)n * 2 * sizeof(float), st>>>(n, piv, piv_stride,
+                                                                                                 b_re, b_im, ldb,
+                                                                                                 b_stride);
+        HBEM_LAUNCH_CHECK("k_trsv_unpermute");
+    }
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// 1-norm condition estimate of the factored matrices, as LAPACK cgecon with
+// norm '1' (the reference's estimateReciprocalCondition, main.swift:463-503,
+// 7898): Hager's method in Higham's formulation (LAPACK CLACN2) on L U
+// without the interchanges, then rcond = (1 / est) / ||A||_1.
+// Per-matrix state machine (st[f]):
+//   0: solve (LU) w = x for the first time        -> est, x = sign(w), go 1
+//   1: solve (LU)^H w = x                         -> j = argmax |w|; x = e_j, go 2
+//                                                    (or the alternative vector, go 3)
+//   2: solve (LU) w = e_j                         -> est; if not larger: go 3,
+//                                                    else x = sign(w), go 1
+//   3: solve (LU) w = alternative vector          -> est = max(est, 2 ||w||_1 / 3n), done (4)
+// ---------------------------------------------------------------------------
+struct RcState {
+    double est, estold;
+    int st, j, iter, pad;
+};
+
+// ||A||_1 = max_j sum_i |a_ij| (clange '1'); thread per column.
+__global__ void k_norm1(int n, const float *a_re, const float *a_im, long long lda, long long a_stride,
+                        unsigned *out_bits) {
+    const int mat = blockIdx.y;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    float v = 0.f;
+    if (j < n) {
+        const float *ar = a_re + (size_t)mat * a_stride + j, *ai = a_im + (size_t)mat * a_stride + j;
+        double sacc = 0.0;
+        for (int i = 0; i < n; ++i) sacc += hypot((double)ar[(size_t)i * lda], (double)ai[(size_t)i * lda]);
+        v = (float)sacc;
+    }
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out_bits + mat, __float_as_uint(v));
+}
+
+__global__ void k_rc_init(int n, float *x_re, float *x_im, long long stride, RcState *state) {
+    const int mat = blockIdx.y;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        x_re[(size_t)mat * stride + i] = 1.0f / (float)n;
+        x_im[(size_t)mat * stride + i] = 0.f;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        RcState s0{};
+        s0.st = 0;
+        state[mat] = s0;
+    }
+}
+
+// w = x for the matrices in `want` states (w is solved in place next)
+__global__ void k_rc_copy(int n, const float *x_re, const float *x_im, float *w_re, float *w_im, long long stride,
+                          const RcState *state, int want_lo, int want_hi) {
+    const int mat = blockIdx.y;
+    const int st = state[mat].st;
+    if (st < want_lo || st > want_hi) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        w_re[(size_t)mat * stride + i] = x_re[(size_t)mat * stride + i];
+        w_im[(size_t)mat * stride + i] = x_im[(size_t)mat * stride + i];
+    }
+}
+
+__device__ void block_sum_max(double &sum, float &mx, int &imx) {
+    __shared__ double s_sum[32];
+    __shared__ float s_mx[32];
+    __shared__ int s_imx[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        const float om = __shfl_xor_sync(0xffffffffu, mx, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, imx, o);
+        if (om > mx || (om == mx && oi < imx)) { mx = om; imx = oi; }
+    }
+    if (lane == 0) { s_sum[warp] = sum; s_mx[warp] = mx; s_imx[warp] = imx; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        float m = -1.f;
+        int im = 0x7fffffff;
+        for (int w = 0; w < nw; ++w) {
+            t += s_sum[w];
+            if (s_mx[w] > m || (s_mx[w] == m && s_imx[w] < im)) { m = s_mx[w]; im = s_imx[w]; }
+        }
+        s_sum[0] = t; s_mx[0] = m; s_imx[0] = im;
+    }
+    __syncthreads();
+    sum = s_sum[0]; mx = s_mx[0]; imx = s_imx[0];
+    __syncthreads();
+}
+
+// After a (LU) w solve (states 0, 2, 3): one CTA per matrix.
+__global__ void k_rc_after_a(int n, float *x_re, float *x_im, const float *w_re, const float *w_im, long long stride,
+                             RcState *state) {
+    const int mat = blockIdx.x;
+    RcState sv = state[mat];
+    if (sv.st != 0 && sv.st != 2 && sv.st != 3) return;
+    const float *wr = w_re + (size_t)mat * stride, *wi = w_im + (size_t)mat * stride;
+    float *xr = x_re + (size_t)mat * stride, *xi = x_im + (size_t)mat * stride;
+    double sum = 0.0;
+    float mx = -1.f;
+    int imx = 0x7fffffff;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) sum += hypot((double)wr[i], (double)wi[i]);
+    block_sum_max(sum, mx, imx);
+    const float safmin = 1.17549435e-38f;
+    bool to_sign = false, to_alt = false;
+    if (sv.st == 0) {
+        sv.est = sum;
+        if (n == 1) { sv.st = 4; }
+        else { to_sign = true; sv.st = 1; }
+    } else if (sv.st == 2) {
+        sv.estold = sv.est;
+        sv.est = sum;
+        if (sv.est <= sv.estold) { to_alt = true; sv.st = 3; }   // LAPACK keeps the new estimate here
+        else { to_sign = true; sv.st = 1; }
+    } else {  // alternative estimate
+        const double temp = 2.0 * sum / (3.0 * n);
+        if (temp > sv.est) sv.est = temp;
+        sv.st = 4;
+    }
+    if (to_sign) {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const float a = hypotf(wr[i], wi[i]);
+            if (a > safmin) { xr[i] = wr[i] / a; xi[i] = wi[i] / a; }
+            else { xr[i] = 1.f; xi[i] = 0.f; }
+        }
+    } else if (to_alt) {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const float sgn = (i & 1) ? -1.f : 1.f;
+            xr[i] = sgn * (1.0f + (float)i / (float)(n - 1));
+            xi[i] = 0.f;
+        }
+    }
+    if (threadIdx.x == 0) state[mat] = sv;
+}
+
+// After a (LU)^H w solve (state 1): one CTA per matrix.
+__global__ void k_rc_after_h(int n, float *x_re, float *x_im, const float *w_re, const float *w_im, long long stride,
+                             RcState *state, int itmax) {
+    const int mat = blockIdx.x;
+    RcState sv = state[mat];
+    if (sv.st != 1) return;
+    const float *wr = w_re + (size_t)mat * stride, *wi = w_im + (size_t)mat * stride;
+    float *xr = x_re + (size_t)mat * stride, *xi = x_im + (size_t)mat * stride;
+    double sum = 0.0;
+    float mx = -1.f;
+    int imx = 0x7fffffff;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const float a = hypotf(wr[i], wi[i]);
+        if (a > mx || (a == mx && i < imx)) { mx = a; imx = i; }
+    }
+    block_sum_max(sum, mx, imx);
+    if (imx < 0 || imx >= n) imx = 0;
+    bool to_ej = false;
+    if (sv.iter == 0) {
+        // first pass (LAPACK ISAVE(1) = 2): j = argmax, iteration 2
+        sv.j = imx;
+        sv.iter = 2;
+        to_ej = true;
+    } else {
+        // LAPACK ISAVE(1) = 4: continue while |w_jlast| != |w_j| and iter < itmax
+        const int jlast = sv.j;
+        sv.j = imx;
+        const float a_last = hypotf(wr[jlast], wi[jlast]);
+        if (a_last != mx && sv.iter < itmax) { sv.iter += 1; to_ej = true; }
+    }
+    if (to_ej) {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) { xr[i] = (i == sv.j) ? 1.f : 0.f; xi[i] = 0.f; }
+        sv.st = 2;
+    } else {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const float sgn = (i & 1) ? -1.f : 1.f;
+            xr[i] = sgn * (1.0f + (float)i / (float)(n - 1));
+            xi[i] = 0.f;
+        }
+        sv.st = 3;
+    }
+    if (threadIdx.x == 0) state[mat] = sv;
+}
+
+__global__ void k_rc_finish(int batch, const RcState *state, const unsigned *anorm_bits, double *rcond, int *pending) {
+    const int mat = blockIdx.x * blockDim.x + threadIdx.x;
+    if (mat >= batch) return;
+    const RcState sv = state[mat];
+    if (sv.st != 4) atomicAdd(pending, 1);
+    const double an = (double)__uint_as_float(anorm_bits[mat]);
+    rcond[mat] = (sv.est != 0.0 && an != 0.0) ? (1.0 / sv.est) / an : 0.0;
 }
 
 // FP64 residual r = b - A x (one warp per row), and per-matrix norms.
@@ -1077,27 +1283,121 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
     return finish(HBEM_OK);
 }
 
+int lu_solve_single(int n, int nrhs, int batch, const float *lu_re, const float *lu_im, long long lda,
+                    long long a_stride, const int *piv, long long piv_stride, float *b_re, float *b_im, long long ldb,
+                    long long b_stride, int trans, cudaStream_t st);
+
+// piv == nullptr solves with L U itself (no interchanges).
 int lu_solve(int n, int nrhs, int batch, const float *lu_re, const float *lu_im, long long lda, long long a_stride,
              const int *piv, long long piv_stride, float *b_re, float *b_im, long long ldb, long long b_stride,
              int trans, cudaStream_t st) {
     const size_t smem = (size_t)n * 2 * sizeof(float);
     if (smem > 200 * 1024) return fail(HBEM_ERR_ARG, "hbem_lu_solve: n too large for the staged solve");
-    dim3 grid(nrhs, batch);
+    // one CTA per right-hand side when there are enough of them to fill the GPU
+    // (or n is small); the blocked multi-CTA steps otherwise
     const int solve_mode = tuning(HBEM_TUNE_LU_SOLVE);
-    if (trans == HBEM_TRANS_N && (solve_mode == 2 || (solve_mode == 0 && n > kTB)))
-        return lu_solve_blocked(n, nrhs, batch, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re, b_im, ldb, b_stride, st);
-    if (trans == HBEM_TRANS_N) {
-        HBEM_CUDA(cudaFuncSetAttribute(k_getrs<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_getrs<0><<<grid, 512, smem, st>>>(n, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re, b_im, ldb, b_stride, nrhs);
-    } else if (trans == HBEM_TRANS_T) {
-        HBEM_CUDA(cudaFuncSetAttribute(k_getrs<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_getrs<1><<<grid, 512, smem, st>>>(n, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re, b_im, ldb, b_stride, nrhs);
-    } else {
-        HBEM_CUDA(cudaFuncSetAttribute(k_getrs<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_getrs<2><<<grid, 512, smem, st>>>(n, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re, b_im, ldb, b_stride, nrhs);
+    const long long ctas = (long long)nrhs * batch;
+    const bool single = solve_mode == 1 || (solve_mode == 0 && (n <= kTB || (n <= 6144 && ctas >= 24)));
+    if (!single)
+        return lu_solve_blocked(n, nrhs, batch, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re, b_im, ldb, b_stride,
+                                trans, st);
+    return lu_solve_single(n, nrhs, batch, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re, b_im, ldb, b_stride,
+                           trans, st);
+}
+
+int lu_solve_single(int n, int nrhs, int batch, const float *lu_re, const float *lu_im, long long lda,
+                    long long a_stride, const int *piv, long long piv_stride, float *b_re, float *b_im, long long ldb,
+                    long long b_stride, int trans, cudaStream_t st) {
+    const size_t smem = (size_t)n * 2 * sizeof(float);
+    static bool attr = false;
+    if (!attr) {
+        HBEM_CUDA(cudaFuncSetAttribute(k_getrs<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        HBEM_CUDA(cudaFuncSetAttribute(k_getrs<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        HBEM_CUDA(cudaFuncSetAttribute(k_getrs<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        attr = true;
     }
+    dim3 grid(nrhs, batch);
+    if (trans == HBEM_TRANS_N)
+        k_getrs<0><<<grid, kGetrsThreads, smem, st>>>(n, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re, b_im, ldb,
+                                                     b_stride);
+    else if (trans == HBEM_TRANS_T)
+        k_getrs<1><<<grid, kGetrsThreads, smem, st>>>(n, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re, b_im, ldb,
+                                                     b_stride);
+    else
+        k_getrs<2><<<grid, kGetrsThreads, smem, st>>>(n, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re, b_im, ldb,
+                                                     b_stride);
     HBEM_LAUNCH_CHECK("k_getrs");
     return HBEM_OK;
+}
+
+int matrix_norm1(int n, int batch, const float *a_re, const float *a_im, long long lda, long long a_stride,
+                 float *anorm, cudaStream_t st) {
+    unsigned *bits = reinterpret_cast<unsigned *>(anorm);
+    HBEM_CUDA(cudaMemsetAsync(bits, 0, sizeof(unsigned) * batch, st));
+    k_norm1<<<dim3((n + 255) / 256, batch), 256, 0, st>>>(n, a_re, a_im, lda, a_stride, bits);
+    HBEM_LAUNCH_CHECK("k_norm1");
+    return HBEM_OK;
+}
+
+int lu_rcond(int n, int batch, const float *lu_re, const float *lu_im, long long lda, long long a_stride,
+             const float *anorm, double *rcond, cudaStream_t st) {
+    constexpr int kItMax = 5;
+    float *x = nullptr, *w = nullptr;
+    RcState *state = nullptr;
+    int *pending = nullptr;
+    const long long stride = n;
+    HBEM_CUDA(cudaMallocAsync((void **)&x, sizeof(float) * 2 * (size_t)batch * n, st));
+    HBEM_CUDA(cudaMallocAsync((void **)&w, sizeof(float) * 2 * (size_t)batch * n, st));
+    HBEM_CUDA(cudaMallocAsync((void **)&state, sizeof(RcState) * batch, st));
+    HBEM_CUDA(cudaMallocAsync((void **)&pending, sizeof(int), st));
+    float *xr = x, *xi = x + (size_t)batch * n, *wr = w, *wi = w + (size_t)batch * n;
+    const dim3 gv((n + 255) / 256 < 64 ? (n + 255) / 256 : 64, batch);
+    int rc = HBEM_OK;
+    auto launched = [&](const char *what) {
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) { rc = cuda_fail(e, what); return false; }
+        count_launch();
+        return true;
+    };
+    k_rc_init<<<gv, 256, 0, st>>>(n, xr, xi, stride, state);
+    // round 0: (LU) w = x for every matrix
+    if (launched("k_rc_init")) {
+        k_rc_copy<<<gv, 256, 0, st>>>(n, xr, xi, wr, wi, stride, state, 0, 3);
+        if (launched("k_rc_copy")) rc = lu_solve(n, 1, batch, lu_re, lu_im, lda, a_stride, nullptr, n, wr, wi, 1,
+                                                         stride, HBEM_TRANS_N, st);
+        if (rc == HBEM_OK) { k_rc_after_a<<<batch, 256, 0, st>>>(n, xr, xi, wr, wi, stride, state); launched("k_rc_after_a"); }
+    }
+    for (int round = 0; round < 2 * kItMax + 2 && rc == HBEM_OK; ++round) {
+        // (LU)^H solves for matrices in state 1, then (LU) solves for states 2 and 3
+        k_rc_copy<<<gv, 256, 0, st>>>(n, xr, xi, wr, wi, stride, state, 1, 1);
+        if (!launched("k_rc_copy")) break;
+        rc = lu_solve(n, 1, batch, lu_re, lu_im, lda, a_stride, nullptr, n, wr, wi, 1, stride, HBEM_TRANS_C, st);
+        if (rc != HBEM_OK) break;
+        k_rc_after_h<<<batch, 256, 0, st>>>(n, xr, xi, wr, wi, stride, state, kItMax);
+        if (!launched("k_rc_after_h")) break;
+        k_rc_copy<<<gv, 256, 0, st>>>(n, xr, xi, wr, wi, stride, state, 2, 3);
+        if (!launched("k_rc_copy")) break;
+        rc = lu_solve(n, 1, batch, lu_re, lu_im, lda, a_stride, nullptr, n, wr, wi, 1, stride, HBEM_TRANS_N, st);
+        if (rc != HBEM_OK) break;
+        k_rc_after_a<<<batch, 256, 0, st>>>(n, xr, xi, wr, wi, stride, state);
+        if (!launched("k_rc_after_a")) break;
+        // stop once every matrix is done
+        cudaError_t e = cudaMemsetAsync(pending, 0, sizeof(int), st);
+        if (e != cudaSuccess) { rc = cuda_fail(e, "rcond memset"); break; }
+        k_rc_finish<<<(batch + 127) / 128, 128, 0, st>>>(batch, state, reinterpret_cast<const unsigned *>(anorm), rcond,
+                                                         pending);
+        if (!launched("k_rc_finish")) break;
+        int h = 0;
+        e = cudaMemcpyAsync(&h, pending, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) { rc = cuda_fail(e, "rcond sync"); break; }
+        if (h == 0) break;
+    }
+    cudaFreeAsync(x, st);
+    cudaFreeAsync(w, st);
+    cudaFreeAsync(state, st);
+    cudaFreeAsync(pending, st);
+    return rc;
 }
 
 int refine(int n, int batch, const float *a_re, const float *a_im, long long lda, long long a_stride,
@@ -1266,6 +1566,7 @@ using namespace hbem;
 
 extern "C" int hbem_lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long long a_stride, int *piv,
                               long long piv_stride, int *info, int precision, void *stream) {
+    keep_pool_memory();
     if (n <= 0 || batch <= 0) return HBEM_OK;
     if (!a_re || !a_im || !piv || !info) return fail(HBEM_ERR_ARG, "hbem_lu_factor: NULL pointer");
     if (lda < n || a_stride < lda * (long long)n || piv_stride < n) return fail(HBEM_ERR_ARG, "hbem_lu_factor: bad strides");
@@ -1292,6 +1593,7 @@ extern "C" int hbem_refine(int n, int batch, const float *a_re, const float *a_i
                            long long piv_stride, const float *b_re, const float *b_im, long long b_stride,
                            float *x_re, float *x_im, long long x_stride, double tol, int max_iter, int *iters,
                            double *resid, void *stream) {
+    keep_pool_memory();
     if (n <= 0 || batch <= 0) return HBEM_OK;
     if (!a_re || !a_im || !lu_re || !lu_im || !piv || !b_re || !b_im || !x_re || !x_im)
         return fail(HBEM_ERR_ARG, "hbem_refine: NULL pointer");
@@ -1313,4 +1615,22 @@ extern "C" int hbem_refine_noalloc(int n, int batch, const float *a_re, const fl
     return refine_noalloc(n, batch, a_re, a_im, lda, a_stride, lu_re, lu_im, lu_stride, piv, piv_stride, b_re, b_im,
                           b_stride, x_re, x_im, x_stride, tol, max_iter, iters, resid,
                           reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" int hbem_matrix_norm1(int n, int batch, const float *a_re, const float *a_im, long long lda,
+                                 long long a_stride, float *anorm, void *stream) {
+    if (n <= 0 || batch <= 0) return HBEM_OK;
+    if (!a_re || !a_im || !anorm) return fail(HBEM_ERR_ARG, "hbem_matrix_norm1: NULL pointer");
+    if (lda < n || a_stride < lda * (long long)n) return fail(HBEM_ERR_ARG, "hbem_matrix_norm1: bad strides");
+    return matrix_norm1(n, batch, a_re, a_im, lda, a_stride, anorm, reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" int hbem_lu_rcond(int n, int batch, const float *lu_re, const float *lu_im, long long lda,
+                             long long a_stride, const float *anorm, double *rcond, void *stream) {
+    keep_pool_memory();
+    if (n <= 0 || batch <= 0) return HBEM_OK;
+    if (!lu_re || !lu_im || !anorm || !rcond) return fail(HBEM_ERR_ARG, "hbem_lu_rcond: NULL pointer");
+    if (lda < n || a_stride < lda * (long long)n) return fail(HBEM_ERR_ARG, "hbem_lu_rcond: bad strides");
+    if ((size_t)n * 2 * sizeof(float) > 200 * 1024) return fail(HBEM_ERR_ARG, "hbem_lu_rcond: n too large");
+    return lu_rcond(n, batch, lu_re, lu_im, lda, a_stride, anorm, rcond, reinterpret_cast<cudaStream_t>(stream));
 }

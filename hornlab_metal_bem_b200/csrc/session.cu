@@ -36,6 +36,25 @@ int cuda_fail(cudaError_t e, const char *what) {
 
 void count_launch(long long n) { g_launches += n; }
 
+// Stream-ordered allocations (workspaces of the LU, refinement, condition
+// estimate) come from the device's default memory pool; by default that pool
+// hands freed memory back to the driver at every synchronisation, so the
+// next allocation maps memory again.  Keep it cached instead (process-local
+// setting of this process's pool, like a caching allocator).
+void keep_pool_memory() {
+    static std::atomic<unsigned long long> done{0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+    const unsigned long long bit = 1ull << dev;
+    if (done.load() & bit) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    done.fetch_or(bit);
+}
+
 // Tuning knobs (HBEM_TUNE_*), process-wide; 0 = the built-in choice.
 static std::atomic<int> g_tuning[HBEM_TUNE_COUNT];
 int tuning(int key) { return (key >= 0 && key < HBEM_TUNE_COUNT) ? g_tuning[key].load() : 0; }
@@ -335,6 +354,7 @@ extern "C" int hbem_session_create(const float *vertices_3xv, int n_vertices, co
     HBEM_CUDA(cudaGetDeviceCount(&ndev));
     if (device < 0 || device >= ndev) return fail(HBEM_ERR_ARG, "hbem_session_create: bad device index");
     HBEM_CUDA(cudaSetDevice(device));
+    keep_pool_memory();
 
     Session *s = new Session();
     s->device = device;

@@ -20,6 +20,10 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
 int lu_solve(int n, int nrhs, int batch, const float *lu_re, const float *lu_im, long long lda, long long a_stride,
              const int *piv, long long piv_stride, float *b_re, float *b_im, long long ldb, long long b_stride,
              int trans, cudaStream_t st);
+int matrix_norm1(int n, int batch, const float *a_re, const float *a_im, long long lda, long long a_stride,
+                 float *anorm, cudaStream_t st);
+int lu_rcond(int n, int batch, const float *lu_re, const float *lu_im, long long lda, long long a_stride,
+             const float *anorm, double *rcond, cudaStream_t st);
 int refine(int n, int batch, const float *a_re, const float *a_im, long long lda, long long a_stride,
            const float *lu_re, const float *lu_im, long long lu_stride, const int *piv, long long piv_stride,
            const float *b_re, const float *b_im, long long b_stride, float *x_re, float *x_im, long long x_stride,
@@ -35,7 +39,7 @@ namespace {
 size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
 
 struct Layout {
-    size_t q, a, a0, x, b, piv, info, obs, fld, tag, want, iters, resid, total;
+    size_t q, a, a0, x, b, piv, info, obs, fld, tag, want, iters, resid, anorm, rcond, total;
 };
 
 Layout layout(const Session &s, int nf, int n_obs, int n_tags, bool keep_a) {
@@ -56,6 +60,8 @@ Layout layout(const Session &s, int nf, int n_obs, int n_tags, bool keep_a) {
     L.want = take(sizeof(int) * std::max(1, n_tags));
     L.iters = take(sizeof(int) * nf);
     L.resid = take(sizeof(double) * nf);
+    L.anorm = take(sizeof(float) * nf);
+    L.rcond = take(sizeof(double) * nf);
     L.total = off;
     return L;
 }
@@ -79,7 +85,8 @@ extern "C" int hbem_solve_batch(hbem_session *h, int n_freq, const float *k_re, 
                                 const float *q_im, const float *obs_3xn, int n_obs, const int *tags, int n_tags,
                                 int precision, double refine_tol, int refine_max_iter, float *field_re,
                                 float *field_im, double *tag_avg, float *surface_re, float *surface_im, int *info,
-                                int *refine_iters, double *refine_resid, float *timings_ms, void *stream) {
+                                int *refine_iters, double *refine_resid, double *rcond, float *timings_ms,
+                                void *stream) {
     Session *s = reinterpret_cast<Session *>(h);
     if (!s) return fail(HBEM_ERR_ARG, "hbem_solve_batch: NULL session");
     if (n_freq <= 0) return HBEM_OK;
@@ -123,6 +130,8 @@ extern "C" int hbem_solve_batch(hbem_session *h, int n_freq, const float *k_re, 
     int *dwant = reinterpret_cast<int *>(ws + L.want);
     int *diters = reinterpret_cast<int *>(ws + L.iters);
     double *dres = reinterpret_cast<double *>(ws + L.resid);
+    float *danorm = reinterpret_cast<float *>(ws + L.anorm);
+    double *drcond = reinterpret_cast<double *>(ws + L.rcond);
 
     cudaEvent_t ev[5];
     for (auto &e : ev) HBEM_CUDA(cudaEventCreate(&e));
@@ -153,8 +162,16 @@ extern "C" int hbem_solve_batch(hbem_session *h, int n_freq, const float *k_re, 
             HBEM_CUDA(cudaMemcpyAsync(a0r, ar, sizeof(float) * nf * n * n, cudaMemcpyDeviceToDevice, st));
             HBEM_CUDA(cudaMemcpyAsync(a0i, ai, sizeof(float) * nf * n * n, cudaMemcpyDeviceToDevice, st));
         }
+        if (rcond) {
+            rc = matrix_norm1((int)n, nf, ar, ai, (long long)n, (long long)(n * n), danorm, st);
+            if (rc != HBEM_OK) break;
+        }
         rc = lu_factor((int)n, nf, ar, ai, (long long)n, (long long)(n * n), dpiv, (long long)n, dinfo, precision, st);
         if (rc != HBEM_OK) break;
+        if (rcond) {
+            rc = lu_rcond((int)n, nf, ar, ai, (long long)n, (long long)(n * n), danorm, drcond, st);
+            if (rc != HBEM_OK) break;
+        }
         rc = lu_solve((int)n, 1, nf, ar, ai, (long long)n, (long long)(n * n), dpiv, (long long)n, xr, xi, 1,
                       (long long)n, HBEM_TRANS_N, st);
         if (rc != HBEM_OK) break;
@@ -187,6 +204,7 @@ extern "C" int hbem_solve_batch(hbem_session *h, int n_freq, const float *k_re, 
             HBEM_CUDA(cudaMemcpyAsync(surface_im + (size_t)f0 * n, xi, sizeof(float) * nf * n, cudaMemcpyDeviceToHost, st));
         }
         HBEM_CUDA(cudaMemcpyAsync(info + f0, dinfo, sizeof(int) * nf, cudaMemcpyDeviceToHost, st));
+        if (rcond) HBEM_CUDA(cudaMemcpyAsync(rcond + f0, drcond, sizeof(double) * nf, cudaMemcpyDeviceToHost, st));
         if (do_refine && refine_iters)
             HBEM_CUDA(cudaMemcpyAsync(refine_iters + f0, diters, sizeof(int) * nf, cudaMemcpyDeviceToHost, st));
         if (do_refine && refine_resid)

@@ -75,9 +75,11 @@ _SIGNATURES = {
     "hbem_field": ([_vp, _c_int, _vp, _vp, _vp, _c_ll, _vp, _vp, _c_ll, _vp, _c_int, _vp, _vp, _c_ll, _vp], _c_int),
     "hbem_reduce_tag_avg": ([_vp, _c_int, _vp, _vp, _c_ll, _vp, _c_int, _vp, _vp], _c_int),
     "hbem_solve_batch": ([_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _c_int, _vp, _c_int, _c_int, _c_d, _c_int, _vp, _vp,
-                          _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _c_int),
+                          _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _c_int),
     "hbem_session_set_aperture": ([_vp, _c_int], _c_int),
     "hbem_set_tuning": ([_c_int, _c_int], _c_int),
+    "hbem_matrix_norm1": ([_c_int, _c_int, _vp, _vp, _c_ll, _c_ll, _vp, _vp], _c_int),
+    "hbem_lu_rcond": ([_c_int, _c_int, _vp, _vp, _c_ll, _c_ll, _vp, _vp, _vp], _c_int),
     "hbem_get_tuning": ([_c_int], _c_int),
     "hbem_reduce_tag_avg_device": ([_vp, _c_int, _vp, _vp, _c_ll, _vp, _c_int, _vp, _vp], _c_int),
     "hbem_session_set_vertices": ([_vp, _vp, _vp, _vp], _c_int),
@@ -321,6 +323,7 @@ class NativeSession:
         refine_tolerance: float = 1e-6,
         refine_max_iterations: int = 10,
         timings_out: dict | None = None,
+        compute_rcond: bool = True,
         **_ignored,
     ) -> list[CaseResult]:
         """Assemble, factor, solve and evaluate every frequency in one native call.
@@ -330,7 +333,9 @@ class NativeSession:
         ``neumann_dp0`` (F, T) complex DP0 Neumann data, ``observation_points``
         (3, N) or (N, 3).  ``dense_solve_dtype="float64"`` keeps the FP32 LU and
         refines the solution with FP64 residuals to 1e-7 (the GPU analogue of
-        the reference's complex128 zgesv path).
+        the reference's complex128 zgesv path).  ``compute_rcond`` adds the
+        1-norm condition estimate of each matrix (``dense_solve_rcond``), as the
+        reference computes with cgecon for every case.
         """
         freqs = np.ascontiguousarray(np.atleast_1d(frequency_hz), dtype=np.float64)
         F = freqs.shape[0]
@@ -364,6 +369,7 @@ class NativeSession:
         info = np.zeros(F, np.int32)
         iters = np.zeros(F, np.int32)
         resid = np.zeros(F, np.float64)
+        rcond = np.zeros(F, np.float64) if compute_rcond else None
         tms = np.zeros(4, np.float32)
         prec = HBEM_PREC_MIXED if precision == "mixed" else HBEM_PREC_PLAIN
         max_it = int(refine_max_iterations) if (prec == HBEM_PREC_MIXED or dense_solve_dtype == "float64") else 0
@@ -372,7 +378,8 @@ class NativeSession:
         check(self.lib.hbem_solve_batch(
             self.handle, F, _np_ptr(k_re), _np_ptr(k_im), _np_ptr(qr), _np_ptr(qi), _np_ptr(obs), N,
             _np_ptr(want_arr), len(want), prec, tol, max_it, _np_ptr(fr), _np_ptr(fi), _np_ptr(tavg), _np_ptr(sr),
-            _np_ptr(si), _np_ptr(info), _np_ptr(iters), _np_ptr(resid), _np_ptr(tms), None), "hbem_solve_batch", self.lib)
+            _np_ptr(si), _np_ptr(info), _np_ptr(iters), _np_ptr(resid), _np_ptr(rcond), _np_ptr(tms), None),
+            "hbem_solve_batch", self.lib)
         wall = time.perf_counter() - t0
         if timings_out is not None:
             timings_out.update(assembly_ms=float(tms[0]), solve_ms=float(tms[1]), field_ms=float(tms[2]),
@@ -387,7 +394,7 @@ class NativeSession:
                 "precision": precision,
                 "refine_iterations": int(iters[f]),
                 "refine_residual_rel": float(resid[f]) if max_it > 0 else None,
-                "dense_solve_rcond": None,
+                "dense_solve_rcond": float(rcond[f]) if rcond is not None and info[f] == 0 else None,
                 "assembly_mode": "corrected",
                 "duffy_pairs": None,
             }
@@ -411,7 +418,7 @@ class NativeSession:
                          field_k_f32=None, source_tags=None, impedance_source_tag=None,
                          write_surface_pressure=False, precision="plain", refine_tolerance=1e-6,
                          refine_max_iterations=10, timings_out=None, coupled_method="auto",
-                         max_chunk_bytes=None, **_ignored) -> list[CaseResult]:
+                         max_chunk_bytes=None, compute_rcond=True, **_ignored) -> list[CaseResult]:
         """Coupled interior BIE + Rayleigh half-space solve (the reference's aperture_tag path).
 
         ``coupled_method="schur"``: A - S_ia (2 S_aa)^-1 P_avg is factored per
@@ -464,7 +471,7 @@ class NativeSession:
             sl = slice(f0, min(F, f0 + chunk))
             run = self._coupled_chunk_augmented if method == "augmented" else self._coupled_chunk_schur
             parts.append(run(k_re[sl], None if k_im is None else k_im[sl], kf[sl], q_all[sl], obs_t, want,
-                             mixed, refine_tolerance, refine_max_iterations, times))
+                             mixed, refine_tolerance, refine_max_iterations, times, compute_rcond))
         if timings_out is not None:
             timings_out.update(assembly_ms=times[0], solve_ms=times[1], field_ms=times[2], coupled_method=method,
                                frequency_chunk=chunk)
@@ -484,16 +491,25 @@ class NativeSession:
                              "aperture_neumann": cat["qa"][f], "aperture_lapack_info": int(cat["info_ap"][f]),
                              "precision": precision, "refine_iterations": int(cat["iters"][f]),
                              "refine_residual_rel": float(cat["resid"][f]) if mixed else None,
-                             "dense_solve_rcond": None, "assembly_mode": "corrected"},
+                             "dense_solve_rcond": (float(cat["rcond"][f]) if "rcond" in cat and cat["info"][f] == 0
+                                                   else None),
+                             "assembly_mode": "corrected"},
             ))
         return out
 
-    def _factor_solve_refine(self, Kr, Ki, br, bi, N, F, mixed, tol, max_iter):
-        """LU (+ BF16x3 refinement) of F systems of order N stored (F, N, lda); returns x, info, iters, resid."""
+    def _factor_solve_refine(self, Kr, Ki, br, bi, N, F, mixed, tol, max_iter, rcond=False):
+        """LU (+ BF16x3 refinement) of F systems of order N stored (F, N, lda); returns x, info, iters,
+        resid and the 1-norm reciprocal condition estimates (or None)."""
         import torch
 
         dev, st = Kr.device, _stream_ptr()
         lda = int(Kr.shape[2])
+        anorm = rc = None
+        if rcond:
+            anorm = torch.empty(F, dtype=torch.float32, device=dev)
+            rc = torch.empty(F, dtype=torch.float64, device=dev)
+            check(self.lib.hbem_matrix_norm1(N, F, _t_ptr(Kr), _t_ptr(Ki), lda, N * lda, _t_ptr(anorm), st),
+                  "hbem_matrix_norm1", self.lib)
         K0r = K0i = None
         if mixed:
             K0r, K0i = Kr.clone(), Ki.clone()
@@ -503,6 +519,9 @@ class NativeSession:
         prec = HBEM_PREC_MIXED if mixed else HBEM_PREC_PLAIN
         check(self.lib.hbem_lu_factor(N, F, _t_ptr(Kr), _t_ptr(Ki), lda, N * lda, _t_ptr(piv), N, _t_ptr(info), prec,
                                       st), "hbem_lu_factor", self.lib)
+        if rcond:
+            check(self.lib.hbem_lu_rcond(N, F, _t_ptr(Kr), _t_ptr(Ki), lda, N * lda, _t_ptr(anorm), _t_ptr(rc), st),
+                  "hbem_lu_rcond", self.lib)
         check(self.lib.hbem_lu_solve(N, 1, F, _t_ptr(Kr), _t_ptr(Ki), lda, N * lda, _t_ptr(piv), N, _t_ptr(xr),
                                      _t_ptr(xi), 1, N, HBEM_TRANS_N, st), "hbem_lu_solve", self.lib)
         iters = torch.zeros(F, dtype=torch.int32, device=dev)
@@ -513,9 +532,9 @@ class NativeSession:
                                        float(tol), int(max_iter), _t_ptr(iters), _t_ptr(resid), st),
                   "hbem_refine", self.lib)
             del K0r, K0i
-        return xr, xi, info, iters, resid
+        return xr, xi, info, iters, resid, rc
 
-    def _coupled_chunk_schur(self, k_re, k_im, kf, q, obs_t, want, mixed, tol, max_iter, times):
+    def _coupled_chunk_schur(self, k_re, k_im, kf, q, obs_t, want, mixed, tol, max_iter, times, rcond=False):
         import torch
 
         dev, st = obs_t.device, _stream_ptr()
@@ -535,7 +554,7 @@ class NativeSession:
                                              _t_ptr(info_ap), st), "hbem_coupled_ib_schur", self.lib)
         del sia_r, sia_i, saa_r, saa_i
         ev[1].record()
-        xr, xi, info, iters, resid = self._factor_solve_refine(Ar, Ai, br, bi, n, F, mixed, tol, max_iter)
+        xr, xi, info, iters, resid, rc = self._factor_solve_refine(Ar, Ai, br, bi, n, F, mixed, tol, max_iter, rcond)
         del Ar, Ai
         ev[2].record()
         qa_r = torch.empty((F, m), dtype=torch.float32, device=dev); qa_i = torch.empty_like(qa_r)
@@ -545,7 +564,7 @@ class NativeSession:
                                              _t_ptr(fi), st), "hbem_coupled_ib_field", self.lib)
         tavg = self.tag_average(xr, xi, want).cpu().numpy() if want else None
         ev[3].record()
-        return self._chunk_out(ev, times, xr, xi, qa_r, qa_i, fr, fi, info, info_ap, iters, resid, tavg)
+        return self._chunk_out(ev, times, xr, xi, qa_r, qa_i, fr, fi, info, info_ap, iters, resid, tavg, rc)
 
     def coupled_ib_system(self, k_re, k_im, kf, q):
         """The augmented coupled system on the device: K (F, N, L) with row stride L = N rounded up to a
@@ -579,7 +598,7 @@ class NativeSession:
               "hbem_coupled_ib_augment", self.lib)
         return Kr, Ki, rr, ri, alpha
 
-    def _coupled_chunk_augmented(self, k_re, k_im, kf, q, obs_t, want, mixed, tol, max_iter, times):
+    def _coupled_chunk_augmented(self, k_re, k_im, kf, q, obs_t, want, mixed, tol, max_iter, times, rcond=False):
         import torch
 
         dev, st = obs_t.device, _stream_ptr()
@@ -589,7 +608,7 @@ class NativeSession:
         ev[0].record()
         Kr, Ki, rr, ri, alpha = self.coupled_ib_system(k_re, k_im, kf, q)
         ev[1].record()
-        xr, xi, info, iters, resid = self._factor_solve_refine(Kr, Ki, rr, ri, N, F, mixed, tol, max_iter)
+        xr, xi, info, iters, resid, rc = self._factor_solve_refine(Kr, Ki, rr, ri, N, F, mixed, tol, max_iter, rcond)
         del Kr, Ki
         ev[2].record()
         qa_r, qa_i = (xr[:, :m] * alpha[:, None]).contiguous(), (xi[:, :m] * alpha[:, None]).contiguous()
@@ -601,10 +620,10 @@ class NativeSession:
         tavg = self.tag_average(pr, pi, want).cpu().numpy() if want else None
         ev[3].record()
         info_ap = torch.zeros(F, dtype=torch.int32, device=dev)
-        return self._chunk_out(ev, times, pr, pi, qa_r, qa_i, fr, fi, info, info_ap, iters, resid, tavg)
+        return self._chunk_out(ev, times, pr, pi, qa_r, qa_i, fr, fi, info, info_ap, iters, resid, tavg, rc)
 
     @staticmethod
-    def _chunk_out(ev, times, pr, pi, qa_r, qa_i, fr, fi, info, info_ap, iters, resid, tavg):
+    def _chunk_out(ev, times, pr, pi, qa_r, qa_i, fr, fi, info, info_ap, iters, resid, tavg, rc=None):
         import torch
 
         torch.cuda.synchronize()
@@ -612,7 +631,7 @@ class NativeSession:
         cplx = lambda a, b: (a.cpu().numpy() + 1j * b.cpu().numpy()).astype(np.complex64)  # noqa: E731
         return {"field": cplx(fr, fi), "p": cplx(pr, pi), "qa": cplx(qa_r, qa_i), "info": info.cpu().numpy(),
                 "info_ap": info_ap.cpu().numpy(), "iters": iters.cpu().numpy(), "resid": resid.cpu().numpy(),
-                "tavg": tavg}
+                "tavg": tavg, "rcond": None if rc is None else rc.cpu().numpy()}
 
 
 # Drop-in alias for the reference's session class name.
@@ -628,7 +647,8 @@ class ResidentSweep:
     host transfer: corrected assembly -> LU -> solve -> field -> tag averages.
     """
 
-    def __init__(self, session: NativeSession, k_re, k_im, q, obs_3xn, tags, precision: str = "plain"):
+    def __init__(self, session: NativeSession, k_re, k_im, q, obs_3xn, tags, precision: str = "plain",
+                 rcond: bool = False):
         torch = require_cuda()
         self.s = session
         self.lib = session.lib
@@ -653,6 +673,8 @@ class ResidentSweep:
         self.f_im = torch.empty_like(self.f_re)
         self.tag_out = torch.empty((F, max(1, self.tags.shape[0]), 2), dtype=torch.float64, device=dev)
         self.precision = HBEM_PREC_MIXED if precision == "mixed" else HBEM_PREC_PLAIN
+        self.rcond = torch.empty(F, dtype=torch.float64, device=dev) if rcond else None
+        self.anorm = torch.empty(F, dtype=torch.float32, device=dev) if rcond else None
 
     def assemble(self, stream=None):
         n = self.n
@@ -665,8 +687,14 @@ class ResidentSweep:
         n, st = self.n, _stream_ptr(stream)
         self.x_re.copy_(self.b_re)
         self.x_im.copy_(self.b_im)
+        if self.rcond is not None:
+            check(self.lib.hbem_matrix_norm1(n, self.F, _t_ptr(self.A_re), _t_ptr(self.A_im), n, n * n,
+                                             _t_ptr(self.anorm), st), "hbem_matrix_norm1", self.lib)
         check(self.lib.hbem_lu_factor(n, self.F, _t_ptr(self.A_re), _t_ptr(self.A_im), n, n * n, _t_ptr(self.piv), n,
                                       _t_ptr(self.info), self.precision, st), "hbem_lu_factor", self.lib)
+        if self.rcond is not None:
+            check(self.lib.hbem_lu_rcond(n, self.F, _t_ptr(self.A_re), _t_ptr(self.A_im), n, n * n, _t_ptr(self.anorm),
+                                         _t_ptr(self.rcond), st), "hbem_lu_rcond", self.lib)
         check(self.lib.hbem_lu_solve(n, 1, self.F, _t_ptr(self.A_re), _t_ptr(self.A_im), n, n * n, _t_ptr(self.piv), n,
                                      _t_ptr(self.x_re), _t_ptr(self.x_im), 1, n, HBEM_TRANS_N, st), "hbem_lu_solve",
               self.lib)

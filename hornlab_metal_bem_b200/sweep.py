@@ -171,6 +171,7 @@ def run_sweep(mesh: LoadedMesh, frequencies, frame: ObservationFrame, config: So
                 impedance_source_tag=imp_tag, write_surface_pressure=config.return_surface_pressure,
                 dense_solve_dtype=config.dense_solve_dtype, precision=config.precision,
                 refine_tolerance=config.refine_tolerance, refine_max_iterations=config.refine_max_iterations,
+                compute_rcond=config.dense_solve_rcond_warning_threshold > 0,
             )
             for j, res in enumerate(results):
                 i = f0 + j

@@ -173,6 +173,21 @@ int hbem_refine(int n, int batch, const float *a_re, const float *a_im, long lon
                 double tol, int max_iter, int *iters, double *resid, void *stream);
 
 /*
+ * 1-norm condition estimate, as LAPACK cgecon (norm '1') on the factors.
+ * hbem_matrix_norm1: anorm[f] = ||A_f||_1 = max_j sum_i |a_ij| (clange '1'),
+ *   device float (batch,), of the matrix BEFORE factorisation.
+ * hbem_lu_rcond: rcond[f] = 1 / (anorm[f] * est ||(L U)^-1||_1), device double
+ *   (batch,), by Hager's method in Higham's formulation (CLACN2) with solves
+ *   by L U and (L U)^H; 0 when the estimate or the norm is 0.
+ * Replaces: matrixOneNorm / estimateReciprocalCondition (main.swift:463-503,
+ *   called per case at 7886 and 7898).
+ */
+int hbem_matrix_norm1(int n, int batch, const float *a_re, const float *a_im, long long lda, long long a_stride,
+                      float *anorm, void *stream);
+int hbem_lu_rcond(int n, int batch, const float *lu_re, const float *lu_im, long long lda, long long a_stride,
+                  const float *anorm, double *rcond, void *stream);
+
+/*
  * hbem_refine without any device allocation: same arguments, same results.
  * No counterpart in the reference, which allocates nothing on a device.
  * For callers that may not allocate device memory, such as a process whose
@@ -233,6 +248,8 @@ int hbem_reduce_tag_avg_device(hbem_session *s, int n_freq, const float *p_re, c
  * Host outputs: field (n_freq, n_obs) planar; tag_avg (n_freq, n_tags, 2)
  *   double; surface (n_freq, n_dof) planar or NULL; info (n_freq,);
  *   refine_iters (n_freq,) or NULL; refine_resid (n_freq,) or NULL;
+ *   rcond (n_freq,) or NULL: 1-norm reciprocal condition estimate of each
+ *   matrix (as cgecon; NULL skips the estimate);
  *   timings_ms (4,) = assembly, solve, field, total (device event times) or NULL.
  */
 int hbem_solve_batch(hbem_session *s, int n_freq, const float *k_re, const float *k_im,
@@ -242,7 +259,7 @@ int hbem_solve_batch(hbem_session *s, int n_freq, const float *k_re, const float
                      int precision, double refine_tol, int refine_max_iter,
                      float *field_re, float *field_im, double *tag_avg,
                      float *surface_re, float *surface_im,
-                     int *info, int *refine_iters, double *refine_resid,
+                     int *info, int *refine_iters, double *refine_resid, double *rcond,
                      float *timings_ms, void *stream);
 
 /*

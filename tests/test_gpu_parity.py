@@ -195,9 +195,10 @@ def test_lu_tall_panels_match_lapack(n):
     assert rel(X[0], ref) < (1e-5 if n < 3000 else 3e-5)
 
 
+@pytest.mark.parametrize("n", [130, 700])
 @pytest.mark.parametrize("trans", [1, 2])
-def test_transposed_solves(trans):
-    n, batch, nrhs = 130, 2, 3
+def test_transposed_solves(trans, n):
+    batch, nrhs = 2, 3
     A, _ = _lu_case(n, batch, 11)
     rng = np.random.default_rng(2)
     B = (rng.normal(size=(batch, n, nrhs)) + 1j * rng.normal(size=(batch, n, nrhs))).astype(np.complex64)
@@ -210,6 +211,91 @@ def test_transposed_solves(trans):
         op = A[m].T if trans == 1 else A[m].conj().T
         ref = np.linalg.solve(op.astype(np.complex128), B[m].astype(np.complex128))
         assert rel(X[m], ref) < 1e-5
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("trans", [0, 1, 2])
+@pytest.mark.parametrize("n", [33, 130, 700])
+def test_solve_schemes_match_lapack(n, trans, mode):
+    """Both solve schemes (1: one CTA per right-hand side, 2: blocked multi-CTA steps) for A, A^T, A^H."""
+    lib = load_library()
+    batch, nrhs = 2, 3
+    A, _ = _lu_case(n, batch, 900 + n)
+    rng = np.random.default_rng(n + trans)
+    B = (rng.normal(size=(batch, n, nrhs)) + 1j * rng.normal(size=(batch, n, nrhs))).astype(np.complex64)
+    Ar, Ai = _dev(A)
+    piv, info = _factor(Ar, Ai, n, batch)
+    Br, Bi = _dev(B)
+    assert lib.hbem_set_tuning(2, mode) == 0
+    try:
+        _solve(Ar, Ai, piv, Br, Bi, n, nrhs, batch, trans)
+    finally:
+        lib.hbem_set_tuning(2, 0)
+    X = _host(Br, Bi)
+    for m in range(batch):
+        op = A[m] if trans == 0 else (A[m].T if trans == 1 else A[m].conj().T)
+        ref = np.linalg.solve(op.astype(np.complex128), B[m].astype(np.complex128))
+        assert rel(X[m], ref) < 1e-5
+
+
+def _rcond_gpu(A):
+    """GPU ||A||_1 and cgecon-style estimate for a (batch, n, n) complex64 stack."""
+    import ctypes
+
+    lib = load_library()
+    batch, n = A.shape[0], A.shape[1]
+    Ar, Ai = _dev(A)
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    anorm = torch.empty(batch, dtype=torch.float32, device="cuda")
+    P = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    assert lib.hbem_matrix_norm1(n, batch, P(Ar), P(Ai), n, n * n, P(anorm), st) == 0
+    piv, info = _factor(Ar, Ai, n, batch)
+    rc = torch.empty(batch, dtype=torch.float64, device="cuda")
+    assert lib.hbem_lu_rcond(n, batch, P(Ar), P(Ai), n, n * n, P(anorm), P(rc), st) == 0
+    return anorm.cpu().numpy(), rc.cpu().numpy()
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("n", [1, 7, 200, 1059])
+def test_rcond_matches_lapack_cgecon(n, mode):
+    """The reference's estimateReciprocalCondition: clange('1') + cgecon on cgetrf factors
+    (with either solve scheme inside the estimator)."""
+    from scipy.linalg import lapack
+
+    A, _ = _lu_case(n, 2, 500 + n)
+    # a badly scaled column makes the estimate non-trivial
+    A[:, :, n // 2] *= 1e-3
+    lib = load_library()
+    assert lib.hbem_set_tuning(2, mode) == 0
+    try:
+        anorm, rc = _rcond_gpu(A)
+    finally:
+        lib.hbem_set_tuning(2, 0)
+    for m in range(A.shape[0]):
+        ref_norm = float(np.abs(A[m].astype(np.complex128)).sum(axis=0).max())
+        assert abs(anorm[m] - ref_norm) <= 1e-5 * ref_norm
+        lu, piv, info = lapack.cgetrf(A[m])
+        ref, info2 = lapack.cgecon(lu, ref_norm, norm="1")
+        assert info == 0 and info2 == 0
+        assert abs(rc[m] - ref) <= 1e-2 * ref, (rc[m], ref)
+        exact = 1.0 / (ref_norm * np.abs(np.linalg.inv(A[m].astype(np.complex128))).sum(axis=0).max())
+        assert rc[m] >= exact * (1 - 1e-3)
+
+
+def test_rcond_of_bem_matrix_matches_lapack():
+    from scipy.linalg import lapack
+
+    b = golden_buffers("horn_quarter")
+    q = _q(b.n_triangles, 1)
+    with _session("horn_quarter") as s:
+        Ar, Ai, br, bi = s.assemble([30.0, 140.0], np.repeat(q[None, :], 2, axis=0))
+        A = _host(Ar, Ai).astype(np.complex64)
+    anorm, rc = _rcond_gpu(A)
+    for m in range(2):
+        ref_norm = float(np.abs(A[m].astype(np.complex128)).sum(axis=0).max())
+        lu, piv, info = lapack.cgetrf(A[m])
+        ref, _ = lapack.cgecon(lu, ref_norm, norm="1")
+        assert abs(rc[m] - ref) <= 1e-2 * ref, (rc[m], ref)
 
 
 def test_singular_pivot_reports_info():

@@ -87,6 +87,11 @@ def test_quarter_horn_solve_matches_oracle():
         assert np.max(np.abs(res.directivity_db[f] - d_ref)) < 0.01
     assert set(res.surface_pressure_avg) == {2}
     assert res.native_diagnostics[0]["mesh_max_edge_m"] > 0
+    # the reference's per-case cgecon estimate and the conditioning policy on top of it
+    for d in res.native_diagnostics:
+        assert 0.0 < d["dense_solve_rcond"] < 1.0
+        assert d["dense_solve_policy_available"] is True
+        assert d["dense_solve_suspect"] is (d["dense_solve_rcond"] < d["dense_solve_rcond_warning_threshold"])
 
 
 def test_streaming_callback_early_stop_and_progress():
