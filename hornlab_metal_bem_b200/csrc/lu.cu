@@ -490,7 +490,7 @@ __device__ __forceinline__ void op_at(const float *Ar, const float *Ai, long lon
 // upper (from the bottom), unit or non-unit diagonal.
 template <bool LOWER, bool UNIT, int TR>
 __device__ void getrs_phase(int n, const float *Ar, const float *Ai, long long lda, float *xr, float *xi, float *t_r,
-                            float *t_i) {
+                            float *t_i, float *wt_r, float *wt_i) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nblk = (n + 31) / 32;
     for (int q = 0; q < nblk; ++q) {
@@ -528,6 +528,41 @@ __device__ void getrs_phase(int n, const float *Ar, const float *Ai, long long l
         // later rows: below the block (lower) or above it (upper)
         const int r0 = LOWER ? j0 + jb : 0, r1 = LOWER ? n : j0;
         const float cs = TR == 2 ? -1.f : 1.f;
+        if (TR == 0 && wt_r) {
+            // op = A: each warp takes 32 rows at a time, loads the 32 x jb block
+            // row by row (one 128-byte line per load) into its own tile, then
+            // lane r reduces row r from shared memory
+            float *mr = wt_r + warp * (32 * 33), *mi = wt_i + warp * (32 * 33);
+            for (int gb = r0 + warp * 32; gb < r1; gb += (blockDim.x >> 5) * 32) {
+                const int nr = min(32, r1 - gb);
+#pragma unroll 8
+                for (int rr = 0; rr < 32; ++rr) {
+                    float vr = 0.f, vi = 0.f;
+                    if (rr < nr && lane < jb) {
+                        vr = Ar[(size_t)(gb + rr) * lda + j0 + lane];
+                        vi = Ai[(size_t)(gb + rr) * lda + j0 + lane];
+                    }
+                    mr[rr * 33 + lane] = vr;
+                    mi[rr * 33 + lane] = vi;
+                }
+                __syncwarp();
+                float pr = 0.f, pi = 0.f;
+#pragma unroll 8
+                for (int c = 0; c < 32; ++c) {
+                    const float ar = mr[lane * 33 + c], ai = mi[lane * 33 + c];
+                    const float x_r = xr[j0 + c], x_i = xi[j0 + c];
+                    pr += ar * x_r - ai * x_i;
+                    pi += ar * x_i + ai * x_r;
+                }
+                if (lane < nr) {
+                    xr[gb + lane] -= pr;
+                    xi[gb + lane] -= pi;
+                }
+                __syncwarp();
+            }
+            __syncthreads();
+            continue;
+        }
         for (int i = r0 + tid; i < r1; i += blockDim.x) {
             float pr = 0.f, pi = 0.f;
             if (TR == 0) {
@@ -590,12 +625,14 @@ __global__ void __launch_bounds__(kGetrsThreads) k_getrs(int n, const float *lu_
     };
     if (TR == 0 && pv) permute(false);
     __syncthreads();
+    float *wt_r = TR == 0 ? s_x + 2 * n : nullptr;          // per-warp 32 x 33 tiles (op = A)
+    float *wt_i = TR == 0 ? wt_r + (kGetrsThreads / 32) * 32 * 33 : nullptr;
     if (TR == 0) {
-        getrs_phase<true, true, 0>(n, Ar, Ai, lda, xr, xi, t_r, t_i);
-        getrs_phase<false, false, 0>(n, Ar, Ai, lda, xr, xi, t_r, t_i);
+        getrs_phase<true, true, 0>(n, Ar, Ai, lda, xr, xi, t_r, t_i, wt_r, wt_i);
+        getrs_phase<false, false, 0>(n, Ar, Ai, lda, xr, xi, t_r, t_i, wt_r, wt_i);
     } else {
-        getrs_phase<true, false, TR>(n, Ar, Ai, lda, xr, xi, t_r, t_i);
-        getrs_phase<false, true, TR>(n, Ar, Ai, lda, xr, xi, t_r, t_i);
+        getrs_phase<true, false, TR>(n, Ar, Ai, lda, xr, xi, t_r, t_i, nullptr, nullptr);
+        getrs_phase<false, true, TR>(n, Ar, Ai, lda, xr, xi, t_r, t_i, nullptr, nullptr);
     }
     if (TR != 0 && pv) permute(true);
     __syncthreads();
@@ -1317,9 +1354,13 @@ int lu_solve_single(int n, int nrhs, int batch, const float *lu_re, const float 
         attr = true;
     }
     dim3 grid(nrhs, batch);
-    if (trans == HBEM_TRANS_N)
-        k_getrs<0><<<grid, kGetrsThreads, smem, st>>>(n, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re, b_im, ldb,
-                                                     b_stride);
+    const size_t tiles = (size_t)2 * (kGetrsThreads / 32) * 32 * 33 * sizeof(float);
+    if (trans == HBEM_TRANS_N && smem + tiles <= 200 * 1024)
+        k_getrs<0><<<grid, kGetrsThreads, smem + tiles, st>>>(n, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re,
+                                                             b_im, ldb, b_stride);
+    else if (trans == HBEM_TRANS_N)
+        return lu_solve_blocked(n, nrhs, batch, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re, b_im, ldb, b_stride,
+                                trans, st);
     else if (trans == HBEM_TRANS_T)
         k_getrs<1><<<grid, kGetrsThreads, smem, st>>>(n, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re, b_im, ldb,
                                                      b_stride);

@@ -324,6 +324,7 @@ class NativeSession:
         refine_max_iterations: int = 10,
         timings_out: dict | None = None,
         compute_rcond: bool = True,
+        impedance_sources=None,
         **_ignored,
     ) -> list[CaseResult]:
         """Assemble, factor, solve and evaluate every frequency in one native call.
@@ -342,6 +343,17 @@ class NativeSession:
         k_re = np.ascontiguousarray(np.atleast_1d(k_real_f32), dtype=np.float32)
         if k_re.shape != (F,):
             raise ValueError("k_real_f32 must have one value per frequency")
+        if impedance_sources:
+            per = impedance_sources if isinstance(impedance_sources, list) else [impedance_sources] * F
+            if len(per) != F:
+                raise ValueError(f"impedance_sources list must have one dict per frequency ({F}), got {len(per)}")
+            if any(per):
+                return self._robin_batch(freqs, k_re, k_imag_f32, neumann_dp0, observation_points, per,
+                                         source_tags=source_tags, impedance_source_tag=impedance_source_tag,
+                                         write_surface_pressure=write_surface_pressure, precision=precision,
+                                         refine_tolerance=refine_tolerance,
+                                         refine_max_iterations=refine_max_iterations, timings_out=timings_out,
+                                         compute_rcond=compute_rcond)
         k_im = None if k_imag_f32 is None else np.ascontiguousarray(np.atleast_1d(k_imag_f32), dtype=np.float32)
         q = np.asarray(neumann_dp0)
         if q.shape != (F, self.n_triangles):
@@ -413,6 +425,120 @@ class NativeSession:
         return results
 
 
+    # -- Robin (impedance) boundaries -----------------------------------------
+    def _robin_batch(self, freqs, k_re, k_imag_f32, neumann_dp0, observation_points, per_freq, *, source_tags,
+                     impedance_source_tag, write_surface_pressure, precision, refine_tolerance,
+                     refine_max_iterations, timings_out, compute_rcond):
+        """Sweep with Robin admittances beta per tag: the assembly adds the Robin terms
+        (``main.swift:1731-1760, 3016``) and the field uses the Neumann data with the
+        Robin contribution q + i k beta p_avg on Robin faces (``neumannWithRobin``,
+        ``main.swift:1646-1674``).  Frequencies sharing one admittance set share one
+        assembly launch."""
+        torch = require_cuda()
+        dev = torch.device("cuda", self.device)
+        st = _stream_ptr()
+        F, n, T = freqs.shape[0], self.n_dof, self.n_triangles
+        k_im = (np.zeros(F, np.float32) if k_imag_f32 is None
+                else np.ascontiguousarray(np.atleast_1d(k_imag_f32), dtype=np.float32))
+        q = np.asarray(neumann_dp0).reshape(F, T)
+        obs = np.asarray(observation_points, dtype=np.float64)
+        if obs.shape[0] != 3:
+            obs = obs.T
+        obs_t = torch.tensor(np.ascontiguousarray(obs, dtype=np.float32), device=dev)
+        N = obs_t.shape[1]
+        tags_tri = np.asarray(self.buffers.physical_tags_i32)
+        l2g = torch.as_tensor(np.asarray(self.buffers.p1_local2global_i32, dtype=np.int64), device=dev)
+        tags = list(source_tags or [])
+        want = tags + ([impedance_source_tag] if impedance_source_tag is not None and impedance_source_tag not in tags
+                       else [])
+        mixed = precision == "mixed"
+        out_field = np.zeros((F, N), np.complex64)
+        out_p = np.zeros((F, n), np.complex64)
+        out_tavg = np.zeros((F, max(1, len(want))), np.complex128)
+        out_info = np.zeros(F, np.int64)
+        out_iter = np.zeros(F, np.int64)
+        out_res = np.zeros(F)
+        out_rc = np.full(F, np.nan)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        t_asm = t_solve = t_field = 0.0
+        # group consecutive frequencies with equal admittance sets
+        groups, start = [], 0
+        for f in range(1, F + 1):
+            if f == F or per_freq[f] != per_freq[start]:
+                groups.append((start, f))
+                start = f
+        for g0, g1 in groups:
+            Fg = g1 - g0
+            sl = slice(g0, g1)
+            beta = np.zeros(T, np.complex64)
+            for tag, b in per_freq[g0].items():
+                beta[tags_tri == int(tag)] = complex(b)
+            b_re = torch.tensor(np.ascontiguousarray(beta.real), device=dev)
+            b_im = torch.tensor(np.ascontiguousarray(beta.imag), device=dev)
+            qr, qi = self._split_device(q[sl], (Fg, T), dev)
+            Ar = torch.empty((Fg, n, n), dtype=torch.float32, device=dev)
+            Ai = torch.empty_like(Ar)
+            br = torch.empty((Fg, n), dtype=torch.float32, device=dev)
+            bi = torch.empty_like(br)
+            kr_g, ki_g = np.ascontiguousarray(k_re[sl]), np.ascontiguousarray(k_im[sl])
+            ev[0].record()
+            check(self.lib.hbem_assemble(self.handle, Fg, _np_ptr(kr_g), _np_ptr(ki_g), _t_ptr(qr), _t_ptr(qi), T,
+                                         _t_ptr(b_re), _t_ptr(b_im), _t_ptr(Ar), _t_ptr(Ai), n, n * n, _t_ptr(br),
+                                         _t_ptr(bi), n, HBEM_ASM_CORRECTED | HBEM_ASM_ZERO, st),
+                  "hbem_assemble", self.lib)
+            ev[1].record()
+            xr, xi, info, iters, resid, rc = self._factor_solve_refine(Ar, Ai, br, bi, n, Fg, mixed, refine_tolerance,
+                                                                     refine_max_iterations, compute_rcond)
+            del Ar, Ai
+            ev[2].record()
+            # Neumann data with the Robin term for the field
+            p_c = torch.complex(xr, xi)
+            p_avg = (p_c[:, l2g[:, 0]] + p_c[:, l2g[:, 1]] + p_c[:, l2g[:, 2]]) / 3.0
+            ik = torch.complex(torch.tensor(-ki_g, device=dev), torch.tensor(kr_g, device=dev))[:, None]
+            beta_t = torch.complex(b_re, b_im)[None, :]
+            q_tot = torch.complex(qr, qi) + ik * beta_t * p_avg
+            qtr, qti = q_tot.real.contiguous(), q_tot.imag.contiguous()
+            fr = torch.empty((Fg, N), dtype=torch.float32, device=dev)
+            fi = torch.empty_like(fr)
+            check(self.lib.hbem_field(self.handle, Fg, _np_ptr(kr_g), _t_ptr(xr), _t_ptr(xi), n, _t_ptr(qtr),
+                                      _t_ptr(qti), T, _t_ptr(obs_t), N, _t_ptr(fr), _t_ptr(fi), N, st),
+                  "hbem_field", self.lib)
+            tavg = self.tag_average(xr, xi, want).cpu().numpy() if want else None
+            ev[3].record()
+            torch.cuda.synchronize()
+            t_asm += ev[0].elapsed_time(ev[1])
+            t_solve += ev[1].elapsed_time(ev[2])
+            t_field += ev[2].elapsed_time(ev[3])
+            out_field[sl] = (fr.cpu().numpy() + 1j * fi.cpu().numpy()).astype(np.complex64)
+            out_p[sl] = p_c.cpu().numpy().astype(np.complex64)
+            if tavg is not None:
+                out_tavg[sl] = tavg[..., 0] + 1j * tavg[..., 1]
+            out_info[sl] = info.cpu().numpy()
+            out_iter[sl] = iters.cpu().numpy()
+            out_res[sl] = resid.cpu().numpy()
+            if rc is not None:
+                out_rc[sl] = rc.cpu().numpy()
+        if timings_out is not None:
+            timings_out.update(assembly_ms=t_asm, solve_ms=t_solve, field_ms=t_field, total_ms=t_asm + t_solve + t_field)
+        results = []
+        for f in range(F):
+            avgs = {int(t): complex(out_tavg[f, j]) for j, t in enumerate(want)}
+            results.append(CaseResult(
+                frequency_hz=float(freqs[f]), field=out_field[f],
+                impedance=avgs.get(int(impedance_source_tag)) if impedance_source_tag is not None else None,
+                surface_pressure_avg={int(t): avgs[int(t)] for t in tags} if tags else None,
+                surface_pressure=out_p[f] if write_surface_pressure else None,
+                assembly_s=t_asm * 1e-3 / F, dense_solve_s=t_solve * 1e-3 / F, field_s=t_field * 1e-3 / F,
+                lapack_info=int(out_info[f]),
+                diagnostics={"dense_solve_impl": "hbem_blocked_lu_" + ("bf16x3_refined" if mixed else "fp32"),
+                             "precision": precision, "refine_iterations": int(out_iter[f]),
+                             "refine_residual_rel": float(out_res[f]) if mixed else None,
+                             "dense_solve_rcond": (float(out_rc[f]) if compute_rcond and out_info[f] == 0 else None),
+                             "robin_tags": sorted(int(t) for t in per_freq[f]),
+                             "assembly_mode": "corrected"},
+            ))
+        return results
+
     # -- coupled infinite baffle ---------------------------------------------
     def coupled_ib_batch(self, frequency_hz, k_real_f32, neumann_dp0, observation_points, *, k_imag_f32=None,
                          field_k_f32=None, source_tags=None, impedance_source_tag=None,
@@ -433,6 +559,10 @@ class NativeSession:
         torch = require_cuda()
         if self.m_aperture <= 0:
             raise ValueError("session has no aperture_tag")
+        if _ignored.get("impedance_sources") and any(
+                _ignored["impedance_sources"] if isinstance(_ignored["impedance_sources"], list)
+                else [_ignored["impedance_sources"]]):
+            raise BackendUnavailable("impedance_sources (Robin) are not supported with the coupled infinite baffle")
         if coupled_method not in ("auto", "schur", "augmented"):
             raise ValueError("coupled_method must be 'auto', 'schur' or 'augmented'")
         method = coupled_method

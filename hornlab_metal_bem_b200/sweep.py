@@ -42,9 +42,42 @@ def should_route_native(config: SolveConfig) -> bool:
         )
     if config.chief_points is not None:
         raise BackendUnavailable("chief_points (CHIEF least squares) is not supported by the B200 path")
-    if config.impedance_sources or config.impedance_source_callback is not None:
-        raise BackendUnavailable("impedance_sources (Robin) are not routed by the B200 sweep yet")
     return True
+
+
+def impedance_sources_for_frequencies(physical_tags, frequencies, config: SolveConfig):
+    """Robin admittance per frequency: the static ``impedance_sources`` dict, or one dict per
+    frequency when ``impedance_source_callback`` is set (its values override / extend the static
+    ones); tags absent from the mesh are skipped with a warning and non-passive values
+    (``Re(beta) < 0``) or non-finite values from the callback raise (``sweep.py:164-239``)."""
+    mesh_tags = {int(t) for t in np.unique(physical_tags)}
+    static: dict[int, complex] = {}
+    for tag, beta in (config.impedance_sources or {}).items():
+        if int(tag) not in mesh_tags:
+            logger.warning("impedance_sources references tag %d but mesh has no elements with that tag; skipping",
+                           int(tag))
+            continue
+        static[int(tag)] = complex(beta)
+    if config.impedance_source_callback is None:
+        return [dict(static) for _ in np.atleast_1d(frequencies)]
+    out = []
+    for freq in np.atleast_1d(frequencies):
+        f = float(freq)
+        merged = dict(static)
+        for tag, beta in config.impedance_source_callback(f).items():
+            t = int(tag)
+            if t not in mesh_tags:
+                logger.warning("impedance_source_callback returned tag %d not in mesh; skipping", t)
+                continue
+            b = complex(beta)
+            if not (math.isfinite(b.real) and math.isfinite(b.imag)):
+                raise ValueError(f"impedance_source_callback({f:.3f}) returned non-finite beta for tag {t}")
+            if b.real < 0.0:
+                raise ValueError(f"impedance_source_callback({f:.3f}) returned Re(beta)={b.real:.4g} < 0 for tag {t}; "
+                                 "admittance must be passive (Re(beta) >= 0)")
+            merged[t] = b
+        out.append(merged)
+    return out
 
 
 def k_values(frequencies, config: SolveConfig) -> tuple[np.ndarray, np.ndarray]:
@@ -57,13 +90,16 @@ def k_values(frequencies, config: SolveConfig) -> tuple[np.ndarray, np.ndarray]:
     return k_re, k_im
 
 
-def neumann_rows(n_faces: int, physical_tags, frequencies, config: SolveConfig, source_face_scale=None) -> np.ndarray:
-    tags_robin = set(config.impedance_sources.keys())
-    return np.stack([
-        build_driver_neumann(n_faces, physical_tags, 2.0 * np.pi * float(f), config, np.complex64,
-                             impedance_tags=tags_robin, source_face_scale=source_face_scale)
-        for f in frequencies
-    ])
+def neumann_rows(n_faces: int, physical_tags, frequencies, config: SolveConfig, source_face_scale=None,
+                 impedance_per_freq=None) -> np.ndarray:
+    """Driver Neumann rows; Robin tags of each frequency are skipped as velocity sources (``sweep.py:242-285``)."""
+    rows = []
+    for i, f in enumerate(frequencies):
+        tags_robin = (set(impedance_per_freq[i].keys()) if impedance_per_freq is not None
+                      else set(config.impedance_sources.keys()))
+        rows.append(build_driver_neumann(n_faces, physical_tags, 2.0 * np.pi * float(f), config, np.complex64,
+                                         impedance_tags=tags_robin, source_face_scale=source_face_scale))
+    return np.stack(rows)
 
 
 def field_points_3xn(obs_points: np.ndarray) -> np.ndarray:
@@ -149,7 +185,12 @@ def run_sweep(mesh: LoadedMesh, frequencies, frame: ObservationFrame, config: So
         n_sphere = sp.shape[1]
         pts = np.concatenate([pts, sp], axis=1)
     k_re, k_im = k_values(freqs, config)
-    q = neumann_rows(buffers.n_triangles, mesh.physical_tags, freqs, config, scale)
+    robin = None
+    if config.impedance_sources or config.impedance_source_callback is not None:
+        robin = impedance_sources_for_frequencies(mesh.physical_tags, freqs, config)
+        if not any(robin):
+            robin = None
+    q = neumann_rows(buffers.n_triangles, mesh.physical_tags, freqs, config, scale, robin)
 
     own = session is None
     if own:
@@ -172,6 +213,7 @@ def run_sweep(mesh: LoadedMesh, frequencies, frame: ObservationFrame, config: So
                 dense_solve_dtype=config.dense_solve_dtype, precision=config.precision,
                 refine_tolerance=config.refine_tolerance, refine_max_iterations=config.refine_max_iterations,
                 compute_rcond=config.dense_solve_rcond_warning_threshold > 0,
+                impedance_sources=None if robin is None else robin[sl],
             )
             for j, res in enumerate(results):
                 i = f0 + j

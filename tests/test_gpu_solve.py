@@ -34,12 +34,22 @@ def _oracle_sweep(mesh, res, config, sym=0):
     k_re, _ = k_values(res.frequencies_hz, config)
     q = neumann_rows(buf.n_triangles, mesh.physical_tags, res.frequencies_hz, config, scale)
     pts = field_points_3xn(res.observation_points)
+    beta = None
+    if config.impedance_sources:
+        beta = np.zeros(buf.n_triangles, np.complex64)
+        for tag, bv in config.impedance_sources.items():
+            beta[np.asarray(mesh.physical_tags) == int(tag)] = complex(bv)
+    l2g = np.asarray(buf.p1_local2global_i32)
     out_p, out_f = [], []
     for f in range(len(res.frequencies_hz)):
-        A, b = o.corrected(float(k_re[f]), q[f])
+        A, b = o.corrected(float(k_re[f]), q[f], 0.0, beta)
         p = dense_solve(A, b, "f64")
         out_p.append(p)
-        out_f.append(o.field(float(k_re[f]), p, q[f], pts))
+        q_f = q[f].astype(np.complex128)
+        if beta is not None:
+            # the field's Neumann data on Robin faces: q + i k beta p_avg (main.swift:1646-1674)
+            q_f = q_f + 1j * float(k_re[f]) * beta * p[l2g].mean(axis=1)
+        out_f.append(o.field(float(k_re[f]), p, q_f, pts))
     return np.array(out_p), np.array(out_f)
 
 
@@ -121,3 +131,32 @@ def test_mixed_precision_refines_to_plain_solution():
         assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-4
         assert mixed.native_diagnostics[f]["refine_residual_rel"] <= 1e-6
     assert np.max(np.abs(mixed.directivity_db - plain.directivity_db)) < 0.01
+
+
+def test_robin_walls_match_oracle():
+    """Impedance (Robin) walls on the quarter horn: assembly Robin terms and the field's
+    Neumann-with-Robin data against the oracle; a per-frequency callback splits the
+    sweep into admittance groups."""
+    mesh = G.horn(G.HornSpec(edge=0.014), quarter=True)
+    base = dict(freq_min_hz=500.0, freq_max_hz=8000.0, freq_count=3, source_motion="axial",
+                native_symmetry_plane="yz+xz", native_check_open_edges=False,
+                observation=hb.ObservationConfig(planes=["horizontal", "vertical"], angle_count=13),
+                return_surface_pressure=True)
+    cfg = hb.native_config(impedance_sources={1: 0.35 + 0.12j}, **base)
+    res = hb.solve(mesh, cfg)
+    p_ref, f_ref = _oracle_sweep(mesh, res, cfg, sym=3)
+    for f in range(3):
+        assert np.linalg.norm(res.surface_pressure_complex[f] - p_ref[f]) / np.linalg.norm(p_ref[f]) < 1e-4
+        fld = res.pressure_complex[f].reshape(-1)
+        assert np.linalg.norm(fld - f_ref[f]) / np.linalg.norm(f_ref[f]) < 1e-4
+        assert res.native_diagnostics[f]["robin_tags"] == [1]
+    # rigid walls give a different answer (the Robin term is live)
+    rigid = hb.solve(mesh, hb.native_config(**base))
+    assert np.linalg.norm(rigid.surface_pressure_complex[1] - res.surface_pressure_complex[1]) > \
+        1e-3 * np.linalg.norm(res.surface_pressure_complex[1])
+    # callback: frequency-dependent admittance, non-passive values rejected
+    cb = hb.native_config(impedance_source_callback=lambda f: {1: 0.2 + 1e-5 * f}, **base)
+    res_cb = hb.solve(mesh, cb)
+    assert all(d["robin_tags"] == [1] for d in res_cb.native_diagnostics)
+    with pytest.raises(ValueError):
+        hb.solve(mesh, hb.native_config(impedance_source_callback=lambda f: {1: -0.1}, **base))

@@ -1,0 +1,31 @@
+"""Host logic of the sweep: per-frequency Robin admittance resolution (sweep.py:164-239 semantics)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import hornlab_metal_bem_b200 as hb
+from hornlab_metal_bem_b200.sweep import impedance_sources_for_frequencies
+
+TAGS = np.array([1, 1, 2, 2, 2], np.int32)
+
+
+def test_static_admittance_skips_missing_tags():
+    cfg = hb.native_config(impedance_sources={1: 0.3 + 0.1j, 9: 1.0})
+    per = impedance_sources_for_frequencies(TAGS, [100.0, 200.0], cfg)
+    assert per == [{1: 0.3 + 0.1j}, {1: 0.3 + 0.1j}]
+
+
+def test_callback_overrides_and_extends_static():
+    cfg = hb.native_config(impedance_sources={1: 0.5}, impedance_source_callback=lambda f: {2: f * 1e-3, 7: 1.0})
+    per = impedance_sources_for_frequencies(TAGS, [100.0, 300.0], cfg)
+    assert per == [{1: 0.5, 2: 0.1}, {1: 0.5, 2: 0.3}]
+    cfg2 = hb.native_config(impedance_sources={1: 0.5}, impedance_source_callback=lambda f: {1: 0.25})
+    assert impedance_sources_for_frequencies(TAGS, [50.0], cfg2) == [{1: 0.25}]
+
+
+@pytest.mark.parametrize("bad", [-0.1, complex(float("nan"), 0.0)])
+def test_callback_rejects_non_passive_or_non_finite(bad):
+    cfg = hb.native_config(impedance_source_callback=lambda f: {1: bad})
+    with pytest.raises(ValueError):
+        impedance_sources_for_frequencies(TAGS, [100.0], cfg)
