@@ -371,6 +371,341 @@ __global__ void __launch_bounds__(kAsmThreads, MINB) k_regular(const __grid_cons
     }
 }
 
+// ---------------------------------------------------------------------------
+// Regular assembly over unordered triangle pairs.  For a sample pair (x on
+// the test triangle tau, y on an image M sigma of the trial triangle) the
+// double-layer kernel in both orders shares everything but a dot product:
+//   dG/dn_y(x, My) = F(r) (d . M n_sigma),   dG/dn_x(y, Mx) = F(r) (-d . n_tau),
+//   F = e^{ikr} (ik - 1/r) / r^2,  d = My - x,  r = |d| = |Mx - y|
+// (M is an involution and an isometry), and G(r) is the same.  So each
+// unordered pair {tau, sigma} (sorted index tau <= sigma) is evaluated once
+// and adds A[tau dofs][sigma dofs], A[sigma dofs][tau dofs] and both RHS
+// rows: one rsqrt / sincos per sample instead of two.  Tiles and the shared
+// accumulation are those of k_regular with a second, transposed plane.
+// ---------------------------------------------------------------------------
+template <bool CK, bool NEED_G>
+__device__ __forceinline__ void sample_sym(float dx, float dy, float dz, float nsx, float nsy, float nsz, float ntx,
+                                           float nty, float ntz, float k, float kt, float ki, float &dre, float &dim,
+                                           float &tre, float &tim, float &gre, float &gim) {
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    float u = rsqrtf(r2);
+    u = r2 > 1.0e-14f ? u : 0.0f;
+    const float r = r2 * u;
+    const float u2 = u * u;
+    float hs = fmaf(dx, nsx, fmaf(dy, nsy, dz * nsz)) * u2;
+    float ht = -fmaf(dx, ntx, fmaf(dy, nty, dz * ntz)) * u2;
+    float t = r * kt;
+    t -= round_fma(t);
+    float sn, cs;
+    __sincosf(t * 6.28318530717958647692f, &sn, &cs);
+    float uu = u, fre = u;
+    if (CK) {
+        const float damp = __expf(-ki * r);
+        hs *= damp;
+        ht *= damp;
+        uu *= damp;
+        fre += ki;
+    }
+    // E = (c + i s)(-fre + i k); D = h E
+    const float e_re = -fmaf(cs, fre, sn * k), e_im = fmaf(cs, k, -sn * fre);
+    dre = fmaf(hs, e_re, dre);
+    dim = fmaf(hs, e_im, dim);
+    tre = fmaf(ht, e_re, tre);
+    tim = fmaf(ht, e_im, tim);
+    if (NEED_G) {
+        gre = fmaf(uu, cs, gre);
+        gim = fmaf(uu, sn, gim);
+    }
+}
+
+// One unordered pair, one wavenumber.  Outputs (times 1/(4 pi) and the
+// Jacobians later): fwd[i*3+j] test dof i x trial dof j, trn[j*3+i] trial dof j
+// x test dof i; SLP rows sfw[i] (test) and str[j] (trial, summed with the
+// test-point weights only).
+template <int SYM, bool CK, bool NEED_G>
+__device__ __forceinline__ void pair_block_sym(const float4 *__restrict__ tq, const float4 *__restrict__ sp, float nx,
+                                               float ny, float nz, float tnx, float tny, float tnz, bool self, float k,
+                                               float kt, float ki, float (&fwr)[9], float (&fwi)[9], float (&tnr)[9],
+                                               float (&tni)[9], float (&sfr)[3], float (&sfi)[3], float (&str_)[3],
+                                               float (&sti)[3]) {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) fwr[i] = fwi[i] = tnr[i] = tni[i] = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) sfr[i] = sfi[i] = str_[i] = sti[i] = 0.0f;
+#pragma unroll 1
+    for (int a = 0; a < 6; ++a) {
+        const float4 x = tq[a * kTestTile];
+        float ere[3], eim[3], tre_[3], tim_[3], hre = 0.f, him = 0.f, g2r[3], g2i[3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) ere[j] = eim[j] = tre_[j] = tim_[j] = g2r[j] = g2i[j] = 0.f;
+#pragma unroll
+        for (int b = 0; b < 6; ++b) {
+            const float4 y = sp[b];
+            float dre = 0.f, dim = 0.f, tre = 0.f, tim = 0.f, gre = 0.f, gim = 0.f;
+            if (!(self && a == b))
+                sample_sym<CK, NEED_G>(y.x - x.x, y.y - x.y, y.z - x.z, nx, ny, nz, tnx, tny, tnz, k, kt, ki, dre,
+                                       dim, tre, tim, gre, gim);
+            if (SYM == 1 || SYM == 3)
+                sample_sym<CK, NEED_G>(-y.x - x.x, y.y - x.y, y.z - x.z, -nx, ny, nz, tnx, tny, tnz, k, kt, ki, dre,
+                                       dim, tre, tim, gre, gim);
+            if (SYM == 2 || SYM == 3)
+                sample_sym<CK, NEED_G>(y.x - x.x, -y.y - x.y, y.z - x.z, nx, -ny, nz, tnx, tny, tnz, k, kt, ki, dre,
+                                       dim, tre, tim, gre, gim);
+            if (SYM == 3)
+                sample_sym<CK, NEED_G>(-y.x - x.x, -y.y - x.y, y.z - x.z, -nx, -ny, nz, tnx, tny, tnz, k, kt, ki, dre,
+                                       dim, tre, tim, gre, gim);
+            if (SYM == 4)
+                sample_sym<CK, NEED_G>(y.x - x.x, y.y - x.y, -y.z - x.z, nx, ny, -nz, tnx, tny, tnz, k, kt, ki, dre,
+                                       dim, tre, tim, gre, gim);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const float wb = qw(b) * bas(b, j);
+                ere[j] = fmaf(dre, wb, ere[j]);
+                eim[j] = fmaf(dim, wb, eim[j]);
+                tre_[j] = fmaf(tre, wb, tre_[j]);
+                tim_[j] = fmaf(tim, wb, tim_[j]);
+                if (NEED_G) {
+                    g2r[j] = fmaf(gre, wb, g2r[j]);
+                    g2i[j] = fmaf(gim, wb, g2i[j]);
+                }
+            }
+            if (NEED_G) {
+                hre = fmaf(gre, qw(b), hre);
+                him = fmaf(gim, qw(b), him);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const float wa = c_wa[a][i];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                fwr[i * 3 + j] = fmaf(wa, ere[j], fwr[i * 3 + j]);
+                fwi[i * 3 + j] = fmaf(wa, eim[j], fwi[i * 3 + j]);
+                tnr[j * 3 + i] = fmaf(wa, tre_[j], tnr[j * 3 + i]);
+                tni[j * 3 + i] = fmaf(wa, tim_[j], tni[j * 3 + i]);
+            }
+            if (NEED_G) {
+                sfr[i] = fmaf(wa, hre, sfr[i]);
+                sfi[i] = fmaf(wa, him, sfi[i]);
+            }
+        }
+        if (NEED_G) {
+            const float wq = c_w[a];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                str_[j] = fmaf(wq, g2r[j], str_[j]);
+                sti[j] = fmaf(wq, g2i[j], sti[j]);
+            }
+        }
+    }
+}
+
+// blockIdx.z = frequency.  CTAs whose test triangles all follow their trial
+// triangles in the sorted order have no unordered pair of their own and exit.
+template <int SYM, bool CK, int MINB>
+__global__ void __launch_bounds__(kAsmThreads, MINB) k_regular_sym(const __grid_constant__ AsmArgs p) {
+    extern __shared__ float2 s_acc[];
+    __shared__ float4 s_qp[kTrialTile * 6];
+    __shared__ float4 s_tq[kTestTile * 6];
+    __shared__ float4 s_nrm[kTrialTile];
+    __shared__ uchar4 s_cs[kTrialTile];
+    __shared__ float4 s_qb[kTrialTile];
+    __shared__ int s_flag[kTrialTile];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int f = blockIdx.z;
+    const int test_tile = blockIdx.y, trial_tile = blockIdx.x;
+    const int T = p.T;
+    const int tbase = trial_tile * kTrialTile;
+    const int ntrial = min(kTrialTile, T - tbase);
+    const int test0 = test_tile * kTestTile;
+    const int ntest = min(kTestTile, T - test0);
+    if (test0 > tbase + ntrial - 1) return;   // every test triangle follows every trial triangle
+    const int r0 = p.row_off[test_tile], nrows = p.row_off[test_tile + 1] - r0;
+    const int c0 = p.col_off[trial_tile], ncols = p.col_off[trial_tile + 1] - c0;
+    const int ldc = ncols | 1, ldr = nrows | 1;
+    float2 *acc = s_acc;                       // nrows x ldc   (test rows, trial columns)
+    float2 *rhs = acc + nrows * ldc;           // nrows
+    float2 *acc2 = rhs + nrows;                // ncols x ldr   (trial rows, test columns)
+    float2 *rhs2 = acc2 + ncols * ldr;         // ncols
+    const int plane = nrows * ldc + nrows + ncols * ldr + ncols;
+
+    for (int i = tid; i < plane; i += kAsmThreads) s_acc[i] = make_float2(0.f, 0.f);
+    for (int i = tid; i < ntrial * 6; i += kAsmThreads) s_qp[i] = p.qp[(size_t)tbase * 6 + i];
+    for (int i = tid; i < ntest * 6; i += kAsmThreads) {
+        const int t = i / 6, a = i - 6 * t;
+        s_tq[a * kTestTile + t] = p.qp[(size_t)(test0 + t) * 6 + a];
+    }
+    for (int i = tid; i < ntrial; i += kAsmThreads) {
+        s_nrm[i] = p.nrm[tbase + i];
+        s_cs[i] = p.trial_slot[tbase + i];
+        const int orig = p.tri[tbase + i].w;
+        float4 qb = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (p.q_re) {
+            qb.x = p.q_re[(size_t)f * p.q_stride + orig];
+            qb.y = p.q_im[(size_t)f * p.q_stride + orig];
+        }
+        if (p.beta_re) {
+            qb.z = p.beta_re[orig];
+            qb.w = p.beta_im[orig];
+        }
+        s_qb[i] = qb;
+        s_flag[i] = (qb.x != 0.f || qb.y != 0.f || qb.z != 0.f || qb.w != 0.f) ? 1 : 0;
+    }
+    __syncthreads();
+
+    const float k = p.k[f], kt = p.kt[f], ki = p.ki[f];
+    const int test = test0 + lane;
+    if (lane < ntest) {
+        const float4 tn = p.nrm[test];
+        const float tjac = tn.w;
+        const uchar4 rs = p.test_slot[test];
+        const int rslot[3] = {rs.x, rs.y, rs.z};
+        const int torig = p.tri[test].w;
+        float4 tqb = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (p.q_re) {
+            tqb.x = p.q_re[(size_t)f * p.q_stride + torig];
+            tqb.y = p.q_im[(size_t)f * p.q_stride + torig];
+        }
+        if (p.beta_re) {
+            tqb.z = p.beta_re[torig];
+            tqb.w = p.beta_im[torig];
+        }
+        const bool tflag = tqb.x != 0.f || tqb.y != 0.f || tqb.z != 0.f || tqb.w != 0.f;
+        const float4 *tq = &s_tq[lane];
+        // i k beta / 3 terms: Robin rows of the trial (forward) and test (transposed) triangles
+        auto robin = [&](float br, float bi, float &rr, float &ri) {
+            rr = 0.f;
+            ri = 0.f;
+            if (br != 0.f || bi != 0.f) {
+                const float ikb_re = -ki * br - k * bi;
+                const float ikb_im = -ki * bi + k * br;
+                rr = -ikb_re * (1.0f / 3.0f);
+                ri = -ikb_im * (1.0f / 3.0f);
+            }
+        };
+        float rob2_re, rob2_im;
+        robin(tqb.z, tqb.w, rob2_re, rob2_im);
+        for (int jj = warp; jj < ntrial; jj += kAsmThreads / 32) {
+            const int sigma = tbase + jj;
+            if (sigma < test) continue;
+            const float4 nj = s_nrm[jj];
+            const bool self = sigma == test;
+            float fwr[9], fwi[9], tnr[9], tni[9], sfr[3], sfi[3], str_[3], sti[3];
+            if (s_flag[jj] || tflag)
+                pair_block_sym<SYM, CK, true>(tq, &s_qp[jj * 6], nj.x, nj.y, nj.z, tn.x, tn.y, tn.z, self, k, kt, ki,
+                                              fwr, fwi, tnr, tni, sfr, sfi, str_, sti);
+            else
+                pair_block_sym<SYM, CK, false>(tq, &s_qp[jj * 6], nj.x, nj.y, nj.z, tn.x, tn.y, tn.z, self, k, kt, ki,
+                                               fwr, fwi, tnr, tni, sfr, sfi, str_, sti);
+            const float scale = HBEM_INV4PI * tjac * nj.w;
+            const uchar4 cs = s_cs[jj];
+            const int cslot[3] = {cs.x, cs.y, cs.z};
+            const float4 qb = s_qb[jj];
+            float rob_re, rob_im;
+            robin(qb.z, qb.w, rob_re, rob_im);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const float s_re = sfr[i] * scale, s_im = sfi[i] * scale;
+                const float radd_re = rob_re * s_re - rob_im * s_im;
+                const float radd_im = rob_re * s_im + rob_im * s_re;
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    float vre = fwr[i * 3 + j] * scale + radd_re;
+                    float vim = fwi[i * 3 + j] * scale + radd_im;
+                    if (self) vre -= 0.25f * tjac * (i == j ? (1.0f / 6.0f) : (1.0f / 12.0f));
+                    float2 *dst = &acc[rslot[i] * ldc + cslot[j]];
+                    atomicAdd(&dst->x, vre * p.rw);
+                    atomicAdd(&dst->y, vim * p.rw);
+                }
+                if (qb.x != 0.f || qb.y != 0.f) {
+                    atomicAdd(&rhs[rslot[i]].x, (s_re * qb.x - s_im * qb.y) * p.rw);
+                    atomicAdd(&rhs[rslot[i]].y, (s_re * qb.y + s_im * qb.x) * p.rw);
+                }
+            }
+            if (self) continue;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const float s_re = str_[j] * scale, s_im = sti[j] * scale;
+                const float radd_re = rob2_re * s_re - rob2_im * s_im;
+                const float radd_im = rob2_re * s_im + rob2_im * s_re;
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    const float vre = tnr[j * 3 + i] * scale + radd_re;
+                    const float vim = tni[j * 3 + i] * scale + radd_im;
+                    float2 *dst = &acc2[cslot[j] * ldr + rslot[i]];
+                    atomicAdd(&dst->x, vre * p.rw);
+                    atomicAdd(&dst->y, vim * p.rw);
+                }
+                if (tqb.x != 0.f || tqb.y != 0.f) {
+                    atomicAdd(&rhs2[cslot[j]].x, (s_re * tqb.x - s_im * tqb.y) * p.rw);
+                    atomicAdd(&rhs2[cslot[j]].y, (s_re * tqb.y + s_im * tqb.x) * p.rw);
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    float *are_g = p.a_re + (size_t)f * p.a_stride;
+    float *aim_g = p.a_im + (size_t)f * p.a_stride;
+    for (int e = tid; e < nrows * ncols; e += kAsmThreads) {
+        const int r = e / ncols, c = e - r * ncols;
+        const float2 v = acc[r * ldc + c];
+        if (v.x != 0.f || v.y != 0.f) {
+            const size_t off = (size_t)p.rows[r0 + r] * p.lda + p.cols[c0 + c];
+            atomicAdd(are_g + off, v.x);
+            atomicAdd(aim_g + off, v.y);
+        }
+    }
+    for (int e = tid; e < ncols * nrows; e += kAsmThreads) {
+        const int c = e / nrows, r = e - c * nrows;
+        const float2 v = acc2[c * ldr + r];
+        if (v.x != 0.f || v.y != 0.f) {
+            const size_t off = (size_t)p.cols[c0 + c] * p.lda + p.rows[r0 + r];
+            atomicAdd(are_g + off, v.x);
+            atomicAdd(aim_g + off, v.y);
+        }
+    }
+    if (p.q_re) {
+        for (int r = tid; r < nrows; r += kAsmThreads) {
+            const float2 v = rhs[r];
+            if (v.x != 0.f || v.y != 0.f) {
+                const size_t off = (size_t)f * p.b_stride + p.rows[r0 + r];
+                atomicAdd(p.b_re + off, v.x);
+                atomicAdd(p.b_im + off, v.y);
+            }
+        }
+        for (int c = tid; c < ncols; c += kAsmThreads) {
+            const float2 v = rhs2[c];
+            if (v.x != 0.f || v.y != 0.f) {
+                const size_t off = (size_t)f * p.b_stride + p.cols[c0 + c];
+                atomicAdd(p.b_re + off, v.x);
+                atomicAdd(p.b_im + off, v.y);
+            }
+        }
+    }
+}
+
+template <int SYM, bool CK, int MINB>
+cudaError_t launch_regular_sym_t(const AsmArgs &a, dim3 grid, size_t smem, cudaStream_t st) {
+    auto kern = k_regular_sym<SYM, CK, MINB>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kern<<<grid, kAsmThreads, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <bool CK>
+cudaError_t dispatch_sym_pairs(int sym, const AsmArgs &a, dim3 grid, size_t smem, cudaStream_t st) {
+    switch (sym) {
+        case 0: return launch_regular_sym_t<0, CK, 2>(a, grid, smem, st);
+        case 1: return launch_regular_sym_t<1, CK, 2>(a, grid, smem, st);
+        case 2: return launch_regular_sym_t<2, CK, 2>(a, grid, smem, st);
+        case 3: return launch_regular_sym_t<3, CK, 2>(a, grid, smem, st);
+        default: return launch_regular_sym_t<4, CK, 2>(a, grid, smem, st);
+    }
+}
+
 template <int SYM, bool CK, int MINB>
 cudaError_t launch_regular_t(const AsmArgs &a, dim3 grid, size_t smem, cudaStream_t st) {
     auto kern = k_regular<SYM, CK, MINB>;
@@ -626,6 +961,8 @@ int launch_regular(Session &s, int n_freq, const float *k_re, const float *k_im,
                    float *a_im, long long lda, long long a_stride, float *b_re, float *b_im, long long b_stride,
                    cudaStream_t st) {
     const size_t smem = (size_t)kAsmFreqs * (s.max_rows * (s.max_cols | 1) + s.max_rows) * sizeof(float2);
+    const size_t smem_sym = (size_t)(s.max_rows * (s.max_cols | 1) + s.max_rows + s.max_cols * (s.max_rows | 1) +
+                                     s.max_cols) * sizeof(float2);
     static bool consts_ready[64] = {false};
     if (s.device >= 0 && s.device < 64 && !consts_ready[s.device]) {
         const double QX[6] = {0.4459484909159651, 0.0915762135097710, 0.1081030181680700,
@@ -645,7 +982,7 @@ int launch_regular(Session &s, int n_freq, const float *k_re, const float *k_im,
         HBEM_CUDA(cudaMemcpyToSymbol(c_w, w, sizeof(w)));
         consts_ready[s.device] = true;
     }
-    if (smem > 180 * 1024)
+    if (smem > 180 * 1024 || smem_sym > 180 * 1024)
         return fail(HBEM_ERR_ARG, "assembly tile needs too much shared memory (mesh ordering too scattered)");
     for (int f0 = 0; f0 < n_freq; f0 += kMaxFreqPerLaunch) {
         const int nf = std::min(kMaxFreqPerLaunch, n_freq - f0);
@@ -666,8 +1003,16 @@ int launch_regular(Session &s, int n_freq, const float *k_re, const float *k_im,
         for (int f = 0; f < nf; ++f) ck |= a.ki[f] != 0.f;
         if (!a.b_re) a.q_re = a.q_im = nullptr;
         a.nf = nf;
-        dim3 grid(s.n_trial_tiles, s.n_test_tiles, (nf + kAsmFreqs - 1) / kAsmFreqs);
-        cudaError_t e = ck ? dispatch_sym<true>(s.sym, a, grid, smem, st) : dispatch_sym<false>(s.sym, a, grid, smem, st);
+        cudaError_t e;
+        if (tuning(HBEM_TUNE_ASM_PAIRS) != 1) {
+            // unordered pairs, one wavenumber per grid slice
+            dim3 grid(s.n_trial_tiles, s.n_test_tiles, nf);
+            e = ck ? dispatch_sym_pairs<true>(s.sym, a, grid, smem_sym, st)
+                   : dispatch_sym_pairs<false>(s.sym, a, grid, smem_sym, st);
+        } else {
+            dim3 grid(s.n_trial_tiles, s.n_test_tiles, (nf + kAsmFreqs - 1) / kAsmFreqs);
+            e = ck ? dispatch_sym<true>(s.sym, a, grid, smem, st) : dispatch_sym<false>(s.sym, a, grid, smem, st);
+        }
         if (e != cudaSuccess) return cuda_fail(e, "k_regular launch");
         count_launch();
         ++s.launches;

@@ -88,13 +88,17 @@ long long hbem_launch_count(void);
  *   HBEM_TUNE_ASM_MINBLOCKS: resident CTAs per SM of the pair-assembly kernel
  *                            (2: 128 registers, 3: 80 registers)
  *   HBEM_TUNE_LU_PANEL:      inner sub-panel width of the LU (16 or 32)
- *   HBEM_TUNE_LU_SOLVE:      no-transpose solve (1: one CTA per right-hand
+ *   HBEM_TUNE_LU_SOLVE:      triangular solves (1: one CTA per right-hand
  *                            side, 2: blocked multi-CTA steps)
+ *   HBEM_TUNE_ASM_PAIRS:     regular assembly (0: unordered pairs, both
+ *                            orders from one kernel evaluation; 1: ordered
+ *                            pairs, two wavenumbers per evaluation)
  */
 #define HBEM_TUNE_ASM_MINBLOCKS 0
 #define HBEM_TUNE_LU_PANEL 1
 #define HBEM_TUNE_LU_SOLVE 2
-#define HBEM_TUNE_COUNT 3
+#define HBEM_TUNE_ASM_PAIRS 3
+#define HBEM_TUNE_COUNT 4
 int hbem_set_tuning(int key, int value);
 int hbem_get_tuning(int key);
 
