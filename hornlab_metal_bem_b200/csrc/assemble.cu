@@ -773,7 +773,7 @@ struct DuffyArgs {
     const int *ap_local;
     float *sia_re, *sia_im, *saa_re, *saa_im;
     long long sia_stride, saa_stride;
-    int m_ap, mode;
+    int m_ap, mode, nf;
     float k[kMaxFreqPerLaunch];
     float kt[kMaxFreqPerLaunch];
     float ki[kMaxFreqPerLaunch];
@@ -802,12 +802,17 @@ __device__ __forceinline__ void remap(float x, float y, int kind, int l1, int l2
     }
 }
 
-template <bool CK>
-__global__ void __launch_bounds__(256) k_duffy(const __grid_constant__ DuffyArgs p) {
+// NF wavenumbers per warp (blockIdx.y = group of NF consecutive wavenumbers;
+// a missing last member is computed on a repeated wavenumber and not
+// written).  The singular points are summed first (FP32 lane partials, FP64
+// warp reduction), then the same registers take the regular points.
+template <bool CK, int NF, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_duffy(const __grid_constant__ DuffyArgs p) {
     const int lane = threadIdx.x & 31;
     const int pi = blockIdx.x * 8 + (threadIdx.x >> 5);
     if (pi >= p.n_pairs) return;
-    const int f = blockIdx.y;
+    const int fg = blockIdx.y * NF;
+    const int nfv = min(NF, p.nf - fg);
     const DuffyPair pr = p.pairs[pi];
     const int V = p.V, T = p.T;
     // pairs without an aperture trial (and, for S_aa, an unmirrored aperture
@@ -831,16 +836,17 @@ __global__ void __launch_bounds__(256) k_duffy(const __grid_constant__ DuffyArgs
     const bool tswap = __popc(pr.test_mask) & 1, sswap = __popc(pr.trial_mask) & 1;
     const float nx = ssx * p.normals[pr.trial], ny = ssy * p.normals[T + pr.trial], nz = ssz * p.normals[2 * T + pr.trial];
     const float jac = (2.f * p.areas[pr.test]) * (2.f * p.areas[pr.trial]);
-    const float k = p.k[f], kt = p.kt[f], ki = p.ki[f];
-
-    // Per-lane partial sums over this lane's <= 48 points stay in FP32 (separate
-    // singular and regular sets, so their difference is never formed in FP32);
-    // the cross-lane reduction and the singular - regular difference are FP64.
-    float accs[24], accr[24];
+    float k[NF], kt[NF], ki[NF];
 #pragma unroll
-    for (int e = 0; e < 24; ++e) accs[e] = accr[e] = 0.0f;
+    for (int f = 0; f < NF; ++f) {
+        const int ff = fg + min(f, nfv - 1);
+        k[f] = p.k[ff];
+        kt[f] = p.kt[ff];
+        ki[f] = p.ki[ff];
+    }
 
-    auto accumulate = [&](float (&acc)[24], float txi, float teta, float sxi, float seta, float w) {
+    float acc[NF][24];
+    auto accumulate = [&](float txi, float teta, float sxi, float seta, float w) {
         if (tswap) { const float t = txi; txi = teta; teta = t; }
         if (sswap) { const float t = sxi; sxi = seta; seta = t; }
         const float tb[3] = {1.f - txi - teta, txi, teta};
@@ -851,30 +857,52 @@ __global__ void __launch_bounds__(256) k_duffy(const __grid_constant__ DuffyArgs
             x[c] = tb[0] * P[0][c] + tb[1] * P[1][c] + tb[2] * P[2][c];
             y[c] = sb[0] * S[0][c] + sb[1] * S[1][c] + sb[2] * S[2][c];
         }
-        float dre = 0, dim = 0, gre = 0, gim = 0;
-        sample<CK, true>(ssx * y[0] - tsx * x[0], ssy * y[1] - tsy * x[1], ssz * y[2] - tsz * x[2], nx, ny, nz, k, kt,
-                         ki, dre, dim, gre, gim);
-        gre *= w; gim *= w; dre *= w; dim *= w;
+        float dre[NF], dim[NF], gre[NF], gim[NF];
 #pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            acc[2 * i] = fmaf(gre, tb[i], acc[2 * i]);
-            acc[2 * i + 1] = fmaf(gim, tb[i], acc[2 * i + 1]);
-            const float dti_re = dre * tb[i], dti_im = dim * tb[i];
+        for (int f = 0; f < NF; ++f) dre[f] = dim[f] = gre[f] = gim[f] = 0.f;
+        sample_nf<NF, CK, true>(ssx * y[0] - tsx * x[0], ssy * y[1] - tsy * x[1], ssz * y[2] - tsz * x[2], nx, ny, nz,
+                                k, kt, ki, dre, dim, gre, gim);
 #pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                acc[6 + 2 * (i * 3 + j)] = fmaf(dti_re, sb[j], acc[6 + 2 * (i * 3 + j)]);
-                acc[7 + 2 * (i * 3 + j)] = fmaf(dti_im, sb[j], acc[7 + 2 * (i * 3 + j)]);
+        for (int f = 0; f < NF; ++f) {
+            const float gr = gre[f] * w, gi = gim[f] * w, dr = dre[f] * w, di = dim[f] * w;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                acc[f][2 * i] = fmaf(gr, tb[i], acc[f][2 * i]);
+                acc[f][2 * i + 1] = fmaf(gi, tb[i], acc[f][2 * i + 1]);
+                const float dti_re = dr * tb[i], dti_im = di * tb[i];
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    acc[f][6 + 2 * (i * 3 + j)] = fmaf(dti_re, sb[j], acc[f][6 + 2 * (i * 3 + j)]);
+                    acc[f][7 + 2 * (i * 3 + j)] = fmaf(dti_im, sb[j], acc[f][7 + 2 * (i * 3 + j)]);
+                }
             }
         }
     };
-
-    // regular 6x6 rule, subtracted; the coincident self-point is excluded by
-    // index exactly as in the regular assembly (main.swift:4323-4336)
-    for (int q = lane; q < 36; q += 32) {
-        const int a = q / 6, b = q - 6 * (q / 6);
-        if (pr.test == pr.trial && pr.test_mask == pr.trial_mask && a == b) continue;
-        accumulate(accr, qx(a), qy(a), qx(b), qy(b), qw(a) * qw(b));
+    // lane e < 9 keeps DLP entry e, lanes 9..11 the SLP rows: (re, im) per wavenumber, FP64
+    double own_re[NF], own_im[NF];
+    auto reduce_keep = [&](double sign) {
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+#pragma unroll
+            for (int e = 0; e < 24; ++e) {
+                double v = (double)acc[f][e];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                const int owner = e < 6 ? 9 + (e >> 1) : (e - 6) >> 1;
+                if (lane == owner) {
+                    if (e & 1) own_im[f] += sign * v;
+                    else own_re[f] += sign * v;
+                }
+            }
+        }
+    };
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+        own_re[f] = own_im[f] = 0.0;
+#pragma unroll
+        for (int e = 0; e < 24; ++e) acc[f][e] = 0.f;
     }
+    // singular (Duffy) points
     const int ri = pr.kind - 1;
     const int off = p.rule_off[ri], cnt = p.rule_cnt[ri];
     for (int q = lane; q < cnt; q += 32) {
@@ -883,65 +911,79 @@ __global__ void __launch_bounds__(256) k_duffy(const __grid_constant__ DuffyArgs
         float tx_, ty_, sx_, sy_;
         remap(r.x, r.y, pr.kind, pr.tl1, pr.tl2, tx_, ty_);
         remap(r.z, r.w, pr.kind, pr.sl1, pr.sl2, sx_, sy_);
-        accumulate(accs, tx_, ty_, sx_, sy_, w);
+        accumulate(tx_, ty_, sx_, sy_, w);
     }
-    double acc[24];
+    reduce_keep(1.0);
+    // regular 6x6 rule, subtracted; the coincident self-point is excluded by
+    // index exactly as in the regular assembly (main.swift:4323-4336)
 #pragma unroll
-    for (int e = 0; e < 24; ++e) {
-        double v = (double)accs[e] - (double)accr[e];
+    for (int f = 0; f < NF; ++f)
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        acc[e] = v;
+        for (int e = 0; e < 24; ++e) acc[f][e] = 0.f;
+    for (int q = lane; q < 36; q += 32) {
+        const int a = q / 6, b = q - 6 * (q / 6);
+        if (pr.test == pr.trial && pr.test_mask == pr.trial_mask && a == b) continue;
+        accumulate(qx(a), qy(a), qx(b), qy(b), qw(a) * qw(b));
     }
+    reduce_keep(-1.0);
     const double scale = (double)HBEM_INV4PI * (double)jac * (double)pr.weight;
-    // lane e < 9 owns DLP entry e; lanes 9..11 own the SLP rows
-    double sr = 0, si = 0, dr = 0, di = 0;
-#pragma unroll
-    for (int e = 0; e < 9; ++e)
-        if (lane == e) { dr = acc[6 + 2 * e]; di = acc[7 + 2 * e]; }
     const int i_row = lane < 9 ? lane / 3 : lane - 9;
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-        if (i_row == i) { sr = acc[2 * i]; si = acc[2 * i + 1]; }
-    sr *= scale; si *= scale; dr *= scale; di *= scale;
     if (p.mode == 1) {
-        // S_aa: sum_i delta_slp_i / area(test), one contribution per unmirrored pair
-        if (lane == 0) {
-            const double s_re = (acc[0] + acc[2] + acc[4]) * (double)HBEM_INV4PI * (double)jac;
-            const double s_im = (acc[1] + acc[3] + acc[5]) * (double)HBEM_INV4PI * (double)jac;
-            const double inv = 1.0 / fmax((double)p.areas[pr.test], 1e-38);
-            const size_t o = (size_t)f * p.saa_stride + (size_t)p.ap_local[pr.test] * p.m_ap + p.ap_local[pr.trial];
-            atomicAdd(p.saa_re + o, (float)(s_re * inv));
-            atomicAdd(p.saa_im + o, (float)(s_im * inv));
+        // S_aa: sum_i delta_slp_i / area(test), one contribution per unmirrored pair:
+        // gather the three SLP rows (lanes 9..11) and let lane 9 write
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+            double s_re = (lane >= 9 && lane < 12) ? own_re[f] : 0.0, s_im = (lane >= 9 && lane < 12) ? own_im[f] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                s_re += __shfl_xor_sync(0xffffffffu, s_re, o);
+                s_im += __shfl_xor_sync(0xffffffffu, s_im, o);
+            }
+            if (lane == 9 && f < nfv) {
+                const double inv = 1.0 / fmax((double)p.areas[pr.test], 1e-38);
+                const size_t o = (size_t)(fg + f) * p.saa_stride + (size_t)p.ap_local[pr.test] * p.m_ap +
+                                 p.ap_local[pr.trial];
+                atomicAdd(p.saa_re + o, (float)(s_re * (double)HBEM_INV4PI * (double)jac * inv));
+                atomicAdd(p.saa_im + o, (float)(s_im * (double)HBEM_INV4PI * (double)jac * inv));
+            }
         }
         return;
     }
-    if (p.sia_re && lane >= 9 && lane < 12) {
-        const int t = p.ap_local[pr.trial];
-        if (t >= 0) {
-            const size_t o = (size_t)f * p.sia_stride + (size_t)p.l2g[pr.test * 3 + i_row] * p.m_ap + t;
-            atomicAdd(p.sia_re + o, (float)sr);
-            atomicAdd(p.sia_im + o, (float)si);
+    // SLP rows (lanes 9..11), broadcast to the DLP lanes of the same row for Robin
+#pragma unroll
+    for (int f = 0; f < nfv; ++f) {
+        const double sr_own = own_re[f] * scale, si_own = own_im[f] * scale;
+        const double sr = __shfl_sync(0xffffffffu, sr_own, 9 + i_row);
+        const double si = __shfl_sync(0xffffffffu, si_own, 9 + i_row);
+        double dr = own_re[f] * scale, di = own_im[f] * scale;
+        if (p.sia_re && lane >= 9 && lane < 12) {
+            const int t = p.ap_local[pr.trial];
+            if (t >= 0) {
+                const size_t o = (size_t)(fg + f) * p.sia_stride + (size_t)p.l2g[pr.test * 3 + i_row] * p.m_ap + t;
+                atomicAdd(p.sia_re + o, (float)sr);
+                atomicAdd(p.sia_im + o, (float)si);
+            }
         }
-    }
-    if (!p.a_re) return;
-    const float br = p.beta_re ? p.beta_re[pr.trial] : 0.f, bi = p.beta_im ? p.beta_im[pr.trial] : 0.f;
-    if (lane < 9) {
-        const int j = lane - 3 * (lane / 3);
-        if (br != 0.f || bi != 0.f) {
-            const double ikb_re = -(double)ki * br - (double)k * bi, ikb_im = -(double)ki * bi + (double)k * br;
-            dr -= (sr * ikb_re - si * ikb_im) / 3.0;
-            di -= (sr * ikb_im + si * ikb_re) / 3.0;
-        }
-        const size_t o = (size_t)f * p.a_stride + (size_t)p.l2g[pr.test * 3 + i_row] * p.lda + p.l2g[pr.trial * 3 + j];
-        atomicAdd(p.a_re + o, (float)dr);
-        atomicAdd(p.a_im + o, (float)di);
-    } else if (lane < 12 && p.q_re) {
-        const float qr = p.q_re[(size_t)f * p.q_stride + pr.trial], qi = p.q_im[(size_t)f * p.q_stride + pr.trial];
-        if (qr != 0.f || qi != 0.f) {
-            const size_t o = (size_t)f * p.b_stride + p.l2g[pr.test * 3 + i_row];
-            atomicAdd(p.b_re + o, (float)(sr * qr - si * qi));
-            atomicAdd(p.b_im + o, (float)(sr * qi + si * qr));
+        if (!p.a_re) continue;
+        const float br = p.beta_re ? p.beta_re[pr.trial] : 0.f, bi = p.beta_im ? p.beta_im[pr.trial] : 0.f;
+        if (lane < 9) {
+            const int j = lane - 3 * (lane / 3);
+            if (br != 0.f || bi != 0.f) {
+                const double ikb_re = -(double)ki[f] * br - (double)k[f] * bi, ikb_im = -(double)ki[f] * bi + (double)k[f] * br;
+                dr -= (sr * ikb_re - si * ikb_im) / 3.0;
+                di -= (sr * ikb_im + si * ikb_re) / 3.0;
+            }
+            const size_t o = (size_t)(fg + f) * p.a_stride + (size_t)p.l2g[pr.test * 3 + i_row] * p.lda +
+                             p.l2g[pr.trial * 3 + j];
+            atomicAdd(p.a_re + o, (float)dr);
+            atomicAdd(p.a_im + o, (float)di);
+        } else if (lane < 12 && p.q_re) {
+            const float qr = p.q_re[(size_t)(fg + f) * p.q_stride + pr.trial], qi = p.q_im[(size_t)(fg + f) * p.q_stride + pr.trial];
+            if (qr != 0.f || qi != 0.f) {
+                const size_t o = (size_t)(fg + f) * p.b_stride + p.l2g[pr.test * 3 + i_row];
+                atomicAdd(p.b_re + o, (float)(sr * qr - si * qi));
+                atomicAdd(p.b_im + o, (float)(sr * qi + si * qr));
+            }
         }
     }
 }
@@ -1053,9 +1095,18 @@ int launch_duffy(Session &s, int n_freq, const float *k_re, const float *k_im, c
         }
         bool ck = false;
         for (int f = 0; f < nf; ++f) ck |= a.ki[f] != 0.f;
-        dim3 grid((s.n_pairs + 7) / 8, nf);
-        if (ck) k_duffy<true><<<grid, 256, 0, st>>>(a);
-        else k_duffy<false><<<grid, 256, 0, st>>>(a);
+        a.nf = nf;
+        // variant: 1 = one wavenumber per warp (3 CTAs/SM), 2 = two (2 CTAs/SM, the default:
+        // 10.6 vs 11.3 ms on the 1043-dof yz+xz horn at 40 wavenumbers)
+        const int var = tuning(HBEM_TUNE_DUFFY) == 1 ? 1 : 2;
+        dim3 grid((s.n_pairs + 7) / 8, (nf + var - 1) / var);
+        if (var == 2) {
+            if (ck) k_duffy<true, 2, 2><<<grid, 256, 0, st>>>(a);
+            else k_duffy<false, 2, 2><<<grid, 256, 0, st>>>(a);
+        } else {
+            if (ck) k_duffy<true, 1, 3><<<grid, 256, 0, st>>>(a);
+            else k_duffy<false, 1, 3><<<grid, 256, 0, st>>>(a);
+        }
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_fail(e, "k_duffy launch");
         count_launch();

@@ -93,12 +93,15 @@ long long hbem_launch_count(void);
  *   HBEM_TUNE_ASM_PAIRS:     regular assembly (0: unordered pairs, both
  *                            orders from one kernel evaluation; 1: ordered
  *                            pairs, two wavenumbers per evaluation)
+ *   HBEM_TUNE_DUFFY:         singular corrections (1: one wavenumber per
+ *                            warp, 2: two wavenumbers per warp)
  */
 #define HBEM_TUNE_ASM_MINBLOCKS 0
 #define HBEM_TUNE_LU_PANEL 1
 #define HBEM_TUNE_LU_SOLVE 2
 #define HBEM_TUNE_ASM_PAIRS 3
-#define HBEM_TUNE_COUNT 4
+#define HBEM_TUNE_DUFFY 4
+#define HBEM_TUNE_COUNT 5
 int hbem_set_tuning(int key, int value);
 int hbem_get_tuning(int key);
 
