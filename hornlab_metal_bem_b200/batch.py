@@ -11,8 +11,9 @@ stays on the device:
   their estimated cost (n^3 for the LU, T^2 M for the assembly), so small
   meshes overlap with large ones; meshes on one stream share one workspace
   sized for the largest of them;
-* an autotuner picks, per mesh-size bucket, the kernel variants (assembly
-  occupancy, LU sub-panel width, solve scheme) by timing candidates on a
+* an autotuner picks, per mesh-size bucket, the kernel variants (ordered or
+  unordered pair assembly and its occupancy, Duffy wavenumbers per warp, LU
+  sub-panel width, solve scheme) by timing candidates on a
   representative mesh, and caches the choice per GPU model.
 """
 from __future__ import annotations
@@ -29,7 +30,7 @@ from .native import (
     load_library, require_cuda,
 )
 
-TUNE_ASM_MINBLOCKS, TUNE_LU_PANEL, TUNE_LU_SOLVE = 0, 1, 2
+TUNE_ASM_MINBLOCKS, TUNE_LU_PANEL, TUNE_LU_SOLVE, TUNE_ASM_PAIRS, TUNE_DUFFY = 0, 1, 2, 3, 4
 IMAGES = {None: 1, "yz": 2, "xz": 2, "yz+xz": 4, "xy": 2}
 
 
@@ -88,10 +89,12 @@ def size_bucket(n: int) -> str:
 
 # ------------------------------------------------------------------ autotuner
 CANDIDATES = (
-    {"asm": 0, "panel": 0, "solve": 0},
-    {"asm": 3, "panel": 0, "solve": 0},
-    {"asm": 0, "panel": 16, "solve": 0},
-    {"asm": 0, "panel": 0, "solve": 1},
+    {"asm": 0, "panel": 0, "solve": 0, "pairs": 0, "duffy": 0},
+    {"asm": 0, "panel": 0, "solve": 0, "pairs": 1, "duffy": 0},
+    {"asm": 3, "panel": 0, "solve": 0, "pairs": 1, "duffy": 0},
+    {"asm": 0, "panel": 16, "solve": 0, "pairs": 0, "duffy": 0},
+    {"asm": 0, "panel": 0, "solve": 2, "pairs": 0, "duffy": 0},
+    {"asm": 0, "panel": 0, "solve": 0, "pairs": 0, "duffy": 1},
 )
 
 
@@ -165,6 +168,8 @@ def apply_variant(lib, variant: dict) -> None:
     check(lib.hbem_set_tuning(TUNE_ASM_MINBLOCKS, int(variant.get("asm", 0))), "hbem_set_tuning", lib)
     check(lib.hbem_set_tuning(TUNE_LU_PANEL, int(variant.get("panel", 0))), "hbem_set_tuning", lib)
     check(lib.hbem_set_tuning(TUNE_LU_SOLVE, int(variant.get("solve", 0))), "hbem_set_tuning", lib)
+    check(lib.hbem_set_tuning(TUNE_ASM_PAIRS, int(variant.get("pairs", 0))), "hbem_set_tuning", lib)
+    check(lib.hbem_set_tuning(TUNE_DUFFY, int(variant.get("duffy", 0))), "hbem_set_tuning", lib)
 
 
 # ------------------------------------------------------------------ batched runner

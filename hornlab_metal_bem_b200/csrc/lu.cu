@@ -497,7 +497,9 @@ __device__ void getrs_phase(int n, const float *Ar, const float *Ai, long long l
         const int b = LOWER ? q : nblk - 1 - q;
         const int j0 = b * 32, jb = min(32, n - j0);
         for (int e = tid; e < 32 * 32; e += blockDim.x) {
-            const int r = e >> 5, c = e & 31;
+            // op = A: lanes along a factor row; op = A^T / A^H: lanes along the
+            // factor row that holds an op-column (coalesced either way)
+            const int r = TR == 0 ? (e >> 5) : (e & 31), c = TR == 0 ? (e & 31) : (e >> 5);
             float tr = 0.f, ti = 0.f;
             if (r < jb && c < jb && (LOWER ? c <= r : c >= r)) op_at<TR>(Ar, Ai, lda, j0 + r, j0 + c, tr, ti);
             t_r[r * 33 + c] = tr;
@@ -993,20 +995,37 @@ struct RcState {
     int st, j, iter, pad;
 };
 
-// ||A||_1 = max_j sum_i |a_ij| (clange '1'); thread per column.
-__global__ void k_norm1(int n, const float *a_re, const float *a_im, long long lda, long long a_stride,
-                        unsigned *out_bits) {
+// ||A||_1 = max_j sum_i |a_ij| (clange '1').  Block (32, 8): lanes over 32
+// consecutive columns (coalesced rows), 8 row groups reduced in shared memory.
+__global__ void __launch_bounds__(256) k_norm1(int n, const float *a_re, const float *a_im, long long lda,
+                                               long long a_stride, unsigned *out_bits) {
+    __shared__ double s_col[8][33];
     const int mat = blockIdx.y;
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    float v = 0.f;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int j = blockIdx.x * 32 + tx;
+    double sacc = 0.0;
     if (j < n) {
         const float *ar = a_re + (size_t)mat * a_stride + j, *ai = a_im + (size_t)mat * a_stride + j;
-        double sacc = 0.0;
-        for (int i = 0; i < n; ++i) sacc += hypot((double)ar[(size_t)i * lda], (double)ai[(size_t)i * lda]);
-        v = (float)sacc;
+        float part = 0.f;
+        int cnt = 0;
+#pragma unroll 4
+        for (int i = ty; i < n; i += 8) {
+            const float re = ar[(size_t)i * lda], im = ai[(size_t)i * lda];
+            part += sqrtf(fmaf(re, re, im * im));
+            if (++cnt == 64) { sacc += part; part = 0.f; cnt = 0; }   // FP32 runs of 64, FP64 total
+        }
+        sacc += part;
     }
-    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out_bits + mat, __float_as_uint(v));
+    s_col[ty][tx] = sacc;
+    __syncthreads();
+    if (ty == 0) {
+        double t = 0.0;
+#pragma unroll
+        for (int g = 0; g < 8; ++g) t += s_col[g][tx];
+        float v = (j < n) ? (float)t : 0.f;
+        for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (tx == 0) atomicMax(out_bits + mat, __float_as_uint(v));
+    }
 }
 
 __global__ void k_rc_init(int n, float *x_re, float *x_im, long long stride, RcState *state) {
@@ -1375,7 +1394,7 @@ int matrix_norm1(int n, int batch, const float *a_re, const float *a_im, long lo
                  float *anorm, cudaStream_t st) {
     unsigned *bits = reinterpret_cast<unsigned *>(anorm);
     HBEM_CUDA(cudaMemsetAsync(bits, 0, sizeof(unsigned) * batch, st));
-    k_norm1<<<dim3((n + 255) / 256, batch), 256, 0, st>>>(n, a_re, a_im, lda, a_stride, bits);
+    k_norm1<<<dim3((n + 31) / 32, batch), 256, 0, st>>>(n, a_re, a_im, lda, a_stride, bits);
     HBEM_LAUNCH_CHECK("k_norm1");
     return HBEM_OK;
 }

@@ -51,7 +51,7 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
-@pytest.mark.parametrize("tuning", [None, {"n<=768": CANDIDATES[3], "n<=1536": CANDIDATES[2]}, "auto"])
+@pytest.mark.parametrize("tuning", [None, {"n<=768": CANDIDATES[4], "n<=1536": CANDIDATES[2]}, "auto"])
 def test_batched_graph_sweeps_match_eager(tuning, tmp_path):
     cases = _cases()
     ref = [_eager(c) for c in cases]
