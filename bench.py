@@ -379,10 +379,11 @@ def run_b200(args, w):
     sfu_peak = N_SM * SFU_LANES_PER_SM * clk_mhz * 1e6 / SFU_PER_SAMPLE
     sfu_achieved = samples / (stage["regular_ms"] * 1e-3)
     roofline = {
-        "kernel": "k_regular (regular pair assembly, %d launch/step)" % ((F + 63) // 64),
+        "kernel": "k_regular_sym (regular pair assembly over unordered pairs, %d launch/step)" % ((F + 63) // 64),
         "bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
         "traffic": profile_traffic("k_regular", w["name"]),
-        "algorithmic": f"{samples:.3e} kernel samples/launch x {FLOPS_PER_SAMPLE:.0f} FP32 flops",
+        "algorithmic": f"{samples:.3e} ordered kernel samples/launch x {FLOPS_PER_SAMPLE:.0f} FP32 flops "
+                       "(F T^2 36 M; the kernel evaluates each unordered pair once)",
         "peak_source": f"148 SM x 128 FP32 lanes x 2 x {clk_mhz:.0f} MHz (sm_max_mhz, {peaks['source']})",
         "sfu": {"achieved_gsamples_s": sfu_achieved / 1e9, "peak_gsamples_s": sfu_peak / 1e9,
                 "frac": sfu_achieved / sfu_peak, "per_sample": "rsqrt + sin + cos (3 MUFU), 16 MUFU/clk/SM"},
