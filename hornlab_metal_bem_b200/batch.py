@@ -93,7 +93,7 @@ CANDIDATES = (
     {"asm": 0, "panel": 0, "solve": 0, "pairs": 1, "duffy": 0},
     {"asm": 3, "panel": 0, "solve": 0, "pairs": 1, "duffy": 0},
     {"asm": 0, "panel": 16, "solve": 0, "pairs": 0, "duffy": 0},
-    {"asm": 0, "panel": 0, "solve": 2, "pairs": 0, "duffy": 0},
+    {"asm": 0, "panel": 0, "solve": 1, "pairs": 0, "duffy": 0},
     {"asm": 0, "panel": 0, "solve": 0, "pairs": 0, "duffy": 1},
 )
 

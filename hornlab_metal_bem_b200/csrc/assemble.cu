@@ -784,6 +784,30 @@ __device__ __forceinline__ float refy(int l) { return l == 2 ? 1.f : 0.f; }
 
 // Map a Duffy point onto the shared edge / vertex of the image triangle
 // (main.swift:4213-4231).
+// Warp totals of NV values per lane (NV = 32, 16 or 8): after the plain
+// butterfly levels h >= NV, each transposing level h < NV halves the values a
+// lane holds, sending the half its partner keeps; lane L ends with the total
+// of value L & (NV - 1), in NV - 1 + (5 - log2 NV) NV shuffles instead of 5 NV.
+template <int NV>
+__device__ __forceinline__ double warp_transpose_reduce(double (&v)[NV]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int h = 16; h >= NV; h >>= 1)
+#pragma unroll
+        for (int i = 0; i < NV; ++i) v[i] += __shfl_xor_sync(0xffffffffu, v[i], h);
+#pragma unroll
+    for (int h = NV / 2; h >= 1; h >>= 1) {
+        const bool hi = (lane & h) != 0;
+#pragma unroll
+        for (int i = 0; i < h; ++i) {
+            const double send = hi ? v[i] : v[i + h];
+            const double keep = hi ? v[i + h] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, h);
+        }
+    }
+    return v[0];
+}
+
 __device__ __forceinline__ void remap(float x, float y, int kind, int l1, int l2, float &ox, float &oy) {
     if (kind == 2) {
         const int vc = 3 - l1 - l2;
@@ -878,54 +902,64 @@ __global__ void __launch_bounds__(256, MINB) k_duffy(const __grid_constant__ Duf
             }
         }
     };
-    // lane e < 9 keeps DLP entry e, lanes 9..11 the SLP rows: (re, im) per wavenumber, FP64
-    double own_re[NF], own_im[NF];
-    auto reduce_keep = [&](double sign) {
-#pragma unroll
-        for (int f = 0; f < NF; ++f) {
-#pragma unroll
-            for (int e = 0; e < 24; ++e) {
-                double v = (double)acc[f][e];
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                const int owner = e < 6 ? 9 + (e >> 1) : (e - 6) >> 1;
-                if (lane == owner) {
-                    if (e & 1) own_im[f] += sign * v;
-                    else own_re[f] += sign * v;
-                }
-            }
-        }
-    };
-#pragma unroll
-    for (int f = 0; f < NF; ++f) {
-        own_re[f] = own_im[f] = 0.0;
-#pragma unroll
-        for (int e = 0; e < 24; ++e) acc[f][e] = 0.f;
-    }
-    // singular (Duffy) points
-    const int ri = pr.kind - 1;
-    const int off = p.rule_off[ri], cnt = p.rule_cnt[ri];
-    for (int q = lane; q < cnt; q += 32) {
-        const float4 r = __ldg(&p.rule[off + q]);
-        const float w = __ldg(&p.rule_w[off + q]);
-        float tx_, ty_, sx_, sy_;
-        remap(r.x, r.y, pr.kind, pr.tl1, pr.tl2, tx_, ty_);
-        remap(r.z, r.w, pr.kind, pr.sl1, pr.sl2, sx_, sy_);
-        accumulate(tx_, ty_, sx_, sy_, w);
-    }
-    reduce_keep(1.0);
-    // regular 6x6 rule, subtracted; the coincident self-point is excluded by
-    // index exactly as in the regular assembly (main.swift:4323-4336)
 #pragma unroll
     for (int f = 0; f < NF; ++f)
 #pragma unroll
         for (int e = 0; e < 24; ++e) acc[f][e] = 0.f;
-    for (int q = lane; q < 36; q += 32) {
-        const int a = q / 6, b = q - 6 * (q / 6);
-        if (pr.test == pr.trial && pr.test_mask == pr.trial_mask && a == b) continue;
-        accumulate(qx(a), qy(a), qx(b), qy(b), qw(a) * qw(b));
+    // singular (Duffy) points, then the regular 6x6 rule with negated weights
+    // (the correction is singular - regular; the coincident self-point is
+    // excluded by index exactly as in the regular assembly,
+    // main.swift:4323-4336): one accumulation and one reduction per pair
+    const int ri = pr.kind - 1;
+    const int off = p.rule_off[ri], cnt = p.rule_cnt[ri];
+    const bool self_pair = pr.test == pr.trial && pr.test_mask == pr.trial_mask;
+    for (int q = lane; q < cnt + 36; q += 32) {
+        float tx_, ty_, sx_, sy_, w;
+        bool skip = false;
+        if (q < cnt) {
+            const float4 r = __ldg(&p.rule[off + q]);
+            w = __ldg(&p.rule_w[off + q]);
+            remap(r.x, r.y, pr.kind, pr.tl1, pr.tl2, tx_, ty_);
+            remap(r.z, r.w, pr.kind, pr.sl1, pr.sl2, sx_, sy_);
+        } else {
+            const int rq = q - cnt, a = rq / 6, b = rq - 6 * a;
+            tx_ = qx(a); ty_ = qy(a); sx_ = qx(b); sy_ = qy(b);
+            w = -(qw(a) * qw(b));
+            skip = self_pair && a == b;
+        }
+        if (!skip) accumulate(tx_, ty_, sx_, sy_, w);
     }
-    reduce_keep(-1.0);
+    // FP64 warp totals of the 24 NF lane partials (value v = 24 f + e): a
+    // transpose-reduce leaves value v of the first set in lane v, of the
+    // second set in lane v - S0 (and its mirror); then lane e < 9 gathers DLP
+    // entry e and lanes 9..11 the SLP rows, (re, im) per wavenumber
+    constexpr int S0 = NF == 2 ? 32 : 16, S1 = NF == 2 ? 16 : 8;
+    double red0, red1;
+    {
+        double v0[S0], v1[S1];
+#pragma unroll
+        for (int i = 0; i < S0; ++i) v0[i] = (double)acc[i / 24][i % 24];
+#pragma unroll
+        for (int i = 0; i < S1; ++i) v1[i] = (double)acc[(S0 + i) / 24][(S0 + i) % 24];
+        red0 = warp_transpose_reduce<S0>(v0);
+        red1 = warp_transpose_reduce<S1>(v1);
+    }
+    double own_re[NF], own_im[NF];
+    {
+        const int e_re = lane < 9 ? 6 + 2 * lane : (lane < 12 ? 2 * (lane - 9) : 0);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const int v = 24 * f + e_re + c;
+                const double g0 = __shfl_sync(0xffffffffu, red0, v & (S0 - 1));
+                const double g1 = __shfl_sync(0xffffffffu, red1, (v - S0) & (S1 - 1));
+                const double g = v < S0 ? g0 : g1;
+                if (c == 0) own_re[f] = g;
+                else own_im[f] = g;
+            }
+        }
+    }
     const double scale = (double)HBEM_INV4PI * (double)jac * (double)pr.weight;
     const int i_row = lane < 9 ? lane / 3 : lane - 9;
     if (p.mode == 1) {

@@ -978,6 +978,335 @@ int lu_solve_blocked(int n, int nrhs, int batch, const float *lu_re, const float
 }
 
 // ---------------------------------------------------------------------------
+// Wavefront triangular solves: one launch per triangular phase with many
+// CTAs per right-hand side.  Each CTA owns one 32-row block of op(A).  It
+// takes a ticket t = q * systems + sys from a counter (q: the block's place
+// in the phase order), so every block it waits for belongs to a CTA that
+// took an earlier ticket and is therefore resident: the wait graph has no
+// cycle and no CTA waits on one that cannot run.
+// Finished x values travel through a mailbox of 64-bit words (re, im),
+// cleared to all-ones before the phase; an x value is never all-ones (NaNs
+// are written in canonical form), so a word that is not all-ones is final,
+// and one relaxed 64-bit load both announces and delivers it: no fence, no
+// flag.  Each warp waits only for the x values it consumes, with the factor
+// entries of that block loaded before the wait.  After the last block the
+// CTA solves its diagonal triangle (warp 0 column sweep) and posts its x.
+// Waits are bounded: past the limit a warp raises the launch's abort word
+// (the other CTAs stop waiting), the CTA writes NaN into its block and sets
+// the module's fault word, which the synchronising callers report.
+// ---------------------------------------------------------------------------
+constexpr int kWaveThreads = 256;
+constexpr int kWaveSpinLimit = 1 << 22;   // polls of >= 32 ns: seconds before a wait gives up
+constexpr unsigned long long kWaveEmpty = ~0ull;
+
+struct WaveCtl {
+    int ticket[2];   // per phase
+    int abort;
+    int pad;
+};
+
+static __device__ int g_wave_fault;
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long *p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long pack_x(float re, float im) {
+    if (re != re) re = __int_as_float(0x7fc00000);
+    if (im != im) im = __int_as_float(0x7fc00000);
+    return (unsigned long long)__float_as_uint(re) | ((unsigned long long)__float_as_uint(im) << 32);
+}
+
+__device__ __forceinline__ float x_re(unsigned long long w) { return __uint_as_float((unsigned)w); }
+__device__ __forceinline__ float x_im(unsigned long long w) { return __uint_as_float((unsigned)(w >> 32)); }
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Warp-wide wait until every lane's word (need: the lane reads one) is
+// posted; returns false on abort or timeout.
+__device__ __forceinline__ bool wave_wait(const unsigned long long *addr, bool need, unsigned long long &w,
+                                          WaveCtl *ctl) {
+    w = need ? ld_relaxed_u64(addr) : 0ull;
+    if (__all_sync(0xffffffffu, w != kWaveEmpty)) return true;
+    unsigned ns = 32;
+    for (int spins = 1;; ++spins) {
+        __nanosleep(ns);
+        if (ns < 256) ns <<= 1;
+        if (w == kWaveEmpty) w = ld_relaxed_u64(addr);
+        if (__all_sync(0xffffffffu, w != kWaveEmpty)) return true;
+        if ((spins & 15) == 0 && __any_sync(0xffffffffu, *(volatile int *)&ctl->abort != 0)) return false;
+        if (spins > kWaveSpinLimit) {
+            if ((threadIdx.x & 31) == 0) {
+                atomicExch(&ctl->abort, 1);
+                atomicExch(&g_wave_fault, 1);
+            }
+            return false;
+        }
+    }
+}
+
+template <bool LOWER, bool UNIT, int TR>
+__global__ void __launch_bounds__(kWaveThreads) k_trsv_wave(int n, int nblk, int nrhs, int systems,
+                                                            const float *__restrict__ lu_re,
+                                                            const float *__restrict__ lu_im, long long lda,
+                                                            long long a_stride, float *b_re, float *b_im,
+                                                            long long ldb, long long b_stride, WaveCtl *ctl,
+                                                            int phase, unsigned long long *mbox,
+                                                            const int *active) {
+    __shared__ float s_tr[32 * 33], s_ti[32 * 33];
+    __shared__ float s_pr[8][33], s_pi[8][33];
+    __shared__ int s_ticket, s_abort;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) {
+        s_ticket = atomicAdd(&ctl->ticket[phase], 1);
+        s_abort = 0;
+    }
+    __syncthreads();
+    const int t = s_ticket;
+    const int q = t / systems, sys = t - q * systems;
+    if (q >= nblk) return;
+    if (active && active[sys / nrhs] == 0) return;   // the whole system is skipped; nobody waits on it
+    const int mat = sys / nrhs, rhs = sys - mat * nrhs;
+    const float *Ar = lu_re + (size_t)mat * a_stride, *Ai = lu_im + (size_t)mat * a_stride;
+    float *xr = b_re + (size_t)mat * b_stride + rhs, *xi = b_im + (size_t)mat * b_stride + rhs;
+    unsigned long long *mb = mbox + (size_t)sys * n;
+    const int b = LOWER ? q : nblk - 1 - q;
+    const int j0 = b * 32, jb = min(32, n - j0);
+
+    // this block's right-hand side (no other CTA writes it in this phase)
+    float rb_r = 0.f, rb_i = 0.f;
+    if (warp == 0 && lane < jb) {
+        rb_r = xr[(size_t)(j0 + lane) * ldb];
+        rb_i = xi[(size_t)(j0 + lane) * ldb];
+    }
+    // diagonal triangle of op(A) (lanes along a factor row for every op)
+    for (int e = tid; e < 32 * 32; e += kWaveThreads) {
+        const int r = TR == 0 ? (e >> 5) : (e & 31), c = TR == 0 ? (e & 31) : (e >> 5);
+        float tr = 0.f, ti = 0.f;
+        if (r < jb && c < jb && (LOWER ? c <= r : c >= r)) op_at<TR>(Ar, Ai, lda, j0 + r, j0 + c, tr, ti);
+        s_tr[r * 33 + c] = tr;
+        s_ti[r * 33 + c] = ti;
+    }
+
+    // op = A: warp w holds rows w + 8k of the block, lanes over the columns of
+    // a finished block; op = A^T / A^H: warp w takes factor rows w + 8k of a
+    // finished block, lane i accumulates op-row i of this block
+    const float cs = TR == 2 ? -1.f : 1.f;
+    auto load_a = [&](int qc, float (&pr)[4], float (&pi)[4]) {
+        const int c0 = (LOWER ? qc : nblk - 1 - qc) * 32;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (TR == 0) {
+                const int col = c0 + lane, r = warp + 8 * k;
+                const bool ok = col < n && r < jb;
+                pr[k] = ok ? __ldg(Ar + (size_t)(j0 + r) * lda + col) : 0.f;
+                pi[k] = ok ? __ldg(Ai + (size_t)(j0 + r) * lda + col) : 0.f;
+            } else {
+                const int jr = c0 + warp + 8 * k;
+                const bool ok = jr < n && lane < jb;
+                pr[k] = ok ? __ldg(Ar + (size_t)jr * lda + j0 + lane) : 0.f;
+                pi[k] = ok ? cs * __ldg(Ai + (size_t)jr * lda + j0 + lane) : 0.f;
+            }
+        }
+    };
+    float accr[4] = {0.f, 0.f, 0.f, 0.f}, acci[4] = {0.f, 0.f, 0.f, 0.f};
+    float nr[4], ni[4];   // factor entries of block qc, loaded before its x is waited for
+    bool aborted = false;
+    if (q > 0) load_a(0, nr, ni);
+    for (int qc = 0; qc < q; ++qc) {
+        const int c0 = (LOWER ? qc : nblk - 1 - qc) * 32;
+        // op = A: lane l needs x[c0 + l]; op = A^T / A^H: lane k < 4 fetches x[c0 + w + 8k]
+        const int xi_idx = TR == 0 ? c0 + lane : c0 + warp + 8 * lane;
+        const bool need = TR == 0 ? xi_idx < n : (lane < 4 && xi_idx < n);
+        unsigned long long w;
+        if (!wave_wait(mb + (need ? xi_idx : 0), need, w, ctl)) {
+            aborted = true;
+            break;
+        }
+        float pr[4], pi[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) { pr[k] = nr[k]; pi[k] = ni[k]; }
+        if (qc + 1 < q) load_a(qc + 1, nr, ni);
+        if (TR == 0) {
+            const float x_r = x_re(w), x_i = x_im(w);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                accr[k] = fmaf(pr[k], x_r, fmaf(-pi[k], x_i, accr[k]));
+                acci[k] = fmaf(pr[k], x_i, fmaf(pi[k], x_r, acci[k]));
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const unsigned long long wk = __shfl_sync(0xffffffffu, w, k);
+                const float x_r = x_re(wk), x_i = x_im(wk);
+                accr[k] = fmaf(pr[k], x_r, fmaf(-pi[k], x_i, accr[k]));
+                acci[k] = fmaf(pr[k], x_i, fmaf(pi[k], x_r, acci[k]));
+            }
+        }
+    }
+    if (aborted && lane == 0) s_abort = 1;
+    // per-row sums of the finished blocks' contributions
+    if (TR == 0) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float vr = warp_sum(accr[k]), vi = warp_sum(acci[k]);
+            if (lane == 0) { s_pr[0][warp + 8 * k] = vr; s_pi[0][warp + 8 * k] = vi; }
+        }
+    } else {
+        s_pr[warp][lane] = (accr[0] + accr[1]) + (accr[2] + accr[3]);
+        s_pi[warp][lane] = (acci[0] + acci[1]) + (acci[2] + acci[3]);
+    }
+    __syncthreads();
+    if (warp != 0) return;
+    float sr, si;
+    if (TR == 0) {
+        sr = s_pr[0][lane];
+        si = s_pi[0][lane];
+    } else {
+        sr = 0.f;
+        si = 0.f;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) { sr += s_pr[w][lane]; si += s_pi[w][lane]; }
+    }
+    float vr = rb_r - sr, vi = rb_i - si;
+    // the lane's own diagonal entry and 1 / |d|^2, ahead of the sweep
+    float dr = 1.f, di = 0.f, den = 1.f;
+    if (!UNIT && lane < jb) {
+        dr = s_tr[lane * 33 + lane];
+        di = s_ti[lane * 33 + lane];
+        den = 1.0f / (dr * dr + di * di);
+    }
+    // column sweep: lane i holds x_i; step j finalises x_j
+#pragma unroll
+    for (int s = 0; s < 32; ++s) {
+        if (s < jb) {
+            const int j = LOWER ? s : jb - 1 - s;
+            if (!UNIT && lane == j) {
+                const float yr = vr, yi = vi;
+                vr = (yr * dr + yi * di) * den;
+                vi = (yi * dr - yr * di) * den;
+            }
+            const float jr = __shfl_sync(0xffffffffu, vr, j), ji = __shfl_sync(0xffffffffu, vi, j);
+            if (LOWER ? lane > j : lane < j) {
+                const float lr = s_tr[lane * 33 + j], li = s_ti[lane * 33 + j];
+                vr -= lr * jr - li * ji;
+                vi -= lr * ji + li * jr;
+            }
+        }
+    }
+    if (s_abort) { vr = __int_as_float(0x7fc00000); vi = vr; }
+    if (lane < jb) {
+        st_relaxed_u64(mb + j0 + lane, pack_x(vr, vi));
+        xr[(size_t)(j0 + lane) * ldb] = vr;
+        xi[(size_t)(j0 + lane) * ldb] = vi;
+    }
+}
+
+template <bool REVERSE>
+__global__ void __launch_bounds__(kTrsvThreads) k_trsv_permute(int n, int nrhs, const int *piv, long long piv_stride,
+                                                               float *b_re, float *b_im, long long ldb,
+                                                               long long b_stride, const int *active) {
+    extern __shared__ float s_x[];
+    const int mat = blockIdx.y, rhs = blockIdx.x;
+    if (active && active[mat] == 0) return;
+    float *xr = b_re + (size_t)mat * b_stride + rhs, *xi = b_im + (size_t)mat * b_stride + rhs;
+    trsv_permute<REVERSE>(n, piv + (size_t)mat * piv_stride, xr, xi, ldb, s_x, s_x + n);
+}
+
+// control block, then one mailbox of n words per system for each phase
+size_t wave_scratch_bytes(long long systems, int n) {
+    return sizeof(WaveCtl) + 2 * sizeof(unsigned long long) * (size_t)systems * (size_t)n;
+}
+
+template <bool LOWER, bool UNIT, int TR>
+int launch_wave(int n, int nrhs, int batch, const float *lu_re, const float *lu_im, long long lda,
+                long long a_stride, float *b_re, float *b_im, long long ldb, long long b_stride, WaveCtl *ctl,
+                int phase, unsigned long long *mbox, const int *active, cudaStream_t st) {
+    const int nblk = (n + 31) / 32;
+    const int systems = nrhs * batch;
+    k_trsv_wave<LOWER, UNIT, TR><<<(unsigned)((long long)nblk * systems), kWaveThreads, 0, st>>>(
+        n, nblk, nrhs, systems, lu_re, lu_im, lda, a_stride, b_re, b_im, ldb, b_stride, ctl, phase, mbox, active);
+    HBEM_LAUNCH_CHECK("k_trsv_wave");
+    return HBEM_OK;
+}
+
+// Both phases of a solve.  `scratch` (wave_scratch_bytes(nrhs * batch, n),
+// 16-byte aligned) may be given by the caller; else it is taken from the
+// stream's pool.  `active` (per matrix, optional) skips matrices.
+int lu_solve_wave(int n, int nrhs, int batch, const float *lu_re, const float *lu_im, long long lda,
+                  long long a_stride, const int *piv, long long piv_stride, float *b_re, float *b_im, long long ldb,
+                  long long b_stride, int trans, const int *active, void *scratch, cudaStream_t st) {
+    const long long systems = (long long)nrhs * batch;
+    if ((long long)((n + 31) / 32) * systems >= (1LL << 31)) return fail(HBEM_ERR_ARG, "hbem_lu_solve: too many blocks");
+    static bool attr = false;
+    if (!attr) {
+        HBEM_CUDA(cudaFuncSetAttribute(k_trsv_permute<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        HBEM_CUDA(cudaFuncSetAttribute(k_trsv_permute<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        attr = true;
+    }
+    const size_t bytes = wave_scratch_bytes(systems, n);
+    void *mem = scratch;
+    if (!mem) HBEM_CUDA(cudaMallocAsync(&mem, bytes, st));
+    auto done = [&](int rc) {
+        if (!scratch) cudaFreeAsync(mem, st);
+        return rc;
+    };
+    WaveCtl *ctl = static_cast<WaveCtl *>(mem);
+    unsigned long long *mb0 = reinterpret_cast<unsigned long long *>(ctl + 1), *mb1 = mb0 + systems * n;
+    cudaError_t e = cudaMemsetAsync(ctl, 0, sizeof(WaveCtl), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(mb0, 0xff, bytes - sizeof(WaveCtl), st);
+    if (e != cudaSuccess) return done(cuda_fail(e, "hbem_lu_solve: scratch"));
+    const size_t psmem = (size_t)n * 2 * sizeof(float);
+    int rc = HBEM_OK;
+    if (trans == HBEM_TRANS_N) {
+        if (piv) {
+            k_trsv_permute<false><<<dim3(nrhs, batch), kTrsvThreads, psmem, st>>>(n, nrhs, piv, piv_stride, b_re, b_im,
+                                                                                 ldb, b_stride, active);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return done(cuda_fail(e, "k_trsv_permute"));
+            count_launch();
+        }
+        rc = launch_wave<true, true, 0>(n, nrhs, batch, lu_re, lu_im, lda, a_stride, b_re, b_im, ldb, b_stride, ctl,
+                                        0, mb0, active, st);
+        if (rc == HBEM_OK)
+            rc = launch_wave<false, false, 0>(n, nrhs, batch, lu_re, lu_im, lda, a_stride, b_re, b_im, ldb, b_stride,
+                                              ctl, 1, mb1, active, st);
+        return done(rc);
+    }
+    if (trans == HBEM_TRANS_T) {
+        rc = launch_wave<true, false, 1>(n, nrhs, batch, lu_re, lu_im, lda, a_stride, b_re, b_im, ldb, b_stride, ctl,
+                                         0, mb0, active, st);
+        if (rc == HBEM_OK)
+            rc = launch_wave<false, true, 1>(n, nrhs, batch, lu_re, lu_im, lda, a_stride, b_re, b_im, ldb, b_stride,
+                                             ctl, 1, mb1, active, st);
+    } else {
+        rc = launch_wave<true, false, 2>(n, nrhs, batch, lu_re, lu_im, lda, a_stride, b_re, b_im, ldb, b_stride, ctl,
+                                         0, mb0, active, st);
+        if (rc == HBEM_OK)
+            rc = launch_wave<false, true, 2>(n, nrhs, batch, lu_re, lu_im, lda, a_stride, b_re, b_im, ldb, b_stride,
+                                             ctl, 1, mb1, active, st);
+    }
+    if (rc == HBEM_OK && piv) {
+        k_trsv_permute<true><<<dim3(nrhs, batch), kTrsvThreads, psmem, st>>>(n, nrhs, piv, piv_stride, b_re, b_im, ldb,
+                                                                            b_stride, active);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return done(cuda_fail(e, "k_trsv_permute"));
+        count_launch();
+    }
+    return done(rc);
+}
+
+// ---------------------------------------------------------------------------
 // 1-norm condition estimate of the factored matrices, as LAPACK cgecon with
 // norm '1' (the reference's estimateReciprocalCondition, main.swift:463-503,
 // 7898): Hager's method in Higham's formulation (LAPACK CLACN2) on L U
@@ -1041,12 +1370,15 @@ __global__ void k_rc_init(int n, float *x_re, float *x_im, long long stride, RcS
     }
 }
 
-// w = x for the matrices in `want` states (w is solved in place next)
+// w = x for the matrices in `want` states (w is solved in place next);
+// active[mat] marks them for the solve
 __global__ void k_rc_copy(int n, const float *x_re, const float *x_im, float *w_re, float *w_im, long long stride,
-                          const RcState *state, int want_lo, int want_hi) {
+                          const RcState *state, int want_lo, int want_hi, int *active) {
     const int mat = blockIdx.y;
     const int st = state[mat].st;
-    if (st < want_lo || st > want_hi) return;
+    const bool want = st >= want_lo && st <= want_hi;
+    if (blockIdx.x == 0 && threadIdx.x == 0) active[mat] = want ? 1 : 0;
+    if (!want) return;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         w_re[(size_t)mat * stride + i] = x_re[(size_t)mat * stride + i];
         w_im[(size_t)mat * stride + i] = x_im[(size_t)mat * stride + i];
@@ -1343,22 +1675,46 @@ int lu_solve_single(int n, int nrhs, int batch, const float *lu_re, const float 
                     long long a_stride, const int *piv, long long piv_stride, float *b_re, float *b_im, long long ldb,
                     long long b_stride, int trans, cudaStream_t st);
 
-// piv == nullptr solves with L U itself (no interchanges).
+// piv == nullptr solves with L U itself (no interchanges).  `active` (per
+// matrix, optional) lets the wavefront solve skip matrices; `wave_scratch`
+// (wave_scratch_bytes(nrhs * batch, n), optional) is its control block and
+// mailboxes.
+int lu_solve_ex(int n, int nrhs, int batch, const float *lu_re, const float *lu_im, long long lda, long long a_stride,
+                const int *piv, long long piv_stride, float *b_re, float *b_im, long long ldb, long long b_stride,
+                int trans, const int *active, void *wave_scratch, cudaStream_t st) {
+    const size_t smem = (size_t)n * 2 * sizeof(float);
+    if (smem > 200 * 1024) return fail(HBEM_ERR_ARG, "hbem_lu_solve: n too large for the staged solve");
+    // one CTA per right-hand side for small n; the wavefront solve otherwise
+    // (the blocked block steps remain selectable)
+    const int solve_mode = tuning(HBEM_TUNE_LU_SOLVE);
+    if (solve_mode == 1 || (solve_mode == 0 && n <= kTB))
+        return lu_solve_single(n, nrhs, batch, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re, b_im, ldb, b_stride,
+                               trans, st);
+    if (solve_mode == 2)
+        return lu_solve_blocked(n, nrhs, batch, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re, b_im, ldb, b_stride,
+                                trans, st);
+    return lu_solve_wave(n, nrhs, batch, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re, b_im, ldb, b_stride, trans,
+                         active, wave_scratch, st);
+}
+
 int lu_solve(int n, int nrhs, int batch, const float *lu_re, const float *lu_im, long long lda, long long a_stride,
              const int *piv, long long piv_stride, float *b_re, float *b_im, long long ldb, long long b_stride,
              int trans, cudaStream_t st) {
-    const size_t smem = (size_t)n * 2 * sizeof(float);
-    if (smem > 200 * 1024) return fail(HBEM_ERR_ARG, "hbem_lu_solve: n too large for the staged solve");
-    // one CTA per right-hand side when there are enough of them to fill the GPU
-    // (or n is small); the blocked multi-CTA steps otherwise
-    const int solve_mode = tuning(HBEM_TUNE_LU_SOLVE);
-    const long long ctas = (long long)nrhs * batch;
-    const bool single = solve_mode == 1 || (solve_mode == 0 && (n <= kTB || (n <= 6144 && ctas >= 24)));
-    if (!single)
-        return lu_solve_blocked(n, nrhs, batch, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re, b_im, ldb, b_stride,
-                                trans, st);
-    return lu_solve_single(n, nrhs, batch, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re, b_im, ldb, b_stride,
-                           trans, st);
+    return lu_solve_ex(n, nrhs, batch, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re, b_im, ldb, b_stride, trans,
+                       nullptr, nullptr, st);
+}
+
+// Reports (and clears) a timed-out wavefront wait; synchronises the stream.
+int wave_fault_check(cudaStream_t st) {
+    int h = 0;
+    cudaError_t e = cudaMemcpyFromSymbolAsync(&h, g_wave_fault, sizeof(int), 0, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "triangular solve status");
+    if (h == 0) return HBEM_OK;
+    const int zero = 0;
+    cudaMemcpyToSymbolAsync(g_wave_fault, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, st);
+    cudaStreamSynchronize(st);
+    return fail(HBEM_ERR_STATE, "triangular solve: a wait for an earlier block timed out (its results are NaN)");
 }
 
 int lu_solve_single(int n, int nrhs, int batch, const float *lu_re, const float *lu_im, long long lda,
@@ -1404,12 +1760,15 @@ int lu_rcond(int n, int batch, const float *lu_re, const float *lu_im, long long
     constexpr int kItMax = 5;
     float *x = nullptr, *w = nullptr;
     RcState *state = nullptr;
-    int *pending = nullptr;
+    int *pending = nullptr, *active = nullptr;
+    void *wave = nullptr;
     const long long stride = n;
     HBEM_CUDA(cudaMallocAsync((void **)&x, sizeof(float) * 2 * (size_t)batch * n, st));
     HBEM_CUDA(cudaMallocAsync((void **)&w, sizeof(float) * 2 * (size_t)batch * n, st));
     HBEM_CUDA(cudaMallocAsync((void **)&state, sizeof(RcState) * batch, st));
     HBEM_CUDA(cudaMallocAsync((void **)&pending, sizeof(int), st));
+    HBEM_CUDA(cudaMallocAsync((void **)&active, sizeof(int) * batch, st));
+    HBEM_CUDA(cudaMallocAsync(&wave, wave_scratch_bytes(batch, n), st));
     float *xr = x, *xi = x + (size_t)batch * n, *wr = w, *wi = w + (size_t)batch * n;
     const dim3 gv((n + 255) / 256 < 64 ? (n + 255) / 256 : 64, batch);
     int rc = HBEM_OK;
@@ -1419,25 +1778,29 @@ int lu_rcond(int n, int batch, const float *lu_re, const float *lu_im, long long
         count_launch();
         return true;
     };
+    // solves for the matrices k_rc_copy marked active
+    auto solve = [&](int trans) {
+        return lu_solve_ex(n, 1, batch, lu_re, lu_im, lda, a_stride, nullptr, n, wr, wi, 1, stride, trans, active, wave,
+                           st);
+    };
     k_rc_init<<<gv, 256, 0, st>>>(n, xr, xi, stride, state);
     // round 0: (LU) w = x for every matrix
     if (launched("k_rc_init")) {
-        k_rc_copy<<<gv, 256, 0, st>>>(n, xr, xi, wr, wi, stride, state, 0, 3);
-        if (launched("k_rc_copy")) rc = lu_solve(n, 1, batch, lu_re, lu_im, lda, a_stride, nullptr, n, wr, wi, 1,
-                                                         stride, HBEM_TRANS_N, st);
+        k_rc_copy<<<gv, 256, 0, st>>>(n, xr, xi, wr, wi, stride, state, 0, 3, active);
+        if (launched("k_rc_copy")) rc = solve(HBEM_TRANS_N);
         if (rc == HBEM_OK) { k_rc_after_a<<<batch, 256, 0, st>>>(n, xr, xi, wr, wi, stride, state); launched("k_rc_after_a"); }
     }
     for (int round = 0; round < 2 * kItMax + 2 && rc == HBEM_OK; ++round) {
         // (LU)^H solves for matrices in state 1, then (LU) solves for states 2 and 3
-        k_rc_copy<<<gv, 256, 0, st>>>(n, xr, xi, wr, wi, stride, state, 1, 1);
+        k_rc_copy<<<gv, 256, 0, st>>>(n, xr, xi, wr, wi, stride, state, 1, 1, active);
         if (!launched("k_rc_copy")) break;
-        rc = lu_solve(n, 1, batch, lu_re, lu_im, lda, a_stride, nullptr, n, wr, wi, 1, stride, HBEM_TRANS_C, st);
+        rc = solve(HBEM_TRANS_C);
         if (rc != HBEM_OK) break;
         k_rc_after_h<<<batch, 256, 0, st>>>(n, xr, xi, wr, wi, stride, state, kItMax);
         if (!launched("k_rc_after_h")) break;
-        k_rc_copy<<<gv, 256, 0, st>>>(n, xr, xi, wr, wi, stride, state, 2, 3);
+        k_rc_copy<<<gv, 256, 0, st>>>(n, xr, xi, wr, wi, stride, state, 2, 3, active);
         if (!launched("k_rc_copy")) break;
-        rc = lu_solve(n, 1, batch, lu_re, lu_im, lda, a_stride, nullptr, n, wr, wi, 1, stride, HBEM_TRANS_N, st);
+        rc = solve(HBEM_TRANS_N);
         if (rc != HBEM_OK) break;
         k_rc_after_a<<<batch, 256, 0, st>>>(n, xr, xi, wr, wi, stride, state);
         if (!launched("k_rc_after_a")) break;
@@ -1453,10 +1816,13 @@ int lu_rcond(int n, int batch, const float *lu_re, const float *lu_im, long long
         if (e != cudaSuccess) { rc = cuda_fail(e, "rcond sync"); break; }
         if (h == 0) break;
     }
+    if (rc == HBEM_OK) rc = wave_fault_check(st);
     cudaFreeAsync(x, st);
     cudaFreeAsync(w, st);
     cudaFreeAsync(state, st);
     cudaFreeAsync(pending, st);
+    cudaFreeAsync(active, st);
+    cudaFreeAsync(wave, st);
     return rc;
 }
 
@@ -1496,7 +1862,8 @@ int refine(int n, int batch, const float *a_re, const float *a_im, long long lda
         if (!any) break;
         e = cudaMemcpyAsync(active, h_active.data(), sizeof(int) * batch, cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess) { rc = cuda_fail(e, "refine copy"); break; }
-        rc = lu_solve(n, 1, batch, lu_re, lu_im, lda, lu_stride, piv, piv_stride, dr, di, 1, x_stride, HBEM_TRANS_N, st);
+        rc = lu_solve_ex(n, 1, batch, lu_re, lu_im, lda, lu_stride, piv, piv_stride, dr, di, 1, x_stride, HBEM_TRANS_N,
+                         active, nullptr, st);
         if (rc != HBEM_OK) break;
         k_axpy_active<<<dim3((n + 255) / 256, batch), 256, 0, st>>>(n, x_re, x_im, x_stride, dr, di, active);
         e = cudaGetLastError();
@@ -1509,6 +1876,7 @@ int refine(int n, int batch, const float *a_re, const float *a_im, long long lda
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) rc = cuda_fail(e, "refine results");
     }
+    if (rc == HBEM_OK) rc = wave_fault_check(st);
     cudaFreeAsync(d, st);
     cudaFreeAsync(norms, st);
     cudaFreeAsync(active, st);
@@ -1517,13 +1885,15 @@ int refine(int n, int batch, const float *a_re, const float *a_im, long long lda
 
 // ---------------------------------------------------------------------------
 // Refinement without allocation.  The scratch of hbem_refine (correction
-// vectors, FP64 norm accumulators, active flags) lives in one fixed
+// vectors, FP64 norm accumulators, active flags, the wavefront solve's
+// control block and mailboxes) lives in one fixed
 // module-scope device array instead of stream-ordered allocations, for
 // callers that may not allocate device memory: a process whose memory is
 // held by another caching allocator (a cudaMallocAsync from the default pool
 // can then fail although the host framework has room cached), or a hot loop
 // that must never enter an allocator.  Sizes: batch <= kNoAllocMaxBatch and
-// batch * x_stride <= kNoAllocMaxElems complex elements (4 MiB of vectors).
+// batch * x_stride <= kNoAllocMaxElems complex elements (4 MiB of vectors,
+// 8 MiB of mailboxes).
 // Every call, on any stream or thread, shares this one array per device, so
 // calls must not overlap; the array keeps the last call's contents, and the
 // norms are cleared by each pass before they accumulate.
@@ -1533,7 +1903,9 @@ constexpr int kNoAllocMaxBatch = 256;
 constexpr size_t kNoAllocVecBytes = sizeof(float) * (size_t)kNoAllocMaxElems;  // one of re / im
 constexpr size_t kNoAllocNormOff = 2 * kNoAllocVecBytes;
 constexpr size_t kNoAllocActiveOff = kNoAllocNormOff + sizeof(double) * 2 * kNoAllocMaxBatch;
-constexpr size_t kNoAllocBytes = kNoAllocActiveOff + sizeof(int) * kNoAllocMaxBatch;
+constexpr size_t kNoAllocWaveOff = kNoAllocActiveOff + sizeof(int) * kNoAllocMaxBatch;   // 16-byte aligned
+constexpr size_t kNoAllocBytes = kNoAllocWaveOff + sizeof(WaveCtl) + 2 * sizeof(unsigned long long) * kNoAllocMaxElems;
+static_assert(kNoAllocWaveOff % 16 == 0, "wave control block alignment");
 
 static __device__ __align__(256) unsigned char g_refine_scratch[kNoAllocBytes];
 
@@ -1575,6 +1947,7 @@ int refine_noalloc(int n, int batch, const float *a_re, const float *a_im, long 
     float *di = reinterpret_cast<float *>(base + kNoAllocVecBytes);
     double *norms = reinterpret_cast<double *>(base + kNoAllocNormOff);
     int *active = reinterpret_cast<int *>(base + kNoAllocActiveOff);
+    void *wave = base + kNoAllocWaveOff;
     double h_norms[2 * kNoAllocMaxBatch];
     int h_active[kNoAllocMaxBatch], h_iters[kNoAllocMaxBatch];
     double h_res[kNoAllocMaxBatch];
@@ -1604,7 +1977,8 @@ int refine_noalloc(int n, int batch, const float *a_re, const float *a_im, long 
         if (!any) break;
         e = cudaMemcpyAsync(active, h_active, sizeof(int) * batch, cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess) { rc = cuda_fail(e, "hbem_refine_noalloc: copy"); break; }
-        rc = lu_solve(n, 1, batch, lu_re, lu_im, lda, lu_stride, piv, piv_stride, dr, di, 1, x_stride, HBEM_TRANS_N, st);
+        rc = lu_solve_ex(n, 1, batch, lu_re, lu_im, lda, lu_stride, piv, piv_stride, dr, di, 1, x_stride, HBEM_TRANS_N,
+                         active, wave, st);
         if (rc != HBEM_OK) break;
         k_axpy_active<<<dim3((n + 255) / 256, batch), 256, 0, st>>>(n, x_re, x_im, x_stride, dr, di, active);
         e = cudaGetLastError();
@@ -1617,6 +1991,7 @@ int refine_noalloc(int n, int batch, const float *a_re, const float *a_im, long 
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) rc = cuda_fail(e, "hbem_refine_noalloc: results");
     }
+    if (rc == HBEM_OK) rc = wave_fault_check(st);
     return rc;
 }
 

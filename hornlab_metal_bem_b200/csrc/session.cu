@@ -318,7 +318,7 @@ extern "C" int hbem_set_tuning(int key, int value) {
             if (value != 0 && value != 16 && value != 32) return fail(HBEM_ERR_ARG, "HBEM_TUNE_LU_PANEL: 0, 16 or 32");
             break;
         case HBEM_TUNE_LU_SOLVE:
-            if (value < 0 || value > 2) return fail(HBEM_ERR_ARG, "HBEM_TUNE_LU_SOLVE: 0, 1 or 2");
+            if (value < 0 || value > 3) return fail(HBEM_ERR_ARG, "HBEM_TUNE_LU_SOLVE: 0, 1, 2 or 3");
             break;
         case HBEM_TUNE_ASM_PAIRS:
             if (value < 0 || value > 1) return fail(HBEM_ERR_ARG, "HBEM_TUNE_ASM_PAIRS: 0 or 1");

@@ -28,6 +28,7 @@ int refine(int n, int batch, const float *a_re, const float *a_im, long long lda
            const float *lu_re, const float *lu_im, long long lu_stride, const int *piv, long long piv_stride,
            const float *b_re, const float *b_im, long long b_stride, float *x_re, float *x_im, long long x_stride,
            double tol, int max_iter, int *iters, double *resid, cudaStream_t st);
+int wave_fault_check(cudaStream_t st);
 int launch_field(Session &s, int n_freq, const float *k_re, const float *p_re, const float *p_im, long long p_stride,
                  const float *q_re, const float *q_im, long long q_stride, const float *obs, int n_obs, float *out_re,
                  float *out_im, long long out_stride, cudaStream_t st);
@@ -219,6 +220,9 @@ extern "C" int hbem_solve_batch(hbem_session *h, int n_freq, const float *k_re, 
         cudaEventRecord(ev[0], st);
         cudaStreamSynchronize(st);
         cudaEventElapsedTime(&t_total, ev[4], ev[0]);
+        rc = wave_fault_check(st);
+    }
+    if (rc == HBEM_OK) {
         if (!do_refine) {
             if (refine_iters) std::memset(refine_iters, 0, sizeof(int) * n_freq);
             if (refine_resid) std::memset(refine_resid, 0, sizeof(double) * n_freq);

@@ -89,7 +89,9 @@ long long hbem_launch_count(void);
  *                            (2: 128 registers, 3: 80 registers)
  *   HBEM_TUNE_LU_PANEL:      inner sub-panel width of the LU (16 or 32)
  *   HBEM_TUNE_LU_SOLVE:      triangular solves (1: one CTA per right-hand
- *                            side, 2: blocked multi-CTA steps)
+ *                            side, 2: blocked multi-CTA steps, 3: wavefront,
+ *                            one CTA per 32-row block; 0: one CTA per
+ *                            right-hand side for n <= 128, else wavefront)
  *   HBEM_TUNE_ASM_PAIRS:     regular assembly (0: unordered pairs, both
  *                            orders from one kernel evaluation; 1: ordered
  *                            pairs, two wavenumbers per evaluation)
@@ -200,7 +202,7 @@ int hbem_lu_rcond(int n, int batch, const float *lu_re, const float *lu_im, long
  * For callers that may not allocate device memory, such as a process whose
  * device memory is held by another caching allocator (a stream-ordered
  * allocation inside hbem_refine can then fail), or a loop that must never
- * enter an allocator.  Its scratch is one fixed device array of 4 MiB per
+ * enter an allocator.  Its scratch is one fixed device array of 12 MiB per
  * device, in this library's module.  Limits: batch <= 256 and
  * batch * x_stride <= 524288 complex elements; larger calls return
  * HBEM_ERR_ARG.  The first call on each device looks the array up (and may

@@ -177,6 +177,33 @@ def test_lu_solve_matches_lapack(n):
         assert rel(x[m], ref) < 1e-5
 
 
+@pytest.mark.parametrize("trans", [0, 2])
+def test_wavefront_solve_many_matrices(trans):
+    """More 32-row blocks than resident CTAs (40 matrices of n = 1043): the wavefront solve against LAPACK
+    and against the one-CTA-per-right-hand-side scheme."""
+    lib = load_library()
+    n, batch = 1043, 40
+    A, b = _lu_case(n, batch, 5)
+    Ar, Ai = _dev(A)
+    piv, info = _factor(Ar, Ai, n, batch)
+    assert int(info.abs().sum()) == 0
+    out = {}
+    for mode in (3, 1):
+        Br, Bi = _dev(b[:, :, None])
+        assert lib.hbem_set_tuning(2, mode) == 0
+        try:
+            _solve(Ar, Ai, piv, Br, Bi, n, 1, batch, trans)
+        finally:
+            lib.hbem_set_tuning(2, 0)
+        out[mode] = _host(Br, Bi)[:, :, 0]
+    assert np.isfinite(out[3]).all()
+    assert rel(out[3], out[1]) < 1e-5
+    for m in (0, 17, 39):
+        op = A[m] if trans == 0 else A[m].conj().T
+        ref = np.linalg.solve(op.astype(np.complex128), b[m].astype(np.complex128))
+        assert rel(out[3][m], ref) < 1e-5
+
+
 @pytest.mark.parametrize("n", [1800, 3300, 6500])
 def test_lu_tall_panels_match_lapack(n):
     """Sizes whose sub-panels spread over 2-, 4- and 8-CTA clusters, two right-hand sides."""
@@ -213,11 +240,11 @@ def test_transposed_solves(trans, n):
         assert rel(X[m], ref) < 1e-5
 
 
-@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("mode", [1, 2, 3])
 @pytest.mark.parametrize("trans", [0, 1, 2])
 @pytest.mark.parametrize("n", [33, 130, 700])
 def test_solve_schemes_match_lapack(n, trans, mode):
-    """Both solve schemes (1: one CTA per right-hand side, 2: blocked multi-CTA steps) for A, A^T, A^H."""
+    """Every solve scheme (1: one CTA per right-hand side, 2: blocked multi-CTA steps, 3: wavefront) for A, A^T, A^H."""
     lib = load_library()
     batch, nrhs = 2, 3
     A, _ = _lu_case(n, batch, 900 + n)
