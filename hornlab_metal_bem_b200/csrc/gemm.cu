@@ -3,8 +3,8 @@
 // block's trailing matrix.
 //
 // CUDA-core path: 64 x 64 complex output tile per 256-thread CTA, 4 x 4
-// complex outputs per thread, L and U tiles staged in shared memory with
-// 128-bit broadcast reads; FP32 FMA gives the exact-FP32 products of
+// complex outputs per thread, L and U chunks staged in shared memory by
+// double-buffered cp.async and read with 128-bit broadcast loads; FP32 FMA gives the exact-FP32 products of
 // LAPACK cgemm-based cgetrf.
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -19,13 +19,24 @@ namespace hbem {
 struct TcWorkspace;
 namespace {
 
+// 4-byte asynchronous copy global -> shared; src_bytes 0 writes a zero
+__device__ __forceinline__ void cp_async4(float *dst, const float *src, int src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(
+                     static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+                 "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+
 // C[start:n, start:col_end] -= L[start:n, k0:k0+kw] * U[k0:k0+kw, start:col_end]
-// with kw a multiple of 16; K is consumed in 16-wide shared-memory chunks.
+// (kw a multiple of 16) for one 64 x 64 complex tile per CTA, K in chunks of
+// 16 double-buffered through cp.async (the next chunk's loads
+// are in flight while the current one is multiplied); 4 x 4 complex
+// accumulators per thread.
 __global__ void __launch_bounds__(256) k_trailing_simt(float *a_re, float *a_im, long long lda, long long a_stride,
                                                        int n, int k0, int kw, int start, int col_end) {
     constexpr int KC = 16;
-    __shared__ __align__(16) float Lr[KC][64], Li[KC][64];
-    __shared__ __align__(16) float Ur[KC][64], Ui[KC][64];
+    __shared__ __align__(16) float Lr[2][KC][64], Li[2][KC][64];
+    __shared__ __align__(16) float Ur[2][KC][64], Ui[2][KC][64];
     const int mat = blockIdx.z;
     float *are = a_re + (size_t)mat * a_stride, *aim = a_im + (size_t)mat * a_stride;
     const int row0 = start + blockIdx.y * 64, col0 = start + blockIdx.x * 64;
@@ -36,36 +47,41 @@ __global__ void __launch_bounds__(256) k_trailing_simt(float *a_re, float *a_im,
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) cr[i][j] = ci[i][j] = 0.f;
-    for (int kc = 0; kc < kw; kc += KC) {
+    auto load_chunk = [&](int kc, int sbuf) {
         for (int e = tid; e < 64 * KC; e += 256) {
             const int r = e / KC, kk = e - r * KC;
             const int gr = row0 + r;
-            float vr = 0.f, vi = 0.f;
-            if (gr < n) {
-                vr = are[(size_t)gr * lda + k0 + kc + kk];
-                vi = aim[(size_t)gr * lda + k0 + kc + kk];
-            }
-            Lr[kk][r] = vr;
-            Li[kk][r] = vi;
+            const bool ok = gr < n;
+            const size_t off = ok ? (size_t)gr * lda + k0 + kc + kk : 0;
+            cp_async4(&Lr[sbuf][kk][r], are + off, ok ? 4 : 0);
+            cp_async4(&Li[sbuf][kk][r], aim + off, ok ? 4 : 0);
         }
         for (int e = tid; e < 64 * KC; e += 256) {
             const int kk = e / 64, c = e - kk * 64;
             const int gc = col0 + c;
-            float vr = 0.f, vi = 0.f;
-            if (gc < col_end) {
-                vr = are[(size_t)(k0 + kc + kk) * lda + gc];
-                vi = aim[(size_t)(k0 + kc + kk) * lda + gc];
-            }
-            Ur[kk][c] = vr;
-            Ui[kk][c] = vi;
+            const bool ok = gc < col_end;
+            const size_t off = ok ? (size_t)(k0 + kc + kk) * lda + gc : 0;
+            cp_async4(&Ur[sbuf][kk][c], are + off, ok ? 4 : 0);
+            cp_async4(&Ui[sbuf][kk][c], aim + off, ok ? 4 : 0);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    load_chunk(0, 0);
+    int sbuf = 0;
+    for (int kc = 0; kc < kw; kc += KC) {
+        if (kc + KC < kw) {
+            load_chunk(kc + KC, sbuf ^ 1);
+            asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         }
         __syncthreads();
 #pragma unroll
         for (int kk = 0; kk < KC; ++kk) {
-            const float4 lr = *reinterpret_cast<const float4 *>(&Lr[kk][ty * 4]);
-            const float4 li = *reinterpret_cast<const float4 *>(&Li[kk][ty * 4]);
-            const float4 ur = *reinterpret_cast<const float4 *>(&Ur[kk][tx * 4]);
-            const float4 ui = *reinterpret_cast<const float4 *>(&Ui[kk][tx * 4]);
+            const float4 lr = *reinterpret_cast<const float4 *>(&Lr[sbuf][kk][ty * 4]);
+            const float4 li = *reinterpret_cast<const float4 *>(&Li[sbuf][kk][ty * 4]);
+            const float4 ur = *reinterpret_cast<const float4 *>(&Ur[sbuf][kk][tx * 4]);
+            const float4 ui = *reinterpret_cast<const float4 *>(&Ui[sbuf][kk][tx * 4]);
             const float a_r[4] = {lr.x, lr.y, lr.z, lr.w}, a_i[4] = {li.x, li.y, li.z, li.w};
             const float b_r[4] = {ur.x, ur.y, ur.z, ur.w}, b_i[4] = {ui.x, ui.y, ui.z, ui.w};
 #pragma unroll
@@ -79,6 +95,7 @@ __global__ void __launch_bounds__(256) k_trailing_simt(float *a_re, float *a_im,
                 }
         }
         __syncthreads();
+        sbuf ^= 1;
     }
 #pragma unroll
     for (int i = 0; i < 4; ++i) {

@@ -176,6 +176,128 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(float *a_re, float *a_i
     if (tid == 0 && first_zero && info[b] == 0) info[b] = first_zero;
 }
 
+// Panel factorisation in one CTA's shared memory (pitch nb + 1), thread per
+// row.  Per column j, two barrier-separated phases:
+//   P (warp 0): reduce the per-warp argmax candidates of column j (first
+//               index on ties, as icamax), swap rows j <-> p, publish the
+//               pivot row;
+//   E (threads over rows > j): scale the row's column-j entry by 1/pivot,
+//               apply the rank-1 update to its columns > j and take the
+//               argmax candidate of column j + 1 from the updated row.
+// The arithmetic of every element is that of k_panel; the fused scaling,
+// update and pivot search save one barrier and a pass per column, and a
+// thread's columns are independent (rows at pitch nb + 1 keep consecutive
+// threads on distinct banks).
+__device__ __forceinline__ void argmax_warp(float &v, int &idx) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float ov = __shfl_xor_sync(0xffffffffu, v, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+        if (ov > v || (ov == v && oi < idx)) { v = ov; idx = oi; }
+    }
+}
+
+__global__ void __launch_bounds__(kPanelThreads) k_panel_rows(float *a_re, float *a_im, long long lda,
+                                                              long long a_stride, int n, int k0, int nb, int *piv,
+                                                              long long piv_stride, int *info) {
+    extern __shared__ float s_panel[];
+    __shared__ float s_v[kPanelThreads / 32];
+    __shared__ int s_i[kPanelThreads / 32];
+    __shared__ float s_pr[32], s_pi[32];
+    const int b = blockIdx.x;
+    int *pv = piv + (size_t)b * piv_stride;
+    const int m = n - k0;
+    const int P = nb + 1;
+    float *pre = s_panel, *pim = s_panel + m * P;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    float *gre = a_re + (size_t)b * a_stride + (size_t)k0 * lda + k0;
+    float *gim = a_im + (size_t)b * a_stride + (size_t)k0 * lda + k0;
+    for (int e = tid; e < m * nb; e += blockDim.x) {
+        const int r = e / nb, j = e - r * nb;
+        pre[r * P + j] = gre[(size_t)r * lda + j];
+        pim[r * P + j] = gim[(size_t)r * lda + j];
+    }
+    __syncthreads();
+    float v = -1.f;
+    int idx = 0x7fffffff;
+    for (int r = tid; r < m; r += blockDim.x) {
+        const float c = cabs1(pre[r * P], pim[r * P]);
+        if (c > v) { v = c; idx = r; }
+    }
+    argmax_warp(v, idx);
+    if (lane == 0) { s_v[warp] = v; s_i[warp] = idx; }
+    __syncthreads();
+    int first_zero = 0;
+    for (int j = 0; j < nb; ++j) {
+        // ---- phase P
+        if (warp == 0) {
+            float bv = lane < nw ? s_v[lane] : -1.f;
+            int p = lane < nw ? s_i[lane] : 0x7fffffff;
+            argmax_warp(bv, p);
+            if (p >= m) p = j;  // column of NaNs: keep the diagonal, as icamax does
+            if (lane < nb) {
+                const int c = lane;
+                const float jr = pre[j * P + c], ji = pim[j * P + c];
+                const float pr = pre[p * P + c], pi = pim[p * P + c];
+                s_pr[c] = pr;
+                s_pi[c] = pi;
+                pre[j * P + c] = pr;
+                pim[j * P + c] = pi;
+                if (p != j) {
+                    pre[p * P + c] = jr;
+                    pim[p * P + c] = ji;
+                }
+                if (c == 0) pv[k0 + j] = k0 + p;
+            }
+        }
+        __syncthreads();
+        const float dr = s_pr[j], di = s_pi[j];
+        const bool zero = (dr == 0.f && di == 0.f);
+        float ir = 0.f, ii = 0.f;
+        if (zero) {
+            if (first_zero == 0) first_zero = k0 + j + 1;
+        } else {
+            const float den = 1.0f / (dr * dr + di * di);
+            ir = dr * den;
+            ii = -di * den;
+        }
+        // ---- phase E
+        v = -1.f;
+        idx = 0x7fffffff;
+        const bool next = j + 1 < nb;
+        for (int r = j + 1 + tid; r < m; r += blockDim.x) {
+            const int o = r * P;
+            const float xr = pre[o + j], xi = pim[o + j];
+            const float lr = xr * ir - xi * ii, li = xr * ii + xi * ir;
+            pre[o + j] = lr;
+            pim[o + j] = li;
+            if (!zero) {
+#pragma unroll 4
+                for (int c = j + 1; c < nb; ++c) {
+                    const float ur = s_pr[c], ui = s_pi[c];
+                    pre[o + c] -= lr * ur - li * ui;
+                    pim[o + c] -= lr * ui + li * ur;
+                }
+            }
+            if (next) {
+                const float a = cabs1(pre[o + j + 1], pim[o + j + 1]);
+                if (a > v) { v = a; idx = r; }
+            }
+        }
+        if (next) {
+            argmax_warp(v, idx);
+            if (lane == 0) { s_v[warp] = v; s_i[warp] = idx; }
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < m * nb; e += blockDim.x) {
+        const int r = e / nb, j = e - r * nb;
+        gre[(size_t)r * lda + j] = pre[r * P + j];
+        gim[(size_t)r * lda + j] = pim[r * P + j];
+    }
+    if (tid == 0 && first_zero && info[b] == 0) info[b] = first_zero;
+}
+
 // Panel factorisation across a thread-block cluster, for panels too tall for
 // one CTA's shared memory.  CTA q of the cluster owns panel rows
 // [q R, (q+1) R) in its shared memory (pitch nb + 1).  Per column j:
@@ -368,16 +490,18 @@ __global__ void __launch_bounds__(kSwapThreads) k_swap_trsm(float *a_re, float *
         s_col[tid] = tid < ncols ? col : -1;
     }
     if (tid < 128) s_row[tid] = tid < np ? k0 + tid : -1;
+    __shared__ int s_pv[64];
+    if (tid < np) s_pv[tid] = pv[k0 + tid];
     __syncthreads();
     if (tid < np) {
-        const int p = pv[k0 + tid];
+        const int p = s_pv[tid];
         int slot;
         if (p < k0 + np) {
             slot = p - k0;
         } else {
             int first = tid;
             for (int j = 0; j < tid; ++j)
-                if (pv[k0 + j] == p) { first = j; break; }
+                if (s_pv[j] == p) { first = j; break; }
             slot = np + first;
             if (first == tid) s_row[slot] = p;
         }
@@ -413,9 +537,19 @@ __global__ void __launch_bounds__(kSwapThreads) k_swap_trsm(float *a_re, float *
                 Xi[sl * XP + c] = ti;
             }
         }
-        if (s_col[c] >= trsm_lo) {
-            for (int q0 = 0; q0 < np; q0 += 16) {
-                const int qn = min(16, np - q0);
+    }
+    // TRSM X[0:np] = L11^-1 X[0:np] on the columns >= trsm_lo, in 16-row
+    // blocks: row group 0 (threads 0..63, one per column) solves the block's
+    // diagonal triangle in registers, then the four row groups update the
+    // rows below it (row r by group r mod 4)
+    if (any_trsm) {
+        static_assert(kSwapCols == 64 && kSwapThreads == 256, "64 columns x 4 row groups");
+        const int c = tid & 63, rg = tid >> 6;
+        const bool col_on = c < ncols && s_col[c] >= trsm_lo;
+        for (int q0 = 0; q0 < np; q0 += 16) {
+            const int qn = min(16, np - q0);
+            __syncthreads();
+            if (rg == 0 && col_on) {
                 float xr[16], xi[16];
 #pragma unroll
                 for (int i = 0; i < 16; ++i)
@@ -437,7 +571,14 @@ __global__ void __launch_bounds__(kSwapThreads) k_swap_trsm(float *a_re, float *
 #pragma unroll
                 for (int i = 0; i < 16; ++i)
                     if (i < qn) { Xr[(q0 + i) * XP + c] = xr[i]; Xi[(q0 + i) * XP + c] = xi[i]; }
-                for (int r = q0 + qn; r < np; ++r) {
+            }
+            __syncthreads();
+            if (col_on && q0 + qn < np) {
+                float xr[16], xi[16];
+#pragma unroll
+                for (int i = 0; i < 16; ++i)
+                    if (i < qn) { xr[i] = Xr[(q0 + i) * XP + c]; xi[i] = Xi[(q0 + i) * XP + c]; }
+                for (int r = q0 + qn + rg; r < np; r += 4) {
                     float sr = Xr[r * XP + c], si = Xi[r * XP + c];
 #pragma unroll
                     for (int j = 0; j < 16; ++j)
@@ -1622,7 +1763,7 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
         }
         return rc;
     };
-    HBEM_CUDA(cudaFuncSetAttribute(k_panel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+    HBEM_CUDA(cudaFuncSetAttribute(k_panel_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
     HBEM_CUDA(cudaFuncSetAttribute(k_swap_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSwapSmem));
     for (int b0 = 0; b0 < n; b0 += NB) {
         const int bw = std::min(NB, n - b0);
@@ -1634,8 +1775,9 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
             const int w = std::min(nbi, b0 + bw - c);
             const size_t psmem = (size_t)(n - c) * (w + 1) * 8;
             if (psmem <= smem_cap) {
-                k_panel<true><<<batch, kPanelThreads, psmem, st>>>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info);
-                HBEM_LAUNCH_CHECK("k_panel");
+                k_panel_rows<<<batch, kPanelThreads, psmem, st>>>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride,
+                                                                  info);
+                HBEM_LAUNCH_CHECK("k_panel_rows");
             } else if ((size_t)(n - c) <= 8 * (smem_cap / ((size_t)(w + 1) * 8))) {
                 int rc = launch_panel_cluster(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info, batch, smem_cap, st);
                 if (rc != HBEM_OK) return finish(rc);
