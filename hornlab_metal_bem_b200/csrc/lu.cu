@@ -165,6 +165,9 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(float *a_re, float *a_i
         __syncthreads();
     }
     if (SMEM) {
+        // the last column was scaled by the R pass, thread per row; the
+        // write-back maps elements to threads differently
+        __syncthreads();
         float *gre = a_re + (size_t)b * a_stride + (size_t)k0 * lda + k0;
         float *gim = a_im + (size_t)b * a_stride + (size_t)k0 * lda + k0;
         for (int e = tid; e < m * nb; e += blockDim.x) {
@@ -440,6 +443,9 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(kPanelThreads)
         }
         __syncthreads();
     }
+    // the last column was scaled by the R pass above, thread per row; the
+    // write-back maps elements to threads differently
+    __syncthreads();
     {
         float *gre = a_re + (size_t)b * a_stride + (size_t)(k0 + r0) * lda + k0;
         float *gim = a_im + (size_t)b * a_stride + (size_t)(k0 + r0) * lda + k0;

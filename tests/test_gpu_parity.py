@@ -204,6 +204,40 @@ def test_wavefront_solve_many_matrices(trans):
         assert rel(out[3][m], ref) < 1e-5
 
 
+def test_lu_bitwise_stable_under_concurrent_work():
+    """The factorisation of matrices whose first panels span 2-CTA clusters (n = 1043) must not depend on
+    what else runs on the GPU: a matrix-multiply load on another stream changes CTA timing, which once
+    exposed a missing barrier between a panel's last scaling pass and its write-back."""
+    n, batch = 1043, 40
+    A, _ = _lu_case(n, batch, 17)
+    A0r, A0i = _dev(A)
+    side = torch.cuda.Stream()
+    X = torch.randn(4096, 4096, device="cuda")
+    runs = []
+    for noisy in (False, True, True, True):
+        Ar, Ai = A0r.clone(), A0i.clone()
+        torch.cuda.synchronize()
+        if noisy:
+            with torch.cuda.stream(side):
+                for _ in range(60):
+                    X @ X
+        piv, info = _factor(Ar, Ai, n, batch)
+        torch.cuda.synchronize()
+        runs.append((Ar, Ai, piv, info))
+    assert int(runs[0][3].abs().sum()) == 0
+    for r in runs[1:]:
+        assert all(torch.equal(x, y) for x, y in zip(runs[0][:3], r[:3]))
+    # and the factors are right: P A = L U for one matrix
+    LU = _host(runs[0][0], runs[0][1])[5]
+    pv = runs[0][2][5].cpu().numpy()
+    PA = A[5].astype(np.complex128).copy()
+    for k in range(n):
+        if pv[k] != k:
+            PA[[k, pv[k]]] = PA[[pv[k], k]]
+    L = np.tril(LU, -1) + np.eye(n)
+    assert rel(L @ np.triu(LU), PA) < 1e-5
+
+
 @pytest.mark.parametrize("n", [1800, 3300, 6500])
 def test_lu_tall_panels_match_lapack(n):
     """Sizes whose sub-panels spread over 2-, 4- and 8-CTA clusters, two right-hand sides."""
