@@ -27,19 +27,21 @@ __device__ __forceinline__ void cp_async4(float *dst, const float *src, int src_
                  : "memory");
 }
 
-// C[start:n, start:col_end] -= L[start:n, k0:k0+kw] * U[k0:k0+kw, start:col_end]
+// C[start:n, col_start:col_end] -= L[start:n, k0:k0+kw] * U[k0:k0+kw, col_start:col_end]
 // (kw a multiple of 16) for one 64 x 64 complex tile per CTA, K in chunks of
 // 16 double-buffered through cp.async (the next chunk's loads
 // are in flight while the current one is multiplied); 4 x 4 complex
-// accumulators per thread.
+// accumulators per thread.  L is stored transposed ([k][row]) with the row
+// index XOR-swizzled by k, so the coalesced row-segment loads do not all
+// land on one bank.
 __global__ void __launch_bounds__(256) k_trailing_simt(float *a_re, float *a_im, long long lda, long long a_stride,
-                                                       int n, int k0, int kw, int start, int col_end) {
+                                                       int n, int k0, int kw, int start, int col_start, int col_end) {
     constexpr int KC = 16;
     __shared__ __align__(16) float Lr[2][KC][64], Li[2][KC][64];
     __shared__ __align__(16) float Ur[2][KC][64], Ui[2][KC][64];
     const int mat = blockIdx.z;
     float *are = a_re + (size_t)mat * a_stride, *aim = a_im + (size_t)mat * a_stride;
-    const int row0 = start + blockIdx.y * 64, col0 = start + blockIdx.x * 64;
+    const int row0 = start + blockIdx.y * 64, col0 = col_start + blockIdx.x * 64;
     const int tid = threadIdx.x;
     const int tx = tid & 15, ty = tid >> 4;
     float cr[4][4], ci[4][4];
@@ -53,8 +55,9 @@ __global__ void __launch_bounds__(256) k_trailing_simt(float *a_re, float *a_im,
             const int gr = row0 + r;
             const bool ok = gr < n;
             const size_t off = ok ? (size_t)gr * lda + k0 + kc + kk : 0;
-            cp_async4(&Lr[sbuf][kk][r], are + off, ok ? 4 : 0);
-            cp_async4(&Li[sbuf][kk][r], aim + off, ok ? 4 : 0);
+            const int rs = r ^ ((kk & 7) << 2);   // 16 k of one row on 8 banks instead of 1
+            cp_async4(&Lr[sbuf][kk][rs], are + off, ok ? 4 : 0);
+            cp_async4(&Li[sbuf][kk][rs], aim + off, ok ? 4 : 0);
         }
         for (int e = tid; e < 64 * KC; e += 256) {
             const int kk = e / 64, c = e - kk * 64;
@@ -78,8 +81,9 @@ __global__ void __launch_bounds__(256) k_trailing_simt(float *a_re, float *a_im,
         __syncthreads();
 #pragma unroll
         for (int kk = 0; kk < KC; ++kk) {
-            const float4 lr = *reinterpret_cast<const float4 *>(&Lr[sbuf][kk][ty * 4]);
-            const float4 li = *reinterpret_cast<const float4 *>(&Li[sbuf][kk][ty * 4]);
+            const int lo = (ty * 4) ^ ((kk & 7) << 2);   // XOR of a multiple of 4 keeps the float4 whole
+            const float4 lr = *reinterpret_cast<const float4 *>(&Lr[sbuf][kk][lo]);
+            const float4 li = *reinterpret_cast<const float4 *>(&Li[sbuf][kk][lo]);
             const float4 ur = *reinterpret_cast<const float4 *>(&Ur[sbuf][kk][tx * 4]);
             const float4 ui = *reinterpret_cast<const float4 *>(&Ui[sbuf][kk][tx * 4]);
             const float a_r[4] = {lr.x, lr.y, lr.z, lr.w}, a_i[4] = {li.x, li.y, li.z, li.w};
@@ -126,6 +130,18 @@ __global__ void __launch_bounds__(256) k_trailing_simt(float *a_re, float *a_im,
 int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int col_end, float *a_re, float *a_im,
                        long long lda, long long a_stride, int *status, cudaStream_t st);
 
+// A[start:n, col_start:col_end] -= L[start:n, k0:k0+kw] U[k0:k0+kw, col_start:col_end] on the CUDA cores
+int launch_trailing_simt(int n, int batch, int k0, int kw, int start, int col_start, int col_end, float *a_re,
+                         float *a_im, long long lda, long long a_stride, cudaStream_t st) {
+    const int m = n - start, w = col_end - col_start;
+    if (m <= 0 || w <= 0) return HBEM_OK;
+    if (kw % 16) return fail(HBEM_ERR_ARG, "trailing update: K must be a multiple of 16");
+    dim3 grid((w + 63) / 64, (m + 63) / 64, batch);
+    k_trailing_simt<<<grid, 256, 0, st>>>(a_re, a_im, lda, a_stride, n, k0, kw, start, col_start, col_end);
+    HBEM_LAUNCH_CHECK("k_trailing_simt");
+    return HBEM_OK;
+}
+
 int launch_trailing_update(int n, int batch, int k0, int kw, int start, int col_end, float *a_re, float *a_im,
                            long long lda, long long a_stride, TcWorkspace *tc, int *status, cudaStream_t st) {
     const int m = n - start, w = col_end - start;
@@ -133,10 +149,7 @@ int launch_trailing_update(int n, int batch, int k0, int kw, int start, int col_
     if (kw % 16) return fail(HBEM_ERR_ARG, "trailing update: K must be a multiple of 16");
     if (tc && kw == 64 && status)
         return launch_trailing_tc(tc, n, batch, k0, start, col_end, a_re, a_im, lda, a_stride, status, st);
-    dim3 grid((w + 63) / 64, (m + 63) / 64, batch);
-    k_trailing_simt<<<grid, 256, 0, st>>>(a_re, a_im, lda, a_stride, n, k0, kw, start, col_end);
-    HBEM_LAUNCH_CHECK("k_trailing_simt");
-    return HBEM_OK;
+    return launch_trailing_simt(n, batch, k0, kw, start, start, col_end, a_re, a_im, lda, a_stride, st);
 }
 
 }  // namespace hbem

@@ -25,6 +25,7 @@
 #include <mutex>
 #include <cmath>
 #include <string>
+#include <vector>
 
 #include "hbem_internal.h"
 
@@ -36,6 +37,8 @@ int tc_workspace_create(int n, int batch, TcWorkspace **out, cudaStream_t st);
 void tc_workspace_destroy(TcWorkspace *w, cudaStream_t st);
 int launch_trailing_update(int n, int batch, int k0, int kw, int start, int col_end, float *a_re, float *a_im,
                            long long lda, long long a_stride, TcWorkspace *tc, int *status, cudaStream_t st);
+int launch_trailing_simt(int n, int batch, int k0, int kw, int start, int col_start, int col_end, float *a_re,
+                         float *a_im, long long lda, long long a_stride, cudaStream_t st);
 
 namespace {
 
@@ -1732,12 +1735,60 @@ int launch_panel_cluster(float *a_re, float *a_im, long long lda, long long a_st
     return launch_panel_cluster_t<8>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info, batch, R, smem, st);
 }
 
+// Look-ahead streams of one caller stream: the factorisation chain runs on a
+// high-priority stream, the bulk of each trailing update on a low-priority
+// one; both fork from and join back into the caller's stream (so a CUDA
+// graph capture of the caller's stream takes them in).  Created on first use
+// per (device, caller stream) and kept for the process.
+struct LookaheadStreams {
+    int device;
+    cudaStream_t key, chain, bulk;
+    cudaEvent_t fork, join_chain, join_bulk, split[2], bulk_done[2];
+};
+
+static std::mutex g_la_mu;
+static std::vector<LookaheadStreams *> g_la;
+
+static int lookahead_streams(cudaStream_t key, LookaheadStreams **out) {
+    int dev = 0;
+    HBEM_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(g_la_mu);
+    for (auto *l : g_la)
+        if (l->device == dev && l->key == key) {
+            *out = l;
+            return HBEM_OK;
+        }
+    int least = 0, greatest = 0;
+    HBEM_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    auto *l = new LookaheadStreams{};
+    l->device = dev;
+    l->key = key;
+    cudaError_t e = cudaStreamCreateWithPriority(&l->chain, cudaStreamNonBlocking, greatest);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&l->bulk, cudaStreamNonBlocking, least);
+    cudaEvent_t *evs[] = {&l->fork, &l->join_chain, &l->join_bulk, &l->split[0], &l->split[1], &l->bulk_done[0],
+                          &l->bulk_done[1]};
+    for (auto *ev : evs)
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        delete l;   // handles created before the failure are left to the process
+        return cuda_fail(e, "hbem_lu_factor: look-ahead streams");
+    }
+    g_la.push_back(l);
+    *out = l;
+    return HBEM_OK;
+}
+
 int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long long a_stride, int *piv,
               long long piv_stride, int *info, int precision, cudaStream_t st) {
     // Two-level blocking: 64-column blocks whose (n - b0) x 64 panel is
     // factored by inner sub-panels (32 wide when the sub-panel fits shared
     // memory, else 16) with updates confined to the block's columns; then one
     // row-swap pass, a 64-row TRSM and a K = 64 trailing update per block.
+    // Plain precision with look-ahead: the trailing update of block b is cut
+    // into the next block's 64 columns (on the chain, so block b+1's panels
+    // can start) and the rest (on the bulk stream, overlapping block b+1's
+    // panels, which touch only block b+1's columns); block b+1's row swaps,
+    // which touch every other column, wait for it.
     const size_t smem_cap = 200 * 1024;
     constexpr int NB = 64;
     HBEM_CUDA(cudaMemsetAsync(info, 0, sizeof(int) * batch, st));
@@ -1754,7 +1805,25 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
             return rc;
         }
     }
+    LookaheadStreams *la = nullptr;
+    if (!tc && n > 2 * NB && tuning(HBEM_TUNE_LU_LOOKAHEAD) != 1) {
+        int rc = lookahead_streams(st, &la);
+        if (rc != HBEM_OK) return rc;
+        HBEM_CUDA(cudaEventRecord(la->fork, st));
+        HBEM_CUDA(cudaStreamWaitEvent(la->chain, la->fork, 0));
+        HBEM_CUDA(cudaStreamWaitEvent(la->bulk, la->fork, 0));
+    }
+    cudaStream_t cs = la ? la->chain : st;   // the factorisation chain
+    bool bulk_pending = false;
+    int parity = 0;
     auto finish = [&](int rc) -> int {
+        if (la) {
+            // join both streams back into the caller's stream, also on errors
+            cudaEventRecord(la->join_chain, la->chain);
+            cudaEventRecord(la->join_bulk, la->bulk);
+            cudaStreamWaitEvent(st, la->join_chain, 0);
+            cudaStreamWaitEvent(st, la->join_bulk, 0);
+        }
         tc_workspace_destroy(tc, st);
         if (status) {
             int h = 0;
@@ -1769,6 +1838,15 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
         }
         return rc;
     };
+    auto launched = [&](const char *what) -> int {
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(e, what);
+        count_launch();
+        return HBEM_OK;
+    };
+    auto stream_call = [&](cudaError_t e, const char *what) -> int {
+        return e == cudaSuccess ? HBEM_OK : cuda_fail(e, what);
+    };
     HBEM_CUDA(cudaFuncSetAttribute(k_panel_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
     HBEM_CUDA(cudaFuncSetAttribute(k_swap_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSwapSmem));
     for (int b0 = 0; b0 < n; b0 += NB) {
@@ -1780,40 +1858,66 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
         for (int c = b0; c < b0 + bw; c += nbi) {
             const int w = std::min(nbi, b0 + bw - c);
             const size_t psmem = (size_t)(n - c) * (w + 1) * 8;
+            int rc = HBEM_OK;
             if (psmem <= smem_cap) {
-                k_panel_rows<<<batch, kPanelThreads, psmem, st>>>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride,
+                k_panel_rows<<<batch, kPanelThreads, psmem, cs>>>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride,
                                                                   info);
-                HBEM_LAUNCH_CHECK("k_panel_rows");
+                rc = launched("k_panel_rows");
             } else if ((size_t)(n - c) <= 8 * (smem_cap / ((size_t)(w + 1) * 8))) {
-                int rc = launch_panel_cluster(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info, batch, smem_cap, st);
-                if (rc != HBEM_OK) return finish(rc);
+                rc = launch_panel_cluster(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info, batch, smem_cap, cs);
             } else {
-                k_panel<false><<<batch, kPanelThreads, 0, st>>>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info);
-                HBEM_LAUNCH_CHECK("k_panel");
+                k_panel<false><<<batch, kPanelThreads, 0, cs>>>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info);
+                rc = launched("k_panel");
             }
+            if (rc != HBEM_OK) return finish(rc);
             const int other = bw - w;  // block columns outside this sub-panel
             if (other > 0) {
                 dim3 grid((other + kSwapCols - 1) / kSwapCols, batch);
-                k_swap_trsm<<<grid, kSwapThreads, kSwapSmem, st>>>(a_re, a_im, lda, a_stride, c, w, b0, b0 + bw, c,
+                k_swap_trsm<<<grid, kSwapThreads, kSwapSmem, cs>>>(a_re, a_im, lda, a_stride, c, w, b0, b0 + bw, c,
                                                                    c + w, piv, piv_stride);
-                HBEM_LAUNCH_CHECK("k_swap_trsm");
-            }
-            if (c + w < b0 + bw) {
-                int rc = launch_trailing_update(n, batch, c, w, c + w, b0 + bw, a_re, a_im, lda, a_stride, nullptr,
-                                                nullptr, st);
+                rc = launched("k_swap_trsm");
                 if (rc != HBEM_OK) return finish(rc);
             }
+            if (c + w < b0 + bw) {
+                rc = launch_trailing_update(n, batch, c, w, c + w, b0 + bw, a_re, a_im, lda, a_stride, nullptr,
+                                            nullptr, cs);
+                if (rc != HBEM_OK) return finish(rc);
+            }
+        }
+        if (bulk_pending) {
+            // the row swaps below touch the columns of the previous bulk update
+            int rc = stream_call(cudaStreamWaitEvent(cs, la->bulk_done[parity ^ 1], 0), "look-ahead join");
+            if (rc != HBEM_OK) return finish(rc);
+            bulk_pending = false;
         }
         const int outside = n - bw;
         if (outside > 0) {
             dim3 grid((outside + kSwapCols - 1) / kSwapCols, batch);
-            k_swap_trsm<<<grid, kSwapThreads, kSwapSmem, st>>>(a_re, a_im, lda, a_stride, b0, bw, 0, n, b0, b0 + bw,
+            k_swap_trsm<<<grid, kSwapThreads, kSwapSmem, cs>>>(a_re, a_im, lda, a_stride, b0, bw, 0, n, b0, b0 + bw,
                                                                piv, piv_stride);
-            HBEM_LAUNCH_CHECK("k_swap_trsm");
+            int rc = launched("k_swap_trsm");
+            if (rc != HBEM_OK) return finish(rc);
         }
         if (b0 + bw < n) {
-            int rc = launch_trailing_update(n, batch, b0, bw, b0 + bw, n, a_re, a_im, lda, a_stride, tc, status, st);
-            if (rc != HBEM_OK) return finish(rc);
+            int rc;
+            const int next_end = std::min(n, b0 + bw + NB);
+            if (la && next_end < n) {
+                rc = launch_trailing_simt(n, batch, b0, bw, b0 + bw, b0 + bw, next_end, a_re, a_im, lda, a_stride, cs);
+                if (rc == HBEM_OK) rc = stream_call(cudaEventRecord(la->split[parity], cs), "look-ahead fork");
+                if (rc == HBEM_OK)
+                    rc = stream_call(cudaStreamWaitEvent(la->bulk, la->split[parity], 0), "look-ahead fork");
+                if (rc == HBEM_OK)
+                    rc = launch_trailing_simt(n, batch, b0, bw, b0 + bw, next_end, n, a_re, a_im, lda, a_stride,
+                                              la->bulk);
+                if (rc == HBEM_OK)
+                    rc = stream_call(cudaEventRecord(la->bulk_done[parity], la->bulk), "look-ahead fork");
+                if (rc != HBEM_OK) return finish(rc);
+                bulk_pending = true;
+                parity ^= 1;
+            } else {
+                rc = launch_trailing_update(n, batch, b0, bw, b0 + bw, n, a_re, a_im, lda, a_stride, tc, status, cs);
+                if (rc != HBEM_OK) return finish(rc);
+            }
         }
     }
     return finish(HBEM_OK);

@@ -238,6 +238,26 @@ def test_lu_bitwise_stable_under_concurrent_work():
     assert rel(L @ np.triu(LU), PA) < 1e-5
 
 
+@pytest.mark.parametrize("n,batch", [(1043, 12), (2100, 3)])
+def test_lu_lookahead_equals_one_stream(n, batch):
+    """The look-ahead schedule (next block updated on the chain, the rest of the trailing update overlapping the
+    next panels on a second stream) does the same arithmetic in the same order: bit-identical factors."""
+    lib = load_library()
+    A, _ = _lu_case(n, batch, 23)
+    out = []
+    for mode in (1, 0, 0):
+        Ar, Ai = _dev(A)
+        assert lib.hbem_set_tuning(5, mode) == 0
+        try:
+            piv, info = _factor(Ar, Ai, n, batch)
+        finally:
+            lib.hbem_set_tuning(5, 0)
+        torch.cuda.synchronize()
+        out.append((Ar, Ai, piv))
+    for r in out[1:]:
+        assert all(torch.equal(x, y) for x, y in zip(out[0], r))
+
+
 @pytest.mark.parametrize("n", [1800, 3300, 6500])
 def test_lu_tall_panels_match_lapack(n):
     """Sizes whose sub-panels spread over 2-, 4- and 8-CTA clusters, two right-hand sides."""
