@@ -152,6 +152,40 @@ __device__ __forceinline__ void sample_nf(float dx, float dy, float dz, float nx
     }
 }
 
+// sample_nf with the quadrature weight folded into the geometric factors
+// (D and G come out multiplied by wgt; the phase and 1/r of E are unscaled).
+template <int NF, bool CK>
+__device__ __forceinline__ void sample_nf_w(float dx, float dy, float dz, float nx, float ny, float nz,
+                                            const float (&k)[NF], const float (&kt)[NF], const float (&ki)[NF],
+                                            float wgt, float (&dre)[NF], float (&dim)[NF], float (&gre)[NF],
+                                            float (&gim)[NF]) {
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    float u = rsqrtf(r2);
+    u = r2 > 1.0e-14f ? u : 0.0f;
+    const float r = r2 * u;
+    const float dn = fmaf(dx, nx, fmaf(dy, ny, dz * nz));
+    const float h = dn * (u * u) * wgt, uw = u * wgt;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+        float t = r * kt[f];
+        t -= round_fma(t);
+        float sn, cs;
+        __sincosf(t * 6.28318530717958647692f, &sn, &cs);
+        float hh = h, uu = uw, fre = u;
+        if (CK) {
+            const float damp = __expf(-ki[f] * r);
+            hh *= damp;
+            uu *= damp;
+            fre += ki[f];
+        }
+        // D = hh (c + i s)(-fre + i k)
+        dre[f] = -hh * fmaf(cs, fre, sn * k[f]);
+        dim[f] = hh * fmaf(cs, k[f], -sn * fre);
+        gre[f] = uu * cs;
+        gim[f] = uu * sn;
+    }
+}
+
 template <int SYM, int NF, bool CK, bool NEED_G>
 __device__ __forceinline__ void pair_block(const float4 *__restrict__ tq, const float4 *__restrict__ sp, float nx,
                                            float ny, float nz, bool self, const float (&k)[NF],
@@ -860,6 +894,19 @@ __global__ void __launch_bounds__(256, MINB) k_duffy(const __grid_constant__ Duf
     const bool tswap = __popc(pr.test_mask) & 1, sswap = __popc(pr.trial_mask) & 1;
     const float nx = ssx * p.normals[pr.trial], ny = ssy * p.normals[T + pr.trial], nz = ssz * p.normals[2 * T + pr.trial];
     const float jac = (2.f * p.areas[pr.test]) * (2.f * p.areas[pr.trial]);
+    // the image triangles as vertex 0 plus edge vectors: a point is x0 + t1 e1 + t2 e2
+    {
+        const float tsg[3] = {tsx, tsy, tsz}, ssg[3] = {ssx, ssy, ssz};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            P[1][c] = tsg[c] * (P[1][c] - P[0][c]);
+            P[2][c] = tsg[c] * (P[2][c] - P[0][c]);
+            P[0][c] = tsg[c] * P[0][c];
+            S[1][c] = ssg[c] * (S[1][c] - S[0][c]);
+            S[2][c] = ssg[c] * (S[2][c] - S[0][c]);
+            S[0][c] = ssg[c] * S[0][c];
+        }
+    }
     float k[NF], kt[NF], ki[NF];
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
@@ -869,38 +916,62 @@ __global__ void __launch_bounds__(256, MINB) k_duffy(const __grid_constant__ Duf
         ki[f] = p.ki[ff];
     }
 
+    // Lane partials as moments over the barycentrics (t0 = s0 = 1, t1, t2, s1,
+    // s2): acc[f][0..5] = sum G t_a (a = 0, 1, 2; re, im), acc[f][6 + 2 (3a + b)]
+    // = sum D t_a s_b; turned into the P1 entries (tb = 1 - t1 - t2, t1, t2)
+    // in FP64 before the warp reduction.
     float acc[NF][24];
     auto accumulate = [&](float txi, float teta, float sxi, float seta, float w) {
         if (tswap) { const float t = txi; txi = teta; teta = t; }
         if (sswap) { const float t = sxi; sxi = seta; seta = t; }
-        const float tb[3] = {1.f - txi - teta, txi, teta};
-        const float sb[3] = {1.f - sxi - seta, sxi, seta};
-        float x[3], y[3];
+        float d[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            x[c] = tb[0] * P[0][c] + tb[1] * P[1][c] + tb[2] * P[2][c];
-            y[c] = sb[0] * S[0][c] + sb[1] * S[1][c] + sb[2] * S[2][c];
+            const float x = fmaf(teta, P[2][c], fmaf(txi, P[1][c], P[0][c]));
+            const float y = fmaf(seta, S[2][c], fmaf(sxi, S[1][c], S[0][c]));
+            d[c] = y - x;
         }
+        const float ts[2][2] = {{txi * sxi, txi * seta}, {teta * sxi, teta * seta}};
+        const float tw[3] = {1.f, txi, teta}, sw[3] = {1.f, sxi, seta};
         float dre[NF], dim[NF], gre[NF], gim[NF];
-#pragma unroll
-        for (int f = 0; f < NF; ++f) dre[f] = dim[f] = gre[f] = gim[f] = 0.f;
-        sample_nf<NF, CK, true>(ssx * y[0] - tsx * x[0], ssy * y[1] - tsy * x[1], ssz * y[2] - tsz * x[2], nx, ny, nz,
-                                k, kt, ki, dre, dim, gre, gim);
+        sample_nf_w<NF, CK>(d[0], d[1], d[2], nx, ny, nz, k, kt, ki, w, dre, dim, gre, gim);
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
-            const float gr = gre[f] * w, gi = gim[f] * w, dr = dre[f] * w, di = dim[f] * w;
+            acc[f][0] += gre[f];
+            acc[f][1] += gim[f];
+            acc[f][2] = fmaf(gre[f], txi, acc[f][2]);
+            acc[f][3] = fmaf(gim[f], txi, acc[f][3]);
+            acc[f][4] = fmaf(gre[f], teta, acc[f][4]);
+            acc[f][5] = fmaf(gim[f], teta, acc[f][5]);
 #pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                acc[f][2 * i] = fmaf(gr, tb[i], acc[f][2 * i]);
-                acc[f][2 * i + 1] = fmaf(gi, tb[i], acc[f][2 * i + 1]);
-                const float dti_re = dr * tb[i], dti_im = di * tb[i];
+            for (int aa = 0; aa < 3; ++aa)
 #pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    acc[f][6 + 2 * (i * 3 + j)] = fmaf(dti_re, sb[j], acc[f][6 + 2 * (i * 3 + j)]);
-                    acc[f][7 + 2 * (i * 3 + j)] = fmaf(dti_im, sb[j], acc[f][7 + 2 * (i * 3 + j)]);
+                for (int bb = 0; bb < 3; ++bb) {
+                    const int e = 6 + 2 * (3 * aa + bb);
+                    if (aa == 0 && bb == 0) {
+                        acc[f][e] += dre[f];
+                        acc[f][e + 1] += dim[f];
+                    } else {
+                        const float wt = aa == 0 ? sw[bb] : (bb == 0 ? tw[aa] : ts[aa - 1][bb - 1]);
+                        acc[f][e] = fmaf(dre[f], wt, acc[f][e]);
+                        acc[f][e + 1] = fmaf(dim[f], wt, acc[f][e + 1]);
+                    }
                 }
-            }
         }
+    };
+    // P1 entry e (layout: 0..5 SLP rows (re, im), 6 + 2 (3 i + j) DLP) of
+    // wavenumber f from the moments, in FP64
+    auto nodal = [&](int f, int e) -> double {
+        const int c = e & 1;
+        if (e < 6) {
+            const int i = e >> 1;
+            const double m0 = acc[f][c], m1 = acc[f][2 + c], m2 = acc[f][4 + c];
+            return i == 0 ? m0 - m1 - m2 : (i == 1 ? m1 : m2);
+        }
+        const int ij = (e - 6) >> 1, i = ij / 3, j = ij - 3 * i;
+        auto M = [&](int aa, int bb) -> double { return (double)acc[f][6 + 2 * (3 * aa + bb) + c]; };
+        auto Tb = [&](int bb) -> double { return i == 0 ? M(0, bb) - M(1, bb) - M(2, bb) : M(i, bb); };
+        return j == 0 ? Tb(0) - Tb(1) - Tb(2) : Tb(j);
     };
 #pragma unroll
     for (int f = 0; f < NF; ++f)
@@ -938,9 +1009,9 @@ __global__ void __launch_bounds__(256, MINB) k_duffy(const __grid_constant__ Duf
     {
         double v0[S0], v1[S1];
 #pragma unroll
-        for (int i = 0; i < S0; ++i) v0[i] = (double)acc[i / 24][i % 24];
+        for (int i = 0; i < S0; ++i) v0[i] = nodal(i / 24, i % 24);
 #pragma unroll
-        for (int i = 0; i < S1; ++i) v1[i] = (double)acc[(S0 + i) / 24][(S0 + i) % 24];
+        for (int i = 0; i < S1; ++i) v1[i] = nodal((S0 + i) / 24, (S0 + i) % 24);
         red0 = warp_transpose_reduce<S0>(v0);
         red1 = warp_transpose_reduce<S1>(v1);
     }
