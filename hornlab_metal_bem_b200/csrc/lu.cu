@@ -203,12 +203,13 @@ __device__ __forceinline__ void argmax_warp(float &v, int &idx) {
     }
 }
 
-__global__ void __launch_bounds__(kPanelThreads) k_panel_rows(float *a_re, float *a_im, long long lda,
+constexpr int kPanelRowsThreads = 1024;   // one row per thread up to 1024 rows
+__global__ void __launch_bounds__(kPanelRowsThreads) k_panel_rows(float *a_re, float *a_im, long long lda,
                                                               long long a_stride, int n, int k0, int nb, int *piv,
                                                               long long piv_stride, int *info) {
     extern __shared__ float s_panel[];
-    __shared__ float s_v[kPanelThreads / 32];
-    __shared__ int s_i[kPanelThreads / 32];
+    __shared__ float s_v[kPanelRowsThreads / 32];
+    __shared__ int s_i[kPanelRowsThreads / 32];
     __shared__ float s_pr[32], s_pi[32];
     const int b = blockIdx.x;
     int *pv = piv + (size_t)b * piv_stride;
@@ -1851,16 +1852,22 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
     HBEM_CUDA(cudaFuncSetAttribute(k_swap_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSwapSmem));
     for (int b0 = 0; b0 < n; b0 += NB) {
         const int bw = std::min(NB, n - b0);
-        // inner width 32 while an 8-CTA cluster can hold the panel, else 16
-        const int fits32 = (size_t)(n - b0) <= 8 * (smem_cap / (33 * 8));
+        // inner width 32 while one CTA holds the sub-panel, else 16 while one
+        // CTA holds that, else 32 while an 8-CTA cluster holds it, else 16
+        const size_t rows = (size_t)(n - b0);
         const int want = tuning(HBEM_TUNE_LU_PANEL);
-        const int nbi = (want == 16 || !fits32) ? 16 : 32;
+        int nbi;
+        if (want == 16) nbi = 16;
+        else if (want == 32) nbi = rows <= 8 * (smem_cap / (33 * 8)) ? 32 : 16;
+        else if (rows * 33 * 8 <= smem_cap) nbi = 32;
+        else if (rows * 17 * 8 <= smem_cap) nbi = 16;
+        else nbi = rows <= 8 * (smem_cap / (33 * 8)) ? 32 : 16;
         for (int c = b0; c < b0 + bw; c += nbi) {
             const int w = std::min(nbi, b0 + bw - c);
             const size_t psmem = (size_t)(n - c) * (w + 1) * 8;
             int rc = HBEM_OK;
             if (psmem <= smem_cap) {
-                k_panel_rows<<<batch, kPanelThreads, psmem, cs>>>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride,
+                k_panel_rows<<<batch, kPanelRowsThreads, psmem, cs>>>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride,
                                                                   info);
                 rc = launched("k_panel_rows");
             } else if ((size_t)(n - c) <= 8 * (smem_cap / ((size_t)(w + 1) * 8))) {

@@ -87,7 +87,10 @@ long long hbem_launch_count(void);
  * reference.
  *   HBEM_TUNE_ASM_MINBLOCKS: resident CTAs per SM of the pair-assembly kernel
  *                            (2: 128 registers, 3: 80 registers)
- *   HBEM_TUNE_LU_PANEL:      inner sub-panel width of the LU (16 or 32)
+ *   HBEM_TUNE_LU_PANEL:      inner sub-panel width of the LU (16: always;
+ *                            32: wherever an 8-CTA cluster holds the
+ *                            sub-panel; 0: 32 where one CTA holds it, else
+ *                            16 where one CTA holds it, else 32 in a cluster)
  *   HBEM_TUNE_LU_SOLVE:      triangular solves (1: one CTA per right-hand
  *                            side, 2: blocked multi-CTA steps, 3: wavefront,
  *                            one CTA per 32-row block; 0: one CTA per
