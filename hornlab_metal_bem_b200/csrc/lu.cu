@@ -478,8 +478,8 @@ constexpr size_t kSwapSmem = (size_t)(2 * 128 * (kSwapCols + 1) + 2 * 64 * 65) *
 
 __global__ void __launch_bounds__(kSwapThreads) k_swap_trsm(float *a_re, float *a_im, long long lda,
                                                             long long a_stride, int k0, int np, int col_lo,
-                                                            int col_hi, int ex_lo, int trsm_lo, const int *piv,
-                                                            long long piv_stride) {
+                                                            int col_hi, int ex_lo, int ex_w, int trsm_lo,
+                                                            const int *piv, long long piv_stride) {
     extern __shared__ float s_dyn[];
     constexpr int XP = kSwapCols + 1;
     float *Xr = s_dyn, *Xi = Xr + 128 * XP;           // [slot][col]
@@ -491,12 +491,12 @@ __global__ void __launch_bounds__(kSwapThreads) k_swap_trsm(float *a_re, float *
     float *are = a_re + (size_t)b * a_stride, *aim = a_im + (size_t)b * a_stride;
     const int *pv = piv + (size_t)b * piv_stride;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int ncols_total = col_hi - col_lo - np;
+    const int ncols_total = col_hi - col_lo - ex_w;
     const int c_first = blockIdx.x * kSwapCols;
     const int ncols = min(kSwapCols, ncols_total - c_first);
     if (tid < kSwapCols) {
         int col = col_lo + c_first + tid;
-        if (col >= ex_lo) col += np;
+        if (col >= ex_lo) col += ex_w;
         s_col[tid] = tid < ncols ? col : -1;
     }
     if (tid < 128) s_row[tid] = tid < np ? k0 + tid : -1;
@@ -1881,7 +1881,7 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
             if (other > 0) {
                 dim3 grid((other + kSwapCols - 1) / kSwapCols, batch);
                 k_swap_trsm<<<grid, kSwapThreads, kSwapSmem, cs>>>(a_re, a_im, lda, a_stride, c, w, b0, b0 + bw, c,
-                                                                   c + w, piv, piv_stride);
+                                                                   w, c + w, piv, piv_stride);
                 rc = launched("k_swap_trsm");
                 if (rc != HBEM_OK) return finish(rc);
             }
@@ -1898,21 +1898,34 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
             bulk_pending = false;
         }
         const int outside = n - bw;
+        const int next_end = std::min(n, b0 + bw + NB);
+        const bool split = la && next_end < n;
         if (outside > 0) {
-            dim3 grid((outside + kSwapCols - 1) / kSwapCols, batch);
-            k_swap_trsm<<<grid, kSwapThreads, kSwapSmem, cs>>>(a_re, a_im, lda, a_stride, b0, bw, 0, n, b0, b0 + bw,
-                                                               piv, piv_stride);
+            // with look-ahead the chain swaps (and solves) only the next block's
+            // columns; the bulk stream swaps the rest before its update
+            const int lo = split ? b0 + bw : 0, hi = split ? next_end : n;
+            const int ex = split ? hi : b0, exw = split ? 0 : bw;
+            dim3 grid((hi - lo - exw + kSwapCols - 1) / kSwapCols, batch);
+            k_swap_trsm<<<grid, kSwapThreads, kSwapSmem, cs>>>(a_re, a_im, lda, a_stride, b0, bw, lo, hi, ex, exw,
+                                                               b0 + bw, piv, piv_stride);
             int rc = launched("k_swap_trsm");
             if (rc != HBEM_OK) return finish(rc);
         }
         if (b0 + bw < n) {
             int rc;
-            const int next_end = std::min(n, b0 + bw + NB);
-            if (la && next_end < n) {
+            if (split) {
                 rc = launch_trailing_simt(n, batch, b0, bw, b0 + bw, b0 + bw, next_end, a_re, a_im, lda, a_stride, cs);
                 if (rc == HBEM_OK) rc = stream_call(cudaEventRecord(la->split[parity], cs), "look-ahead fork");
                 if (rc == HBEM_OK)
                     rc = stream_call(cudaStreamWaitEvent(la->bulk, la->split[parity], 0), "look-ahead fork");
+                if (rc == HBEM_OK) {
+                    // columns [0, b0) and [next_end, n): swaps, and the TRSM on those right of the block
+                    dim3 grid((n - (next_end - b0) + kSwapCols - 1) / kSwapCols, batch);
+                    k_swap_trsm<<<grid, kSwapThreads, kSwapSmem, la->bulk>>>(a_re, a_im, lda, a_stride, b0, bw, 0, n,
+                                                                             b0, next_end - b0, b0 + bw, piv,
+                                                                             piv_stride);
+                    rc = launched("k_swap_trsm");
+                }
                 if (rc == HBEM_OK)
                     rc = launch_trailing_simt(n, batch, b0, bw, b0 + bw, next_end, n, a_re, a_im, lda, a_stride,
                                               la->bulk);
