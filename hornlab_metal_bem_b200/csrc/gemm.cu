@@ -127,8 +127,8 @@ __global__ void __launch_bounds__(256) k_trailing_simt(float *a_re, float *a_im,
 
 }  // namespace
 
-int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int col_end, float *a_re, float *a_im,
-                       long long lda, long long a_stride, int *status, cudaStream_t st);
+int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int col_start, int col_end, float *a_re,
+                       float *a_im, long long lda, long long a_stride, int *status, cudaStream_t st);
 
 // A[start:n, col_start:col_end] -= L[start:n, k0:k0+kw] U[k0:k0+kw, col_start:col_end] on the CUDA cores
 int launch_trailing_simt(int n, int batch, int k0, int kw, int start, int col_start, int col_end, float *a_re,
@@ -148,7 +148,7 @@ int launch_trailing_update(int n, int batch, int k0, int kw, int start, int col_
     if (m <= 0 || w <= 0) return HBEM_OK;
     if (kw % 16) return fail(HBEM_ERR_ARG, "trailing update: K must be a multiple of 16");
     if (tc && kw == 64 && status)
-        return launch_trailing_tc(tc, n, batch, k0, start, col_end, a_re, a_im, lda, a_stride, status, st);
+        return launch_trailing_tc(tc, n, batch, k0, start, start, col_end, a_re, a_im, lda, a_stride, status, st);
     return launch_trailing_simt(n, batch, k0, kw, start, start, col_end, a_re, a_im, lda, a_stride, st);
 }
 
@@ -271,7 +271,8 @@ __device__ __forceinline__ TcTile tc_tile(int t, int tiles_m, int tiles_n) {
 __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_constant__ CUtensorMap tmA,
                                                                 const __grid_constant__ CUtensorMap tmB, float *a_re,
                                                                 float *a_im, long long lda, long long a_stride, int n,
-                                                                int start, int col_end, int rows3, int cols_pad,
+                                                                int start, int col_start, int col_end, int rows3,
+                                                                int cols_pad,
                                                                 int tiles_m, int tiles_n, int n_tiles, int *status) {
     extern __shared__ uint8_t s_raw[];
     __shared__ uint64_t s_full[kTcStages], s_empty[kTcStages];
@@ -413,7 +414,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
         auto sidx = [](int r, int c) { return r * kTcN + ((((c >> 2) ^ (r & 7)) << 2) | (c & 3)); };
         auto prefetch = [&](int t, float *sC) {
             const TcTile tt = tc_tile(t, tiles_m, tiles_n);
-            const int row_c0 = start + tt.tm * 64, gcol = start + tt.tn * kTcN + 4 * gq;
+            const int row_c0 = start + tt.tm * 64, gcol = col_start + tt.tn * kTcN + 4 * gq;
             if (gcol >= col_end) {
                 asm volatile("cp.async.commit_group;" ::: "memory");
                 return;
@@ -494,7 +495,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
             epi_bar();   // the whole tile is drained
             {
                 const TcTile tt = tc_tile(blockIdx.x + i * G, tiles_m, tiles_n);
-                const int row_c0 = start + tt.tm * 64, gcol = start + tt.tn * kTcN + 4 * gq;
+                const int row_c0 = start + tt.tm * 64, gcol = col_start + tt.tn * kTcN + 4 * gq;
                 if (gcol < col_end) {
                     const bool full4 = gcol + 3 < col_end;
                     float *mre = a_re + (size_t)tt.mat * a_stride + gcol, *mim = a_im + (size_t)tt.mat * a_stride + gcol;
@@ -654,9 +655,10 @@ void tc_workspace_destroy(TcWorkspace *w, cudaStream_t st) {
 
 // Mixed-precision trailing update with K = 64 (one LU block); status
 // receives 1/2 if a barrier wait timed out.
-int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int col_end, float *a_re, float *a_im,
-                       long long lda, long long a_stride, int *status, cudaStream_t st) {
-    const int m = n - start, wd = col_end - start;
+// A[start:n, col_start:col_end] -= L[start:n, k0:k0+64] U[k0:k0+64, col_start:col_end] on the tensor cores
+int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int col_start, int col_end, float *a_re,
+                       float *a_im, long long lda, long long a_stride, int *status, cudaStream_t st) {
+    const int m = n - start, wd = col_end - col_start;
     if (m <= 0 || wd <= 0) return HBEM_OK;
     const int tiles_m = (m + 63) / 64, tiles_n = (wd + kTcN - 1) / kTcN;
     // packed rows use the workspace's fixed per-matrix pitch (rows3 / cols_pad)
@@ -667,7 +669,8 @@ int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int 
     }
     {
         dim3 grd((tiles_n * kTcN + 127) / 128, 64, batch);
-        k_pack_b<<<grd, 128, 0, st>>>(a_re, a_im, lda, a_stride, start, col_end, k0, w->cols_pad, tiles_n * kTcN, w->B3);
+        k_pack_b<<<grd, 128, 0, st>>>(a_re, a_im, lda, a_stride, col_start, col_end, k0, w->cols_pad, tiles_n * kTcN,
+                                      w->B3);
         HBEM_LAUNCH_CHECK("k_pack_b");
     }
     static int n_sm = 0;
@@ -680,8 +683,9 @@ int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int 
     const long long total = (long long)tiles_m * tiles_n * batch;
     if (total > 0x7fffffffLL) return fail(HBEM_ERR_ARG, "trailing update: too many tiles");
     const int grid = (int)std::min<long long>(total, n_sm);
-    k_trailing_tc<<<grid, kTcThreads, kTcSmem, st>>>(w->ma, w->mb, a_re, a_im, lda, a_stride, n, start, col_end,
-                                                    w->rows3, w->cols_pad, tiles_m, tiles_n, (int)total, status);
+    k_trailing_tc<<<grid, kTcThreads, kTcSmem, st>>>(w->ma, w->mb, a_re, a_im, lda, a_stride, n, start, col_start,
+                                                    col_end, w->rows3, w->cols_pad, tiles_m, tiles_n, (int)total,
+                                                    status);
     HBEM_LAUNCH_CHECK("k_trailing_tc");
     return HBEM_OK;
 }

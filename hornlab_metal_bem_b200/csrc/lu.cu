@@ -39,6 +39,8 @@ int launch_trailing_update(int n, int batch, int k0, int kw, int start, int col_
                            long long lda, long long a_stride, TcWorkspace *tc, int *status, cudaStream_t st);
 int launch_trailing_simt(int n, int batch, int k0, int kw, int start, int col_start, int col_end, float *a_re,
                          float *a_im, long long lda, long long a_stride, cudaStream_t st);
+int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int col_start, int col_end, float *a_re,
+                       float *a_im, long long lda, long long a_stride, int *status, cudaStream_t st);
 
 namespace {
 
@@ -1785,11 +1787,13 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
     // factored by inner sub-panels (32 wide when the sub-panel fits shared
     // memory, else 16) with updates confined to the block's columns; then one
     // row-swap pass, a 64-row TRSM and a K = 64 trailing update per block.
-    // Plain precision with look-ahead: the trailing update of block b is cut
-    // into the next block's 64 columns (on the chain, so block b+1's panels
-    // can start) and the rest (on the bulk stream, overlapping block b+1's
-    // panels, which touch only block b+1's columns); block b+1's row swaps,
-    // which touch every other column, wait for it.
+    // Look-ahead: the trailing update of block b is cut into the next block's
+    // 64 columns (on the chain, in FP32 on the CUDA cores, so block b+1's
+    // panels can start) and the rest (on the bulk stream, on the tensor cores
+    // in mixed precision, overlapping block b+1's panels, which touch only
+    // block b+1's columns); block b+1's row swaps, which touch every other
+    // column, wait for it.  The tensor-core workspace and status word are
+    // only used on the bulk stream (and on the chain after it has joined).
     const size_t smem_cap = 200 * 1024;
     constexpr int NB = 64;
     HBEM_CUDA(cudaMemsetAsync(info, 0, sizeof(int) * batch, st));
@@ -1807,7 +1811,7 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
         }
     }
     LookaheadStreams *la = nullptr;
-    if (!tc && n > 2 * NB && tuning(HBEM_TUNE_LU_LOOKAHEAD) != 1) {
+    if (n > 2 * NB && tuning(HBEM_TUNE_LU_LOOKAHEAD) != 1) {
         int rc = lookahead_streams(st, &la);
         if (rc != HBEM_OK) return rc;
         HBEM_CUDA(cudaEventRecord(la->fork, st));
@@ -1927,8 +1931,10 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
                     rc = launched("k_swap_trsm");
                 }
                 if (rc == HBEM_OK)
-                    rc = launch_trailing_simt(n, batch, b0, bw, b0 + bw, next_end, n, a_re, a_im, lda, a_stride,
-                                              la->bulk);
+                    rc = tc ? launch_trailing_tc(tc, n, batch, b0, b0 + bw, next_end, n, a_re, a_im, lda, a_stride,
+                                                 status, la->bulk)
+                            : launch_trailing_simt(n, batch, b0, bw, b0 + bw, next_end, n, a_re, a_im, lda, a_stride,
+                                                   la->bulk);
                 if (rc == HBEM_OK)
                     rc = stream_call(cudaEventRecord(la->bulk_done[parity], la->bulk), "look-ahead fork");
                 if (rc != HBEM_OK) return finish(rc);

@@ -100,10 +100,10 @@ long long hbem_launch_count(void);
  *                            pairs, two wavenumbers per evaluation)
  *   HBEM_TUNE_DUFFY:         singular corrections (1: one wavenumber per
  *                            warp, 2: two wavenumbers per warp)
- *   HBEM_TUNE_LU_LOOKAHEAD:  plain-precision LU (0: look-ahead, the block
- *                            after the panel is updated first and the rest
- *                            of the trailing update overlaps the next
- *                            panel on a second stream; 1: one stream)
+ *   HBEM_TUNE_LU_LOOKAHEAD:  LU schedule (0: look-ahead, the block after
+ *                            the panel is updated first and the rest of the
+ *                            trailing update overlaps the next panel on a
+ *                            second stream; 1: one stream)
  */
 #define HBEM_TUNE_ASM_MINBLOCKS 0
 #define HBEM_TUNE_LU_PANEL 1
