@@ -309,24 +309,25 @@ __global__ void __launch_bounds__(kPanelRowsThreads) k_panel_rows(float *a_re, f
 
 // Panel factorisation across a thread-block cluster, for panels too tall for
 // one CTA's shared memory.  CTA q of the cluster owns panel rows
-// [q R, (q+1) R) in its shared memory (pitch nb + 1).  Per column j:
-//   R: every CTA scales its rows of column j-1 and finds its local argmax of
-//      column j;                                           -> cluster barrier
-//   P: every CTA reduces the CS candidates (same order everywhere), copies the
-//      pivot row from its owner's shared memory (DSMEM), the owner of the
-//      pivot row copies the old row j;                     -> cluster barrier
+// [q R, (q+1) R) in its shared memory (pitch nb + 1), thread per row as in
+// k_panel_rows.  Per column j:
+//   P: warp 0 of every CTA reduces its warps' candidates; -> cluster barrier
+//      every CTA reduces the CS candidates (same order everywhere), copies
+//      the pivot row from its owner's shared memory (DSMEM), the owner of
+//      the pivot row copies the old row j;                 -> cluster barrier
 //      row j := pivot row, pivot row := old row j (owners write locally);
-//   E: every CTA updates its own rows below j.
-// Both barriers are executed by every CTA on every column.
+//   E: every CTA scales, updates and takes the next column's candidate from
+//      its own rows below j in one pass.
+// Both cluster barriers are executed by every CTA on every column.
 template <int CS>
-__global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(kPanelThreads)
+__global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(kPanelRowsThreads)
     k_panel_cluster(float *a_re, float *a_im, long long lda, long long a_stride, int n, int k0, int nb, int R,
                     int *piv, long long piv_stride, int *info) {
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
     extern __shared__ float s_panel[];
-    __shared__ float s_v[kPanelThreads / 32];
-    __shared__ int s_i[kPanelThreads / 32];
+    __shared__ float s_v[kPanelRowsThreads / 32];
+    __shared__ int s_i[kPanelRowsThreads / 32];
     __shared__ float s_cv;   // this CTA's candidate
     __shared__ int s_ci;
     __shared__ float s_pr[32], s_pi[32];   // pivot row
@@ -340,55 +341,33 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(kPanelThreads)
     const int nr = max(0, r1 - r0);
     float *pre = s_panel, *pim = s_panel + R * P;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-    {
-        const float *gre = a_re + (size_t)b * a_stride + (size_t)(k0 + r0) * lda + k0;
-        const float *gim = a_im + (size_t)b * a_stride + (size_t)(k0 + r0) * lda + k0;
-        for (int e = tid; e < nr * nb; e += blockDim.x) {
-            const int r = e / nb, j = e - r * nb;
-            pre[r * P + j] = gre[(size_t)r * lda + j];
-            pim[r * P + j] = gim[(size_t)r * lda + j];
-        }
+    float *gre = a_re + (size_t)b * a_stride + (size_t)(k0 + r0) * lda + k0;
+    float *gim = a_im + (size_t)b * a_stride + (size_t)(k0 + r0) * lda + k0;
+    for (int e = tid; e < nr * nb; e += blockDim.x) {
+        const int r = e / nb, j = e - r * nb;
+        pre[r * P + j] = gre[(size_t)r * lda + j];
+        pim[r * P + j] = gim[(size_t)r * lda + j];
     }
     __syncthreads();
-    const int LPR = nb > 16 ? 32 : 16;
-    const int c_off = lane & (LPR - 1), r_sub = lane / LPR, r_step = nw * (32 / LPR);
+    float v = -1.f;
+    int idx = 0x7fffffff;
+    for (int lr = tid; lr < nr; lr += blockDim.x) {
+        const float c = cabs1(pre[lr * P], pim[lr * P]);
+        if (c > v) { v = c; idx = r0 + lr; }
+    }
+    argmax_warp(v, idx);
+    if (lane == 0) { s_v[warp] = v; s_i[warp] = idx; }
+    __syncthreads();
     int first_zero = 0;
-    float ir = 0.f, ii = 0.f;
-    for (int j = 0; j <= nb; ++j) {
-        // ---- R (local rows r >= j, global panel index r0 + lr)
-        float v = -1.f;
-        int idx = 0x7fffffff;
-        const int lr0 = max(0, j - r0);
-        for (int lr = lr0 + tid; lr < nr; lr += blockDim.x) {
-            const int o = lr * P;
-            if (j > 0) {
-                const float xr = pre[o + j - 1], xi = pim[o + j - 1];
-                pre[o + j - 1] = xr * ir - xi * ii;
-                pim[o + j - 1] = xr * ii + xi * ir;
-            }
-            if (j < nb) {
-                const float c = cabs1(pre[o + j], pim[o + j]);
-                if (c > v) { v = c; idx = r0 + lr; }
-            }
-        }
-        if (j == nb) break;
-        for (int o = 16; o > 0; o >>= 1) {
-            const float ov = __shfl_xor_sync(0xffffffffu, v, o);
-            const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
-            if (ov > v || (ov == v && oi < idx)) { v = ov; idx = oi; }
-        }
-        if (lane == 0) { s_v[warp] = v; s_i[warp] = idx; }
-        __syncthreads();
-        if (tid == 0) {
-            float bv = s_v[0];
-            int bi = s_i[0];
-            for (int w = 1; w < nw; ++w)
-                if (s_v[w] > bv || (s_v[w] == bv && s_i[w] < bi)) { bv = s_v[w]; bi = s_i[w]; }
-            s_cv = bv;
-            s_ci = bi;
+    for (int j = 0; j < nb; ++j) {
+        // ---- P
+        if (warp == 0) {
+            float cv = lane < nw ? s_v[lane] : -1.f;
+            int ci = lane < nw ? s_i[lane] : 0x7fffffff;
+            argmax_warp(cv, ci);
+            if (lane == 0) { s_cv = cv; s_ci = ci; }
         }
         cluster.sync();
-        // ---- P
         float bv = -1.f;
         int p = 0x7fffffff;
         for (int c = 0; c < CS; ++c) {
@@ -425,41 +404,48 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(kPanelThreads)
         __syncthreads();
         const float dr = s_pr[j], di = s_pi[j];
         const bool zero = (dr == 0.f && di == 0.f);
+        float ir = 0.f, ii = 0.f;
         if (zero) {
             if (first_zero == 0) first_zero = k0 + j + 1;
-            ir = 0.f;
-            ii = 0.f;
         } else {
             const float den = 1.0f / (dr * dr + di * di);
             ir = dr * den;
             ii = -di * den;
         }
         // ---- E (own rows below j)
-        const int c = j + 1 + c_off;
-        if (c < nb && !zero) {
-            const float ur = s_pr[c], ui = s_pi[c];
-            const int lstart = max(0, j + 1 - r0);
-            for (int lr = lstart + warp * (32 / LPR) + r_sub; lr < nr; lr += r_step) {
-                const int o = lr * P;
-                const float xr = pre[o + j], xi = pim[o + j];
-                const float lr_ = xr * ir - xi * ii, li_ = xr * ii + xi * ir;
-                pre[o + c] -= lr_ * ur - li_ * ui;
-                pim[o + c] -= lr_ * ui + li_ * ur;
+        v = -1.f;
+        idx = 0x7fffffff;
+        const bool next = j + 1 < nb;
+        for (int lr = max(0, j + 1 - r0) + tid; lr < nr; lr += blockDim.x) {
+            const int o = lr * P;
+            const float xr = pre[o + j], xi = pim[o + j];
+            const float l_r = xr * ir - xi * ii, l_i = xr * ii + xi * ir;
+            pre[o + j] = l_r;
+            pim[o + j] = l_i;
+            if (!zero) {
+#pragma unroll 4
+                for (int c = j + 1; c < nb; ++c) {
+                    const float ur = s_pr[c], ui = s_pi[c];
+                    pre[o + c] -= l_r * ur - l_i * ui;
+                    pim[o + c] -= l_r * ui + l_i * ur;
+                }
+            }
+            if (next) {
+                const float a = cabs1(pre[o + j + 1], pim[o + j + 1]);
+                if (a > v) { v = a; idx = r0 + lr; }
             }
         }
+        if (next) {
+            argmax_warp(v, idx);
+            if (lane == 0) { s_v[warp] = v; s_i[warp] = idx; }
+        }
+        // also orders the last column's scaling before the write-back
         __syncthreads();
     }
-    // the last column was scaled by the R pass above, thread per row; the
-    // write-back maps elements to threads differently
-    __syncthreads();
-    {
-        float *gre = a_re + (size_t)b * a_stride + (size_t)(k0 + r0) * lda + k0;
-        float *gim = a_im + (size_t)b * a_stride + (size_t)(k0 + r0) * lda + k0;
-        for (int e = tid; e < nr * nb; e += blockDim.x) {
-            const int r = e / nb, j = e - r * nb;
-            gre[(size_t)r * lda + j] = pre[r * P + j];
-            gim[(size_t)r * lda + j] = pim[r * P + j];
-        }
+    for (int e = tid; e < nr * nb; e += blockDim.x) {
+        const int r = e / nb, j = e - r * nb;
+        gre[(size_t)r * lda + j] = pre[r * P + j];
+        gim[(size_t)r * lda + j] = pim[r * P + j];
     }
     if (q == 0 && tid == 0 && first_zero && info[b] == 0) info[b] = first_zero;
     // no CTA may exit while another can still read its shared memory
@@ -1717,8 +1703,8 @@ int launch_panel_cluster_t(float *a_re, float *a_im, long long lda, long long a_
         HBEM_CUDA(cudaFuncSetAttribute(k_panel_cluster<CS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(200 * 1024)));
         attr = true;
     }
-    k_panel_cluster<CS><<<dim3(CS, batch), kPanelThreads, smem, st>>>(a_re, a_im, lda, a_stride, n, c, w, R, piv,
-                                                                      piv_stride, info);
+    k_panel_cluster<CS><<<dim3(CS, batch), kPanelRowsThreads, smem, st>>>(a_re, a_im, lda, a_stride, n, c, w, R, piv,
+                                                                          piv_stride, info);
     HBEM_LAUNCH_CHECK("k_panel_cluster");
     return HBEM_OK;
 }

@@ -208,22 +208,27 @@ def test_lu_bitwise_stable_under_concurrent_work():
     """The factorisation of matrices whose first panels span 2-CTA clusters (n = 1043) must not depend on
     what else runs on the GPU: a matrix-multiply load on another stream changes CTA timing, which once
     exposed a missing barrier between a panel's last scaling pass and its write-back."""
+    lib = load_library()
     n, batch = 1043, 40
     A, _ = _lu_case(n, batch, 17)
     A0r, A0i = _dev(A)
     side = torch.cuda.Stream()
     X = torch.randn(4096, 4096, device="cuda")
     runs = []
-    for noisy in (False, True, True, True):
-        Ar, Ai = A0r.clone(), A0i.clone()
-        torch.cuda.synchronize()
-        if noisy:
-            with torch.cuda.stream(side):
-                for _ in range(60):
-                    X @ X
-        piv, info = _factor(Ar, Ai, n, batch)
-        torch.cuda.synchronize()
-        runs.append((Ar, Ai, piv, info))
+    assert lib.hbem_set_tuning(1, 32) == 0   # 32-wide sub-panels: 2-CTA clusters for the first blocks
+    try:
+        for noisy in (False, True, True, True):
+            Ar, Ai = A0r.clone(), A0i.clone()
+            torch.cuda.synchronize()
+            if noisy:
+                with torch.cuda.stream(side):
+                    for _ in range(60):
+                        X @ X
+            piv, info = _factor(Ar, Ai, n, batch)
+            torch.cuda.synchronize()
+            runs.append((Ar, Ai, piv, info))
+    finally:
+        lib.hbem_set_tuning(1, 0)
     assert int(runs[0][3].abs().sum()) == 0
     for r in runs[1:]:
         assert all(torch.equal(x, y) for x, y in zip(runs[0][:3], r[:3]))
