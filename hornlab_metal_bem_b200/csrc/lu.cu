@@ -310,15 +310,17 @@ __global__ void __launch_bounds__(kPanelRowsThreads) k_panel_rows(float *a_re, f
 // Panel factorisation across a thread-block cluster, for panels too tall for
 // one CTA's shared memory.  CTA q of the cluster owns panel rows
 // [q R, (q+1) R) in its shared memory (pitch nb + 1), thread per row as in
-// k_panel_rows.  Per column j:
-//   P: warp 0 of every CTA reduces its warps' candidates; -> cluster barrier
-//      every CTA reduces the CS candidates (same order everywhere), copies
-//      the pivot row from its owner's shared memory (DSMEM), the owner of
-//      the pivot row copies the old row j;                 -> cluster barrier
-//      row j := pivot row, pivot row := old row j (owners write locally);
-//   E: every CTA scales, updates and takes the next column's candidate from
-//      its own rows below j in one pass.
-// Both cluster barriers are executed by every CTA on every column.
+// k_panel_rows.  Per column j, one cluster barrier:
+//   before it, warp 0 of every CTA publishes its best candidate (value,
+//   row) and a copy of that row, and CTA 0 a copy of row j, in buffers
+//   double-buffered by column parity;
+//   after it, every CTA picks the pivot from the CS candidates (same order
+//   everywhere) and reads the pivot row, and the pivot row's owner the old
+//   row j, from those buffers (DSMEM); owners then write row j := pivot row,
+//   row p := old row j locally, and every CTA scales, updates and takes the
+//   next column's candidate from its own rows below j in one pass.
+// A buffer of parity j is rewritten only after the barrier of column j + 1,
+// which every CTA reaches after its reads of column j.
 template <int CS>
 __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(kPanelRowsThreads)
     k_panel_cluster(float *a_re, float *a_im, long long lda, long long a_stride, int n, int k0, int nb, int R,
@@ -328,10 +330,12 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(kPanelRowsThreads)
     extern __shared__ float s_panel[];
     __shared__ float s_v[kPanelRowsThreads / 32];
     __shared__ int s_i[kPanelRowsThreads / 32];
-    __shared__ float s_cv;   // this CTA's candidate
-    __shared__ int s_ci;
-    __shared__ float s_pr[32], s_pi[32];   // pivot row
-    __shared__ float s_or[32], s_oi[32];   // old row j (used by the pivot row's owner)
+    __shared__ float s_cv[2];                 // this CTA's candidate (by column parity)
+    __shared__ int s_ci[2];
+    __shared__ float s_cr[2][32], s_cim[2][32];   // its row
+    __shared__ float s_jr[2][32], s_jim[2][32];   // CTA 0: row j
+    __shared__ float s_pr[32], s_pi[32];          // pivot row
+    __shared__ float s_or[32], s_oi[32];          // old row j (used by the pivot row's owner)
     const int q = (int)cluster.block_rank();
     const int b = blockIdx.y;
     int *pv = piv + (size_t)b * piv_stride;
@@ -360,38 +364,46 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(kPanelRowsThreads)
     __syncthreads();
     int first_zero = 0;
     for (int j = 0; j < nb; ++j) {
-        // ---- P
+        const int par = j & 1;
+        // ---- publish this CTA's candidate (and, CTA 0, row j)
         if (warp == 0) {
             float cv = lane < nw ? s_v[lane] : -1.f;
             int ci = lane < nw ? s_i[lane] : 0x7fffffff;
             argmax_warp(cv, ci);
-            if (lane == 0) { s_cv = cv; s_ci = ci; }
-        }
-        cluster.sync();
-        float bv = -1.f;
-        int p = 0x7fffffff;
-        for (int c = 0; c < CS; ++c) {
-            const float ov = *cluster.map_shared_rank(&s_cv, c);
-            const int oi = *cluster.map_shared_rank(&s_ci, c);
-            if (ov > bv || (ov == bv && oi < p)) { bv = ov; p = oi; }
-        }
-        if (p >= m) p = j;  // column of NaNs: keep the diagonal, as icamax does
-        const int owner_p = p / R, owner_j = j / R;
-        if (tid < nb) {
-            const float *rre = cluster.map_shared_rank(pre, owner_p);
-            const float *rim = cluster.map_shared_rank(pim, owner_p);
-            s_pr[tid] = rre[(p - owner_p * R) * P + tid];
-            s_pi[tid] = rim[(p - owner_p * R) * P + tid];
-            if (q == owner_p && p != j) {
-                const float *jre = cluster.map_shared_rank(pre, owner_j);
-                const float *jim = cluster.map_shared_rank(pim, owner_j);
-                s_or[tid] = jre[(j - owner_j * R) * P + tid];
-                s_oi[tid] = jim[(j - owner_j * R) * P + tid];
+            if (lane == 0) { s_cv[par] = cv; s_ci[par] = ci; }
+            if (ci < m && lane < nb) {
+                s_cr[par][lane] = pre[(ci - r0) * P + lane];
+                s_cim[par][lane] = pim[(ci - r0) * P + lane];
+            }
+            if (q == 0 && lane < nb) {
+                s_jr[par][lane] = pre[(j - r0) * P + lane];
+                s_jim[par][lane] = pim[(j - r0) * P + lane];
             }
         }
         cluster.sync();
+        // ---- pivot
+        float bv = -1.f;
+        int p = 0x7fffffff;
+        for (int c = 0; c < CS; ++c) {
+            const float ov = *cluster.map_shared_rank(&s_cv[par], c);
+            const int oi = *cluster.map_shared_rank(&s_ci[par], c);
+            if (ov > bv || (ov == bv && oi < p)) { bv = ov; p = oi; }
+        }
+        if (p >= m) p = j;  // column of NaNs: keep the diagonal, as icamax does
+        const int owner_p = p / R;
         if (tid < nb) {
-            if (q == owner_j) {
+            if (p == j) {
+                s_pr[tid] = *cluster.map_shared_rank(&s_jr[par][tid], 0);
+                s_pi[tid] = *cluster.map_shared_rank(&s_jim[par][tid], 0);
+            } else {
+                s_pr[tid] = *cluster.map_shared_rank(&s_cr[par][tid], owner_p);
+                s_pi[tid] = *cluster.map_shared_rank(&s_cim[par][tid], owner_p);
+                if (q == owner_p) {
+                    s_or[tid] = *cluster.map_shared_rank(&s_jr[par][tid], 0);
+                    s_oi[tid] = *cluster.map_shared_rank(&s_jim[par][tid], 0);
+                }
+            }
+            if (q == 0) {   // row j (< 32 <= R) lives in CTA 0
                 pre[(j - r0) * P + tid] = s_pr[tid];
                 pim[(j - r0) * P + tid] = s_pi[tid];
             }
