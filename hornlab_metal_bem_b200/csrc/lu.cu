@@ -381,38 +381,41 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(kPanelRowsThreads)
             }
         }
         cluster.sync();
-        // ---- pivot
-        float bv = -1.f;
-        int p = 0x7fffffff;
-        for (int c = 0; c < CS; ++c) {
-            const float ov = *cluster.map_shared_rank(&s_cv[par], c);
-            const int oi = *cluster.map_shared_rank(&s_ci[par], c);
-            if (ov > bv || (ov == bv && oi < p)) { bv = ov; p = oi; }
-        }
-        if (p >= m) p = j;  // column of NaNs: keep the diagonal, as icamax does
-        const int owner_p = p / R;
-        if (tid < nb) {
-            if (p == j) {
-                s_pr[tid] = *cluster.map_shared_rank(&s_jr[par][tid], 0);
-                s_pi[tid] = *cluster.map_shared_rank(&s_jim[par][tid], 0);
-            } else {
-                s_pr[tid] = *cluster.map_shared_rank(&s_cr[par][tid], owner_p);
-                s_pi[tid] = *cluster.map_shared_rank(&s_cim[par][tid], owner_p);
-                if (q == owner_p) {
-                    s_or[tid] = *cluster.map_shared_rank(&s_jr[par][tid], 0);
-                    s_oi[tid] = *cluster.map_shared_rank(&s_jim[par][tid], 0);
+        // ---- pivot: warp 0 alone (lane c reads CTA c's candidate); the other
+        // warps only need the pivot row, which they read after the barrier
+        if (warp == 0) {
+            float bv = -1.f;
+            int p = 0x7fffffff;
+            if (lane < CS) {
+                bv = *cluster.map_shared_rank(&s_cv[par], lane);
+                p = *cluster.map_shared_rank(&s_ci[par], lane);
+            }
+            argmax_warp(bv, p);
+            if (p >= m) p = j;  // column of NaNs: keep the diagonal, as icamax does
+            const int owner_p = p / R;
+            if (tid < nb) {
+                if (p == j) {
+                    s_pr[tid] = *cluster.map_shared_rank(&s_jr[par][tid], 0);
+                    s_pi[tid] = *cluster.map_shared_rank(&s_jim[par][tid], 0);
+                } else {
+                    s_pr[tid] = *cluster.map_shared_rank(&s_cr[par][tid], owner_p);
+                    s_pi[tid] = *cluster.map_shared_rank(&s_cim[par][tid], owner_p);
+                    if (q == owner_p) {
+                        s_or[tid] = *cluster.map_shared_rank(&s_jr[par][tid], 0);
+                        s_oi[tid] = *cluster.map_shared_rank(&s_jim[par][tid], 0);
+                    }
+                }
+                if (q == 0) {   // row j (< 32 <= R) lives in CTA 0
+                    pre[(j - r0) * P + tid] = s_pr[tid];
+                    pim[(j - r0) * P + tid] = s_pi[tid];
+                }
+                if (q == owner_p && p != j) {
+                    pre[(p - r0) * P + tid] = s_or[tid];
+                    pim[(p - r0) * P + tid] = s_oi[tid];
                 }
             }
-            if (q == 0) {   // row j (< 32 <= R) lives in CTA 0
-                pre[(j - r0) * P + tid] = s_pr[tid];
-                pim[(j - r0) * P + tid] = s_pi[tid];
-            }
-            if (q == owner_p && p != j) {
-                pre[(p - r0) * P + tid] = s_or[tid];
-                pim[(p - r0) * P + tid] = s_oi[tid];
-            }
+            if (q == 0 && tid == 0) pv[k0 + j] = k0 + p;
         }
-        if (q == 0 && tid == 0) pv[k0 + j] = k0 + p;
         __syncthreads();
         const float dr = s_pr[j], di = s_pi[j];
         const bool zero = (dr == 0.f && di == 0.f);
