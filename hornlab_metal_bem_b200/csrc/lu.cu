@@ -184,8 +184,9 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(float *a_re, float *a_i
     if (tid == 0 && first_zero && info[b] == 0) info[b] = first_zero;
 }
 
-// Panel factorisation in one CTA's shared memory (pitch nb + 1), thread per
-// row.  Per column j, two barrier-separated phases:
+// Panel factorisation in one CTA's shared memory (pitch nb + 1, nb <= 64:
+// a whole 64-column block when it fits), thread per row.  Per column j, two
+// barrier-separated phases:
 //   P (warp 0): reduce the per-warp argmax candidates of column j (first
 //               index on ties, as icamax), swap rows j <-> p, publish the
 //               pivot row;
@@ -212,7 +213,7 @@ __global__ void __launch_bounds__(kPanelRowsThreads) k_panel_rows(float *a_re, f
     extern __shared__ float s_panel[];
     __shared__ float s_v[kPanelRowsThreads / 32];
     __shared__ int s_i[kPanelRowsThreads / 32];
-    __shared__ float s_pr[32], s_pi[32];
+    __shared__ float s_pr[64], s_pi[64];   // nb <= 64
     const int b = blockIdx.x;
     int *pv = piv + (size_t)b * piv_stride;
     const int m = n - k0;
@@ -244,8 +245,7 @@ __global__ void __launch_bounds__(kPanelRowsThreads) k_panel_rows(float *a_re, f
             int p = lane < nw ? s_i[lane] : 0x7fffffff;
             argmax_warp(bv, p);
             if (p >= m) p = j;  // column of NaNs: keep the diagonal, as icamax does
-            if (lane < nb) {
-                const int c = lane;
+            for (int c = lane; c < nb; c += 32) {
                 const float jr = pre[j * P + c], ji = pim[j * P + c];
                 const float pr = pre[p * P + c], pi = pim[p * P + c];
                 s_pr[c] = pr;
@@ -256,8 +256,8 @@ __global__ void __launch_bounds__(kPanelRowsThreads) k_panel_rows(float *a_re, f
                     pre[p * P + c] = jr;
                     pim[p * P + c] = ji;
                 }
-                if (c == 0) pv[k0 + j] = k0 + p;
             }
+            if (lane == 0) pv[k0 + j] = k0 + p;
         }
         __syncthreads();
         const float dr = s_pr[j], di = s_pi[j];
@@ -1857,13 +1857,15 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
     HBEM_CUDA(cudaFuncSetAttribute(k_swap_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSwapSmem));
     for (int b0 = 0; b0 < n; b0 += NB) {
         const int bw = std::min(NB, n - b0);
-        // inner width 32 while one CTA holds the sub-panel, else 16 while one
-        // CTA holds that, else 32 while an 8-CTA cluster holds it, else 16
+        // the whole block as one panel while one CTA holds it; else inner width
+        // 32 while one CTA holds the sub-panel, else 16 while one CTA holds
+        // that, else 32 while an 8-CTA cluster holds it, else 16
         const size_t rows = (size_t)(n - b0);
         const int want = tuning(HBEM_TUNE_LU_PANEL);
         int nbi;
         if (want == 16) nbi = 16;
         else if (want == 32) nbi = rows <= 8 * (smem_cap / (33 * 8)) ? 32 : 16;
+        else if (rows * 65 * 8 <= smem_cap) nbi = 64;
         else if (rows * 33 * 8 <= smem_cap) nbi = 32;
         else if (rows * 17 * 8 <= smem_cap) nbi = 16;
         else nbi = rows <= 8 * (smem_cap / (33 * 8)) ? 32 : 16;
