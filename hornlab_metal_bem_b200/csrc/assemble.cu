@@ -921,9 +921,9 @@ __global__ void __launch_bounds__(256, MINB) k_duffy(const __grid_constant__ Duf
     // = sum D t_a s_b; turned into the P1 entries (tb = 1 - t1 - t2, t1, t2)
     // in FP64 before the warp reduction.
     float acc[NF][24];
+    // (txi, teta), (sxi, seta): the point's base-local barycentrics (t1, t2),
+    // (s1, s2) on the test and trial triangles
     auto accumulate = [&](float txi, float teta, float sxi, float seta, float w) {
-        if (tswap) { const float t = txi; txi = teta; teta = t; }
-        if (sswap) { const float t = sxi; sxi = seta; seta = t; }
         float d[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
@@ -984,21 +984,46 @@ __global__ void __launch_bounds__(256, MINB) k_duffy(const __grid_constant__ Duf
     const int ri = pr.kind - 1;
     const int off = p.rule_off[ri], cnt = p.rule_cnt[ri];
     const bool self_pair = pr.test == pr.trial && pr.test_mask == pr.trial_mask;
+    // A rule point (x, y) on the reference triangle reaches the base-local
+    // barycentrics through the pair's Duffy remap (anchoring the rule on the
+    // shared vertices, image-local order) and, for a mirrored triangle, the
+    // swap back to base-local order: one affine map per side, composed here
+    // from three evaluations (its coefficients are 0 or +-1, so the composed
+    // map reproduces the two steps exactly).
+    float tmap[6], smap[6];   // t1 = m0 + m1 x + m2 y, t2 = m3 + m4 x + m5 y
+    auto compose = [&](int l1, int l2, bool swp, float (&mm)[6]) {
+        float o[3][2];
+        const float xs[3] = {0.f, 1.f, 0.f}, ys[3] = {0.f, 0.f, 1.f};
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+            remap(xs[e], ys[e], pr.kind, l1, l2, o[e][0], o[e][1]);
+            if (swp) { const float t = o[e][0]; o[e][0] = o[e][1]; o[e][1] = t; }
+        }
+        mm[0] = o[0][0]; mm[1] = o[1][0] - o[0][0]; mm[2] = o[2][0] - o[0][0];
+        mm[3] = o[0][1]; mm[4] = o[1][1] - o[0][1]; mm[5] = o[2][1] - o[0][1];
+    };
+    compose(pr.tl1, pr.tl2, tswap, tmap);
+    compose(pr.sl1, pr.sl2, sswap, smap);
     for (int q = lane; q < cnt + 36; q += 32) {
-        float tx_, ty_, sx_, sy_, w;
+        float t1, t2, s1, s2, w;
         bool skip = false;
-        if (q < cnt) {
+        if (q < cnt) {   // warp-uniform: cnt is a multiple of 32
             const float4 r = __ldg(&p.rule[off + q]);
             w = __ldg(&p.rule_w[off + q]);
-            remap(r.x, r.y, pr.kind, pr.tl1, pr.tl2, tx_, ty_);
-            remap(r.z, r.w, pr.kind, pr.sl1, pr.sl2, sx_, sy_);
+            t1 = fmaf(tmap[2], r.y, fmaf(tmap[1], r.x, tmap[0]));
+            t2 = fmaf(tmap[5], r.y, fmaf(tmap[4], r.x, tmap[3]));
+            s1 = fmaf(smap[2], r.w, fmaf(smap[1], r.z, smap[0]));
+            s2 = fmaf(smap[5], r.w, fmaf(smap[4], r.z, smap[3]));
         } else {
             const int rq = q - cnt, a = rq / 6, b = rq - 6 * a;
-            tx_ = qx(a); ty_ = qy(a); sx_ = qx(b); sy_ = qy(b);
+            t1 = tswap ? qy(a) : qx(a);
+            t2 = tswap ? qx(a) : qy(a);
+            s1 = sswap ? qy(b) : qx(b);
+            s2 = sswap ? qx(b) : qy(b);
             w = -(qw(a) * qw(b));
             skip = self_pair && a == b;
         }
-        if (!skip) accumulate(tx_, ty_, sx_, sy_, w);
+        if (!skip) accumulate(t1, t2, s1, s2, w);
     }
     // FP64 warp totals of the 24 NF lane partials (value v = 24 f + e): a
     // transpose-reduce leaves value v of the first set in lane v, of the
