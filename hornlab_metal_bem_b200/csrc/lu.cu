@@ -332,10 +332,10 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(kPanelRowsThreads)
     __shared__ int s_i[kPanelRowsThreads / 32];
     __shared__ float s_cv[2];                 // this CTA's candidate (by column parity)
     __shared__ int s_ci[2];
-    __shared__ float s_cr[2][32], s_cim[2][32];   // its row
-    __shared__ float s_jr[2][32], s_jim[2][32];   // CTA 0: row j
-    __shared__ float s_pr[32], s_pi[32];          // pivot row
-    __shared__ float s_or[32], s_oi[32];          // old row j (used by the pivot row's owner)
+    __shared__ float s_cr[2][64], s_cim[2][64];   // its row (nb <= 64)
+    __shared__ float s_jr[2][64], s_jim[2][64];   // CTA 0: row j
+    __shared__ float s_pr[64], s_pi[64];          // pivot row
+    __shared__ float s_or[64], s_oi[64];          // old row j (used by the pivot row's owner)
     const int q = (int)cluster.block_rank();
     const int b = blockIdx.y;
     int *pv = piv + (size_t)b * piv_stride;
@@ -371,13 +371,15 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(kPanelRowsThreads)
             int ci = lane < nw ? s_i[lane] : 0x7fffffff;
             argmax_warp(cv, ci);
             if (lane == 0) { s_cv[par] = cv; s_ci[par] = ci; }
-            if (ci < m && lane < nb) {
-                s_cr[par][lane] = pre[(ci - r0) * P + lane];
-                s_cim[par][lane] = pim[(ci - r0) * P + lane];
-            }
-            if (q == 0 && lane < nb) {
-                s_jr[par][lane] = pre[(j - r0) * P + lane];
-                s_jim[par][lane] = pim[(j - r0) * P + lane];
+            for (int c = lane; c < nb; c += 32) {
+                if (ci < m) {
+                    s_cr[par][c] = pre[(ci - r0) * P + c];
+                    s_cim[par][c] = pim[(ci - r0) * P + c];
+                }
+                if (q == 0) {
+                    s_jr[par][c] = pre[(j - r0) * P + c];
+                    s_jim[par][c] = pim[(j - r0) * P + c];
+                }
             }
         }
         cluster.sync();
@@ -393,25 +395,25 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(kPanelRowsThreads)
             argmax_warp(bv, p);
             if (p >= m) p = j;  // column of NaNs: keep the diagonal, as icamax does
             const int owner_p = p / R;
-            if (tid < nb) {
+            for (int c = lane; c < nb; c += 32) {
                 if (p == j) {
-                    s_pr[tid] = *cluster.map_shared_rank(&s_jr[par][tid], 0);
-                    s_pi[tid] = *cluster.map_shared_rank(&s_jim[par][tid], 0);
+                    s_pr[c] = *cluster.map_shared_rank(&s_jr[par][c], 0);
+                    s_pi[c] = *cluster.map_shared_rank(&s_jim[par][c], 0);
                 } else {
-                    s_pr[tid] = *cluster.map_shared_rank(&s_cr[par][tid], owner_p);
-                    s_pi[tid] = *cluster.map_shared_rank(&s_cim[par][tid], owner_p);
+                    s_pr[c] = *cluster.map_shared_rank(&s_cr[par][c], owner_p);
+                    s_pi[c] = *cluster.map_shared_rank(&s_cim[par][c], owner_p);
                     if (q == owner_p) {
-                        s_or[tid] = *cluster.map_shared_rank(&s_jr[par][tid], 0);
-                        s_oi[tid] = *cluster.map_shared_rank(&s_jim[par][tid], 0);
+                        s_or[c] = *cluster.map_shared_rank(&s_jr[par][c], 0);
+                        s_oi[c] = *cluster.map_shared_rank(&s_jim[par][c], 0);
                     }
                 }
-                if (q == 0) {   // row j (< 32 <= R) lives in CTA 0
-                    pre[(j - r0) * P + tid] = s_pr[tid];
-                    pim[(j - r0) * P + tid] = s_pi[tid];
+                if (q == 0) {   // row j (< 64 <= R) lives in CTA 0
+                    pre[(j - r0) * P + c] = s_pr[c];
+                    pim[(j - r0) * P + c] = s_pi[c];
                 }
                 if (q == owner_p && p != j) {
-                    pre[(p - r0) * P + tid] = s_or[tid];
-                    pim[(p - r0) * P + tid] = s_oi[tid];
+                    pre[(p - r0) * P + c] = s_or[c];
+                    pim[(p - r0) * P + c] = s_oi[c];
                 }
             }
             if (q == 0 && tid == 0) pv[k0 + j] = k0 + p;
@@ -1732,7 +1734,7 @@ int launch_panel_cluster(float *a_re, float *a_im, long long lda, long long a_st
     int cs = 2;
     while (cs < 8 && (long long)cs * rows_cap < m) cs *= 2;
     int R = (m + cs - 1) / cs;
-    if (R < 32) R = 32;  // row j (< 32) always lives in CTA 0
+    if (R < 64) R = 64;  // row j (< nb <= 64) always lives in CTA 0
     const size_t smem = (size_t)R * row_bytes;
     if (cs == 2) return launch_panel_cluster_t<2>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info, batch, R, smem, st);
     if (cs == 4) return launch_panel_cluster_t<4>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info, batch, R, smem, st);
@@ -1865,7 +1867,7 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
         int nbi;
         if (want == 16) nbi = 16;
         else if (want == 32) nbi = rows <= 8 * (smem_cap / (33 * 8)) ? 32 : 16;
-        else if (rows * 65 * 8 <= smem_cap) nbi = 64;
+        else if (rows * 65 * 8 <= smem_cap || (want == 64 && rows <= 8 * (smem_cap / (65 * 8)))) nbi = 64;
         else if (rows * 33 * 8 <= smem_cap) nbi = 32;
         else if (rows * 17 * 8 <= smem_cap) nbi = 16;
         else nbi = rows <= 8 * (smem_cap / (33 * 8)) ? 32 : 16;

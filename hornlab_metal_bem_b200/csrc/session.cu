@@ -315,7 +315,8 @@ extern "C" int hbem_set_tuning(int key, int value) {
             if (value != 0 && value != 2 && value != 3) return fail(HBEM_ERR_ARG, "HBEM_TUNE_ASM_MINBLOCKS: 0, 2 or 3");
             break;
         case HBEM_TUNE_LU_PANEL:
-            if (value != 0 && value != 16 && value != 32) return fail(HBEM_ERR_ARG, "HBEM_TUNE_LU_PANEL: 0, 16 or 32");
+            if (value != 0 && value != 16 && value != 32 && value != 64)
+                return fail(HBEM_ERR_ARG, "HBEM_TUNE_LU_PANEL: 0, 16, 32 or 64");
             break;
         case HBEM_TUNE_LU_SOLVE:
             if (value < 0 || value > 3) return fail(HBEM_ERR_ARG, "HBEM_TUNE_LU_SOLVE: 0, 1, 2 or 3");

@@ -89,8 +89,11 @@ long long hbem_launch_count(void);
  *                            (2: 128 registers, 3: 80 registers)
  *   HBEM_TUNE_LU_PANEL:      inner sub-panel width of the LU (16: always;
  *                            32: wherever an 8-CTA cluster holds the
- *                            sub-panel; 0: 32 where one CTA holds it, else
- *                            16 where one CTA holds it, else 32 in a cluster)
+ *                            sub-panel; 0: the whole 64-column block where
+ *                            one CTA holds it, else 32 where one CTA holds
+ *                            it, else 16 where one CTA holds it, else 32 in
+ *                            a cluster; 64: as 0, but the whole block also
+ *                            in an 8-CTA cluster where that holds it)
  *   HBEM_TUNE_LU_SOLVE:      triangular solves (1: one CTA per right-hand
  *                            side, 2: blocked multi-CTA steps, 3: wavefront,
  *                            one CTA per 32-row block; 0: one CTA per

@@ -204,10 +204,12 @@ def test_wavefront_solve_many_matrices(trans):
         assert rel(out[3][m], ref) < 1e-5
 
 
-def test_lu_bitwise_stable_under_concurrent_work():
-    """The factorisation of matrices whose first panels span 2-CTA clusters (n = 1043) must not depend on
-    what else runs on the GPU: a matrix-multiply load on another stream changes CTA timing, which once
-    exposed a missing barrier between a panel's last scaling pass and its write-back."""
+@pytest.mark.parametrize("panel", [32, 64])
+def test_lu_bitwise_stable_under_concurrent_work(panel):
+    """The factorisation of matrices whose first panels span thread-block clusters (n = 1043: 2 CTAs for
+    32-wide sub-panels, 4 for whole 64-column blocks) must not depend on what else runs on the GPU: a
+    matrix-multiply load on another stream changes CTA timing, which once exposed a missing barrier between
+    a panel's last scaling pass and its write-back."""
     lib = load_library()
     n, batch = 1043, 40
     A, _ = _lu_case(n, batch, 17)
@@ -215,7 +217,7 @@ def test_lu_bitwise_stable_under_concurrent_work():
     side = torch.cuda.Stream()
     X = torch.randn(4096, 4096, device="cuda")
     runs = []
-    assert lib.hbem_set_tuning(1, 32) == 0   # 32-wide sub-panels: 2-CTA clusters for the first blocks
+    assert lib.hbem_set_tuning(1, panel) == 0
     try:
         for noisy in (False, True, True, True):
             Ar, Ai = A0r.clone(), A0i.clone()
