@@ -19,14 +19,6 @@ namespace hbem {
 struct TcWorkspace;
 namespace {
 
-// 4-byte asynchronous copy global -> shared; src_bytes 0 writes a zero
-__device__ __forceinline__ void cp_async4(float *dst, const float *src, int src_bytes) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(
-                     static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
-                 "l"(src), "r"(src_bytes)
-                 : "memory");
-}
-
 // C[start:n, col_start:col_end] -= L[start:n, k0:k0+kw] * U[k0:k0+kw, col_start:col_end]
 // (kw a multiple of 16) for one 64 x 64 complex tile per CTA, K in chunks of
 // 16 double-buffered through cp.async (the next chunk's loads
@@ -128,7 +120,8 @@ __global__ void __launch_bounds__(256) k_trailing_simt(float *a_re, float *a_im,
 }  // namespace
 
 int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int col_start, int col_end, float *a_re,
-                       float *a_im, long long lda, long long a_stride, int *status, cudaStream_t st);
+                       float *a_im, long long lda, long long a_stride, int *status, cudaStream_t st,
+                       int reserve_sms = 0);
 
 // A[start:n, col_start:col_end] -= L[start:n, k0:k0+kw] U[k0:k0+kw, col_start:col_end] on the CUDA cores
 int launch_trailing_simt(int n, int batch, int k0, int kw, int start, int col_start, int col_end, float *a_re,
@@ -654,10 +647,12 @@ void tc_workspace_destroy(TcWorkspace *w, cudaStream_t st) {
 }
 
 // Mixed-precision trailing update with K = 64 (one LU block); status
-// receives 1/2 if a barrier wait timed out.
+// receives 1/2 if a barrier wait timed out.  The persistent grid leaves
+// reserve_sms SMs (at most half of them) to kernels on other streams.
 // A[start:n, col_start:col_end] -= L[start:n, k0:k0+64] U[k0:k0+64, col_start:col_end] on the tensor cores
 int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int col_start, int col_end, float *a_re,
-                       float *a_im, long long lda, long long a_stride, int *status, cudaStream_t st) {
+                       float *a_im, long long lda, long long a_stride, int *status, cudaStream_t st,
+                       int reserve_sms) {
     const int m = n - start, wd = col_end - col_start;
     if (m <= 0 || wd <= 0) return HBEM_OK;
     const int tiles_m = (m + 63) / 64, tiles_n = (wd + kTcN - 1) / kTcN;
@@ -682,7 +677,8 @@ int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int 
     }
     const long long total = (long long)tiles_m * tiles_n * batch;
     if (total > 0x7fffffffLL) return fail(HBEM_ERR_ARG, "trailing update: too many tiles");
-    const int grid = (int)std::min<long long>(total, n_sm);
+    const int ctas = n_sm - std::min(std::max(reserve_sms, 0), n_sm / 2);
+    const int grid = (int)std::min<long long>(total, ctas);
     k_trailing_tc<<<grid, kTcThreads, kTcSmem, st>>>(w->ma, w->mb, a_re, a_im, lda, a_stride, n, start, col_start,
                                                     col_end, w->rows3, w->cols_pad, tiles_m, tiles_n, (int)total,
                                                     status);

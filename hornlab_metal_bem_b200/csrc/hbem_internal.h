@@ -32,6 +32,16 @@ void keep_pool_memory();   // cache freed stream-ordered allocations of the curr
         ::hbem::count_launch();                                \
     } while (0)
 
+#ifdef __CUDACC__
+// 4-byte asynchronous copy global -> shared; src_bytes 0 writes a zero
+__device__ __forceinline__ void cp_async4(float *dst, const float *src, int src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(
+                     static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+                 "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+#endif
+
 // ---- assembly tiling constants -------------------------------------------
 constexpr int kTestTile = 32;    // test triangles per CTA (one per lane)
 constexpr int kTrialTile = 64;   // trial triangles per CTA (split over 8 warps)

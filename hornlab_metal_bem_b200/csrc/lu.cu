@@ -4,11 +4,11 @@
 //
 // Two-level right-looking blocked factorisation, batched over matrices:
 //   for each 64-column block b0:
-//     for each inner sub-panel c (32 or 16 columns):
+//     for each inner sub-panel c (64, 32 or 16 columns):
 //       k_panel      : factor rows c..n of the sub-panel with partial pivoting
 //                      (pivot = first max |re|+|im|, as LAPACK's icamax),
 //                      staged in one CTA's shared memory when it fits, else
-//                      spread over a 2/4/8-CTA cluster's shared memory
+//                      spread over a 2/4/8/16-CTA cluster's shared memory
 //                      (k_panel_cluster), else in L2;
 //       k_swap_trsm  : swap + forward-solve the other columns of the block;
 //       trailing     : update the block's remaining columns (K = 16/32);
@@ -40,7 +40,8 @@ int launch_trailing_update(int n, int batch, int k0, int kw, int start, int col_
 int launch_trailing_simt(int n, int batch, int k0, int kw, int start, int col_start, int col_end, float *a_re,
                          float *a_im, long long lda, long long a_stride, cudaStream_t st);
 int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int col_start, int col_end, float *a_re,
-                       float *a_im, long long lda, long long a_stride, int *status, cudaStream_t st);
+                       float *a_im, long long lda, long long a_stride, int *status, cudaStream_t st,
+                       int reserve_sms = 0);
 
 namespace {
 
@@ -322,7 +323,7 @@ __global__ void __launch_bounds__(kPanelRowsThreads) k_panel_rows(float *a_re, f
 // A buffer of parity j is rewritten only after the barrier of column j + 1,
 // which every CTA reaches after its reads of column j.
 template <int CS>
-__global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(kPanelRowsThreads)
+__global__ void __launch_bounds__(kPanelRowsThreads)
     k_panel_cluster(float *a_re, float *a_im, long long lda, long long a_stride, int n, int k0, int nb, int R,
                     int *piv, long long piv_stride, int *info) {
     namespace cg = cooperative_groups;
@@ -522,12 +523,13 @@ __global__ void __launch_bounds__(kSwapThreads) k_swap_trsm(float *a_re, float *
         }
         s_slot[tid] = slot;
     }
+    // every global read is an asynchronous copy, all in flight together
     const bool any_trsm = trsm_lo < col_hi;
     if (any_trsm)
         for (int e = tid; e < np * np; e += blockDim.x) {
             const int r = e / np, c = e - r * np;
-            Lr[r * 65 + c] = are[(size_t)(k0 + r) * lda + k0 + c];
-            Li[r * 65 + c] = aim[(size_t)(k0 + r) * lda + k0 + c];
+            cp_async4(&Lr[r * 65 + c], are + (size_t)(k0 + r) * lda + k0 + c, 4);
+            cp_async4(&Li[r * 65 + c], aim + (size_t)(k0 + r) * lda + k0 + c, 4);
         }
     __syncthreads();
     // load touched rows: warps over slots, lanes over columns
@@ -535,10 +537,12 @@ __global__ void __launch_bounds__(kSwapThreads) k_swap_trsm(float *a_re, float *
         const int row = s_row[sl];
         if (row < 0) continue;
         for (int c = lane; c < ncols; c += 32) {
-            Xr[sl * XP + c] = are[(size_t)row * lda + s_col[c]];
-            Xi[sl * XP + c] = aim[(size_t)row * lda + s_col[c]];
+            cp_async4(&Xr[sl * XP + c], are + (size_t)row * lda + s_col[c], 4);
+            cp_async4(&Xi[sl * XP + c], aim + (size_t)row * lda + s_col[c], 4);
         }
     }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
     if (tid < ncols) {
         const int c = tid;
@@ -1718,27 +1722,70 @@ int launch_panel_cluster_t(float *a_re, float *a_im, long long lda, long long a_
     static bool attr = false;
     if (!attr) {
         HBEM_CUDA(cudaFuncSetAttribute(k_panel_cluster<CS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(200 * 1024)));
+        if (CS > 8) HBEM_CUDA(cudaFuncSetAttribute(k_panel_cluster<CS>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
         attr = true;
     }
-    k_panel_cluster<CS><<<dim3(CS, batch), kPanelRowsThreads, smem, st>>>(a_re, a_im, lda, a_stride, n, c, w, R, piv,
-                                                                          piv_stride, info);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(CS, batch);
+    cfg.blockDim = dim3(kPanelRowsThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = CS;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    HBEM_CUDA(cudaLaunchKernelEx(&cfg, k_panel_cluster<CS>, a_re, a_im, lda, a_stride, n, c, w, R, piv, piv_stride,
+                                 info));
     HBEM_LAUNCH_CHECK("k_panel_cluster");
     return HBEM_OK;
 }
 
+// Largest cluster the panel kernel uses: 16 CTAs (a non-portable size) where
+// the device co-schedules a 16-CTA cluster of full-size panel CTAs, else 8.
+int panel_cluster_max(size_t smem_cap) {
+    static int cached = 0;
+    if (cached) return cached;
+    int cmax = 8;
+    if (cudaFuncSetAttribute(k_panel_cluster<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(200 * 1024)) ==
+            cudaSuccess &&
+        cudaFuncSetAttribute(k_panel_cluster<16>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(16, 1);
+        cfg.blockDim = dim3(kPanelRowsThreads);
+        cfg.dynamicSmemBytes = smem_cap;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = 16;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, k_panel_cluster<16>, &cfg) == cudaSuccess && clusters > 0)
+            cmax = 16;
+    }
+    cudaGetLastError();   // a refused query leaves no sticky error
+    cached = cmax;
+    return cached;
+}
+
 int launch_panel_cluster(float *a_re, float *a_im, long long lda, long long a_stride, int n, int c, int w, int *piv,
-                         long long piv_stride, int *info, int batch, size_t smem_cap, cudaStream_t st) {
+                         long long piv_stride, int *info, int batch, size_t smem_cap, int cmax, cudaStream_t st) {
     const int m = n - c;
     const size_t row_bytes = (size_t)(w + 1) * 8;
     const int rows_cap = (int)(smem_cap / row_bytes);
     int cs = 2;
-    while (cs < 8 && (long long)cs * rows_cap < m) cs *= 2;
+    while (cs < cmax && (long long)cs * rows_cap < m) cs *= 2;
     int R = (m + cs - 1) / cs;
     if (R < 64) R = 64;  // row j (< nb <= 64) always lives in CTA 0
     const size_t smem = (size_t)R * row_bytes;
     if (cs == 2) return launch_panel_cluster_t<2>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info, batch, R, smem, st);
     if (cs == 4) return launch_panel_cluster_t<4>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info, batch, R, smem, st);
-    return launch_panel_cluster_t<8>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info, batch, R, smem, st);
+    if (cs == 8) return launch_panel_cluster_t<8>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info, batch, R, smem, st);
+    return launch_panel_cluster_t<16>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info, batch, R, smem, st);
 }
 
 // Look-ahead streams of one caller stream: the factorisation chain runs on a
@@ -1857,11 +1904,13 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
     };
     HBEM_CUDA(cudaFuncSetAttribute(k_panel_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
     HBEM_CUDA(cudaFuncSetAttribute(k_swap_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSwapSmem));
+    const int cmax = panel_cluster_max(smem_cap);
     for (int b0 = 0; b0 < n; b0 += NB) {
         const int bw = std::min(NB, n - b0);
         // the whole block as one panel while one CTA holds it; else inner width
         // 32 while one CTA holds the sub-panel, else 16 while one CTA holds
-        // that, else 32 while an 8-CTA cluster holds it, else 16
+        // that, else 32 while an 8-CTA cluster holds it, else 16 (in a 16-CTA
+        // cluster where an 8-CTA one is too small and the device has them)
         const size_t rows = (size_t)(n - b0);
         const int want = tuning(HBEM_TUNE_LU_PANEL);
         int nbi;
@@ -1879,8 +1928,9 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
                 k_panel_rows<<<batch, kPanelRowsThreads, psmem, cs>>>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride,
                                                                   info);
                 rc = launched("k_panel_rows");
-            } else if ((size_t)(n - c) <= 8 * (smem_cap / ((size_t)(w + 1) * 8))) {
-                rc = launch_panel_cluster(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info, batch, smem_cap, cs);
+            } else if ((size_t)(n - c) <= (size_t)cmax * (smem_cap / ((size_t)(w + 1) * 8))) {
+                rc = launch_panel_cluster(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info, batch, smem_cap,
+                                          cmax, cs);
             } else {
                 k_panel<false><<<batch, kPanelThreads, 0, cs>>>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info);
                 rc = launched("k_panel");
@@ -1908,6 +1958,8 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
         }
         const int outside = n - bw;
         const int next_end = std::min(n, b0 + bw + NB);
+        // SMs the persistent tensor-core update leaves to the chain
+        const int tc_reserve = tuning(HBEM_TUNE_LU_RESERVE) - 1;
         const bool split = la && next_end < n;
         if (outside > 0) {
             // with look-ahead the chain swaps (and solves) only the next block's
@@ -1937,7 +1989,7 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
                 }
                 if (rc == HBEM_OK)
                     rc = tc ? launch_trailing_tc(tc, n, batch, b0, b0 + bw, next_end, n, a_re, a_im, lda, a_stride,
-                                                 status, la->bulk)
+                                                 status, la->bulk, tc_reserve)
                             : launch_trailing_simt(n, batch, b0, bw, b0 + bw, next_end, n, a_re, a_im, lda, a_stride,
                                                    la->bulk);
                 if (rc == HBEM_OK)

@@ -330,6 +330,9 @@ extern "C" int hbem_set_tuning(int key, int value) {
         case HBEM_TUNE_LU_LOOKAHEAD:
             if (value < 0 || value > 1) return fail(HBEM_ERR_ARG, "HBEM_TUNE_LU_LOOKAHEAD: 0 or 1");
             break;
+        case HBEM_TUNE_LU_RESERVE:
+            if (value < 0 || value > 1024) return fail(HBEM_ERR_ARG, "HBEM_TUNE_LU_RESERVE: 0 .. 1024");
+            break;
         default:
             return fail(HBEM_ERR_ARG, "hbem_set_tuning: unknown key " + std::to_string(key));
     }

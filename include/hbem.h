@@ -107,6 +107,9 @@ long long hbem_launch_count(void);
  *                            the panel is updated first and the rest of the
  *                            trailing update overlaps the next panel on a
  *                            second stream; 1: one stream)
+ *   HBEM_TUNE_LU_RESERVE:    SMs the look-ahead's persistent tensor-core
+ *                            update leaves to the factorisation chain
+ *                            (v >= 1: v - 1 SMs, at most half; 0: built-in)
  */
 #define HBEM_TUNE_ASM_MINBLOCKS 0
 #define HBEM_TUNE_LU_PANEL 1
@@ -114,7 +117,8 @@ long long hbem_launch_count(void);
 #define HBEM_TUNE_ASM_PAIRS 3
 #define HBEM_TUNE_DUFFY 4
 #define HBEM_TUNE_LU_LOOKAHEAD 5
-#define HBEM_TUNE_COUNT 6
+#define HBEM_TUNE_LU_RESERVE 6
+#define HBEM_TUNE_COUNT 7
 int hbem_set_tuning(int key, int value);
 int hbem_get_tuning(int key);
 

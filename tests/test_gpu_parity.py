@@ -245,6 +245,40 @@ def test_lu_bitwise_stable_under_concurrent_work(panel):
     assert rel(L @ np.triu(LU), PA) < 1e-5
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_lu_tall_panels_sixteen_cta_clusters(precision):
+    """n = 12200: the first 16-column panels (over 12 047 rows) outgrow an 8-CTA cluster's shared memory and
+    are factored in 16-CTA clusters.  The pivot is the first maximum of |re| + |im|, which bounds every
+    multiplier's modulus by sqrt(2); and the factors solve the system (residual in FP64)."""
+    import ctypes
+
+    lib = load_library()
+    n = 12200
+    g = torch.Generator(device="cuda").manual_seed(5)
+    A0r = torch.randn((1, n, n), device="cuda", generator=g)
+    A0i = torch.randn((1, n, n), device="cuda", generator=g)
+    Ar, Ai = A0r.clone(), A0i.clone()
+    piv, info = _factor(Ar, Ai, n, 1, precision)
+    torch.cuda.synchronize()
+    assert int(info.abs().sum()) == 0
+    low = torch.tril(torch.hypot(Ar[0], Ai[0]), -1)
+    assert float(low.max()) <= 2 ** 0.5 * (1 + 1e-6)
+    del low
+    br = torch.randn((1, n), device="cuda", generator=g)
+    bi = torch.randn((1, n), device="cuda", generator=g)
+    xr, xi = br.clone(), bi.clone()
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    P = lambda t: ctypes.c_void_p(t.data_ptr())
+    assert lib.hbem_lu_solve(n, 1, 1, P(Ar), P(Ai), n, n * n, P(piv), n, P(xr), P(xi), 1, n, 0, st) == 0
+    torch.cuda.synchronize()
+    A = torch.complex(A0r[0].double(), A0i[0].double())
+    x = torch.complex(xr[0].double(), xi[0].double())
+    b = torch.complex(br[0].double(), bi[0].double())
+    r = float(torch.linalg.norm(A @ x - b) / (torch.linalg.norm(A) * torch.linalg.norm(x)))
+    # normwise backward error: FP32 updates, or BF16x3 ones (16 significand bits per operand)
+    assert r < (1e-5 if precision == 0 else 1e-4)
+
+
 @pytest.mark.parametrize("n,batch", [(1043, 12), (2100, 3)])
 def test_lu_lookahead_equals_one_stream(n, batch):
     """The look-ahead schedule (next block updated on the chain, the rest of the trailing update overlapping the
