@@ -153,13 +153,16 @@ int launch_trailing_update(int n, int batch, int k0, int kw, int start, int col_
 //
 // The complex update C -= L U is one real GEMM: for a tile of 64 complex rows
 // the 128 MMA rows are [Lr, -Li] (real part) and [Li, Lr] (imaginary part)
-// against B = [Ur; Ui].  Each FP32 operand x is split into hi = bf16(x) and
-// lo = bf16(x - hi); A B ~ Ah Bh + Ah Bl + Al Bh is a single K = 3 * 2 * 64
-// = 384 contraction over the packed operands A3 = [Ah | Ah | Al] and
-// B3^T = [Bh | Bl | Bh] (both K-major, written by k_pack_*), tiles of 64
-// complex rows x 64 columns (k_trailing_tc: TMA ring, single-thread MMA
-// issue into a 128 x 64 FP32 TMEM accumulator, C staged through shared
-// memory by the epilogue warps).
+// against B = [Ur; Ui] (K = 2 x 64).  Each FP32 operand x is split into
+// hi = bf16(x) and lo = bf16(x - hi); A B ~ Ah Bh + Ah Bl + Al Bh.  The packed
+// operands hold each split once, A2 = [Ah | Al] and B2^T = [Bh | Bl] (both
+// K-major, K = 256, written by k_pack_*); the three products are three MMA
+// groups over the same shared-memory blocks.  Tiles are 64 complex rows x 64
+// columns; a CTA takes work units of consecutive column tiles of one row block
+// and keeps that row block's A2 (64 KB) resident in shared memory while B2
+// streams through a ring (k_trailing_tc: TMA, single-thread MMA issue into
+// 128 x 64 FP32 TMEM accumulators, C staged through shared memory by the
+// epilogue warps).
 // Every mbarrier wait is bounded; a timeout sets the status word and the CTA
 // returns after releasing its TMEM.
 // ===========================================================================
@@ -169,15 +172,16 @@ namespace {
 constexpr int kTcM = 128;          // MMA rows per tile (64 complex rows: real and imaginary parts)
 constexpr int kTcN = 64;           // columns per tile
 constexpr int kTcKBlk = 64;        // bf16 elements per K-block (128 bytes)
-constexpr int kTcK3 = 384;         // 3 x 2 x 64
-constexpr int kTcKBlocks = kTcK3 / kTcKBlk;
-constexpr int kTcStages = 4;       // operand ring
-constexpr int kTcABytes = kTcM * kTcKBlk * 2;
-constexpr int kTcBBytes = kTcN * kTcKBlk * 2;
-constexpr int kTcStageBytes = kTcABytes + kTcBBytes;
+constexpr int kTcK2 = 256;         // packed K: hi (2 x 64) then lo (2 x 64)
+constexpr int kTcABlk = kTcM * kTcKBlk * 2;      // one A K-block, 16 KB
+constexpr int kTcABytes = 4 * kTcABlk;           // resident A2 of a row block, 64 KB
+constexpr int kTcBBlk = kTcN * kTcKBlk * 2;      // one B K-block, 8 KB
+constexpr int kTcStageBytes = 2 * kTcBBlk;       // ring stage: Bh and Bl of one K half
+constexpr int kTcStages = 6;       // B ring: three tiles ahead
 constexpr int kTcCBytes = kTcM * kTcN * 4;   // one C tile staged in shared memory
 constexpr int kTcThreads = 320;    // warp 0: MMA issuer, warp 1: TMA producer, warps 2-9: C tiles
-constexpr size_t kTcSmem = (size_t)kTcStages * kTcStageBytes + 2 * kTcCBytes + 1024;
+constexpr size_t kTcSmem = (size_t)kTcABytes + (size_t)kTcStages * kTcStageBytes + 2 * kTcCBytes + 1024;
+static_assert(kTcSmem <= 227 * 1024, "tensor-core trailing update: shared memory");
 constexpr long long kSpinLimit = 1LL << 24;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -239,21 +243,48 @@ __device__ __forceinline__ bool epi_bar_or(bool pred) {
 struct TcTile {
     int mat, tm, tn;
 };
-__device__ __forceinline__ TcTile tc_tile(int t, int tiles_m, int tiles_n) {
-    const int per = tiles_m * tiles_n;
-    const int mat = t / per, rem = t - mat * per;
-    return {mat, rem / tiles_n, rem - (rem / tiles_n) * tiles_n};
-}
 
-// Persistent trailing update: each CTA walks tiles b, b + G, b + 2G, ... of
-// 64 complex rows x 64 columns (columns fastest, so consecutive tiles share
-// their L panel in L2).
-//   warp 1 (TMA producer): streams the six 64-wide K-blocks of A3 / B3 of
-//     every tile through a 4-stage ring, running ahead across tiles;
-//   warp 0 (MMA issuer): 4 x tcgen05.mma (M = 128, N = 64, K = 16) per block
-//     into one of two TMEM accumulators, releases ring slots with
-//     tcgen05.commit and signals "accumulator full";
-//   warps 2-5 (C tiles): prefetch the next tile's C (real rows, then
+// Work unit u = (matrix, row block, chunk of at most `chunk` column tiles);
+// this CTA's tiles in order: units blockIdx.x, + G, + 2G, ..., column tiles
+// ascending inside a unit.
+struct TcWalk {
+    int u, tn, tn_end, mat, tm;
+    bool valid;
+    int tiles_m, tiles_n, n_chunks, chunk, n_units, G;
+    __device__ void load() {
+        valid = u < n_units;
+        if (!valid) return;
+        const int row = u / n_chunks, c = u - row * n_chunks;
+        mat = row / tiles_m;
+        tm = row - mat * tiles_m;
+        tn = c * chunk;
+        tn_end = min(tiles_n, tn + chunk);
+    }
+    __device__ TcWalk(int u0, int tiles_m_, int tiles_n_, int n_chunks_, int chunk_, int n_units_, int G_)
+        : u(u0), tiles_m(tiles_m_), tiles_n(tiles_n_), n_chunks(n_chunks_), chunk(chunk_), n_units(n_units_),
+          G(G_) {
+        load();
+    }
+    __device__ bool last_of_unit() const { return tn + 1 == tn_end; }
+    __device__ TcTile tile() const { return {mat, tm, tn}; }
+    __device__ void advance() {
+        if (++tn == tn_end) {
+            u += G;
+            load();
+        }
+    }
+};
+
+// Persistent trailing update over work units (see TcWalk).
+//   warp 1 (TMA producer): per unit, the row block's four A2 K-blocks into the
+//     resident A buffer (after the MMAs of the previous unit released it),
+//     then per tile the two K halves of B2 (Bh and Bl blocks) through a
+//     6-stage ring, running ahead across tiles;
+//   warp 0 (MMA issuer): per K half, Ah Bh + Ah Bl + Al Bh as 3 x 4
+//     tcgen05.mma (M = 128, N = 64, K = 16) into one of two TMEM
+//     accumulators, releases ring slots with tcgen05.commit, signals
+//     "accumulator full", and releases A after a unit's last tile;
+//   warps 2-9 (C tiles): prefetch the next tile's C (real rows, then
 //     imaginary rows) into one of two shared buffers with cp.async, drain the
 //     finished accumulator into the current buffer (C - L U), hand the
 //     accumulator back, and write the tile out with coalesced stores.
@@ -265,17 +296,20 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
                                                                 const __grid_constant__ CUtensorMap tmB, float *a_re,
                                                                 float *a_im, long long lda, long long a_stride, int n,
                                                                 int start, int col_start, int col_end, int rows3,
-                                                                int cols_pad,
-                                                                int tiles_m, int tiles_n, int n_tiles, int *status) {
+                                                                int cols_pad, int tiles_m, int tiles_n, int n_chunks,
+                                                                int chunk, int n_units, int *status) {
     extern __shared__ uint8_t s_raw[];
     __shared__ uint64_t s_full[kTcStages], s_empty[kTcStages];
     __shared__ uint64_t s_acc_full[2], s_acc_empty[2];
+    __shared__ uint64_t s_a_full, s_a_empty;
     __shared__ uint64_t s_done;
     __shared__ uint32_t s_tmem;
     __shared__ volatile int s_fail;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(s_raw) + 1023) & ~(uintptr_t)1023);
-    float *sC0 = reinterpret_cast<float *>(base + (size_t)kTcStages * kTcStageBytes);
+    uint8_t *sA = base;
+    uint8_t *ring = base + kTcABytes;
+    float *sC0 = reinterpret_cast<float *>(ring + (size_t)kTcStages * kTcStageBytes);
     if (tid == 0) {
         s_fail = 0;
         for (int s = 0; s < kTcStages; ++s) {
@@ -286,6 +320,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_acc_full[b])));
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 8;" ::"r"(smem_u32(&s_acc_empty[b])));
         }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_a_full)));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_a_empty)));
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_done)));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -299,7 +335,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
     const int G = gridDim.x;
-    const int my_tiles = blockIdx.x < n_tiles ? (n_tiles - 1 - blockIdx.x) / G + 1 : 0;
 
     if (warp == 1) {
         // ---- TMA producer
@@ -308,32 +343,55 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
             for (int s = 0; s < kTcStages; ++s) last_use[s] = -1;
             bool ok = true;
             long long g = 0;   // ring position
-            for (int i = 0; i < my_tiles && ok; ++i) {
-                const TcTile tt = tc_tile(blockIdx.x + i * G, tiles_m, tiles_n);
-                const int row_a = tt.mat * rows3 + tt.tm * kTcM;
-                const int row_b = tt.mat * cols_pad + tt.tn * kTcN;
-                for (int kb = 0; kb < kTcKBlocks; ++kb, ++g) {
-                    const int s = (int)(g % kTcStages);
-                    const int u = (int)(g / kTcStages);
-                    if (u > 0 && !mbar_wait(smem_u32(&s_empty[s]), (u - 1) & 1, &s_fail)) { ok = false; break; }
-                    uint8_t *sa = base + (size_t)s * kTcStageBytes;
-                    uint8_t *sb = sa + kTcABytes;
-                    const uint32_t bar = smem_u32(&s_full[s]);
-                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
-                                 "r"(kTcStageBytes)
-                                 : "memory");
-                    asm volatile(
-                        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
-                        ::"r"(smem_u32(sa)), "l"(reinterpret_cast<uint64_t>(&tmA)), "r"(kb * kTcKBlk), "r"(row_a),
-                          "r"(bar)
-                        : "memory");
-                    asm volatile(
-                        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
-                        ::"r"(smem_u32(sb)), "l"(reinterpret_cast<uint64_t>(&tmB)), "r"(kb * kTcKBlk), "r"(row_b),
-                          "r"(bar)
-                        : "memory");
-                    last_use[s] = u;
+            int units = 0;     // A loads issued
+            TcWalk w(blockIdx.x, tiles_m, tiles_n, n_chunks, chunk, n_units, G);
+            while (w.valid && ok) {
+                // the previous unit's MMAs must be done with the resident A
+                if (units > 0 && !mbar_wait(smem_u32(&s_a_empty), (units - 1) & 1, &s_fail)) {
+                    ok = false;
+                    break;
                 }
+                {
+                    const uint32_t bar = smem_u32(&s_a_full);
+                    const int row_a = w.mat * rows3 + w.tm * kTcM;
+                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kTcABytes)
+                                 : "memory");
+                    for (int kb = 0; kb < 4; ++kb)
+                        asm volatile(
+                            "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                            ::"r"(smem_u32(sA + (size_t)kb * kTcABlk)), "l"(reinterpret_cast<uint64_t>(&tmA)),
+                              "r"(kb * kTcKBlk), "r"(row_a), "r"(bar)
+                            : "memory");
+                    ++units;
+                }
+                bool last;
+                do {
+                    const int row_b = w.mat * cols_pad + w.tn * kTcN;
+                    for (int kh = 0; kh < 2; ++kh, ++g) {
+                        const int s = (int)(g % kTcStages);
+                        const int u = (int)(g / kTcStages);
+                        if (u > 0 && !mbar_wait(smem_u32(&s_empty[s]), (u - 1) & 1, &s_fail)) { ok = false; break; }
+                        uint8_t *sb = ring + (size_t)s * kTcStageBytes;
+                        const uint32_t bar = smem_u32(&s_full[s]);
+                        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                                     "r"(kTcStageBytes)
+                                     : "memory");
+                        // Bh of this K half, then Bl
+                        asm volatile(
+                            "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                            ::"r"(smem_u32(sb)), "l"(reinterpret_cast<uint64_t>(&tmB)), "r"(kh * kTcKBlk),
+                              "r"(row_b), "r"(bar)
+                            : "memory");
+                        asm volatile(
+                            "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                            ::"r"(smem_u32(sb + kTcBBlk)), "l"(reinterpret_cast<uint64_t>(&tmB)),
+                              "r"(128 + kh * kTcKBlk), "r"(row_b), "r"(bar)
+                            : "memory");
+                        last_use[s] = u;
+                    }
+                    last = w.last_of_unit();
+                    w.advance();
+                } while (!last && ok);
             }
             if (!ok) {
                 s_fail = 1;
@@ -342,6 +400,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
             // every issued copy must land before the CTA may exit
             for (int s = 0; s < kTcStages; ++s)
                 if (last_use[s] >= 0) mbar_wait(smem_u32(&s_full[s]), last_use[s] & 1);
+            if (units > 0) mbar_wait(smem_u32(&s_a_full), (units - 1) & 1);
         }
     } else if (warp == 0) {
         // ---- MMA issuer
@@ -349,42 +408,65 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
             constexpr uint32_t idesc = umma_idesc_bf16(kTcM, kTcN);
             bool ok = true;
             long long g = 0;
-            for (int i = 0; i < my_tiles && ok; ++i) {
-                const int b = i & 1;
-                // the epilogue must have drained this accumulator (tile i - 2)
-                if (i >= 2 && !mbar_wait(smem_u32(&s_acc_empty[b]), ((i >> 1) - 1) & 1, &s_fail)) {
-                    ok = false;
-                    break;
-                }
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t acc_addr = tmem + (uint32_t)(b * kTcN);
-                for (int kb = 0; kb < kTcKBlocks; ++kb, ++g) {
-                    const int s = (int)(g % kTcStages);
-                    const int u = (int)(g / kTcStages);
-                    if (!mbar_wait(smem_u32(&s_full[s]), u & 1, &s_fail)) { ok = false; break; }
-                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    const uint32_t sa = smem_u32(base + (size_t)s * kTcStageBytes);
-                    const uint32_t sb = sa + kTcABytes;
-#pragma unroll
-                    for (int kk = 0; kk < kTcKBlk / 16; ++kk) {
-                        const uint64_t da = umma_desc_sw128(sa + kk * 32);
-                        const uint64_t db = umma_desc_sw128(sb + kk * 32);
-                        const uint32_t acc = (kb > 0 || kk > 0) ? 1u : 0u;
-                        asm volatile(
-                            "{\n\t.reg .pred p;\n\t"
-                            "setp.ne.b32 p, %4, 0;\n\t"
-                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-                            ::"r"(acc_addr), "l"(da), "l"(db), "r"(idesc), "r"(acc)
-                            : "memory");
+            int i = 0;        // tiles
+            int units = 0;
+            TcWalk w(blockIdx.x, tiles_m, tiles_n, n_chunks, chunk, n_units, G);
+            while (w.valid && ok) {
+                if (!mbar_wait(smem_u32(&s_a_full), units & 1, &s_fail)) { ok = false; break; }
+                const uint32_t a0 = smem_u32(sA);
+                bool last;
+                do {
+                    const int b = i & 1;
+                    // the epilogue must have drained this accumulator (tile i - 2)
+                    if (i >= 2 && !mbar_wait(smem_u32(&s_acc_empty[b]), ((i >> 1) - 1) & 1, &s_fail)) {
+                        ok = false;
+                        break;
                     }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t acc_addr = tmem + (uint32_t)(b * kTcN);
+                    for (int kh = 0; kh < 2; ++kh, ++g) {
+                        const int s = (int)(g % kTcStages);
+                        const int u = (int)(g / kTcStages);
+                        if (!mbar_wait(smem_u32(&s_full[s]), u & 1, &s_fail)) { ok = false; break; }
+                        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                        const uint32_t sb = smem_u32(ring + (size_t)s * kTcStageBytes);
+                        // (A block, B block): Ah Bh, Ah Bl, Al Bh of this K half
+                        const uint32_t pa[3] = {a0 + (uint32_t)(kh * kTcABlk), a0 + (uint32_t)(kh * kTcABlk),
+                                                a0 + (uint32_t)((2 + kh) * kTcABlk)};
+                        const uint32_t pb[3] = {sb, sb + (uint32_t)kTcBBlk, sb};
+#pragma unroll
+                        for (int pr = 0; pr < 3; ++pr) {
+#pragma unroll
+                            for (int kk = 0; kk < kTcKBlk / 16; ++kk) {
+                                const uint64_t da = umma_desc_sw128(pa[pr] + kk * 32);
+                                const uint64_t db = umma_desc_sw128(pb[pr] + kk * 32);
+                                const uint32_t acc = (kh > 0 || pr > 0 || kk > 0) ? 1u : 0u;
+                                asm volatile(
+                                    "{\n\t.reg .pred p;\n\t"
+                                    "setp.ne.b32 p, %4, 0;\n\t"
+                                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                                    ::"r"(acc_addr), "l"(da), "l"(db), "r"(idesc), "r"(acc)
+                                    : "memory");
+                            }
+                        }
+                        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                         smem_u32(&s_empty[s]))
+                                     : "memory");
+                    }
+                    if (!ok) break;
                     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                                     smem_u32(&s_empty[s]))
+                                     smem_u32(&s_acc_full[b]))
                                  : "memory");
-                }
+                    ++i;
+                    last = w.last_of_unit();
+                    w.advance();
+                } while (!last);
                 if (!ok) break;
+                // A may be replaced once this unit's MMAs have completed
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                                 smem_u32(&s_acc_full[b]))
+                                 smem_u32(&s_a_empty))
                              : "memory");
+                ++units;
             }
             if (!ok) {
                 s_fail = 1;
@@ -405,8 +487,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
         const int h = (warp - 2) >> 2;
         const int gq = et & 15, r_first = et >> 4;
         auto sidx = [](int r, int c) { return r * kTcN + ((((c >> 2) ^ (r & 7)) << 2) | (c & 3)); };
-        auto prefetch = [&](int t, float *sC) {
-            const TcTile tt = tc_tile(t, tiles_m, tiles_n);
+        auto prefetch = [&](const TcTile tt, float *sC) {
             const int row_c0 = start + tt.tm * 64, gcol = col_start + tt.tn * kTcN + 4 * gq;
             if (gcol >= col_end) {
                 asm volatile("cp.async.commit_group;" ::: "memory");
@@ -434,12 +515,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
             }
             asm volatile("cp.async.commit_group;" ::: "memory");
         };
-        if (my_tiles > 0) prefetch(blockIdx.x, sC0);
-        for (int i = 0; i < my_tiles; ++i) {
+        TcWalk cur(blockIdx.x, tiles_m, tiles_n, n_chunks, chunk, n_units, G);
+        TcWalk nxt = cur;
+        if (nxt.valid) {
+            prefetch(nxt.tile(), sC0);
+            nxt.advance();
+        }
+        for (int i = 0; cur.valid; ++i) {
             const int b = i & 1;
             float *sC = sC0 + (size_t)b * (kTcM * kTcN);
-            if (i + 1 < my_tiles) {
-                prefetch(blockIdx.x + (i + 1) * G, sC0 + (size_t)(b ^ 1) * (kTcM * kTcN));
+            if (nxt.valid) {
+                prefetch(nxt.tile(), sC0 + (size_t)(b ^ 1) * (kTcM * kTcN));
+                nxt.advance();
                 asm volatile("cp.async.wait_group 1;" ::: "memory");
             } else {
                 asm volatile("cp.async.wait_group 0;" ::: "memory");
@@ -487,7 +574,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
                 asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&s_acc_empty[b])) : "memory");
             epi_bar();   // the whole tile is drained
             {
-                const TcTile tt = tc_tile(blockIdx.x + i * G, tiles_m, tiles_n);
+                const TcTile tt = cur.tile();
                 const int row_c0 = start + tt.tm * 64, gcol = col_start + tt.tn * kTcN + 4 * gq;
                 if (gcol < col_end) {
                     const bool full4 = gcol + 3 < col_end;
@@ -510,6 +597,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
                 }
             }
             epi_bar();   // buffer b may be refilled by the prefetch of tile i + 2
+            cur.advance();
         }
         asm volatile("cp.async.wait_all;" ::: "memory");
     }
@@ -533,14 +621,13 @@ __global__ void k_pack_a(const float *a_re, const float *a_im, long long lda, lo
         li = a_im[(size_t)mat * a_stride + (size_t)(start + i) * lda + k0 + k];
     }
     const int t = i >> 6, rl = i & 63;
-    __nv_bfloat16 *re_row = A3 + ((size_t)mat * rows3 + (size_t)t * 128 + rl) * kTcK3;
-    __nv_bfloat16 *im_row = re_row + (size_t)64 * kTcK3;
+    __nv_bfloat16 *re_row = A3 + ((size_t)mat * rows3 + (size_t)t * 128 + rl) * kTcK2;
+    __nv_bfloat16 *im_row = re_row + (size_t)64 * kTcK2;
     auto put = [](__nv_bfloat16 *row, int k2, float x) {
         const __nv_bfloat16 h = __float2bfloat16_rn(x);
         const __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
         row[k2] = h;
-        row[128 + k2] = h;
-        row[256 + k2] = l;
+        row[128 + k2] = l;
     };
     put(re_row, k, lr);
     put(re_row, 64 + k, -li);
@@ -560,13 +647,12 @@ __global__ void k_pack_b(const float *a_re, const float *a_im, long long lda, lo
         ur = a_re[(size_t)mat * a_stride + (size_t)(k0 + k) * lda + start + j];
         ui = a_im[(size_t)mat * a_stride + (size_t)(k0 + k) * lda + start + j];
     }
-    __nv_bfloat16 *row = B3 + ((size_t)mat * cols_pad + j) * kTcK3;
+    __nv_bfloat16 *row = B3 + ((size_t)mat * cols_pad + j) * kTcK2;
     auto put = [&](int k2, float x) {
         const __nv_bfloat16 h = __float2bfloat16_rn(x);
         const __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
         row[k2] = h;
         row[128 + k2] = l;
-        row[256 + k2] = h;
     };
     put(k, ur);
     put(64 + k, ui);
@@ -593,8 +679,8 @@ EncodeTiledFn encode_fn() {
 int make_map(CUtensorMap *map, void *ptr, long long rows, int box_rows) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return fail(HBEM_ERR_CUDA, "cuTensorMapEncodeTiled entry point unavailable");
-    const cuuint64_t dims[2] = {(cuuint64_t)kTcK3, (cuuint64_t)rows};
-    const cuuint64_t strides[1] = {(cuuint64_t)kTcK3 * 2};
+    const cuuint64_t dims[2] = {(cuuint64_t)kTcK2, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)kTcK2 * 2};
     const cuuint32_t box[2] = {(cuuint32_t)kTcKBlk, (cuuint32_t)box_rows};
     const cuuint32_t estr[2] = {1, 1};
     CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, ptr, dims, strides, box, estr,
@@ -620,8 +706,8 @@ int tc_workspace_create(int n, int batch, TcWorkspace **out, cudaStream_t st) {
     w->rows3 = ((n + 63) / 64) * kTcM;
     w->cols_pad = ((n + kTcN - 1) / kTcN) * kTcN;
     w->batch = batch;
-    cudaError_t e = cudaMallocAsync((void **)&w->A3, (size_t)batch * w->rows3 * kTcK3 * 2, st);
-    if (e == cudaSuccess) e = cudaMallocAsync((void **)&w->B3, (size_t)batch * w->cols_pad * kTcK3 * 2, st);
+    cudaError_t e = cudaMallocAsync((void **)&w->A3, (size_t)batch * w->rows3 * kTcK2 * 2, st);
+    if (e == cudaSuccess) e = cudaMallocAsync((void **)&w->B3, (size_t)batch * w->cols_pad * kTcK2 * 2, st);
     if (e != cudaSuccess) {
         if (w->A3) cudaFreeAsync(w->A3, st);
         delete w;
@@ -675,13 +761,21 @@ int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int 
         HBEM_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
         HBEM_CUDA(cudaFuncSetAttribute(k_trailing_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
     }
-    const long long total = (long long)tiles_m * tiles_n * batch;
-    if (total > 0x7fffffffLL) return fail(HBEM_ERR_ARG, "trailing update: too many tiles");
     const int ctas = n_sm - std::min(std::max(reserve_sms, 0), n_sm / 2);
-    const int grid = (int)std::min<long long>(total, ctas);
+    // work units of `chunk` consecutive column tiles: about ten units per CTA
+    // where the tiles allow (load balance), else one tile per unit
+    const long long total = (long long)tiles_m * tiles_n * batch;
+    long long want = total / (10LL * ctas);
+    int chunk = (int)std::max(1LL, std::min<long long>(want, tiles_n));
+    const int n_chunks = (tiles_n + chunk - 1) / chunk;
+    chunk = (tiles_n + n_chunks - 1) / n_chunks;
+    const long long units = (long long)batch * tiles_m * n_chunks;
+    if (units > 0x7fffffffLL) return fail(HBEM_ERR_ARG, "trailing update: too many tiles");
+    if ((long long)(n_chunks - 1) * chunk >= tiles_n) return fail(HBEM_ERR_STATE, "trailing update: empty work unit");
+    const int grid = (int)std::min<long long>(units, ctas);
     k_trailing_tc<<<grid, kTcThreads, kTcSmem, st>>>(w->ma, w->mb, a_re, a_im, lda, a_stride, n, start, col_start,
-                                                    col_end, w->rows3, w->cols_pad, tiles_m, tiles_n, (int)total,
-                                                    status);
+                                                    col_end, w->rows3, w->cols_pad, tiles_m, tiles_n, n_chunks, chunk,
+                                                    (int)units, status);
     HBEM_LAUNCH_CHECK("k_trailing_tc");
     return HBEM_OK;
 }
