@@ -607,9 +607,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kTcN));
 }
 
-// Pack L21 (rows start..n, cols k0..k0+64) into A3 (K-major, bf16 hi/lo).
+// Pack L21 (rows start..n, cols k0..k0+64) into A2 (K-major, bf16 hi/lo).
 __global__ void k_pack_a(const float *a_re, const float *a_im, long long lda, long long a_stride, int n, int start,
-                         int k0, int rows3, int rows_used, __nv_bfloat16 *A3) {
+                         int k0, int rows3, int rows_used, __nv_bfloat16 *A2) {
     const int mat = blockIdx.z;
     const int i = blockIdx.x * blockDim.y + threadIdx.y;  // complex row offset
     const int k = threadIdx.x;                            // 0..63
@@ -621,7 +621,7 @@ __global__ void k_pack_a(const float *a_re, const float *a_im, long long lda, lo
         li = a_im[(size_t)mat * a_stride + (size_t)(start + i) * lda + k0 + k];
     }
     const int t = i >> 6, rl = i & 63;
-    __nv_bfloat16 *re_row = A3 + ((size_t)mat * rows3 + (size_t)t * 128 + rl) * kTcK2;
+    __nv_bfloat16 *re_row = A2 + ((size_t)mat * rows3 + (size_t)t * 128 + rl) * kTcK2;
     __nv_bfloat16 *im_row = re_row + (size_t)64 * kTcK2;
     auto put = [](__nv_bfloat16 *row, int k2, float x) {
         const __nv_bfloat16 h = __float2bfloat16_rn(x);
@@ -635,27 +635,46 @@ __global__ void k_pack_a(const float *a_re, const float *a_im, long long lda, lo
     put(im_row, 64 + k, lr);
 }
 
-// Pack U12 (rows k0..k0+64, cols start..col_end) into B3^T (K-major).
-__global__ void k_pack_b(const float *a_re, const float *a_im, long long lda, long long a_stride, int start,
-                         int col_end, int k0, int cols_pad, int cols_used, __nv_bfloat16 *B3) {
+// Pack U12 (rows k0..k0+64, cols start..col_end) into B2^T (K-major, bf16 hi/lo).
+__global__ void __launch_bounds__(256) k_pack_b(const float *a_re, const float *a_im, long long lda,
+                                                long long a_stride, int start, int col_end, int k0, int cols_pad,
+                                                int cols_used, __nv_bfloat16 *B2) {
+    // 64 columns per CTA: the 64 x 64 block of U12 is read along its rows
+    // (coalesced), transposed in shared memory and written as 64 packed
+    // K-major rows of 512 bytes (consecutive threads, consecutive bf16 pairs)
+    __shared__ float s_ur[64][65], s_ui[64][65];
     const int mat = blockIdx.z;
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;  // column offset
-    const int k = blockIdx.y;                             // 0..63
-    if (j >= cols_used) return;
-    float ur = 0.f, ui = 0.f;
-    if (start + j < col_end) {
-        ur = a_re[(size_t)mat * a_stride + (size_t)(k0 + k) * lda + start + j];
-        ui = a_im[(size_t)mat * a_stride + (size_t)(k0 + k) * lda + start + j];
+    const int j0 = blockIdx.x * 64;
+    const int tid = threadIdx.x;
+    const float *ure = a_re + (size_t)mat * a_stride + (size_t)k0 * lda + start;
+    const float *uim = a_im + (size_t)mat * a_stride + (size_t)k0 * lda + start;
+    for (int e = tid; e < 64 * 64; e += 256) {
+        const int k = e >> 6, jj = e & 63, j = j0 + jj;
+        const bool in = start + j < col_end;
+        s_ur[k][jj] = in ? ure[(size_t)k * lda + j] : 0.f;
+        s_ui[k][jj] = in ? uim[(size_t)k * lda + j] : 0.f;
     }
-    __nv_bfloat16 *row = B3 + ((size_t)mat * cols_pad + j) * kTcK2;
-    auto put = [&](int k2, float x) {
-        const __nv_bfloat16 h = __float2bfloat16_rn(x);
-        const __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
-        row[k2] = h;
-        row[128 + k2] = l;
-    };
-    put(k, ur);
-    put(64 + k, ui);
+    __syncthreads();
+    // pair p of a packed row covers K entries 2p, 2p + 1:
+    // [0, 64) hi(Ur), [64, 128) hi(Ui), [128, 192) lo(Ur), [192, 256) lo(Ui)
+    const int p = tid & 127;
+    const int kk = 2 * p;
+    const int part = kk >> 6, k = kk & 63;   // part: 0 hi Ur, 1 hi Ui, 2 lo Ur, 3 lo Ui
+    for (int jj = tid >> 7; jj < 64; jj += 2) {
+        const int j = j0 + jj;
+        if (j >= cols_used) break;
+        const float x0 = (part & 1) ? s_ui[k][jj] : s_ur[k][jj];
+        const float x1 = (part & 1) ? s_ui[k + 1][jj] : s_ur[k + 1][jj];
+        __nv_bfloat16 v0 = __float2bfloat16_rn(x0), v1 = __float2bfloat16_rn(x1);
+        if (part >= 2) {
+            v0 = __float2bfloat16_rn(x0 - __bfloat162float(v0));
+            v1 = __float2bfloat16_rn(x1 - __bfloat162float(v1));
+        }
+        __nv_bfloat162 pr;
+        pr.x = v0;
+        pr.y = v1;
+        *reinterpret_cast<__nv_bfloat162 *>(B2 + ((size_t)mat * cols_pad + j) * kTcK2 + kk) = pr;
+    }
 }
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
@@ -695,7 +714,7 @@ int make_map(CUtensorMap *map, void *ptr, long long rows, int box_rows) {
 // Packed-operand workspace and tensor maps for one factorisation: sized for
 // the first (largest) trailing update and reused by the later, smaller ones.
 struct TcWorkspace {
-    __nv_bfloat16 *A3 = nullptr, *B3 = nullptr;
+    __nv_bfloat16 *A2 = nullptr, *B2 = nullptr;
     int rows3 = 0, cols_pad = 0, batch = 0;
     CUtensorMap ma, mb;
 };
@@ -706,18 +725,18 @@ int tc_workspace_create(int n, int batch, TcWorkspace **out, cudaStream_t st) {
     w->rows3 = ((n + 63) / 64) * kTcM;
     w->cols_pad = ((n + kTcN - 1) / kTcN) * kTcN;
     w->batch = batch;
-    cudaError_t e = cudaMallocAsync((void **)&w->A3, (size_t)batch * w->rows3 * kTcK2 * 2, st);
-    if (e == cudaSuccess) e = cudaMallocAsync((void **)&w->B3, (size_t)batch * w->cols_pad * kTcK2 * 2, st);
+    cudaError_t e = cudaMallocAsync((void **)&w->A2, (size_t)batch * w->rows3 * kTcK2 * 2, st);
+    if (e == cudaSuccess) e = cudaMallocAsync((void **)&w->B2, (size_t)batch * w->cols_pad * kTcK2 * 2, st);
     if (e != cudaSuccess) {
-        if (w->A3) cudaFreeAsync(w->A3, st);
+        if (w->A2) cudaFreeAsync(w->A2, st);
         delete w;
         return cuda_fail(e, "tensor-core workspace");
     }
-    int rc = make_map(&w->ma, w->A3, (long long)batch * w->rows3, kTcM);
-    if (rc == HBEM_OK) rc = make_map(&w->mb, w->B3, (long long)batch * w->cols_pad, kTcN);
+    int rc = make_map(&w->ma, w->A2, (long long)batch * w->rows3, kTcM);
+    if (rc == HBEM_OK) rc = make_map(&w->mb, w->B2, (long long)batch * w->cols_pad, kTcN);
     if (rc != HBEM_OK) {
-        cudaFreeAsync(w->A3, st);
-        cudaFreeAsync(w->B3, st);
+        cudaFreeAsync(w->A2, st);
+        cudaFreeAsync(w->B2, st);
         delete w;
         return rc;
     }
@@ -727,8 +746,8 @@ int tc_workspace_create(int n, int batch, TcWorkspace **out, cudaStream_t st) {
 
 void tc_workspace_destroy(TcWorkspace *w, cudaStream_t st) {
     if (!w) return;
-    cudaFreeAsync(w->A3, st);
-    cudaFreeAsync(w->B3, st);
+    cudaFreeAsync(w->A2, st);
+    cudaFreeAsync(w->B2, st);
     delete w;
 }
 
@@ -745,13 +764,13 @@ int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int 
     // packed rows use the workspace's fixed per-matrix pitch (rows3 / cols_pad)
     {
         dim3 blk(64, 4), grd((tiles_m * 64 + 3) / 4, 1, batch);
-        k_pack_a<<<grd, blk, 0, st>>>(a_re, a_im, lda, a_stride, n, start, k0, w->rows3, tiles_m * 64, w->A3);
+        k_pack_a<<<grd, blk, 0, st>>>(a_re, a_im, lda, a_stride, n, start, k0, w->rows3, tiles_m * 64, w->A2);
         HBEM_LAUNCH_CHECK("k_pack_a");
     }
     {
-        dim3 grd((tiles_n * kTcN + 127) / 128, 64, batch);
-        k_pack_b<<<grd, 128, 0, st>>>(a_re, a_im, lda, a_stride, col_start, col_end, k0, w->cols_pad, tiles_n * kTcN,
-                                      w->B3);
+        dim3 grd((tiles_n * kTcN + 63) / 64, 1, batch);
+        k_pack_b<<<grd, 256, 0, st>>>(a_re, a_im, lda, a_stride, col_start, col_end, k0, w->cols_pad, tiles_n * kTcN,
+                                      w->B2);
         HBEM_LAUNCH_CHECK("k_pack_b");
     }
     static int n_sm = 0;
