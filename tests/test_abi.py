@@ -55,3 +55,38 @@ def test_session_requires_cuda_without_fallback(monkeypatch):
 
     with pytest.raises(native.BackendUnavailable):
         native.NativeSession(golden_buffers("tiny"))
+
+
+def test_tuning_knobs_validate_and_read_back():
+    """hbem_set_tuning accepts each knob's documented values (0 = built-in choice), rejects the rest with a
+    message naming the knob, and hbem_get_tuning reads the value back; host-only, no device needed."""
+    lib = native.load_library()
+    text = (REPO / "include" / "hbem.h").read_text()
+    keys = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define (HBEM_TUNE_\w+) (\d+)", text)}
+    count = keys.pop("HBEM_TUNE_COUNT")
+    assert sorted(keys.values()) == list(range(count))
+    valid = {
+        "HBEM_TUNE_ASM_MINBLOCKS": ([0, 2, 3], [1, 4]),
+        "HBEM_TUNE_LU_PANEL": ([0, 16, 32, 64], [8, 48, 128]),
+        "HBEM_TUNE_LU_SOLVE": ([0, 1, 2, 3], [-1, 4]),
+        "HBEM_TUNE_ASM_PAIRS": ([0, 1], [2]),
+        "HBEM_TUNE_DUFFY": ([0, 1, 2], [3]),
+        "HBEM_TUNE_LU_LOOKAHEAD": ([0, 1], [2]),
+        "HBEM_TUNE_LU_RESERVE": ([0, 1, 17, 1024], [-1, 1025]),
+    }
+    assert set(valid) == set(keys)
+    try:
+        for name, key in keys.items():
+            ok, bad = valid[name]
+            for v in ok:
+                assert lib.hbem_set_tuning(key, v) == 0, (name, v)
+                assert lib.hbem_get_tuning(key) == v
+            for v in bad:
+                assert lib.hbem_set_tuning(key, v) == -1, (name, v)
+                assert name in native.last_error(lib)
+                assert lib.hbem_get_tuning(key) == ok[-1]   # a rejected value changes nothing
+        assert lib.hbem_set_tuning(count, 0) == -1
+        assert "unknown key" in native.last_error(lib)
+    finally:
+        for key in keys.values():
+            lib.hbem_set_tuning(key, 0)
