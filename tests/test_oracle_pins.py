@@ -7,6 +7,9 @@
 * Pair blocks: FP64 level-4 subdivided quadrature of the reference test helper
   (:230-350) reproduced exactly, and approached by the regular rule off contact.
 * Pulsating sphere: surface pressure vs the analytic Z/(rho c) = ika/(ika-1).
+* Baffled circular piston: the half-space Rayleigh field of a uniform aperture
+  Neumann value vs the closed-form on-axis pressure (reference tests
+  tests/test_native_coupled_ib_validation.py:423-548).
 """
 from __future__ import annotations
 
@@ -97,6 +100,37 @@ def test_pulsating_sphere_matches_analytic(freq):
     fld = o.field(k, p, q, np.array([[0.0], [0.0], [2.0]]))
     pr = pa * (a / 2.0) * np.exp(1j * k * (2.0 - a))
     assert abs(fld[0] - pr) / abs(pr) < 2e-2
+
+
+@pytest.mark.parametrize("freq", [1000.0, 4000.0])
+def test_rayleigh_disc_matches_analytic_baffled_piston(freq):
+    """A uniform aperture Neumann value q over the flush mouth disc (radius a, z = 0) of a coupled-baffle
+    horn radiates, through the oracle's restatement of the reference's half-space field p = -2 sum over
+    the aperture of int G q (main.swift:1397-1444, e^{+ikr} convention), the on-axis pressure
+    p(z) = -2 q / (4 pi) int_disc e^{ikr} / r dA = -q (e^{ik sqrt(z^2 + a^2)} - e^{ikz}) / (ik).
+    The faceted disc (inscribed polygon rings, edge a / 15) and the 6-point rule leave ~1e-3."""
+    from hornlab_metal_bem_b200 import generators as G
+    from hornlab_metal_bem_b200.geometry import build_geometry_buffers
+    from hornlab_metal_bem_b200.mesh import make_pure_function_spaces
+
+    spec = G.HornSpec(edge=0.01)
+    m = G.baffled_horn(spec, quarter=False, aperture_tag=12)
+    p1, dp0 = make_pure_function_spaces(m.grid)
+    buf = build_geometry_buffers(m.grid, m.physical_tags, p1, dp0)
+    o = Oracle(buf, 0, "f64")
+    ap = o.aperture_triangles(12)
+    a = spec.mouth_radius
+    k = 2 * np.pi * freq / 343.0
+    q0 = 1j * 1.2041 * 2 * np.pi * freq
+    z = np.array([1.0, 2.0, 5.0, 2.0 / a]) * a
+    obs = np.stack([np.zeros_like(z), np.zeros_like(z), z])
+    got = o.rayleigh(ap, k, np.full(ap.shape[0], q0, np.complex128), obs)
+    want = -q0 * (np.exp(1j * k * np.hypot(z, a)) - np.exp(1j * k * z)) / (1j * k)
+    assert np.linalg.norm(got - want) / np.linalg.norm(want) < 5e-3
+    assert np.all(np.abs(got - want) / np.abs(want) < 1e-2)
+    # below the baffle plane the half-space field is zero
+    below = o.rayleigh(ap, k, np.full(ap.shape[0], q0, np.complex128), np.array([[0.0], [0.0], [-0.1]]))
+    assert below[0] == 0
 
 
 def test_f32_oracle_tracks_f64_oracle():
