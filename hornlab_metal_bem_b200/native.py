@@ -124,6 +124,25 @@ def last_error(lib: ctypes.CDLL | None = None) -> str:
     return buf.value.decode(errors="replace")
 
 
+def _case_flags(k_re: float, k_im: float, *, robin: bool = False, coupled: bool = False,
+                field_k: float | None = None) -> dict:
+    """Per-case capability keys of the reference helper's case results, present only when they apply
+    (``main.swift:9749-9761``): ``complex_k`` with ``assembly_k_imag_f32`` for a complex wavenumber,
+    ``robin_boundary`` (and ``field_uses_total_neumann`` without the coupled baffle) for Robin faces,
+    ``field_k_real_f32`` when the field wavenumber differs from the assembly one."""
+    out: dict = {}
+    if k_im != 0.0:
+        out["assembly_k_imag_f32"] = float(k_im)
+        out["complex_k"] = True
+    if robin:
+        out["robin_boundary"] = True
+        if not coupled:
+            out["field_uses_total_neumann"] = True
+    if field_k is not None and float(field_k) != float(k_re):
+        out["field_k_real_f32"] = float(field_k)
+    return out
+
+
 def check(status: int, what: str, lib: ctypes.CDLL | None = None) -> int:
     if status < 0:
         raise RuntimeError(f"{what} failed ({status}): {last_error(lib)}")
@@ -409,6 +428,7 @@ class NativeSession:
                 "dense_solve_rcond": float(rcond[f]) if rcond is not None and info[f] == 0 else None,
                 "assembly_mode": "corrected",
                 "duffy_pairs": None,
+                **_case_flags(float(k_re[f]), 0.0 if k_im is None else float(k_im[f])),
             }
             results.append(CaseResult(
                 frequency_hz=float(freqs[f]),
@@ -535,7 +555,8 @@ class NativeSession:
                              "refine_residual_rel": float(out_res[f]) if mixed else None,
                              "dense_solve_rcond": (float(out_rc[f]) if compute_rcond and out_info[f] == 0 else None),
                              "robin_tags": sorted(int(t) for t in per_freq[f]),
-                             "assembly_mode": "corrected"},
+                             "assembly_mode": "corrected",
+                             **_case_flags(float(k_re[f]), float(k_im[f]), robin=True)},
             ))
         return results
 
@@ -623,7 +644,9 @@ class NativeSession:
                              "refine_residual_rel": float(cat["resid"][f]) if mixed else None,
                              "dense_solve_rcond": (float(cat["rcond"][f]) if "rcond" in cat and cat["info"][f] == 0
                                                    else None),
-                             "assembly_mode": "corrected"},
+                             "assembly_mode": "corrected",
+                             **_case_flags(float(k_re[f]), 0.0 if k_im is None else float(k_im[f]), coupled=True,
+                                           field_k=float(kf[f]))},
             ))
         return out
 
