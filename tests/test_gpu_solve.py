@@ -193,22 +193,34 @@ def test_complex_k_suppresses_unit_sphere_resonance():
 
 
 def test_multi_source_equals_sequential_solves():
-    """solve_multi_source (one session, one result per velocity-source dict) equals separate solve() calls
-    per source (the reference's multi-source parity, tests/test_multi_source_parity.py:113-141, rtol 2e-4)."""
+    """solve_multi_source (one session, one result per velocity-source dict) equals separate
+    solve_frequencies() calls per source (the reference's multi-source parity,
+    tests/test_multi_source_parity.py:113-141, rtol 2e-4): unit sphere with driven caps at +z (tag 2) and
+    -z (tag 3); both sources name both tags (one at zero velocity), so every run infers the same frame and
+    records the cross-source cap averages."""
     from hornlab_metal_bem_b200.mesh import mesh_from_arrays
 
-    sphere = G.icosphere(2, 0.1)
+    sphere = G.icosphere(2, 1.0)
     v = sphere.grid.vertices.T.copy()
     f = sphere.grid.elements.T.copy()
-    tags = np.where(v[f].mean(axis=1)[:, 2] > 0.05, 2, 1).astype(np.int32)
-    mesh = mesh_from_arrays(v, f, tags, physical_groups={1: "body", 2: "cap"})
-    sources = [{2: 1.0}, {1: 0.25, 2: 1.0}]
-    base = dict(freq_min_hz=300.0, freq_max_hz=3000.0, freq_count=4,
-                observation=hb.ObservationConfig(planes=["horizontal", "vertical"], angle_count=13))
-    multi = hb.solve_multi_source(mesh, sources, hb.native_config(velocity_sources=sources[0], **base))
+    cz = v[f].mean(axis=1)[:, 2]
+    tags = np.where(cz > 0.55, 2, np.where(cz < -0.55, 3, 1)).astype(np.int32)
+    mesh = mesh_from_arrays(v, f, tags, physical_groups={1: "rigid", 2: "cap_top", 3: "cap_bottom"})
+    probe = hb.ObservationConfig(planes=["probe"], angle_count=3, custom_points={
+        "probe": np.array([[0.0, 0.0, 2.2], [0.6, 0.0, 2.1], [0.0, -0.4, 2.4]])})
+    sources = [{2: 1.0, 3: 0.0}, {3: 1.0, 2: 0.0}]
+    freqs = [180.0, 240.0, 320.0]
+    multi = hb.solve_multi_source(mesh, sources, hb.native_config(velocity_sources=sources[0], observation=probe,
+                                                                  return_surface_pressure=True),
+                                  frequencies_hz=freqs)
     assert len(multi) == 2
+    tol = dict(rtol=2e-4, atol=1e-6)
     for src, got in zip(sources, multi):
-        ref = hb.solve(mesh, hb.native_config(velocity_sources=src, **base))
-        np.testing.assert_allclose(got.pressure_complex, ref.pressure_complex, rtol=2e-4,
-                                   atol=2e-4 * np.abs(ref.pressure_complex).max())
-        np.testing.assert_allclose(got.impedance, ref.impedance, rtol=2e-4)
+        ref = hb.solve_frequencies(mesh, freqs, hb.native_config(velocity_sources=src, observation=probe,
+                                                                 return_surface_pressure=True))
+        np.testing.assert_allclose(got.pressure_complex, ref.pressure_complex, **tol)
+        np.testing.assert_allclose(got.impedance, ref.impedance, **tol)
+        assert set(got.surface_pressure_avg) == set(ref.surface_pressure_avg) == {2, 3}
+        for tag, vals in ref.surface_pressure_avg.items():
+            np.testing.assert_allclose(got.surface_pressure_avg[tag], vals, **tol)
+        np.testing.assert_allclose(got.surface_pressure_complex, ref.surface_pressure_complex, **tol)
