@@ -1227,7 +1227,8 @@ int launch_duffy(Session &s, int n_freq, const float *k_re, const float *k_im, c
         for (int f = 0; f < nf; ++f) ck |= a.ki[f] != 0.f;
         a.nf = nf;
         // variant: 1 = one wavenumber per warp (3 CTAs/SM), 2 = two (2 CTAs/SM, the default:
-        // 10.6 vs 11.3 ms on the 1043-dof yz+xz horn at 40 wavenumbers)
+        // the faster one on the 1043-dof yz+xz horn at 40 wavenumbers, where it shares the
+        // per-point geometry between the two wavenumbers)
         const int var = tuning(HBEM_TUNE_DUFFY) == 1 ? 1 : 2;
         dim3 grid((s.n_pairs + 7) / 8, (nf + var - 1) / var);
         if (var == 2) {

@@ -29,3 +29,16 @@ def test_callback_rejects_non_passive_or_non_finite(bad):
     cfg = hb.native_config(impedance_source_callback=lambda f: {1: bad})
     with pytest.raises(ValueError):
         impedance_sources_for_frequencies(TAGS, [100.0], cfg)
+
+
+def test_case_flags_follow_the_reference_helper():
+    """Per-case capability keys appear only when they apply, as the reference helper writes them
+    (main.swift:9749-9761)."""
+    from hornlab_metal_bem_b200.native import _case_flags
+
+    assert _case_flags(3.0, 0.0) == {}
+    assert _case_flags(3.0, 0.06) == {"assembly_k_imag_f32": 0.06, "complex_k": True}
+    assert _case_flags(3.0, 0.0, robin=True) == {"robin_boundary": True, "field_uses_total_neumann": True}
+    assert _case_flags(3.0, 0.0, robin=True, coupled=True) == {"robin_boundary": True}
+    assert _case_flags(3.0, 0.0, coupled=True, field_k=3.0) == {}
+    assert _case_flags(3.0, 0.0, coupled=True, field_k=2.5) == {"field_k_real_f32": 2.5}
