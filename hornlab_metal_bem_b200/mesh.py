@@ -205,7 +205,8 @@ def write_gmsh22(path: str | Path, points, triangles, tags, names: dict[int, str
         out += [f'2 {int(t)} "{n}"' for t, n in sorted(names.items())]
         out += ["$EndPhysicalNames"]
     out += ["$Nodes", str(points.shape[0])]
-    out += [f"{i + 1} {p[0]!r} {p[1]!r} {p[2]!r}" for i, p in enumerate(points)]
+    # repr of a Python float round-trips exactly (NumPy 2 scalars would print as "np.float64(...)")
+    out += [f"{i + 1} {float(p[0])!r} {float(p[1])!r} {float(p[2])!r}" for i, p in enumerate(points)]
     out += ["$EndNodes", "$Elements", str(triangles.shape[0])]
     out += [
         f"{i + 1} 2 2 {int(tags[i])} {int(tags[i])} {t[0] + 1} {t[1] + 1} {t[2] + 1}"
