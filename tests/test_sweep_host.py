@@ -42,3 +42,33 @@ def test_case_flags_follow_the_reference_helper():
     assert _case_flags(3.0, 0.0, robin=True, coupled=True) == {"robin_boundary": True}
     assert _case_flags(3.0, 0.0, coupled=True, field_k=3.0) == {}
     assert _case_flags(3.0, 0.0, coupled=True, field_k=2.5) == {"field_k_real_f32": 2.5}
+
+
+def test_dense_solve_and_mesh_resolution_policies():
+    """The per-frequency policy keys of the reference's sweep (tests/test_sweep_results.py:157-215)."""
+    from types import SimpleNamespace
+
+    from hornlab_metal_bem_b200.sweep import apply_dense_solve_policy, apply_mesh_resolution_policy, mesh_max_edge
+
+    low = {"dense_solve_rcond": 1e-8}
+    apply_dense_solve_policy(low, threshold=1e-6)
+    assert low["dense_solve_rcond_warning_threshold"] == 1e-6
+    assert low["dense_solve_suspect"] is True and low["dense_solve_policy_available"] is True
+    assert "nudge or densify" in low["dense_solve_recommendation"]
+    fine = {"dense_solve_rcond": 1e-2}
+    apply_dense_solve_policy(fine, threshold=1e-6)
+    assert fine["dense_solve_policy_available"] is True and fine["dense_solve_suspect"] is False
+    unchecked = {}
+    apply_dense_solve_policy(unchecked, threshold=1e-6)
+    assert unchecked["dense_solve_policy_available"] is False and unchecked["dense_solve_suspect"] is False
+
+    d = {}
+    apply_mesh_resolution_policy(d, 1000.0, 0.1, 6.0)
+    np.testing.assert_allclose(d["mesh_elements_per_wavelength"], 3.43)
+    np.testing.assert_allclose(d["mesh_max_valid_frequency_hz"], 571.6666666666666)
+    assert d["mesh_resolution_suspect"] is True
+
+    mesh = SimpleNamespace(grid=SimpleNamespace(
+        vertices=np.array([[0.0, 1.0, 0.0], [0.0, 0.0, 1.0], [0.0, 0.0, 0.0]]),
+        elements=np.array([[0], [1], [2]], dtype=np.int32)))
+    np.testing.assert_allclose(mesh_max_edge(mesh), np.sqrt(2.0))
