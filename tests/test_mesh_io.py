@@ -158,3 +158,29 @@ def test_reader_errors(tmp_path):
     not_msh.write_text("solid x\nendsolid x\n")
     with pytest.raises(MeshError, match="not a Gmsh"):
         read_gmsh(not_msh)
+
+
+def test_pure_grid_and_function_spaces():
+    """Array-only grid and P1 / DP0 spaces (reference tests/test_pure_mesh.py:19-56)."""
+    from hornlab_metal_bem_b200.mesh import make_pure_function_spaces, make_pure_grid
+
+    g = make_pure_grid(TET_V, np.array([[0, 1, 2], [0, 1, 3]]))
+    assert g.vertices.shape == (3, 4) and g.elements.shape == (3, 2) and g.number_of_elements == 2
+    np.testing.assert_allclose(g.volumes, [0.5, 0.5])
+    p1, dp0 = make_pure_function_spaces(make_pure_grid(np.eye(3), np.array([[0, 1, 2]])))
+    np.testing.assert_array_equal(p1.local2global, [[0, 1, 2]])
+    assert p1.global_dof_count == 3 and dp0.global_dof_count == 1
+
+
+@pytest.mark.parametrize(("verts", "tris", "plane"), [
+    ([[0, 0, 0], [0, 1, 0], [0, 0, 1], [1, 0.2, 0.3]], [[0, 1, 3], [0, 3, 2], [1, 2, 3]], "yz"),
+    ([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], [[0, 1, 2], [1, 3, 2]], "yz+xz"),
+    ([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0.2, 0.3, 1]], [[0, 1, 3], [0, 3, 2], [1, 2, 3]], "xy"),
+    (TET_V, TET_F, None),     # closed: no open rim, no reduced plane
+])
+def test_reduced_symmetry_plane_detection(verts, tris, plane):
+    """Open rims lying on the coordinate planes name the mirror plane(s) of a reduced mesh (reference
+    tests/test_pure_mesh.py:97-160)."""
+    from hornlab_metal_bem_b200.mesh import detect_reduced_symmetry_plane
+
+    assert detect_reduced_symmetry_plane(np.asarray(verts, float), np.asarray(tris)) == plane
