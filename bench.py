@@ -119,6 +119,33 @@ def dist_env():
     return world, rank, local
 
 
+def init_replicas(world: int, backend: str = "nccl", timeout_s: int = 120):
+    """Process group of the N replicas (used only for barriers and the max-over-ranks times), or None
+    for one process.  The rendezvous comes from MASTER_ADDR / MASTER_PORT / RANK / WORLD_SIZE."""
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+    return dist
+
+
+def max_over_ranks(dist, values):
+    """Element-wise maximum of this rank's values (device times in ms) over all ranks; the values
+    themselves without a process group."""
+    vals = [float(v) for v in values]
+    if dist is None:
+        return vals
+    import torch
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor(vals, dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
 class Clocks:
     """nvidia-smi sampler running during the timed region."""
 
@@ -246,13 +273,7 @@ def run_b200(args, w):
 
     world, rank, local = dist_env()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dist = init_replicas(world, "nccl", 120)
     from hornlab_metal_bem_b200.native import (
         HBEM_ASM_DUFFY, HBEM_ASM_REGULAR, NativeSession, ResidentSweep, _np_ptr, _stream_ptr, _t_ptr, check,
         load_library,
@@ -327,11 +348,7 @@ def run_b200(args, w):
         dist.barrier()
     clk = clocks.stop()
     launches = lib.hbem_launch_count() - launches0
-    ms = t_start.elapsed_time(t_end)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    (ms,) = max_over_ranks(dist, [t_start.elapsed_time(t_end)])
     stage = {"regular_ms": [], "duffy_ms": [], "lu_solve_ms": [], "field_ms": []}
     for e in stage_evs:
         stage["regular_ms"].append(e[0].elapsed_time(e[1]))
@@ -357,11 +374,7 @@ def run_b200(args, w):
         res = sess.assemble_solve_evaluate_standard_neumann_batch(w["freqs"], w["k_re"], q, w["obs"], **e2e_kw)
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    (e2e_ms,) = max_over_ranks(dist, [e0.elapsed_time(e1)])
     assert all(r.lapack_info == 0 for r in res)
     n_obs = w["obs"].shape[1]
     ntag = len(w["tags"])
@@ -420,13 +433,7 @@ def run_b200_c4(args, w):
 
     world, rank, local = dist_env()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dist = init_replicas(world, "nccl", 600)
     from hornlab_metal_bem_b200.native import NativeSession, _np_ptr, _stream_ptr, _t_ptr, check, load_library
     from hornlab_metal_bem_b200.sweep import directivity_from_pressure
 
@@ -474,12 +481,8 @@ def run_b200_c4(args, w):
         dist.barrier()
     clk = clocks.stop()
     launches = lib.hbem_launch_count() - launches0
-    e2e_ms = e0.elapsed_time(e1)
-    dev_ms = sum(t["assembly_ms"] + t["solve_ms"] + t["field_ms"] for t in stages)
-    if dist is not None:
-        tt = torch.tensor([e2e_ms, dev_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms, dev_ms = (float(v) for v in tt.tolist())
+    e2e_ms, dev_ms = max_over_ranks(dist, [e0.elapsed_time(e1),
+                                           sum(t["assembly_ms"] + t["solve_ms"] + t["field_ms"] for t in stages)])
     stage = {k: statistics.median(t[k] for t in stages) for k in ("assembly_ms", "solve_ms", "field_ms")}
 
     # ---- accuracy against an FP64 GPU solve of the same FP32-assembled system
