@@ -49,47 +49,28 @@ constexpr int kPanelThreads = 512;
 
 __device__ __forceinline__ float cabs1(float r, float i) { return fabsf(r) + fabsf(i); }
 
-// Panel factorisation of rows k0..n-1 x nb columns (nb <= 32).
-// SMEM: the panel is staged in shared memory with an odd row pitch (nb + 1),
-// so column reads across rows are bank-conflict free; otherwise it is worked
-// in place through L2.  Per column j, three barrier-separated phases:
+// Panel factorisation of rows k0..n-1 x nb columns (nb <= 32), worked in
+// place through L2: the fallback for panels taller than a cluster's shared
+// memory holds.  Per column j, three barrier-separated phases:
 //   R (threads over rows)    : scale column j-1 by 1/pivot, local argmax of
 //                              |re| + |im| in column j (first index on ties);
 //   P (nb threads)           : pick the pivot, swap rows j <-> p, publish the
 //                              pivot row;
 //   E (threads over elements): A[r][c] -= (A[r][j] / pivot) * A[j][c], r, c > j.
-template <bool SMEM>
 __global__ void __launch_bounds__(kPanelThreads) k_panel(float *a_re, float *a_im, long long lda, long long a_stride,
                                                          int n, int k0, int nb, int *piv, long long piv_stride,
                                                          int *info) {
-    extern __shared__ float s_panel[];
     __shared__ float s_v[kPanelThreads / 32];
     __shared__ int s_i[kPanelThreads / 32];
     __shared__ float s_pr[32], s_pi[32];
     const int b = blockIdx.x;
     int *pv = piv + (size_t)b * piv_stride;
     const int m = n - k0;  // panel rows
-    // element (r, c) of the panel: smem pitch P, or global pitch lda
-    const int P = SMEM ? nb + 1 : (int)lda;
-    float *pre, *pim;
-    if (SMEM) {
-        pre = s_panel;
-        pim = s_panel + m * P;
-    } else {
-        pre = a_re + (size_t)b * a_stride + (size_t)k0 * lda + k0;
-        pim = a_im + (size_t)b * a_stride + (size_t)k0 * lda + k0;
-    }
+    // element (r, c) of the panel at global pitch lda
+    const int P = (int)lda;
+    float *pre = a_re + (size_t)b * a_stride + (size_t)k0 * lda + k0;
+    float *pim = a_im + (size_t)b * a_stride + (size_t)k0 * lda + k0;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-    if (SMEM) {
-        const float *gre = a_re + (size_t)b * a_stride + (size_t)k0 * lda + k0;
-        const float *gim = a_im + (size_t)b * a_stride + (size_t)k0 * lda + k0;
-        for (int e = tid; e < m * nb; e += blockDim.x) {
-            const int r = e / nb, j = e - r * nb;
-            pre[r * P + j] = gre[(size_t)r * lda + j];
-            pim[r * P + j] = gim[(size_t)r * lda + j];
-        }
-        __syncthreads();
-    }
     // element-phase mapping: LPR lanes per row, RPW rows per warp instruction
     const int LPR = nb > 16 ? 32 : 16;
     const int c_off = lane & (LPR - 1);
@@ -169,18 +150,6 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(float *a_re, float *a_i
             }
         }
         __syncthreads();
-    }
-    if (SMEM) {
-        // the last column was scaled by the R pass, thread per row; the
-        // write-back maps elements to threads differently
-        __syncthreads();
-        float *gre = a_re + (size_t)b * a_stride + (size_t)k0 * lda + k0;
-        float *gim = a_im + (size_t)b * a_stride + (size_t)k0 * lda + k0;
-        for (int e = tid; e < m * nb; e += blockDim.x) {
-            const int r = e / nb, j = e - r * nb;
-            gre[(size_t)r * lda + j] = pre[r * P + j];
-            gim[(size_t)r * lda + j] = pim[r * P + j];
-        }
     }
     if (tid == 0 && first_zero && info[b] == 0) info[b] = first_zero;
 }
@@ -1932,7 +1901,7 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
                 rc = launch_panel_cluster(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info, batch, smem_cap,
                                           cmax, cs);
             } else {
-                k_panel<false><<<batch, kPanelThreads, 0, cs>>>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info);
+                k_panel<<<batch, kPanelThreads, 0, cs>>>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride, info);
                 rc = launched("k_panel");
             }
             if (rc != HBEM_OK) return finish(rc);
