@@ -90,3 +90,65 @@ def test_tuning_knobs_validate_and_read_back():
     finally:
         for key in keys.values():
             lib.hbem_set_tuning(key, 0)
+
+
+def test_entry_points_validate_arguments_before_any_device_work():
+    """Every rejection below happens on the host, before a device is touched (this runs without one):
+    status -1 (HBEM_ERR_ARG) and a message naming the entry point; empty problems are no-ops."""
+    import numpy as np
+
+    lib = native.load_library()
+    D = ctypes.c_void_p(256)          # a non-NULL pointer the checks never dereference
+    err = lambda: native.last_error(lib)
+
+    # empty problems succeed without looking at any pointer
+    assert lib.hbem_lu_factor(0, 1, None, None, 1, 1, None, 1, None, 0, None) == 0
+    assert lib.hbem_lu_solve(4, 1, 0, None, None, 4, 16, None, 4, None, None, 1, 4, 0, None) == 0
+    assert lib.hbem_refine(4, 0, None, None, 4, 16, None, None, 16, None, 4, None, None, 4, None, None, 4,
+                           1e-6, 3, None, None, None) == 0
+    # factor: strides, precision
+    assert lib.hbem_lu_factor(4, 1, D, D, 3, 16, D, 4, D, 0, None) == -1 and "bad strides" in err()
+    assert lib.hbem_lu_factor(4, 1, D, D, 4, 12, D, 4, D, 0, None) == -1 and "bad strides" in err()
+    assert lib.hbem_lu_factor(4, 1, D, D, 4, 16, D, 4, D, 2, None) == -1 and "precision" in err()
+    # solve: NULL, strides, transposition
+    assert lib.hbem_lu_solve(4, 1, 1, D, D, 4, 16, None, 4, D, D, 1, 4, 0, None) == -1 and "NULL" in err()
+    assert lib.hbem_lu_solve(4, 1, 1, D, D, 4, 16, D, 3, D, D, 1, 4, 0, None) == -1 and "bad strides" in err()
+    assert lib.hbem_lu_solve(4, 1, 1, D, D, 4, 16, D, 4, D, D, 1, 4, 3, None) == -1 and "trans" in err()
+    # refinement: tolerance and iteration count
+    args = (4, 1, D, D, 4, 16, D, D, 16, D, 4, D, D, 4, D, D, 4)
+    assert lib.hbem_refine(*args, 0.0, 3, None, None, None) == -1 and "hbem_refine" in err()
+    assert lib.hbem_refine(*args, 1e-6, -1, None, None, None) == -1 and "hbem_refine" in err()
+    assert lib.hbem_refine_noalloc(*args, float("nan"), 3, None, None, None) == -1 and "noalloc" in err()
+    # condition estimate: strides and the largest order its shared-memory vector holds
+    assert lib.hbem_matrix_norm1(4, 1, D, D, 4, 15, D, None) == -1 and "bad strides" in err()
+    n = 30000
+    assert lib.hbem_lu_rcond(n, 1, D, D, n, n * n, D, D, None) == -1 and "too large" in err()
+    # batch sweep without a session
+    assert lib.hbem_solve_batch(None, 1, *([None] * 5), 0, None, 0, 0, 1e-6, 0, *([None] * 11)) == -1
+    assert "NULL session" in err()
+
+    # session creation: geometry checks run before the device is queried
+    v = np.ascontiguousarray(np.array([[0.0, 1, 0, 0], [0, 0, 1, 0], [0, 0, 0, 1]], np.float32))
+    t = np.ascontiguousarray(np.array([[0, 0, 0, 1], [2, 1, 3, 2], [1, 3, 2, 3]], np.int32))
+    l2g = np.ascontiguousarray(t.T)
+    tags = np.array([1, 1, 1, 2], np.int32)
+    areas = np.full(4, 0.5, np.float32)
+    normals = np.ascontiguousarray(np.zeros((3, 4), np.float32))
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    out = ctypes.c_void_p()
+
+    def create(v=v, t=t, l2g=l2g, areas=areas, n_dof=4, sym=0):
+        return lib.hbem_session_create(P(v), v.shape[1], P(t), t.shape[1], P(l2g), n_dof, P(tags), P(areas),
+                                       P(normals), sym, 0, ctypes.byref(out))
+
+    assert create(sym=5) == -1 and "sym_code" in err()
+    bad_t = t.copy()
+    bad_t[0, 0] = 7
+    assert create(t=bad_t) == -1 and "vertex index out of range" in err()
+    bad_l2g = l2g.copy()
+    bad_l2g[0, 0] = 4
+    assert create(l2g=bad_l2g) == -1 and "out-of-range DOF" in err()
+    bad_areas = areas.copy()
+    bad_areas[2] = 0.0
+    assert create(areas=bad_areas) == -1 and "non-positive area" in err()
+    assert create(n_dof=0) == -1 and "empty geometry" in err()
