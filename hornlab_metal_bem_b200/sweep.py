@@ -156,8 +156,11 @@ def apply_mesh_resolution_policy(diag: dict, frequency_hz: float, max_edge: floa
 
 
 def run_sweep(mesh: LoadedMesh, frequencies, frame: ObservationFrame, config: SolveConfig,
-              *, session: NativeSession | None = None) -> SolveResult:
-    """Standard-Neumann sweep on the GPU (the reference's ``run_sweep_native_metal``)."""
+              *, session: NativeSession | None = None, average_tags=None) -> SolveResult:
+    """Standard-Neumann sweep on the GPU (the reference's ``run_sweep_native_metal``).
+
+    ``average_tags`` adds tags to the surface-pressure averages (the sorted union with the
+    velocity-source tags is recorded); multi-source sweeps pass every source's tags."""
     should_route_native(config)
     freqs = np.asarray(frequencies, dtype=np.float64)
     if freqs.size == 0:
@@ -174,6 +177,8 @@ def run_sweep(mesh: LoadedMesh, frequencies, frame: ObservationFrame, config: So
     buffers = build_geometry_buffers(mesh.grid, mesh.physical_tags, p1, dp0)
     max_edge = mesh_max_edge(mesh)
     source_tags = list(config.velocity_sources.keys())
+    if average_tags is not None:
+        source_tags = sorted({int(t) for t in source_tags} | {int(t) for t in average_tags})
     scale = build_source_face_scale(mesh.grid, mesh.physical_tags, config, frame.axis, frame.source_center)
     on_axis = int(np.argmin(np.abs(angles)))
     imp_tag = min(config.velocity_sources.keys(), default=2)
@@ -290,15 +295,70 @@ def run_sweep(mesh: LoadedMesh, frequencies, frame: ObservationFrame, config: So
 
 def run_sweep_multi_source(mesh: LoadedMesh, frequencies, frame: ObservationFrame, config: SolveConfig,
                            sources: list[dict[int, complex]]) -> list[SolveResult]:
-    """One result per velocity-source dict (the reference's ``run_sweep_native_metal_multi_source``).
+    """One result per velocity-source dict (the reference's ``run_sweep_native_metal_multi_source``,
+    ``sweep.py:957-1301``), every source on one resident session, each result recording the surface
+    averages of the sorted union of all source tags.
 
-    Each source is an independent sweep on one resident session; the
-    factorisation is recomputed per source.
+    Without a streaming callback each source is one sweep (the factorisation is recomputed per
+    source).  With ``on_frequency_result`` the sources are interleaved per frequency and the callback
+    runs once per frequency with the first source's entry plus ``source_results`` (one entry per
+    source), as the reference's multi-RHS stream; returning False stops after that frequency and the
+    results hold the completed frequencies.  ``velocity_source_callback`` is rejected: each source
+    vector is fixed for the whole sweep.
     """
+    if not sources:
+        raise ValueError("sources must contain at least one velocity dict")
+    if config.velocity_source_callback is not None:
+        raise ValueError("multi-source solves do not support velocity_source_callback")
     p1, dp0 = make_pure_function_spaces(mesh.grid)
     buffers = build_geometry_buffers(mesh.grid, mesh.physical_tags, p1, dp0)
     all_tags = sorted({int(t) for s in sources for t in s})
+    per_source = [replace(config, velocity_sources=dict(src)) for src in sources]
     with NativeSession(buffers, symmetry_plane=config.native_symmetry_plane, aperture_tag=config.aperture_tag,
                        velocity_source_tags=all_tags, check_open_edges=config.native_check_open_edges) as session:
-        return [run_sweep(mesh, frequencies, frame, replace(config, velocity_sources=dict(src)), session=session)
-                for src in sources]
+        if config.on_frequency_result is None:
+            return [run_sweep(mesh, frequencies, frame, c, session=session, average_tags=all_tags)
+                    for c in per_source]
+        quiet = [replace(c, on_frequency_result=None, progress_callback=None) for c in per_source]
+        freqs = np.atleast_1d(np.asarray(frequencies, dtype=np.float64))
+        parts: list[list[SolveResult]] = [[] for _ in sources]
+        for i, f in enumerate(freqs):
+            entries = []
+            for s, c in enumerate(quiet):
+                r = run_sweep(mesh, [f], frame, c, session=session, average_tags=all_tags)
+                parts[s].append(r)
+                entry = dict(r.solver_log[-1])
+                entry.update(observation_pressure_complex=r.pressure_complex[0],
+                             observation_directivity_db=r.directivity_db[0],
+                             observation_angles_deg=r.observation_angles_deg,
+                             observation_planes=r.observation_planes)
+                entries.append(entry)
+            if config.progress_callback is not None:
+                config.progress_callback(i, freqs.size, float(f))
+            if config.on_frequency_result(i, float(f), {**entries[0], "source_results": entries}) is False:
+                logger.info("Early stop requested after %.1f Hz", float(f))
+                break
+        return [_concat_results(p, c) for p, c in zip(parts, per_source)]
+
+
+def _concat_results(parts: list[SolveResult], config: SolveConfig) -> SolveResult:
+    """One ``SolveResult`` from per-frequency results of the same source, in order."""
+    first = parts[0]
+    cat = lambda name: np.concatenate([getattr(p, name) for p in parts], axis=0)
+    return SolveResult(
+        frequencies_hz=cat("frequencies_hz"),
+        pressure_complex=cat("pressure_complex"),
+        directivity_db=cat("directivity_db"),
+        impedance=cat("impedance"),
+        observation_angles_deg=first.observation_angles_deg,
+        observation_points=first.observation_points,
+        observation_planes=first.observation_planes,
+        config=config,
+        mesh_info=first.mesh_info,
+        timings={k: sum(float(p.timings.get(k, 0.0)) for p in parts) for k in first.timings},
+        solver_log=[e for p in parts for e in p.solver_log],
+        surface_pressure_avg=None if first.surface_pressure_avg is None else {
+            t: np.concatenate([p.surface_pressure_avg[t] for p in parts]) for t in first.surface_pressure_avg},
+        surface_pressure_complex=None if first.surface_pressure_complex is None else cat("surface_pressure_complex"),
+        native_diagnostics=[d for p in parts for d in p.native_diagnostics],
+    )

@@ -72,3 +72,86 @@ def test_dense_solve_and_mesh_resolution_policies():
         vertices=np.array([[0.0, 1.0, 0.0], [0.0, 0.0, 1.0], [0.0, 0.0, 0.0]]),
         elements=np.array([[0], [1], [2]], dtype=np.int32)))
     np.testing.assert_allclose(mesh_max_edge(mesh), np.sqrt(2.0))
+
+
+def _fake_multi_source_env(monkeypatch):
+    """Replace the GPU session and the single-source sweep with host fakes; returns the call log."""
+    from contextlib import nullcontext
+
+    import hornlab_metal_bem_b200.sweep as sw
+    from hornlab_metal_bem_b200.result import MeshInfo, SolveResult
+
+    calls = []
+
+    def fake_run_sweep(mesh, frequencies, frame, config, *, session=None, average_tags=None):
+        f = np.asarray(frequencies, dtype=np.float64)
+        src = dict(config.velocity_sources)
+        calls.append((tuple(f), src, tuple(average_tags or ()), config.on_frequency_result is None))
+        base = float(sum(abs(v) * t for t, v in src.items()))
+        p = (base + f[:, None, None] / 1000.0) * np.ones((f.size, 2, 3))
+        log = [{"frequency_hz": float(x), "impedance": complex(base, x), "lapack_info": 0,
+                "observation_sphere_pressure_complex": None} for x in f]
+        return SolveResult(frequencies_hz=f, pressure_complex=p.astype(np.complex128), directivity_db=np.zeros_like(p),
+                           impedance=np.array([complex(base, x) for x in f]), observation_angles_deg=np.array([-45.0, 0.0, 45.0]),
+                           observation_points=np.zeros((2, 3, 3)), observation_planes=["horizontal", "vertical"],
+                           config=config, mesh_info=MeshInfo(3, 1, {}, (np.zeros(3), np.ones(3))),
+                           timings={"solve_s": 0.1 * f.size}, solver_log=log,
+                           surface_pressure_avg={t: np.full(f.size, complex(t)) for t in (average_tags or src)},
+                           native_diagnostics=[{"f": float(x)} for x in f])
+
+    monkeypatch.setattr(sw, "run_sweep", fake_run_sweep)
+    monkeypatch.setattr(sw, "NativeSession", lambda *a, **k: nullcontext(object()))
+    return sw, calls
+
+
+def _tiny_mesh_and_frame():
+    from hornlab_metal_bem_b200 import generators as G
+    from hornlab_metal_bem_b200.observation import infer_frame
+
+    m = G.icosphere(1, 0.1)
+    return m, infer_frame(m.grid, m.physical_tags, source_tag=2)
+
+
+def test_multi_source_stream_interleaves_sources_per_frequency(monkeypatch):
+    """With a streaming callback the sources are solved frequency by frequency and the callback sees one
+    entry per frequency carrying ``source_results`` (the reference's multi-RHS stream, sweep.py:1165-1210);
+    False stops the sweep and the results keep the completed frequencies."""
+    sw, calls = _fake_multi_source_env(monkeypatch)
+    mesh, frame = _tiny_mesh_and_frame()
+    seen, progress = [], []
+
+    def on_result(i, f, entry):
+        seen.append((i, f, entry))
+        return i < 1                       # stop after the second frequency
+
+    cfg = hb.native_config(velocity_sources={2: 1.0}, on_frequency_result=on_result,
+                           progress_callback=lambda i, n, f: progress.append((i, n, f)))
+    sources = [{2: 1.0}, {2: 0.5, 3: 1.0}]
+    out = sw.run_sweep_multi_source(mesh, [500.0, 1000.0, 2000.0], frame, cfg, sources)
+    assert [(c[0], c[1]) for c in calls] == [((500.0,), {2: 1.0}), ((500.0,), {2: 0.5, 3: 1.0}),
+                                             ((1000.0,), {2: 1.0}), ((1000.0,), {2: 0.5, 3: 1.0})]
+    assert all(c[2] == (2, 3) and c[3] for c in calls)     # tag union; per-frequency calls stream nothing
+    assert [(i, f) for i, f, _ in seen] == [(0, 500.0), (1, 1000.0)]
+    assert progress == [(0, 3, 500.0), (1, 3, 1000.0)]
+    e = seen[1][2]
+    assert len(e["source_results"]) == 2 and e["impedance"] == e["source_results"][0]["impedance"]
+    np.testing.assert_allclose(e["source_results"][1]["observation_pressure_complex"], (4.0 + 1.0) * np.ones((2, 3)))
+    assert e["observation_planes"] == ["horizontal", "vertical"] and len(e["observation_angles_deg"]) == 3
+    assert [r.frequencies_hz.tolist() for r in out] == [[500.0, 1000.0]] * 2
+    assert out[1].pressure_complex.shape == (2, 2, 3) and set(out[1].surface_pressure_avg) == {2, 3}
+    assert out[0].config.velocity_sources == {2: 1.0} and out[0].timings["solve_s"] == pytest.approx(0.2)
+    assert [d["f"] for d in out[0].native_diagnostics] == [500.0, 1000.0]
+
+
+def test_multi_source_without_stream_is_one_sweep_per_source(monkeypatch):
+    sw, calls = _fake_multi_source_env(monkeypatch)
+    mesh, frame = _tiny_mesh_and_frame()
+    out = sw.run_sweep_multi_source(mesh, [500.0, 1000.0], frame, hb.native_config(), [{2: 1.0}, {3: 1.0}])
+    assert [(c[0], c[1], c[2]) for c in calls] == [((500.0, 1000.0), {2: 1.0}, (2, 3)),
+                                                   ((500.0, 1000.0), {3: 1.0}, (2, 3))]
+    assert len(out) == 2
+    with pytest.raises(ValueError, match="at least one"):
+        sw.run_sweep_multi_source(mesh, [500.0], frame, hb.native_config(), [])
+    with pytest.raises(ValueError, match="velocity_source_callback"):
+        sw.run_sweep_multi_source(mesh, [500.0], frame,
+                                  hb.native_config(velocity_source_callback=lambda f: {2: 1.0}), [{2: 1.0}])
