@@ -2088,7 +2088,7 @@ int lu_rcond(int n, int batch, const float *lu_re, const float *lu_im, long long
                            st);
     };
     k_rc_init<<<gv, 256, 0, st>>>(n, xr, xi, stride, state);
-    // round 0: (LU) w = x for every matrix
+    // first estimator step: (LU) w = x for every matrix
     if (launched("k_rc_init")) {
         k_rc_copy<<<gv, 256, 0, st>>>(n, xr, xi, wr, wi, stride, state, 0, 3, active);
         if (launched("k_rc_copy")) rc = solve(HBEM_TRANS_N);

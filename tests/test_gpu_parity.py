@@ -1,6 +1,6 @@
 """GPU parity: every CUDA stage through the C ABI against the CPU oracle.
 
-Tolerances: assembled matrix and RHS within 1e-4
+Tolerances (the path's accuracy targets): assembled matrix and RHS within 1e-4
 relative L2 of the reference method (here the FP64 oracle, which is pinned to
 the reference's known answers in test_oracle_pins.py); LU solutions within
 1e-5 of LAPACK; field within 1e-4 relative; directivity within 0.01 dB.
