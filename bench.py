@@ -240,6 +240,32 @@ def cpu_baseline(w, n_freq_sample: int = 1) -> dict:
                       f"{dt:.1f} s: corrected assembly + cgesv + field + tag averages"}
 
 
+def accuracy_vs_fp64(sess, w, rs) -> dict:
+    """Error of the timed sweep's last step against the FP64 GPU path (FP64 corrected assembly, complex128 LU,
+    FP64 field: ``NativeSession.reference_solve_f64``) at sampled frequencies: the top of the band and the
+    frequency where the FP32 LU's pivot growth is worst on this mesh (16 kHz)."""
+    from hornlab_metal_bem_b200.sweep import directivity_from_pressure
+
+    freqs = np.asarray(w["freqs"])
+    idx = sorted({int(np.argmin(np.abs(freqs - 16000.0))), len(freqs) - 1})
+    n_planes = len(w["cfg"].observation.planes)
+    out = []
+    for f in idx:
+        p64, f64 = sess.reference_solve_f64([float(w["k_re"][f])], w["q"][f][None, :], w["obs"])
+        p64, f64 = p64.cpu().numpy()[0], f64.cpu().numpy()[0]
+        p32 = rs.x_re[f].double().cpu().numpy() + 1j * rs.x_im[f].double().cpu().numpy()
+        f32 = rs.f_re[f].double().cpu().numpy() + 1j * rs.f_im[f].double().cpu().numpy()
+        d64 = directivity_from_pressure(f64.reshape(n_planes, -1), 0)
+        d32 = directivity_from_pressure(f32.reshape(n_planes, -1), 0)
+        out.append({"frequency_hz": float(freqs[f]),
+                    "surface_pressure_rel": float(np.linalg.norm(p32 - p64) / np.linalg.norm(p64)),
+                    "field_rel": float(np.linalg.norm(f32 - f64) / np.linalg.norm(f64)),
+                    "directivity_max_abs_db": float(np.max(np.abs(d32 - d64))),
+                    "refine_passes": int(rs.iters[f])})
+    return {"against": "FP64 GPU path (hbem_assemble_f64 + hbem_lu_factor_f64/solve_f64 + hbem_field_f64)",
+            "cases": out}
+
+
 # --------------------------------------------------------------------------- arms
 def run_reference(args, w):
     world, rank, _ = dist_env()
@@ -285,7 +311,8 @@ def run_b200(args, w):
     sess = NativeSession(buf, symmetry_plane=w["cfg"].native_symmetry_plane, check_open_edges=False)
     want_rcond = w["cfg"].dense_solve_rcond_warning_threshold > 0   # the reference's per-case cgecon
     rs = ResidentSweep(sess, w["k_re"], w["k_im"], w["q"], w["obs"], w["tags"], precision=args.precision,
-                       rcond=want_rcond)
+                       rcond=want_rcond, refine_tolerance=w["cfg"].refine_tolerance,
+                       refine_max_iterations=w["cfg"].refine_max_iterations)
     n = rs.n
     stream = torch.cuda.current_stream()
 
@@ -381,6 +408,8 @@ def run_b200(args, w):
     h2d = F * buf.n_triangles * 8 + F * 8 + 3 * n_obs * 4 + ntag * 4
     d2h = F * n_obs * 8 + F * ntag * 16 + F * 4 + F * 12
 
+    accuracy = accuracy_vs_fp64(sess, w, rs)
+
     # ---- roofline of the dominant kernel
     peaks = measured_peaks()
     m_img = {0: 1, 1: 2, 2: 2, 3: 4, 4: 2}[w["sym"]]
@@ -407,11 +436,14 @@ def run_b200(args, w):
         "vs_baseline": None, "dtype": "c64 (f32 planar)", "data": "synthetic",
         "config": {"workload": w["desc"], "n_dof": buf.p1_dof_count, "n_triangles": T, "n_freq": F,
                    "n_obs": n_obs, "precision": args.precision, "rcond_estimate": bool(want_rcond),
+                   "refine": (f"FP64-residual refinement, tolerance {rs.refine_tol:g}, at most {rs.refine_max} passes"
+                              if rs.refine else "none"),
                    "parallelism": f"replicas x{world} (frequency-parallel)",
                    "l2": f"working set {2 * F * n * n * 4 / 1e6:.0f} MB of dense matrices > 126 MB L2"},
         "e2e": {"value": world * F * args.steps / (e2e_ms * 1e-3), "unit": "freq-solves/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
+        "accuracy": accuracy,
         "stages_ms_per_step": stage,
         "clocks": clk,
         "roofline": roofline,

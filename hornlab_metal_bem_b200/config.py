@@ -9,11 +9,24 @@ backend the threadgroup sizes map onto CUDA block-size overrides.
 Three keys are new and only affect the B200 path:
 
 * ``precision``: ``"plain"`` (FP32-accurate LU, the reference's complex64
-  ``cgesv`` semantics) or ``"mixed"`` (BF16x3 tensor-core trailing updates
-  recovered by FP64-residual iterative refinement).
-* ``refine_tolerance`` / ``refine_max_iterations``: refinement stopping rule
-  (the reference stops at 1e-7 after at most 10 passes,
-  ``main.swift:4995-5005``, ``6975``).
+  ``cgesv`` semantics) or ``"mixed"`` (BF16x3 tensor-core trailing updates).
+  Either is followed by FP64-residual iterative refinement against the
+  assembled matrix (the reference's optional refinement passes,
+  ``main.swift:4855-4857, 6964-7070``).  Plain refines by default because an
+  FP32 LU alone can lose digits to pivot growth: on the 1043-dof quarter horn
+  at 16 kHz partial pivoting grows the entries ~8e3-fold and complex64
+  ``cgesv`` (the reference's default) and this LU alike miss the FP64
+  solution by 3e-3 to 5e-3, where one or two refinement passes recover 1e-6.
+  ``refine_max_iterations=0`` keeps the unrefined cgesv result.
+* ``refine_tolerance`` / ``refine_max_iterations``: refinement stopping rule:
+  relative residual at most ``refine_tolerance``, at most
+  ``refine_max_iterations`` passes, and a stop as soon as a pass no longer
+  lowers the residual (the reference stops at 1e-7, after at most 10 passes
+  or on the first pass that does not improve, ``main.swift:4995-5005``,
+  ``6975-7063``).
+* ``dense_solve_dtype="float64"`` (a reference key): the FP32-assembled
+  system widened to complex128, factored and solved in FP64 on the GPU (the
+  reference's ``zgesv`` path, ``main.swift:7101-7185``); no refinement.
 """
 from __future__ import annotations
 

@@ -7,6 +7,15 @@
 // triangles, interpolate the P1 pressure to the 6 quadrature points once per
 // triangle, and accumulate the 8 observation sums in registers before a block
 // reduction.  Tag averages (main.swift:807-841) use FP64 block sums.
+//
+// Phase accuracy: at 2 m and 20 kHz, k r is ~730 rad, so an FP32 distance
+// (relative error ~6e-8) alone puts ~4e-5 rad into the phase, which the sum
+// over the surface turns into a field error of the same size and up to
+// 0.01 dB of directivity near the pattern's nulls.  The distance is therefore
+// carried in FP64 from the exact difference of the float coordinates (an FP32
+// root refined by one FP64 Newton step) and the phase is reduced in turns in
+// FP64; sine and cosine of the reduced phase, the amplitudes and the sums
+// stay FP32.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -28,7 +37,8 @@ struct FieldArgs {
     float *out_re, *out_im;
     long long p_stride, q_stride, out_stride;
     int T, n_obs, sym;
-    float k[64], kt[64];
+    float k[64];
+    double kt[64];   // k / (2 pi): turns per metre
 };
 
 __device__ __forceinline__ float fqw(int q) { return (q == 0 || q == 2 || q == 3) ? HBEM_QWA : HBEM_QWB; }
@@ -39,17 +49,25 @@ __device__ __forceinline__ float fqy(int q) {
     return q == 0 ? HBEM_QY0 : q == 1 ? HBEM_QY1 : q == 2 ? HBEM_QY2 : q == 3 ? HBEM_QY3 : q == 4 ? HBEM_QY4 : HBEM_QY5;
 }
 
-// adds (D p - G q) for one source point
-__device__ __forceinline__ void fsample(float dx, float dy, float dz, float nx, float ny, float nz, float k, float kt,
-                                        float pr, float pi, float qr, float qi, float &ar, float &ai) {
-    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+// adds (D p - G q) for one source point y (double coordinates, exact copies of
+// the float inputs) seen from the observation point o
+__device__ __forceinline__ void fsample(double yx, double yy, double yz, double ox, double oy, double oz, float nx,
+                                        float ny, float nz, float k, double kt, float pr, float pi, float qr, float qi,
+                                        float &ar, float &ai) {
+    const double dxd = yx - ox, dyd = yy - oy, dzd = yz - oz;
+    const double r2d = fma(dxd, dxd, fma(dyd, dyd, dzd * dzd));
+    const float dx = (float)dxd, dy = (float)dyd, dz = (float)dzd;
+    const float r2 = (float)r2d;
     float rinv = rsqrtf(r2);
     rinv = r2 > 1.0e-14f ? rinv : 0.0f;
-    const float r = r2 * rinv;
-    float t = r * kt;
-    t -= rintf(t);
+    const float rf = r2 * rinv;
+    // one Newton step in FP64: r = rf + (r2 - rf^2) / (2 rf)
+    const double rfd = (double)rf;
+    const double r = fma(fma(-rfd, rfd, r2d), (double)(0.5f * rinv), rfd);
+    double td = r * kt;
+    td -= rint(td);
     float s, c;
-    sincospif(2.0f * t, &s, &c);
+    sincospif(2.0f * (float)td, &s, &c);
     const float gc = rinv * c, gs = rinv * s;
     const float proj = fmaf(dx, nx, fmaf(dy, ny, dz * nz)) * rinv;
     const float dre = fmaf(gc, -rinv, -gs * k) * proj;
@@ -60,17 +78,18 @@ __device__ __forceinline__ void fsample(float dx, float dy, float dz, float nx, 
 
 template <int SYM>
 __global__ void __launch_bounds__(kFieldThreads) k_field(const __grid_constant__ FieldArgs a) {
-    __shared__ float s_obs[kObsTile][3];
+    __shared__ double s_obs[kObsTile][3];
     __shared__ float s_red[kFieldThreads / 32][kObsTile][2];
     const int f = blockIdx.y;
     const int o0 = blockIdx.x * kObsTile;
     const int nob = min(kObsTile, a.n_obs - o0);
     if (threadIdx.x < kObsTile * 3) {
         const int o = threadIdx.x / 3, c = threadIdx.x % 3;
-        s_obs[o][c] = o < nob ? a.obs[(size_t)c * a.n_obs + o0 + o] : 0.f;
+        s_obs[o][c] = o < nob ? (double)a.obs[(size_t)c * a.n_obs + o0 + o] : 0.0;
     }
     __syncthreads();
-    const float k = a.k[f], kt = a.kt[f];
+    const float k = a.k[f];
+    const double kt = a.kt[f];
     const float *pre = a.p_re + (size_t)f * a.p_stride, *pim = a.p_im + (size_t)f * a.p_stride;
     const float *qre = a.q_re + (size_t)f * a.q_stride, *qim = a.q_im + (size_t)f * a.q_stride;
     float accr[kObsTile], acci[kObsTile];
@@ -84,23 +103,24 @@ __global__ void __launch_bounds__(kFieldThreads) k_field(const __grid_constant__
         const float qr = qre[t], qi = qim[t];
 #pragma unroll
         for (int q = 0; q < 6; ++q) {
-            const float4 y = a.qp[(size_t)t * 6 + q];
+            const float4 yf = a.qp[(size_t)t * 6 + q];
+            const double yx = yf.x, yy = yf.y, yz = yf.z;
             const float b1 = fqx(q), b2 = fqy(q), b0 = 1.f - b1 - b2;
             const float w = fqw(q) * nj.w;
             const float pr = (b0 * p0r + b1 * p1r + b2 * p2r) * w, pi = (b0 * p0i + b1 * p1i + b2 * p2i) * w;
             const float wqr = qr * w, wqi = qi * w;
 #pragma unroll
             for (int o = 0; o < kObsTile; ++o) {
-                const float ox = s_obs[o][0], oy = s_obs[o][1], oz = s_obs[o][2];
-                fsample(y.x - ox, y.y - oy, y.z - oz, nj.x, nj.y, nj.z, k, kt, pr, pi, wqr, wqi, accr[o], acci[o]);
+                const double ox = s_obs[o][0], oy = s_obs[o][1], oz = s_obs[o][2];
+                fsample(yx, yy, yz, ox, oy, oz, nj.x, nj.y, nj.z, k, kt, pr, pi, wqr, wqi, accr[o], acci[o]);
                 if (SYM == 1 || SYM == 3)
-                    fsample(-y.x - ox, y.y - oy, y.z - oz, -nj.x, nj.y, nj.z, k, kt, pr, pi, wqr, wqi, accr[o], acci[o]);
+                    fsample(-yx, yy, yz, ox, oy, oz, -nj.x, nj.y, nj.z, k, kt, pr, pi, wqr, wqi, accr[o], acci[o]);
                 if (SYM == 2 || SYM == 3)
-                    fsample(y.x - ox, -y.y - oy, y.z - oz, nj.x, -nj.y, nj.z, k, kt, pr, pi, wqr, wqi, accr[o], acci[o]);
+                    fsample(yx, -yy, yz, ox, oy, oz, nj.x, -nj.y, nj.z, k, kt, pr, pi, wqr, wqi, accr[o], acci[o]);
                 if (SYM == 3)
-                    fsample(-y.x - ox, -y.y - oy, y.z - oz, -nj.x, -nj.y, nj.z, k, kt, pr, pi, wqr, wqi, accr[o], acci[o]);
+                    fsample(-yx, -yy, yz, ox, oy, oz, -nj.x, -nj.y, nj.z, k, kt, pr, pi, wqr, wqi, accr[o], acci[o]);
                 if (SYM == 4)
-                    fsample(y.x - ox, y.y - oy, -y.z - oz, nj.x, nj.y, -nj.z, k, kt, pr, pi, wqr, wqi, accr[o], acci[o]);
+                    fsample(yx, yy, -yz, ox, oy, oz, nj.x, nj.y, -nj.z, k, kt, pr, pi, wqr, wqi, accr[o], acci[o]);
             }
         }
     }
@@ -179,7 +199,7 @@ int launch_field(Session &s, int n_freq, const float *k_re, const float *p_re, c
         a.T = s.n_triangles; a.n_obs = n_obs; a.sym = s.sym;
         for (int f = 0; f < nf; ++f) {
             a.k[f] = k_re[f0 + f];
-            a.kt[f] = (float)((double)k_re[f0 + f] / (2.0 * 3.14159265358979323846));
+            a.kt[f] = (double)k_re[f0 + f] / (2.0 * 3.14159265358979323846);
         }
         dim3 grid((n_obs + kObsTile - 1) / kObsTile, nf);
         switch (s.sym) {

@@ -102,6 +102,8 @@ struct Session {
 
     int *d_status = nullptr;        // device-side status word (bounds / wait failures)
     unsigned *d_sing_bits = nullptr; // T x T bitmap of touching pairs (shape gradients, built on first use)
+    double *d_geo64 = nullptr;      // FP64 path (built on first use): (T, 9) vertices per triangle,
+                                    // (T, 4) normal + area, then the Duffy rules as 5 doubles per point
 
     // coupled infinite baffle: aperture triangles (ascending ids) and their
     // local index per triangle (-1 elsewhere)
@@ -122,6 +124,7 @@ struct Session {
 // ---- pieces implemented in separate translation units ---------------------
 int build_duffy_pairs(Session &s, std::vector<DuffyPair> &pairs);
 void duffy_rule_table(int kind, std::vector<float> &rec);  // 5 floats per point
+void duffy_rule_table64(int kind, std::vector<double> &rec);  // the same rule in double
 
 int launch_regular(Session &s, int n_freq, const float *k_re, const float *k_im,
                    const float *q_re, const float *q_im, long long q_stride,

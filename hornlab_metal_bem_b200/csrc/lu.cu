@@ -2143,7 +2143,7 @@ int refine(int n, int batch, const float *a_re, const float *a_im, long long lda
     HBEM_CUDA(cudaMallocAsync((void **)&active, sizeof(int) * batch, st));
     std::vector<double> h_norms(2 * batch);
     std::vector<int> h_active(batch, 1), h_iters(batch, 0);
-    std::vector<double> h_res(batch, 0.0);
+    std::vector<double> h_res(batch, 0.0), h_best(batch, 0.0);
     int rc = HBEM_OK;
     float *dr = d, *di = d + (size_t)batch * x_stride;
     for (int it = 0; it <= max_iter && rc == HBEM_OK; ++it) {
@@ -2158,9 +2158,14 @@ int refine(int n, int batch, const float *a_re, const float *a_im, long long lda
         if (e != cudaSuccess) { rc = cuda_fail(e, "refine sync"); break; }
         bool any = false;
         for (int m = 0; m < batch; ++m) {
+            if (!h_active[m]) continue;
             const double rel = h_norms[2 * m + 1] > 0 ? std::sqrt(h_norms[2 * m] / h_norms[2 * m + 1]) : 0.0;
-            h_res[m] = rel;
-            h_active[m] = (h_active[m] && rel > tol && it < max_iter) ? 1 : 0;
+            // stop at the tolerance, after max_iter passes, or once a pass no
+            // longer lowers the residual (the FP32 storage floor of x)
+            const bool stalled = it > 0 && !(rel < h_best[m]);
+            h_res[m] = stalled ? h_best[m] : rel;
+            h_best[m] = h_res[m];
+            h_active[m] = (!stalled && rel > tol && it < max_iter) ? 1 : 0;
             if (h_active[m]) { ++h_iters[m]; any = true; }
         }
         if (!any) break;
@@ -2174,8 +2179,9 @@ int refine(int n, int batch, const float *a_re, const float *a_im, long long lda
         if (e != cudaSuccess) { rc = cuda_fail(e, "k_axpy_active"); break; }
         count_launch();
     }
-    if (rc == HBEM_OK && iters) {
-        cudaError_t e = cudaMemcpyAsync(iters, h_iters.data(), sizeof(int) * batch, cudaMemcpyHostToDevice, st);
+    if (rc == HBEM_OK && (iters || resid)) {
+        cudaError_t e = cudaSuccess;
+        if (iters) e = cudaMemcpyAsync(iters, h_iters.data(), sizeof(int) * batch, cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess && resid) e = cudaMemcpyAsync(resid, h_res.data(), sizeof(double) * batch, cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) rc = cuda_fail(e, "refine results");
@@ -2254,11 +2260,12 @@ int refine_noalloc(int n, int batch, const float *a_re, const float *a_im, long 
     void *wave = base + kNoAllocWaveOff;
     double h_norms[2 * kNoAllocMaxBatch];
     int h_active[kNoAllocMaxBatch], h_iters[kNoAllocMaxBatch];
-    double h_res[kNoAllocMaxBatch];
+    double h_res[kNoAllocMaxBatch], h_best[kNoAllocMaxBatch];
     for (int m = 0; m < batch; ++m) {
         h_active[m] = 1;
         h_iters[m] = 0;
         h_res[m] = 0.0;
+        h_best[m] = 0.0;
     }
     for (int it = 0; it <= max_iter && rc == HBEM_OK; ++it) {
         cudaError_t e = cudaMemsetAsync(norms, 0, sizeof(double) * 2 * batch, st);
@@ -2273,9 +2280,12 @@ int refine_noalloc(int n, int batch, const float *a_re, const float *a_im, long 
         if (e != cudaSuccess) { rc = cuda_fail(e, "hbem_refine_noalloc: sync"); break; }
         bool any = false;
         for (int m = 0; m < batch; ++m) {
+            if (!h_active[m]) continue;
             const double rel = h_norms[2 * m + 1] > 0 ? std::sqrt(h_norms[2 * m] / h_norms[2 * m + 1]) : 0.0;
-            h_res[m] = rel;
-            h_active[m] = (h_active[m] && rel > tol && it < max_iter) ? 1 : 0;
+            const bool stalled = it > 0 && !(rel < h_best[m]);
+            h_res[m] = stalled ? h_best[m] : rel;
+            h_best[m] = h_res[m];
+            h_active[m] = (!stalled && rel > tol && it < max_iter) ? 1 : 0;
             if (h_active[m]) { ++h_iters[m]; any = true; }
         }
         if (!any) break;
@@ -2289,8 +2299,9 @@ int refine_noalloc(int n, int batch, const float *a_re, const float *a_im, long 
         if (e != cudaSuccess) { rc = cuda_fail(e, "k_axpy_active"); break; }
         count_launch();
     }
-    if (rc == HBEM_OK && iters) {
-        cudaError_t e = cudaMemcpyAsync(iters, h_iters, sizeof(int) * batch, cudaMemcpyHostToDevice, st);
+    if (rc == HBEM_OK && (iters || resid)) {
+        cudaError_t e = cudaSuccess;
+        if (iters) e = cudaMemcpyAsync(iters, h_iters, sizeof(int) * batch, cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess && resid) e = cudaMemcpyAsync(resid, h_res, sizeof(double) * batch, cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) rc = cuda_fail(e, "hbem_refine_noalloc: results");
@@ -2337,6 +2348,8 @@ extern "C" int hbem_refine(int n, int batch, const float *a_re, const float *a_i
     if (!a_re || !a_im || !lu_re || !lu_im || !piv || !b_re || !b_im || !x_re || !x_im)
         return fail(HBEM_ERR_ARG, "hbem_refine: NULL pointer");
     if (x_stride < n || b_stride < n || max_iter < 0 || !(tol > 0)) return fail(HBEM_ERR_ARG, "hbem_refine: bad arguments");
+    if (lda < n || a_stride < lda * (long long)n || lu_stride < lda * (long long)n || piv_stride < n)
+        return fail(HBEM_ERR_ARG, "hbem_refine: lda/a_stride/lu_stride/piv_stride too small");
     return refine(n, batch, a_re, a_im, lda, a_stride, lu_re, lu_im, lu_stride, piv, piv_stride, b_re, b_im, b_stride,
                   x_re, x_im, x_stride, tol, max_iter, iters, resid, reinterpret_cast<cudaStream_t>(stream));
 }
@@ -2351,6 +2364,8 @@ extern "C" int hbem_refine_noalloc(int n, int batch, const float *a_re, const fl
         return fail(HBEM_ERR_ARG, "hbem_refine_noalloc: NULL pointer");
     if (x_stride < n || b_stride < n || max_iter < 0 || !(tol > 0))
         return fail(HBEM_ERR_ARG, "hbem_refine_noalloc: bad arguments");
+    if (lda < n || a_stride < lda * (long long)n || lu_stride < lda * (long long)n || piv_stride < n)
+        return fail(HBEM_ERR_ARG, "hbem_refine_noalloc: lda/a_stride/lu_stride/piv_stride too small");
     return refine_noalloc(n, batch, a_re, a_im, lda, a_stride, lu_re, lu_im, lu_stride, piv, piv_stride, b_re, b_im,
                           b_stride, x_re, x_im, x_stride, tol, max_iter, iters, resid,
                           reinterpret_cast<cudaStream_t>(stream));

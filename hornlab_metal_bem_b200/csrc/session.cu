@@ -254,7 +254,7 @@ void free_session(Session *s) {
     void *ptrs[] = {s->d_qp, s->d_nrm, s->d_tri, s->d_test_slot, s->d_trial_slot, s->d_row_off, s->d_rows,
                     s->d_col_off, s->d_cols, s->d_verts, s->d_tris, s->d_l2g, s->d_tags, s->d_areas,
                     s->d_normals, s->d_fqp, s->d_fnrm, s->d_pairs, s->d_rule, s->d_rule_w, s->d_status, s->ws,
-                    s->d_ap_tris, s->d_ap_local, s->d_sing_bits};
+                    s->d_ap_tris, s->d_ap_local, s->d_sing_bits, s->d_geo64};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (s->pinned) cudaFreeHost(s->pinned);

@@ -34,16 +34,25 @@ int launch_field(Session &s, int n_freq, const float *k_re, const float *p_re, c
                  float *out_im, long long out_stride, cudaStream_t st);
 int launch_tag_avg(Session &s, int n_freq, const float *p_re, const float *p_im, long long p_stride,
                    const int *d_want, int n_tags, double *out, cudaStream_t st);
+int lu_factor_f64(int n, int batch, double *a_re, double *a_im, long long lda, long long a_stride, int *piv,
+                  long long piv_stride, int *info, cudaStream_t st);
+int lu_solve_f64(int n, int nrhs, int batch, const double *lu_re, const double *lu_im, long long lda,
+                 long long a_stride, const int *piv, long long piv_stride, double *b_re, double *b_im, long long ldb,
+                 long long b_stride, cudaStream_t st);
+int widen_f64(int rows, int cols, int batch, const float *sr, const float *si, long long sld, long long sstride,
+              double *dr, double *di, long long dld, long long dstride, cudaStream_t st);
+int narrow_f64(int rows, int cols, int batch, const double *sr, const double *si, long long sld, long long sstride,
+               float *dr, float *di, long long dld, long long dstride, cudaStream_t st);
 
 namespace {
 
 size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
 
 struct Layout {
-    size_t q, a, a0, x, b, piv, info, obs, fld, tag, want, iters, resid, anorm, rcond, total;
+    size_t q, a, a0, a64, x64, x, b, piv, info, obs, fld, tag, want, iters, resid, anorm, rcond, total;
 };
 
-Layout layout(const Session &s, int nf, int n_obs, int n_tags, bool keep_a) {
+Layout layout(const Session &s, int nf, int n_obs, int n_tags, bool keep_a, bool fp64) {
     const size_t n = s.n_dof, T = s.n_triangles;
     Layout L{};
     size_t off = 0;
@@ -51,6 +60,8 @@ Layout layout(const Session &s, int nf, int n_obs, int n_tags, bool keep_a) {
     L.q = take(2 * sizeof(float) * nf * T);
     L.a = take(2 * sizeof(float) * nf * n * n);
     L.a0 = keep_a ? take(2 * sizeof(float) * nf * n * n) : 0;
+    L.a64 = fp64 ? take(2 * sizeof(double) * nf * n * n) : 0;
+    L.x64 = fp64 ? take(2 * sizeof(double) * nf * n) : 0;
     L.x = take(2 * sizeof(float) * nf * n);
     L.b = take(2 * sizeof(float) * nf * n);
     L.piv = take(sizeof(int) * nf * n);
@@ -96,14 +107,15 @@ extern "C" int hbem_solve_batch(hbem_session *h, int n_freq, const float *k_re, 
     if (n_tags > 0 && (!tags || !tag_avg)) return fail(HBEM_ERR_ARG, "hbem_solve_batch: NULL tag buffers");
     if (n_tags > 64) return fail(HBEM_ERR_ARG, "hbem_solve_batch: at most 64 tags");
     if ((surface_re == nullptr) != (surface_im == nullptr)) return fail(HBEM_ERR_ARG, "hbem_solve_batch: surface pointers");
-    if (precision != HBEM_PREC_PLAIN && precision != HBEM_PREC_MIXED)
+    if (precision != HBEM_PREC_PLAIN && precision != HBEM_PREC_MIXED && precision != HBEM_PREC_FP64)
         return fail(HBEM_ERR_ARG, "hbem_solve_batch: bad precision");
     for (int f = 0; f < n_freq; ++f)
         if (!std::isfinite(k_re[f]) || (k_im && !std::isfinite(k_im[f])))
             return fail(HBEM_ERR_ARG, "hbem_solve_batch: non-finite wavenumber");
     HBEM_CUDA(cudaSetDevice(s->device));
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    const bool do_refine = (precision == HBEM_PREC_MIXED) || refine_max_iter > 0;
+    const bool fp64 = precision == HBEM_PREC_FP64;
+    const bool do_refine = !fp64 && ((precision == HBEM_PREC_MIXED) || refine_max_iter > 0);
     const int max_iter = precision == HBEM_PREC_MIXED ? std::max(1, refine_max_iter) : refine_max_iter;
     const double tol = refine_tol > 0 ? refine_tol : 1e-6;
     const size_t n = s->n_dof, T = s->n_triangles;
@@ -113,8 +125,9 @@ extern "C" int hbem_solve_batch(hbem_session *h, int n_freq, const float *k_re, 
     HBEM_CUDA(cudaMemGetInfo(&free_b, &total_b));
     free_b += s->ws_bytes;
     int chunk = n_freq;
-    while (chunk > 1 && layout(*s, chunk, n_obs, n_tags, do_refine).total > free_b * 6 / 10) chunk = (chunk + 1) / 2;
-    const Layout L = layout(*s, chunk, n_obs, n_tags, do_refine);
+    while (chunk > 1 && layout(*s, chunk, n_obs, n_tags, do_refine, fp64).total > free_b * 6 / 10)
+        chunk = (chunk + 1) / 2;
+    const Layout L = layout(*s, chunk, n_obs, n_tags, do_refine, fp64);
     int rc = ensure_ws(*s, L.total);
     if (rc != HBEM_OK) return rc;
     char *ws = static_cast<char *>(s->ws);
@@ -133,6 +146,8 @@ extern "C" int hbem_solve_batch(hbem_session *h, int n_freq, const float *k_re, 
     double *dres = reinterpret_cast<double *>(ws + L.resid);
     float *danorm = reinterpret_cast<float *>(ws + L.anorm);
     double *drcond = reinterpret_cast<double *>(ws + L.rcond);
+    double *da64 = fp64 ? reinterpret_cast<double *>(ws + L.a64) : nullptr;
+    double *dx64 = fp64 ? reinterpret_cast<double *>(ws + L.x64) : nullptr;
 
     cudaEvent_t ev[5];
     for (auto &e : ev) HBEM_CUDA(cudaEventCreate(&e));
@@ -167,15 +182,42 @@ extern "C" int hbem_solve_batch(hbem_session *h, int n_freq, const float *k_re, 
             rc = matrix_norm1((int)n, nf, ar, ai, (long long)n, (long long)(n * n), danorm, st);
             if (rc != HBEM_OK) break;
         }
-        rc = lu_factor((int)n, nf, ar, ai, (long long)n, (long long)(n * n), dpiv, (long long)n, dinfo, precision, st);
-        if (rc != HBEM_OK) break;
-        if (rcond) {
-            rc = lu_rcond((int)n, nf, ar, ai, (long long)n, (long long)(n * n), danorm, drcond, st);
+        if (fp64) {
+            // the reference's float64 dense solve: widen the FP32 system to
+            // complex128, factor and solve in FP64, narrow the solution
+            const long long nn = (long long)(n * n);
+            double *a64r = da64, *a64i = da64 + (size_t)nf * n * n;
+            double *x64r = dx64, *x64i = dx64 + (size_t)nf * n;
+            rc = widen_f64((int)n, (int)n, nf, ar, ai, (long long)n, nn, a64r, a64i, (long long)n, nn, st);
+            if (rc == HBEM_OK)
+                rc = widen_f64(1, (int)n, nf, br, bi, (long long)n, (long long)n, x64r, x64i, (long long)n,
+                               (long long)n, st);
+            if (rc == HBEM_OK)
+                rc = lu_factor_f64((int)n, nf, a64r, a64i, (long long)n, nn, dpiv, (long long)n, dinfo, st);
+            if (rc == HBEM_OK)
+                rc = lu_solve_f64((int)n, 1, nf, a64r, a64i, (long long)n, nn, dpiv, (long long)n, x64r, x64i, 1,
+                                  (long long)n, st);
+            if (rc == HBEM_OK)
+                rc = narrow_f64(1, (int)n, nf, x64r, x64i, (long long)n, (long long)n, xr, xi, (long long)n,
+                                (long long)n, st);
+            if (rc == HBEM_OK && rcond) {
+                // condition estimate from the FP64 factors narrowed to FP32
+                rc = narrow_f64((int)n, (int)n, nf, a64r, a64i, (long long)n, nn, ar, ai, (long long)n, nn, st);
+                if (rc == HBEM_OK) rc = lu_rcond((int)n, nf, ar, ai, (long long)n, nn, danorm, drcond, st);
+            }
+            if (rc != HBEM_OK) break;
+        } else {
+            rc = lu_factor((int)n, nf, ar, ai, (long long)n, (long long)(n * n), dpiv, (long long)n, dinfo, precision,
+                           st);
+            if (rc != HBEM_OK) break;
+            if (rcond) {
+                rc = lu_rcond((int)n, nf, ar, ai, (long long)n, (long long)(n * n), danorm, drcond, st);
+                if (rc != HBEM_OK) break;
+            }
+            rc = lu_solve((int)n, 1, nf, ar, ai, (long long)n, (long long)(n * n), dpiv, (long long)n, xr, xi, 1,
+                          (long long)n, HBEM_TRANS_N, st);
             if (rc != HBEM_OK) break;
         }
-        rc = lu_solve((int)n, 1, nf, ar, ai, (long long)n, (long long)(n * n), dpiv, (long long)n, xr, xi, 1,
-                      (long long)n, HBEM_TRANS_N, st);
-        if (rc != HBEM_OK) break;
         if (do_refine) {
             rc = refine((int)n, nf, a0r, a0i, (long long)n, (long long)(n * n), ar, ai, (long long)(n * n), dpiv,
                         (long long)n, br, bi, (long long)n, xr, xi, (long long)n, tol, max_iter, diters, dres, st);

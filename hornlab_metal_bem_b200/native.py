@@ -37,6 +37,7 @@ HBEM_ASM_ZERO = 4
 HBEM_ASM_CORRECTED = 7
 HBEM_PREC_PLAIN = 0
 HBEM_PREC_MIXED = 1
+HBEM_PREC_FP64 = 2
 HBEM_TRANS_N, HBEM_TRANS_T, HBEM_TRANS_C = 0, 1, 2
 # aperture faces from which the coupled solve uses the augmented (m + n) system
 AUGMENTED_MIN_APERTURE = 512
@@ -92,6 +93,13 @@ _SIGNATURES = {
     "hbem_aperture_assemble": ([_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _c_int),
     "hbem_coupled_ib_schur": ([_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _c_int),
     "hbem_coupled_ib_field": ([_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _vp, _vp], _c_int),
+    "hbem_assemble_f64": ([_vp, _c_int, _vp, _vp, _vp, _vp, _c_ll, _vp, _vp, _vp, _vp, _c_ll, _c_ll, _vp, _vp, _c_ll,
+                           _c_int, _vp], _c_int),
+    "hbem_field_f64": ([_vp, _c_int, _vp, _vp, _vp, _c_ll, _vp, _vp, _c_ll, _vp, _c_int, _vp, _vp, _c_ll, _vp],
+                       _c_int),
+    "hbem_lu_factor_f64": ([_c_int, _c_int, _vp, _vp, _c_ll, _c_ll, _vp, _c_ll, _vp, _vp], _c_int),
+    "hbem_lu_solve_f64": ([_c_int, _c_int, _c_int, _vp, _vp, _c_ll, _c_ll, _vp, _c_ll, _vp, _vp, _c_ll, _c_ll,
+                           _c_int, _vp], _c_int),
 }
 
 _LIB: ctypes.CDLL | None = None
@@ -141,6 +149,23 @@ def _case_flags(k_re: float, k_im: float, *, robin: bool = False, coupled: bool 
     if field_k is not None and float(field_k) != float(k_re):
         out["field_k_real_f32"] = float(field_k)
     return out
+
+
+def solve_mode(precision: str, dense_solve_dtype: str = "float32") -> str:
+    """The dense-solve variant of a case: ``"fp64"`` for ``dense_solve_dtype="float64"`` (complex128 LU of the
+    widened FP32 system, the reference's zgesv path), else ``"mixed"`` (BF16x3 tensor-core LU) or ``"plain"``
+    (FP32 LU, the reference's cgesv); plain and mixed are followed by FP64-residual refinement when
+    ``refine_max_iterations`` > 0."""
+    if dense_solve_dtype == "float64":
+        return "fp64"
+    return "mixed" if precision == "mixed" else "plain"
+
+
+SOLVE_IMPL = {"plain": "hbem_blocked_lu_fp32", "mixed": "hbem_blocked_lu_bf16x3", "fp64": "hbem_blocked_lu_fp64"}
+
+
+def _refines(mode: str, max_iter) -> bool:
+    return mode == "mixed" or (mode == "plain" and int(max_iter) > 0)
 
 
 def check(status: int, what: str, lib: ctypes.CDLL | None = None) -> int:
@@ -286,6 +311,77 @@ class NativeSession:
             _stream_ptr(stream)), "hbem_assemble", self.lib)
         return Ar, Ai, b_re, b_im
 
+    def assemble_f64(self, k_re, q, *, k_imag=None, beta=None, flags: int = HBEM_ASM_CORRECTED, stream=None):
+        """The FP64 twin of :meth:`assemble` (``hbem_assemble_f64``): float64 CUDA tensors
+        ``(A_re, A_im, b_re, b_im)`` of shape (F, n, n) / (F, n), the same discretisation in double precision."""
+        torch = require_cuda()
+        k_re = np.ascontiguousarray(np.atleast_1d(k_re), dtype=np.float64)
+        F = k_re.shape[0]
+        k_im = None if k_imag is None else np.ascontiguousarray(np.atleast_1d(k_imag), dtype=np.float64)
+        dev = torch.device("cuda", self.device)
+        qz = np.asarray(q).reshape(F, self.n_triangles)
+        qr = torch.tensor(np.ascontiguousarray(qz.real, dtype=np.float64), device=dev)
+        qi = torch.tensor(np.ascontiguousarray(qz.imag, dtype=np.float64), device=dev)
+        br_ = bi_ = None
+        if beta is not None:
+            bz = np.asarray(beta).reshape(self.n_triangles)
+            br_ = torch.tensor(np.ascontiguousarray(bz.real, dtype=np.float64), device=dev)
+            bi_ = torch.tensor(np.ascontiguousarray(bz.imag, dtype=np.float64), device=dev)
+        n = self.n_dof
+        Ar = torch.empty((F, n, n), dtype=torch.float64, device=dev)
+        Ai = torch.empty_like(Ar)
+        b_re = torch.empty((F, n), dtype=torch.float64, device=dev)
+        b_im = torch.empty_like(b_re)
+        check(self.lib.hbem_assemble_f64(
+            self.handle, F, _np_ptr(k_re), _np_ptr(k_im), _t_ptr(qr), _t_ptr(qi), self.n_triangles, _t_ptr(br_),
+            _t_ptr(bi_), _t_ptr(Ar), _t_ptr(Ai), n, n * n, _t_ptr(b_re), _t_ptr(b_im), n, flags | HBEM_ASM_ZERO,
+            _stream_ptr(stream)), "hbem_assemble_f64", self.lib)
+        return Ar, Ai, b_re, b_im
+
+    def field_f64(self, k_re, p, q, obs_3xn, stream=None):
+        """The FP64 twin of :meth:`field`: p (F, n) and q (F, T) complex arrays or tensors in, (F, N) complex128
+        CUDA tensor out."""
+        torch = require_cuda()
+        k_re = np.ascontiguousarray(np.atleast_1d(k_re), dtype=np.float64)
+        F = k_re.shape[0]
+        dev = torch.device("cuda", self.device)
+
+        def planes(z, shape):
+            z = torch.as_tensor(z, device=dev).reshape(shape)
+            if z.is_complex():
+                return z.real.double().contiguous(), z.imag.double().contiguous()
+            return z.double().contiguous(), torch.zeros(shape, dtype=torch.float64, device=dev)
+
+        pr, pi = planes(p, (F, self.n_dof))
+        qr, qi = planes(q, (F, self.n_triangles))
+        obs = torch.as_tensor(np.ascontiguousarray(obs_3xn, dtype=np.float32), device=dev).contiguous()
+        N = obs.shape[1]
+        out_re = torch.empty((F, N), dtype=torch.float64, device=dev)
+        out_im = torch.empty_like(out_re)
+        check(self.lib.hbem_field_f64(
+            self.handle, F, _np_ptr(k_re), _t_ptr(pr), _t_ptr(pi), self.n_dof, _t_ptr(qr), _t_ptr(qi),
+            self.n_triangles, _t_ptr(obs), N, _t_ptr(out_re), _t_ptr(out_im), N, _stream_ptr(stream)),
+            "hbem_field_f64", self.lib)
+        return torch.complex(out_re, out_im)
+
+    def reference_solve_f64(self, k_re, q, obs_3xn, *, k_imag=None, beta=None):
+        """The FP64 path of one batch: corrected assembly, complex128 LU and solve, field, all in double
+        precision on the GPU.  Returns (surface pressure (F, n), field (F, N)) as complex128 CUDA tensors; the
+        error every FP32 result states is measured against these."""
+        Ar, Ai, br, bi = self.assemble_f64(k_re, q, k_imag=k_imag, beta=beta)
+        F = Ar.shape[0]
+        x_re, x_im = lu_solve_f64(Ar, Ai, br, bi)
+        p = torch_complex(x_re, x_im)
+        qz = np.asarray(q).reshape(F, self.n_triangles).astype(np.complex128)
+        if beta is not None:
+            # the field's Neumann data on Robin faces: q + i k beta p_avg (main.swift:1646-1674)
+            l2g = np.asarray(self.buffers.p1_local2global_i32)
+            k = np.atleast_1d(k_re).astype(np.float64)[:, None]
+            ki = (np.zeros_like(k) if k_imag is None else np.atleast_1d(k_imag).astype(np.float64)[:, None])
+            p_h = p.cpu().numpy()
+            qz = qz + (1j * k - ki) * np.asarray(beta).reshape(1, -1) * p_h[:, l2g].mean(axis=2)
+        return p, self.field_f64(k_re, p, qz, obs_3xn)
+
     @staticmethod
     def _split_device(z, shape, dev):
         import torch
@@ -351,9 +447,14 @@ class NativeSession:
         Same argument meaning as the reference (``native.py:737-764``):
         ``frequency_hz`` (F,), ``k_real_f32`` (F,) float32 wavenumbers,
         ``neumann_dp0`` (F, T) complex DP0 Neumann data, ``observation_points``
-        (3, N) or (N, 3).  ``dense_solve_dtype="float64"`` keeps the FP32 LU and
-        refines the solution with FP64 residuals to 1e-7 (the GPU analogue of
-        the reference's complex128 zgesv path).  ``compute_rcond`` adds the
+        (3, N) or (N, 3).  ``dense_solve_dtype="float64"`` factors the widened
+        system in complex128 (the reference's zgesv path).  Otherwise the FP32
+        (``precision="plain"``) or BF16x3 (``"mixed"``) LU solution is refined
+        with FP64 residuals (``refine_tolerance``, at most
+        ``refine_max_iterations`` passes, stopping when a pass no longer lowers
+        the residual: the reference's HORNLAB_METAL_BEM_NATIVE_DENSE_SOLVE_REFINE
+        passes, main.swift:6964-7070); ``refine_max_iterations=0`` leaves the
+        plain LU solution as cgesv gives it.  ``compute_rcond`` adds the
         1-norm condition estimate of each matrix (``dense_solve_rcond``), as the
         reference computes with cgecon for every case.
         """
@@ -369,7 +470,8 @@ class NativeSession:
             if any(per):
                 return self._robin_batch(freqs, k_re, k_imag_f32, neumann_dp0, observation_points, per,
                                          source_tags=source_tags, impedance_source_tag=impedance_source_tag,
-                                         write_surface_pressure=write_surface_pressure, precision=precision,
+                                         write_surface_pressure=write_surface_pressure,
+                                         precision=solve_mode(precision, dense_solve_dtype),
                                          refine_tolerance=refine_tolerance,
                                          refine_max_iterations=refine_max_iterations, timings_out=timings_out,
                                          compute_rcond=compute_rcond)
@@ -402,9 +504,12 @@ class NativeSession:
         resid = np.zeros(F, np.float64)
         rcond = np.zeros(F, np.float64) if compute_rcond else None
         tms = np.zeros(4, np.float32)
-        prec = HBEM_PREC_MIXED if precision == "mixed" else HBEM_PREC_PLAIN
-        max_it = int(refine_max_iterations) if (prec == HBEM_PREC_MIXED or dense_solve_dtype == "float64") else 0
-        tol = 1e-7 if (dense_solve_dtype == "float64" and prec == HBEM_PREC_PLAIN) else float(refine_tolerance)
+        mode = solve_mode(precision, dense_solve_dtype)
+        prec = {"plain": HBEM_PREC_PLAIN, "mixed": HBEM_PREC_MIXED, "fp64": HBEM_PREC_FP64}[mode]
+        max_it = 0 if mode == "fp64" else int(refine_max_iterations)
+        if mode == "mixed":
+            max_it = max(1, max_it)
+        tol = float(refine_tolerance)
         t0 = time.perf_counter()
         check(self.lib.hbem_solve_batch(
             self.handle, F, _np_ptr(k_re), _np_ptr(k_im), _np_ptr(qr), _np_ptr(qi), _np_ptr(obs), N,
@@ -420,7 +525,7 @@ class NativeSession:
         for f in range(F):
             avgs = {int(t): complex(tavg[f, j, 0], tavg[f, j, 1]) for j, t in enumerate(want)}
             diag = {
-                "dense_solve_impl": "hbem_blocked_lu_" + ("bf16x3_refined" if prec else "fp32"),
+                "dense_solve_impl": SOLVE_IMPL[mode] + ("_refined" if max_it > 0 else ""),
                 "dense_solve_dtype": dense_solve_dtype,
                 "precision": precision,
                 "refine_iterations": int(iters[f]),
@@ -471,7 +576,7 @@ class NativeSession:
         tags = list(source_tags or [])
         want = tags + ([impedance_source_tag] if impedance_source_tag is not None and impedance_source_tag not in tags
                        else [])
-        mixed = precision == "mixed"
+        mode = precision  # "plain", "mixed" or "fp64" (solve_mode)
         out_field = np.zeros((F, N), np.complex64)
         out_p = np.zeros((F, n), np.complex64)
         out_tavg = np.zeros((F, max(1, len(want))), np.complex128)
@@ -507,7 +612,7 @@ class NativeSession:
                                          _t_ptr(bi), n, HBEM_ASM_CORRECTED | HBEM_ASM_ZERO, st),
                   "hbem_assemble", self.lib)
             ev[1].record()
-            xr, xi, info, iters, resid, rc = self._factor_solve_refine(Ar, Ai, br, bi, n, Fg, mixed, refine_tolerance,
+            xr, xi, info, iters, resid, rc = self._factor_solve_refine(Ar, Ai, br, bi, n, Fg, mode, refine_tolerance,
                                                                      refine_max_iterations, compute_rcond)
             del Ar, Ai
             ev[2].record()
@@ -550,9 +655,13 @@ class NativeSession:
                 surface_pressure=out_p[f] if write_surface_pressure else None,
                 assembly_s=t_asm * 1e-3 / F, dense_solve_s=t_solve * 1e-3 / F, field_s=t_field * 1e-3 / F,
                 lapack_info=int(out_info[f]),
-                diagnostics={"dense_solve_impl": "hbem_blocked_lu_" + ("bf16x3_refined" if mixed else "fp32"),
-                             "precision": precision, "refine_iterations": int(out_iter[f]),
-                             "refine_residual_rel": float(out_res[f]) if mixed else None,
+                diagnostics={"dense_solve_impl": SOLVE_IMPL[mode] + ("_refined" if _refines(mode, refine_max_iterations)
+                                                                      else ""),
+                             "precision": "mixed" if mode == "mixed" else "plain",
+                             "dense_solve_dtype": "float64" if mode == "fp64" else "float32",
+                             "refine_iterations": int(out_iter[f]),
+                             "refine_residual_rel": (float(out_res[f]) if _refines(mode, refine_max_iterations)
+                                                     else None),
                              "dense_solve_rcond": (float(out_rc[f]) if compute_rcond and out_info[f] == 0 else None),
                              "robin_tags": sorted(int(t) for t in per_freq[f]),
                              "assembly_mode": "corrected",
@@ -565,7 +674,8 @@ class NativeSession:
                          field_k_f32=None, source_tags=None, impedance_source_tag=None,
                          write_surface_pressure=False, precision="plain", refine_tolerance=1e-6,
                          refine_max_iterations=10, timings_out=None, coupled_method="auto",
-                         max_chunk_bytes=None, compute_rcond=True, **_ignored) -> list[CaseResult]:
+                         max_chunk_bytes=None, compute_rcond=True, dense_solve_dtype="float32",
+                         **_ignored) -> list[CaseResult]:
         """Coupled interior BIE + Rayleigh half-space solve (the reference's aperture_tag path).
 
         ``coupled_method="schur"``: A - S_ia (2 S_aa)^-1 P_avg is factored per
@@ -604,12 +714,14 @@ class NativeSession:
         if obs.shape[0] != 3:
             obs = obs.T
         obs_t = torch.tensor(np.ascontiguousarray(obs, dtype=np.float32), device=dev)
-        mixed = precision == "mixed"
+        mode = solve_mode(precision, dense_solve_dtype)
+        # dense copies per system: the factored matrix, plus the original for refinement or the FP64 twin
+        copies = 3 if mode == "fp64" else (2 if _refines(mode, refine_max_iterations) else 1)
         N = n + m
         if method == "augmented":
-            per_freq = 8 * (N * N * (2 if mixed else 1) + n * m + m * m + 4 * N)
+            per_freq = 8 * (N * N * copies + n * m + m * m + 4 * N)
         else:
-            per_freq = 8 * (n * n * (2 if mixed else 1) + 2 * n * m + 2 * m * m + 4 * n)
+            per_freq = 8 * (n * n * copies + 2 * n * m + 2 * m * m + 4 * n)
         if max_chunk_bytes is None:
             free, _ = torch.cuda.mem_get_info(dev)
             max_chunk_bytes = free // 2
@@ -622,7 +734,7 @@ class NativeSession:
             sl = slice(f0, min(F, f0 + chunk))
             run = self._coupled_chunk_augmented if method == "augmented" else self._coupled_chunk_schur
             parts.append(run(k_re[sl], None if k_im is None else k_im[sl], kf[sl], q_all[sl], obs_t, want,
-                             mixed, refine_tolerance, refine_max_iterations, times, compute_rcond))
+                             mode, refine_tolerance, refine_max_iterations, times, compute_rcond))
         if timings_out is not None:
             timings_out.update(assembly_ms=times[0], solve_ms=times[1], field_ms=times[2], coupled_method=method,
                                frequency_chunk=chunk)
@@ -640,8 +752,12 @@ class NativeSession:
                 lapack_info=int(cat["info"][f] or cat["info_ap"][f]),
                 diagnostics={"coupled_ib": True, "ib_coupled_solve": method, "aperture_triangles": m,
                              "aperture_neumann": cat["qa"][f], "aperture_lapack_info": int(cat["info_ap"][f]),
-                             "precision": precision, "refine_iterations": int(cat["iters"][f]),
-                             "refine_residual_rel": float(cat["resid"][f]) if mixed else None,
+                             "precision": precision, "dense_solve_dtype": dense_solve_dtype,
+                             "dense_solve_impl": SOLVE_IMPL[mode] + ("_refined" if _refines(mode, refine_max_iterations)
+                                                                     else ""),
+                             "refine_iterations": int(cat["iters"][f]),
+                             "refine_residual_rel": (float(cat["resid"][f]) if _refines(mode, refine_max_iterations)
+                                                     else None),
                              "dense_solve_rcond": (float(cat["rcond"][f]) if "rcond" in cat and cat["info"][f] == 0
                                                    else None),
                              "assembly_mode": "corrected",
@@ -650,9 +766,11 @@ class NativeSession:
             ))
         return out
 
-    def _factor_solve_refine(self, Kr, Ki, br, bi, N, F, mixed, tol, max_iter, rcond=False):
-        """LU (+ BF16x3 refinement) of F systems of order N stored (F, N, lda); returns x, info, iters,
-        resid and the 1-norm reciprocal condition estimates (or None)."""
+    def _factor_solve_refine(self, Kr, Ki, br, bi, N, F, mode, tol, max_iter, rcond=False):
+        """Factor and solve F systems of order N stored (F, N, lda): ``mode`` "plain" (FP32 LU) or "mixed"
+        (BF16x3 LU), each refined with FP64 residuals when ``max_iter`` > 0 (mixed: at least one pass), or
+        "fp64" (complex128 LU of the widened system, solution narrowed to FP32).  Returns x, info, iters, resid
+        and the 1-norm reciprocal condition estimates (or None).  Kr/Ki are overwritten by FP32 factors."""
         import torch
 
         dev, st = Kr.device, _stream_ptr()
@@ -663,13 +781,35 @@ class NativeSession:
             rc = torch.empty(F, dtype=torch.float64, device=dev)
             check(self.lib.hbem_matrix_norm1(N, F, _t_ptr(Kr), _t_ptr(Ki), lda, N * lda, _t_ptr(anorm), st),
                   "hbem_matrix_norm1", self.lib)
-        K0r = K0i = None
-        if mixed:
-            K0r, K0i = Kr.clone(), Ki.clone()
         piv = torch.empty((F, N), dtype=torch.int32, device=dev)
         info = torch.empty(F, dtype=torch.int32, device=dev)
+        iters = torch.zeros(F, dtype=torch.int32, device=dev)
+        resid = torch.zeros(F, dtype=torch.float64, device=dev)
+        if mode == "fp64":
+            K64r, K64i = Kr.double().contiguous(), Ki.double().contiguous()
+            x64r, x64i = br.double().contiguous(), bi.double().contiguous()
+            check(self.lib.hbem_lu_factor_f64(N, F, _t_ptr(K64r), _t_ptr(K64i), lda, N * lda, _t_ptr(piv), N,
+                                              _t_ptr(info), st), "hbem_lu_factor_f64", self.lib)
+            check(self.lib.hbem_lu_solve_f64(N, 1, F, _t_ptr(K64r), _t_ptr(K64i), lda, N * lda, _t_ptr(piv), N,
+                                             _t_ptr(x64r), _t_ptr(x64i), 1, N, HBEM_TRANS_N, st),
+                  "hbem_lu_solve_f64", self.lib)
+            xr, xi = x64r.float(), x64i.float()
+            if rcond:
+                # condition estimate from the FP64 factors narrowed to FP32
+                Kr.copy_(K64r)
+                Ki.copy_(K64i)
+                check(self.lib.hbem_lu_rcond(N, F, _t_ptr(Kr), _t_ptr(Ki), lda, N * lda, _t_ptr(anorm), _t_ptr(rc),
+                                             st), "hbem_lu_rcond", self.lib)
+            del K64r, K64i
+            return xr, xi, info, iters, resid, rc
+        refine = _refines(mode, max_iter)
+        if mode == "mixed":
+            max_iter = max(1, int(max_iter))
+        K0r = K0i = None
+        if refine:
+            K0r, K0i = Kr.clone(), Ki.clone()
         xr, xi = br.clone(), bi.clone()
-        prec = HBEM_PREC_MIXED if mixed else HBEM_PREC_PLAIN
+        prec = HBEM_PREC_MIXED if mode == "mixed" else HBEM_PREC_PLAIN
         check(self.lib.hbem_lu_factor(N, F, _t_ptr(Kr), _t_ptr(Ki), lda, N * lda, _t_ptr(piv), N, _t_ptr(info), prec,
                                       st), "hbem_lu_factor", self.lib)
         if rcond:
@@ -677,9 +817,7 @@ class NativeSession:
                   "hbem_lu_rcond", self.lib)
         check(self.lib.hbem_lu_solve(N, 1, F, _t_ptr(Kr), _t_ptr(Ki), lda, N * lda, _t_ptr(piv), N, _t_ptr(xr),
                                      _t_ptr(xi), 1, N, HBEM_TRANS_N, st), "hbem_lu_solve", self.lib)
-        iters = torch.zeros(F, dtype=torch.int32, device=dev)
-        resid = torch.zeros(F, dtype=torch.float64, device=dev)
-        if mixed:
+        if refine:
             check(self.lib.hbem_refine(N, F, _t_ptr(K0r), _t_ptr(K0i), lda, N * lda, _t_ptr(Kr), _t_ptr(Ki), N * lda,
                                        _t_ptr(piv), N, _t_ptr(br), _t_ptr(bi), N, _t_ptr(xr), _t_ptr(xi), N,
                                        float(tol), int(max_iter), _t_ptr(iters), _t_ptr(resid), st),
@@ -687,7 +825,7 @@ class NativeSession:
             del K0r, K0i
         return xr, xi, info, iters, resid, rc
 
-    def _coupled_chunk_schur(self, k_re, k_im, kf, q, obs_t, want, mixed, tol, max_iter, times, rcond=False):
+    def _coupled_chunk_schur(self, k_re, k_im, kf, q, obs_t, want, mode, tol, max_iter, times, rcond=False):
         import torch
 
         dev, st = obs_t.device, _stream_ptr()
@@ -707,7 +845,7 @@ class NativeSession:
                                              _t_ptr(info_ap), st), "hbem_coupled_ib_schur", self.lib)
         del sia_r, sia_i, saa_r, saa_i
         ev[1].record()
-        xr, xi, info, iters, resid, rc = self._factor_solve_refine(Ar, Ai, br, bi, n, F, mixed, tol, max_iter, rcond)
+        xr, xi, info, iters, resid, rc = self._factor_solve_refine(Ar, Ai, br, bi, n, F, mode, tol, max_iter, rcond)
         del Ar, Ai
         ev[2].record()
         qa_r = torch.empty((F, m), dtype=torch.float32, device=dev); qa_i = torch.empty_like(qa_r)
@@ -751,7 +889,7 @@ class NativeSession:
               "hbem_coupled_ib_augment", self.lib)
         return Kr, Ki, rr, ri, alpha
 
-    def _coupled_chunk_augmented(self, k_re, k_im, kf, q, obs_t, want, mixed, tol, max_iter, times, rcond=False):
+    def _coupled_chunk_augmented(self, k_re, k_im, kf, q, obs_t, want, mode, tol, max_iter, times, rcond=False):
         import torch
 
         dev, st = obs_t.device, _stream_ptr()
@@ -761,7 +899,7 @@ class NativeSession:
         ev[0].record()
         Kr, Ki, rr, ri, alpha = self.coupled_ib_system(k_re, k_im, kf, q)
         ev[1].record()
-        xr, xi, info, iters, resid, rc = self._factor_solve_refine(Kr, Ki, rr, ri, N, F, mixed, tol, max_iter, rcond)
+        xr, xi, info, iters, resid, rc = self._factor_solve_refine(Kr, Ki, rr, ri, N, F, mode, tol, max_iter, rcond)
         del Kr, Ki
         ev[2].record()
         qa_r, qa_i = (xr[:, :m] * alpha[:, None]).contiguous(), (xi[:, :m] * alpha[:, None]).contiguous()
@@ -791,6 +929,34 @@ class NativeSession:
 MetalNativeStandardSession = NativeSession
 
 
+def torch_complex(re, im):
+    import torch
+
+    return torch.complex(re, im)
+
+
+def lu_solve_f64(A_re, A_im, b_re, b_im, nrhs: int = 1):
+    """Factor (F, n, n) float64 CUDA tensors with ``hbem_lu_factor_f64`` (copies: the inputs are kept) and solve
+    (F, n) right-hand sides (or (F, n, nrhs)) with ``hbem_lu_solve_f64``.  Raises on a zero pivot."""
+    import torch
+
+    lib = load_library()
+    F, n = int(A_re.shape[0]), int(A_re.shape[1])
+    Ar, Ai = A_re.clone().contiguous(), A_im.clone().contiguous()
+    xr, xi = b_re.clone().contiguous(), b_im.clone().contiguous()
+    piv = torch.empty((F, n), dtype=torch.int32, device=A_re.device)
+    info = torch.empty(F, dtype=torch.int32, device=A_re.device)
+    st = _stream_ptr()
+    check(lib.hbem_lu_factor_f64(n, F, _t_ptr(Ar), _t_ptr(Ai), n, n * n, _t_ptr(piv), n, _t_ptr(info), st),
+          "hbem_lu_factor_f64", lib)
+    check(lib.hbem_lu_solve_f64(n, nrhs, F, _t_ptr(Ar), _t_ptr(Ai), n, n * n, _t_ptr(piv), n, _t_ptr(xr), _t_ptr(xi),
+                                nrhs, n * nrhs, HBEM_TRANS_N, st), "hbem_lu_solve_f64", lib)
+    bad = info.cpu().numpy()
+    if np.any(bad != 0):
+        raise RuntimeError(f"hbem_lu_factor_f64: zero pivot (info {bad.tolist()})")
+    return xr, xi
+
+
 class ResidentSweep:
     """Device-resident batched sweep: inputs and outputs stay in HBM.
 
@@ -801,7 +967,7 @@ class ResidentSweep:
     """
 
     def __init__(self, session: NativeSession, k_re, k_im, q, obs_3xn, tags, precision: str = "plain",
-                 rcond: bool = False):
+                 rcond: bool = False, refine_tolerance: float = 1e-6, refine_max_iterations: int = 10):
         torch = require_cuda()
         self.s = session
         self.lib = session.lib
@@ -828,6 +994,15 @@ class ResidentSweep:
         self.precision = HBEM_PREC_MIXED if precision == "mixed" else HBEM_PREC_PLAIN
         self.rcond = torch.empty(F, dtype=torch.float64, device=dev) if rcond else None
         self.anorm = torch.empty(F, dtype=torch.float32, device=dev) if rcond else None
+        mode = "mixed" if precision == "mixed" else "plain"
+        self.refine_tol = float(refine_tolerance)
+        self.refine_max = max(1, int(refine_max_iterations)) if mode == "mixed" else int(refine_max_iterations)
+        self.refine = _refines(mode, refine_max_iterations)
+        # the assembled matrices kept for the FP64 residuals of the refinement
+        self.A0_re = torch.empty_like(self.A_re) if self.refine else None
+        self.A0_im = torch.empty_like(self.A_im) if self.refine else None
+        self.iters = torch.zeros(F, dtype=torch.int32, device=dev)
+        self.resid = torch.zeros(F, dtype=torch.float64, device=dev)
 
     def assemble(self, stream=None):
         n = self.n
@@ -840,6 +1015,9 @@ class ResidentSweep:
         n, st = self.n, _stream_ptr(stream)
         self.x_re.copy_(self.b_re)
         self.x_im.copy_(self.b_im)
+        if self.refine:
+            self.A0_re.copy_(self.A_re)
+            self.A0_im.copy_(self.A_im)
         if self.rcond is not None:
             check(self.lib.hbem_matrix_norm1(n, self.F, _t_ptr(self.A_re), _t_ptr(self.A_im), n, n * n,
                                              _t_ptr(self.anorm), st), "hbem_matrix_norm1", self.lib)
@@ -851,6 +1029,12 @@ class ResidentSweep:
         check(self.lib.hbem_lu_solve(n, 1, self.F, _t_ptr(self.A_re), _t_ptr(self.A_im), n, n * n, _t_ptr(self.piv), n,
                                      _t_ptr(self.x_re), _t_ptr(self.x_im), 1, n, HBEM_TRANS_N, st), "hbem_lu_solve",
               self.lib)
+        if self.refine:
+            check(self.lib.hbem_refine(
+                n, self.F, _t_ptr(self.A0_re), _t_ptr(self.A0_im), n, n * n, _t_ptr(self.A_re), _t_ptr(self.A_im),
+                n * n, _t_ptr(self.piv), n, _t_ptr(self.b_re), _t_ptr(self.b_im), n, _t_ptr(self.x_re),
+                _t_ptr(self.x_im), n, self.refine_tol, self.refine_max, _t_ptr(self.iters), _t_ptr(self.resid), st),
+                "hbem_refine", self.lib)
 
     def field(self, stream=None):
         st = _stream_ptr(stream)

@@ -47,6 +47,7 @@ extern "C" {
 /* LU precision */
 #define HBEM_PREC_PLAIN 0      /* FP32-accurate trailing updates (complex64 cgesv semantics) */
 #define HBEM_PREC_MIXED 1      /* BF16x3 tensor-core trailing updates; pair with hbem_refine */
+#define HBEM_PREC_FP64 2       /* hbem_solve_batch only: complex128 LU of the widened FP32 system (zgesv semantics) */
 
 /* Solve transposition */
 #define HBEM_TRANS_N 0
@@ -186,7 +187,10 @@ int hbem_lu_solve(int n, int nrhs, int batch, const float *lu_re, const float *l
 /*
  * FP64-residual iterative refinement of X for A X = B (nrhs = 1 per matrix):
  * r = b - A x in FP64 from the ORIGINAL matrix, d = LU \ r, x += d, until
- * ||r|| / ||b|| <= tol or max_iter passes.  iters/resid: device per matrix.
+ * ||r||_2 / ||b||_2 <= tol, max_iter passes, or a pass that no longer lowers
+ * the residual (as the reference stops).  The LU factors are read with A's
+ * leading dimension lda (lu_stride >= lda * n).  iters/resid: device per
+ * matrix, either may be NULL.
  * Replaces: refineDenseSolveSolution (main.swift:6964-7070).
  */
 int hbem_refine(int n, int batch, const float *a_re, const float *a_im, long long lda, long long a_stride,
@@ -275,6 +279,10 @@ int hbem_reduce_tag_avg_device(hbem_session *s, int n_freq, const float *p_re, c
  *   rcond (n_freq,) or NULL: 1-norm reciprocal condition estimate of each
  *   matrix (as cgecon; NULL skips the estimate);
  *   timings_ms (4,) = assembly, solve, field, total (device event times) or NULL.
+ * precision: HBEM_PREC_PLAIN, HBEM_PREC_MIXED (with refinement) or
+ *   HBEM_PREC_FP64 (dense_solve_dtype "float64": the FP32-assembled system
+ *   widened to complex128, factored and solved in FP64, the solution narrowed
+ *   to complex64 for the field; rcond from the factors narrowed to FP32).
  */
 int hbem_solve_batch(hbem_session *s, int n_freq, const float *k_re, const float *k_im,
                      const float *q_re, const float *q_im,
@@ -357,6 +365,42 @@ int hbem_assemble_backward(hbem_session *s, int n_freq, const float *k_re, const
                            const float *p_re, const float *p_im, long long p_stride,
                            const float *q_re, const float *q_im, long long q_stride,
                            double *grad_3xv, void *stream);
+
+/*
+ * FP64 path: the corrected assembly, the exterior field and a complex128 LU in
+ * double precision on the GPU.  Same discretisation as the FP32 entry points
+ * (6-point rule on far pairs with images, row weight, mass and Robin terms,
+ * the 4^4-point Duffy rules on touching pairs, built in double), evaluated in
+ * double from the session's float32 geometry: the difference between an FP32
+ * result and its FP64 twin is the FP32 arithmetic error, which every result
+ * line states.  Replaces the reference's own FP64 checks: the assembly parity
+ * gate (main.swift:8257-8307) and the float64 dense solve (zgesv on the
+ * widened system, main.swift:7101-7185).
+ *
+ * hbem_assemble_f64: as hbem_assemble with double buffers (k on the host, q,
+ *   beta, A, b on the device).
+ * hbem_field_f64: as hbem_field with double p, q and output (obs stays float).
+ * hbem_lu_factor_f64: batched in-place complex128 LU with partial pivoting
+ *   (getrf semantics: first maximum of |re| + |im|; piv 0-based; info 0 or the
+ *   1-based index of the first zero pivot), n <= 131072, batch <= 65535.
+ * hbem_lu_solve_f64: op(A) X = B with those factors, HBEM_TRANS_N only;
+ *   B (n, nrhs) row-major with leading dimension ldb; batch * nrhs <= 65535.
+ */
+int hbem_assemble_f64(hbem_session *s, int n_freq, const double *k_re, const double *k_im,
+                      const double *q_re, const double *q_im, long long q_stride,
+                      const double *beta_re, const double *beta_im,
+                      double *a_re, double *a_im, long long lda, long long a_stride,
+                      double *b_re, double *b_im, long long b_stride, int flags, void *stream);
+int hbem_field_f64(hbem_session *s, int n_freq, const double *k_re,
+                   const double *p_re, const double *p_im, long long p_stride,
+                   const double *q_re, const double *q_im, long long q_stride,
+                   const float *obs_3xn, int n_obs,
+                   double *out_re, double *out_im, long long out_stride, void *stream);
+int hbem_lu_factor_f64(int n, int batch, double *a_re, double *a_im, long long lda, long long a_stride,
+                       int *piv, long long piv_stride, int *info, void *stream);
+int hbem_lu_solve_f64(int n, int nrhs, int batch, const double *lu_re, const double *lu_im, long long lda,
+                      long long a_stride, const int *piv, long long piv_stride,
+                      double *b_re, double *b_im, long long ldb, long long b_stride, int trans, void *stream);
 
 #ifdef __cplusplus
 }

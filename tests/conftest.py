@@ -56,3 +56,44 @@ def grid_from_buffers(b):
 @pytest.fixture
 def rng():
     return np.random.default_rng(1234)
+
+
+def oracle_sweep(mesh, res, config, sym=0, systems=None):
+    """The reference's corrected path in FP64 (oracle assembly, LAPACK zgesv, oracle field) at the
+    frequencies of a ``SolveResult``: returns (surface pressure (F, n), field (F, N_obs)).  When a
+    list is passed as ``systems``, each frequency's (A, b, q) is appended to it."""
+    from hornlab_metal_bem_b200.bie import build_source_face_scale
+    from hornlab_metal_bem_b200.geometry import build_geometry_buffers
+    from hornlab_metal_bem_b200.mesh import make_pure_function_spaces
+    from hornlab_metal_bem_b200.observation import infer_frame
+    from hornlab_metal_bem_b200.sweep import field_points_3xn, k_values, neumann_rows
+    from oracle.oracle import Oracle, dense_solve
+
+    p1, dp0 = make_pure_function_spaces(mesh.grid)
+    buf = build_geometry_buffers(mesh.grid, mesh.physical_tags, p1, dp0)
+    o = Oracle(buf, sym, "f64")
+    frame = infer_frame(mesh.grid, mesh.physical_tags, source_tag=min(config.velocity_sources),
+                        symmetry_plane=config.native_symmetry_plane)
+    scale = build_source_face_scale(mesh.grid, mesh.physical_tags, config, frame.axis, frame.source_center)
+    k_re, _ = k_values(res.frequencies_hz, config)
+    q = neumann_rows(buf.n_triangles, mesh.physical_tags, res.frequencies_hz, config, scale)
+    pts = field_points_3xn(res.observation_points)
+    beta = None
+    if config.impedance_sources:
+        beta = np.zeros(buf.n_triangles, np.complex64)
+        for tag, bv in config.impedance_sources.items():
+            beta[np.asarray(mesh.physical_tags) == int(tag)] = complex(bv)
+    l2g = np.asarray(buf.p1_local2global_i32)
+    out_p, out_f = [], []
+    for f in range(len(res.frequencies_hz)):
+        A, b = o.corrected(float(k_re[f]), q[f], 0.0, beta)
+        p = dense_solve(A, b, "f64")
+        if systems is not None:
+            systems.append((A, b, q[f]))
+        out_p.append(p)
+        q_f = q[f].astype(np.complex128)
+        if beta is not None:
+            # the field's Neumann data on Robin faces: q + i k beta p_avg (main.swift:1646-1674)
+            q_f = q_f + 1j * float(k_re[f]) * beta * p[l2g].mean(axis=1)
+        out_f.append(o.field(float(k_re[f]), p, q_f, pts))
+    return np.array(out_p), np.array(out_f)

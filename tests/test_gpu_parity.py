@@ -50,8 +50,9 @@ def _host(t_re, t_im):
 
 
 @pytest.mark.parametrize("name", ["tiny", "near", "ico2", "horn_quarter", "yzxz_quarter", "yz_half", "xy_half"])
-@pytest.mark.parametrize("k", [1.8318326, 18.3, 91.6])
+@pytest.mark.parametrize("k", [1.8318326, 18.3, 91.6, 250.0, 366.366])
 def test_corrected_assembly_matches_oracle(name, k):
+    """k up to 366.366 rad/m: 20 kHz, the top of the benchmark sweep."""
     b = golden_buffers(name)
     o = Oracle(b, SYM[name], "f64")
     q = _q(b.n_triangles)

@@ -6,7 +6,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from oracle.oracle import Oracle, dense_solve
+from conftest import oracle_sweep
 
 pytestmark = pytest.mark.gpu
 
@@ -16,41 +16,7 @@ if not torch.cuda.is_available():  # pragma: no cover
 
 import hornlab_metal_bem_b200 as hb  # noqa: E402
 from hornlab_metal_bem_b200 import generators as G  # noqa: E402
-from hornlab_metal_bem_b200.geometry import build_geometry_buffers  # noqa: E402
-from hornlab_metal_bem_b200.mesh import make_pure_function_spaces  # noqa: E402
-from hornlab_metal_bem_b200.sweep import directivity_from_pressure, field_points_3xn  # noqa: E402
-
-
-def _oracle_sweep(mesh, res, config, sym=0):
-    p1, dp0 = make_pure_function_spaces(mesh.grid)
-    buf = build_geometry_buffers(mesh.grid, mesh.physical_tags, p1, dp0)
-    o = Oracle(buf, sym, "f64")
-    from hornlab_metal_bem_b200.sweep import k_values, neumann_rows
-    from hornlab_metal_bem_b200.bie import build_source_face_scale
-    from hornlab_metal_bem_b200.observation import infer_frame
-
-    frame = infer_frame(mesh.grid, mesh.physical_tags, source_tag=min(config.velocity_sources), symmetry_plane=config.native_symmetry_plane)
-    scale = build_source_face_scale(mesh.grid, mesh.physical_tags, config, frame.axis, frame.source_center)
-    k_re, _ = k_values(res.frequencies_hz, config)
-    q = neumann_rows(buf.n_triangles, mesh.physical_tags, res.frequencies_hz, config, scale)
-    pts = field_points_3xn(res.observation_points)
-    beta = None
-    if config.impedance_sources:
-        beta = np.zeros(buf.n_triangles, np.complex64)
-        for tag, bv in config.impedance_sources.items():
-            beta[np.asarray(mesh.physical_tags) == int(tag)] = complex(bv)
-    l2g = np.asarray(buf.p1_local2global_i32)
-    out_p, out_f = [], []
-    for f in range(len(res.frequencies_hz)):
-        A, b = o.corrected(float(k_re[f]), q[f], 0.0, beta)
-        p = dense_solve(A, b, "f64")
-        out_p.append(p)
-        q_f = q[f].astype(np.complex128)
-        if beta is not None:
-            # the field's Neumann data on Robin faces: q + i k beta p_avg (main.swift:1646-1674)
-            q_f = q_f + 1j * float(k_re[f]) * beta * p[l2g].mean(axis=1)
-        out_f.append(o.field(float(k_re[f]), p, q_f, pts))
-    return np.array(out_p), np.array(out_f)
+from hornlab_metal_bem_b200.sweep import directivity_from_pressure  # noqa: E402
 
 
 def test_pulsating_sphere_solve_matches_oracle_and_analytic():
@@ -62,7 +28,7 @@ def test_pulsating_sphere_solve_matches_oracle_and_analytic():
     )
     res = hb.solve(mesh, cfg)
     assert res.pressure_complex.shape == (8, 1, 37)
-    p_ref, f_ref = _oracle_sweep(mesh, res, cfg)
+    p_ref, f_ref = oracle_sweep(mesh, res, cfg)
     for f in range(8):
         sp = res.surface_pressure_complex[f]
         assert np.linalg.norm(sp - p_ref[f]) / np.linalg.norm(p_ref[f]) < 1e-4
@@ -88,7 +54,7 @@ def test_quarter_horn_solve_matches_oracle():
         return_surface_pressure=True,
     )
     res = hb.solve(mesh, cfg)
-    p_ref, f_ref = _oracle_sweep(mesh, res, cfg, sym=3)
+    p_ref, f_ref = oracle_sweep(mesh, res, cfg, sym=3)
     for f in range(3):
         assert np.linalg.norm(res.surface_pressure_complex[f] - p_ref[f]) / np.linalg.norm(p_ref[f]) < 1e-4
         fld = res.pressure_complex[f].reshape(-1)
@@ -144,7 +110,7 @@ def test_robin_walls_match_oracle():
                 return_surface_pressure=True)
     cfg = hb.native_config(impedance_sources={1: 0.35 + 0.12j}, **base)
     res = hb.solve(mesh, cfg)
-    p_ref, f_ref = _oracle_sweep(mesh, res, cfg, sym=3)
+    p_ref, f_ref = oracle_sweep(mesh, res, cfg, sym=3)
     for f in range(3):
         assert np.linalg.norm(res.surface_pressure_complex[f] - p_ref[f]) / np.linalg.norm(p_ref[f]) < 1e-4
         fld = res.pressure_complex[f].reshape(-1)
