@@ -18,8 +18,10 @@ corrected assembly -> LU -> solve -> exterior field -> tag reductions.
   oracle port; the reference itself needs Apple Metal/Accelerate), same
   metric and config, rank 0 only.
 
-Multi-GPU (torchrun): replicas only -- every rank sweeps its own copy of the
-workload (frequencies are independent); no collective on the data path.
+Multi-GPU (torchrun, N ranks): frequencies are independent, so the job at N
+GPUs is a sweep of 40 N log-spaced frequencies over the same band, dealt out
+round-robin (equal cost per frequency on one mesh), 40 per rank (weak
+scaling); each step ends with an all-gather of the fields to every rank.
 """
 from __future__ import annotations
 
@@ -61,9 +63,11 @@ def parse():
 
 
 # --------------------------------------------------------------------------- workload
-def workload(name: str):
+def workload(name: str, world: int = 1, rank: int = 0):
     """C2: seeded yz+xz quarter exponential horn, ~1k P1 dofs, 40 log freqs 0.5-20 kHz, 3 x 37 obs at 2 m.
-    C1: icosphere level 3 (642 dofs), 8 log freqs 0.2-5 kHz, 1 x 37 obs."""
+    C1: icosphere level 3 (642 dofs), 8 log freqs 0.2-5 kHz, 1 x 37 obs.
+    With ``world`` ranks the sweep has ``world`` times the frequencies over the same band and this rank takes
+    every ``world``-th one from ``rank`` (C2 and C1)."""
     import hornlab_metal_bem_b200 as hb
     from hornlab_metal_bem_b200 import generators as G
     from hornlab_metal_bem_b200.bie import build_source_face_scale
@@ -76,12 +80,12 @@ def workload(name: str):
         spec = G.horn_spec_from_seed(0, edge=0.007)
         mesh = G.horn(spec, quarter=True)
         cfg = hb.native_config(
-            freq_min_hz=500.0, freq_max_hz=20000.0, freq_count=40, source_motion="axial",
+            freq_min_hz=500.0, freq_max_hz=20000.0, freq_count=40 * world, source_motion="axial",
             native_symmetry_plane="yz+xz", native_check_open_edges=False,
             observation=hb.ObservationConfig(planes=["horizontal", "vertical", "diagonal"], angle_count=37),
         )
         desc = (f"C2 yz+xz quarter exponential horn (seed 0: flare {spec.flare:.2f} 1/m, lip {spec.lip * 1e3:.2f} mm), "
-                "40 log freqs 0.5-20 kHz, 3x37 obs @ 2 m")
+                f"{40 * world} log freqs 0.5-20 kHz, 3x37 obs @ 2 m")
     elif name == "c4":
         spec = G.horn_spec_from_seed(0, edge=0.004)
         mesh = G.baffled_horn(spec, aperture_tag=12)
@@ -93,22 +97,37 @@ def workload(name: str):
                 "aperture tag 12 at z=0, 20 log freqs 1-20 kHz, 3x37 obs @ 2 m")
     else:
         mesh = G.icosphere(3, 0.1)
-        cfg = hb.native_config(freq_min_hz=200.0, freq_max_hz=5000.0, freq_count=8, velocity_mode="velocity",
+        cfg = hb.native_config(freq_min_hz=200.0, freq_max_hz=5000.0, freq_count=8 * world, velocity_mode="velocity",
                                air_density=1.205,
                                observation=hb.ObservationConfig(planes=["horizontal"], angle_count=37))
-        desc = "C1 pulsating icosphere L3, 8 log freqs 0.2-5 kHz, 1x37 obs @ 2 m"
+        desc = f"C1 pulsating icosphere L3, {8 * world} log freqs 0.2-5 kHz, 1x37 obs @ 2 m"
     frame = hb._resolve_frame(mesh, cfg)
     obs, _ = build_observation_points(frame, cfg.observation)
     p1, dp0 = make_pure_function_spaces(mesh.grid)
     buf = build_geometry_buffers(mesh.grid, mesh.physical_tags, p1, dp0)
-    freqs = build_frequency_grid(cfg)
+    freqs_all = build_frequency_grid(cfg)
+    freqs = freqs_all[rank::world] if name in ("c1", "c2") else freqs_all
     k_re, k_im = k_values(freqs, cfg)
     scale = build_source_face_scale(mesh.grid, mesh.physical_tags, cfg, frame.axis, frame.source_center)
     q = neumann_rows(buf.n_triangles, mesh.physical_tags, freqs, cfg, scale)
     sym = {None: 0, "yz+xz": 3}[cfg.native_symmetry_plane]
     q_kf = k_re.copy() if cfg.aperture_tag is not None else None  # Rayleigh field at the real wavenumber
     return dict(name=name, desc=desc, mesh=mesh, cfg=cfg, buf=buf, freqs=freqs, k_re=k_re, k_im=k_im, q=q,
-                obs=field_points_3xn(obs), tags=sorted(cfg.velocity_sources), sym=sym, kf=q_kf)
+                obs=field_points_3xn(obs), tags=sorted(cfg.velocity_sources), sym=sym, kf=q_kf,
+                n_freq_total=len(freqs_all))
+
+
+def common_config(w, precision: str, world: int) -> dict:
+    """The job's configuration, identical in both arms of the benchmark."""
+    cfg, n = w["cfg"], int(w["buf"].p1_dof_count)
+    refine = (f"FP64-residual refinement, tolerance {cfg.refine_tolerance:g}, at most "
+              f"{max(1, cfg.refine_max_iterations) if precision == 'mixed' else cfg.refine_max_iterations} passes"
+              if (precision == "mixed" or cfg.refine_max_iterations > 0) else "none")
+    return {"workload": w["desc"], "n_dof": n, "n_triangles": int(w["buf"].n_triangles),
+            "n_freq": int(w["n_freq_total"]), "n_obs": int(w["obs"].shape[1]), "precision": precision,
+            "rcond_estimate": bool(cfg.dense_solve_rcond_warning_threshold > 0), "refine": refine,
+            "parallelism": f"frequencies dealt round-robin over {world} rank(s), one GPU each",
+            "l2": f"working set {2 * len(w['freqs']) * n * n * 4 / 1e6:.0f} MB of dense matrices per GPU > 126 MB L2"}
 
 
 # --------------------------------------------------------------------------- helpers
@@ -284,8 +303,8 @@ def run_reference(args, w):
         "impl": "reference", "metric": "freq-solves/s", "value": value, "unit": "freq-solves/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": warm, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64 (f32)",
-        "data": "synthetic", "config": {"workload": w["desc"], "n_dof": w["buf"].p1_dof_count,
-                                         "n_triangles": w["buf"].n_triangles, "parallelism": "host threads"},
+        "data": "synthetic", "config": common_config(w, args.precision, world),
+        "execution": "rank 0 alone, all host threads (OpenMP oracle + OpenBLAS cgesv)",
         "cpu_baseline": {"value": value, "unit": "freq-solves/s", "cores": vals[0]["cores"], "kind": "port",
                          "sample": "each step: 1 middle frequency of the workload (corrected assembly, cgesv, field, "
                                    "tag averages); the reference's own Swift/Metal/Accelerate path cannot run here"},
@@ -332,6 +351,9 @@ def run_b200(args, w):
                                 n * n, _t_ptr(rs.b_re), _t_ptr(rs.b_im), n, HBEM_ASM_DUFFY, _stream_ptr()),
               "hbem_assemble", lib)
 
+    # the job's result: every rank's fields, gathered to all ranks (NCCL) after each sweep
+    gathered = ([torch.empty_like(rs.f_re) for _ in range(world)], [torch.empty_like(rs.f_im) for _ in range(world)])
+
     def step(evs=None):
         if evs is None:
             assemble_split()
@@ -343,6 +365,9 @@ def run_b200(args, w):
         if evs is not None:
             evs[3].record(stream)
         rs.field()
+        if dist is not None:
+            dist.all_gather(gathered[0], rs.f_re)
+            dist.all_gather(gathered[1], rs.f_im)
         if evs is not None:
             evs[4].record(stream)
 
@@ -434,12 +459,7 @@ def run_b200(args, w):
         "metric": "freq-solves/s", "value": value, "unit": "freq-solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c64 (f32 planar)", "data": "synthetic",
-        "config": {"workload": w["desc"], "n_dof": buf.p1_dof_count, "n_triangles": T, "n_freq": F,
-                   "n_obs": n_obs, "precision": args.precision, "rcond_estimate": bool(want_rcond),
-                   "refine": (f"FP64-residual refinement, tolerance {rs.refine_tol:g}, at most {rs.refine_max} passes"
-                              if rs.refine else "none"),
-                   "parallelism": f"replicas x{world} (frequency-parallel)",
-                   "l2": f"working set {2 * F * n * n * 4 / 1e6:.0f} MB of dense matrices > 126 MB L2"},
+        "config": common_config(w, args.precision, world),
         "e2e": {"value": world * F * args.steps / (e2e_ms * 1e-3), "unit": "freq-solves/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
@@ -864,7 +884,8 @@ def main():
     if args.workload == "c3" and args.impl != "reference":
         run_b200_c3(args)
         return
-    w = workload(args.workload)
+    world, rank, _ = dist_env()
+    w = workload(args.workload, world, rank) if args.workload in ("c1", "c2") else workload(args.workload)
     if args.impl == "reference":
         run_reference(args, w)
     elif args.workload == "c4":

@@ -613,8 +613,15 @@ class BoundaryLabSession:
                      "velocity_sources": dict(basis[0]), "velocity_source_callback": None}
         solve_config, _ = solve_config_from_boundary_lab(cfg, **overrides)
 
+        # a new host thread starts on CUDA device 0: run the sweep on the caller's current device
+        device = _current_cuda_device()
+
         def work() -> None:
             try:
+                if device is not None:
+                    import torch
+
+                    torch.cuda.set_device(device)
                 _solve_multi_source(mesh_file, basis, solve_config, frequencies_hz=freqs)
             except BaseException as exc:   # re-raised in the consumer
                 results.put(exc)
@@ -671,3 +678,13 @@ class BoundaryLabBackend:
 
 def create_backend(**default_overrides: Any) -> BoundaryLabBackend:
     return BoundaryLabBackend(default_overrides=dict(default_overrides))
+
+
+def _current_cuda_device() -> int | None:
+    """The calling thread's current CUDA device, or None without torch / CUDA."""
+    try:
+        import torch
+
+        return int(torch.cuda.current_device()) if torch.cuda.is_available() else None
+    except Exception:
+        return None

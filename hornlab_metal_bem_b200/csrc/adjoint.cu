@@ -785,10 +785,9 @@ extern "C" int hbem_assemble_backward(hbem_session *h, int n_freq, const float *
             HBEM_LAUNCH_CHECK("k_sing_bits");
         }
     }
-    static bool attr = false;
-    if (!attr) {
-        HBEM_CUDA(cudaFuncSetAttribute(k_asm_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        attr = true;
+    {
+        const int rc = func_opt_in((const void *)k_asm_bwd, 200 * 1024);
+        if (rc != HBEM_OK) return rc;
     }
     for (int f0 = 0; f0 < n_freq; f0 += kBwdMaxF) {
         const int nf = std::min(kBwdMaxF, n_freq - f0);

@@ -225,8 +225,8 @@ __host__ __device__ constexpr uint32_t umma_idesc_bf16(int m, int n) {
 
 __device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 
-// Barrier of the four C-tile warps that also ORs a predicate across them, so
-// every warp takes the same branch afterwards.
+// Barrier of the eight C-tile warps (256 threads, named barrier 1) that also
+// ORs a predicate across them, so every warp takes the same branch afterwards.
 __device__ __forceinline__ bool epi_bar_or(bool pred) {
     uint32_t r;
     asm volatile(
@@ -773,12 +773,13 @@ int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int 
                                       w->B2);
         HBEM_LAUNCH_CHECK("k_pack_b");
     }
-    static int n_sm = 0;
-    if (!n_sm) {
+    int n_sm = 0;
+    {
         int dev = 0;
         HBEM_CUDA(cudaGetDevice(&dev));
         HBEM_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
-        HBEM_CUDA(cudaFuncSetAttribute(k_trailing_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+        const int rc = func_opt_in((const void *)k_trailing_tc, (int)kTcSmem);
+        if (rc != HBEM_OK) return rc;
     }
     const int ctas = n_sm - std::min(std::max(reserve_sms, 0), n_sm / 2);
     // work units of `chunk` consecutive column tiles: about ten units per CTA

@@ -18,6 +18,8 @@ int cuda_fail(cudaError_t e, const char *what);
 void count_launch(long long n = 1);
 int tuning(int key);   // HBEM_TUNE_* value, 0 = built-in choice
 void keep_pool_memory();   // cache freed stream-ordered allocations of the current device
+// raise a kernel's dynamic shared-memory limit once per device (thread-safe)
+int func_opt_in(const void *func, int smem_bytes, bool nonportable_cluster = false);
 
 #define HBEM_CUDA(call)                                        \
     do {                                                       \

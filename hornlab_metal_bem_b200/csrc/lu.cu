@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <cmath>
 #include <string>
@@ -1034,11 +1035,9 @@ template <bool LOWER, bool UNIT, int TR>
 int trsv_phase(int n, int nrhs, int batch, const float *lu_re, const float *lu_im, long long lda, long long a_stride,
                const int *piv, long long piv_stride, float *b_re, float *b_im, long long ldb, long long b_stride,
                cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        HBEM_CUDA(cudaFuncSetAttribute(k_trsv_first<LOWER, UNIT, TR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       200 * 1024));
-        attr = true;
+    {
+        const int rc = func_opt_in((const void *)k_trsv_first<LOWER, UNIT, TR>, 200 * 1024);
+        if (rc != HBEM_OK) return rc;
     }
     constexpr int RPC = TR == 0 ? kTrsvRows : kTrsvRowsT;
     const int nblk = (n + kTB - 1) / kTB;
@@ -1093,10 +1092,9 @@ int lu_solve_blocked(int n, int nrhs, int batch, const float *lu_re, const float
                                             b_im, ldb, b_stride, st);
     }
     if (rc == HBEM_OK && piv) {
-        static bool attr = false;
-        if (!attr) {
-            HBEM_CUDA(cudaFuncSetAttribute(k_trsv_unpermute, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-            attr = true;
+        {
+            const int rc = func_opt_in((const void *)k_trsv_unpermute, 200 * 1024);
+            if (rc != HBEM_OK) return rc;
         }
         k_trsv_unpermute<<<dim3(nrhs, batch), kTrsvThreads, (size_t)n * 2 * sizeof(float), st>>>(n, piv, piv_stride,
                                                                                                  b_re, b_im, ldb,
@@ -1126,6 +1124,7 @@ int lu_solve_blocked(int n, int nrhs, int batch, const float *lu_re, const float
 // ---------------------------------------------------------------------------
 constexpr int kWaveThreads = 256;
 constexpr int kWaveSpinLimit = 1 << 22;   // polls of >= 32 ns: seconds before a wait gives up
+// (HBEM_TUNE_WAVE_SPIN lowers it, so that a test can make a wait run out)
 constexpr unsigned long long kWaveEmpty = ~0ull;
 
 struct WaveCtl {
@@ -1164,7 +1163,7 @@ __device__ __forceinline__ float warp_sum(float v) {
 // Warp-wide wait until every lane's word (need: the lane reads one) is
 // posted; returns false on abort or timeout.
 __device__ __forceinline__ bool wave_wait(const unsigned long long *addr, bool need, unsigned long long &w,
-                                          WaveCtl *ctl) {
+                                          WaveCtl *ctl, int spin_limit) {
     w = need ? ld_relaxed_u64(addr) : 0ull;
     if (__all_sync(0xffffffffu, w != kWaveEmpty)) return true;
     unsigned ns = 32;
@@ -1174,7 +1173,7 @@ __device__ __forceinline__ bool wave_wait(const unsigned long long *addr, bool n
         if (w == kWaveEmpty) w = ld_relaxed_u64(addr);
         if (__all_sync(0xffffffffu, w != kWaveEmpty)) return true;
         if ((spins & 15) == 0 && __any_sync(0xffffffffu, *(volatile int *)&ctl->abort != 0)) return false;
-        if (spins > kWaveSpinLimit) {
+        if (spins > spin_limit) {
             if ((threadIdx.x & 31) == 0) {
                 atomicExch(&ctl->abort, 1);
                 atomicExch(&g_wave_fault, 1);
@@ -1191,7 +1190,7 @@ __global__ void __launch_bounds__(kWaveThreads) k_trsv_wave(int n, int nblk, int
                                                             long long a_stride, float *b_re, float *b_im,
                                                             long long ldb, long long b_stride, WaveCtl *ctl,
                                                             int phase, unsigned long long *mbox,
-                                                            const int *active) {
+                                                            const int *active, int spin_limit) {
     __shared__ float s_tr[32 * 33], s_ti[32 * 33];
     __shared__ float s_pr[8][33], s_pi[8][33];
     __shared__ int s_ticket, s_abort;
@@ -1258,7 +1257,7 @@ __global__ void __launch_bounds__(kWaveThreads) k_trsv_wave(int n, int nblk, int
         const int xi_idx = TR == 0 ? c0 + lane : c0 + warp + 8 * lane;
         const bool need = TR == 0 ? xi_idx < n : (lane < 4 && xi_idx < n);
         unsigned long long w;
-        if (!wave_wait(mb + (need ? xi_idx : 0), need, w, ctl)) {
+        if (!wave_wait(mb + (need ? xi_idx : 0), need, w, ctl, spin_limit)) {
             aborted = true;
             break;
         }
@@ -1363,8 +1362,10 @@ int launch_wave(int n, int nrhs, int batch, const float *lu_re, const float *lu_
                 int phase, unsigned long long *mbox, const int *active, cudaStream_t st) {
     const int nblk = (n + 31) / 32;
     const int systems = nrhs * batch;
+    const int spin = tuning(HBEM_TUNE_WAVE_SPIN) > 0 ? tuning(HBEM_TUNE_WAVE_SPIN) : kWaveSpinLimit;
     k_trsv_wave<LOWER, UNIT, TR><<<(unsigned)((long long)nblk * systems), kWaveThreads, 0, st>>>(
-        n, nblk, nrhs, systems, lu_re, lu_im, lda, a_stride, b_re, b_im, ldb, b_stride, ctl, phase, mbox, active);
+        n, nblk, nrhs, systems, lu_re, lu_im, lda, a_stride, b_re, b_im, ldb, b_stride, ctl, phase, mbox, active,
+        spin);
     HBEM_LAUNCH_CHECK("k_trsv_wave");
     return HBEM_OK;
 }
@@ -1377,11 +1378,10 @@ int lu_solve_wave(int n, int nrhs, int batch, const float *lu_re, const float *l
                   long long b_stride, int trans, const int *active, void *scratch, cudaStream_t st) {
     const long long systems = (long long)nrhs * batch;
     if ((long long)((n + 31) / 32) * systems >= (1LL << 31)) return fail(HBEM_ERR_ARG, "hbem_lu_solve: too many blocks");
-    static bool attr = false;
-    if (!attr) {
-        HBEM_CUDA(cudaFuncSetAttribute(k_trsv_permute<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        HBEM_CUDA(cudaFuncSetAttribute(k_trsv_permute<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        attr = true;
+    {
+        int rc = func_opt_in((const void *)k_trsv_permute<false>, 200 * 1024);
+        if (rc == HBEM_OK) rc = func_opt_in((const void *)k_trsv_permute<true>, 200 * 1024);
+        if (rc != HBEM_OK) return rc;
     }
     const size_t bytes = wave_scratch_bytes(systems, n);
     void *mem = scratch;
@@ -1688,11 +1688,9 @@ __global__ void k_axpy_active(int n, float *x_re, float *x_im, long long x_strid
 template <int CS>
 int launch_panel_cluster_t(float *a_re, float *a_im, long long lda, long long a_stride, int n, int c, int w, int *piv,
                            long long piv_stride, int *info, int batch, int R, size_t smem, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        HBEM_CUDA(cudaFuncSetAttribute(k_panel_cluster<CS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(200 * 1024)));
-        if (CS > 8) HBEM_CUDA(cudaFuncSetAttribute(k_panel_cluster<CS>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-        attr = true;
+    {
+        const int rc = func_opt_in((const void *)k_panel_cluster<CS>, 200 * 1024, CS > 8);
+        if (rc != HBEM_OK) return rc;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(CS, batch);
@@ -1715,12 +1713,14 @@ int launch_panel_cluster_t(float *a_re, float *a_im, long long lda, long long a_
 // Largest cluster the panel kernel uses: 16 CTAs (a non-portable size) where
 // the device co-schedules a 16-CTA cluster of full-size panel CTAs, else 8.
 int panel_cluster_max(size_t smem_cap) {
-    static int cached = 0;
-    if (cached) return cached;
+    // per device (the query and the attributes are per device); a data race
+    // on the cache only repeats the same query
+    static std::atomic<int> cached[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
+    if (const int c = cached[dev].load()) return c;
     int cmax = 8;
-    if (cudaFuncSetAttribute(k_panel_cluster<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(200 * 1024)) ==
-            cudaSuccess &&
-        cudaFuncSetAttribute(k_panel_cluster<16>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+    if (func_opt_in((const void *)k_panel_cluster<16>, 200 * 1024, true) == HBEM_OK) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(16, 1);
         cfg.blockDim = dim3(kPanelRowsThreads);
@@ -1737,8 +1737,8 @@ int panel_cluster_max(size_t smem_cap) {
             cmax = 16;
     }
     cudaGetLastError();   // a refused query leaves no sticky error
-    cached = cmax;
-    return cached;
+    cached[dev].store(cmax);
+    return cmax;
 }
 
 int launch_panel_cluster(float *a_re, float *a_im, long long lda, long long a_stride, int n, int c, int w, int *piv,
@@ -2025,12 +2025,11 @@ int lu_solve_single(int n, int nrhs, int batch, const float *lu_re, const float 
                     long long a_stride, const int *piv, long long piv_stride, float *b_re, float *b_im, long long ldb,
                     long long b_stride, int trans, cudaStream_t st) {
     const size_t smem = (size_t)n * 2 * sizeof(float);
-    static bool attr = false;
-    if (!attr) {
-        HBEM_CUDA(cudaFuncSetAttribute(k_getrs<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        HBEM_CUDA(cudaFuncSetAttribute(k_getrs<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        HBEM_CUDA(cudaFuncSetAttribute(k_getrs<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        attr = true;
+    {
+        int rc = func_opt_in((const void *)k_getrs<0>, 200 * 1024);
+        if (rc == HBEM_OK) rc = func_opt_in((const void *)k_getrs<1>, 200 * 1024);
+        if (rc == HBEM_OK) rc = func_opt_in((const void *)k_getrs<2>, 200 * 1024);
+        if (rc != HBEM_OK) return rc;
     }
     dim3 grid(nrhs, batch);
     const size_t tiles = (size_t)2 * (kGetrsThreads / 32) * 32 * 33 * sizeof(float);
@@ -2387,4 +2386,8 @@ extern "C" int hbem_lu_rcond(int n, int batch, const float *lu_re, const float *
     if (lda < n || a_stride < lda * (long long)n) return fail(HBEM_ERR_ARG, "hbem_lu_rcond: bad strides");
     if ((size_t)n * 2 * sizeof(float) > 200 * 1024) return fail(HBEM_ERR_ARG, "hbem_lu_rcond: n too large");
     return lu_rcond(n, batch, lu_re, lu_im, lda, a_stride, anorm, rcond, reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" int hbem_solve_status(void *stream) {
+    return wave_fault_check(reinterpret_cast<cudaStream_t>(stream));
 }

@@ -13,6 +13,8 @@
 #include <cstring>
 #include <mutex>
 #include <numeric>
+#include <set>
+#include <tuple>
 #include <unordered_map>
 
 #include "hbem_internal.h"
@@ -35,6 +37,23 @@ int cuda_fail(cudaError_t e, const char *what) {
 }
 
 void count_launch(long long n) { g_launches += n; }
+
+// Kernel attributes belong to a kernel on one device: raise the dynamic
+// shared-memory limit (and, when asked, allow non-portable cluster sizes) the
+// first time a kernel runs on each device, under a lock.
+int func_opt_in(const void *func, int smem_bytes, bool nonportable_cluster) {
+    static std::mutex mu;
+    static std::set<std::tuple<int, const void *, int, bool>> done;
+    int dev = 0;
+    HBEM_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    const auto key = std::make_tuple(dev, func, smem_bytes, nonportable_cluster);
+    if (done.count(key)) return HBEM_OK;
+    HBEM_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes));
+    if (nonportable_cluster) HBEM_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    done.insert(key);
+    return HBEM_OK;
+}
 
 // Stream-ordered allocations (workspaces of the LU, refinement, condition
 // estimate) come from the device's default memory pool; by default that pool
@@ -332,6 +351,9 @@ extern "C" int hbem_set_tuning(int key, int value) {
             break;
         case HBEM_TUNE_LU_RESERVE:
             if (value < 0 || value > 1024) return fail(HBEM_ERR_ARG, "HBEM_TUNE_LU_RESERVE: 0 .. 1024");
+            break;
+        case HBEM_TUNE_WAVE_SPIN:
+            if (value < 0 || value > (1 << 22)) return fail(HBEM_ERR_ARG, "HBEM_TUNE_WAVE_SPIN: 0 .. 4194304");
             break;
         default:
             return fail(HBEM_ERR_ARG, "hbem_set_tuning: unknown key " + std::to_string(key));

@@ -97,6 +97,7 @@ _SIGNATURES = {
                            _c_int, _vp], _c_int),
     "hbem_field_f64": ([_vp, _c_int, _vp, _vp, _vp, _c_ll, _vp, _vp, _c_ll, _vp, _c_int, _vp, _vp, _c_ll, _vp],
                        _c_int),
+    "hbem_solve_status": ([_vp], _c_int),
     "hbem_lu_factor_f64": ([_c_int, _c_int, _vp, _vp, _c_ll, _c_ll, _vp, _c_ll, _vp, _vp], _c_int),
     "hbem_lu_solve_f64": ([_c_int, _c_int, _c_int, _vp, _vp, _c_ll, _c_ll, _vp, _c_ll, _vp, _vp, _c_ll, _c_ll,
                            _c_int, _vp], _c_int),

@@ -111,6 +111,12 @@ long long hbem_launch_count(void);
  *   HBEM_TUNE_LU_RESERVE:    SMs the look-ahead's persistent tensor-core
  *                            update leaves to the factorisation chain
  *                            (v >= 1: v - 1 SMs, at most half; 0: built-in)
+ *   HBEM_TUNE_WAVE_SPIN:     polls (of >= 32 ns) a wavefront-solve warp waits
+ *                            for an earlier block before it gives up (0: the
+ *                            built-in 2^22); a wait that runs out makes the
+ *                            launch abort, writes NaN into the unfinished x
+ *                            and is reported by hbem_solve_status and the
+ *                            synchronising entry points as HBEM_ERR_STATE
  */
 #define HBEM_TUNE_ASM_MINBLOCKS 0
 #define HBEM_TUNE_LU_PANEL 1
@@ -119,7 +125,8 @@ long long hbem_launch_count(void);
 #define HBEM_TUNE_DUFFY 4
 #define HBEM_TUNE_LU_LOOKAHEAD 5
 #define HBEM_TUNE_LU_RESERVE 6
-#define HBEM_TUNE_COUNT 7
+#define HBEM_TUNE_WAVE_SPIN 7
+#define HBEM_TUNE_COUNT 8
 int hbem_set_tuning(int key, int value);
 int hbem_get_tuning(int key);
 
@@ -183,6 +190,16 @@ int hbem_lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, lo
 int hbem_lu_solve(int n, int nrhs, int batch, const float *lu_re, const float *lu_im, long long lda,
                   long long a_stride, const int *piv, long long piv_stride,
                   float *b_re, float *b_im, long long ldb, long long b_stride, int trans, void *stream);
+
+/*
+ * Synchronise `stream` and report the device-side status of the asynchronous
+ * solves issued before it: HBEM_ERR_STATE when a wavefront triangular-solve
+ * wait timed out since the last report (that solve's unfinished x is NaN),
+ * else HBEM_OK.  Clears the status.  hbem_refine, hbem_lu_rcond and
+ * hbem_solve_batch report it themselves.  No counterpart in the reference,
+ * whose LAPACK solves are synchronous.
+ */
+int hbem_solve_status(void *stream);
 
 /*
  * FP64-residual iterative refinement of X for A X = B (nrhs = 1 per matrix):

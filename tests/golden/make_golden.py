@@ -1,8 +1,8 @@
 """Generate the golden fixtures under tests/golden/ from the reference's own Python.
 
-Run in a container where the reference checkout is available:
+Run where a checkout of the reference is available, naming its root:
 
-    python tests/golden/make_golden.py --reference /root/reference
+    python tests/golden/make_golden.py --reference <path to the hornlab-metal-bem checkout>
 
 It imports ``hornlab_metal_bem`` (and the fixture helpers of the reference's
 ``tests/test_metal_native.py``) from that checkout, evaluates the front-end
@@ -77,7 +77,7 @@ def _buffers_dict(prefix, b):
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="root of the hornlab-metal-bem checkout")
     args = ap.parse_args()
     R = _load_reference(Path(args.reference))
     meshes = _meshes()

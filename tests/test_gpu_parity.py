@@ -24,8 +24,12 @@ from hornlab_metal_bem_b200 import generators as G  # noqa: E402
 from hornlab_metal_bem_b200.geometry import build_geometry_buffers  # noqa: E402
 from hornlab_metal_bem_b200.mesh import make_pure_function_spaces  # noqa: E402
 from hornlab_metal_bem_b200.native import (  # noqa: E402
-    HBEM_ASM_CORRECTED, HBEM_ASM_REGULAR, HBEM_ASM_ZERO, NativeSession, load_library,
+    HBEM_ASM_CORRECTED, HBEM_ASM_REGULAR, HBEM_ASM_ZERO, HBEM_TRANS_N, NativeSession, _t_ptr, last_error,
+    load_library,
 )
+
+HBEM_ERR_STATE = -4
+HBEM_TUNE_LU_SOLVE, HBEM_TUNE_WAVE_SPIN = 2, 7
 
 SYM = {"tiny": 0, "near": 0, "ico2": 0, "horn_quarter": 3, "yzxz_quarter": 3, "yzxz_full": 0, "yz_half": 1,
        "xy_half": 4, "ib_box": 0, "yz_full": 0}
@@ -512,3 +516,37 @@ def test_mixed_precision_lu_with_refinement(n):
         assert rel(x0[m], ref) < 1e-3          # unrefined BF16x3 factors
         assert resid[m] <= 1e-6
         assert rel(x[m], ref) < 1e-5           # refined
+
+
+def test_wavefront_wait_that_runs_out_reports_state_error_and_nan():
+    """A wavefront-solve wait bounded to one poll (HBEM_TUNE_WAVE_SPIN = 1) gives up before the earlier block's
+    x arrives: the launch aborts, the unfinished x is NaN, and hbem_solve_status reports HBEM_ERR_STATE once (the
+    report clears it).  With the built-in limit the same solve is exact again: the context stays usable."""
+    lib = load_library()
+    n = 2048
+    A, b = _lu_case(n, 1, 77)
+    Ar, Ai = _dev(A)
+    br, bi = _dev(b)
+    piv = torch.empty((1, n), dtype=torch.int32, device="cuda")
+    info = torch.empty(1, dtype=torch.int32, device="cuda")
+    assert lib.hbem_lu_factor(n, 1, _t_ptr(Ar), _t_ptr(Ai), n, n * n, _t_ptr(piv), n, _t_ptr(info), 0, None) == 0
+    try:
+        assert lib.hbem_set_tuning(HBEM_TUNE_LU_SOLVE, 3) == 0
+        assert lib.hbem_set_tuning(HBEM_TUNE_WAVE_SPIN, 1) == 0
+        xr, xi = br.clone(), bi.clone()
+        assert lib.hbem_lu_solve(n, 1, 1, _t_ptr(Ar), _t_ptr(Ai), n, n * n, _t_ptr(piv), n, _t_ptr(xr), _t_ptr(xi),
+                                 1, n, HBEM_TRANS_N, None) == 0
+        assert lib.hbem_solve_status(None) == HBEM_ERR_STATE
+        assert "timed out" in last_error(lib)
+        assert torch.isnan(xr).any()
+        assert lib.hbem_solve_status(None) == 0   # reported once
+    finally:
+        lib.hbem_set_tuning(HBEM_TUNE_WAVE_SPIN, 0)
+        lib.hbem_set_tuning(HBEM_TUNE_LU_SOLVE, 0)
+    xr, xi = br.clone(), bi.clone()
+    assert lib.hbem_lu_solve(n, 1, 1, _t_ptr(Ar), _t_ptr(Ai), n, n * n, _t_ptr(piv), n, _t_ptr(xr), _t_ptr(xi), 1, n,
+                             HBEM_TRANS_N, None) == 0
+    assert lib.hbem_solve_status(None) == 0
+    x = _host(xr, xi)[0]
+    ref = np.linalg.solve(A[0].astype(np.complex128), b[0].astype(np.complex128))
+    assert rel(x, ref) < 1e-4

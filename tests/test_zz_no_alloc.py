@@ -108,3 +108,60 @@ def test_noalloc_refine_rejects_sizes_beyond_its_scratch():
     assert "scratch limit" in last_error(lib)
     assert lib.hbem_refine_noalloc(*args(2, 2, 1 << 19)) == HBEM_ERR_ARG
     assert "scratch limit" in last_error(lib)
+
+
+_POOL_USED_CURRENT, _POOL_USED_HIGH = 7, 8   # cudaMemPoolAttrUsedMemCurrent / cudaMemPoolAttrUsedMemHigh
+
+
+def _pool():
+    """The device's default stream-ordered pool, queried through the CUDA runtime the library loaded."""
+    rt = ctypes.CDLL("libcudart.so.12")
+    pool = ctypes.c_void_p()
+    assert rt.cudaDeviceGetDefaultMemPool(ctypes.byref(pool), torch.cuda.current_device()) == 0
+    return rt, pool
+
+
+def _pool_attr(rt, pool, attr):
+    v = ctypes.c_uint64()
+    assert rt.cudaMemPoolGetAttribute(pool, attr, ctypes.byref(v)) == 0
+    return v.value
+
+
+def _pool_reset_high(rt, pool):
+    zero = ctypes.c_uint64(0)
+    assert rt.cudaMemPoolSetAttribute(pool, _POOL_USED_HIGH, ctypes.byref(zero)) == 0
+
+
+def test_noalloc_refine_takes_nothing_from_the_stream_ordered_pool():
+    """The point of the entry: no device allocation on any path it takes.  Around each call, the default pool's
+    high-water mark of memory in use is reset and must not rise above what was in use before, for every
+    triangular-solve variant (HBEM_TUNE_LU_SOLVE 0..3) of its correction solves.  hbem_refine, which takes its
+    scratch from that pool, raises the mark: the measurement sees allocations."""
+    lib = load_library()
+    n, batch = 300, 2
+    A, b = _case(n, batch, 43)
+    A0r, A0i, LUr, LUi, piv, Br, Bi, Xr, Xi = _factor_and_first_solve(lib, A, b, n, batch)
+    case = (A0r, A0i, LUr, LUi, piv, Br, Bi)
+    rt, pool = _pool()
+    ref = [np.linalg.solve(A[m].astype(np.complex128), b[m].astype(np.complex128)) for m in range(batch)]
+    try:
+        for mode in (0, 1, 2, 3):
+            assert lib.hbem_set_tuning(2, mode) == 0
+            X2r, X2i = Xr.clone(), Xi.clone()
+            torch.cuda.synchronize()
+            before = _pool_attr(rt, pool, _POOL_USED_CURRENT)
+            _pool_reset_high(rt, pool)
+            _refine(lib, "hbem_refine_noalloc", n, batch, case, X2r, X2i)
+            assert _pool_attr(rt, pool, _POOL_USED_HIGH) <= before, mode
+            x = _host(X2r, X2i)
+            for m in range(batch):
+                assert _rel(x[m], ref[m]) < 1e-5
+        # control: the allocating twin shows up in the same measurement
+        X3r, X3i = Xr.clone(), Xi.clone()
+        torch.cuda.synchronize()
+        before = _pool_attr(rt, pool, _POOL_USED_CURRENT)
+        _pool_reset_high(rt, pool)
+        _refine(lib, "hbem_refine", n, batch, case, X3r, X3i)
+        assert _pool_attr(rt, pool, _POOL_USED_HIGH) > before
+    finally:
+        lib.hbem_set_tuning(2, 0)
