@@ -285,6 +285,37 @@ def accuracy_vs_fp64(sess, w, rs) -> dict:
             "cases": out}
 
 
+def multi_source_cost(sess, w, e2e_kw, stream, dist, n_src: int = 4, reps: int = 3) -> dict:
+    """End-to-end cost of a sweep with ``n_src`` velocity sources sharing each frequency's assembly pass and
+    LU (``extra_neumann_dp0``, the reference's multi-RHS batch) against the same sweep with one source.  The
+    extra sources drive the same faces with seeded per-face phases."""
+    import torch
+
+    rng = np.random.default_rng(7)
+    q = w["q"]
+    extra = np.stack([q * np.exp(1j * rng.uniform(0.0, 2.0 * np.pi, size=q.shape[1]))[None, :]
+                      for _ in range(n_src - 1)]).astype(np.complex64)
+    tags = [min(w["tags"])] * (n_src - 1)
+
+    def timed(kw):
+        sess.assemble_solve_evaluate_standard_neumann_batch(w["freqs"], w["k_re"], q, w["obs"], **kw)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            sess.assemble_solve_evaluate_standard_neumann_batch(w["freqs"], w["k_re"], q, w["obs"], **kw)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    one = timed(e2e_kw)
+    many = timed({**e2e_kw, "extra_neumann_dp0": extra, "extra_impedance_source_tags": tags})
+    return {"sources": n_src, "ms_per_sweep_one_source": one, "ms_per_sweep_all_sources": many,
+            "cost_ratio": many / one,
+            "how": "hbem_solve_batch_multi through the session call with host buffers: one assembly pass and one "
+                   "LU per frequency, one solve and refinement per source"}
+
+
 # --------------------------------------------------------------------------- arms
 def run_reference(args, w):
     world, rank, _ = dist_env()
@@ -434,6 +465,7 @@ def run_b200(args, w):
     d2h = F * n_obs * 8 + F * ntag * 16 + F * 4 + F * 12
 
     accuracy = accuracy_vs_fp64(sess, w, rs)
+    multi_source = multi_source_cost(sess, w, e2e_kw, stream, dist) if world == 1 else None
 
     # ---- roofline of the dominant kernel
     peaks = measured_peaks()
@@ -464,6 +496,7 @@ def run_b200(args, w):
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
         "accuracy": accuracy,
+        "multi_source": multi_source,
         "stages_ms_per_step": stage,
         "clocks": clk,
         "roofline": roofline,

@@ -33,6 +33,7 @@ namespace {
 
 constexpr int kMaxFreqPerLaunch = 64;
 constexpr int kAsmFreqs = 2;  // wavenumbers per geometric sample in the pair kernel
+constexpr int kMaxSources = 8;   // right-hand sides (velocity sources) one assembly pass fills
 
 struct AsmArgs {
     const float4 *qp;
@@ -53,7 +54,8 @@ struct AsmArgs {
     float *b_re;
     float *b_im;
     long long q_stride, lda, a_stride, b_stride;
-    int T, nf;
+    long long q_src_stride, b_src_stride;   // between sources' Neumann rows / right-hand sides
+    int T, nf, n_src;
     float rw;
     float k[kMaxFreqPerLaunch];
     float kt[kMaxFreqPerLaunch];  // k / (2 pi): phase in turns per metre
@@ -543,7 +545,9 @@ __global__ void __launch_bounds__(kAsmThreads, MINB) k_regular_sym(const __grid_
     __shared__ float4 s_tq[kTestTile * 6];
     __shared__ float4 s_nrm[kTrialTile];
     __shared__ uchar4 s_cs[kTrialTile];
-    __shared__ float4 s_qb[kTrialTile];
+    __shared__ float2 s_q[kMaxSources][kTrialTile];    // Neumann data of the trial triangles per source
+    __shared__ float2 s_tqq[kMaxSources][kTestTile];   // ... and of the test triangles
+    __shared__ float2 s_beta[kTrialTile];
     __shared__ int s_flag[kTrialTile];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -558,11 +562,12 @@ __global__ void __launch_bounds__(kAsmThreads, MINB) k_regular_sym(const __grid_
     const int r0 = p.row_off[test_tile], nrows = p.row_off[test_tile + 1] - r0;
     const int c0 = p.col_off[trial_tile], ncols = p.col_off[trial_tile + 1] - c0;
     const int ldc = ncols | 1, ldr = nrows | 1;
+    const int nsrc = p.n_src;
     float2 *acc = s_acc;                       // nrows x ldc   (test rows, trial columns)
-    float2 *rhs = acc + nrows * ldc;           // nrows
-    float2 *acc2 = rhs + nrows;                // ncols x ldr   (trial rows, test columns)
-    float2 *rhs2 = acc2 + ncols * ldr;         // ncols
-    const int plane = nrows * ldc + nrows + ncols * ldr + ncols;
+    float2 *rhs = acc + nrows * ldc;           // nsrc x nrows
+    float2 *acc2 = rhs + nsrc * nrows;         // ncols x ldr   (trial rows, test columns)
+    float2 *rhs2 = acc2 + ncols * ldr;         // nsrc x ncols
+    const int plane = nrows * ldc + nsrc * nrows + ncols * ldr + nsrc * ncols;
 
     for (int i = tid; i < plane; i += kAsmThreads) s_acc[i] = make_float2(0.f, 0.f);
     for (int i = tid; i < ntrial * 6; i += kAsmThreads) s_qp[i] = p.qp[(size_t)tbase * 6 + i];
@@ -574,17 +579,28 @@ __global__ void __launch_bounds__(kAsmThreads, MINB) k_regular_sym(const __grid_
         s_nrm[i] = p.nrm[tbase + i];
         s_cs[i] = p.trial_slot[tbase + i];
         const int orig = p.tri[tbase + i].w;
-        float4 qb = make_float4(0.f, 0.f, 0.f, 0.f);
+        int flag = 0;
+        for (int sv = 0; sv < nsrc; ++sv) {
+            float2 qv = make_float2(0.f, 0.f);
+            if (p.q_re) {
+                const size_t o = (size_t)sv * p.q_src_stride + (size_t)f * p.q_stride + orig;
+                qv = make_float2(p.q_re[o], p.q_im[o]);
+            }
+            s_q[sv][i] = qv;
+            flag |= (qv.x != 0.f || qv.y != 0.f) ? 1 : 0;
+        }
+        const float2 be = p.beta_re ? make_float2(p.beta_re[orig], p.beta_im[orig]) : make_float2(0.f, 0.f);
+        s_beta[i] = be;
+        s_flag[i] = flag | ((be.x != 0.f || be.y != 0.f) ? 1 : 0);
+    }
+    for (int i = tid; i < nsrc * ntest; i += kAsmThreads) {
+        const int sv = i / ntest, t = i - sv * ntest;
+        float2 qv = make_float2(0.f, 0.f);
         if (p.q_re) {
-            qb.x = p.q_re[(size_t)f * p.q_stride + orig];
-            qb.y = p.q_im[(size_t)f * p.q_stride + orig];
+            const size_t o = (size_t)sv * p.q_src_stride + (size_t)f * p.q_stride + p.tri[test0 + t].w;
+            qv = make_float2(p.q_re[o], p.q_im[o]);
         }
-        if (p.beta_re) {
-            qb.z = p.beta_re[orig];
-            qb.w = p.beta_im[orig];
-        }
-        s_qb[i] = qb;
-        s_flag[i] = (qb.x != 0.f || qb.y != 0.f || qb.z != 0.f || qb.w != 0.f) ? 1 : 0;
+        s_tqq[sv][t] = qv;
     }
     __syncthreads();
 
@@ -596,16 +612,9 @@ __global__ void __launch_bounds__(kAsmThreads, MINB) k_regular_sym(const __grid_
         const uchar4 rs = p.test_slot[test];
         const int rslot[3] = {rs.x, rs.y, rs.z};
         const int torig = p.tri[test].w;
-        float4 tqb = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (p.q_re) {
-            tqb.x = p.q_re[(size_t)f * p.q_stride + torig];
-            tqb.y = p.q_im[(size_t)f * p.q_stride + torig];
-        }
-        if (p.beta_re) {
-            tqb.z = p.beta_re[torig];
-            tqb.w = p.beta_im[torig];
-        }
-        const bool tflag = tqb.x != 0.f || tqb.y != 0.f || tqb.z != 0.f || tqb.w != 0.f;
+        const float2 tbe = p.beta_re ? make_float2(p.beta_re[torig], p.beta_im[torig]) : make_float2(0.f, 0.f);
+        bool tflag = tbe.x != 0.f || tbe.y != 0.f;
+        for (int sv = 0; sv < nsrc; ++sv) tflag |= s_tqq[sv][lane].x != 0.f || s_tqq[sv][lane].y != 0.f;
         const float4 *tq = &s_tq[lane];
         // i k beta / 3 terms: Robin rows of the trial (forward) and test (transposed) triangles
         auto robin = [&](float br, float bi, float &rr, float &ri) {
@@ -619,7 +628,7 @@ __global__ void __launch_bounds__(kAsmThreads, MINB) k_regular_sym(const __grid_
             }
         };
         float rob2_re, rob2_im;
-        robin(tqb.z, tqb.w, rob2_re, rob2_im);
+        robin(tbe.x, tbe.y, rob2_re, rob2_im);
         for (int jj = warp; jj < ntrial; jj += kAsmThreads / 32) {
             const int sigma = tbase + jj;
             if (sigma < test) continue;
@@ -635,9 +644,9 @@ __global__ void __launch_bounds__(kAsmThreads, MINB) k_regular_sym(const __grid_
             const float scale = HBEM_INV4PI * tjac * nj.w;
             const uchar4 cs = s_cs[jj];
             const int cslot[3] = {cs.x, cs.y, cs.z};
-            const float4 qb = s_qb[jj];
+            const float2 be = s_beta[jj];
             float rob_re, rob_im;
-            robin(qb.z, qb.w, rob_re, rob_im);
+            robin(be.x, be.y, rob_re, rob_im);
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
                 const float s_re = sfr[i] * scale, s_im = sfi[i] * scale;
@@ -652,9 +661,13 @@ __global__ void __launch_bounds__(kAsmThreads, MINB) k_regular_sym(const __grid_
                     atomicAdd(&dst->x, vre * p.rw);
                     atomicAdd(&dst->y, vim * p.rw);
                 }
-                if (qb.x != 0.f || qb.y != 0.f) {
-                    atomicAdd(&rhs[rslot[i]].x, (s_re * qb.x - s_im * qb.y) * p.rw);
-                    atomicAdd(&rhs[rslot[i]].y, (s_re * qb.y + s_im * qb.x) * p.rw);
+#pragma unroll 1
+                for (int sv = 0; sv < nsrc; ++sv) {
+                    const float2 qv = s_q[sv][jj];
+                    if (qv.x != 0.f || qv.y != 0.f) {
+                        atomicAdd(&rhs[sv * nrows + rslot[i]].x, (s_re * qv.x - s_im * qv.y) * p.rw);
+                        atomicAdd(&rhs[sv * nrows + rslot[i]].y, (s_re * qv.y + s_im * qv.x) * p.rw);
+                    }
                 }
             }
             if (self) continue;
@@ -671,9 +684,13 @@ __global__ void __launch_bounds__(kAsmThreads, MINB) k_regular_sym(const __grid_
                     atomicAdd(&dst->x, vre * p.rw);
                     atomicAdd(&dst->y, vim * p.rw);
                 }
-                if (tqb.x != 0.f || tqb.y != 0.f) {
-                    atomicAdd(&rhs2[cslot[j]].x, (s_re * tqb.x - s_im * tqb.y) * p.rw);
-                    atomicAdd(&rhs2[cslot[j]].y, (s_re * tqb.y + s_im * tqb.x) * p.rw);
+#pragma unroll 1
+                for (int sv = 0; sv < nsrc; ++sv) {
+                    const float2 qv = s_tqq[sv][lane];
+                    if (qv.x != 0.f || qv.y != 0.f) {
+                        atomicAdd(&rhs2[sv * ncols + cslot[j]].x, (s_re * qv.x - s_im * qv.y) * p.rw);
+                        atomicAdd(&rhs2[sv * ncols + cslot[j]].y, (s_re * qv.y + s_im * qv.x) * p.rw);
+                    }
                 }
             }
         }
@@ -701,18 +718,20 @@ __global__ void __launch_bounds__(kAsmThreads, MINB) k_regular_sym(const __grid_
         }
     }
     if (p.q_re) {
-        for (int r = tid; r < nrows; r += kAsmThreads) {
-            const float2 v = rhs[r];
+        for (int e = tid; e < nsrc * nrows; e += kAsmThreads) {
+            const int sv = e / nrows, r = e - sv * nrows;
+            const float2 v = rhs[e];
             if (v.x != 0.f || v.y != 0.f) {
-                const size_t off = (size_t)f * p.b_stride + p.rows[r0 + r];
+                const size_t off = (size_t)sv * p.b_src_stride + (size_t)f * p.b_stride + p.rows[r0 + r];
                 atomicAdd(p.b_re + off, v.x);
                 atomicAdd(p.b_im + off, v.y);
             }
         }
-        for (int c = tid; c < ncols; c += kAsmThreads) {
-            const float2 v = rhs2[c];
+        for (int e = tid; e < nsrc * ncols; e += kAsmThreads) {
+            const int sv = e / ncols, c = e - sv * ncols;
+            const float2 v = rhs2[e];
             if (v.x != 0.f || v.y != 0.f) {
-                const size_t off = (size_t)f * p.b_stride + p.cols[c0 + c];
+                const size_t off = (size_t)sv * p.b_src_stride + (size_t)f * p.b_stride + p.cols[c0 + c];
                 atomicAdd(p.b_re + off, v.x);
                 atomicAdd(p.b_im + off, v.y);
             }
@@ -800,7 +819,8 @@ struct DuffyArgs {
     const float *q_re, *q_im, *beta_re, *beta_im;
     float *a_re, *a_im, *b_re, *b_im;
     long long q_stride, lda, a_stride, b_stride;
-    int V, T, n_pairs;
+    long long q_src_stride, b_src_stride;
+    int V, T, n_pairs, n_src;
     int rule_off[3], rule_cnt[3];
     // coupled-baffle projections: ap_local[t] = aperture index or -1.
     // mode 0: A/b (when a_re) and S_ia (when sia); mode 1: S_aa only.
@@ -1108,11 +1128,15 @@ __global__ void __launch_bounds__(256, MINB) k_duffy(const __grid_constant__ Duf
             atomicAdd(p.a_re + o, (float)dr);
             atomicAdd(p.a_im + o, (float)di);
         } else if (lane < 12 && p.q_re) {
-            const float qr = p.q_re[(size_t)(fg + f) * p.q_stride + pr.trial], qi = p.q_im[(size_t)(fg + f) * p.q_stride + pr.trial];
-            if (qr != 0.f || qi != 0.f) {
-                const size_t o = (size_t)(fg + f) * p.b_stride + p.l2g[pr.test * 3 + i_row];
-                atomicAdd(p.b_re + o, (float)(sr * qr - si * qi));
-                atomicAdd(p.b_im + o, (float)(sr * qi + si * qr));
+            for (int sv = 0; sv < p.n_src; ++sv) {
+                const size_t oq = (size_t)sv * p.q_src_stride + (size_t)(fg + f) * p.q_stride + pr.trial;
+                const float qr = p.q_re[oq], qi = p.q_im[oq];
+                if (qr != 0.f || qi != 0.f) {
+                    const size_t o = (size_t)sv * p.b_src_stride + (size_t)(fg + f) * p.b_stride +
+                                     p.l2g[pr.test * 3 + i_row];
+                    atomicAdd(p.b_re + o, (float)(sr * qr - si * qi));
+                    atomicAdd(p.b_im + o, (float)(sr * qi + si * qr));
+                }
             }
         }
     }
@@ -1131,10 +1155,11 @@ void fill_k(float *k, float *kt, float *ki, const float *k_re, const float *k_im
 int launch_regular(Session &s, int n_freq, const float *k_re, const float *k_im, const float *q_re,
                    const float *q_im, long long q_stride, const float *beta_re, const float *beta_im, float *a_re,
                    float *a_im, long long lda, long long a_stride, float *b_re, float *b_im, long long b_stride,
-                   cudaStream_t st) {
+                   cudaStream_t st, int n_src, long long q_src_stride, long long b_src_stride) {
+    if (n_src < 1 || n_src > kMaxSources) return fail(HBEM_ERR_ARG, "assembly: 1 .. 8 sources per pass");
     const size_t smem = (size_t)kAsmFreqs * (s.max_rows * (s.max_cols | 1) + s.max_rows) * sizeof(float2);
-    const size_t smem_sym = (size_t)(s.max_rows * (s.max_cols | 1) + s.max_rows + s.max_cols * (s.max_rows | 1) +
-                                     s.max_cols) * sizeof(float2);
+    const size_t smem_sym = (size_t)(s.max_rows * (s.max_cols | 1) + n_src * s.max_rows +
+                                     s.max_cols * (s.max_rows | 1) + n_src * s.max_cols) * sizeof(float2);
     static bool consts_ready[64] = {false};
     if (s.device >= 0 && s.device < 64 && !consts_ready[s.device]) {
         const double QX[6] = {0.4459484909159651, 0.0915762135097710, 0.1081030181680700,
@@ -1168,6 +1193,7 @@ int launch_regular(Session &s, int n_freq, const float *k_re, const float *k_im,
         a.b_re = b_re ? b_re + (size_t)f0 * b_stride : nullptr;
         a.b_im = b_im ? b_im + (size_t)f0 * b_stride : nullptr;
         a.q_stride = q_stride; a.lda = lda; a.a_stride = a_stride; a.b_stride = b_stride;
+        a.q_src_stride = q_src_stride; a.b_src_stride = b_src_stride; a.n_src = n_src;
         a.T = s.n_triangles;
         a.rw = (float)(1 << ((s.sym & 1) + ((s.sym >> 1) & 1) + ((s.sym >> 2) & 1)));
         bool ck = false;
@@ -1176,7 +1202,7 @@ int launch_regular(Session &s, int n_freq, const float *k_re, const float *k_im,
         if (!a.b_re) a.q_re = a.q_im = nullptr;
         a.nf = nf;
         cudaError_t e;
-        if (tuning(HBEM_TUNE_ASM_PAIRS) != 1) {
+        if (tuning(HBEM_TUNE_ASM_PAIRS) != 1 || n_src > 1) {
             // unordered pairs, one wavenumber per grid slice
             dim3 grid(s.n_trial_tiles, s.n_test_tiles, nf);
             e = ck ? dispatch_sym_pairs<true>(s.sym, a, grid, smem_sym, st)
@@ -1195,7 +1221,7 @@ int launch_regular(Session &s, int n_freq, const float *k_re, const float *k_im,
 int launch_duffy(Session &s, int n_freq, const float *k_re, const float *k_im, const float *q_re, const float *q_im,
                  long long q_stride, const float *beta_re, const float *beta_im, float *a_re, float *a_im,
                  long long lda, long long a_stride, float *b_re, float *b_im, long long b_stride, cudaStream_t st,
-                 const ApertureOut *ap) {
+                 const ApertureOut *ap, int n_src, long long q_src_stride, long long b_src_stride) {
     if (s.n_pairs == 0) return HBEM_OK;
     for (int f0 = 0; f0 < n_freq; f0 += kMaxFreqPerLaunch) {
         const int nf = std::min(kMaxFreqPerLaunch, n_freq - f0);
@@ -1209,6 +1235,7 @@ int launch_duffy(Session &s, int n_freq, const float *k_re, const float *k_im, c
         a.b_re = b_re ? b_re + (size_t)f0 * b_stride : nullptr;
         a.b_im = b_im ? b_im + (size_t)f0 * b_stride : nullptr;
         a.q_stride = q_stride; a.lda = lda; a.a_stride = a_stride; a.b_stride = b_stride;
+        a.q_src_stride = q_src_stride; a.b_src_stride = b_src_stride; a.n_src = n_src;
         a.V = s.n_vertices; a.T = s.n_triangles; a.n_pairs = s.n_pairs;
         for (int r = 0; r < 3; ++r) { a.rule_off[r] = s.rule_off[r]; a.rule_cnt[r] = s.rule_cnt[r]; }
         fill_k(a.k, a.kt, a.ki, k_re + f0, k_im ? k_im + f0 : nullptr, nf);
@@ -1250,19 +1277,23 @@ int launch_duffy(Session &s, int n_freq, const float *k_re, const float *k_im, c
 
 using namespace hbem;
 
-extern "C" int hbem_assemble(hbem_session *h, int n_freq, const float *k_re, const float *k_im, const float *q_re,
-                             const float *q_im, long long q_stride, const float *beta_re, const float *beta_im,
-                             float *a_re, float *a_im, long long lda, long long a_stride, float *b_re, float *b_im,
-                             long long b_stride, int flags, void *stream) {
+extern "C" int hbem_assemble_multi(hbem_session *h, int n_freq, const float *k_re, const float *k_im, int n_src,
+                                   const float *q_re, const float *q_im, long long q_stride, long long q_src_stride,
+                                   const float *beta_re, const float *beta_im, float *a_re, float *a_im,
+                                   long long lda, long long a_stride, float *b_re, float *b_im, long long b_stride,
+                                   long long b_src_stride, int flags, void *stream) {
     Session *s = reinterpret_cast<Session *>(h);
     if (!s) return fail(HBEM_ERR_ARG, "hbem_assemble: NULL session");
     if (n_freq <= 0) return HBEM_OK;
     if (!k_re || !a_re || !a_im) return fail(HBEM_ERR_ARG, "hbem_assemble: NULL k or A pointer");
+    if (n_src < 1 || n_src > kMaxSources) return fail(HBEM_ERR_ARG, "hbem_assemble_multi: n_src must be 1 .. 8");
     if (lda < s->n_dof || a_stride < lda * s->n_dof) return fail(HBEM_ERR_ARG, "hbem_assemble: lda/a_stride too small");
     if ((q_re == nullptr) != (q_im == nullptr) || (b_re == nullptr) != (b_im == nullptr))
         return fail(HBEM_ERR_ARG, "hbem_assemble: real/imag pointers must be given together");
     if (q_re && q_stride < s->n_triangles) return fail(HBEM_ERR_ARG, "hbem_assemble: q_stride < n_triangles");
     if (b_re && b_stride < s->n_dof) return fail(HBEM_ERR_ARG, "hbem_assemble: b_stride < n_dof");
+    if (n_src > 1 && ((q_re && q_src_stride < q_stride * n_freq) || (b_re && b_src_stride < b_stride * n_freq)))
+        return fail(HBEM_ERR_ARG, "hbem_assemble_multi: q_src_stride / b_src_stride overlap the frequencies");
     if ((beta_re == nullptr) != (beta_im == nullptr)) return fail(HBEM_ERR_ARG, "hbem_assemble: beta pointers");
     for (int f = 0; f < n_freq; ++f)
         if (!std::isfinite(k_re[f]) || (k_im && !std::isfinite(k_im[f])))
@@ -1280,16 +1311,27 @@ extern "C" int hbem_assemble(hbem_session *h, int n_freq, const float *k_re, con
             }
         }
         if (b_re) {
-            HBEM_CUDA(cudaMemset2DAsync(b_re, b_stride * sizeof(float), 0, s->n_dof * sizeof(float), n_freq, st));
-            HBEM_CUDA(cudaMemset2DAsync(b_im, b_stride * sizeof(float), 0, s->n_dof * sizeof(float), n_freq, st));
+            for (int sv = 0; sv < n_src; ++sv) {
+                float *br = b_re + (size_t)sv * b_src_stride, *bi = b_im + (size_t)sv * b_src_stride;
+                HBEM_CUDA(cudaMemset2DAsync(br, b_stride * sizeof(float), 0, s->n_dof * sizeof(float), n_freq, st));
+                HBEM_CUDA(cudaMemset2DAsync(bi, b_stride * sizeof(float), 0, s->n_dof * sizeof(float), n_freq, st));
+            }
         }
     }
     int rc = HBEM_OK;
     if (flags & HBEM_ASM_REGULAR)
         rc = launch_regular(*s, n_freq, k_re, k_im, q_re, q_im, q_stride, beta_re, beta_im, a_re, a_im, lda, a_stride,
-                            b_re, b_im, b_stride, st);
+                            b_re, b_im, b_stride, st, n_src, q_src_stride, b_src_stride);
     if (rc == HBEM_OK && (flags & HBEM_ASM_DUFFY))
         rc = launch_duffy(*s, n_freq, k_re, k_im, q_re, q_im, q_stride, beta_re, beta_im, a_re, a_im, lda, a_stride,
-                          b_re, b_im, b_stride, st, nullptr);
+                          b_re, b_im, b_stride, st, nullptr, n_src, q_src_stride, b_src_stride);
     return rc;
+}
+
+extern "C" int hbem_assemble(hbem_session *h, int n_freq, const float *k_re, const float *k_im, const float *q_re,
+                             const float *q_im, long long q_stride, const float *beta_re, const float *beta_im,
+                             float *a_re, float *a_im, long long lda, long long a_stride, float *b_re, float *b_im,
+                             long long b_stride, int flags, void *stream) {
+    return hbem_assemble_multi(h, n_freq, k_re, k_im, 1, q_re, q_im, q_stride, 0, beta_re, beta_im, a_re, a_im, lda,
+                               a_stride, b_re, b_im, b_stride, 0, flags, stream);
 }

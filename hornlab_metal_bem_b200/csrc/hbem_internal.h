@@ -132,7 +132,8 @@ int launch_regular(Session &s, int n_freq, const float *k_re, const float *k_im,
                    const float *q_re, const float *q_im, long long q_stride,
                    const float *beta_re, const float *beta_im,
                    float *a_re, float *a_im, long long lda, long long a_stride,
-                   float *b_re, float *b_im, long long b_stride, cudaStream_t st);
+                   float *b_re, float *b_im, long long b_stride, cudaStream_t st,
+                   int n_src = 1, long long q_src_stride = 0, long long b_src_stride = 0);
 struct ApertureOut {
     int mode;                        // 0: S_ia (with or without A/b), 1: S_aa
     float *sia_re, *sia_im, *saa_re, *saa_im;
@@ -143,7 +144,7 @@ int launch_duffy(Session &s, int n_freq, const float *k_re, const float *k_im,
                  const float *beta_re, const float *beta_im,
                  float *a_re, float *a_im, long long lda, long long a_stride,
                  float *b_re, float *b_im, long long b_stride, cudaStream_t st,
-                 const ApertureOut *ap);
+                 const ApertureOut *ap, int n_src = 1, long long q_src_stride = 0, long long b_src_stride = 0);
 
 }  // namespace hbem
 

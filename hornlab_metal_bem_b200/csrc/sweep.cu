@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "hbem_internal.h"
 
@@ -52,26 +53,26 @@ struct Layout {
     size_t q, a, a0, a64, x64, x, b, piv, info, obs, fld, tag, want, iters, resid, anorm, rcond, total;
 };
 
-Layout layout(const Session &s, int nf, int n_obs, int n_tags, bool keep_a, bool fp64) {
-    const size_t n = s.n_dof, T = s.n_triangles;
+Layout layout(const Session &s, int nf, int n_src, int n_obs, int n_tags, bool keep_a, bool fp64) {
+    const size_t n = s.n_dof, T = s.n_triangles, ns = (size_t)n_src;
     Layout L{};
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t o = off; off += align_up(bytes); return o; };
-    L.q = take(2 * sizeof(float) * nf * T);
+    L.q = take(2 * sizeof(float) * ns * nf * T);
     L.a = take(2 * sizeof(float) * nf * n * n);
     L.a0 = keep_a ? take(2 * sizeof(float) * nf * n * n) : 0;
     L.a64 = fp64 ? take(2 * sizeof(double) * nf * n * n) : 0;
-    L.x64 = fp64 ? take(2 * sizeof(double) * nf * n) : 0;
-    L.x = take(2 * sizeof(float) * nf * n);
-    L.b = take(2 * sizeof(float) * nf * n);
+    L.x64 = fp64 ? take(2 * sizeof(double) * ns * nf * n) : 0;
+    L.x = take(2 * sizeof(float) * ns * nf * n);
+    L.b = take(2 * sizeof(float) * ns * nf * n);
     L.piv = take(sizeof(int) * nf * n);
     L.info = take(sizeof(int) * nf);
     L.obs = take(3 * sizeof(float) * std::max(1, n_obs));
-    L.fld = take(2 * sizeof(float) * nf * std::max(1, n_obs));
-    L.tag = take(2 * sizeof(double) * nf * std::max(1, n_tags));
+    L.fld = take(2 * sizeof(float) * ns * nf * std::max(1, n_obs));
+    L.tag = take(2 * sizeof(double) * ns * nf * std::max(1, n_tags));
     L.want = take(sizeof(int) * std::max(1, n_tags));
-    L.iters = take(sizeof(int) * nf);
-    L.resid = take(sizeof(double) * nf);
+    L.iters = take(sizeof(int) * ns * nf);
+    L.resid = take(sizeof(double) * ns * nf);
     L.anorm = take(sizeof(float) * nf);
     L.rcond = take(sizeof(double) * nf);
     L.total = off;
@@ -93,15 +94,22 @@ int ensure_ws(Session &s, size_t bytes) {
 
 using namespace hbem;
 
-extern "C" int hbem_solve_batch(hbem_session *h, int n_freq, const float *k_re, const float *k_im, const float *q_re,
-                                const float *q_im, const float *obs_3xn, int n_obs, const int *tags, int n_tags,
-                                int precision, double refine_tol, int refine_max_iter, float *field_re,
-                                float *field_im, double *tag_avg, float *surface_re, float *surface_im, int *info,
-                                int *refine_iters, double *refine_resid, double *rcond, float *timings_ms,
-                                void *stream) {
+// The sweep for n_src right-hand sides (velocity sources) sharing each
+// frequency's matrix: one assembly pass fills A and every source's b, one LU,
+// then one solve (and refinement) per source, field and tag averages for all
+// (source, frequency) cases in one launch each.  Host arrays per source are
+// source-major: q (n_src, n_freq, T), field (n_src, n_freq, n_obs), tag_avg
+// (n_src, n_freq, n_tags, 2), surface (n_src, n_freq, n), refine_iters /
+// refine_resid (n_src, n_freq); info and rcond are per frequency.
+static int solve_batch_impl(hbem_session *h, int n_freq, int n_src, const float *k_re, const float *k_im,
+                            const float *q_re, const float *q_im, const float *obs_3xn, int n_obs, const int *tags,
+                            int n_tags, int precision, double refine_tol, int refine_max_iter, float *field_re,
+                            float *field_im, double *tag_avg, float *surface_re, float *surface_im, int *info,
+                            int *refine_iters, double *refine_resid, double *rcond, float *timings_ms, void *stream) {
     Session *s = reinterpret_cast<Session *>(h);
     if (!s) return fail(HBEM_ERR_ARG, "hbem_solve_batch: NULL session");
     if (n_freq <= 0) return HBEM_OK;
+    if (n_src < 1 || n_src > 8) return fail(HBEM_ERR_ARG, "hbem_solve_batch_multi: n_src must be 1 .. 8");
     if (!k_re || !q_re || !q_im || !info) return fail(HBEM_ERR_ARG, "hbem_solve_batch: NULL input");
     if (n_obs > 0 && (!obs_3xn || !field_re || !field_im)) return fail(HBEM_ERR_ARG, "hbem_solve_batch: NULL field buffers");
     if (n_tags > 0 && (!tags || !tag_avg)) return fail(HBEM_ERR_ARG, "hbem_solve_batch: NULL tag buffers");
@@ -118,16 +126,16 @@ extern "C" int hbem_solve_batch(hbem_session *h, int n_freq, const float *k_re, 
     const bool do_refine = !fp64 && ((precision == HBEM_PREC_MIXED) || refine_max_iter > 0);
     const int max_iter = precision == HBEM_PREC_MIXED ? std::max(1, refine_max_iter) : refine_max_iter;
     const double tol = refine_tol > 0 ? refine_tol : 1e-6;
-    const size_t n = s->n_dof, T = s->n_triangles;
+    const size_t n = s->n_dof, T = s->n_triangles, ns = (size_t)n_src;
 
     // chunk size: dense matrices within ~60 % of free memory
     size_t free_b = 0, total_b = 0;
     HBEM_CUDA(cudaMemGetInfo(&free_b, &total_b));
     free_b += s->ws_bytes;
     int chunk = n_freq;
-    while (chunk > 1 && layout(*s, chunk, n_obs, n_tags, do_refine, fp64).total > free_b * 6 / 10)
+    while (chunk > 1 && layout(*s, chunk, n_src, n_obs, n_tags, do_refine, fp64).total > free_b * 6 / 10)
         chunk = (chunk + 1) / 2;
-    const Layout L = layout(*s, chunk, n_obs, n_tags, do_refine, fp64);
+    const Layout L = layout(*s, chunk, n_src, n_obs, n_tags, do_refine, fp64);
     int rc = ensure_ws(*s, L.total);
     if (rc != HBEM_OK) return rc;
     char *ws = static_cast<char *>(s->ws);
@@ -149,56 +157,73 @@ extern "C" int hbem_solve_batch(hbem_session *h, int n_freq, const float *k_re, 
     double *da64 = fp64 ? reinterpret_cast<double *>(ws + L.a64) : nullptr;
     double *dx64 = fp64 ? reinterpret_cast<double *>(ws + L.x64) : nullptr;
 
-    cudaEvent_t ev[5];
-    for (auto &e : ev) HBEM_CUDA(cudaEventCreate(&e));
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    for (auto &e : ev) {
+        if (rc == HBEM_OK) {
+            const cudaError_t err = cudaEventCreate(&e);
+            if (err != cudaSuccess) rc = cuda_fail(err, "cudaEventCreate");
+        }
+    }
+    auto ok = [&](cudaError_t e, const char *what) {
+        if (rc == HBEM_OK && e != cudaSuccess) rc = cuda_fail(e, what);
+        return rc == HBEM_OK;
+    };
     float t_asm = 0, t_solve = 0, t_field = 0, t_total = 0;
-    HBEM_CUDA(cudaEventRecord(ev[4], st));
-    if (n_obs > 0) HBEM_CUDA(cudaMemcpyAsync(dobs, obs_3xn, 3 * sizeof(float) * n_obs, cudaMemcpyHostToDevice, st));
-    if (n_tags > 0) HBEM_CUDA(cudaMemcpyAsync(dwant, tags, sizeof(int) * n_tags, cudaMemcpyHostToDevice, st));
+    if (rc == HBEM_OK) ok(cudaEventRecord(ev[4], st), "cudaEventRecord");
+    if (n_obs > 0) ok(cudaMemcpyAsync(dobs, obs_3xn, 3 * sizeof(float) * n_obs, cudaMemcpyHostToDevice, st), "obs");
+    if (n_tags > 0) ok(cudaMemcpyAsync(dwant, tags, sizeof(int) * n_tags, cudaMemcpyHostToDevice, st), "tags");
+    std::vector<float> k_rep;
 
     for (int f0 = 0; f0 < n_freq && rc == HBEM_OK; f0 += chunk) {
         const int nf = std::min(chunk, n_freq - f0);
-        float *qr = dq, *qi = dq + (size_t)nf * T;
-        HBEM_CUDA(cudaMemcpyAsync(qr, q_re + (size_t)f0 * T, sizeof(float) * nf * T, cudaMemcpyHostToDevice, st));
-        HBEM_CUDA(cudaMemcpyAsync(qi, q_im + (size_t)f0 * T, sizeof(float) * nf * T, cudaMemcpyHostToDevice, st));
+        const size_t qs = (size_t)nf * T, xs = (size_t)nf * n;   // per-source strides on the device
+        float *qr = dq, *qi = dq + ns * qs;
+        for (int sv = 0; sv < n_src; ++sv) {
+            const size_t ho = ((size_t)sv * n_freq + f0) * T;
+            ok(cudaMemcpyAsync(qr + sv * qs, q_re + ho, sizeof(float) * qs, cudaMemcpyHostToDevice, st), "q");
+            ok(cudaMemcpyAsync(qi + sv * qs, q_im + ho, sizeof(float) * qs, cudaMemcpyHostToDevice, st), "q");
+        }
         float *ar = da, *ai = da + (size_t)nf * n * n;
-        float *br = db, *bi = db + (size_t)nf * n;
-        float *xr = dx, *xi = dx + (size_t)nf * n;
-        HBEM_CUDA(cudaEventRecord(ev[0], st));
-        rc = hbem_assemble(h, nf, k_re + f0, k_im ? k_im + f0 : nullptr, qr, qi, (long long)T, nullptr, nullptr, ar, ai,
-                           (long long)n, (long long)(n * n), br, bi, (long long)n, HBEM_ASM_CORRECTED, st);
+        float *br = db, *bi = db + ns * xs;
+        float *xr = dx, *xi = dx + ns * xs;
+        ok(cudaEventRecord(ev[0], st), "cudaEventRecord");
         if (rc != HBEM_OK) break;
-        HBEM_CUDA(cudaEventRecord(ev[1], st));
-        HBEM_CUDA(cudaMemcpyAsync(xr, br, sizeof(float) * nf * n, cudaMemcpyDeviceToDevice, st));
-        HBEM_CUDA(cudaMemcpyAsync(xi, bi, sizeof(float) * nf * n, cudaMemcpyDeviceToDevice, st));
+        rc = hbem_assemble_multi(h, nf, k_re + f0, k_im ? k_im + f0 : nullptr, n_src, qr, qi, (long long)T,
+                                 (long long)qs, nullptr, nullptr, ar, ai, (long long)n, (long long)(n * n), br, bi,
+                                 (long long)n, (long long)xs, HBEM_ASM_CORRECTED, st);
+        if (rc != HBEM_OK) break;
+        ok(cudaEventRecord(ev[1], st), "cudaEventRecord");
+        ok(cudaMemcpyAsync(xr, br, sizeof(float) * ns * xs, cudaMemcpyDeviceToDevice, st), "x");
+        ok(cudaMemcpyAsync(xi, bi, sizeof(float) * ns * xs, cudaMemcpyDeviceToDevice, st), "x");
         float *a0r = nullptr, *a0i = nullptr;
         if (do_refine) {
             a0r = da0;
             a0i = da0 + (size_t)nf * n * n;
-            HBEM_CUDA(cudaMemcpyAsync(a0r, ar, sizeof(float) * nf * n * n, cudaMemcpyDeviceToDevice, st));
-            HBEM_CUDA(cudaMemcpyAsync(a0i, ai, sizeof(float) * nf * n * n, cudaMemcpyDeviceToDevice, st));
+            ok(cudaMemcpyAsync(a0r, ar, sizeof(float) * nf * n * n, cudaMemcpyDeviceToDevice, st), "A copy");
+            ok(cudaMemcpyAsync(a0i, ai, sizeof(float) * nf * n * n, cudaMemcpyDeviceToDevice, st), "A copy");
         }
+        if (rc != HBEM_OK) break;
         if (rcond) {
             rc = matrix_norm1((int)n, nf, ar, ai, (long long)n, (long long)(n * n), danorm, st);
             if (rc != HBEM_OK) break;
         }
+        const long long nn = (long long)(n * n);
         if (fp64) {
             // the reference's float64 dense solve: widen the FP32 system to
             // complex128, factor and solve in FP64, narrow the solution
-            const long long nn = (long long)(n * n);
             double *a64r = da64, *a64i = da64 + (size_t)nf * n * n;
-            double *x64r = dx64, *x64i = dx64 + (size_t)nf * n;
+            double *x64r = dx64, *x64i = dx64 + ns * xs;
             rc = widen_f64((int)n, (int)n, nf, ar, ai, (long long)n, nn, a64r, a64i, (long long)n, nn, st);
             if (rc == HBEM_OK)
-                rc = widen_f64(1, (int)n, nf, br, bi, (long long)n, (long long)n, x64r, x64i, (long long)n,
+                rc = widen_f64(1, (int)n, n_src * nf, br, bi, (long long)n, (long long)n, x64r, x64i, (long long)n,
                                (long long)n, st);
             if (rc == HBEM_OK)
                 rc = lu_factor_f64((int)n, nf, a64r, a64i, (long long)n, nn, dpiv, (long long)n, dinfo, st);
+            for (int sv = 0; sv < n_src && rc == HBEM_OK; ++sv)
+                rc = lu_solve_f64((int)n, 1, nf, a64r, a64i, (long long)n, nn, dpiv, (long long)n, x64r + sv * xs,
+                                  x64i + sv * xs, 1, (long long)n, st);
             if (rc == HBEM_OK)
-                rc = lu_solve_f64((int)n, 1, nf, a64r, a64i, (long long)n, nn, dpiv, (long long)n, x64r, x64i, 1,
-                                  (long long)n, st);
-            if (rc == HBEM_OK)
-                rc = narrow_f64(1, (int)n, nf, x64r, x64i, (long long)n, (long long)n, xr, xi, (long long)n,
+                rc = narrow_f64(1, (int)n, n_src * nf, x64r, x64i, (long long)n, (long long)n, xr, xi, (long long)n,
                                 (long long)n, st);
             if (rc == HBEM_OK && rcond) {
                 // condition estimate from the FP64 factors narrowed to FP32
@@ -207,52 +232,65 @@ extern "C" int hbem_solve_batch(hbem_session *h, int n_freq, const float *k_re, 
             }
             if (rc != HBEM_OK) break;
         } else {
-            rc = lu_factor((int)n, nf, ar, ai, (long long)n, (long long)(n * n), dpiv, (long long)n, dinfo, precision,
-                           st);
+            rc = lu_factor((int)n, nf, ar, ai, (long long)n, nn, dpiv, (long long)n, dinfo, precision, st);
             if (rc != HBEM_OK) break;
             if (rcond) {
-                rc = lu_rcond((int)n, nf, ar, ai, (long long)n, (long long)(n * n), danorm, drcond, st);
+                rc = lu_rcond((int)n, nf, ar, ai, (long long)n, nn, danorm, drcond, st);
                 if (rc != HBEM_OK) break;
             }
-            rc = lu_solve((int)n, 1, nf, ar, ai, (long long)n, (long long)(n * n), dpiv, (long long)n, xr, xi, 1,
-                          (long long)n, HBEM_TRANS_N, st);
+            for (int sv = 0; sv < n_src && rc == HBEM_OK; ++sv)
+                rc = lu_solve((int)n, 1, nf, ar, ai, (long long)n, nn, dpiv, (long long)n, xr + sv * xs, xi + sv * xs,
+                              1, (long long)n, HBEM_TRANS_N, st);
             if (rc != HBEM_OK) break;
         }
         if (do_refine) {
-            rc = refine((int)n, nf, a0r, a0i, (long long)n, (long long)(n * n), ar, ai, (long long)(n * n), dpiv,
-                        (long long)n, br, bi, (long long)n, xr, xi, (long long)n, tol, max_iter, diters, dres, st);
+            for (int sv = 0; sv < n_src && rc == HBEM_OK; ++sv)
+                rc = refine((int)n, nf, a0r, a0i, (long long)n, nn, ar, ai, nn, dpiv, (long long)n, br + sv * xs,
+                            bi + sv * xs, (long long)n, xr + sv * xs, xi + sv * xs, (long long)n, tol, max_iter,
+                            diters + (size_t)sv * nf, dres + (size_t)sv * nf, st);
             if (rc != HBEM_OK) break;
         }
-        HBEM_CUDA(cudaEventRecord(ev[2], st));
-        float *fr = dfld, *fi = dfld + (size_t)nf * std::max(1, n_obs);
-        if (n_obs > 0) {
-            rc = launch_field(*s, nf, k_re + f0, xr, xi, (long long)n, qr, qi, (long long)T, dobs, n_obs, fr, fi,
-                              (long long)n_obs, st);
-            if (rc != HBEM_OK) break;
+        ok(cudaEventRecord(ev[2], st), "cudaEventRecord");
+        // field and tag averages for every (source, frequency) case at once
+        k_rep.resize(ns * nf);
+        for (int sv = 0; sv < n_src; ++sv)
+            for (int f = 0; f < nf; ++f) k_rep[(size_t)sv * nf + f] = k_re[f0 + f];
+        const size_t fs = (size_t)nf * std::max(1, n_obs);
+        float *fr = dfld, *fi = dfld + ns * fs;
+        if (rc == HBEM_OK && n_obs > 0)
+            rc = launch_field(*s, n_src * nf, k_rep.data(), xr, xi, (long long)n, qr, qi, (long long)T, dobs, n_obs, fr,
+                              fi, (long long)n_obs, st);
+        if (rc == HBEM_OK && n_tags > 0) rc = launch_tag_avg(*s, n_src * nf, xr, xi, (long long)n, dwant, n_tags, dtag, st);
+        if (rc != HBEM_OK) break;
+        ok(cudaEventRecord(ev[3], st), "cudaEventRecord");
+        for (int sv = 0; sv < n_src; ++sv) {
+            const size_t hf = (size_t)sv * n_freq + f0;   // first host case of this source in the chunk
+            if (n_obs > 0) {
+                ok(cudaMemcpyAsync(field_re + hf * n_obs, fr + sv * fs, sizeof(float) * nf * n_obs,
+                                   cudaMemcpyDeviceToHost, st), "field");
+                ok(cudaMemcpyAsync(field_im + hf * n_obs, fi + sv * fs, sizeof(float) * nf * n_obs,
+                                   cudaMemcpyDeviceToHost, st), "field");
+            }
+            if (n_tags > 0)
+                ok(cudaMemcpyAsync(tag_avg + hf * n_tags * 2, dtag + (size_t)sv * nf * n_tags * 2,
+                                   2 * sizeof(double) * nf * n_tags, cudaMemcpyDeviceToHost, st), "tag averages");
+            if (surface_re) {
+                ok(cudaMemcpyAsync(surface_re + hf * n, xr + sv * xs, sizeof(float) * xs, cudaMemcpyDeviceToHost, st),
+                   "surface");
+                ok(cudaMemcpyAsync(surface_im + hf * n, xi + sv * xs, sizeof(float) * xs, cudaMemcpyDeviceToHost, st),
+                   "surface");
+            }
+            if (do_refine && refine_iters)
+                ok(cudaMemcpyAsync(refine_iters + hf, diters + (size_t)sv * nf, sizeof(int) * nf,
+                                   cudaMemcpyDeviceToHost, st), "iters");
+            if (do_refine && refine_resid)
+                ok(cudaMemcpyAsync(refine_resid + hf, dres + (size_t)sv * nf, sizeof(double) * nf,
+                                   cudaMemcpyDeviceToHost, st), "resid");
         }
-        if (n_tags > 0) {
-            rc = launch_tag_avg(*s, nf, xr, xi, (long long)n, dwant, n_tags, dtag, st);
-            if (rc != HBEM_OK) break;
-        }
-        HBEM_CUDA(cudaEventRecord(ev[3], st));
-        if (n_obs > 0) {
-            HBEM_CUDA(cudaMemcpyAsync(field_re + (size_t)f0 * n_obs, fr, sizeof(float) * nf * n_obs, cudaMemcpyDeviceToHost, st));
-            HBEM_CUDA(cudaMemcpyAsync(field_im + (size_t)f0 * n_obs, fi, sizeof(float) * nf * n_obs, cudaMemcpyDeviceToHost, st));
-        }
-        if (n_tags > 0)
-            HBEM_CUDA(cudaMemcpyAsync(tag_avg + (size_t)f0 * n_tags * 2, dtag, 2 * sizeof(double) * nf * n_tags,
-                                      cudaMemcpyDeviceToHost, st));
-        if (surface_re) {
-            HBEM_CUDA(cudaMemcpyAsync(surface_re + (size_t)f0 * n, xr, sizeof(float) * nf * n, cudaMemcpyDeviceToHost, st));
-            HBEM_CUDA(cudaMemcpyAsync(surface_im + (size_t)f0 * n, xi, sizeof(float) * nf * n, cudaMemcpyDeviceToHost, st));
-        }
-        HBEM_CUDA(cudaMemcpyAsync(info + f0, dinfo, sizeof(int) * nf, cudaMemcpyDeviceToHost, st));
-        if (rcond) HBEM_CUDA(cudaMemcpyAsync(rcond + f0, drcond, sizeof(double) * nf, cudaMemcpyDeviceToHost, st));
-        if (do_refine && refine_iters)
-            HBEM_CUDA(cudaMemcpyAsync(refine_iters + f0, diters, sizeof(int) * nf, cudaMemcpyDeviceToHost, st));
-        if (do_refine && refine_resid)
-            HBEM_CUDA(cudaMemcpyAsync(refine_resid + f0, dres, sizeof(double) * nf, cudaMemcpyDeviceToHost, st));
-        HBEM_CUDA(cudaStreamSynchronize(st));
+        ok(cudaMemcpyAsync(info + f0, dinfo, sizeof(int) * nf, cudaMemcpyDeviceToHost, st), "info");
+        if (rcond) ok(cudaMemcpyAsync(rcond + f0, drcond, sizeof(double) * nf, cudaMemcpyDeviceToHost, st), "rcond");
+        ok(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        if (rc != HBEM_OK) break;
         float ms = 0;
         cudaEventElapsedTime(&ms, ev[0], ev[1]); t_asm += ms;
         cudaEventElapsedTime(&ms, ev[1], ev[2]); t_solve += ms;
@@ -266,8 +304,8 @@ extern "C" int hbem_solve_batch(hbem_session *h, int n_freq, const float *k_re, 
     }
     if (rc == HBEM_OK) {
         if (!do_refine) {
-            if (refine_iters) std::memset(refine_iters, 0, sizeof(int) * n_freq);
-            if (refine_resid) std::memset(refine_resid, 0, sizeof(double) * n_freq);
+            if (refine_iters) std::memset(refine_iters, 0, sizeof(int) * ns * n_freq);
+            if (refine_resid) std::memset(refine_resid, 0, sizeof(double) * ns * n_freq);
         }
         if (timings_ms) {
             timings_ms[0] = t_asm;
@@ -278,6 +316,29 @@ extern "C" int hbem_solve_batch(hbem_session *h, int n_freq, const float *k_re, 
     } else {
         cudaStreamSynchronize(st);
     }
-    for (auto &e : ev) cudaEventDestroy(e);
+    for (auto &e : ev)
+        if (e) cudaEventDestroy(e);
     return rc;
+}
+
+extern "C" int hbem_solve_batch(hbem_session *h, int n_freq, const float *k_re, const float *k_im, const float *q_re,
+                                const float *q_im, const float *obs_3xn, int n_obs, const int *tags, int n_tags,
+                                int precision, double refine_tol, int refine_max_iter, float *field_re,
+                                float *field_im, double *tag_avg, float *surface_re, float *surface_im, int *info,
+                                int *refine_iters, double *refine_resid, double *rcond, float *timings_ms,
+                                void *stream) {
+    return solve_batch_impl(h, n_freq, 1, k_re, k_im, q_re, q_im, obs_3xn, n_obs, tags, n_tags, precision, refine_tol,
+                            refine_max_iter, field_re, field_im, tag_avg, surface_re, surface_im, info, refine_iters,
+                            refine_resid, rcond, timings_ms, stream);
+}
+
+extern "C" int hbem_solve_batch_multi(hbem_session *h, int n_freq, int n_src, const float *k_re, const float *k_im,
+                                      const float *q_re, const float *q_im, const float *obs_3xn, int n_obs,
+                                      const int *tags, int n_tags, int precision, double refine_tol,
+                                      int refine_max_iter, float *field_re, float *field_im, double *tag_avg,
+                                      float *surface_re, float *surface_im, int *info, int *refine_iters,
+                                      double *refine_resid, double *rcond, float *timings_ms, void *stream) {
+    return solve_batch_impl(h, n_freq, n_src, k_re, k_im, q_re, q_im, obs_3xn, n_obs, tags, n_tags, precision,
+                            refine_tol, refine_max_iter, field_re, field_im, tag_avg, surface_re, surface_im, info,
+                            refine_iters, refine_resid, rcond, timings_ms, stream);
 }

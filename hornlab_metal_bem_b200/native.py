@@ -98,6 +98,10 @@ _SIGNATURES = {
     "hbem_field_f64": ([_vp, _c_int, _vp, _vp, _vp, _c_ll, _vp, _vp, _c_ll, _vp, _c_int, _vp, _vp, _c_ll, _vp],
                        _c_int),
     "hbem_solve_status": ([_vp], _c_int),
+    "hbem_assemble_multi": ([_vp, _c_int, _vp, _vp, _c_int, _vp, _vp, _c_ll, _c_ll, _vp, _vp, _vp, _vp, _c_ll, _c_ll,
+                             _vp, _vp, _c_ll, _c_ll, _c_int, _vp], _c_int),
+    "hbem_solve_batch_multi": ([_vp, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp, _c_int, _vp, _c_int, _c_int, _c_d,
+                                _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _c_int),
     "hbem_lu_factor_f64": ([_c_int, _c_int, _vp, _vp, _c_ll, _c_ll, _vp, _c_ll, _vp, _vp], _c_int),
     "hbem_lu_solve_f64": ([_c_int, _c_int, _c_int, _vp, _vp, _c_ll, _c_ll, _vp, _c_ll, _vp, _vp, _c_ll, _c_ll,
                            _c_int, _vp], _c_int),
@@ -212,6 +216,24 @@ class CaseResult:
     field_s: float
     lapack_info: int
     diagnostics: dict[str, Any] = field(default_factory=dict)
+    extra_sources: tuple = ()              # ExtraSourceResult per extra velocity source
+
+
+@dataclass
+class ExtraSourceResult:
+    """Outputs of one extra velocity source sharing a case's assembled and factored matrix (the reference's
+    ``ExtraSourceSolveResult``, ``hornlab_metal_bem/metal/session.py:330-350``, in memory)."""
+
+    source_index: int                      # 1-based: the primary source is 0
+    field: np.ndarray                      # (N_obs,) complex64
+    impedance: complex | None
+    surface_pressure_avg: dict[int, complex] | None
+    surface_pressure: np.ndarray | None
+    refine_iterations: int = 0
+    refine_residual_rel: float | None = None
+
+
+MAX_SOURCES_PER_PASS = 8
 
 
 class NativeSession:
@@ -441,6 +463,8 @@ class NativeSession:
         timings_out: dict | None = None,
         compute_rcond: bool = True,
         impedance_sources=None,
+        extra_neumann_dp0=None,
+        extra_impedance_source_tags=None,
         **_ignored,
     ) -> list[CaseResult]:
         """Assemble, factor, solve and evaluate every frequency in one native call.
@@ -458,16 +482,41 @@ class NativeSession:
         plain LU solution as cgesv gives it.  ``compute_rcond`` adds the
         1-norm condition estimate of each matrix (``dense_solve_rcond``), as the
         reference computes with cgecon for every case.
+
+        ``extra_neumann_dp0`` (n_extra, F, T) adds velocity sources that share
+        each frequency's assembled and factored matrix (the reference's
+        multi-RHS batch, ``native.py:775-779``): one assembly pass evaluates
+        the kernel once for the matrix and every source's right-hand side,
+        one LU per frequency, one solve per source.  Their outputs are each
+        result's ``extra_sources``; ``extra_impedance_source_tags`` names the
+        tag whose average becomes each extra source's ``impedance``.
         """
         freqs = np.ascontiguousarray(np.atleast_1d(frequency_hz), dtype=np.float64)
         F = freqs.shape[0]
         k_re = np.ascontiguousarray(np.atleast_1d(k_real_f32), dtype=np.float32)
         if k_re.shape != (F,):
             raise ValueError("k_real_f32 must have one value per frequency")
+        extra = None
+        if extra_neumann_dp0 is not None:
+            extra = np.asarray(extra_neumann_dp0)
+            if extra.ndim != 3 or extra.shape[1:] != (F, self.n_triangles):
+                raise ValueError(f"extra_neumann_dp0 must have shape (n_extra, {F}, {self.n_triangles}), "
+                                 f"got {extra.shape}")
+            if extra.shape[0] == 0:
+                raise ValueError("extra_neumann_dp0 must be None or non-empty")
+            if not np.all(np.isfinite(extra)):
+                raise ValueError("extra_neumann_dp0 must contain only finite values")
+            if extra_impedance_source_tags is not None and len(extra_impedance_source_tags) != extra.shape[0]:
+                raise ValueError("extra_impedance_source_tags must name one tag (or None) per extra source")
+        elif extra_impedance_source_tags is not None:
+            raise ValueError("extra_impedance_source_tags requires extra_neumann_dp0")
         if impedance_sources:
             per = impedance_sources if isinstance(impedance_sources, list) else [impedance_sources] * F
             if len(per) != F:
                 raise ValueError(f"impedance_sources list must have one dict per frequency ({F}), got {len(per)}")
+            if any(per) and extra is not None:
+                raise BackendUnavailable("extra_neumann_dp0 with impedance_sources (Robin) is solved one source at a "
+                                         "time; call once per source")
             if any(per):
                 return self._robin_batch(freqs, k_re, k_imag_f32, neumann_dp0, observation_points, per,
                                          source_tags=source_tags, impedance_source_tag=impedance_source_tag,
@@ -491,62 +540,94 @@ class NativeSession:
         N = obs.shape[1]
         tags = list(source_tags or [])
         imp_tag = impedance_source_tag
-        want = list(tags) + ([imp_tag] if imp_tag is not None and imp_tag not in tags else [])
+        extra_tags = list(extra_impedance_source_tags) if extra is not None and extra_impedance_source_tags else []
+        want = list(tags)
+        for t in [imp_tag] + extra_tags:
+            if t is not None and t not in want:
+                want.append(t)
         want_arr = np.ascontiguousarray(want, dtype=np.int32) if want else np.zeros(1, np.int32)
-        qr = np.ascontiguousarray(q.real, dtype=np.float32)
-        qi = np.ascontiguousarray(q.imag, dtype=np.float32)
-        fr = np.zeros((F, N), np.float32)
-        fi = np.zeros((F, N), np.float32)
-        tavg = np.zeros((F, max(1, len(want)), 2), np.float64)
-        sr = np.zeros((F, self.n_dof), np.float32) if write_surface_pressure else None
-        si = np.zeros((F, self.n_dof), np.float32) if write_surface_pressure else None
-        info = np.zeros(F, np.int32)
-        iters = np.zeros(F, np.int32)
-        resid = np.zeros(F, np.float64)
-        rcond = np.zeros(F, np.float64) if compute_rcond else None
-        tms = np.zeros(4, np.float32)
+        qs = q[None] if extra is None else np.concatenate([q[None], extra], axis=0)   # (S, F, T)
+        S = qs.shape[0]
         mode = solve_mode(precision, dense_solve_dtype)
         prec = {"plain": HBEM_PREC_PLAIN, "mixed": HBEM_PREC_MIXED, "fp64": HBEM_PREC_FP64}[mode]
         max_it = 0 if mode == "fp64" else int(refine_max_iterations)
         if mode == "mixed":
             max_it = max(1, max_it)
         tol = float(refine_tolerance)
+        fr = np.zeros((S, F, N), np.float32)
+        fi = np.zeros((S, F, N), np.float32)
+        tavg = np.zeros((S, F, max(1, len(want)), 2), np.float64)
+        sr = np.zeros((S, F, self.n_dof), np.float32) if (write_surface_pressure or S > 1) else None
+        si = np.zeros((S, F, self.n_dof), np.float32) if sr is not None else None
+        info = np.zeros(F, np.int32)
+        iters = np.zeros((S, F), np.int32)
+        resid = np.zeros((S, F), np.float64)
+        rcond = np.zeros(F, np.float64) if compute_rcond else None
+        tms = np.zeros(4, np.float32)
         t0 = time.perf_counter()
-        check(self.lib.hbem_solve_batch(
-            self.handle, F, _np_ptr(k_re), _np_ptr(k_im), _np_ptr(qr), _np_ptr(qi), _np_ptr(obs), N,
-            _np_ptr(want_arr), len(want), prec, tol, max_it, _np_ptr(fr), _np_ptr(fi), _np_ptr(tavg), _np_ptr(sr),
-            _np_ptr(si), _np_ptr(info), _np_ptr(iters), _np_ptr(resid), _np_ptr(rcond), _np_ptr(tms), None),
-            "hbem_solve_batch", self.lib)
+        for s0 in range(0, S, MAX_SOURCES_PER_PASS):
+            sl = slice(s0, min(S, s0 + MAX_SOURCES_PER_PASS))
+            ns = sl.stop - sl.start
+            qr = np.ascontiguousarray(qs[sl].real, dtype=np.float32)
+            qi = np.ascontiguousarray(qs[sl].imag, dtype=np.float32)
+            tpart = np.zeros(4, np.float32)
+            views = [np.ascontiguousarray(a[sl]) if a is not None else None for a in (fr, fi, tavg, sr, si, iters, resid)]
+            check(self.lib.hbem_solve_batch_multi(
+                self.handle, F, ns, _np_ptr(k_re), _np_ptr(k_im), _np_ptr(qr), _np_ptr(qi), _np_ptr(obs), N,
+                _np_ptr(want_arr), len(want), prec, tol, max_it, _np_ptr(views[0]), _np_ptr(views[1]),
+                _np_ptr(views[2]), _np_ptr(views[3]), _np_ptr(views[4]), _np_ptr(info), _np_ptr(views[5]),
+                _np_ptr(views[6]), _np_ptr(rcond), _np_ptr(tpart), None), "hbem_solve_batch", self.lib)
+            for a, v in zip((fr, fi, tavg, sr, si, iters, resid), views):
+                if a is not None:
+                    a[sl] = v
+            tms += tpart
         wall = time.perf_counter() - t0
         if timings_out is not None:
             timings_out.update(assembly_ms=float(tms[0]), solve_ms=float(tms[1]), field_ms=float(tms[2]),
-                               total_ms=float(tms[3]), wall_s=wall)
+                               total_ms=float(tms[3]), wall_s=wall, sources=S)
         per = 1.0 / F
         results = []
         for f in range(F):
-            avgs = {int(t): complex(tavg[f, j, 0], tavg[f, j, 1]) for j, t in enumerate(want)}
+            avgs = [{int(t): complex(tavg[s_, f, j, 0], tavg[s_, f, j, 1]) for j, t in enumerate(want)}
+                    for s_ in range(S)]
             diag = {
                 "dense_solve_impl": SOLVE_IMPL[mode] + ("_refined" if max_it > 0 else ""),
                 "dense_solve_dtype": dense_solve_dtype,
                 "precision": precision,
-                "refine_iterations": int(iters[f]),
-                "refine_residual_rel": float(resid[f]) if max_it > 0 else None,
+                "refine_iterations": int(iters[0, f]),
+                "refine_residual_rel": float(resid[0, f]) if max_it > 0 else None,
                 "dense_solve_rcond": float(rcond[f]) if rcond is not None and info[f] == 0 else None,
                 "assembly_mode": "corrected",
                 "duffy_pairs": None,
                 **_case_flags(float(k_re[f]), 0.0 if k_im is None else float(k_im[f])),
             }
+            if S > 1:
+                diag["multi_source"] = True
+                diag["sources_sharing_factorisation"] = S
+            extras = tuple(
+                ExtraSourceResult(
+                    source_index=s_,
+                    field=(fr[s_, f] + 1j * fi[s_, f]).astype(np.complex64),
+                    impedance=(avgs[s_].get(int(extra_tags[s_ - 1]))
+                               if extra_tags and extra_tags[s_ - 1] is not None else None),
+                    surface_pressure_avg={int(t): avgs[s_][int(t)] for t in tags} if tags else None,
+                    surface_pressure=(sr[s_, f] + 1j * si[s_, f]).astype(np.complex64) if sr is not None else None,
+                    refine_iterations=int(iters[s_, f]),
+                    refine_residual_rel=float(resid[s_, f]) if max_it > 0 else None,
+                ) for s_ in range(1, S))
             results.append(CaseResult(
                 frequency_hz=float(freqs[f]),
-                field=(fr[f] + 1j * fi[f]).astype(np.complex64),
-                impedance=avgs.get(int(imp_tag)) if imp_tag is not None else None,
-                surface_pressure_avg={int(t): avgs[int(t)] for t in tags} if tags else None,
-                surface_pressure=None if sr is None else (sr[f] + 1j * si[f]).astype(np.complex64),
+                field=(fr[0, f] + 1j * fi[0, f]).astype(np.complex64),
+                impedance=avgs[0].get(int(imp_tag)) if imp_tag is not None else None,
+                surface_pressure_avg={int(t): avgs[0][int(t)] for t in tags} if tags else None,
+                surface_pressure=(None if not write_surface_pressure
+                                  else (sr[0, f] + 1j * si[0, f]).astype(np.complex64)),
                 assembly_s=float(tms[0]) * 1e-3 * per,
                 dense_solve_s=float(tms[1]) * 1e-3 * per,
                 field_s=float(tms[2]) * 1e-3 * per,
                 lapack_info=int(info[f]),
                 diagnostics=diag,
+                extra_sources=extras,
             ))
         return results
 

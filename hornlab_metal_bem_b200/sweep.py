@@ -161,27 +161,44 @@ def run_sweep(mesh: LoadedMesh, frequencies, frame: ObservationFrame, config: So
 
     ``average_tags`` adds tags to the surface-pressure averages (the sorted union with the
     velocity-source tags is recorded); multi-source sweeps pass every source's tags."""
-    should_route_native(config)
+    return _run_sweep_sources(mesh, frequencies, frame, [config], session=session, average_tags=average_tags)[0]
+
+
+def _run_sweep_sources(mesh: LoadedMesh, frequencies, frame: ObservationFrame, configs: list[SolveConfig],
+                       *, session: NativeSession | None = None, average_tags=None) -> list[SolveResult]:
+    """One sweep for one or more velocity-source configurations that differ only in their sources.
+
+    With several sources every frequency's matrix is assembled and factored once and each source is a
+    right-hand side of it (the reference's multi-RHS sweep, ``sweep.py:957-1301`` with
+    ``main.swift:6348-6368, 7887``); the streaming callback then fires once per frequency with the first
+    source's entry plus ``source_results`` (one entry per source)."""
+    config = configs[0]
+    for c in configs:
+        should_route_native(c)
     freqs = np.asarray(frequencies, dtype=np.float64)
     if freqs.size == 0:
         raise ValueError("frequencies must contain at least one value")
     mesh_tags = {int(t) for t in np.unique(mesh.physical_tags)}
-    missing = sorted(set(config.velocity_sources) - mesh_tags)
-    if missing:
-        raise ValueError(
-            f"velocity_sources tags {missing} are not present in the mesh; available physical tags: {sorted(mesh_tags)}"
-        )
+    for c in configs:
+        missing = sorted(set(c.velocity_sources) - mesh_tags)
+        if missing:
+            raise ValueError(
+                f"velocity_sources tags {missing} are not present in the mesh; available physical tags: "
+                f"{sorted(mesh_tags)}"
+            )
+    n_src = len(configs)
     t_total = time.time()
     obs_points, angles = build_observation_points(frame, config.observation)
     p1, dp0 = make_pure_function_spaces(mesh.grid)
     buffers = build_geometry_buffers(mesh.grid, mesh.physical_tags, p1, dp0)
     max_edge = mesh_max_edge(mesh)
-    source_tags = list(config.velocity_sources.keys())
+    source_tags = sorted({int(t) for c in configs for t in c.velocity_sources})
+    if n_src == 1:
+        source_tags = list(config.velocity_sources.keys())
     if average_tags is not None:
         source_tags = sorted({int(t) for t in source_tags} | {int(t) for t in average_tags})
-    scale = build_source_face_scale(mesh.grid, mesh.physical_tags, config, frame.axis, frame.source_center)
     on_axis = int(np.argmin(np.abs(angles)))
-    imp_tag = min(config.velocity_sources.keys(), default=2)
+    imp_tags = [min(c.velocity_sources.keys(), default=2) for c in configs]
     n_planes, n_angles, _ = obs_points.shape
     pts = field_points_3xn(obs_points)
     n_sphere = 0
@@ -195,15 +212,22 @@ def run_sweep(mesh: LoadedMesh, frequencies, frame: ObservationFrame, config: So
         robin = impedance_sources_for_frequencies(mesh.physical_tags, freqs, config)
         if not any(robin):
             robin = None
-    q = neumann_rows(buffers.n_triangles, mesh.physical_tags, freqs, config, scale, robin)
+    if n_src > 1 and (robin is not None or config.aperture_tag is not None):
+        raise ValueError("shared-factorisation multi-source sweeps support neither Robin walls nor the coupled baffle")
+    qs = []
+    for c in configs:
+        scale = build_source_face_scale(mesh.grid, mesh.physical_tags, c, frame.axis, frame.source_center)
+        qs.append(neumann_rows(buffers.n_triangles, mesh.physical_tags, freqs, c, scale, robin))
+    q = qs[0]
+    extra = np.stack(qs[1:], axis=0) if n_src > 1 else None
 
     own = session is None
     if own:
         session = NativeSession(buffers, symmetry_plane=config.native_symmetry_plane,
                                 aperture_tag=config.aperture_tag, velocity_source_tags=source_tags,
                                 check_open_edges=config.native_check_open_edges)
-    pressure_rows, spl_rows, imp_rows, surf_rows, diag_rows, log = [], [], [], [], [], []
-    pavg: dict[int, list[complex]] = {t: [] for t in source_tags}
+    rows = [dict(pressure=[], spl=[], imp=[], surf=[], diag=[], log=[], pavg={t: [] for t in source_tags})
+            for _ in configs]
     done: list[float] = []
     try:
         chunk = freqs.size if config.on_frequency_result is None else 1
@@ -212,53 +236,65 @@ def run_sweep(mesh: LoadedMesh, frequencies, frame: ObservationFrame, config: So
             sl = slice(f0, f0 + chunk)
             batch_fn = (session.coupled_ib_batch if config.aperture_tag is not None
                         else session.assemble_solve_evaluate_standard_neumann_batch)
+            kw = {}
+            if extra is not None:
+                kw = dict(extra_neumann_dp0=extra[:, sl], extra_impedance_source_tags=imp_tags[1:])
             results = batch_fn(
                 freqs[sl], k_re[sl], q[sl], pts, k_imag_f32=k_im[sl], source_tags=source_tags,
-                impedance_source_tag=imp_tag, write_surface_pressure=config.return_surface_pressure,
+                impedance_source_tag=imp_tags[0], write_surface_pressure=config.return_surface_pressure,
                 dense_solve_dtype=config.dense_solve_dtype, precision=config.precision,
                 refine_tolerance=config.refine_tolerance, refine_max_iterations=config.refine_max_iterations,
                 compute_rcond=config.dense_solve_rcond_warning_threshold > 0,
-                impedance_sources=None if robin is None else robin[sl],
+                impedance_sources=None if robin is None else robin[sl], **kw,
             )
             for j, res in enumerate(results):
                 i = f0 + j
                 if res.lapack_info != 0:
                     raise RuntimeError(f"dense LU failed at {res.frequency_hz:.3f} Hz: zero pivot {res.lapack_info}")
-                flat = res.field.astype(np.complex128)
-                arc = flat[: n_planes * n_angles].reshape(n_planes, n_angles)
-                sphere = flat[n_planes * n_angles:] if n_sphere else None
-                spl = directivity_from_pressure(arc, on_axis)
-                diag = dict(res.diagnostics)
-                apply_dense_solve_policy(diag, config.dense_solve_rcond_warning_threshold)
-                apply_mesh_resolution_policy(diag, res.frequency_hz, max_edge, config.mesh_elements_per_wavelength_min)
-                for t in source_tags:
-                    pavg[t].append(res.surface_pressure_avg[int(t)])
-                entry = {
-                    "frequency_hz": res.frequency_hz,
-                    "iterations": None,
-                    "timing_s": res.assembly_s + res.dense_solve_s + res.field_s,
-                    "backend": "hbem_b200_batch" if chunk > 1 else "hbem_b200_streamed",
-                    "assembly_s": res.assembly_s,
-                    "dense_solve_s": res.dense_solve_s,
-                    "field_s": res.field_s,
-                    "lapack_info": res.lapack_info,
-                    "impedance": res.impedance,
-                    "native_diagnostics": diag,
-                    "observation_sphere_pressure_complex": sphere,
-                }
+                diag0 = dict(res.diagnostics)
+                apply_dense_solve_policy(diag0, config.dense_solve_rcond_warning_threshold)
+                apply_mesh_resolution_policy(diag0, res.frequency_hz, max_edge, config.mesh_elements_per_wavelength_min)
+                entries = []
+                for s_, acc in enumerate(rows):
+                    out = res if s_ == 0 else res.extra_sources[s_ - 1]
+                    flat = out.field.astype(np.complex128)
+                    arc = flat[: n_planes * n_angles].reshape(n_planes, n_angles)
+                    sphere = flat[n_planes * n_angles:] if n_sphere else None
+                    spl = directivity_from_pressure(arc, on_axis)
+                    diag = dict(diag0)
+                    if s_ > 0:
+                        diag.update(refine_iterations=out.refine_iterations,
+                                    refine_residual_rel=out.refine_residual_rel, source_index=s_)
+                    for t in source_tags:
+                        acc["pavg"][t].append(out.surface_pressure_avg[int(t)])
+                    entry = {
+                        "frequency_hz": res.frequency_hz,
+                        "iterations": None,
+                        "timing_s": res.assembly_s + res.dense_solve_s + res.field_s,
+                        "backend": "hbem_b200_batch" if chunk > 1 else "hbem_b200_streamed",
+                        "assembly_s": res.assembly_s,
+                        "dense_solve_s": res.dense_solve_s,
+                        "field_s": res.field_s,
+                        "lapack_info": res.lapack_info,
+                        "impedance": out.impedance,
+                        "native_diagnostics": diag,
+                        "observation_sphere_pressure_complex": sphere,
+                    }
+                    acc["pressure"].append(arc)
+                    acc["spl"].append(spl)
+                    acc["imp"].append(out.impedance)
+                    if config.return_surface_pressure:
+                        acc["surf"].append(out.surface_pressure.astype(np.complex128))
+                    acc["diag"].append(diag)
+                    acc["log"].append(entry)
+                    entries.append({**entry, "observation_pressure_complex": arc, "observation_directivity_db": spl,
+                                    "observation_angles_deg": angles,
+                                    "observation_planes": config.observation.planes})
                 done.append(res.frequency_hz)
-                pressure_rows.append(arc)
-                spl_rows.append(spl)
-                imp_rows.append(res.impedance)
-                if config.return_surface_pressure:
-                    surf_rows.append(res.surface_pressure.astype(np.complex128))
-                diag_rows.append(diag)
-                log.append(entry)
                 if config.progress_callback is not None:
                     config.progress_callback(i, freqs.size, res.frequency_hz)
                 if config.on_frequency_result is not None:
-                    cb = {**entry, "observation_pressure_complex": arc, "observation_directivity_db": spl,
-                          "observation_angles_deg": angles, "observation_planes": config.observation.planes}
+                    cb = entries[0] if n_src == 1 else {**entries[0], "source_results": entries}
                     if config.on_frequency_result(i, res.frequency_hz, cb) is False:
                         logger.info("Early stop requested after %.1f Hz", res.frequency_hz)
                         stop = True
@@ -268,29 +304,33 @@ def run_sweep(mesh: LoadedMesh, frequencies, frame: ObservationFrame, config: So
     finally:
         if own:
             session.close()
-    timings = {
-        "solve_s": sum(e["timing_s"] for e in log),
-        "assembly_s": sum(e["assembly_s"] for e in log),
-        "dense_solve_s": sum(e["dense_solve_s"] for e in log),
-        "directivity_s": sum(e["field_s"] for e in log),
-        "total_s": time.time() - t_total,
-    }
-    return SolveResult(
-        frequencies_hz=np.array(done, dtype=np.float64),
-        pressure_complex=np.stack(pressure_rows, axis=0),
-        directivity_db=np.stack(spl_rows, axis=0),
-        impedance=np.array(imp_rows, dtype=np.complex128),
-        observation_angles_deg=angles,
-        observation_points=obs_points,
-        observation_planes=config.observation.planes,
-        config=config,
-        mesh_info=mesh.info,
-        timings=timings,
-        solver_log=log,
-        surface_pressure_avg={t: np.array(v, dtype=np.complex128) for t, v in pavg.items()} or None,
-        surface_pressure_complex=np.stack(surf_rows, axis=0) if config.return_surface_pressure else None,
-        native_diagnostics=diag_rows,
-    )
+    out_results = []
+    for c, acc in zip(configs, rows):
+        log = acc["log"]
+        timings = {
+            "solve_s": sum(e["timing_s"] for e in log),
+            "assembly_s": sum(e["assembly_s"] for e in log),
+            "dense_solve_s": sum(e["dense_solve_s"] for e in log),
+            "directivity_s": sum(e["field_s"] for e in log),
+            "total_s": time.time() - t_total,
+        }
+        out_results.append(SolveResult(
+            frequencies_hz=np.array(done, dtype=np.float64),
+            pressure_complex=np.stack(acc["pressure"], axis=0),
+            directivity_db=np.stack(acc["spl"], axis=0),
+            impedance=np.array(acc["imp"], dtype=np.complex128),
+            observation_angles_deg=angles,
+            observation_points=obs_points,
+            observation_planes=config.observation.planes,
+            config=c,
+            mesh_info=mesh.info,
+            timings=timings,
+            solver_log=log,
+            surface_pressure_avg={t: np.array(v, dtype=np.complex128) for t, v in acc["pavg"].items()} or None,
+            surface_pressure_complex=np.stack(acc["surf"], axis=0) if config.return_surface_pressure else None,
+            native_diagnostics=acc["diag"],
+        ))
+    return out_results
 
 
 def run_sweep_multi_source(mesh: LoadedMesh, frequencies, frame: ObservationFrame, config: SolveConfig,
@@ -299,12 +339,13 @@ def run_sweep_multi_source(mesh: LoadedMesh, frequencies, frame: ObservationFram
     ``sweep.py:957-1301``), every source on one resident session, each result recording the surface
     averages of the sorted union of all source tags.
 
-    Without a streaming callback each source is one sweep (the factorisation is recomputed per
-    source).  With ``on_frequency_result`` the sources are interleaved per frequency and the callback
-    runs once per frequency with the first source's entry plus ``source_results`` (one entry per
-    source), as the reference's multi-RHS stream; returning False stops after that frequency and the
-    results hold the completed frequencies.  ``velocity_source_callback`` is rejected: each source
-    vector is fixed for the whole sweep.
+    Every frequency's matrix is assembled and factored once for all sources: one assembly pass fills the
+    matrix and each source's right-hand side, one LU, one solve per source (the reference's multi-RHS
+    ``cgesv``, ``main.swift:7887``).  With ``on_frequency_result`` the callback runs once per frequency with
+    the first source's entry plus ``source_results`` (one entry per source), as the reference's multi-RHS
+    stream; returning False stops after that frequency and the results hold the completed frequencies.
+    Robin walls and the coupled baffle solve one source at a time (same results, one factorisation per
+    source).  ``velocity_source_callback`` is rejected: each source vector is fixed for the whole sweep.
     """
     if not sources:
         raise ValueError("sources must contain at least one velocity dict")
@@ -314,8 +355,12 @@ def run_sweep_multi_source(mesh: LoadedMesh, frequencies, frame: ObservationFram
     buffers = build_geometry_buffers(mesh.grid, mesh.physical_tags, p1, dp0)
     all_tags = sorted({int(t) for s in sources for t in s})
     per_source = [replace(config, velocity_sources=dict(src)) for src in sources]
+    shared = not (config.impedance_sources or config.impedance_source_callback is not None
+                  or config.aperture_tag is not None)
     with NativeSession(buffers, symmetry_plane=config.native_symmetry_plane, aperture_tag=config.aperture_tag,
                        velocity_source_tags=all_tags, check_open_edges=config.native_check_open_edges) as session:
+        if shared:
+            return _run_sweep_sources(mesh, frequencies, frame, per_source, session=session, average_tags=all_tags)
         if config.on_frequency_result is None:
             return [run_sweep(mesh, frequencies, frame, c, session=session, average_tags=all_tags)
                     for c in per_source]

@@ -172,6 +172,23 @@ int hbem_assemble(hbem_session *s, int n_freq, const float *k_re, const float *k
                   int flags, void *stream);
 
 /*
+ * hbem_assemble for n_src right-hand sides (velocity sources) at once: one
+ * pass assembles A (shared) and b_s = SLP q_s for every source s (1 .. 8),
+ * the kernel samples shared by all of them.  Source s reads q at
+ * q + s * q_src_stride (then frequency f at + f * q_stride) and writes b at
+ * b + s * b_src_stride (+ f * b_stride).
+ * Replaces: the reference's extra-source right-hand-side dispatches and their
+ *   Duffy deltas (main.swift:6348-6368, 6467-6496), which evaluate the kernel
+ *   once per source.
+ */
+int hbem_assemble_multi(hbem_session *s, int n_freq, const float *k_re, const float *k_im, int n_src,
+                        const float *q_re, const float *q_im, long long q_stride, long long q_src_stride,
+                        const float *beta_re, const float *beta_im,
+                        float *a_re, float *a_im, long long lda, long long a_stride,
+                        float *b_re, float *b_im, long long b_stride, long long b_src_stride,
+                        int flags, void *stream);
+
+/*
  * Batched in-place complex LU with partial pivoting (LAPACK getrf semantics:
  * unit-lower L and U overwrite A; piv[i] = 0-based row swapped with row i).
  * Replaces: cgesv_/cgetrf_ in solveDenseAccelerateCgesvMulti
@@ -310,6 +327,29 @@ int hbem_solve_batch(hbem_session *s, int n_freq, const float *k_re, const float
                      float *surface_re, float *surface_im,
                      int *info, int *refine_iters, double *refine_resid, double *rcond,
                      float *timings_ms, void *stream);
+
+/*
+ * hbem_solve_batch for n_src velocity sources (1 .. 8) sharing each
+ * frequency's matrix: one assembly pass (hbem_assemble_multi), one LU per
+ * frequency, one solve (and refinement) per source.  Host arrays are
+ * source-major: q (n_src, n_freq, n_triangles); field (n_src, n_freq, n_obs);
+ * tag_avg (n_src, n_freq, n_tags, 2); surface (n_src, n_freq, n_dof);
+ * refine_iters, refine_resid (n_src, n_freq); info and rcond (n_freq,) as the
+ * matrix is shared.  n_src = 1 is hbem_solve_batch.
+ * Replaces: the multi-RHS batch op (extra_neumann_dp0 of
+ *   assemble_solve_evaluate_standard_neumann_batch,
+ *   hornlab_metal_bem/metal/native.py:760-779; cgesv with nrhs = sources,
+ *   main.swift:7887).
+ */
+int hbem_solve_batch_multi(hbem_session *s, int n_freq, int n_src, const float *k_re, const float *k_im,
+                           const float *q_re, const float *q_im,
+                           const float *obs_3xn, int n_obs,
+                           const int *tags, int n_tags,
+                           int precision, double refine_tol, int refine_max_iter,
+                           float *field_re, float *field_im, double *tag_avg,
+                           float *surface_re, float *surface_im,
+                           int *info, int *refine_iters, double *refine_resid, double *rcond,
+                           float *timings_ms, void *stream);
 
 /*
  * Coupled infinite baffle (interior BIE + Rayleigh half-space through the

@@ -7,6 +7,8 @@ the reference's known answers in test_oracle_pins.py); LU solutions within
 """
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -550,3 +552,34 @@ def test_wavefront_wait_that_runs_out_reports_state_error_and_nan():
     x = _host(xr, xi)[0]
     ref = np.linalg.solve(A[0].astype(np.complex128), b[0].astype(np.complex128))
     assert rel(x, ref) < 1e-4
+
+
+@pytest.mark.parametrize("name", ["ico2", "yzxz_quarter", "xy_half"])
+def test_assemble_multi_equals_one_pass_per_source(name):
+    """hbem_assemble_multi: one pass for 3 sources gives the matrix of a single-source pass and each source's
+    right-hand side as its own pass gives it (FP32 atomics reorder sums: 1e-6)."""
+    b = golden_buffers(name)
+    T, n = b.n_triangles, b.p1_dof_count
+    ks = [18.3, 91.6]
+    qs = np.stack([np.stack([_q(T, 10 * s + f) for f in range(2)]) for s in range(3)])   # (S, F, T)
+    qs[1, :, ::3] = 0.0   # sources with different supports
+    lib = load_library()
+    with _session(name) as s:
+        Ar, Ai, br1, bi1 = s.assemble(ks, qs[0])
+        refs = [_host(*s.assemble(ks, qs[k])[2:]) for k in range(3)]
+        qr = torch.tensor(np.ascontiguousarray(qs.real, np.float32), device="cuda")
+        qi = torch.tensor(np.ascontiguousarray(qs.imag, np.float32), device="cuda")
+        Mr, Mi = torch.empty_like(Ar), torch.empty_like(Ai)
+        Br = torch.empty((3, 2, n), dtype=torch.float32, device="cuda")
+        Bi = torch.empty_like(Br)
+        k_arr = np.asarray(ks, np.float32)
+        rc = lib.hbem_assemble_multi(s.handle, 2, k_arr.ctypes.data_as(ctypes.c_void_p), None, 3, _t_ptr(qr),
+                                     _t_ptr(qi), T, 2 * T, None, None, _t_ptr(Mr), _t_ptr(Mi), n, n * n, _t_ptr(Br),
+                                     _t_ptr(Bi), n, 2 * n, 7, None)
+        assert rc == 0, last_error(lib)
+        torch.cuda.synchronize()
+    A = _host(Ar, Ai)
+    assert rel(_host(Mr, Mi), A) < 1e-6
+    B = _host(Br, Bi)
+    for k in range(3):   # (a one-triangle mesh leaves the zeroed source with b = 0 exactly)
+        assert np.linalg.norm(B[k] - refs[k]) <= 1e-6 * max(np.linalg.norm(refs[k]), 1e-30)

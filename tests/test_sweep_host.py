@@ -104,20 +104,68 @@ def _fake_multi_source_env(monkeypatch):
     return sw, calls
 
 
-def _tiny_mesh_and_frame():
+class _FakeBatchSession:
+    """Host stand-in of a GPU session for the shared-factorisation multi-source sweep: each source's field is
+    the sum of its Neumann row (so sources are told apart) plus f / 1000; every call is logged."""
+
+    def __init__(self, calls):
+        self.calls = calls
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return False
+
+    def assemble_solve_evaluate_standard_neumann_batch(self, freqs, k_re, q, pts, *, extra_neumann_dp0=None,
+                                                       extra_impedance_source_tags=None, source_tags=None,
+                                                       impedance_source_tag=None, **kw):
+        from hornlab_metal_bem_b200.native import CaseResult, ExtraSourceResult
+
+        freqs = np.atleast_1d(freqs)
+        extra = np.zeros((0,) + np.shape(q)) if extra_neumann_dp0 is None else np.asarray(extra_neumann_dp0)
+        self.calls.append((tuple(freqs), extra.shape, tuple(source_tags), impedance_source_tag,
+                           tuple(extra_impedance_source_tags or ())))
+        n_obs = pts.shape[1]
+        out = []
+        for f, fr in enumerate(freqs):
+            def fields(row):
+                return (np.abs(row).sum() + fr / 1000.0) * np.ones(n_obs, np.complex64)
+            avg = {int(t): complex(t, fr) for t in source_tags}
+            out.append(CaseResult(
+                frequency_hz=float(fr), field=fields(q[f]), impedance=complex(np.abs(q[f]).sum(), fr),
+                surface_pressure_avg=avg, surface_pressure=None, assembly_s=0.05, dense_solve_s=0.03, field_s=0.02,
+                lapack_info=0, diagnostics={"f": float(fr), "dense_solve_rcond": 0.5},
+                extra_sources=tuple(ExtraSourceResult(source_index=s + 1, field=fields(extra[s, f]),
+                                                      impedance=complex(np.abs(extra[s, f]).sum(), fr),
+                                                      surface_pressure_avg=avg, surface_pressure=None,
+                                                      refine_iterations=1, refine_residual_rel=1e-8)
+                                    for s in range(extra.shape[0]))))
+        return out
+
+
+def _two_tag_mesh_and_frame():
     from hornlab_metal_bem_b200 import generators as G
+    from hornlab_metal_bem_b200.mesh import mesh_from_arrays
     from hornlab_metal_bem_b200.observation import infer_frame
 
     m = G.icosphere(1, 0.1)
-    return m, infer_frame(m.grid, m.physical_tags, source_tag=2)
+    v, f = m.grid.vertices.T.copy(), m.grid.elements.T.copy()
+    tags = np.where(v[f].mean(axis=1)[:, 2] < -0.05, 3, 2).astype(np.int32)
+    mesh = mesh_from_arrays(v, f, tags, physical_groups={2: "2", 3: "3"})
+    return mesh, infer_frame(mesh.grid, mesh.physical_tags, source_tag=2)
 
 
 def test_multi_source_stream_interleaves_sources_per_frequency(monkeypatch):
-    """With a streaming callback the sources are solved frequency by frequency and the callback sees one
-    entry per frequency carrying ``source_results`` (the reference's multi-RHS stream, sweep.py:1165-1210);
-    False stops the sweep and the results keep the completed frequencies."""
-    sw, calls = _fake_multi_source_env(monkeypatch)
-    mesh, frame = _tiny_mesh_and_frame()
+    """With a streaming callback the shared-factorisation sweep runs one frequency per native call with every
+    source as a right-hand side, and the callback sees one entry per frequency carrying ``source_results``
+    (the reference's multi-RHS stream, sweep.py:1165-1210); False stops the sweep and the results keep the
+    completed frequencies."""
+    import hornlab_metal_bem_b200.sweep as sw
+
+    calls = []
+    monkeypatch.setattr(sw, "NativeSession", lambda *a, **k: _FakeBatchSession(calls))
+    mesh, frame = _two_tag_mesh_and_frame()
     seen, progress = [], []
 
     def on_result(i, f, entry):
@@ -128,25 +176,43 @@ def test_multi_source_stream_interleaves_sources_per_frequency(monkeypatch):
                            progress_callback=lambda i, n, f: progress.append((i, n, f)))
     sources = [{2: 1.0}, {2: 0.5, 3: 1.0}]
     out = sw.run_sweep_multi_source(mesh, [500.0, 1000.0, 2000.0], frame, cfg, sources)
-    assert [(c[0], c[1]) for c in calls] == [((500.0,), {2: 1.0}), ((500.0,), {2: 0.5, 3: 1.0}),
-                                             ((1000.0,), {2: 1.0}), ((1000.0,), {2: 0.5, 3: 1.0})]
-    assert all(c[2] == (2, 3) and c[3] for c in calls)     # tag union; per-frequency calls stream nothing
+    T = mesh.grid.number_of_elements
+    assert [c[0] for c in calls] == [(500.0,), (1000.0,)]
+    assert all(c[1] == (1, 1, T) and c[2] == (2, 3) and c[3] == 2 and c[4] == (2,) for c in calls)
     assert [(i, f) for i, f, _ in seen] == [(0, 500.0), (1, 1000.0)]
     assert progress == [(0, 3, 500.0), (1, 3, 1000.0)]
     e = seen[1][2]
     assert len(e["source_results"]) == 2 and e["impedance"] == e["source_results"][0]["impedance"]
-    np.testing.assert_allclose(e["source_results"][1]["observation_pressure_complex"], (4.0 + 1.0) * np.ones((2, 3)))
-    assert e["observation_planes"] == ["horizontal", "vertical"] and len(e["observation_angles_deg"]) == 3
+    a0 = e["source_results"][0]["observation_pressure_complex"]
+    a1 = e["source_results"][1]["observation_pressure_complex"]
+    assert a0.shape == a1.shape and not np.allclose(a0, a1)
+    assert e["observation_planes"] == cfg.observation.planes
     assert [r.frequencies_hz.tolist() for r in out] == [[500.0, 1000.0]] * 2
-    assert out[1].pressure_complex.shape == (2, 2, 3) and set(out[1].surface_pressure_avg) == {2, 3}
-    assert out[0].config.velocity_sources == {2: 1.0} and out[0].timings["solve_s"] == pytest.approx(0.2)
-    assert [d["f"] for d in out[0].native_diagnostics] == [500.0, 1000.0]
+    assert set(out[1].surface_pressure_avg) == {2, 3}
+    assert out[0].config.velocity_sources == {2: 1.0} and out[1].config.velocity_sources == {2: 0.5, 3: 1.0}
+    assert out[1].native_diagnostics[0]["refine_iterations"] == 1 and out[1].native_diagnostics[0]["source_index"] == 1
 
 
-def test_multi_source_without_stream_is_one_sweep_per_source(monkeypatch):
-    sw, calls = _fake_multi_source_env(monkeypatch)
-    mesh, frame = _tiny_mesh_and_frame()
+def test_multi_source_without_stream_is_one_batch_for_all_sources(monkeypatch):
+    """Without streaming every frequency and every source go into one native call (one assembly pass and one
+    factorisation per frequency); each source gets its own result."""
+    import hornlab_metal_bem_b200.sweep as sw
+
+    calls = []
+    monkeypatch.setattr(sw, "NativeSession", lambda *a, **k: _FakeBatchSession(calls))
+    mesh, frame = _two_tag_mesh_and_frame()
     out = sw.run_sweep_multi_source(mesh, [500.0, 1000.0], frame, hb.native_config(), [{2: 1.0}, {3: 1.0}])
+    T = mesh.grid.number_of_elements
+    assert [(c[0], c[1], c[2]) for c in calls] == [((500.0, 1000.0), (1, 2, T), (2, 3))]
+    assert len(out) == 2 and [r.config.velocity_sources for r in out] == [{2: 1.0}, {3: 1.0}]
+    assert not np.allclose(out[0].pressure_complex, out[1].pressure_complex)
+
+
+def test_multi_source_with_robin_walls_is_one_sweep_per_source(monkeypatch):
+    sw, calls = _fake_multi_source_env(monkeypatch)
+    mesh, frame = _two_tag_mesh_and_frame()
+    cfg = hb.native_config(impedance_sources={3: 0.3 + 0.1j})
+    out = sw.run_sweep_multi_source(mesh, [500.0, 1000.0], frame, cfg, [{2: 1.0}, {3: 1.0}])
     assert [(c[0], c[1], c[2]) for c in calls] == [((500.0, 1000.0), {2: 1.0}, (2, 3)),
                                                    ((500.0, 1000.0), {3: 1.0}, (2, 3))]
     assert len(out) == 2
