@@ -423,19 +423,55 @@ int OGP(duffy_unique_triplets)(const og_geom *g, const int *pairs, int np) {
 }
 
 /* ---- Duffy rules (main.swift:2617-2699) ------------------------------- */
-/* One rule record per point: test (xi, eta), trial (xi, eta), weight. */
-static int duffy_rule(int kind, REAL *rec) {
-    double a1 = sqrt(3.0 / 7.0 - 2.0 / 7.0 * sqrt(6.0 / 5.0)) / 2.0;
-    double a2 = sqrt(3.0 / 7.0 + 2.0 / 7.0 * sqrt(6.0 / 5.0)) / 2.0;
-    double w1 = (18.0 + sqrt(30.0)) / 72.0, w2 = (18.0 - sqrt(30.0)) / 72.0;
-    REAL xs[4] = {(REAL)(0.5 - a2), (REAL)(0.5 - a1), (REAL)(0.5 + a1), (REAL)(0.5 + a2)};
-    REAL ws[4] = {(REAL)w2, (REAL)w1, (REAL)w1, (REAL)w2};
+#define MAX_GL 16   /* Gauss-Legendre points per Duffy coordinate (the reference uses 4) */
+
+/* m-point Gauss-Legendre nodes (ascending) and weights on [0, 1].  m = 4 uses
+   the closed form of the reference's rule; other orders Newton's iteration on
+   the Legendre recurrence P_k = ((2k - 1) x P_{k-1} - (k - 1) P_{k-2}) / k
+   from the Chebyshev initial guesses (Numerical Recipes' gauleg method). */
+static void gauss_legendre01(int m, double *x, double *w) {
+    if (m == 4) {
+        double a1 = sqrt(3.0 / 7.0 - 2.0 / 7.0 * sqrt(6.0 / 5.0)) / 2.0;
+        double a2 = sqrt(3.0 / 7.0 + 2.0 / 7.0 * sqrt(6.0 / 5.0)) / 2.0;
+        double w1 = (18.0 + sqrt(30.0)) / 72.0, w2 = (18.0 - sqrt(30.0)) / 72.0;
+        x[0] = 0.5 - a2; x[1] = 0.5 - a1; x[2] = 0.5 + a1; x[3] = 0.5 + a2;
+        w[0] = w2; w[1] = w1; w[2] = w1; w[3] = w2;
+        return;
+    }
+    for (int i = 0; i < (m + 1) / 2; ++i) {
+        double z = cos(3.14159265358979323846 * (i + 0.75) / (m + 0.5)), dp = 1.0;
+        for (int it = 0; it < 100; ++it) {
+            double p0 = 1.0, p1 = 0.0;
+            for (int k = 1; k <= m; ++k) {
+                double p2 = p1;
+                p1 = p0;
+                p0 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p2) / k;
+            }
+            dp = m * (z * p0 - p1) / (z * z - 1.0);
+            double dz = p0 / dp;
+            z -= dz;
+            if (fabs(dz) < 1e-16) break;
+        }
+        /* z is the i-th largest root on [-1, 1]: map to [0, 1] */
+        x[m - 1 - i] = 0.5 * (1.0 + z);
+        x[i] = 0.5 * (1.0 - z);
+        w[i] = w[m - 1 - i] = 1.0 / ((1.0 - z * z) * dp * dp);
+    }
+}
+
+/* One rule record per point: test (xi, eta), trial (xi, eta), weight; m
+   Gauss-Legendre points per Duffy coordinate ({6, 5, 2} m^4 points). */
+static int duffy_rule_m(int kind, int m, REAL *rec) {
+    double xd[MAX_GL], wd[MAX_GL];
+    gauss_legendre01(m, xd, wd);
+    REAL xs[MAX_GL], ws[MAX_GL];
+    for (int i = 0; i < m; ++i) { xs[i] = (REAL)xd[i]; ws[i] = (REAL)wd[i]; }
     int n = 0;
 #define PUT(TX, TY, SX, SY, W) do { REAL *o = rec + 5 * n++; o[0] = (TX) - (TY); o[1] = (TY); o[2] = (SX) - (SY); o[3] = (SY); o[4] = (W); } while (0)
-    for (int a = 0; a < 4; ++a)
-        for (int b = 0; b < 4; ++b)
-            for (int c = 0; c < 4; ++c)
-                for (int d = 0; d < 4; ++d) {
+    for (int a = 0; a < m; ++a)
+        for (int b = 0; b < m; ++b)
+            for (int c = 0; c < m; ++c)
+                for (int d = 0; d < m; ++d) {
                     REAL xi = xs[b], e1 = xs[a], e2 = xs[c], e3 = xs[d];
                     REAL e12 = e1 * e2, e123 = e12 * e3;
                     REAL base = ws[a] * ws[b] * ws[c] * ws[d];
@@ -464,7 +500,14 @@ static int duffy_rule(int kind, REAL *rec) {
     return n;
 }
 
+static int duffy_rule(int kind, REAL *rec) { return duffy_rule_m(kind, 4, rec); }
+static size_t rule_len(int m) { return (size_t)6 * m * m * m * m; }
+
 int OGP(duffy_rule_table)(int kind, REAL *rec) { return duffy_rule(kind, rec); }
+int OGP(duffy_rule_table_m)(int kind, int m, REAL *rec) {
+    if (m < 1 || m > MAX_GL) return -1;
+    return duffy_rule_m(kind, m, rec);
+}
 
 static inline REAL refx(int l) { return l == 1 ? 1 : 0; }
 static inline REAL refy(int l) { return l == 2 ? 1 : 0; }
@@ -578,13 +621,21 @@ static void pair_blocks(const og_geom *g, int test, int trial, int tm, int sm, i
     }
 }
 
-/* Public pair-block probe: out[0..5] = slp re/im, out[6..23] = dlp re/im. */
+/* Public pair-block probe: out[0..5] = slp re/im, out[6..23] = dlp re/im.
+   mode 1 uses the Duffy rule with `level` Gauss-Legendre points per
+   coordinate (0: the reference's 4). */
 int OGP(pair_blocks)(const og_geom *g, int test, int trial, int tm, int sm, int mode, int kind,
                      const int *locals, int level, REAL kr, REAL ki, REAL *out) {
     static const int zero[4] = {0, 1, 0, 1};
     REAL *rule = NULL;
     int nrule = 0;
-    if (mode == 1) { rule = malloc(1536 * 5 * sizeof(REAL)); nrule = duffy_rule(kind, rule); }
+    if (mode == 1) {
+        int m = level > 0 ? level : 4;
+        if (m > MAX_GL) return -1;
+        rule = malloc(rule_len(m) * 5 * sizeof(REAL));
+        nrule = duffy_rule_m(kind, m, rule);
+        level = 0;
+    }
     cplx slp[3], dl[9];
     pair_blocks(g, test, trial, tm, sm, mode, kind, locals ? locals : zero, level, rule, nrule, kr, ki, slp, dl);
     for (int i = 0; i < 3; ++i) { out[2 * i] = slp[i].re; out[2 * i + 1] = slp[i].im; }
@@ -597,16 +648,35 @@ int OGP(pair_blocks)(const og_geom *g, int test, int trial, int tm, int sm, int 
    every singular pair into A and b at weight 1, Robin coupling included.  The
    per-entry sums are accumulated in double before the final add, as in the
    reference.  Returns the number of unique (row, col) triplets. */
+static int duffy_correct_m(const og_geom *g, REAL kr, REAL ki, const float *q_re, const float *q_im,
+                           const float *beta_re, const float *beta_im,
+                           REAL *A_re, REAL *A_im, REAL *b_re, REAL *b_im, int m);
+
 int OGP(duffy_correct)(const og_geom *g, REAL kr, REAL ki, const float *q_re, const float *q_im,
                        const float *beta_re, const float *beta_im,
                        REAL *A_re, REAL *A_im, REAL *b_re, REAL *b_im) {
+    return duffy_correct_m(g, kr, ki, q_re, q_im, beta_re, beta_im, A_re, A_im, b_re, b_im, 4);
+}
+
+/* The same correction with an m-point Gauss-Legendre Duffy rule per
+   coordinate: the convergence reference for the reference's 4-point rule. */
+int OGP(duffy_correct_m)(const og_geom *g, REAL kr, REAL ki, const float *q_re, const float *q_im,
+                         const float *beta_re, const float *beta_im,
+                         REAL *A_re, REAL *A_im, REAL *b_re, REAL *b_im, int m) {
+    if (m < 1 || m > MAX_GL) return -1;
+    return duffy_correct_m(g, kr, ki, q_re, q_im, beta_re, beta_im, A_re, A_im, b_re, b_im, m);
+}
+
+static int duffy_correct_m(const og_geom *g, REAL kr, REAL ki, const float *q_re, const float *q_im,
+                           const float *beta_re, const float *beta_im,
+                           REAL *A_re, REAL *A_im, REAL *b_re, REAL *b_im, int m) {
     int counts[3];
     int np = OGP(duffy_pairs)(g, NULL, 0, counts);
     int *pairs = malloc((size_t)(np ? np : 1) * PAIR_INTS * sizeof(int));
     OGP(duffy_pairs)(g, pairs, np, counts);
     REAL *rules[3];
     int nr[3];
-    for (int k = 0; k < 3; ++k) { rules[k] = malloc(1536 * 5 * sizeof(REAL)); nr[k] = duffy_rule(k + 1, rules[k]); }
+    for (int k = 0; k < 3; ++k) { rules[k] = malloc(rule_len(m) * 5 * sizeof(REAL)); nr[k] = duffy_rule_m(k + 1, m, rules[k]); }
     int n = g->n_dof;
     double *acc_re = calloc((size_t)n * n, sizeof(double));
     double *acc_im = calloc((size_t)n * n, sizeof(double));

@@ -113,24 +113,26 @@ class Oracle:
         )
         return Are + 1j * Aim, bre + 1j * bim
 
-    def duffy_correct(self, A, b, k: float, q=None, k_imag: float = 0.0, beta=None) -> int:
-        """Add the Duffy singular corrections to ``A``/``b`` in place; returns unique triplets."""
+    def duffy_correct(self, A, b, k: float, q=None, k_imag: float = 0.0, beta=None, order: int = 4) -> int:
+        """Add the Duffy singular corrections to ``A``/``b`` in place; returns unique triplets.  ``order``:
+        Gauss-Legendre points per Duffy coordinate (the reference's rule has 4)."""
         Are = np.ascontiguousarray(A.real, dtype=self.real); Aim = np.ascontiguousarray(A.imag, dtype=self.real)
         bre = np.ascontiguousarray(b.real, dtype=self.real); bim = np.ascontiguousarray(b.imag, dtype=self.real)
         qre, qim = self._split(q, self.T)
         brr, bri = self._split(beta, self.T)
-        u = self._fn("duffy_correct")(
-            ctypes.byref(self.geom), self._ct(k), self._ct(k_imag), _ptr(qre), _ptr(qim), _ptr(brr), _ptr(bri),
-            _ptr(Are), _ptr(Aim), _ptr(bre), _ptr(bim),
-        )
+        args = (ctypes.byref(self.geom), self._ct(k), self._ct(k_imag), _ptr(qre), _ptr(qim), _ptr(brr), _ptr(bri),
+                _ptr(Are), _ptr(Aim), _ptr(bre), _ptr(bim))
+        u = (self._fn("duffy_correct")(*args) if order == 4
+             else self._fn("duffy_correct_m")(*args, ctypes.c_int(int(order))))
         A[...] = Are + 1j * Aim
         b[...] = bre + 1j * bim
         return int(u)
 
-    def corrected(self, k: float, q=None, k_imag: float = 0.0, beta=None):
-        """Regular 6x6 assembly plus Duffy corrections: the reference's 'corrected' mode."""
+    def corrected(self, k: float, q=None, k_imag: float = 0.0, beta=None, duffy_order: int = 4):
+        """Regular 6x6 assembly plus Duffy corrections: the reference's 'corrected' mode (``duffy_order`` 4);
+        other orders give the convergence study of its singular quadrature."""
         A, b = self.regular(k, q, k_imag, beta)
-        self.duffy_correct(A, b, k, q, k_imag, beta)
+        self.duffy_correct(A, b, k, q, k_imag, beta, order=duffy_order)
         return A, b
 
     def duffy_pairs(self):

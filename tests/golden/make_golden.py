@@ -75,6 +75,28 @@ def _buffers_dict(prefix, b):
     }
 
 
+def _near_pairs(buffers, count: int) -> list[tuple[int, int]]:
+    """Deterministic near, non-touching (test, trial) pairs: scanning test triangles in order, the nearest
+    triangle that shares no vertex, kept when its centroid distance is under 1.5 x the larger diameter."""
+    v = np.asarray(buffers.vertices_3xn_f32, dtype=np.float64)
+    tri = np.asarray(buffers.triangles_3xm_i32)
+    pts = v[:, tri]                                  # (3 coords, 3 vertices, T)
+    cen = pts.mean(axis=1)
+    diam = np.max([np.linalg.norm(pts[:, i] - pts[:, j], axis=0) for i in range(3) for j in range(3)], axis=0)
+    out = []
+    for t in range(tri.shape[1]):
+        ratio = np.linalg.norm(cen - cen[:, [t]], axis=0) / np.maximum(diam, diam[t])
+        for s_ in np.argsort(ratio):
+            if s_ == t or set(tri[:, t]) & set(tri[:, s_]):
+                continue
+            if ratio[s_] < 1.5:
+                out.append((int(t), int(s_)))
+            break
+        if len(out) == count:
+            break
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", required=True, help="root of the hornlab-metal-bem checkout")
@@ -213,8 +235,18 @@ def main() -> None:
         if len(set(tris[0]) & set(tris[t])) == 0 and len(picks) < 3 and t > 5:
             picks.append(t)
     cases += [("ico2", 0, t, 18.3) for t in picks]
+    # near but not touching pairs: for each triangle in turn, the closest triangle sharing no vertex
+    # (centroid distance under 1.5 times the larger diameter), on the sphere and on the quarter horn
+    # (whose folded lip brings walls close together)
+    built = {"ico2": icob}
+    for name, count in (("ico2", 2), ("horn_quarter", 4)):
+        if name not in built:
+            m = meshes[name]
+            p1m, dp0m = make_pure_function_spaces(m.grid)
+            built[name] = R.geometry.build_metal_geometry_buffers(m.grid, m.physical_tags, p1m, dp0m)
+        cases += [(name, t, s_, 18.3) for t, s_ in _near_pairs(built[name], count)]
     for i, (name, test, trial, k) in enumerate(cases):
-        b = near if name == "near" else icob
+        b = near if name == "near" else built[name]
         ref = R.tmod._reference_pair_blocks(b, test, trial, k, 4)
         pb[f"{i}__slp"] = ref.slp
         pb[f"{i}__dlp"] = ref.dlp
