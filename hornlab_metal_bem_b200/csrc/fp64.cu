@@ -377,6 +377,202 @@ __global__ void __launch_bounds__(256) k64_field(const __grid_constant__ Field64
 }
 
 // ---------------------------------------------------------------------------
+// Coupled infinite baffle in FP64 (main.swift:1178-1290 projections, their
+// Duffy deltas 1011-1087, Rayleigh field 1397-1444)
+// ---------------------------------------------------------------------------
+struct Ap64Args {
+    Geo64 g;
+    const int *ap;        // (m) aperture triangles, ascending ids
+    const int *ap_local;  // (T) aperture index or -1
+    int m;
+    double *out_re, *out_im;
+    long long stride;
+    double kr[kMaxF64], ki[kMaxF64];
+};
+
+// G summed over the images of y (the 1 / (4 pi) included), seen from x
+__device__ __forceinline__ void green_images(const Geo64 &g, double yx, double yy, double yz, double x0, double x1,
+                                             double x2, double kr, double ki, double &gre, double &gim) {
+    double dre = 0, dim = 0;
+    green_dlp(yx - x0, yy - x1, yz - x2, 0.0, 0.0, 0.0, kr, ki, gre, gim, dre, dim);
+    for (int m = 0; m < g.n_masks; ++m) {
+        double ix = yx, iy = yy, iz = yz;
+        mirror3(ix, iy, iz, g.masks[m]);
+        green_dlp(ix - x0, iy - x1, iz - x2, 0.0, 0.0, 0.0, kr, ki, gre, gim, dre, dim);
+    }
+}
+
+// S_ia regular part: thread per (test triangle, aperture face); SLP rows of
+// the test's three dofs against the face (with images), 2^planes row weight.
+__global__ void __launch_bounds__(128) k64_ap_slp(const __grid_constant__ Ap64Args a) {
+    const Geo64 &g = a.g;
+    const int test = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.y, f = blockIdx.z;
+    if (test >= g.T) return;
+    const int trial = a.ap[t];
+    const double kr = a.kr[f], ki = a.ki[f];
+    const double jac = (2.0 * g.nrm[4 * test + 3]) * (2.0 * g.nrm[4 * trial + 3]);
+    double sr[3] = {0, 0, 0}, si[3] = {0, 0, 0};
+    for (int qa = 0; qa < 6; ++qa) {
+        double x0, x1, x2;
+        point_on(g.tv, test, c64_qx[qa], c64_qy[qa], x0, x1, x2);
+        const double tb[3] = {1.0 - c64_qx[qa] - c64_qy[qa], c64_qx[qa], c64_qy[qa]};
+        for (int qb = 0; qb < 6; ++qb) {
+            double yx, yy, yz;
+            point_on(g.tv, trial, c64_qx[qb], c64_qy[qb], yx, yy, yz);
+            double gre = 0, gim = 0;
+            green_images(g, yx, yy, yz, x0, x1, x2, kr, ki, gre, gim);
+            const double w = c64_qw[qa] * c64_qw[qb] * jac;
+            for (int i = 0; i < 3; ++i) {
+                sr[i] += gre * (tb[i] * w);
+                si[i] += gim * (tb[i] * w);
+            }
+        }
+    }
+    for (int i = 0; i < 3; ++i) {
+        const size_t o = (size_t)f * a.stride + (size_t)g.l2g[test * 3 + i] * a.m + t;
+        atomicAdd(a.out_re + o, sr[i] * g.rw);
+        atomicAdd(a.out_im + o, si[i] * g.rw);
+    }
+}
+
+// S_aa regular part: thread per (test face r, trial face c) of the aperture,
+// the SLP summed over the test's basis functions, divided by its area, at the
+// real field wavenumber.
+__global__ void __launch_bounds__(128) k64_ap_avg(const __grid_constant__ Ap64Args a) {
+    const Geo64 &g = a.g;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y, f = blockIdx.z;
+    if (c >= a.m) return;
+    const int test = a.ap[r], trial = a.ap[c];
+    const double kr = a.kr[f];
+    const double jac = (2.0 * g.nrm[4 * test + 3]) * (2.0 * g.nrm[4 * trial + 3]);
+    double sr = 0, si = 0;
+    for (int qa = 0; qa < 6; ++qa) {
+        double x0, x1, x2;
+        point_on(g.tv, test, c64_qx[qa], c64_qy[qa], x0, x1, x2);
+        for (int qb = 0; qb < 6; ++qb) {
+            double yx, yy, yz;
+            point_on(g.tv, trial, c64_qx[qb], c64_qy[qb], yx, yy, yz);
+            double gre = 0, gim = 0;
+            green_images(g, yx, yy, yz, x0, x1, x2, kr, 0.0, gre, gim);
+            const double w = c64_qw[qa] * c64_qw[qb] * jac;
+            sr += gre * w;
+            si += gim * w;
+        }
+    }
+    const double inv = 1.0 / fmax(g.nrm[4 * test + 3], 1e-300);
+    const size_t o = (size_t)f * a.stride + (size_t)r * a.m + c;
+    a.out_re[o] += sr * inv;
+    a.out_im[o] += si * inv;
+}
+
+// Duffy SLP deltas of the projections.  mode 1: S_ia gets the delta of every
+// pair whose trial is an aperture face (at the pair's weight); mode 2: S_aa
+// gets the delta summed over the test basis, divided by the test area, for
+// pairs of two aperture faces with an unmirrored test (once each).
+__global__ void __launch_bounds__(128) k64_ap_duffy(const __grid_constant__ Ap64Args a, const DuffyPair *pairs,
+                                                    int n_pairs, const double *rule_all, int mode, int off1, int cnt1,
+                                                    int off2, int cnt2, int off3, int cnt3) {
+    const int pi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pi >= n_pairs) return;
+    const Geo64 &g = a.g;
+    const int f = blockIdx.y;
+    const DuffyPair pr = pairs[pi];
+    const int ls = a.ap_local[pr.trial];
+    if (ls < 0) return;
+    if (mode == 2 && (pr.test_mask != 0 || a.ap_local[pr.test] < 0)) return;
+    const double kr = a.kr[f], ki = mode == 2 ? 0.0 : a.ki[f];
+    double nx = 0, ny = 0, nz = 0;   // the SLP needs no normal
+    const double jac = (2.0 * g.nrm[4 * pr.test + 3]) * (2.0 * g.nrm[4 * pr.trial + 3]);
+    double rs_re[3] = {0, 0, 0}, rs_im[3] = {0, 0, 0}, ss_re[3] = {0, 0, 0}, ss_im[3] = {0, 0, 0};
+    double d_re[9], d_im[9];
+    for (int a6 = 0; a6 < 6; ++a6)
+        for (int b6 = 0; b6 < 6; ++b6)
+            pair_point(g, pr.test, pr.trial, pr.test_mask, pr.trial_mask, c64_qx[a6], c64_qy[a6], c64_qx[b6],
+                       c64_qy[b6], c64_qw[a6] * c64_qw[b6] * jac, nx, ny, nz, kr, ki, rs_re, rs_im, d_re, d_im);
+    const int kind = pr.kind;
+    const int off = kind == 1 ? off1 : (kind == 2 ? off2 : off3), cnt = kind == 1 ? cnt1 : (kind == 2 ? cnt2 : cnt3);
+    const double *rule = rule_all + 5 * (size_t)off;
+    for (int q = 0; q < cnt; ++q) {
+        const double *r = rule + 5 * q;
+        double tx, ty, sx, sy;
+        remap(r[0], r[1], kind, pr.tl1, pr.tl2, tx, ty);
+        remap(r[2], r[3], kind, pr.sl1, pr.sl2, sx, sy);
+        pair_point(g, pr.test, pr.trial, pr.test_mask, pr.trial_mask, tx, ty, sx, sy, r[4] * jac, nx, ny, nz, kr, ki,
+                   ss_re, ss_im, d_re, d_im);
+    }
+    if (mode == 1) {
+        const double wgt = (double)pr.weight;
+        for (int i = 0; i < 3; ++i) {
+            const size_t o = (size_t)f * a.stride + (size_t)g.l2g[pr.test * 3 + i] * a.m + ls;
+            atomicAdd(a.out_re + o, (ss_re[i] - rs_re[i]) * wgt);
+            atomicAdd(a.out_im + o, (ss_im[i] - rs_im[i]) * wgt);
+        }
+    } else {
+        double dr = 0, di = 0;
+        for (int i = 0; i < 3; ++i) {
+            dr += ss_re[i] - rs_re[i];
+            di += ss_im[i] - rs_im[i];
+        }
+        const double inv = 1.0 / fmax(g.nrm[4 * pr.test + 3], 1e-300);
+        const size_t o = (size_t)f * a.stride + (size_t)a.ap_local[pr.test] * a.m + ls;
+        atomicAdd(a.out_re + o, dr * inv);
+        atomicAdd(a.out_im + o, di * inv);
+    }
+}
+
+// Rayleigh field p(x) = -2 sum_t q_t sum_a w 2|t| sum_images G(y, x') with
+// x' = (x, y, max(z, 0)) for z >= -1e-5, zero below.  CTA per (point, wavenumber).
+__global__ void __launch_bounds__(256) k64_rayleigh(const __grid_constant__ Ap64Args a, const double *qa_re,
+                                                    const double *qa_im, long long qa_stride, const float *obs,
+                                                    int n_obs, long long out_stride) {
+    const Geo64 &g = a.g;
+    const int o = blockIdx.x, f = blockIdx.y;
+    const double kr = a.kr[f];
+    const double ox = obs[o], oy = obs[n_obs + o], oz = obs[2 * n_obs + o];
+    double acc_re = 0.0, acc_im = 0.0;
+    if (oz >= -1e-5) {
+        const double ez = oz < 0.0 ? 0.0 : oz;
+        for (int t = threadIdx.x; t < a.m; t += blockDim.x) {
+            const double q_re = qa_re[(size_t)f * qa_stride + t], q_im = qa_im[(size_t)f * qa_stride + t];
+            if (q_re == 0.0 && q_im == 0.0) continue;
+            const int tri = a.ap[t];
+            const double jac = 2.0 * g.nrm[4 * tri + 3];
+            for (int qa = 0; qa < 6; ++qa) {
+                double yx, yy, yz;
+                point_on(g.tv, tri, c64_qx[qa], c64_qy[qa], yx, yy, yz);
+                double gre = 0, gim = 0;
+                green_images(g, yx, yy, yz, ox, oy, ez, kr, 0.0, gre, gim);
+                const double w = c64_qw[qa] * jac;
+                acc_re += (gre * q_re - gim * q_im) * w;
+                acc_im += (gre * q_im + gim * q_re) * w;
+            }
+        }
+    }
+    __shared__ double s_re[8], s_im[8];
+    for (int off = 16; off > 0; off >>= 1) {
+        acc_re += __shfl_xor_sync(0xffffffffu, acc_re, off);
+        acc_im += __shfl_xor_sync(0xffffffffu, acc_im, off);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        s_re[warp] = acc_re;
+        s_im[warp] = acc_im;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = 0, i = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            r += s_re[w];
+            i += s_im[w];
+        }
+        a.out_re[(size_t)f * out_stride + o] = -2.0 * r;
+        a.out_im[(size_t)f * out_stride + o] = -2.0 * i;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // complex128 LU (planar, row-major, lda) and solve
 // ---------------------------------------------------------------------------
 constexpr int kNB64 = 32;            // panel width
@@ -1102,4 +1298,103 @@ extern "C" int hbem_lu_solve_f64(int n, int nrhs, int batch, const double *lu_re
         return fail(HBEM_ERR_ARG, "hbem_lu_solve_f64: lda/a_stride/piv_stride/ldb/b_stride too small");
     return lu_solve_f64(n, nrhs, batch, lu_re, lu_im, lda, a_stride, piv, piv_stride, b_re, b_im, ldb, b_stride,
                         reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" int hbem_aperture_assemble_f64(hbem_session *h, int n_freq, const double *k_re, const double *k_im,
+                                          const double *kf_re, double *sia_re, double *sia_im, double *saa_re,
+                                          double *saa_im, void *stream) {
+    Session *s = reinterpret_cast<Session *>(h);
+    if (!s) return fail(HBEM_ERR_ARG, "hbem_aperture_assemble_f64: NULL session");
+    if (s->m_ap <= 0) return fail(HBEM_ERR_STATE, "hbem_aperture_assemble_f64: no aperture set on the session");
+    if (n_freq <= 0) return HBEM_OK;
+    if (!k_re || !kf_re || !sia_re || !sia_im || !saa_re || !saa_im)
+        return fail(HBEM_ERR_ARG, "hbem_aperture_assemble_f64: NULL pointer");
+    for (int f = 0; f < n_freq; ++f)
+        if (!std::isfinite(k_re[f]) || !std::isfinite(kf_re[f]) || (k_im && !std::isfinite(k_im[f])))
+            return fail(HBEM_ERR_ARG, "hbem_aperture_assemble_f64: non-finite wavenumber");
+    HBEM_CUDA(cudaSetDevice(s->device));
+    int rc = ensure_geo64(*s);
+    if (rc != HBEM_OK) return rc;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const int n = s->n_dof, m = s->m_ap, T = s->n_triangles;
+    const size_t sia_stride = (size_t)n * m, saa_stride = (size_t)m * m;
+    HBEM_CUDA(cudaMemsetAsync(sia_re, 0, sizeof(double) * sia_stride * n_freq, st));
+    HBEM_CUDA(cudaMemsetAsync(sia_im, 0, sizeof(double) * sia_stride * n_freq, st));
+    HBEM_CUDA(cudaMemsetAsync(saa_re, 0, sizeof(double) * saa_stride * n_freq, st));
+    HBEM_CUDA(cudaMemsetAsync(saa_im, 0, sizeof(double) * saa_stride * n_freq, st));
+    const double *rule = s->d_geo64 + (size_t)T * 13;
+    for (int f0 = 0; f0 < n_freq; f0 += kMaxF64) {
+        const int nf = std::min(kMaxF64, n_freq - f0);
+        Ap64Args a{};
+        a.g = geo64(*s);
+        a.ap = s->d_ap_tris;
+        a.ap_local = s->d_ap_local;
+        a.m = m;
+        // S_ia at the (possibly complex) assembly wavenumber
+        for (int f = 0; f < nf; ++f) {
+            a.kr[f] = k_re[f0 + f];
+            a.ki[f] = k_im ? k_im[f0 + f] : 0.0;
+        }
+        a.out_re = sia_re + (size_t)f0 * sia_stride;
+        a.out_im = sia_im + (size_t)f0 * sia_stride;
+        a.stride = (long long)sia_stride;
+        k64_ap_slp<<<dim3((T + 127) / 128, m, nf), 128, 0, st>>>(a);
+        HBEM_LAUNCH_CHECK("k64_ap_slp");
+        if (s->n_pairs > 0) {
+            k64_ap_duffy<<<dim3((s->n_pairs + 127) / 128, nf), 128, 0, st>>>(
+                a, s->d_pairs, s->n_pairs, rule, 1, s->rule_off[0], s->rule_cnt[0], s->rule_off[1], s->rule_cnt[1],
+                s->rule_off[2], s->rule_cnt[2]);
+            HBEM_LAUNCH_CHECK("k64_ap_duffy");
+        }
+        // S_aa at the real field wavenumber
+        for (int f = 0; f < nf; ++f) {
+            a.kr[f] = kf_re[f0 + f];
+            a.ki[f] = 0.0;
+        }
+        a.out_re = saa_re + (size_t)f0 * saa_stride;
+        a.out_im = saa_im + (size_t)f0 * saa_stride;
+        a.stride = (long long)saa_stride;
+        k64_ap_avg<<<dim3((m + 127) / 128, m, nf), 128, 0, st>>>(a);
+        HBEM_LAUNCH_CHECK("k64_ap_avg");
+        if (s->n_pairs > 0) {
+            k64_ap_duffy<<<dim3((s->n_pairs + 127) / 128, nf), 128, 0, st>>>(
+                a, s->d_pairs, s->n_pairs, rule, 2, s->rule_off[0], s->rule_cnt[0], s->rule_off[1], s->rule_cnt[1],
+                s->rule_off[2], s->rule_cnt[2]);
+            HBEM_LAUNCH_CHECK("k64_ap_duffy");
+        }
+    }
+    return HBEM_OK;
+}
+
+extern "C" int hbem_coupled_ib_field_f64(hbem_session *h, int n_freq, const double *kf_re, const double *qa_re,
+                                         const double *qa_im, const float *obs_3xn, int n_obs, double *out_re,
+                                         double *out_im, void *stream) {
+    Session *s = reinterpret_cast<Session *>(h);
+    if (!s) return fail(HBEM_ERR_ARG, "hbem_coupled_ib_field_f64: NULL session");
+    if (s->m_ap <= 0) return fail(HBEM_ERR_STATE, "hbem_coupled_ib_field_f64: no aperture set on the session");
+    if (n_freq <= 0 || n_obs <= 0) return HBEM_OK;
+    if (!kf_re || !qa_re || !qa_im || !obs_3xn || !out_re || !out_im)
+        return fail(HBEM_ERR_ARG, "hbem_coupled_ib_field_f64: NULL pointer");
+    if (n_obs > 65535) return fail(HBEM_ERR_ARG, "hbem_coupled_ib_field_f64: at most 65535 points per call");
+    for (int f = 0; f < n_freq; ++f)
+        if (!std::isfinite(kf_re[f])) return fail(HBEM_ERR_ARG, "hbem_coupled_ib_field_f64: non-finite wavenumber");
+    HBEM_CUDA(cudaSetDevice(s->device));
+    int rc = ensure_geo64(*s);
+    if (rc != HBEM_OK) return rc;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    for (int f0 = 0; f0 < n_freq; f0 += kMaxF64) {
+        const int nf = std::min(kMaxF64, n_freq - f0);
+        Ap64Args a{};
+        a.g = geo64(*s);
+        a.ap = s->d_ap_tris;
+        a.ap_local = s->d_ap_local;
+        a.m = s->m_ap;
+        for (int f = 0; f < nf; ++f) a.kr[f] = kf_re[f0 + f];
+        a.out_re = out_re + (size_t)f0 * n_obs;
+        a.out_im = out_im + (size_t)f0 * n_obs;
+        k64_rayleigh<<<dim3(n_obs, nf), 256, 0, st>>>(a, qa_re + (size_t)f0 * s->m_ap, qa_im + (size_t)f0 * s->m_ap,
+                                                      s->m_ap, obs_3xn, n_obs, n_obs);
+        HBEM_LAUNCH_CHECK("k64_rayleigh");
+    }
+    return HBEM_OK;
 }

@@ -98,6 +98,8 @@ _SIGNATURES = {
     "hbem_field_f64": ([_vp, _c_int, _vp, _vp, _vp, _c_ll, _vp, _vp, _c_ll, _vp, _c_int, _vp, _vp, _c_ll, _vp],
                        _c_int),
     "hbem_solve_status": ([_vp], _c_int),
+    "hbem_aperture_assemble_f64": ([_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _c_int),
+    "hbem_coupled_ib_field_f64": ([_vp, _c_int, _vp, _vp, _vp, _vp, _c_int, _vp, _vp, _vp], _c_int),
     "hbem_assemble_multi": ([_vp, _c_int, _vp, _vp, _c_int, _vp, _vp, _c_ll, _c_ll, _vp, _vp, _vp, _vp, _c_ll, _c_ll,
                              _vp, _vp, _c_ll, _c_ll, _c_int, _vp], _c_int),
     "hbem_solve_batch_multi": ([_vp, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp, _c_int, _vp, _c_int, _c_int, _c_d,
@@ -404,6 +406,66 @@ class NativeSession:
             p_h = p.cpu().numpy()
             qz = qz + (1j * k - ki) * np.asarray(beta).reshape(1, -1) * p_h[:, l2g].mean(axis=2)
         return p, self.field_f64(k_re, p, qz, obs_3xn)
+
+    def coupled_reference_solve_f64(self, k_re, q, obs_3xn, *, k_imag=None, field_k=None):
+        """The coupled infinite baffle on the FP64 path, one frequency at a time: FP64 corrected assembly of A
+        and b, FP64 aperture projections S_ia (at k) and S_aa (at the real field wavenumber), the augmented
+        system [[A, -S_ia], [P_avg, -2 S_aa]] [p; q_a] = [b; 0] (``main.swift:7504-7595``) factored by the
+        complex128 LU, and the FP64 Rayleigh field of q_a.  Returns complex128 numpy arrays p (F, n),
+        q_a (F, m) and field (F, N)."""
+        torch = require_cuda()
+        if self.m_aperture <= 0:
+            raise ValueError("session has no aperture_tag")
+        k_re = np.atleast_1d(np.asarray(k_re, dtype=np.float64))
+        F = k_re.shape[0]
+        k_im = None if k_imag is None else np.atleast_1d(np.asarray(k_imag, dtype=np.float64))
+        kf = k_re if field_k is None else np.atleast_1d(np.asarray(field_k, dtype=np.float64))
+        n, m = self.n_dof, self.m_aperture
+        N = n + m
+        dev = torch.device("cuda", self.device)
+        q = np.asarray(q).reshape(F, self.n_triangles)
+        obs = torch.as_tensor(np.ascontiguousarray(obs_3xn, dtype=np.float32), device=dev).contiguous()
+        n_obs = int(obs.shape[1])
+        l2g = torch.as_tensor(np.asarray(self.buffers.p1_local2global_i32, dtype=np.int64), device=dev)
+        ap = np.flatnonzero(np.asarray(self.buffers.physical_tags_i32) == int(self.aperture_tag))
+        rows_p = torch.arange(m, device=dev).repeat_interleave(3)
+        cols_p = l2g[torch.as_tensor(ap, device=dev)].reshape(-1)
+        out_p, out_qa, out_f = [], [], []
+        for f in range(F):
+            kr1 = np.ascontiguousarray(k_re[f:f + 1])
+            ki1 = None if k_im is None else np.ascontiguousarray(k_im[f:f + 1])
+            kf1 = np.ascontiguousarray(kf[f:f + 1])
+            Ar, Ai, br, bi = self.assemble_f64(kr1, q[f:f + 1], k_imag=ki1)
+            sia_r = torch.empty((1, n, m), dtype=torch.float64, device=dev)
+            sia_i, saa_r, saa_i = torch.empty_like(sia_r), torch.empty((1, m, m), dtype=torch.float64,
+                                                                       device=dev), None
+            saa_i = torch.empty_like(saa_r)
+            check(self.lib.hbem_aperture_assemble_f64(self.handle, 1, _np_ptr(kr1), _np_ptr(ki1), _np_ptr(kf1),
+                                                      _t_ptr(sia_r), _t_ptr(sia_i), _t_ptr(saa_r), _t_ptr(saa_i),
+                                                      _stream_ptr()), "hbem_aperture_assemble_f64", self.lib)
+            Kr = torch.zeros((1, N, N), dtype=torch.float64, device=dev)
+            Ki = torch.zeros_like(Kr)
+            Kr[0, :n, :n], Ki[0, :n, :n] = Ar[0], Ai[0]
+            del Ar, Ai
+            Kr[0, :n, n:], Ki[0, :n, n:] = -sia_r[0], -sia_i[0]
+            Kr[0].index_put_((n + rows_p, cols_p), torch.full_like(rows_p, 1.0 / 3.0, dtype=torch.float64),
+                             accumulate=True)
+            Kr[0, n:, n:], Ki[0, n:, n:] = -2.0 * saa_r[0], -2.0 * saa_i[0]
+            rr = torch.zeros((1, N), dtype=torch.float64, device=dev)
+            ri = torch.zeros_like(rr)
+            rr[0, :n], ri[0, :n] = br[0], bi[0]
+            xr, xi = lu_solve_f64(Kr, Ki, rr, ri)
+            del Kr, Ki
+            qa_r, qa_i = xr[:, n:].contiguous(), xi[:, n:].contiguous()
+            fr = torch.empty((1, n_obs), dtype=torch.float64, device=dev)
+            fi = torch.empty_like(fr)
+            check(self.lib.hbem_coupled_ib_field_f64(self.handle, 1, _np_ptr(kf1), _t_ptr(qa_r), _t_ptr(qa_i),
+                                                     _t_ptr(obs), n_obs, _t_ptr(fr), _t_ptr(fi), _stream_ptr()),
+                  "hbem_coupled_ib_field_f64", self.lib)
+            out_p.append(torch.complex(xr[0, :n], xi[0, :n]).cpu().numpy())
+            out_qa.append(torch.complex(qa_r[0], qa_i[0]).cpu().numpy())
+            out_f.append(torch.complex(fr[0], fi[0]).cpu().numpy())
+        return np.array(out_p), np.array(out_qa), np.array(out_f)
 
     @staticmethod
     def _split_device(z, shape, dev):

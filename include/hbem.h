@@ -458,6 +458,22 @@ int hbem_lu_factor_f64(int n, int batch, double *a_re, double *a_im, long long l
 int hbem_lu_solve_f64(int n, int nrhs, int batch, const double *lu_re, const double *lu_im, long long lda,
                       long long a_stride, const int *piv, long long piv_stride,
                       double *b_re, double *b_im, long long ldb, long long b_stride, int trans, void *stream);
+/*
+ * The coupled infinite baffle on the FP64 path: hbem_aperture_assemble_f64
+ * writes S_ia (n_freq, n, m) and S_aa (n_freq, m, m) as hbem_aperture_assemble
+ * does (double buffers, k and kf on the host; zeroed first), and
+ * hbem_coupled_ib_field_f64 the Rayleigh field -2 sum G(y, x') q_a from given
+ * aperture data q_a (n_freq, m) (x' = (x, y, max(z, 0)) for z >= -1e-5, 0
+ * below; n_obs <= 65535).  With hbem_assemble_f64 and hbem_lu_*_f64 they
+ * solve the augmented system [[A, -S_ia], [P_avg, -2 S_aa]] [p; q_a] = [b; 0]
+ * in FP64 (main.swift:7504-7595), the error reference of the coupled sweeps.
+ */
+int hbem_aperture_assemble_f64(hbem_session *s, int n_freq, const double *k_re, const double *k_im,
+                               const double *kf_re, double *sia_re, double *sia_im, double *saa_re,
+                               double *saa_im, void *stream);
+int hbem_coupled_ib_field_f64(hbem_session *s, int n_freq, const double *kf_re, const double *qa_re,
+                              const double *qa_im, const float *obs_3xn, int n_obs, double *out_re,
+                              double *out_im, void *stream);
 
 #ifdef __cplusplus
 }

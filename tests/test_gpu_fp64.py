@@ -202,3 +202,41 @@ def test_dense_solve_dtype_float64_end_to_end():
         assert 0.0 < d["dense_solve_rcond"] < 1.0
         assert d["dense_solve_rcond"] == pytest.approx(plain.native_diagnostics[f]["dense_solve_rcond"], rel=0.05)
     assert np.max(np.abs(f64.directivity_db - plain.directivity_db)) < 1e-3
+
+
+@pytest.mark.parametrize("name,sym,plane", [("ib_box", 0, None), ("ib_quarter_box", 3, "yz+xz")])
+def test_f64_coupled_baffle_matches_fp64_oracle(name, sym, plane):
+    """The coupled infinite baffle on the FP64 path (FP64 projections with their Duffy deltas, augmented
+    complex128 solve, FP64 Rayleigh field) against the oracle's FP64 restatement of the reference's augmented
+    solve (main.swift:7504-7595) and Rayleigh field (1397-1444)."""
+    import ctypes
+
+    buf = golden_buffers(name)
+    obs = np.array([[0.0, 0.3, -0.2, 0.1, 0.0], [0.0, 0.1, 0.4, -0.3, 0.0], [2.0, 1.5, 0.8, 0.02, -0.5]],
+                   np.float32)
+    k = 2 * np.pi * 1500.0 / 343.0
+    q = np.zeros((1, buf.n_triangles), np.complex64)
+    q[0, buf.physical_tags_i32 == 2] = 1j * 1.2041 * 2 * np.pi * 1500.0
+    o = Oracle(buf, sym, "f64")
+    ap = o.aperture_triangles(7)
+    A, b = o.corrected(k, q[0])
+    p_ref, qa_ref, S_ia, S_aa = o.coupled_ib_solve(A, b, ap, k, k)
+    f_ref = o.rayleigh(ap, k, qa_ref, obs)
+    with NativeSession(buf, symmetry_plane=plane, aperture_tag=7, velocity_source_tags=[2],
+                       check_open_edges=False) as s:
+        n, m = s.n_dof, s.m_aperture
+        sr = torch.empty((1, n, m), dtype=torch.float64, device="cuda")
+        si = torch.empty_like(sr)
+        ar = torch.empty((1, m, m), dtype=torch.float64, device="cuda")
+        ai = torch.empty_like(ar)
+        kk = np.array([k]), np.array([k])
+        lib = load_library()
+        assert lib.hbem_aperture_assemble_f64(s.handle, 1, kk[0].ctypes.data_as(ctypes.c_void_p), None,
+                                              kk[1].ctypes.data_as(ctypes.c_void_p), _t_ptr(sr), _t_ptr(si),
+                                              _t_ptr(ar), _t_ptr(ai), None) == 0
+        assert rel(_c(sr, si)[0], S_ia) < 1e-11
+        assert rel(_c(ar, ai)[0], S_aa) < 1e-11
+        p, qa, fld = s.coupled_reference_solve_f64([k], q, obs)
+    assert rel(p[0], p_ref) < 1e-9
+    assert rel(qa[0], qa_ref) < 1e-9
+    assert rel(fld[0], f_ref) < 1e-9
