@@ -117,6 +117,10 @@ struct Session {
     // sweep workspace (grown on demand)
     void *ws = nullptr;
     size_t ws_bytes = 0;
+    // second stream of the sweep (the condition estimate beside the solves)
+    // and its fork / join events, created on first use
+    cudaStream_t aux = nullptr;
+    cudaEvent_t aux_fork = nullptr, aux_join = nullptr;
     void *pinned = nullptr;
     size_t pinned_bytes = 0;
 

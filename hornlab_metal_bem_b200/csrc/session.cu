@@ -277,6 +277,9 @@ void free_session(Session *s) {
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (s->pinned) cudaFreeHost(s->pinned);
+    if (s->aux_fork) cudaEventDestroy(s->aux_fork);
+    if (s->aux_join) cudaEventDestroy(s->aux_join);
+    if (s->aux) cudaStreamDestroy(s->aux);
     cudaSetDevice(prev);
     delete s;
 }

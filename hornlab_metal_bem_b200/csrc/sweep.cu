@@ -138,6 +138,15 @@ static int solve_batch_impl(hbem_session *h, int n_freq, int n_src, const float 
     const Layout L = layout(*s, chunk, n_src, n_obs, n_tags, do_refine, fp64);
     int rc = ensure_ws(*s, L.total);
     if (rc != HBEM_OK) return rc;
+    if (rcond && !s->aux) {
+        // the condition estimate runs on a second stream beside the solves,
+        // refinement and field (it only reads the factors)
+        int lo = 0, hi = 0;
+        HBEM_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        HBEM_CUDA(cudaStreamCreateWithPriority(&s->aux, cudaStreamNonBlocking, lo));
+        HBEM_CUDA(cudaEventCreateWithFlags(&s->aux_fork, cudaEventDisableTiming));
+        HBEM_CUDA(cudaEventCreateWithFlags(&s->aux_join, cudaEventDisableTiming));
+    }
     char *ws = static_cast<char *>(s->ws);
     float *dq = reinterpret_cast<float *>(ws + L.q);
     float *da = reinterpret_cast<float *>(ws + L.a);
@@ -226,16 +235,22 @@ static int solve_batch_impl(hbem_session *h, int n_freq, int n_src, const float 
                 rc = narrow_f64(1, (int)n, n_src * nf, x64r, x64i, (long long)n, (long long)n, xr, xi, (long long)n,
                                 (long long)n, st);
             if (rc == HBEM_OK && rcond) {
-                // condition estimate from the FP64 factors narrowed to FP32
+                // condition estimate from the FP64 factors narrowed to FP32, on the second stream
                 rc = narrow_f64((int)n, (int)n, nf, a64r, a64i, (long long)n, nn, ar, ai, (long long)n, nn, st);
-                if (rc == HBEM_OK) rc = lu_rcond((int)n, nf, ar, ai, (long long)n, nn, danorm, drcond, st);
+                if (rc == HBEM_OK && ok(cudaEventRecord(s->aux_fork, st), "fork") &&
+                    ok(cudaStreamWaitEvent(s->aux, s->aux_fork, 0), "fork"))
+                    rc = lu_rcond((int)n, nf, ar, ai, (long long)n, nn, danorm, drcond, s->aux);
+                if (rc == HBEM_OK) ok(cudaEventRecord(s->aux_join, s->aux), "join");
             }
             if (rc != HBEM_OK) break;
         } else {
             rc = lu_factor((int)n, nf, ar, ai, (long long)n, nn, dpiv, (long long)n, dinfo, precision, st);
             if (rc != HBEM_OK) break;
             if (rcond) {
-                rc = lu_rcond((int)n, nf, ar, ai, (long long)n, nn, danorm, drcond, st);
+                // condition estimate on the second stream, beside the solves (both only read the factors)
+                if (ok(cudaEventRecord(s->aux_fork, st), "fork") && ok(cudaStreamWaitEvent(s->aux, s->aux_fork, 0), "fork"))
+                    rc = lu_rcond((int)n, nf, ar, ai, (long long)n, nn, danorm, drcond, s->aux);
+                if (rc == HBEM_OK) ok(cudaEventRecord(s->aux_join, s->aux), "join");
                 if (rc != HBEM_OK) break;
             }
             for (int sv = 0; sv < n_src && rc == HBEM_OK; ++sv)
@@ -262,6 +277,8 @@ static int solve_batch_impl(hbem_session *h, int n_freq, int n_src, const float 
                               fi, (long long)n_obs, st);
         if (rc == HBEM_OK && n_tags > 0) rc = launch_tag_avg(*s, n_src * nf, xr, xi, (long long)n, dwant, n_tags, dtag, st);
         if (rc != HBEM_OK) break;
+        // join the condition estimate before the next chunk reuses the factors' buffer
+        if (rcond) ok(cudaStreamWaitEvent(st, s->aux_join, 0), "join");
         ok(cudaEventRecord(ev[3], st), "cudaEventRecord");
         for (int sv = 0; sv < n_src; ++sv) {
             const size_t hf = (size_t)sv * n_freq + f0;   // first host case of this source in the chunk
@@ -315,6 +332,7 @@ static int solve_batch_impl(hbem_session *h, int n_freq, int n_src, const float 
         }
     } else {
         cudaStreamSynchronize(st);
+        if (s->aux) cudaStreamSynchronize(s->aux);
     }
     for (auto &e : ev)
         if (e) cudaEventDestroy(e);

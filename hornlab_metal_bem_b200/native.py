@@ -1138,6 +1138,8 @@ class ResidentSweep:
         self.precision = HBEM_PREC_MIXED if precision == "mixed" else HBEM_PREC_PLAIN
         self.rcond = torch.empty(F, dtype=torch.float64, device=dev) if rcond else None
         self.anorm = torch.empty(F, dtype=torch.float32, device=dev) if rcond else None
+        # the condition estimate runs on a second stream beside the solves, refinement and field
+        self.aux = torch.cuda.Stream(device=dev, priority=0) if rcond else None
         mode = "mixed" if precision == "mixed" else "plain"
         self.refine_tol = float(refine_tolerance)
         self.refine_max = max(1, int(refine_max_iterations)) if mode == "mixed" else int(refine_max_iterations)
@@ -1168,8 +1170,12 @@ class ResidentSweep:
         check(self.lib.hbem_lu_factor(n, self.F, _t_ptr(self.A_re), _t_ptr(self.A_im), n, n * n, _t_ptr(self.piv), n,
                                       _t_ptr(self.info), self.precision, st), "hbem_lu_factor", self.lib)
         if self.rcond is not None:
+            import torch
+
+            main = torch.cuda.current_stream() if stream is None else stream
+            self.aux.wait_stream(main)
             check(self.lib.hbem_lu_rcond(n, self.F, _t_ptr(self.A_re), _t_ptr(self.A_im), n, n * n, _t_ptr(self.anorm),
-                                         _t_ptr(self.rcond), st), "hbem_lu_rcond", self.lib)
+                                         _t_ptr(self.rcond), _stream_ptr(self.aux)), "hbem_lu_rcond", self.lib)
         check(self.lib.hbem_lu_solve(n, 1, self.F, _t_ptr(self.A_re), _t_ptr(self.A_im), n, n * n, _t_ptr(self.piv), n,
                                      _t_ptr(self.x_re), _t_ptr(self.x_im), 1, n, HBEM_TRANS_N, st), "hbem_lu_solve",
               self.lib)
@@ -1190,6 +1196,11 @@ class ResidentSweep:
             check(self.lib.hbem_reduce_tag_avg(
                 self.s.handle, self.F, _t_ptr(self.x_re), _t_ptr(self.x_im), self.n, _np_ptr(self.tags),
                 self.tags.shape[0], _t_ptr(self.tag_out), st), "hbem_reduce_tag_avg", self.lib)
+        if self.aux is not None:
+            # join the condition estimate before the next sweep overwrites the factors
+            import torch
+
+            (torch.cuda.current_stream() if stream is None else stream).wait_stream(self.aux)
 
     def run(self, stream=None):
         self.assemble(stream)

@@ -243,6 +243,10 @@ int hbem_refine(int n, int batch, const float *a_re, const float *a_im, long lon
  *   by L U and (L U)^H; 0 when the estimate or the norm is 0.
  * Replaces: matrixOneNorm / estimateReciprocalCondition (main.swift:463-503,
  *   called per case at 7886 and 7898).
+ * Both are asynchronous on `stream` (no host synchronisation: the estimate
+ * runs a fixed six rounds, matrices that finish earlier drop out on the
+ * device), so the estimate can run on a second stream beside the solves; a
+ * timed-out triangular-solve wait inside it is reported by hbem_solve_status.
  */
 int hbem_matrix_norm1(int n, int batch, const float *a_re, const float *a_im, long long lda, long long a_stride,
                       float *anorm, void *stream);
