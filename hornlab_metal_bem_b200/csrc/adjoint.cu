@@ -642,6 +642,9 @@ void fill_freqs(Freqs &fq, const float *k_re, int f0, int nf) {
 int check_adjoint_session(const Session *s, const char *who) {
     if (!s) return fail(HBEM_ERR_ARG, std::string(who) + ": NULL session");
     if (s->sym != 0) return fail(HBEM_ERR_ARG, std::string(who) + ": shape gradients need a session without symmetry planes");
+    if (s->n_near > 0)
+        return fail(HBEM_ERR_STATE, std::string(who) + ": shape gradients do not include the near-field subdivision; "
+                                                       "turn it off (level 0)");
     return HBEM_OK;
 }
 

@@ -1325,6 +1325,10 @@ extern "C" int hbem_assemble_multi(hbem_session *h, int n_freq, const float *k_r
     if (rc == HBEM_OK && (flags & HBEM_ASM_DUFFY))
         rc = launch_duffy(*s, n_freq, k_re, k_im, q_re, q_im, q_stride, beta_re, beta_im, a_re, a_im, lda, a_stride,
                           b_re, b_im, b_stride, st, nullptr, n_src, q_src_stride, b_src_stride);
+    // near-field subdivision (when the session has it on) with the singular corrections
+    if (rc == HBEM_OK && (flags & HBEM_ASM_DUFFY) && s->n_near > 0)
+        rc = launch_near(*s, n_freq, k_re, k_im, n_src, q_re, q_im, q_stride, q_src_stride, beta_re, beta_im, a_re,
+                         a_im, lda, a_stride, b_re, b_im, b_stride, b_src_stride, st);
     return rc;
 }
 

@@ -22,7 +22,7 @@ PKG = HERE.parent
 REPO = PKG.parent
 OUT = PKG / "libhbem.so"
 BUILD = REPO / "_build" / "hbem"
-SOURCES = ["session.cu", "assemble.cu", "field.cu", "lu.cu", "gemm.cu", "sweep.cu", "aperture.cu", "adjoint.cu", "fp64.cu"]
+SOURCES = ["session.cu", "assemble.cu", "field.cu", "lu.cu", "gemm.cu", "sweep.cu", "aperture.cu", "adjoint.cu", "fp64.cu", "near.cu"]
 HEADERS = ["hbem_internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",

@@ -114,6 +114,14 @@ struct Session {
     int *d_ap_tris = nullptr;
     int *d_ap_local = nullptr;
 
+    // near-field subdivision (the reference's optional near quadrature): near,
+    // non-touching image pairs and the subdivided 6-point rule of the level
+    int near_level = 0;
+    double near_threshold = 0.0;
+    int n_near = 0, n_sub = 0;
+    int4 *d_near = nullptr;         // test, trial, test mask, trial mask
+    float4 *d_subrule = nullptr;    // (xi, eta, weight, 0) of the subdivided rule
+
     // sweep workspace (grown on demand)
     void *ws = nullptr;
     size_t ws_bytes = 0;
@@ -129,6 +137,11 @@ struct Session {
 
 // ---- pieces implemented in separate translation units ---------------------
 int build_duffy_pairs(Session &s, std::vector<DuffyPair> &pairs);
+int image_shared_vertices(const Session &s, int test, int trial, int test_mask, int trial_mask);
+int launch_near(Session &s, int n_freq, const float *k_re, const float *k_im, int n_src, const float *q_re,
+                const float *q_im, long long q_stride, long long q_src_stride, const float *beta_re,
+                const float *beta_im, float *a_re, float *a_im, long long lda, long long a_stride, float *b_re,
+                float *b_im, long long b_stride, long long b_src_stride, cudaStream_t st);
 void duffy_rule_table(int kind, std::vector<float> &rec);  // 5 floats per point
 void duffy_rule_table64(int kind, std::vector<double> &rec);  // the same rule in double
 

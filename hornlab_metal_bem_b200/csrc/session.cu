@@ -239,6 +239,13 @@ int build_duffy_pairs(Session &s, std::vector<DuffyPair> &pairs) {
     return HBEM_OK;
 }
 
+// Vertices an image pair of triangles shares (matched on the 1e-6 lattice of
+// the mirrored coordinates, as for the singular pairs).
+int image_shared_vertices(const Session &s, int test, int trial, int test_mask, int trial_mask) {
+    int loc[4];
+    return shared(s, test, trial, test_mask, trial_mask, loc);
+}
+
 }  // namespace hbem
 
 using namespace hbem;
@@ -273,7 +280,7 @@ void free_session(Session *s) {
     void *ptrs[] = {s->d_qp, s->d_nrm, s->d_tri, s->d_test_slot, s->d_trial_slot, s->d_row_off, s->d_rows,
                     s->d_col_off, s->d_cols, s->d_verts, s->d_tris, s->d_l2g, s->d_tags, s->d_areas,
                     s->d_normals, s->d_fqp, s->d_fnrm, s->d_pairs, s->d_rule, s->d_rule_w, s->d_status, s->ws,
-                    s->d_ap_tris, s->d_ap_local, s->d_sing_bits, s->d_geo64};
+                    s->d_ap_tris, s->d_ap_local, s->d_sing_bits, s->d_geo64, s->d_near, s->d_subrule};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (s->pinned) cudaFreeHost(s->pinned);
@@ -572,6 +579,7 @@ extern "C" int hbem_session_query(const hbem_session *h, int key, long long *val
         case HBEM_Q_UNIQUE_TRIPLETS: *value = s->n_unique_triplets; break;
         case HBEM_Q_SYMMETRY: *value = s->sym; break;
         case HBEM_Q_APERTURE_TRIANGLES: *value = s->m_ap; break;
+        case HBEM_Q_NEAR_PAIRS: *value = s->n_near; break;
         case HBEM_Q_KERNEL_LAUNCHES: *value = s->launches; break;
         case HBEM_Q_REGULAR_EVALS: *value = T * T * 36 * M; break;
         case HBEM_Q_DUFFY_EVALS: {

@@ -13,6 +13,7 @@ visible, construction raises ``BackendUnavailable``.
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 import time
 from dataclasses import dataclass, field
@@ -44,7 +45,7 @@ AUGMENTED_MIN_APERTURE = 512
 QUERY_KEYS = {
     "n_dof": 0, "n_triangles": 1, "n_pairs": 2, "coincident": 3, "edge": 4, "vertex": 5,
     "image_pairs": 6, "unique_triplets": 7, "symmetry": 8, "kernel_launches": 9,
-    "regular_evals": 10, "duffy_evals": 11, "aperture_triangles": 12,
+    "regular_evals": 10, "duffy_evals": 11, "aperture_triangles": 12, "near_pairs": 13,
 }
 
 
@@ -98,6 +99,7 @@ _SIGNATURES = {
     "hbem_field_f64": ([_vp, _c_int, _vp, _vp, _vp, _c_ll, _vp, _vp, _c_ll, _vp, _c_int, _vp, _vp, _c_ll, _vp],
                        _c_int),
     "hbem_solve_status": ([_vp], _c_int),
+    "hbem_session_set_near_quadrature": ([_vp, _c_int, _c_d], _c_int),
     "hbem_aperture_assemble_f64": ([_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _c_int),
     "hbem_coupled_ib_field_f64": ([_vp, _c_int, _vp, _vp, _vp, _vp, _c_int, _vp, _vp, _vp], _c_int),
     "hbem_assemble_multi": ([_vp, _c_int, _vp, _vp, _c_int, _vp, _vp, _c_ll, _c_ll, _vp, _vp, _vp, _vp, _c_ll, _c_ll,
@@ -169,6 +171,39 @@ def solve_mode(precision: str, dense_solve_dtype: str = "float32") -> str:
 
 
 SOLVE_IMPL = {"plain": "hbem_blocked_lu_fp32", "mixed": "hbem_blocked_lu_bf16x3", "fp64": "hbem_blocked_lu_fp64"}
+
+
+NEAR_QUADRATURE_ENV = "HORNLAB_METAL_BEM_NATIVE_NEAR_QUADRATURE"
+
+
+def parse_near_quadrature(raw) -> tuple[int, float] | None:
+    """The reference's near-quadrature setting (``main.swift:5024-5054``): unset, "" or "0" = off; "1" / "2" =
+    that subdivision level at threshold 1.5; "<level>:<threshold>" with level 1 or 2 and a finite positive
+    threshold.  A (level, threshold) tuple passes through."""
+    if raw is None:
+        return None
+    if isinstance(raw, tuple):
+        level, threshold = int(raw[0]), float(raw[1])
+        if level == 0:
+            return None
+        if level in (1, 2) and math.isfinite(threshold) and threshold > 0.0:
+            return level, threshold
+    else:
+        text = str(raw).strip()
+        if text in ("", "0"):
+            return None
+        if text in ("1", "2"):
+            return int(text), 1.5
+        parts = text.split(":")
+        if len(parts) == 2 and parts[0] in ("1", "2"):
+            try:
+                threshold = float(parts[1])
+            except ValueError:
+                threshold = float("nan")
+            if math.isfinite(threshold) and threshold > 0.0:
+                return int(parts[0]), threshold
+    raise ValueError(f"{NEAR_QUADRATURE_ENV} must be unset, '0', '1', '2', or '<level>:<positive threshold>' "
+                     "with level 1...2")
 
 
 def _refines(mode: str, max_iter) -> bool:
@@ -243,7 +278,7 @@ class NativeSession:
 
     def __init__(self, geometry_buffers: GeometryBuffers, *, symmetry_plane: str | None = None,
                  aperture_tag: int | None = None, velocity_source_tags=None, check_open_edges: bool = True,
-                 device: int | None = None):
+                 device: int | None = None, near_quadrature=None):
         torch = require_cuda()
         self.lib = load_library()
         self.buffers = geometry_buffers
@@ -281,13 +316,24 @@ class NativeSession:
             check(self.lib.hbem_session_set_aperture(self.handle, int(self.aperture_tag)),
                   "hbem_session_set_aperture", self.lib)
             self.m_aperture = self.query("aperture_triangles")
+        # near-field subdivision: argument, else the reference's environment variable
+        self.near_quadrature = None
+        near = parse_near_quadrature(near_quadrature if near_quadrature is not None
+                                     else os.environ.get(NEAR_QUADRATURE_ENV))
+        if near is not None:
+            t1 = time.perf_counter()
+            check(self.lib.hbem_session_set_near_quadrature(self.handle, near[0], near[1]),
+                  "hbem_session_set_near_quadrature", self.lib)
+            self.near_quadrature = {"level": near[0], "threshold": near[1],
+                                    "pair_count": self.query("near_pairs"), "seconds": time.perf_counter() - t1}
 
     # -- lifecycle -------------------------------------------------------------
     @classmethod
     def create_session(cls, *, geometry_buffers, symmetry_plane=None, aperture_tag=None, velocity_source_tags=None,
-                       check_open_edges=True, device=None, **_ignored) -> "NativeSession":
+                       check_open_edges=True, device=None, near_quadrature=None, **_ignored) -> "NativeSession":
         return cls(geometry_buffers, symmetry_plane=symmetry_plane, aperture_tag=aperture_tag,
-                   velocity_source_tags=velocity_source_tags, check_open_edges=check_open_edges, device=device)
+                   velocity_source_tags=velocity_source_tags, check_open_edges=check_open_edges, device=device,
+                   near_quadrature=near_quadrature)
 
     def close(self) -> None:
         if getattr(self, "handle", None) is not None and self.handle.value:
@@ -666,6 +712,8 @@ class NativeSession:
             if S > 1:
                 diag["multi_source"] = True
                 diag["sources_sharing_factorisation"] = S
+            if self.near_quadrature is not None:
+                diag["near_quadrature"] = dict(self.near_quadrature)
             extras = tuple(
                 ExtraSourceResult(
                     source_index=s_,

@@ -68,6 +68,7 @@ extern "C" {
 #define HBEM_Q_REGULAR_EVALS 10    /* kernel evaluations per frequency, regular part */
 #define HBEM_Q_DUFFY_EVALS 11      /* kernel evaluations per frequency, Duffy part */
 #define HBEM_Q_APERTURE_TRIANGLES 12  /* m: aperture triangles of the coupled baffle (0 when unset) */
+#define HBEM_Q_NEAR_PAIRS 13       /* near, non-touching image pairs of the near-field option (0 when off) */
 
 typedef struct hbem_session hbem_session;
 
@@ -146,6 +147,22 @@ int hbem_session_create(const float *vertices_3xv, int n_vertices,
                         const int *p1_local2global_tx3, int n_dof,
                         const int *tags, const float *areas, const float *normals_3xt,
                         int sym_code, int device, hbem_session **out);
+
+/*
+ * Near-field subdivision of the regular quadrature: for every pair of (image)
+ * triangles that share no vertex and whose centroids are closer than
+ * threshold x the longer of their longest edges, the assembly adds (the
+ * 6-point rule on each of the 4^level sub-triangles of both - the 6 x 6 rule)
+ * to A and the right-hand sides, with the Robin coupling, on every following
+ * hbem_assemble / hbem_assemble_multi / hbem_solve_batch call that includes
+ * HBEM_ASM_DUFFY.  level 0 turns it off; level 1 or 2; threshold > 0 (the
+ * reference's default 1.5).  The pair count is HBEM_Q_NEAR_PAIRS.
+ * Replaces: HORNLAB_METAL_BEM_NATIVE_NEAR_QUADRATURE = "<level>[:<threshold>]"
+ *   (main.swift:5024-5054 parsing, 2471-2556 pair list, 2840-2912 subdivided
+ *   blocks, 3072-3202 correction).  The FP64 path and the shape gradients do
+ *   not include it.
+ */
+int hbem_session_set_near_quadrature(hbem_session *s, int level, double threshold);
 
 /* Release a session and its device memory. */
 int hbem_session_destroy(hbem_session *s);

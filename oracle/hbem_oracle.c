@@ -722,6 +722,124 @@ static int duffy_correct_m(const og_geom *g, REAL kr, REAL ki, const float *q_re
     return uniq;
 }
 
+/* ---- near-field subdivision (main.swift:2410-2560, 3072-3202) ---------- */
+/* Near, non-touching (test image, trial image) pairs: centroid distance under
+   threshold x the longer of the two longest edges (bounding boxes pre-filter),
+   no shared vertex; each gets (subdivided block at `level` - regular 6 x 6
+   block) added at weight 1 (the image-pair enumeration carries the symmetry
+   factor), Robin coupling included.  Returns the number of near pairs. */
+typedef struct { double c[3], lo[3], hi[3], edge; } near_metric;
+
+static void near_metrics(const og_geom *g, int tri, int mask, near_metric *m) {
+    REAL p[3][3];
+    for (int l = 0; l < 3; ++l) {
+        vertex_point(g, tv(g, tri, l), p[l]);
+        mirror(p[l], mask);
+    }
+    double e2 = 0;
+    for (int c = 0; c < 3; ++c) {
+        m->c[c] = ((double)p[0][c] + (double)p[1][c] + (double)p[2][c]) / 3.0;
+        m->lo[c] = fmin(p[0][c], fmin(p[1][c], p[2][c]));
+        m->hi[c] = fmax(p[0][c], fmax(p[1][c], p[2][c]));
+    }
+    for (int a = 0; a < 3; ++a) {
+        int b = (a + 1) % 3;
+        double d2 = 0;
+        for (int c = 0; c < 3; ++c) d2 += ((double)p[a][c] - p[b][c]) * ((double)p[a][c] - p[b][c]);
+        if (d2 > e2) e2 = d2;
+    }
+    m->edge = sqrt(e2);
+}
+
+static double axis_gap(double alo, double ahi, double blo, double bhi) {
+    if (ahi < blo) return blo - ahi;
+    if (bhi < alo) return alo - bhi;
+    return 0.0;
+}
+
+int OGP(near_pairs)(const og_geom *g, double threshold, int *out, int cap) {
+    int T = g->n_triangles;
+    int masks[4] = {0, 0, 0, 0};
+    int nm = 1 + mirror_masks(g->sym, masks + 1);
+    near_metric *mt = malloc((size_t)T * nm * sizeof(near_metric));
+    for (int mi = 0; mi < nm; ++mi)
+        for (int t = 0; t < T; ++t) near_metrics(g, t, masks[mi], &mt[(size_t)mi * T + t]);
+    int np = 0;
+    for (int trial = 0; trial < T; ++trial)
+        for (int si = 0; si < nm; ++si) {
+            const near_metric *sm = &mt[(size_t)si * T + trial];
+            for (int ti = 0; ti < nm; ++ti)
+                for (int test = 0; test < T; ++test) {
+                    const near_metric *tm = &mt[(size_t)ti * T + test];
+                    double cut = threshold * fmax(tm->edge, sm->edge), cut2 = cut * cut;
+                    double gx = axis_gap(tm->lo[0], tm->hi[0], sm->lo[0], sm->hi[0]);
+                    double gy = axis_gap(tm->lo[1], tm->hi[1], sm->lo[1], sm->hi[1]);
+                    double gz = axis_gap(tm->lo[2], tm->hi[2], sm->lo[2], sm->hi[2]);
+                    if (gx * gx + gy * gy + gz * gz > cut2) continue;
+                    double dx = tm->c[0] - sm->c[0], dy = tm->c[1] - sm->c[1], dz = tm->c[2] - sm->c[2];
+                    if (dx * dx + dy * dy + dz * dz >= cut2) continue;
+                    int sh[4];
+                    if (shared_locals(g, test, trial, masks[ti], masks[si], sh) > 0) continue;
+                    if (out && np < cap) {
+                        int *r = out + (size_t)np * 4;
+                        r[0] = test; r[1] = trial; r[2] = masks[ti]; r[3] = masks[si];
+                    }
+                    ++np;
+                }
+        }
+    free(mt);
+    return np;
+}
+
+int OGP(near_correct)(const og_geom *g, REAL kr, REAL ki, const float *q_re, const float *q_im,
+                      const float *beta_re, const float *beta_im, REAL *A_re, REAL *A_im, REAL *b_re, REAL *b_im,
+                      int level, double threshold) {
+    int np = OGP(near_pairs)(g, threshold, NULL, 0);
+    int *pairs = malloc((size_t)(np ? np : 1) * 4 * sizeof(int));
+    OGP(near_pairs)(g, threshold, pairs, np);
+    int n = g->n_dof;
+    double *acc_re = calloc((size_t)n * n, sizeof(double));
+    double *acc_im = calloc((size_t)n * n, sizeof(double));
+    cplx iK = {-ki, kr};
+#pragma omp parallel for schedule(dynamic, 8)
+    for (int p = 0; p < np; ++p) {
+        const int *r = pairs + (size_t)p * 4;
+        int test = r[0], trial = r[1], tm = r[2], sm = r[3];
+        cplx rs[3], rd[9], ss[3], sd[9];
+        pair_blocks(g, test, trial, tm, sm, 0, 0, NULL, 0, NULL, 0, kr, ki, rs, rd);
+        pair_blocks(g, test, trial, tm, sm, 2, 0, NULL, level, NULL, 0, kr, ki, ss, sd);
+        cplx qv = {q_re ? (REAL)q_re[trial] : 0, q_im ? (REAL)q_im[trial] : 0};
+        cplx beta = {beta_re ? (REAL)beta_re[trial] : 0, beta_im ? (REAL)beta_im[trial] : 0};
+        int robin = beta.re != 0 || beta.im != 0;
+        cplx rc = cmul(iK, beta);
+        for (int i = 0; i < 3; ++i) {
+            int row = dof(g, test, i);
+            cplx ds = csub(ss[i], rs[i]);
+            cplx rv = cmul(ds, qv);
+            atomic_add(&b_re[row], rv.re);
+            atomic_add(&b_im[row], rv.im);
+            for (int j = 0; j < 3; ++j) {
+                int col = dof(g, trial, j);
+                cplx d = csub(sd[i * 3 + j], rd[i * 3 + j]);
+                if (robin) d = csub(d, cscale(cmul(ds, rc), (REAL)(1.0 / 3.0)));
+                double *pr = &acc_re[(size_t)row * n + col], *pi = &acc_im[(size_t)row * n + col];
+#pragma omp atomic
+                *pr += (double)d.re;
+#pragma omp atomic
+                *pi += (double)d.im;
+            }
+        }
+    }
+    for (size_t i = 0; i < (size_t)n * n; ++i) {
+        if (acc_re[i] != 0.0 || acc_im[i] != 0.0) {
+            A_re[i] += (REAL)acc_re[i];
+            A_im[i] += (REAL)acc_im[i];
+        }
+    }
+    free(acc_re); free(acc_im); free(pairs);
+    return np;
+}
+
 /* ---- exterior field (main.swift:1843-1895) ---------------------------- */
 int OGP(field)(const og_geom *g, REAL kr, const REAL *p_re, const REAL *p_im,
                const REAL *q_re, const REAL *q_im, const float *obs3xN, int nobs,

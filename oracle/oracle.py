@@ -128,6 +128,28 @@ class Oracle:
         b[...] = bre + 1j * bim
         return int(u)
 
+    def near_pairs(self, threshold: float = 1.5):
+        """Near, non-touching (test, trial, test_mask, trial_mask) pairs of the near-field option."""
+        npairs = self._fn("near_pairs")(ctypes.byref(self.geom), ctypes.c_double(threshold), None, 0)
+        out = np.zeros((max(npairs, 1), 4), np.int32)
+        self._fn("near_pairs")(ctypes.byref(self.geom), ctypes.c_double(threshold), _ptr(out), ctypes.c_int(npairs))
+        return out[:npairs]
+
+    def near_correct(self, A, b, k: float, q=None, k_imag: float = 0.0, beta=None, level: int = 2,
+                     threshold: float = 1.5) -> int:
+        """Add the near-field subdivision corrections (subdivided - regular blocks of near, non-touching
+        pairs, the reference's optional near quadrature) to ``A``/``b`` in place; returns the pair count."""
+        Are = np.ascontiguousarray(A.real, dtype=self.real); Aim = np.ascontiguousarray(A.imag, dtype=self.real)
+        bre = np.ascontiguousarray(b.real, dtype=self.real); bim = np.ascontiguousarray(b.imag, dtype=self.real)
+        qre, qim = self._split(q, self.T)
+        brr, bri = self._split(beta, self.T)
+        npairs = self._fn("near_correct")(
+            ctypes.byref(self.geom), self._ct(k), self._ct(k_imag), _ptr(qre), _ptr(qim), _ptr(brr), _ptr(bri),
+            _ptr(Are), _ptr(Aim), _ptr(bre), _ptr(bim), ctypes.c_int(int(level)), ctypes.c_double(threshold))
+        A[...] = Are + 1j * Aim
+        b[...] = bre + 1j * bim
+        return int(npairs)
+
     def corrected(self, k: float, q=None, k_imag: float = 0.0, beta=None, duffy_order: int = 4):
         """Regular 6x6 assembly plus Duffy corrections: the reference's 'corrected' mode (``duffy_order`` 4);
         other orders give the convergence study of its singular quadrature."""

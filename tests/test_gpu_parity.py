@@ -583,3 +583,49 @@ def test_assemble_multi_equals_one_pass_per_source(name):
     B = _host(Br, Bi)
     for k in range(3):   # (a one-triangle mesh leaves the zeroed source with b = 0 exactly)
         assert np.linalg.norm(B[k] - refs[k]) <= 1e-6 * max(np.linalg.norm(refs[k]), 1e-30)
+
+
+@pytest.mark.parametrize("name,level,threshold", [("near", 2, 1.5), ("ico2", 1, 1.5), ("horn_quarter", 2, 1.5),
+                                                  ("xy_half", 1, 2.0), ("yz_half", 2, 1.5)])
+def test_near_quadrature_assembly_matches_oracle(name, level, threshold):
+    """Near-field subdivision on the GPU (hbem_session_set_near_quadrature) against the oracle's restatement of
+    the reference's CPU correction (main.swift:3072-3202): the same near pairs, and the corrected matrix and
+    right-hand side with the near corrections within 1e-4."""
+    b = golden_buffers(name)
+    o = Oracle(b, SYM[name], "f64")
+    q = _q(b.n_triangles, 8)
+    k = 18.3
+    A_ref, b_ref = o.corrected(k, q)
+    n_ref = o.near_correct(A_ref, b_ref, k, q, level=level, threshold=threshold)
+    with NativeSession(b, symmetry_plane={0: None, 1: "yz", 3: "yz+xz", 4: "xy"}[SYM[name]],
+                       check_open_edges=False, near_quadrature=(level, threshold)) as s:
+        assert s.query("near_pairs") == n_ref == len(o.near_pairs(threshold))
+        assert s.near_quadrature["pair_count"] == n_ref
+        Ar, Ai, br, bi = s.assemble([k], q[None, :])
+    assert n_ref > 0
+    assert rel(_host(Ar, Ai)[0], A_ref) < 1e-4
+    assert rel(_host(br, bi)[0], b_ref) < 1e-4
+
+
+def test_near_quadrature_on_the_reference_fixture_and_off_again():
+    """The reference's test on the GPU path: level 2 at threshold 1.5 moves the near fixture's (0, 1) block
+    towards the level-4 subdivided helper (golden); level 0 restores the plain corrected matrix exactly."""
+    from conftest import golden
+
+    b = golden_buffers("near")
+    q = np.array([1.0, 0.0], np.complex64)
+    k = 1.8318326
+    with NativeSession(b, check_open_edges=False) as s:
+        A0 = _host(*s.assemble([k], q[None, :])[:2])[0]
+        lib = load_library()
+        assert lib.hbem_session_set_near_quadrature(s.handle, 2, 1.5) == 0
+        A1 = _host(*s.assemble([k], q[None, :])[:2])[0]
+        assert lib.hbem_session_set_near_quadrature(s.handle, 0, 0.0) == 0
+        assert s.query("near_pairs") == 0
+        A2 = _host(*s.assemble([k], q[None, :])[:2])[0]
+        assert lib.hbem_session_set_near_quadrature(s.handle, 3, 1.5) == -1
+        assert lib.hbem_session_set_near_quadrature(s.handle, 1, -1.0) == -1
+    ref = golden("pair_blocks.npz")["0__dlp"]
+    blk = np.ix_([0, 1, 2], [3, 4, 5])
+    assert np.linalg.norm(A1[blk] - ref) < 0.1 * np.linalg.norm(A0[blk] - ref)
+    assert rel(A2, A0) < 1e-6

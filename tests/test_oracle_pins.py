@@ -232,3 +232,33 @@ def test_f32_oracle_tracks_f64_oracle():
     A64, b64 = o64.corrected(18.3, q)
     assert np.linalg.norm(A32 - A64) / np.linalg.norm(A64) < 1e-5
     assert np.linalg.norm(b32 - b64) / np.linalg.norm(b64) < 1e-5
+
+
+def test_near_quadrature_corrects_the_close_non_touching_pair():
+    """The reference's near-quadrature test (tests/test_metal_native.py:1881-1950) on the oracle: on its
+    two-triangle near fixture, level-2 subdivision at threshold 1.5 finds both orders of the close pair and
+    moves the (0, 1) block towards the level-4 subdivided FP64 helper (golden)."""
+    o = Oracle(golden_buffers("near"), 0, "f64")
+    pairs = o.near_pairs(1.5)
+    assert sorted(map(tuple, pairs.tolist())) == [(0, 1, 0, 0), (1, 0, 0, 0)]
+    k = 1.8318326
+    q = np.array([1.0, 0.0], np.complex64)
+    A0, b0 = o.corrected(k, q)
+    A1, b1 = A0.copy(), b0.copy()
+    assert o.near_correct(A1, b1, k, q, level=2, threshold=1.5) == 2
+    ref = golden("pair_blocks.npz")["0__dlp"]   # case 0: near (0, 1) at k = 1.8318326, level 4
+    base = A0[np.ix_([0, 1, 2], [3, 4, 5])]
+    near = A1[np.ix_([0, 1, 2], [3, 4, 5])]
+    assert np.linalg.norm(near - base) > 0.0
+    assert np.linalg.norm(near - ref) < 0.1 * np.linalg.norm(base - ref)
+
+
+def test_near_pairs_exclude_touching_and_far_pairs():
+    """Every near pair of the quarter horn shares no vertex (image-aware) and passes the centroid cut; a larger
+    threshold finds a superset."""
+    o = Oracle(golden_buffers("horn_quarter"), 3, "f64")
+    small = {tuple(r) for r in o.near_pairs(1.0).tolist()}
+    large = {tuple(r) for r in o.near_pairs(1.5).tolist()}
+    assert small and small < large
+    touching = {tuple(r[:4]) for r in o.duffy_pairs()[0].tolist()}
+    assert not (large & touching)

@@ -221,3 +221,18 @@ def test_multi_source_with_robin_walls_is_one_sweep_per_source(monkeypatch):
     with pytest.raises(ValueError, match="velocity_source_callback"):
         sw.run_sweep_multi_source(mesh, [500.0], frame,
                                   hb.native_config(velocity_source_callback=lambda f: {2: 1.0}), [{2: 1.0}])
+
+
+def test_near_quadrature_setting_parses_as_the_reference():
+    """HORNLAB_METAL_BEM_NATIVE_NEAR_QUADRATURE values (main.swift:5024-5054): unset / '' / '0' = off, '1' /
+    '2' = that level at threshold 1.5, '<level>:<threshold>'; anything else is rejected."""
+    from hornlab_metal_bem_b200.native import parse_near_quadrature
+
+    assert parse_near_quadrature(None) is None
+    assert parse_near_quadrature("") is None and parse_near_quadrature("0") is None
+    assert parse_near_quadrature("1") == (1, 1.5) and parse_near_quadrature("2") == (2, 1.5)
+    assert parse_near_quadrature("2:1.25") == (2, 1.25)
+    assert parse_near_quadrature((1, 2.0)) == (1, 2.0) and parse_near_quadrature((0, 1.0)) is None
+    for bad in ("3", "1:0", "1:-2", "2:nan", "2:inf", "x", "1:2:3", "0:1.5"):
+        with pytest.raises(ValueError, match="NEAR_QUADRATURE"):
+            parse_near_quadrature(bad)
