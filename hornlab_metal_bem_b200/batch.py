@@ -4,9 +4,10 @@ No counterpart in the reference, which runs one mesh per session and one
 helper process per operation.  Here every (mesh, frequency) case of a batch
 stays on the device:
 
-* each mesh's sweep (corrected assembly -> LU -> solve -> field -> tag
-  averages over all its frequencies) is captured once into a CUDA graph and
-  replayed, so its hundreds of launches cost one graph launch;
+* each mesh's sweep (corrected assembly -> LU -> solve -> FP64-residual
+  refinement -> field -> tag averages over all its frequencies) is captured
+  once into a CUDA graph and replayed, so its hundreds of launches cost one
+  graph launch (the refinement decides its stopping rule on the device);
 * meshes are spread over a few streams by longest-processing-time order of
   their estimated cost (n^3 for the LU, T^2 M for the assembly), so small
   meshes overlap with large ones; meshes on one stream share one workspace
@@ -66,6 +67,8 @@ class CaseOutput:
     tag_average: np.ndarray          # (F, n_tags) complex128
     lapack_info: np.ndarray          # (F,) int
     surface_pressure: np.ndarray | None = None
+    refine_iterations: np.ndarray | None = None     # (F,) refinement passes applied
+    refine_residual_rel: np.ndarray | None = None   # (F,) ||b - A x|| / ||b|| after them (0 without refinement)
 
 
 def lpt_slots(costs, n_slots: int) -> list[list[int]]:
@@ -176,10 +179,13 @@ def apply_variant(lib, variant: dict) -> None:
 class _Slot:
     """One stream and the workspace shared by the meshes assigned to it."""
 
-    def __init__(self, torch, dev, n_max: int, F_max: int):
+    def __init__(self, torch, dev, n_max: int, F_max: int, refine: bool):
         self.stream = torch.cuda.Stream(device=dev)
         self.A_re = torch.empty((F_max, n_max, n_max), dtype=torch.float32, device=dev)
         self.A_im = torch.empty_like(self.A_re)
+        # the assembled matrices, kept for the FP64 residuals of the refinement
+        self.A0_re = torch.empty_like(self.A_re) if refine else None
+        self.A0_im = torch.empty_like(self.A_re) if refine else None
         self.b_re = torch.empty((F_max, n_max), dtype=torch.float32, device=dev)
         self.b_im = torch.empty_like(self.b_re)
         self.x_re = torch.empty_like(self.b_re)
@@ -190,8 +196,11 @@ class _Slot:
 class _CaseRun:
     """Device inputs / outputs of one case and its launch sequence."""
 
-    def __init__(self, torch, dev, case: SweepCase, write_surface_pressure: bool):
+    def __init__(self, torch, dev, case: SweepCase, write_surface_pressure: bool, refine_tolerance: float,
+                 refine_max_iterations: int):
         self.case = case
+        self.refine_tol = float(refine_tolerance)
+        self.refine_max = int(refine_max_iterations)
         self.s = NativeSession(case.buffers, symmetry_plane=case.symmetry_plane, check_open_edges=False)
         self.lib = self.s.lib
         F, T = len(case.k_re), case.T
@@ -204,6 +213,8 @@ class _CaseRun:
         self.tags_h = np.ascontiguousarray(case.tags, dtype=np.int32)
         self.tags = torch.as_tensor(self.tags_h, device=dev)
         self.info = torch.empty(F, dtype=torch.int32, device=dev)
+        self.iters = torch.zeros(F, dtype=torch.int32, device=dev)
+        self.resid = torch.zeros(F, dtype=torch.float64, device=dev)
         self.f_re = torch.empty((F, self.n_obs), dtype=torch.float32, device=dev)
         self.f_im = torch.empty_like(self.f_re)
         self.tag_out = torch.zeros((F, max(1, len(case.tags)), 2), dtype=torch.float64, device=dev)
@@ -223,10 +234,19 @@ class _CaseRun:
                                 _t_ptr(b_re), _t_ptr(b_im), n, HBEM_ASM_CORRECTED | 4, st), "hbem_assemble", lib)
         x_re.copy_(b_re)
         x_im.copy_(b_im)
+        if self.refine_max > 0:
+            A0_re, A0_im = slot.A0_re.view(-1)[:F * n * n], slot.A0_im.view(-1)[:F * n * n]
+            A0_re.copy_(A_re)
+            A0_im.copy_(A_im)
         check(lib.hbem_lu_factor(n, F, _t_ptr(A_re), _t_ptr(A_im), n, n * n, _t_ptr(piv), n, _t_ptr(self.info),
                                  HBEM_PREC_PLAIN, st), "hbem_lu_factor", lib)
         check(lib.hbem_lu_solve(n, 1, F, _t_ptr(A_re), _t_ptr(A_im), n, n * n, _t_ptr(piv), n, _t_ptr(x_re),
                                 _t_ptr(x_im), 1, n, HBEM_TRANS_N, st), "hbem_lu_solve", lib)
+        if self.refine_max > 0:
+            check(lib.hbem_refine_async(n, F, _t_ptr(A0_re), _t_ptr(A0_im), n, n * n, _t_ptr(A_re), _t_ptr(A_im),
+                                        n * n, _t_ptr(piv), n, _t_ptr(b_re), _t_ptr(b_im), n, _t_ptr(x_re),
+                                        _t_ptr(x_im), n, self.refine_tol, self.refine_max, _t_ptr(self.iters),
+                                        _t_ptr(self.resid), st), "hbem_refine_async", lib)
         check(lib.hbem_field(s.handle, F, _np_ptr(self.k_re), _t_ptr(x_re), _t_ptr(x_im), n, _t_ptr(self.q_re),
                              _t_ptr(self.q_im), s.n_triangles, _t_ptr(self.obs), self.n_obs, _t_ptr(self.f_re),
                              _t_ptr(self.f_im), self.n_obs, st), "hbem_field", lib)
@@ -245,7 +265,8 @@ class _CaseRun:
         sp = None
         if self.p_re is not None:
             sp = (self.p_re.cpu().numpy() + 1j * self.p_im.cpu().numpy()).astype(np.complex64)
-        return CaseOutput(field=f, tag_average=tav, lapack_info=self.info.cpu().numpy(), surface_pressure=sp)
+        return CaseOutput(field=f, tag_average=tav, lapack_info=self.info.cpu().numpy(), surface_pressure=sp,
+                          refine_iterations=self.iters.cpu().numpy(), refine_residual_rel=self.resid.cpu().numpy())
 
 
 class BatchedSweeps:
@@ -253,17 +274,22 @@ class BatchedSweeps:
 
     ``tuning``: "auto" (autotune per size bucket, cached), None (built-in
     variants) or a dict bucket -> variant.  Call ``run()`` any number of
-    times; ``outputs()`` copies the last results to the host.
+    times; ``outputs()`` copies the last results to the host.  Each FP32 LU
+    solution is refined with FP64 residuals (``hbem_refine_async``: at most
+    ``refine_max_iterations`` passes, stopping at ``refine_tolerance`` or when
+    a pass no longer lowers the residual; 0 keeps the unrefined cgesv result).
     """
 
     def __init__(self, cases: list[SweepCase], n_streams: int = 4, tuning="auto", cache_path=None,
-                 write_surface_pressure: bool = False, use_graphs: bool = True):
+                 write_surface_pressure: bool = False, use_graphs: bool = True, refine_tolerance: float = 1e-6,
+                 refine_max_iterations: int = 3):
         torch = require_cuda()
         self.torch = torch
         self.lib = load_library()
         self.dev = torch.device("cuda", torch.cuda.current_device())
         self.cases = list(cases)
-        self.runs = [_CaseRun(torch, self.dev, c, write_surface_pressure) for c in self.cases]
+        self.runs = [_CaseRun(torch, self.dev, c, write_surface_pressure, refine_tolerance, refine_max_iterations)
+                     for c in self.cases]
         costs = [c.cost() for c in self.cases]
         self.slot_of_case: dict[int, int] = {}
         self.slot_cases = lpt_slots(costs, n_streams)
@@ -271,7 +297,7 @@ class BatchedSweeps:
         for si, members in enumerate(self.slot_cases):
             n_max = max(self.runs[i].n for i in members)
             F_max = max(self.runs[i].F for i in members)
-            self.slots.append(_Slot(torch, self.dev, n_max, F_max))
+            self.slots.append(_Slot(torch, self.dev, n_max, F_max, refine_max_iterations > 0))
             for i in members:
                 self.slot_of_case[i] = si
         self.autotuner = None

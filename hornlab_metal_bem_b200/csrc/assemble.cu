@@ -13,8 +13,10 @@
 // (one per lane) x 64 trial triangles (eight per warp, warp-uniform).  The
 // trial tile's quadrature points are staged once in shared memory and read
 // as broadcasts; the test points live in registers.  Each lane evaluates
-// 36 x (1 + images) kernel samples per pair with one rsqrt and one sincos
-// (phase reduced in turns before the fast sine/cosine), factorises the 3x3
+// 36 x (1 + images) kernel samples per pair with one rsqrt and one fast
+// sincos of k r (the hardware reduces the argument in turns itself, as
+// accurately as the FP32 product k r is; the rounding of that product is the
+// phase error either way), factorises the 3x3
 // basis products (inner sum over trial points first) and adds the pair block
 // into a shared-memory accumulator indexed by the tile's distinct dofs.  The
 // tile is flushed once with red.global.add, which cuts global atomics by the
@@ -58,7 +60,6 @@ struct AsmArgs {
     int T, nf, n_src;
     float rw;
     float k[kMaxFreqPerLaunch];
-    float kt[kMaxFreqPerLaunch];  // k / (2 pi): phase in turns per metre
     float ki[kMaxFreqPerLaunch];
 };
 
@@ -71,43 +72,6 @@ __device__ __forceinline__ float qy(int q) {
 __device__ __forceinline__ float qw(int q) { return (q == 0 || q == 2 || q == 3) ? HBEM_QWA : HBEM_QWB; }
 __device__ __forceinline__ float bas(int q, int i) {
     return i == 0 ? 1.0f - qx(q) - qy(q) : (i == 1 ? qx(q) : qy(q));
-}
-
-// Round to nearest integer on the FMA pipe (|t| < 2^22): adding and removing
-// 1.5 * 2^23 leaves the rounded value.
-__device__ __forceinline__ float round_fma(float t) {
-    const float big = 12582912.0f;
-    return __fsub_rn(__fadd_rn(t, big), big);
-}
-
-// One kernel sample: adds dG/dn_y (D) and, when NEED_G, G to the running
-// sums.  The 1/(4 pi) factor is applied once per pair block.  r^2 <= 1e-14
-// is treated as the singular point and contributes nothing (main.swift:3443-3480).
-template <bool CK, bool NEED_G>
-__device__ __forceinline__ void sample(float dx, float dy, float dz, float nx, float ny, float nz, float k,
-                                       float kt, float ki, float &dre, float &dim, float &gre, float &gim) {
-    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    float rinv = rsqrtf(r2);
-    rinv = r2 > 1.0e-14f ? rinv : 0.0f;
-    const float r = r2 * rinv;
-    float t = r * kt;
-    t -= round_fma(t);
-    float s, c;
-    __sincosf(t * 6.28318530717958647692f, &s, &c);
-    float g = rinv;
-    float fre = -rinv;
-    if (CK) {
-        g *= __expf(-ki * r);
-        fre -= ki;
-    }
-    const float gc = g * c, gs = g * s;
-    const float proj = fmaf(dx, nx, fmaf(dy, ny, dz * nz)) * rinv;
-    dre = fmaf(fmaf(gc, fre, -gs * k), proj, dre);
-    dim = fmaf(fmaf(gc, k, gs * fre), proj, dim);
-    if (NEED_G) {
-        gre += gc;
-        gim += gs;
-    }
 }
 
 // Per test quadrature point a: wa[a][i] = w_a * phi_i(x_a) (uniform across the
@@ -123,7 +87,7 @@ __constant__ float c_w[6];       // w_b
 // and, when NEED_G, G = (c + i s) / r.
 template <int NF, bool CK, bool NEED_G>
 __device__ __forceinline__ void sample_nf(float dx, float dy, float dz, float nx, float ny, float nz,
-                                          const float (&k)[NF], const float (&kt)[NF], const float (&ki)[NF],
+                                          const float (&k)[NF], const float (&ki)[NF],
                                           float (&dre)[NF], float (&dim)[NF], float (&gre)[NF], float (&gim)[NF]) {
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     float u = rsqrtf(r2);
@@ -133,10 +97,8 @@ __device__ __forceinline__ void sample_nf(float dx, float dy, float dz, float nx
     const float h = dn * (u * u);
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
-        float t = r * kt[f];
-        t -= round_fma(t);
         float sn, cs;
-        __sincosf(t * 6.28318530717958647692f, &sn, &cs);
+        __sincosf(r * k[f], &sn, &cs);
         float hh = h, uu = u, fre = u;
         if (CK) {
             const float damp = __expf(-ki[f] * r);
@@ -158,7 +120,7 @@ __device__ __forceinline__ void sample_nf(float dx, float dy, float dz, float nx
 // (D and G come out multiplied by wgt; the phase and 1/r of E are unscaled).
 template <int NF, bool CK>
 __device__ __forceinline__ void sample_nf_w(float dx, float dy, float dz, float nx, float ny, float nz,
-                                            const float (&k)[NF], const float (&kt)[NF], const float (&ki)[NF],
+                                            const float (&k)[NF], const float (&ki)[NF],
                                             float wgt, float (&dre)[NF], float (&dim)[NF], float (&gre)[NF],
                                             float (&gim)[NF]) {
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
@@ -169,10 +131,8 @@ __device__ __forceinline__ void sample_nf_w(float dx, float dy, float dz, float 
     const float h = dn * (u * u) * wgt, uw = u * wgt;
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
-        float t = r * kt[f];
-        t -= round_fma(t);
         float sn, cs;
-        __sincosf(t * 6.28318530717958647692f, &sn, &cs);
+        __sincosf(r * k[f], &sn, &cs);
         float hh = h, uu = uw, fre = u;
         if (CK) {
             const float damp = __expf(-ki[f] * r);
@@ -191,7 +151,7 @@ __device__ __forceinline__ void sample_nf_w(float dx, float dy, float dz, float 
 template <int SYM, int NF, bool CK, bool NEED_G>
 __device__ __forceinline__ void pair_block(const float4 *__restrict__ tq, const float4 *__restrict__ sp, float nx,
                                            float ny, float nz, bool self, const float (&k)[NF],
-                                           const float (&kt)[NF], const float (&ki)[NF], float (&are)[NF][9],
+                                           const float (&ki)[NF], float (&are)[NF][9],
                                            float (&aim)[NF][9], float (&sre)[NF][3], float (&sim)[NF][3]) {
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
@@ -220,16 +180,16 @@ __device__ __forceinline__ void pair_block(const float4 *__restrict__ tq, const 
 #pragma unroll
             for (int f = 0; f < NF; ++f) dre[f] = dim[f] = gre[f] = gim[f] = 0.f;
             if (!(self && a == b))
-                sample_nf<NF, CK, NEED_G>(y.x - x.x, y.y - x.y, y.z - x.z, nx, ny, nz, k, kt, ki, dre, dim, gre, gim);
+                sample_nf<NF, CK, NEED_G>(y.x - x.x, y.y - x.y, y.z - x.z, nx, ny, nz, k, ki, dre, dim, gre, gim);
             if (SYM == 1 || SYM == 3)
-                sample_nf<NF, CK, NEED_G>(-y.x - x.x, y.y - x.y, y.z - x.z, -nx, ny, nz, k, kt, ki, dre, dim, gre, gim);
+                sample_nf<NF, CK, NEED_G>(-y.x - x.x, y.y - x.y, y.z - x.z, -nx, ny, nz, k, ki, dre, dim, gre, gim);
             if (SYM == 2 || SYM == 3)
-                sample_nf<NF, CK, NEED_G>(y.x - x.x, -y.y - x.y, y.z - x.z, nx, -ny, nz, k, kt, ki, dre, dim, gre, gim);
+                sample_nf<NF, CK, NEED_G>(y.x - x.x, -y.y - x.y, y.z - x.z, nx, -ny, nz, k, ki, dre, dim, gre, gim);
             if (SYM == 3)
-                sample_nf<NF, CK, NEED_G>(-y.x - x.x, -y.y - x.y, y.z - x.z, -nx, -ny, nz, k, kt, ki, dre, dim, gre,
+                sample_nf<NF, CK, NEED_G>(-y.x - x.x, -y.y - x.y, y.z - x.z, -nx, -ny, nz, k, ki, dre, dim, gre,
                                           gim);
             if (SYM == 4)
-                sample_nf<NF, CK, NEED_G>(y.x - x.x, y.y - x.y, -y.z - x.z, nx, ny, -nz, k, kt, ki, dre, dim, gre, gim);
+                sample_nf<NF, CK, NEED_G>(y.x - x.x, y.y - x.y, -y.z - x.z, nx, ny, -nz, k, ki, dre, dim, gre, gim);
 #pragma unroll
             for (int f = 0; f < NF; ++f) {
 #pragma unroll
@@ -319,12 +279,11 @@ __global__ void __launch_bounds__(kAsmThreads, MINB) k_regular(const __grid_cons
     }
     __syncthreads();
 
-    float k[NF], kt[NF], ki[NF];
+    float k[NF], ki[NF];
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
         const int ff = f0 + min(f, nfv - 1);
         k[f] = p.k[ff];
-        kt[f] = p.kt[ff];
         ki[f] = p.ki[ff];
     }
     const int test = test0 + lane;
@@ -338,9 +297,9 @@ __global__ void __launch_bounds__(kAsmThreads, MINB) k_regular(const __grid_cons
             const bool self = (tbase + jj) == test;
             float are[NF][9], aim[NF][9], sre[NF][3], sim[NF][3];
             if (s_flag[jj])
-                pair_block<SYM, NF, CK, true>(tq, &s_qp[jj * 6], nj.x, nj.y, nj.z, self, k, kt, ki, are, aim, sre, sim);
+                pair_block<SYM, NF, CK, true>(tq, &s_qp[jj * 6], nj.x, nj.y, nj.z, self, k, ki, are, aim, sre, sim);
             else
-                pair_block<SYM, NF, CK, false>(tq, &s_qp[jj * 6], nj.x, nj.y, nj.z, self, k, kt, ki, are, aim, sre,
+                pair_block<SYM, NF, CK, false>(tq, &s_qp[jj * 6], nj.x, nj.y, nj.z, self, k, ki, are, aim, sre,
                                                sim);
             const float scale = HBEM_INV4PI * tjac * nj.w;
             const uchar4 cs = s_cs[jj];
@@ -415,13 +374,15 @@ __global__ void __launch_bounds__(kAsmThreads, MINB) k_regular(const __grid_cons
 //   F = e^{ikr} (ik - 1/r) / r^2,  d = My - x,  r = |d| = |Mx - y|
 // (M is an involution and an isometry), and G(r) is the same.  So each
 // unordered pair {tau, sigma} (sorted index tau <= sigma) is evaluated once
+// (the coincident self-point of tau = sigma has r^2 = 0 exactly and drops out
+// through the singular-point guard, as the reference excludes it)
 // and adds A[tau dofs][sigma dofs], A[sigma dofs][tau dofs] and both RHS
 // rows: one rsqrt / sincos per sample instead of two.  Tiles and the shared
 // accumulation are those of k_regular with a second, transposed plane.
 // ---------------------------------------------------------------------------
 template <bool CK, bool NEED_G>
 __device__ __forceinline__ void sample_sym(float dx, float dy, float dz, float nsx, float nsy, float nsz, float ntx,
-                                           float nty, float ntz, float k, float kt, float ki, float &dre, float &dim,
+                                           float nty, float ntz, float k, float ki, float &dre, float &dim,
                                            float &tre, float &tim, float &gre, float &gim) {
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     float u = rsqrtf(r2);
@@ -430,10 +391,8 @@ __device__ __forceinline__ void sample_sym(float dx, float dy, float dz, float n
     const float u2 = u * u;
     float hs = fmaf(dx, nsx, fmaf(dy, nsy, dz * nsz)) * u2;
     float ht = -fmaf(dx, ntx, fmaf(dy, nty, dz * ntz)) * u2;
-    float t = r * kt;
-    t -= round_fma(t);
     float sn, cs;
-    __sincosf(t * 6.28318530717958647692f, &sn, &cs);
+    __sincosf(r * k, &sn, &cs);
     float uu = u, fre = u;
     if (CK) {
         const float damp = __expf(-ki * r);
@@ -460,8 +419,8 @@ __device__ __forceinline__ void sample_sym(float dx, float dy, float dz, float n
 // test-point weights only).
 template <int SYM, bool CK, bool NEED_G>
 __device__ __forceinline__ void pair_block_sym(const float4 *__restrict__ tq, const float4 *__restrict__ sp, float nx,
-                                               float ny, float nz, float tnx, float tny, float tnz, bool self, float k,
-                                               float kt, float ki, float (&fwr)[9], float (&fwi)[9], float (&tnr)[9],
+                                               float ny, float nz, float tnx, float tny, float tnz, float k, float ki,
+                                               float (&fwr)[9], float (&fwi)[9], float (&tnr)[9],
                                                float (&tni)[9], float (&sfr)[3], float (&sfi)[3], float (&str_)[3],
                                                float (&sti)[3]) {
 #pragma unroll
@@ -478,20 +437,19 @@ __device__ __forceinline__ void pair_block_sym(const float4 *__restrict__ tq, co
         for (int b = 0; b < 6; ++b) {
             const float4 y = sp[b];
             float dre = 0.f, dim = 0.f, tre = 0.f, tim = 0.f, gre = 0.f, gim = 0.f;
-            if (!(self && a == b))
-                sample_sym<CK, NEED_G>(y.x - x.x, y.y - x.y, y.z - x.z, nx, ny, nz, tnx, tny, tnz, k, kt, ki, dre,
+            sample_sym<CK, NEED_G>(y.x - x.x, y.y - x.y, y.z - x.z, nx, ny, nz, tnx, tny, tnz, k, ki, dre,
                                        dim, tre, tim, gre, gim);
             if (SYM == 1 || SYM == 3)
-                sample_sym<CK, NEED_G>(-y.x - x.x, y.y - x.y, y.z - x.z, -nx, ny, nz, tnx, tny, tnz, k, kt, ki, dre,
+                sample_sym<CK, NEED_G>(-y.x - x.x, y.y - x.y, y.z - x.z, -nx, ny, nz, tnx, tny, tnz, k, ki, dre,
                                        dim, tre, tim, gre, gim);
             if (SYM == 2 || SYM == 3)
-                sample_sym<CK, NEED_G>(y.x - x.x, -y.y - x.y, y.z - x.z, nx, -ny, nz, tnx, tny, tnz, k, kt, ki, dre,
+                sample_sym<CK, NEED_G>(y.x - x.x, -y.y - x.y, y.z - x.z, nx, -ny, nz, tnx, tny, tnz, k, ki, dre,
                                        dim, tre, tim, gre, gim);
             if (SYM == 3)
-                sample_sym<CK, NEED_G>(-y.x - x.x, -y.y - x.y, y.z - x.z, -nx, -ny, nz, tnx, tny, tnz, k, kt, ki, dre,
+                sample_sym<CK, NEED_G>(-y.x - x.x, -y.y - x.y, y.z - x.z, -nx, -ny, nz, tnx, tny, tnz, k, ki, dre,
                                        dim, tre, tim, gre, gim);
             if (SYM == 4)
-                sample_sym<CK, NEED_G>(y.x - x.x, y.y - x.y, -y.z - x.z, nx, ny, -nz, tnx, tny, tnz, k, kt, ki, dre,
+                sample_sym<CK, NEED_G>(y.x - x.x, y.y - x.y, -y.z - x.z, nx, ny, -nz, tnx, tny, tnz, k, ki, dre,
                                        dim, tre, tim, gre, gim);
 #pragma unroll
             for (int j = 0; j < 3; ++j) {
@@ -604,7 +562,7 @@ __global__ void __launch_bounds__(kAsmThreads, MINB) k_regular_sym(const __grid_
     }
     __syncthreads();
 
-    const float k = p.k[f], kt = p.kt[f], ki = p.ki[f];
+    const float k = p.k[f], ki = p.ki[f];
     const int test = test0 + lane;
     if (lane < ntest) {
         const float4 tn = p.nrm[test];
@@ -636,10 +594,10 @@ __global__ void __launch_bounds__(kAsmThreads, MINB) k_regular_sym(const __grid_
             const bool self = sigma == test;
             float fwr[9], fwi[9], tnr[9], tni[9], sfr[3], sfi[3], str_[3], sti[3];
             if (s_flag[jj] || tflag)
-                pair_block_sym<SYM, CK, true>(tq, &s_qp[jj * 6], nj.x, nj.y, nj.z, tn.x, tn.y, tn.z, self, k, kt, ki,
+                pair_block_sym<SYM, CK, true>(tq, &s_qp[jj * 6], nj.x, nj.y, nj.z, tn.x, tn.y, tn.z, k, ki,
                                               fwr, fwi, tnr, tni, sfr, sfi, str_, sti);
             else
-                pair_block_sym<SYM, CK, false>(tq, &s_qp[jj * 6], nj.x, nj.y, nj.z, tn.x, tn.y, tn.z, self, k, kt, ki,
+                pair_block_sym<SYM, CK, false>(tq, &s_qp[jj * 6], nj.x, nj.y, nj.z, tn.x, tn.y, tn.z, k, ki,
                                                fwr, fwi, tnr, tni, sfr, sfi, str_, sti);
             const float scale = HBEM_INV4PI * tjac * nj.w;
             const uchar4 cs = s_cs[jj];
@@ -829,7 +787,6 @@ struct DuffyArgs {
     long long sia_stride, saa_stride;
     int m_ap, mode, nf;
     float k[kMaxFreqPerLaunch];
-    float kt[kMaxFreqPerLaunch];
     float ki[kMaxFreqPerLaunch];
 };
 
@@ -927,12 +884,11 @@ __global__ void __launch_bounds__(256, MINB) k_duffy(const __grid_constant__ Duf
             S[0][c] = ssg[c] * S[0][c];
         }
     }
-    float k[NF], kt[NF], ki[NF];
+    float k[NF], ki[NF];
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
         const int ff = fg + min(f, nfv - 1);
         k[f] = p.k[ff];
-        kt[f] = p.kt[ff];
         ki[f] = p.ki[ff];
     }
 
@@ -954,7 +910,7 @@ __global__ void __launch_bounds__(256, MINB) k_duffy(const __grid_constant__ Duf
         const float ts[2][2] = {{txi * sxi, txi * seta}, {teta * sxi, teta * seta}};
         const float tw[3] = {1.f, txi, teta}, sw[3] = {1.f, sxi, seta};
         float dre[NF], dim[NF], gre[NF], gim[NF];
-        sample_nf_w<NF, CK>(d[0], d[1], d[2], nx, ny, nz, k, kt, ki, w, dre, dim, gre, gim);
+        sample_nf_w<NF, CK>(d[0], d[1], d[2], nx, ny, nz, k, ki, w, dre, dim, gre, gim);
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
             acc[f][0] += gre[f];
@@ -1142,10 +1098,9 @@ __global__ void __launch_bounds__(256, MINB) k_duffy(const __grid_constant__ Duf
     }
 }
 
-void fill_k(float *k, float *kt, float *ki, const float *k_re, const float *k_im, int n) {
+void fill_k(float *k, float *ki, const float *k_re, const float *k_im, int n) {
     for (int f = 0; f < n; ++f) {
         k[f] = k_re[f];
-        kt[f] = (float)((double)k_re[f] / (2.0 * 3.14159265358979323846));
         ki[f] = k_im ? k_im[f] : 0.f;
     }
 }
@@ -1197,7 +1152,7 @@ int launch_regular(Session &s, int n_freq, const float *k_re, const float *k_im,
         a.T = s.n_triangles;
         a.rw = (float)(1 << ((s.sym & 1) + ((s.sym >> 1) & 1) + ((s.sym >> 2) & 1)));
         bool ck = false;
-        fill_k(a.k, a.kt, a.ki, k_re + f0, k_im ? k_im + f0 : nullptr, nf);
+        fill_k(a.k, a.ki, k_re + f0, k_im ? k_im + f0 : nullptr, nf);
         for (int f = 0; f < nf; ++f) ck |= a.ki[f] != 0.f;
         if (!a.b_re) a.q_re = a.q_im = nullptr;
         a.nf = nf;
@@ -1238,7 +1193,7 @@ int launch_duffy(Session &s, int n_freq, const float *k_re, const float *k_im, c
         a.q_src_stride = q_src_stride; a.b_src_stride = b_src_stride; a.n_src = n_src;
         a.V = s.n_vertices; a.T = s.n_triangles; a.n_pairs = s.n_pairs;
         for (int r = 0; r < 3; ++r) { a.rule_off[r] = s.rule_off[r]; a.rule_cnt[r] = s.rule_cnt[r]; }
-        fill_k(a.k, a.kt, a.ki, k_re + f0, k_im ? k_im + f0 : nullptr, nf);
+        fill_k(a.k, a.ki, k_re + f0, k_im ? k_im + f0 : nullptr, nf);
         if (ap) {
             a.ap_local = s.d_ap_local;
             a.m_ap = s.m_ap;

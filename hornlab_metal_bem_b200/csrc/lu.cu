@@ -1640,14 +1640,16 @@ __global__ void k_rc_finish(int batch, const RcState *state, const unsigned *ano
     rcond[mat] = (sv.est != 0.0 && an != 0.0) ? (1.0 / sv.est) / an : 0.0;
 }
 
-// FP64 residual r = b - A x (one warp per row), and per-matrix norms.
+// FP64 residual r = b - A x (one warp per row), and per-matrix norms;
+// matrices whose `active` flag (optional) is 0 are skipped.
 __global__ void __launch_bounds__(256) k_residual(int n, const float *a_re, const float *a_im, long long lda,
                                                   long long a_stride, const float *b_re, const float *b_im,
                                                   long long b_stride, const float *x_re, const float *x_im,
-                                                  long long x_stride, float *r_re, float *r_im, double *norms) {
+                                                  long long x_stride, float *r_re, float *r_im, double *norms,
+                                                  const int *active = nullptr) {
     const int mat = blockIdx.y;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (warp >= n) return;
+    if (warp >= n || (active && !active[mat])) return;
     const float *Ar = a_re + (size_t)mat * a_stride + (size_t)warp * lda;
     const float *Ai = a_im + (size_t)mat * a_stride + (size_t)warp * lda;
     const float *xr = x_re + (size_t)mat * x_stride, *xi = x_im + (size_t)mat * x_stride;
@@ -1671,6 +1673,28 @@ __global__ void __launch_bounds__(256) k_residual(int n, const float *a_re, cons
         atomicAdd(&norms[2 * mat], rr * rr + ri * ri);
         atomicAdd(&norms[2 * mat + 1], bb);
     }
+}
+
+// The stopping rule of refine() on the device, one thread per matrix, for the
+// refinement without host synchronisation: pass `it` has just computed the
+// residual norms of the matrices still active; a matrix stops at the
+// tolerance, after max_iter passes, or once a pass no longer lowered its
+// residual.  iters / resid (optional) receive the passes applied and the
+// best relative residual.
+__global__ void k_refine_decide(int batch, int it, int max_iter, double tol, const double *norms, double *best,
+                                int *active, int *count, int *iters, double *resid) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= batch || (it > 0 && !active[m])) return;
+    if (it == 0) count[m] = 0;
+    const double rel = norms[2 * m + 1] > 0 ? sqrt(norms[2 * m] / norms[2 * m + 1]) : 0.0;
+    const bool stalled = it > 0 && !(rel < best[m]);
+    const double res = stalled ? best[m] : rel;
+    best[m] = res;
+    const int act = (!stalled && rel > tol && it < max_iter) ? 1 : 0;
+    active[m] = act;
+    count[m] += act;
+    if (iters) iters[m] = count[m];
+    if (resid) resid[m] = res;
 }
 
 __global__ void k_axpy_active(int n, float *x_re, float *x_im, long long x_stride, const float *d_re,
@@ -2147,7 +2171,8 @@ int refine(int n, int batch, const float *a_re, const float *a_im, long long lda
     for (int it = 0; it <= max_iter && rc == HBEM_OK; ++it) {
         if (cudaMemsetAsync(norms, 0, sizeof(double) * 2 * batch, st) != cudaSuccess) { rc = cuda_fail(cudaGetLastError(), "memset"); break; }
         dim3 g((n * 32 + 255) / 256, batch);
-        k_residual<<<g, 256, 0, st>>>(n, a_re, a_im, lda, a_stride, b_re, b_im, b_stride, x_re, x_im, x_stride, dr, di, norms);
+        k_residual<<<g, 256, 0, st>>>(n, a_re, a_im, lda, a_stride, b_re, b_im, b_stride, x_re, x_im, x_stride, dr, di, norms,
+                                      it > 0 ? active : nullptr);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) { rc = cuda_fail(e, "k_residual"); break; }
         count_launch();
@@ -2188,6 +2213,50 @@ int refine(int n, int batch, const float *a_re, const float *a_im, long long lda
     cudaFreeAsync(d, st);
     cudaFreeAsync(norms, st);
     cudaFreeAsync(active, st);
+    return rc;
+}
+
+// refine() without host synchronisation: max_iter correction passes are
+// always issued (a matrix that has stopped skips the residual, the solve's
+// wavefront blocks and the update) and the stopping rule runs on the device,
+// so the whole call can be captured in a CUDA graph.  A timed-out wavefront
+// wait is left for hbem_solve_status.
+int refine_async(int n, int batch, const float *a_re, const float *a_im, long long lda, long long a_stride,
+                 const float *lu_re, const float *lu_im, long long lu_stride, const int *piv, long long piv_stride,
+                 const float *b_re, const float *b_im, long long b_stride, float *x_re, float *x_im,
+                 long long x_stride, double tol, int max_iter, int *iters, double *resid, cudaStream_t st) {
+    const size_t nd = 2 * (size_t)batch * x_stride;
+    const size_t bytes = sizeof(double) * 3 * (size_t)batch + sizeof(float) * nd + sizeof(int) * 2 * (size_t)batch;
+    unsigned char *mem = nullptr;
+    HBEM_CUDA(cudaMallocAsync((void **)&mem, bytes, st));
+    double *norms = reinterpret_cast<double *>(mem), *best = norms + 2 * batch;
+    float *dr = reinterpret_cast<float *>(best + batch), *di = dr + (size_t)batch * x_stride;
+    int *active = reinterpret_cast<int *>(dr + nd), *count = active + batch;
+    int rc = HBEM_OK;
+    for (int it = 0; it <= max_iter && rc == HBEM_OK; ++it) {
+        cudaError_t e = cudaMemsetAsync(norms, 0, sizeof(double) * 2 * batch, st);
+        if (e != cudaSuccess) { rc = cuda_fail(e, "memset"); break; }
+        k_residual<<<dim3((n * 32 + 255) / 256, batch), 256, 0, st>>>(n, a_re, a_im, lda, a_stride, b_re, b_im,
+                                                                      b_stride, x_re, x_im, x_stride, dr, di, norms,
+                                                                      it > 0 ? active : nullptr);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) { rc = cuda_fail(e, "k_residual"); break; }
+        count_launch();
+        k_refine_decide<<<(batch + 127) / 128, 128, 0, st>>>(batch, it, max_iter, tol, norms, best, active, count,
+                                                              iters, resid);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) { rc = cuda_fail(e, "k_refine_decide"); break; }
+        count_launch();
+        if (it == max_iter) break;
+        rc = lu_solve_ex(n, 1, batch, lu_re, lu_im, lda, lu_stride, piv, piv_stride, dr, di, 1, x_stride, HBEM_TRANS_N,
+                         active, nullptr, st);
+        if (rc != HBEM_OK) break;
+        k_axpy_active<<<dim3((n + 255) / 256, batch), 256, 0, st>>>(n, x_re, x_im, x_stride, dr, di, active);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) { rc = cuda_fail(e, "k_axpy_active"); break; }
+        count_launch();
+    }
+    cudaFreeAsync(mem, st);
     return rc;
 }
 
@@ -2269,7 +2338,8 @@ int refine_noalloc(int n, int batch, const float *a_re, const float *a_im, long 
         cudaError_t e = cudaMemsetAsync(norms, 0, sizeof(double) * 2 * batch, st);
         if (e != cudaSuccess) { rc = cuda_fail(e, "hbem_refine_noalloc: memset"); break; }
         dim3 g((n * 32 + 255) / 256, batch);
-        k_residual<<<g, 256, 0, st>>>(n, a_re, a_im, lda, a_stride, b_re, b_im, b_stride, x_re, x_im, x_stride, dr, di, norms);
+        k_residual<<<g, 256, 0, st>>>(n, a_re, a_im, lda, a_stride, b_re, b_im, b_stride, x_re, x_im, x_stride, dr, di, norms,
+                                      it > 0 ? active : nullptr);
         e = cudaGetLastError();
         if (e != cudaSuccess) { rc = cuda_fail(e, "k_residual"); break; }
         count_launch();
@@ -2350,6 +2420,24 @@ extern "C" int hbem_refine(int n, int batch, const float *a_re, const float *a_i
         return fail(HBEM_ERR_ARG, "hbem_refine: lda/a_stride/lu_stride/piv_stride too small");
     return refine(n, batch, a_re, a_im, lda, a_stride, lu_re, lu_im, lu_stride, piv, piv_stride, b_re, b_im, b_stride,
                   x_re, x_im, x_stride, tol, max_iter, iters, resid, reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" int hbem_refine_async(int n, int batch, const float *a_re, const float *a_im, long long lda,
+                                 long long a_stride, const float *lu_re, const float *lu_im, long long lu_stride,
+                                 const int *piv, long long piv_stride, const float *b_re, const float *b_im,
+                                 long long b_stride, float *x_re, float *x_im, long long x_stride, double tol,
+                                 int max_iter, int *iters, double *resid, void *stream) {
+    keep_pool_memory();
+    if (n <= 0 || batch <= 0) return HBEM_OK;
+    if (!a_re || !a_im || !lu_re || !lu_im || !piv || !b_re || !b_im || !x_re || !x_im)
+        return fail(HBEM_ERR_ARG, "hbem_refine_async: NULL pointer");
+    if (x_stride < n || b_stride < n || max_iter < 0 || !(tol > 0))
+        return fail(HBEM_ERR_ARG, "hbem_refine_async: bad arguments");
+    if (lda < n || a_stride < lda * (long long)n || lu_stride < lda * (long long)n || piv_stride < n)
+        return fail(HBEM_ERR_ARG, "hbem_refine_async: lda/a_stride/lu_stride/piv_stride too small");
+    return refine_async(n, batch, a_re, a_im, lda, a_stride, lu_re, lu_im, lu_stride, piv, piv_stride, b_re, b_im,
+                        b_stride, x_re, x_im, x_stride, tol, max_iter, iters, resid,
+                        reinterpret_cast<cudaStream_t>(stream));
 }
 
 extern "C" int hbem_refine_noalloc(int n, int batch, const float *a_re, const float *a_im, long long lda,

@@ -74,6 +74,8 @@ _SIGNATURES = {
                      _c_ll, _c_d, _c_int, _vp, _vp, _vp], _c_int),
     "hbem_refine_noalloc": ([_c_int, _c_int, _vp, _vp, _c_ll, _c_ll, _vp, _vp, _c_ll, _vp, _c_ll, _vp, _vp, _c_ll, _vp,
                              _vp, _c_ll, _c_d, _c_int, _vp, _vp, _vp], _c_int),
+    "hbem_refine_async": ([_c_int, _c_int, _vp, _vp, _c_ll, _c_ll, _vp, _vp, _c_ll, _vp, _c_ll, _vp, _vp, _c_ll, _vp,
+                           _vp, _c_ll, _c_d, _c_int, _vp, _vp, _vp], _c_int),
     "hbem_field": ([_vp, _c_int, _vp, _vp, _vp, _c_ll, _vp, _vp, _c_ll, _vp, _c_int, _vp, _vp, _c_ll, _vp], _c_int),
     "hbem_reduce_tag_avg": ([_vp, _c_int, _vp, _vp, _c_ll, _vp, _c_int, _vp, _vp], _c_int),
     "hbem_solve_batch": ([_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _c_int, _vp, _c_int, _c_int, _c_d, _c_int, _vp, _vp,

@@ -252,6 +252,22 @@ int hbem_refine(int n, int batch, const float *a_re, const float *a_im, long lon
                 double tol, int max_iter, int *iters, double *resid, void *stream);
 
 /*
+ * hbem_refine without host synchronisation: same arguments, same stopping
+ * rule, applied on the device.  All max_iter passes are issued; a matrix that
+ * has stopped skips the rest of them (residual, wavefront solve blocks,
+ * update).  The call can be captured in a CUDA graph (its scratch is a
+ * stream-ordered allocation).  A timed-out wait of its triangular solves is
+ * reported by hbem_solve_status.  No counterpart in the reference, whose
+ * refinement runs on the host after a synchronous LAPACK solve.
+ */
+int hbem_refine_async(int n, int batch, const float *a_re, const float *a_im, long long lda, long long a_stride,
+                      const float *lu_re, const float *lu_im, long long lu_stride,
+                      const int *piv, long long piv_stride,
+                      const float *b_re, const float *b_im, long long b_stride,
+                      float *x_re, float *x_im, long long x_stride,
+                      double tol, int max_iter, int *iters, double *resid, void *stream);
+
+/*
  * 1-norm condition estimate, as LAPACK cgecon (norm '1') on the factors.
  * hbem_matrix_norm1: anorm[f] = ||A_f||_1 = max_j sum_i |a_ij| (clange '1'),
  *   device float (batch,), of the matrix BEFORE factorisation.

@@ -120,6 +120,9 @@ def test_entry_points_validate_arguments_before_any_device_work():
     assert lib.hbem_refine(*args, 0.0, 3, None, None, None) == -1 and "hbem_refine" in err()
     assert lib.hbem_refine(*args, 1e-6, -1, None, None, None) == -1 and "hbem_refine" in err()
     assert lib.hbem_refine_noalloc(*args, float("nan"), 3, None, None, None) == -1 and "noalloc" in err()
+    assert lib.hbem_refine_async(*args, 1e-6, -2, None, None, None) == -1 and "async" in err()
+    assert lib.hbem_refine_async(4, 1, D, D, 4, 16, D, D, 15, D, 4, D, D, 4, D, D, 4, 1e-6, 2, None, None,
+                                 None) == -1 and "too small" in err()
     # condition estimate: strides and the largest order its shared-memory vector holds
     assert lib.hbem_matrix_norm1(4, 1, D, D, 4, 15, D, None) == -1 and "bad strides" in err()
     n = 30000

@@ -71,3 +71,66 @@ def test_batched_graph_sweeps_match_eager(tuning, tmp_path):
         assert _rel(o.tag_average, t_ref) < tol
     if tuning == "auto":
         assert (tmp_path / "tune.json").exists()
+
+
+def _c3_case(seed: int, freqs_hz):
+    """One of the batching workload's seeded half (yz) waveguides at a few of its frequencies."""
+    import hornlab_metal_bem_b200 as hb
+    from hornlab_metal_bem_b200 import generators as G
+    from hornlab_metal_bem_b200.bie import build_source_face_scale
+    from hornlab_metal_bem_b200.geometry import build_geometry_buffers
+    from hornlab_metal_bem_b200.mesh import make_pure_function_spaces
+    from hornlab_metal_bem_b200.observation import build_observation_points
+    from hornlab_metal_bem_b200.sweep import field_points_3xn, k_values, neumann_rows
+
+    cfg = hb.native_config(freq_min_hz=500.0, freq_max_hz=20000.0, freq_count=40, source_motion="axial",
+                           native_symmetry_plane="yz", native_check_open_edges=False,
+                           observation=hb.ObservationConfig(planes=["horizontal", "vertical", "diagonal"],
+                                                            angle_count=37))
+    spec = G.horn_spec_from_seed(seed, edge=343.0 / 8000.0 / 6.0, flare_range=(10.0, 40.0),
+                                 mouth_range=(0.080, 0.200))
+    mesh = G.horn(spec, quarter=False, half=True)
+    frame = hb._resolve_frame(mesh, cfg)
+    obs, _ = build_observation_points(frame, cfg.observation)
+    p1, dp0 = make_pure_function_spaces(mesh.grid)
+    buf = build_geometry_buffers(mesh.grid, mesh.physical_tags, p1, dp0)
+    freqs = np.asarray(freqs_hz, np.float64)
+    k_re, _ = k_values(freqs, cfg)
+    scale = build_source_face_scale(mesh.grid, mesh.physical_tags, cfg, frame.axis, frame.source_center)
+    q = neumann_rows(buf.n_triangles, mesh.physical_tags, freqs, cfg, scale)
+    return SweepCase(buf, k_re, q, field_points_3xn(obs), sorted(cfg.velocity_sources), "yz")
+
+
+def _db(z):
+    return 20 * np.log10(np.abs(z))
+
+
+def test_batched_sweeps_match_oracle_on_waveguide_batch_meshes():
+    """The two smallest meshes of the 64-waveguide batch (seeds 43 and 0: 829 and 866 dofs), captured and
+    replayed with the device-side refinement, against the FP64 oracle (oracle assembly, LAPACK zgesv,
+    oracle field and tag averages) across the band, 20 kHz included."""
+    from oracle.oracle import Oracle, dense_solve
+
+    cases = [_c3_case(43, (2000.0, 12000.0, 20000.0)), _c3_case(0, (700.0, 16000.0))]
+    bs = BatchedSweeps(cases, n_streams=2, tuning=None)
+    try:
+        bs.run()
+        bs.run()
+        outs = bs.outputs()
+    finally:
+        bs.close()
+    for c, o in zip(cases, outs):
+        assert c.n in (829, 866)
+        assert np.all(o.lapack_info == 0)
+        assert np.all(o.refine_iterations >= 1)
+        assert np.all(o.refine_residual_rel < 1e-5)
+        orc = Oracle(c.buffers, 1, "f64")
+        for f in range(len(c.k_re)):
+            A, b = orc.corrected(float(c.k_re[f]), c.q[f], 0.0, None)
+            p = dense_solve(A, b, "f64")
+            fld = orc.field(float(c.k_re[f]), p, c.q[f].astype(np.complex128), c.obs)
+            assert _rel(o.field[f], fld) < 1e-4, (c.n, f)
+            assert np.max(np.abs(_db(o.field[f]) - _db(fld))) < 0.01
+            for t, tag in enumerate(c.tags):
+                ref = orc.tag_average(p, tag)
+                assert abs(o.tag_average[f, t] - ref) <= 1e-4 * abs(ref), (c.n, f, tag)
