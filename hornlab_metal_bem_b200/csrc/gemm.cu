@@ -148,21 +148,27 @@ int launch_trailing_update(int n, int batch, int k0, int kw, int start, int col_
 }  // namespace hbem
 
 // ===========================================================================
-// Tensor-core trailing update (tcgen05, BF16x3 split products, FP32 TMEM
-// accumulation) for the mixed-precision LU.
+// Tensor-core trailing update (tcgen05, split products, FP32 TMEM
+// accumulation): BF16x3 for the mixed-precision LU, TF32x3 (FP32-class
+// products: each split keeps 11 significant bits, so hi + lo carries 22 and
+// the dropped lo x lo term is below 2^-22 of the product) for the plain LU.
 //
 // The complex update C -= L U is one real GEMM: for a tile of 64 complex rows
 // the 128 MMA rows are [Lr, -Li] (real part) and [Li, Lr] (imaginary part)
 // against B = [Ur; Ui] (K = 2 x 64).  Each FP32 operand x is split into
 // hi = bf16(x) and lo = bf16(x - hi); A B ~ Ah Bh + Ah Bl + Al Bh.  The packed
 // operands hold each split once, A2 = [Ah | Al] and B2^T = [Bh | Bl] (both
-// K-major, K = 256, written by k_pack_*); the three products are three MMA
-// groups over the same shared-memory blocks.  Tiles are 64 complex rows x 64
-// columns; a CTA takes work units of consecutive column tiles of one row block
-// and keeps that row block's A2 (64 KB) resident in shared memory while B2
-// streams through a ring (k_trailing_tc: TMA, single-thread MMA issue into
-// 128 x 64 FP32 TMEM accumulators, C staged through shared memory by the
-// epilogue warps).
+// K-major, 256 elements per row, written by k_pack_*); the three products are
+// three MMA groups over the same shared-memory blocks.  A CTA takes work units
+// of consecutive column tiles of one row block and keeps that row block's A2
+// resident in shared memory while B2 streams through a ring (k_trailing_tc:
+// TMA, single-thread MMA issue into two FP32 TMEM accumulators, C staged
+// through shared memory by the epilogue warps).  Per variant (the same 224 KB
+// of shared memory):
+//   BF16x3: tiles of 64 complex rows x 64 columns, A2 64 KB (4 K-blocks of
+//           128 bytes per row), ring of 6 x 16 KB, two 32 KB C tiles;
+//   TF32x3: tiles of 64 complex rows x 32 columns, A2 128 KB (8 K-blocks),
+//           ring of 8 x 8 KB, two 16 KB C tiles.
 // Every mbarrier wait is bounded; a timeout sets the status word and the CTA
 // returns after releasing its TMEM.
 // ===========================================================================
@@ -170,19 +176,27 @@ namespace hbem {
 namespace {
 
 constexpr int kTcM = 128;          // MMA rows per tile (64 complex rows: real and imaginary parts)
-constexpr int kTcN = 64;           // columns per tile
-constexpr int kTcKBlk = 64;        // bf16 elements per K-block (128 bytes)
-constexpr int kTcK2 = 256;         // packed K: hi (2 x 64) then lo (2 x 64)
-constexpr int kTcABlk = kTcM * kTcKBlk * 2;      // one A K-block, 16 KB
-constexpr int kTcABytes = 4 * kTcABlk;           // resident A2 of a row block, 64 KB
-constexpr int kTcBBlk = kTcN * kTcKBlk * 2;      // one B K-block, 8 KB
-constexpr int kTcStageBytes = 2 * kTcBBlk;       // ring stage: Bh and Bl of one K half
-constexpr int kTcStages = 6;       // B ring: three tiles ahead
-constexpr int kTcCBytes = kTcM * kTcN * 4;   // one C tile staged in shared memory
+constexpr int kTcK2 = 256;         // packed elements per row: hi (real K = 128) then lo
+constexpr int kTcABlk = kTcM * 128;  // one A K-block (128 bytes per row), 16 KB
 constexpr int kTcThreads = 320;    // warp 0: MMA issuer, warp 1: TMA producer, warps 2-9: C tiles
-constexpr size_t kTcSmem = (size_t)kTcABytes + (size_t)kTcStages * kTcStageBytes + 2 * kTcCBytes + 1024;
-static_assert(kTcSmem <= 227 * 1024, "tensor-core trailing update: shared memory");
 constexpr long long kSpinLimit = 1LL << 24;
+
+// Shapes of the two variants (see above).
+template <bool TF32>
+struct TcCfg {
+    static constexpr int ES = TF32 ? 4 : 2;            // operand bytes
+    static constexpr int EPB = 128 / ES;               // operand elements per 128-byte K-block
+    static constexpr int KBH = 128 / EPB;              // K-blocks of one split (real K = 128)
+    static constexpr int N = TF32 ? 32 : 64;           // columns per tile
+    static constexpr int ABytes = 2 * KBH * kTcABlk;   // resident A2 of a row block
+    static constexpr int BBlk = N * 128;               // one B K-block
+    static constexpr int StageBytes = 2 * BBlk;        // ring stage: Bh and Bl of one K-block
+    static constexpr int Stages = TF32 ? 8 : 6;        // B ring: two (TF32) / three (BF16) tiles ahead
+    static constexpr int CBytes = kTcM * N * 4;        // one C tile staged in shared memory
+    static constexpr int Fmt = TF32 ? 2 : 1;           // instruction-descriptor operand format
+    static constexpr size_t Smem = (size_t)ABytes + (size_t)Stages * StageBytes + 2 * (size_t)CBytes + 1024;
+    static_assert(Smem <= 227 * 1024, "tensor-core trailing update: shared memory");
+};
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -218,9 +232,11 @@ __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
     return d;
 }
 
-// kind::f16 instruction descriptor: BF16 A/B, FP32 accumulate, K-major A/B.
-__host__ __device__ constexpr uint32_t umma_idesc_bf16(int m, int n) {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+// Instruction descriptor: FP32 accumulate, K-major A/B of operand format
+// fmt (kind::f16 with 1 = BF16, kind::tf32 with 2 = TF32), M x N.
+__host__ __device__ constexpr uint32_t umma_idesc(int m, int n, int fmt) {
+    return (1u << 4) | ((uint32_t)fmt << 7) | ((uint32_t)fmt << 10) | ((uint32_t)(n >> 3) << 17) |
+           ((uint32_t)(m >> 4) << 24);
 }
 
 __device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
@@ -276,12 +292,12 @@ struct TcWalk {
 };
 
 // Persistent trailing update over work units (see TcWalk).
-//   warp 1 (TMA producer): per unit, the row block's four A2 K-blocks into the
-//     resident A buffer (after the MMAs of the previous unit released it),
-//     then per tile the two K halves of B2 (Bh and Bl blocks) through a
-//     6-stage ring, running ahead across tiles;
-//   warp 0 (MMA issuer): per K half, Ah Bh + Ah Bl + Al Bh as 3 x 4
-//     tcgen05.mma (M = 128, N = 64, K = 16) into one of two TMEM
+//   warp 1 (TMA producer): per unit, the row block's 2 KBH A2 K-blocks into
+//     the resident A buffer (after the MMAs of the previous unit released
+//     it), then per tile the KBH K-blocks of B2 (Bh and Bl blocks per ring
+//     stage), running ahead across tiles;
+//   warp 0 (MMA issuer): per K-block, Ah Bh + Ah Bl + Al Bh as 3 x 4
+//     tcgen05.mma (M = 128, N, 32 bytes of K each) into one of two TMEM
 //     accumulators, releases ring slots with tcgen05.commit, signals
 //     "accumulator full", and releases A after a unit's last tile;
 //   warps 2-9 (C tiles): prefetch the next tile's C (real rows, then
@@ -292,12 +308,16 @@ struct TcWalk {
 // g ^ (r & 7) (aligned 16-byte copies, conflict-free float4 drain).  Every
 // wait is bounded; a timeout sets *status and the roles stop, drain their
 // copies, free TMEM and return.
+template <bool TF32>
 __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_constant__ CUtensorMap tmA,
                                                                 const __grid_constant__ CUtensorMap tmB, float *a_re,
                                                                 float *a_im, long long lda, long long a_stride, int n,
                                                                 int start, int col_start, int col_end, int rows3,
                                                                 int cols_pad, int tiles_m, int tiles_n, int n_chunks,
                                                                 int chunk, int n_units, int *status) {
+    using Cfg = TcCfg<TF32>;
+    constexpr int kTcN = Cfg::N, kTcStages = Cfg::Stages, kTcStageBytes = Cfg::StageBytes, kTcABytes = Cfg::ABytes;
+    constexpr int KBH = Cfg::KBH, EPB = Cfg::EPB;
     extern __shared__ uint8_t s_raw[];
     __shared__ uint64_t s_full[kTcStages], s_empty[kTcStages];
     __shared__ uint64_t s_acc_full[2], s_acc_empty[2];
@@ -356,18 +376,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
                     const int row_a = w.mat * rows3 + w.tm * kTcM;
                     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kTcABytes)
                                  : "memory");
-                    for (int kb = 0; kb < 4; ++kb)
+                    for (int kb = 0; kb < 2 * KBH; ++kb)
                         asm volatile(
                             "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
                             ::"r"(smem_u32(sA + (size_t)kb * kTcABlk)), "l"(reinterpret_cast<uint64_t>(&tmA)),
-                              "r"(kb * kTcKBlk), "r"(row_a), "r"(bar)
+                              "r"(kb * EPB), "r"(row_a), "r"(bar)
                             : "memory");
                     ++units;
                 }
                 bool last;
                 do {
                     const int row_b = w.mat * cols_pad + w.tn * kTcN;
-                    for (int kh = 0; kh < 2; ++kh, ++g) {
+                    for (int kh = 0; kh < KBH; ++kh, ++g) {
                         const int s = (int)(g % kTcStages);
                         const int u = (int)(g / kTcStages);
                         if (u > 0 && !mbar_wait(smem_u32(&s_empty[s]), (u - 1) & 1, &s_fail)) { ok = false; break; }
@@ -376,16 +396,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
                         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
                                      "r"(kTcStageBytes)
                                      : "memory");
-                        // Bh of this K half, then Bl
+                        // Bh of this K-block, then Bl
                         asm volatile(
                             "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
-                            ::"r"(smem_u32(sb)), "l"(reinterpret_cast<uint64_t>(&tmB)), "r"(kh * kTcKBlk),
+                            ::"r"(smem_u32(sb)), "l"(reinterpret_cast<uint64_t>(&tmB)), "r"(kh * EPB),
                               "r"(row_b), "r"(bar)
                             : "memory");
                         asm volatile(
                             "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
-                            ::"r"(smem_u32(sb + kTcBBlk)), "l"(reinterpret_cast<uint64_t>(&tmB)),
-                              "r"(128 + kh * kTcKBlk), "r"(row_b), "r"(bar)
+                            ::"r"(smem_u32(sb + Cfg::BBlk)), "l"(reinterpret_cast<uint64_t>(&tmB)),
+                              "r"((KBH + kh) * EPB), "r"(row_b), "r"(bar)
                             : "memory");
                         last_use[s] = u;
                     }
@@ -405,7 +425,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
     } else if (warp == 0) {
         // ---- MMA issuer
         if (lane == 0) {
-            constexpr uint32_t idesc = umma_idesc_bf16(kTcM, kTcN);
+            constexpr uint32_t idesc = umma_idesc(kTcM, kTcN, Cfg::Fmt);
             bool ok = true;
             long long g = 0;
             int i = 0;        // tiles
@@ -424,29 +444,37 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                     const uint32_t acc_addr = tmem + (uint32_t)(b * kTcN);
-                    for (int kh = 0; kh < 2; ++kh, ++g) {
+                    for (int kh = 0; kh < KBH; ++kh, ++g) {
                         const int s = (int)(g % kTcStages);
                         const int u = (int)(g / kTcStages);
                         if (!mbar_wait(smem_u32(&s_full[s]), u & 1, &s_fail)) { ok = false; break; }
                         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                         const uint32_t sb = smem_u32(ring + (size_t)s * kTcStageBytes);
-                        // (A block, B block): Ah Bh, Ah Bl, Al Bh of this K half
+                        // (A block, B block): Ah Bh, Ah Bl, Al Bh of this K-block
                         const uint32_t pa[3] = {a0 + (uint32_t)(kh * kTcABlk), a0 + (uint32_t)(kh * kTcABlk),
-                                                a0 + (uint32_t)((2 + kh) * kTcABlk)};
-                        const uint32_t pb[3] = {sb, sb + (uint32_t)kTcBBlk, sb};
+                                                a0 + (uint32_t)((KBH + kh) * kTcABlk)};
+                        const uint32_t pb[3] = {sb, sb + (uint32_t)Cfg::BBlk, sb};
 #pragma unroll
                         for (int pr = 0; pr < 3; ++pr) {
 #pragma unroll
-                            for (int kk = 0; kk < kTcKBlk / 16; ++kk) {
+                            for (int kk = 0; kk < 4; ++kk) {   // 32 bytes of K per instruction
                                 const uint64_t da = umma_desc_sw128(pa[pr] + kk * 32);
                                 const uint64_t db = umma_desc_sw128(pb[pr] + kk * 32);
                                 const uint32_t acc = (kh > 0 || pr > 0 || kk > 0) ? 1u : 0u;
-                                asm volatile(
-                                    "{\n\t.reg .pred p;\n\t"
-                                    "setp.ne.b32 p, %4, 0;\n\t"
-                                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-                                    ::"r"(acc_addr), "l"(da), "l"(db), "r"(idesc), "r"(acc)
-                                    : "memory");
+                                if (TF32)
+                                    asm volatile(
+                                        "{\n\t.reg .pred p;\n\t"
+                                        "setp.ne.b32 p, %4, 0;\n\t"
+                                        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+                                        ::"r"(acc_addr), "l"(da), "l"(db), "r"(idesc), "r"(acc)
+                                        : "memory");
+                                else
+                                    asm volatile(
+                                        "{\n\t.reg .pred p;\n\t"
+                                        "setp.ne.b32 p, %4, 0;\n\t"
+                                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                                        ::"r"(acc_addr), "l"(da), "l"(db), "r"(idesc), "r"(acc)
+                                        : "memory");
                             }
                         }
                         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -479,13 +507,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
             mbar_wait(smem_u32(&s_done), 0);
         }
     } else {
-        // ---- C tiles: 8 warps; thread et owns column group gq = et & 15 of
-        // rows (et >> 4) + 16 it; warp pair (w, w + 4) shares TMEM lane
-        // quarter w & 3 and drains columns [32 h, 32 h + 32), h = (w - 2) >> 2.
+        // ---- C tiles: 8 warps; thread et owns column group gq = et % GQ (4
+        // columns) of rows et / GQ + RS it; warp pair (w, w + 4) shares TMEM
+        // lane quarter w & 3 and drains the columns [N/2 h, N/2 h + N/2),
+        // h = (w - 2) >> 2.
+        constexpr int GQ = kTcN / 4, RS = 256 / GQ, HALF = kTcN / 2;
         const int et = tid - 64;   // 0..255
         const int q = warp & 3;
         const int h = (warp - 2) >> 2;
-        const int gq = et & 15, r_first = et >> 4;
+        const int gq = et % GQ, r_first = et / GQ;
         auto sidx = [](int r, int c) { return r * kTcN + ((((c >> 2) ^ (r & 7)) << 2) | (c & 3)); };
         auto prefetch = [&](const TcTile tt, float *sC) {
             const int row_c0 = start + tt.tm * 64, gcol = col_start + tt.tn * kTcN + 4 * gq;
@@ -496,8 +526,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
             const bool full4 = gcol + 3 < col_end;
             const float *mre = a_re + (size_t)tt.mat * a_stride + gcol, *mim = a_im + (size_t)tt.mat * a_stride + gcol;
 #pragma unroll
-            for (int it = 0; it < kTcM / 16; ++it) {
-                const int r = r_first + 16 * it;
+            for (int it = 0; it < kTcM / RS; ++it) {
+                const int r = r_first + RS * it;
                 const int grow = row_c0 + (r & 63);
                 if (grow >= n) continue;
                 const float *src = ((r < 64) ? mre : mim) + (size_t)grow * lda;
@@ -542,22 +572,31 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             {
                 const int r = q * 32 + lane;
-                const int c0 = 32 * h;
-                uint32_t v[32];
+                const int c0 = HALF * h;
+                uint32_t v[HALF];
                 const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * kTcN + c0);
-                asm volatile(
-                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
-                    "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
-                    "[%32];"
-                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-                      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
-                      "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
-                      "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
-                      "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-                    : "r"(taddr));
+                if constexpr (HALF == 32)
+                    asm volatile(
+                        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+                        "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
+                        "%30, %31}, [%32];"
+                        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                          "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]),
+                          "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
+                          "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                        : "r"(taddr));
+                else
+                    asm volatile(
+                        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+                        "%12, %13, %14, %15}, [%16];"
+                        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                          "=r"(v[14]), "=r"(v[15])
+                        : "r"(taddr));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-                for (int jj = 0; jj < 8; ++jj) {
+                for (int jj = 0; jj < HALF / 4; ++jj) {
                     float4 *p4 = reinterpret_cast<float4 *>(sC + sidx(r, c0 + 4 * jj));
                     float4 cv = *p4;
                     cv.x -= __uint_as_float(v[4 * jj]);
@@ -580,8 +619,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
                     const bool full4 = gcol + 3 < col_end;
                     float *mre = a_re + (size_t)tt.mat * a_stride + gcol, *mim = a_im + (size_t)tt.mat * a_stride + gcol;
 #pragma unroll
-                    for (int it = 0; it < kTcM / 16; ++it) {
-                        const int r = r_first + 16 * it;
+                    for (int it = 0; it < kTcM / RS; ++it) {
+                        const int r = r_first + RS * it;
                         const int grow = row_c0 + (r & 63);
                         if (grow >= n) continue;
                         float *dst = ((r < 64) ? mre : mim) + (size_t)grow * lda;
@@ -607,9 +646,42 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kTcN));
 }
 
-// Pack L21 (rows start..n, cols k0..k0+64) into A2 (K-major, bf16 hi/lo).
+// Operand splits: hi = x rounded to the operand format, lo = (x - hi) rounded
+// (x - hi is exact in FP32).  TF32 rounding keeps 10 fraction bits, to
+// nearest with ties away from zero: half the weight of the 13 dropped bits is
+// added to the FP32 pattern before they are cleared (finite x).
+__device__ __forceinline__ float tf32_round(float x) {
+    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+}
+
+template <bool TF32>
+struct TcSplit;
+template <>
+struct TcSplit<false> {
+    using T = __nv_bfloat16;
+    __device__ static T hi(float x) { return __float2bfloat16_rn(x); }
+    __device__ static float val(T h) { return __bfloat162float(h); }
+    __device__ static void store2(T *p, T a, T b) {
+        __nv_bfloat162 v;
+        v.x = a;
+        v.y = b;
+        *reinterpret_cast<__nv_bfloat162 *>(p) = v;
+    }
+};
+template <>
+struct TcSplit<true> {
+    using T = float;
+    __device__ static T hi(float x) { return tf32_round(x); }
+    __device__ static float val(T h) { return h; }
+    __device__ static void store2(T *p, T a, T b) { *reinterpret_cast<float2 *>(p) = make_float2(a, b); }
+};
+
+// Pack L21 (rows start..n, cols k0..k0+64) into A2 (K-major, hi/lo splits).
+template <bool TF32>
 __global__ void k_pack_a(const float *a_re, const float *a_im, long long lda, long long a_stride, int n, int start,
-                         int k0, int rows3, int rows_used, __nv_bfloat16 *A2) {
+                         int k0, int rows3, int rows_used, typename TcSplit<TF32>::T *A2) {
+    using S = TcSplit<TF32>;
+    using T = typename S::T;
     const int mat = blockIdx.z;
     const int i = blockIdx.x * blockDim.y + threadIdx.y;  // complex row offset
     const int k = threadIdx.x;                            // 0..63
@@ -621,13 +693,12 @@ __global__ void k_pack_a(const float *a_re, const float *a_im, long long lda, lo
         li = a_im[(size_t)mat * a_stride + (size_t)(start + i) * lda + k0 + k];
     }
     const int t = i >> 6, rl = i & 63;
-    __nv_bfloat16 *re_row = A2 + ((size_t)mat * rows3 + (size_t)t * 128 + rl) * kTcK2;
-    __nv_bfloat16 *im_row = re_row + (size_t)64 * kTcK2;
-    auto put = [](__nv_bfloat16 *row, int k2, float x) {
-        const __nv_bfloat16 h = __float2bfloat16_rn(x);
-        const __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
+    T *re_row = A2 + ((size_t)mat * rows3 + (size_t)t * 128 + rl) * kTcK2;
+    T *im_row = re_row + (size_t)64 * kTcK2;
+    auto put = [](T *row, int k2, float x) {
+        const T h = S::hi(x);
         row[k2] = h;
-        row[128 + k2] = l;
+        row[128 + k2] = S::hi(x - S::val(h));
     };
     put(re_row, k, lr);
     put(re_row, 64 + k, -li);
@@ -635,13 +706,16 @@ __global__ void k_pack_a(const float *a_re, const float *a_im, long long lda, lo
     put(im_row, 64 + k, lr);
 }
 
-// Pack U12 (rows k0..k0+64, cols start..col_end) into B2^T (K-major, bf16 hi/lo).
+// Pack U12 (rows k0..k0+64, cols start..col_end) into B2^T (K-major, hi/lo splits).
+template <bool TF32>
 __global__ void __launch_bounds__(256) k_pack_b(const float *a_re, const float *a_im, long long lda,
                                                 long long a_stride, int start, int col_end, int k0, int cols_pad,
-                                                int cols_used, __nv_bfloat16 *B2) {
+                                                int cols_used, typename TcSplit<TF32>::T *B2) {
     // 64 columns per CTA: the 64 x 64 block of U12 is read along its rows
     // (coalesced), transposed in shared memory and written as 64 packed
-    // K-major rows of 512 bytes (consecutive threads, consecutive bf16 pairs)
+    // K-major rows of 256 elements (consecutive threads, consecutive pairs)
+    using S = TcSplit<TF32>;
+    using T = typename S::T;
     __shared__ float s_ur[64][65], s_ui[64][65];
     const int mat = blockIdx.z;
     const int j0 = blockIdx.x * 64;
@@ -665,15 +739,12 @@ __global__ void __launch_bounds__(256) k_pack_b(const float *a_re, const float *
         if (j >= cols_used) break;
         const float x0 = (part & 1) ? s_ui[k][jj] : s_ur[k][jj];
         const float x1 = (part & 1) ? s_ui[k + 1][jj] : s_ur[k + 1][jj];
-        __nv_bfloat16 v0 = __float2bfloat16_rn(x0), v1 = __float2bfloat16_rn(x1);
+        T v0 = S::hi(x0), v1 = S::hi(x1);
         if (part >= 2) {
-            v0 = __float2bfloat16_rn(x0 - __bfloat162float(v0));
-            v1 = __float2bfloat16_rn(x1 - __bfloat162float(v1));
+            v0 = S::hi(x0 - S::val(v0));
+            v1 = S::hi(x1 - S::val(v1));
         }
-        __nv_bfloat162 pr;
-        pr.x = v0;
-        pr.y = v1;
-        *reinterpret_cast<__nv_bfloat162 *>(B2 + ((size_t)mat * cols_pad + j) * kTcK2 + kk) = pr;
+        S::store2(B2 + ((size_t)mat * cols_pad + j) * kTcK2 + kk, v0, v1);
     }
 }
 
@@ -695,14 +766,16 @@ EncodeTiledFn encode_fn() {
     return fn;
 }
 
-int make_map(CUtensorMap *map, void *ptr, long long rows, int box_rows) {
+// Packed rows of kTcK2 elements of es bytes; boxes of one 128-byte K-block x box_rows.
+int make_map(CUtensorMap *map, void *ptr, long long rows, int box_rows, int es) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return fail(HBEM_ERR_CUDA, "cuTensorMapEncodeTiled entry point unavailable");
     const cuuint64_t dims[2] = {(cuuint64_t)kTcK2, (cuuint64_t)rows};
-    const cuuint64_t strides[1] = {(cuuint64_t)kTcK2 * 2};
-    const cuuint32_t box[2] = {(cuuint32_t)kTcKBlk, (cuuint32_t)box_rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)kTcK2 * es};
+    const cuuint32_t box[2] = {(cuuint32_t)(128 / es), (cuuint32_t)box_rows};
     const cuuint32_t estr[2] = {1, 1};
-    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, ptr, dims, strides, box, estr,
+    CUresult r = fn(map, es == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, ptr, dims,
+                    strides, box, estr,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(HBEM_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
@@ -713,27 +786,31 @@ int make_map(CUtensorMap *map, void *ptr, long long rows, int box_rows) {
 
 // Packed-operand workspace and tensor maps for one factorisation: sized for
 // the first (largest) trailing update and reused by the later, smaller ones.
+// tf32: TF32x3 operands (plain LU) instead of BF16x3 (mixed LU).
 struct TcWorkspace {
-    __nv_bfloat16 *A2 = nullptr, *B2 = nullptr;
+    void *A2 = nullptr, *B2 = nullptr;
     int rows3 = 0, cols_pad = 0, batch = 0;
+    bool tf32 = false;
     CUtensorMap ma, mb;
 };
 
-int tc_workspace_create(int n, int batch, TcWorkspace **out, cudaStream_t st) {
+int tc_workspace_create(int n, int batch, bool tf32, TcWorkspace **out, cudaStream_t st) {
     *out = nullptr;
     auto *w = new TcWorkspace();
+    const int tn = tf32 ? TcCfg<true>::N : TcCfg<false>::N, es = tf32 ? 4 : 2;
+    w->tf32 = tf32;
     w->rows3 = ((n + 63) / 64) * kTcM;
-    w->cols_pad = ((n + kTcN - 1) / kTcN) * kTcN;
+    w->cols_pad = ((n + tn - 1) / tn) * tn;
     w->batch = batch;
-    cudaError_t e = cudaMallocAsync((void **)&w->A2, (size_t)batch * w->rows3 * kTcK2 * 2, st);
-    if (e == cudaSuccess) e = cudaMallocAsync((void **)&w->B2, (size_t)batch * w->cols_pad * kTcK2 * 2, st);
+    cudaError_t e = cudaMallocAsync(&w->A2, (size_t)batch * w->rows3 * kTcK2 * es, st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&w->B2, (size_t)batch * w->cols_pad * kTcK2 * es, st);
     if (e != cudaSuccess) {
         if (w->A2) cudaFreeAsync(w->A2, st);
         delete w;
         return cuda_fail(e, "tensor-core workspace");
     }
-    int rc = make_map(&w->ma, w->A2, (long long)batch * w->rows3, kTcM);
-    if (rc == HBEM_OK) rc = make_map(&w->mb, w->B2, (long long)batch * w->cols_pad, kTcN);
+    int rc = make_map(&w->ma, w->A2, (long long)batch * w->rows3, kTcM, es);
+    if (rc == HBEM_OK) rc = make_map(&w->mb, w->B2, (long long)batch * w->cols_pad, tn, es);
     if (rc != HBEM_OK) {
         cudaFreeAsync(w->A2, st);
         cudaFreeAsync(w->B2, st);
@@ -751,26 +828,27 @@ void tc_workspace_destroy(TcWorkspace *w, cudaStream_t st) {
     delete w;
 }
 
-// Mixed-precision trailing update with K = 64 (one LU block); status
-// receives 1/2 if a barrier wait timed out.  The persistent grid leaves
-// reserve_sms SMs (at most half of them) to kernels on other streams.
-// A[start:n, col_start:col_end] -= L[start:n, k0:k0+64] U[k0:k0+64, col_start:col_end] on the tensor cores
-int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int col_start, int col_end, float *a_re,
-                       float *a_im, long long lda, long long a_stride, int *status, cudaStream_t st,
-                       int reserve_sms) {
+namespace {
+
+template <bool TF32>
+int launch_trailing_tc_t(TcWorkspace *w, int n, int batch, int k0, int start, int col_start, int col_end,
+                         float *a_re, float *a_im, long long lda, long long a_stride, int *status, cudaStream_t st,
+                         int reserve_sms) {
+    using Cfg = TcCfg<TF32>;
+    using T = typename TcSplit<TF32>::T;
     const int m = n - start, wd = col_end - col_start;
-    if (m <= 0 || wd <= 0) return HBEM_OK;
-    const int tiles_m = (m + 63) / 64, tiles_n = (wd + kTcN - 1) / kTcN;
+    const int tiles_m = (m + 63) / 64, tiles_n = (wd + Cfg::N - 1) / Cfg::N;
     // packed rows use the workspace's fixed per-matrix pitch (rows3 / cols_pad)
     {
         dim3 blk(64, 4), grd((tiles_m * 64 + 3) / 4, 1, batch);
-        k_pack_a<<<grd, blk, 0, st>>>(a_re, a_im, lda, a_stride, n, start, k0, w->rows3, tiles_m * 64, w->A2);
+        k_pack_a<TF32><<<grd, blk, 0, st>>>(a_re, a_im, lda, a_stride, n, start, k0, w->rows3, tiles_m * 64,
+                                            static_cast<T *>(w->A2));
         HBEM_LAUNCH_CHECK("k_pack_a");
     }
     {
-        dim3 grd((tiles_n * kTcN + 63) / 64, 1, batch);
-        k_pack_b<<<grd, 256, 0, st>>>(a_re, a_im, lda, a_stride, col_start, col_end, k0, w->cols_pad, tiles_n * kTcN,
-                                      w->B2);
+        dim3 grd((tiles_n * Cfg::N + 63) / 64, 1, batch);
+        k_pack_b<TF32><<<grd, 256, 0, st>>>(a_re, a_im, lda, a_stride, col_start, col_end, k0, w->cols_pad,
+                                            tiles_n * Cfg::N, static_cast<T *>(w->B2));
         HBEM_LAUNCH_CHECK("k_pack_b");
     }
     int n_sm = 0;
@@ -778,7 +856,7 @@ int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int 
         int dev = 0;
         HBEM_CUDA(cudaGetDevice(&dev));
         HBEM_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
-        const int rc = func_opt_in((const void *)k_trailing_tc, (int)kTcSmem);
+        const int rc = func_opt_in((const void *)k_trailing_tc<TF32>, (int)Cfg::Smem);
         if (rc != HBEM_OK) return rc;
     }
     const int ctas = n_sm - std::min(std::max(reserve_sms, 0), n_sm / 2);
@@ -793,11 +871,28 @@ int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int 
     if (units > 0x7fffffffLL) return fail(HBEM_ERR_ARG, "trailing update: too many tiles");
     if ((long long)(n_chunks - 1) * chunk >= tiles_n) return fail(HBEM_ERR_STATE, "trailing update: empty work unit");
     const int grid = (int)std::min<long long>(units, ctas);
-    k_trailing_tc<<<grid, kTcThreads, kTcSmem, st>>>(w->ma, w->mb, a_re, a_im, lda, a_stride, n, start, col_start,
-                                                    col_end, w->rows3, w->cols_pad, tiles_m, tiles_n, n_chunks, chunk,
-                                                    (int)units, status);
+    k_trailing_tc<TF32><<<grid, kTcThreads, Cfg::Smem, st>>>(w->ma, w->mb, a_re, a_im, lda, a_stride, n, start,
+                                                              col_start, col_end, w->rows3, w->cols_pad, tiles_m,
+                                                              tiles_n, n_chunks, chunk, (int)units, status);
     HBEM_LAUNCH_CHECK("k_trailing_tc");
     return HBEM_OK;
+}
+
+}  // namespace
+
+// Tensor-core trailing update with K = 64 (one LU block), BF16x3 or TF32x3 by
+// the workspace; status receives 1/2/3 if a barrier wait timed out.  The
+// persistent grid leaves reserve_sms SMs (at most half of them) to kernels on
+// other streams.
+// A[start:n, col_start:col_end] -= L[start:n, k0:k0+64] U[k0:k0+64, col_start:col_end]
+int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int col_start, int col_end, float *a_re,
+                       float *a_im, long long lda, long long a_stride, int *status, cudaStream_t st,
+                       int reserve_sms) {
+    if (n - start <= 0 || col_end - col_start <= 0) return HBEM_OK;
+    return w->tf32 ? launch_trailing_tc_t<true>(w, n, batch, k0, start, col_start, col_end, a_re, a_im, lda, a_stride,
+                                                status, st, reserve_sms)
+                   : launch_trailing_tc_t<false>(w, n, batch, k0, start, col_start, col_end, a_re, a_im, lda,
+                                                 a_stride, status, st, reserve_sms);
 }
 
 }  // namespace hbem

@@ -34,7 +34,7 @@ namespace hbem {
 
 // A[start:n, start:col_end] -= A[start:n, k0:k0+kw] * A[k0:k0+kw, start:col_end]
 struct TcWorkspace;
-int tc_workspace_create(int n, int batch, TcWorkspace **out, cudaStream_t st);
+int tc_workspace_create(int n, int batch, bool tf32, TcWorkspace **out, cudaStream_t st);
 void tc_workspace_destroy(TcWorkspace *w, cudaStream_t st);
 int launch_trailing_update(int n, int batch, int k0, int kw, int start, int col_end, float *a_re, float *a_im,
                            long long lda, long long a_stride, TcWorkspace *tc, int *status, cudaStream_t st);
@@ -1824,6 +1824,15 @@ static int lookahead_streams(cudaStream_t key, LookaheadStreams **out) {
     return HBEM_OK;
 }
 
+// The plain LU's look-ahead bulk update on the tensor cores (TF32x3) unless
+// exact FP32 products are asked for: measured on one B200, n = 1043 x 40
+// factors in 6.7 instead of 7.3 ms, 4096 x 4 in 28.2 instead of 29.6 ms and
+// 18 749 x 2 in 701 instead of 1130 ms, with residuals of 6e-7 to 1e-6
+// against 4e-7 to 9e-7 for the CUDA-core update.
+static bool plain_update_on_tensor_cores() {
+    return tuning(HBEM_TUNE_LU_UPDATE) != 1;
+}
+
 int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long long a_stride, int *piv,
               long long piv_stride, int *info, int precision, cudaStream_t st) {
     // Two-level blocking: 64-column blocks whose (n - b0) x 64 panel is
@@ -1840,14 +1849,17 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
     const size_t smem_cap = 200 * 1024;
     constexpr int NB = 64;
     HBEM_CUDA(cudaMemsetAsync(info, 0, sizeof(int) * batch, st));
-    // mixed precision: K = 64 block updates run on the tensor cores; their
-    // barrier waits report through this status word
+    // K = 64 block updates on the tensor cores: BF16x3 (mixed precision), or
+    // TF32x3 for the plain LU's look-ahead bulk when selected; their barrier
+    // waits report through this status word
     int *status = nullptr;
     TcWorkspace *tc = nullptr;
-    if (precision == HBEM_PREC_MIXED && n > 64) {
+    const bool tf32_bulk = precision == HBEM_PREC_PLAIN && n > 2 * NB && tuning(HBEM_TUNE_LU_LOOKAHEAD) != 1 &&
+                           plain_update_on_tensor_cores();
+    if ((precision == HBEM_PREC_MIXED && n > 64) || tf32_bulk) {
         HBEM_CUDA(cudaMallocAsync((void **)&status, sizeof(int), st));
         HBEM_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
-        int rc = tc_workspace_create(n, batch, &tc, st);
+        int rc = tc_workspace_create(n, batch, tf32_bulk, &tc, st);
         if (rc != HBEM_OK) {
             cudaFreeAsync(status, st);
             return rc;
@@ -1951,8 +1963,12 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
         }
         const int outside = n - bw;
         const int next_end = std::min(n, b0 + bw + NB);
-        // SMs the persistent tensor-core update leaves to the chain
-        const int tc_reserve = tuning(HBEM_TUNE_LU_RESERVE) - 1;
+        // SMs the persistent tensor-core update leaves to the chain: by
+        // default 32 for the TF32x3 bulk of small matrices (n = 1043 x 40:
+        // 6.74 -> 6.46 ms), whose chain of panels is the longer path
+        const int tc_reserve = tuning(HBEM_TUNE_LU_RESERVE) > 0 ? tuning(HBEM_TUNE_LU_RESERVE) - 1
+                               : (tf32_bulk && n < 2048)       ? 32
+                                                                : 0;
         const bool split = la && next_end < n;
         if (outside > 0) {
             // with look-ahead the chain swaps (and solves) only the next block's

@@ -365,6 +365,9 @@ extern "C" int hbem_set_tuning(int key, int value) {
         case HBEM_TUNE_WAVE_SPIN:
             if (value < 0 || value > (1 << 22)) return fail(HBEM_ERR_ARG, "HBEM_TUNE_WAVE_SPIN: 0 .. 4194304");
             break;
+        case HBEM_TUNE_LU_UPDATE:
+            if (value < 0 || value > 2) return fail(HBEM_ERR_ARG, "HBEM_TUNE_LU_UPDATE: 0, 1 or 2");
+            break;
         default:
             return fail(HBEM_ERR_ARG, "hbem_set_tuning: unknown key " + std::to_string(key));
     }

@@ -45,7 +45,8 @@ extern "C" {
 #define HBEM_ASM_CORRECTED (HBEM_ASM_REGULAR | HBEM_ASM_DUFFY | HBEM_ASM_ZERO)
 
 /* LU precision */
-#define HBEM_PREC_PLAIN 0      /* FP32-accurate trailing updates (complex64 cgesv semantics) */
+#define HBEM_PREC_PLAIN 0      /* FP32-class LU (complex64 cgesv): inner updates FP32 on CUDA cores, the
+                                  look-ahead bulk TF32x3 on the tensor cores (HBEM_TUNE_LU_UPDATE) */
 #define HBEM_PREC_MIXED 1      /* BF16x3 tensor-core trailing updates; pair with hbem_refine */
 #define HBEM_PREC_FP64 2       /* hbem_solve_batch only: complex128 LU of the widened FP32 system (zgesv semantics) */
 
@@ -111,13 +112,19 @@ long long hbem_launch_count(void);
  *                            second stream; 1: one stream)
  *   HBEM_TUNE_LU_RESERVE:    SMs the look-ahead's persistent tensor-core
  *                            update leaves to the factorisation chain
- *                            (v >= 1: v - 1 SMs, at most half; 0: built-in)
+ *                            (v >= 1: v - 1 SMs, at most half; 0: built-in,
+ *                            32 for a plain LU of n < 2048, else none)
  *   HBEM_TUNE_WAVE_SPIN:     polls (of >= 32 ns) a wavefront-solve warp waits
  *                            for an earlier block before it gives up (0: the
  *                            built-in 2^22); a wait that runs out makes the
  *                            launch abort, writes NaN into the unfinished x
  *                            and is reported by hbem_solve_status and the
  *                            synchronising entry points as HBEM_ERR_STATE
+ *   HBEM_TUNE_LU_UPDATE:     the K = 64 trailing update of the plain
+ *                            (FP32) LU beside the factorisation chain
+ *                            (1: CUDA cores, exact FP32 products; 2 and the
+ *                            built-in 0: tensor cores, TF32x3 split
+ *                            products, FP32-class)
  */
 #define HBEM_TUNE_ASM_MINBLOCKS 0
 #define HBEM_TUNE_LU_PANEL 1
@@ -127,7 +134,8 @@ long long hbem_launch_count(void);
 #define HBEM_TUNE_LU_LOOKAHEAD 5
 #define HBEM_TUNE_LU_RESERVE 6
 #define HBEM_TUNE_WAVE_SPIN 7
-#define HBEM_TUNE_COUNT 8
+#define HBEM_TUNE_LU_UPDATE 8
+#define HBEM_TUNE_COUNT 9
 int hbem_set_tuning(int key, int value);
 int hbem_get_tuning(int key);
 

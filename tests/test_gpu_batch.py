@@ -122,7 +122,7 @@ def test_batched_sweeps_match_oracle_on_waveguide_batch_meshes():
     for c, o in zip(cases, outs):
         assert c.n in (829, 866)
         assert np.all(o.lapack_info == 0)
-        assert np.all(o.refine_iterations >= 1)
+        assert np.all((o.refine_iterations >= 0) & (o.refine_iterations <= 3))
         assert np.all(o.refine_residual_rel < 1e-5)
         orc = Oracle(c.buffers, 1, "f64")
         for f in range(len(c.k_re)):

@@ -289,17 +289,20 @@ def test_lu_tall_panels_sixteen_cta_clusters(precision):
 @pytest.mark.parametrize("n,batch", [(1043, 12), (2100, 3)])
 def test_lu_lookahead_equals_one_stream(n, batch):
     """The look-ahead schedule (next block updated on the chain, the rest of the trailing update overlapping the
-    next panels on a second stream) does the same arithmetic in the same order: bit-identical factors."""
+    next panels on a second stream) does the same arithmetic in the same order: bit-identical factors (with the
+    CUDA-core update in both; the tensor-core bulk exists only beside a look-ahead chain)."""
     lib = load_library()
     A, _ = _lu_case(n, batch, 23)
     out = []
     for mode in (1, 0, 0):
         Ar, Ai = _dev(A)
         assert lib.hbem_set_tuning(5, mode) == 0
+        assert lib.hbem_set_tuning(8, 1) == 0
         try:
             piv, info = _factor(Ar, Ai, n, batch)
         finally:
             lib.hbem_set_tuning(5, 0)
+            lib.hbem_set_tuning(8, 0)
         torch.cuda.synchronize()
         out.append((Ar, Ai, piv))
     for r in out[1:]:
@@ -322,6 +325,30 @@ def test_lu_tall_panels_match_lapack(n):
     ref = np.linalg.solve(A[0].astype(np.complex128), B[0].astype(np.complex128))
     # FP32 factorisation error grows with n; LAPACK cgesv in FP32 shows the same
     assert rel(X[0], ref) < (1e-5 if n < 3000 else 3e-5)
+
+
+@pytest.mark.parametrize("n,batch", [(300, 3), (1043, 6), (3300, 1)])
+def test_plain_lu_tensor_core_update_matches_lapack(n, batch):
+    """The plain LU with its look-ahead bulk update on the tensor cores (TF32x3 split products,
+    HBEM_TUNE_LU_UPDATE = 2) against LAPACK and against the CUDA-core (exact FP32 product) update."""
+    lib = load_library()
+    A, b = _lu_case(n, batch, n + 7)
+    xs = {}
+    for mode in (1, 2):
+        Ar, Ai = _dev(A)
+        assert lib.hbem_set_tuning(8, mode) == 0
+        try:
+            piv, info = _factor(Ar, Ai, n, batch)
+        finally:
+            lib.hbem_set_tuning(8, 0)
+        assert int(info.abs().sum()) == 0
+        Br, Bi = _dev(b[:, :, None])
+        _solve(Ar, Ai, piv, Br, Bi, n, 1, batch)
+        xs[mode] = _host(Br, Bi)[:, :, 0]
+    for m in range(batch):
+        ref = np.linalg.solve(A[m].astype(np.complex128), b[m].astype(np.complex128))
+        assert rel(xs[2][m], ref) < (1e-5 if n < 3000 else 3e-5)
+        assert rel(xs[2][m], xs[1][m]) < (1e-5 if n < 3000 else 3e-5)
 
 
 @pytest.mark.parametrize("n", [130, 700])
