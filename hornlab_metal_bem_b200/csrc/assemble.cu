@@ -380,13 +380,18 @@ __global__ void __launch_bounds__(kAsmThreads, MINB) k_regular(const __grid_cons
 // rows: one rsqrt / sincos per sample instead of two.  Tiles and the shared
 // accumulation are those of k_regular with a second, transposed plane.
 // ---------------------------------------------------------------------------
+// Without G (NEED_G false) the singular-point guard costs two instructions
+// a sample: there r^2 gets 1e-30 added instead, which leaves r^2 of every
+// distinct point pair unchanged in FP32 and makes the coincident point
+// (d = 0 exactly) contribute exactly 0: its dG/dn terms carry the factor
+// d.n = 0 times a finite 1/r^2 = 1e30.
 template <bool CK, bool NEED_G>
 __device__ __forceinline__ void sample_sym(float dx, float dy, float dz, float nsx, float nsy, float nsz, float ntx,
                                            float nty, float ntz, float k, float ki, float &dre, float &dim,
                                            float &tre, float &tim, float &gre, float &gim) {
-    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    const float r2 = NEED_G ? fmaf(dx, dx, fmaf(dy, dy, dz * dz)) : fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, 1.0e-30f)));
     float u = rsqrtf(r2);
-    u = r2 > 1.0e-14f ? u : 0.0f;
+    if (NEED_G) u = r2 > 1.0e-14f ? u : 0.0f;
     const float r = r2 * u;
     const float u2 = u * u;
     float hs = fmaf(dx, nsx, fmaf(dy, nsy, dz * nsz)) * u2;

@@ -122,6 +122,7 @@ __global__ void __launch_bounds__(256) k_trailing_simt(float *a_re, float *a_im,
 int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int col_start, int col_end, float *a_re,
                        float *a_im, long long lda, long long a_stride, int *status, cudaStream_t st,
                        int reserve_sms = 0);
+int tc_workspace_k(const TcWorkspace *w);
 
 // A[start:n, col_start:col_end] -= L[start:n, k0:k0+kw] U[k0:k0+kw, col_start:col_end] on the CUDA cores
 int launch_trailing_simt(int n, int batch, int k0, int kw, int start, int col_start, int col_end, float *a_re,
@@ -140,7 +141,7 @@ int launch_trailing_update(int n, int batch, int k0, int kw, int start, int col_
     const int m = n - start, w = col_end - start;
     if (m <= 0 || w <= 0) return HBEM_OK;
     if (kw % 16) return fail(HBEM_ERR_ARG, "trailing update: K must be a multiple of 16");
-    if (tc && kw == 64 && status)
+    if (tc && kw == tc_workspace_k(tc) && status)
         return launch_trailing_tc(tc, n, batch, k0, start, start, col_end, a_re, a_im, lda, a_stride, status, st);
     return launch_trailing_simt(n, batch, k0, kw, start, start, col_end, a_re, a_im, lda, a_stride, st);
 }
@@ -176,22 +177,24 @@ namespace hbem {
 namespace {
 
 constexpr int kTcM = 128;          // MMA rows per tile (64 complex rows: real and imaginary parts)
-constexpr int kTcK2 = 256;         // packed elements per row: hi (real K = 128) then lo
 constexpr int kTcABlk = kTcM * 128;  // one A K-block (128 bytes per row), 16 KB
 constexpr int kTcThreads = 320;    // warp 0: MMA issuer, warp 1: TMA producer, warps 2-9: C tiles
 constexpr long long kSpinLimit = 1LL << 24;
 
-// Shapes of the two variants (see above).
-template <bool TF32>
+// Shapes of the variants (see above): operand format and KC, the complex K
+// of one update (64: one LU block; 128: two blocks, BF16x3 only).
+template <bool TF32, int KC>
 struct TcCfg {
+    static_assert(KC == 64 || (KC == 128 && !TF32), "tensor-core update: K = 64, or 128 with BF16x3");
     static constexpr int ES = TF32 ? 4 : 2;            // operand bytes
     static constexpr int EPB = 128 / ES;               // operand elements per 128-byte K-block
-    static constexpr int KBH = 128 / EPB;              // K-blocks of one split (real K = 128)
-    static constexpr int N = TF32 ? 32 : 64;           // columns per tile
+    static constexpr int K2 = 4 * KC;                  // packed elements per row: hi (real K = 2 KC), lo
+    static constexpr int KBH = 2 * KC / EPB;           // K-blocks of one split
+    static constexpr int N = KBH == 4 ? 32 : 64;       // columns per tile
     static constexpr int ABytes = 2 * KBH * kTcABlk;   // resident A2 of a row block
     static constexpr int BBlk = N * 128;               // one B K-block
     static constexpr int StageBytes = 2 * BBlk;        // ring stage: Bh and Bl of one K-block
-    static constexpr int Stages = TF32 ? 8 : 6;        // B ring: two (TF32) / three (BF16) tiles ahead
+    static constexpr int Stages = KBH == 4 ? 8 : 6;    // B ring: two (K-block 4) / three tiles ahead
     static constexpr int CBytes = kTcM * N * 4;        // one C tile staged in shared memory
     static constexpr int Fmt = TF32 ? 2 : 1;           // instruction-descriptor operand format
     static constexpr size_t Smem = (size_t)ABytes + (size_t)Stages * StageBytes + 2 * (size_t)CBytes + 1024;
@@ -304,18 +307,18 @@ struct TcWalk {
 //     imaginary rows) into one of two shared buffers with cp.async, drain the
 //     finished accumulator into the current buffer (C - L U), hand the
 //     accumulator back, and write the tile out with coalesced stores.
-// Shared C layout: row r holds 16 groups of 4 columns, group g at position
+// Shared C layout: row r holds N / 4 groups of 4 columns, group g at position
 // g ^ (r & 7) (aligned 16-byte copies, conflict-free float4 drain).  Every
 // wait is bounded; a timeout sets *status and the roles stop, drain their
 // copies, free TMEM and return.
-template <bool TF32>
+template <bool TF32, int KC>
 __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_constant__ CUtensorMap tmA,
                                                                 const __grid_constant__ CUtensorMap tmB, float *a_re,
                                                                 float *a_im, long long lda, long long a_stride, int n,
                                                                 int start, int col_start, int col_end, int rows3,
                                                                 int cols_pad, int tiles_m, int tiles_n, int n_chunks,
                                                                 int chunk, int n_units, int *status) {
-    using Cfg = TcCfg<TF32>;
+    using Cfg = TcCfg<TF32, KC>;
     constexpr int kTcN = Cfg::N, kTcStages = Cfg::Stages, kTcStageBytes = Cfg::StageBytes, kTcABytes = Cfg::ABytes;
     constexpr int KBH = Cfg::KBH, EPB = Cfg::EPB;
     extern __shared__ uint8_t s_raw[];
@@ -676,15 +679,17 @@ struct TcSplit<true> {
     __device__ static void store2(T *p, T a, T b) { *reinterpret_cast<float2 *>(p) = make_float2(a, b); }
 };
 
-// Pack L21 (rows start..n, cols k0..k0+64) into A2 (K-major, hi/lo splits).
-template <bool TF32>
+// Pack L21 (rows start..n, cols k0..k0+KC) into A2 (K-major, hi/lo splits):
+// real-part row [Lr | -Li], imaginary-part row [Li | Lr], hi then lo.
+template <bool TF32, int KC>
 __global__ void k_pack_a(const float *a_re, const float *a_im, long long lda, long long a_stride, int n, int start,
                          int k0, int rows3, int rows_used, typename TcSplit<TF32>::T *A2) {
     using S = TcSplit<TF32>;
     using T = typename S::T;
+    constexpr int K2 = TcCfg<TF32, KC>::K2;
     const int mat = blockIdx.z;
     const int i = blockIdx.x * blockDim.y + threadIdx.y;  // complex row offset
-    const int k = threadIdx.x;                            // 0..63
+    const int k = threadIdx.x;                            // 0..KC-1
     const int m = n - start;
     if (i >= rows_used) return;                           // complex rows incl. tile padding
     float lr = 0.f, li = 0.f;
@@ -693,58 +698,62 @@ __global__ void k_pack_a(const float *a_re, const float *a_im, long long lda, lo
         li = a_im[(size_t)mat * a_stride + (size_t)(start + i) * lda + k0 + k];
     }
     const int t = i >> 6, rl = i & 63;
-    T *re_row = A2 + ((size_t)mat * rows3 + (size_t)t * 128 + rl) * kTcK2;
-    T *im_row = re_row + (size_t)64 * kTcK2;
+    T *re_row = A2 + ((size_t)mat * rows3 + (size_t)t * 128 + rl) * K2;
+    T *im_row = re_row + (size_t)64 * K2;
     auto put = [](T *row, int k2, float x) {
         const T h = S::hi(x);
         row[k2] = h;
-        row[128 + k2] = S::hi(x - S::val(h));
+        row[2 * KC + k2] = S::hi(x - S::val(h));
     };
     put(re_row, k, lr);
-    put(re_row, 64 + k, -li);
+    put(re_row, KC + k, -li);
     put(im_row, k, li);
-    put(im_row, 64 + k, lr);
+    put(im_row, KC + k, lr);
 }
 
-// Pack U12 (rows k0..k0+64, cols start..col_end) into B2^T (K-major, hi/lo splits).
-template <bool TF32>
+// Pack U12 (rows k0..k0+KC, cols start..col_end) into B2^T (K-major, hi/lo
+// splits): per column [hi Ur | hi Ui | lo Ur | lo Ui], KC entries each.
+template <bool TF32, int KC>
 __global__ void __launch_bounds__(256) k_pack_b(const float *a_re, const float *a_im, long long lda,
                                                 long long a_stride, int start, int col_end, int k0, int cols_pad,
                                                 int cols_used, typename TcSplit<TF32>::T *B2) {
-    // 64 columns per CTA: the 64 x 64 block of U12 is read along its rows
-    // (coalesced), transposed in shared memory and written as 64 packed
-    // K-major rows of 256 elements (consecutive threads, consecutive pairs)
+    // 64 columns per CTA, 64 rows of U12 at a time: the 64 x 64 block is read
+    // along its rows (coalesced), transposed in shared memory and written
+    // into the packed K-major rows (consecutive threads, consecutive pairs)
     using S = TcSplit<TF32>;
     using T = typename S::T;
+    constexpr int K2 = TcCfg<TF32, KC>::K2;
     __shared__ float s_ur[64][65], s_ui[64][65];
     const int mat = blockIdx.z;
     const int j0 = blockIdx.x * 64;
     const int tid = threadIdx.x;
-    const float *ure = a_re + (size_t)mat * a_stride + (size_t)k0 * lda + start;
-    const float *uim = a_im + (size_t)mat * a_stride + (size_t)k0 * lda + start;
-    for (int e = tid; e < 64 * 64; e += 256) {
-        const int k = e >> 6, jj = e & 63, j = j0 + jj;
-        const bool in = start + j < col_end;
-        s_ur[k][jj] = in ? ure[(size_t)k * lda + j] : 0.f;
-        s_ui[k][jj] = in ? uim[(size_t)k * lda + j] : 0.f;
-    }
-    __syncthreads();
-    // pair p of a packed row covers K entries 2p, 2p + 1:
-    // [0, 64) hi(Ur), [64, 128) hi(Ui), [128, 192) lo(Ur), [192, 256) lo(Ui)
+    // pair p of a chunk covers its entries 2p, 2p + 1 of [hi Ur, hi Ui, lo Ur, lo Ui] (64 each)
     const int p = tid & 127;
     const int kk = 2 * p;
     const int part = kk >> 6, k = kk & 63;   // part: 0 hi Ur, 1 hi Ui, 2 lo Ur, 3 lo Ui
-    for (int jj = tid >> 7; jj < 64; jj += 2) {
-        const int j = j0 + jj;
-        if (j >= cols_used) break;
-        const float x0 = (part & 1) ? s_ui[k][jj] : s_ur[k][jj];
-        const float x1 = (part & 1) ? s_ui[k + 1][jj] : s_ur[k + 1][jj];
-        T v0 = S::hi(x0), v1 = S::hi(x1);
-        if (part >= 2) {
-            v0 = S::hi(x0 - S::val(v0));
-            v1 = S::hi(x1 - S::val(v1));
+    for (int kc = 0; kc < KC; kc += 64) {
+        const float *ure = a_re + (size_t)mat * a_stride + (size_t)(k0 + kc) * lda + start;
+        const float *uim = a_im + (size_t)mat * a_stride + (size_t)(k0 + kc) * lda + start;
+        if (kc) __syncthreads();   // the previous chunk's reads of s_ur / s_ui are done
+        for (int e = tid; e < 64 * 64; e += 256) {
+            const int kr = e >> 6, jj = e & 63, j = j0 + jj;
+            const bool in = start + j < col_end;
+            s_ur[kr][jj] = in ? ure[(size_t)kr * lda + j] : 0.f;
+            s_ui[kr][jj] = in ? uim[(size_t)kr * lda + j] : 0.f;
         }
-        S::store2(B2 + ((size_t)mat * cols_pad + j) * kTcK2 + kk, v0, v1);
+        __syncthreads();
+        for (int jj = tid >> 7; jj < 64; jj += 2) {
+            const int j = j0 + jj;
+            if (j >= cols_used) break;
+            const float x0 = (part & 1) ? s_ui[k][jj] : s_ur[k][jj];
+            const float x1 = (part & 1) ? s_ui[k + 1][jj] : s_ur[k + 1][jj];
+            T v0 = S::hi(x0), v1 = S::hi(x1);
+            if (part >= 2) {
+                v0 = S::hi(x0 - S::val(v0));
+                v1 = S::hi(x1 - S::val(v1));
+            }
+            S::store2(B2 + ((size_t)mat * cols_pad + j) * K2 + part * KC + kc + k, v0, v1);
+        }
     }
 }
 
@@ -766,12 +775,12 @@ EncodeTiledFn encode_fn() {
     return fn;
 }
 
-// Packed rows of kTcK2 elements of es bytes; boxes of one 128-byte K-block x box_rows.
-int make_map(CUtensorMap *map, void *ptr, long long rows, int box_rows, int es) {
+// Packed rows of k2 elements of es bytes; boxes of one 128-byte K-block x box_rows.
+int make_map(CUtensorMap *map, void *ptr, long long rows, int box_rows, int es, int k2) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return fail(HBEM_ERR_CUDA, "cuTensorMapEncodeTiled entry point unavailable");
-    const cuuint64_t dims[2] = {(cuuint64_t)kTcK2, (cuuint64_t)rows};
-    const cuuint64_t strides[1] = {(cuuint64_t)kTcK2 * es};
+    const cuuint64_t dims[2] = {(cuuint64_t)k2, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)k2 * es};
     const cuuint32_t box[2] = {(cuuint32_t)(128 / es), (cuuint32_t)box_rows};
     const cuuint32_t estr[2] = {1, 1};
     CUresult r = fn(map, es == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, ptr, dims,
@@ -786,31 +795,34 @@ int make_map(CUtensorMap *map, void *ptr, long long rows, int box_rows, int es) 
 
 // Packed-operand workspace and tensor maps for one factorisation: sized for
 // the first (largest) trailing update and reused by the later, smaller ones.
-// tf32: TF32x3 operands (plain LU) instead of BF16x3 (mixed LU).
+// tf32: TF32x3 operands (plain LU) instead of BF16x3 (mixed LU); kc: the
+// complex K of one update (64, or 128 for BF16x3).
 struct TcWorkspace {
     void *A2 = nullptr, *B2 = nullptr;
-    int rows3 = 0, cols_pad = 0, batch = 0;
+    int rows3 = 0, cols_pad = 0, batch = 0, kc = 64;
     bool tf32 = false;
     CUtensorMap ma, mb;
 };
 
-int tc_workspace_create(int n, int batch, bool tf32, TcWorkspace **out, cudaStream_t st) {
+int tc_workspace_create(int n, int batch, bool tf32, int kc, TcWorkspace **out, cudaStream_t st) {
     *out = nullptr;
+    if (kc != 64 && (kc != 128 || tf32)) return fail(HBEM_ERR_ARG, "tensor-core update: K = 64, or 128 with BF16x3");
     auto *w = new TcWorkspace();
-    const int tn = tf32 ? TcCfg<true>::N : TcCfg<false>::N, es = tf32 ? 4 : 2;
+    const int tn = (tf32 || kc == 128) ? 32 : 64, es = tf32 ? 4 : 2, k2 = 4 * kc;
     w->tf32 = tf32;
+    w->kc = kc;
     w->rows3 = ((n + 63) / 64) * kTcM;
     w->cols_pad = ((n + tn - 1) / tn) * tn;
     w->batch = batch;
-    cudaError_t e = cudaMallocAsync(&w->A2, (size_t)batch * w->rows3 * kTcK2 * es, st);
-    if (e == cudaSuccess) e = cudaMallocAsync(&w->B2, (size_t)batch * w->cols_pad * kTcK2 * es, st);
+    cudaError_t e = cudaMallocAsync(&w->A2, (size_t)batch * w->rows3 * k2 * es, st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&w->B2, (size_t)batch * w->cols_pad * k2 * es, st);
     if (e != cudaSuccess) {
         if (w->A2) cudaFreeAsync(w->A2, st);
         delete w;
         return cuda_fail(e, "tensor-core workspace");
     }
-    int rc = make_map(&w->ma, w->A2, (long long)batch * w->rows3, kTcM, es);
-    if (rc == HBEM_OK) rc = make_map(&w->mb, w->B2, (long long)batch * w->cols_pad, tn, es);
+    int rc = make_map(&w->ma, w->A2, (long long)batch * w->rows3, kTcM, es, k2);
+    if (rc == HBEM_OK) rc = make_map(&w->mb, w->B2, (long long)batch * w->cols_pad, tn, es, k2);
     if (rc != HBEM_OK) {
         cudaFreeAsync(w->A2, st);
         cudaFreeAsync(w->B2, st);
@@ -828,27 +840,29 @@ void tc_workspace_destroy(TcWorkspace *w, cudaStream_t st) {
     delete w;
 }
 
+int tc_workspace_k(const TcWorkspace *w) { return w ? w->kc : 0; }
+
 namespace {
 
-template <bool TF32>
+template <bool TF32, int KC>
 int launch_trailing_tc_t(TcWorkspace *w, int n, int batch, int k0, int start, int col_start, int col_end,
                          float *a_re, float *a_im, long long lda, long long a_stride, int *status, cudaStream_t st,
                          int reserve_sms) {
-    using Cfg = TcCfg<TF32>;
+    using Cfg = TcCfg<TF32, KC>;
     using T = typename TcSplit<TF32>::T;
     const int m = n - start, wd = col_end - col_start;
     const int tiles_m = (m + 63) / 64, tiles_n = (wd + Cfg::N - 1) / Cfg::N;
     // packed rows use the workspace's fixed per-matrix pitch (rows3 / cols_pad)
     {
-        dim3 blk(64, 4), grd((tiles_m * 64 + 3) / 4, 1, batch);
-        k_pack_a<TF32><<<grd, blk, 0, st>>>(a_re, a_im, lda, a_stride, n, start, k0, w->rows3, tiles_m * 64,
-                                            static_cast<T *>(w->A2));
+        dim3 blk(KC, 256 / KC), grd((tiles_m * 64 + blk.y - 1) / blk.y, 1, batch);
+        k_pack_a<TF32, KC><<<grd, blk, 0, st>>>(a_re, a_im, lda, a_stride, n, start, k0, w->rows3, tiles_m * 64,
+                                                static_cast<T *>(w->A2));
         HBEM_LAUNCH_CHECK("k_pack_a");
     }
     {
         dim3 grd((tiles_n * Cfg::N + 63) / 64, 1, batch);
-        k_pack_b<TF32><<<grd, 256, 0, st>>>(a_re, a_im, lda, a_stride, col_start, col_end, k0, w->cols_pad,
-                                            tiles_n * Cfg::N, static_cast<T *>(w->B2));
+        k_pack_b<TF32, KC><<<grd, 256, 0, st>>>(a_re, a_im, lda, a_stride, col_start, col_end, k0, w->cols_pad,
+                                                tiles_n * Cfg::N, static_cast<T *>(w->B2));
         HBEM_LAUNCH_CHECK("k_pack_b");
     }
     int n_sm = 0;
@@ -856,7 +870,7 @@ int launch_trailing_tc_t(TcWorkspace *w, int n, int batch, int k0, int start, in
         int dev = 0;
         HBEM_CUDA(cudaGetDevice(&dev));
         HBEM_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
-        const int rc = func_opt_in((const void *)k_trailing_tc<TF32>, (int)Cfg::Smem);
+        const int rc = func_opt_in((const void *)k_trailing_tc<TF32, KC>, (int)Cfg::Smem);
         if (rc != HBEM_OK) return rc;
     }
     const int ctas = n_sm - std::min(std::max(reserve_sms, 0), n_sm / 2);
@@ -871,28 +885,32 @@ int launch_trailing_tc_t(TcWorkspace *w, int n, int batch, int k0, int start, in
     if (units > 0x7fffffffLL) return fail(HBEM_ERR_ARG, "trailing update: too many tiles");
     if ((long long)(n_chunks - 1) * chunk >= tiles_n) return fail(HBEM_ERR_STATE, "trailing update: empty work unit");
     const int grid = (int)std::min<long long>(units, ctas);
-    k_trailing_tc<TF32><<<grid, kTcThreads, Cfg::Smem, st>>>(w->ma, w->mb, a_re, a_im, lda, a_stride, n, start,
-                                                              col_start, col_end, w->rows3, w->cols_pad, tiles_m,
-                                                              tiles_n, n_chunks, chunk, (int)units, status);
+    k_trailing_tc<TF32, KC><<<grid, kTcThreads, Cfg::Smem, st>>>(w->ma, w->mb, a_re, a_im, lda, a_stride, n, start,
+                                                                  col_start, col_end, w->rows3, w->cols_pad, tiles_m,
+                                                                  tiles_n, n_chunks, chunk, (int)units, status);
     HBEM_LAUNCH_CHECK("k_trailing_tc");
     return HBEM_OK;
 }
 
 }  // namespace
 
-// Tensor-core trailing update with K = 64 (one LU block), BF16x3 or TF32x3 by
-// the workspace; status receives 1/2/3 if a barrier wait timed out.  The
-// persistent grid leaves reserve_sms SMs (at most half of them) to kernels on
-// other streams.
-// A[start:n, col_start:col_end] -= L[start:n, k0:k0+64] U[k0:k0+64, col_start:col_end]
+// Tensor-core trailing update with the workspace's K (64: one LU block, 128:
+// two), BF16x3 or TF32x3 by the workspace; status receives 1/2/3 if a
+// barrier wait timed out.  The persistent grid leaves reserve_sms SMs (at
+// most half of them) to kernels on other streams.
+// A[start:n, col_start:col_end] -= L[start:n, k0:k0+K] U[k0:k0+K, col_start:col_end]
 int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int col_start, int col_end, float *a_re,
                        float *a_im, long long lda, long long a_stride, int *status, cudaStream_t st,
                        int reserve_sms) {
     if (n - start <= 0 || col_end - col_start <= 0) return HBEM_OK;
-    return w->tf32 ? launch_trailing_tc_t<true>(w, n, batch, k0, start, col_start, col_end, a_re, a_im, lda, a_stride,
-                                                status, st, reserve_sms)
-                   : launch_trailing_tc_t<false>(w, n, batch, k0, start, col_start, col_end, a_re, a_im, lda,
-                                                 a_stride, status, st, reserve_sms);
+    if (w->tf32)
+        return launch_trailing_tc_t<true, 64>(w, n, batch, k0, start, col_start, col_end, a_re, a_im, lda, a_stride,
+                                              status, st, reserve_sms);
+    if (w->kc == 128)
+        return launch_trailing_tc_t<false, 128>(w, n, batch, k0, start, col_start, col_end, a_re, a_im, lda,
+                                                a_stride, status, st, reserve_sms);
+    return launch_trailing_tc_t<false, 64>(w, n, batch, k0, start, col_start, col_end, a_re, a_im, lda, a_stride,
+                                           status, st, reserve_sms);
 }
 
 }  // namespace hbem

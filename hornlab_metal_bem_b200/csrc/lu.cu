@@ -34,7 +34,7 @@ namespace hbem {
 
 // A[start:n, start:col_end] -= A[start:n, k0:k0+kw] * A[k0:k0+kw, start:col_end]
 struct TcWorkspace;
-int tc_workspace_create(int n, int batch, bool tf32, TcWorkspace **out, cudaStream_t st);
+int tc_workspace_create(int n, int batch, bool tf32, int kc, TcWorkspace **out, cudaStream_t st);
 void tc_workspace_destroy(TcWorkspace *w, cudaStream_t st);
 int launch_trailing_update(int n, int batch, int k0, int kw, int start, int col_end, float *a_re, float *a_im,
                            long long lda, long long a_stride, TcWorkspace *tc, int *status, cudaStream_t st);
@@ -465,7 +465,7 @@ __global__ void __launch_bounds__(kSwapThreads) k_swap_trsm(float *a_re, float *
     __shared__ int s_col[kSwapCols];
     const int b = blockIdx.y;
     float *are = a_re + (size_t)b * a_stride, *aim = a_im + (size_t)b * a_stride;
-    const int *pv = piv + (size_t)b * piv_stride;
+    const int *pv = piv ? piv + (size_t)b * piv_stride : nullptr;   // NULL: no interchanges, TRSM only
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int ncols_total = col_hi - col_lo - ex_w;
     const int c_first = blockIdx.x * kSwapCols;
@@ -477,7 +477,7 @@ __global__ void __launch_bounds__(kSwapThreads) k_swap_trsm(float *a_re, float *
     }
     if (tid < 128) s_row[tid] = tid < np ? k0 + tid : -1;
     __shared__ int s_pv[64];
-    if (tid < np) s_pv[tid] = pv[k0 + tid];
+    if (tid < np) s_pv[tid] = pv ? pv[k0 + tid] : k0 + tid;
     __syncthreads();
     if (tid < np) {
         const int p = s_pv[tid];
@@ -1134,6 +1134,12 @@ struct WaveCtl {
 };
 
 static __device__ int g_wave_fault;
+
+// A non-zero status word of a captured factorisation's tensor-core update
+// raises the fault word as well.
+__global__ void k_fold_status(const int *status) {
+    if (*status) atomicExch(&g_wave_fault, 1);
+}
 
 __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p) {
     unsigned long long v;
@@ -1835,10 +1841,11 @@ static bool plain_update_on_tensor_cores() {
 
 int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long long a_stride, int *piv,
               long long piv_stride, int *info, int precision, cudaStream_t st) {
-    // Two-level blocking: 64-column blocks whose (n - b0) x 64 panel is
-    // factored by inner sub-panels (32 wide when the sub-panel fits shared
-    // memory, else 16) with updates confined to the block's columns; then one
-    // row-swap pass, a 64-row TRSM and a K = 64 trailing update per block.
+    // Two-level blocking: 64-column blocks (128 for the mixed LU, so its
+    // tensor-core update streams the trailing matrix once per 128 columns)
+    // whose (n - b0) x NB panel is factored by inner sub-panels (64, 32 or 16
+    // wide) with updates confined to the block's columns; then the row swaps,
+    // the NB-row TRSM (in 64-row halves) and a K = NB trailing update per block.
     // Look-ahead: the trailing update of block b is cut into the next block's
     // 64 columns (on the chain, in FP32 on the CUDA cores, so block b+1's
     // panels can start) and the rest (on the bulk stream, on the tensor cores
@@ -1847,7 +1854,7 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
     // column, wait for it.  The tensor-core workspace and status word are
     // only used on the bulk stream (and on the chain after it has joined).
     const size_t smem_cap = 200 * 1024;
-    constexpr int NB = 64;
+    const int NB = (precision == HBEM_PREC_MIXED && n > 256 && tuning(HBEM_TUNE_LU_BLOCK) != 64) ? 128 : 64;
     HBEM_CUDA(cudaMemsetAsync(info, 0, sizeof(int) * batch, st));
     // K = 64 block updates on the tensor cores: BF16x3 (mixed precision), or
     // TF32x3 for the plain LU's look-ahead bulk when selected; their barrier
@@ -1859,7 +1866,7 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
     if ((precision == HBEM_PREC_MIXED && n > 64) || tf32_bulk) {
         HBEM_CUDA(cudaMallocAsync((void **)&status, sizeof(int), st));
         HBEM_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
-        int rc = tc_workspace_create(n, batch, tf32_bulk, &tc, st);
+        int rc = tc_workspace_create(n, batch, tf32_bulk, tf32_bulk ? 64 : NB, &tc, st);
         if (rc != HBEM_OK) {
             cudaFreeAsync(status, st);
             return rc;
@@ -1885,7 +1892,17 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
             cudaStreamWaitEvent(st, la->join_bulk, 0);
         }
         tc_workspace_destroy(tc, st);
-        if (status) {
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        if (status && cudaStreamIsCapturing(st, &cap) == cudaSuccess && cap != cudaStreamCaptureStatusNone) {
+            // inside a graph capture nothing may wait for the host: a timed-out
+            // wait of the tensor-core update is folded into the module fault
+            // word that hbem_solve_status reports
+            k_fold_status<<<1, 1, 0, st>>>(status);
+            cudaError_t e = cudaGetLastError();
+            if (e == cudaSuccess) count_launch();
+            else if (rc == HBEM_OK) rc = cuda_fail(e, "k_fold_status");
+            cudaFreeAsync(status, st);
+        } else if (status) {
             int h = 0;
             if (rc == HBEM_OK) {
                 cudaError_t e = cudaMemcpyAsync(&h, status, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -1910,6 +1927,33 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
     HBEM_CUDA(cudaFuncSetAttribute(k_panel_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
     HBEM_CUDA(cudaFuncSetAttribute(k_swap_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSwapSmem));
     const int cmax = panel_cluster_max(smem_cap);
+    // Row swaps of block [b0, b0 + bw) on the columns [lo, hi) minus
+    // [ex, ex + exw), and U12 = L11^-1 A12 on its columns [t_lo, t_hi) (all
+    // >= b0 + bw).  A block wider than 64 goes in two 64-row halves: swaps and
+    // TRSM of the first half, swaps of the second, the second half's rows of
+    // [t_lo, t_hi) updated with the first half's U12 (CUDA cores), then the
+    // TRSM of the second half alone.
+    auto swap_trsm = [&](int b0, int bw, int lo, int hi, int ex, int exw, int t_lo, int t_hi,
+                         cudaStream_t s) -> int {
+        if (hi - lo - exw <= 0) return HBEM_OK;
+        dim3 grid((hi - lo - exw + kSwapCols - 1) / kSwapCols, batch);
+        k_swap_trsm<<<grid, kSwapThreads, kSwapSmem, s>>>(a_re, a_im, lda, a_stride, b0, std::min(bw, 64), lo, hi, ex,
+                                                          exw, b0 + bw, piv, piv_stride);
+        int rc = launched("k_swap_trsm");
+        if (rc != HBEM_OK || bw <= 64) return rc;
+        const int b1 = b0 + 64, h2 = bw - 64;
+        k_swap_trsm<<<grid, kSwapThreads, kSwapSmem, s>>>(a_re, a_im, lda, a_stride, b1, h2, lo, hi, ex, exw, hi, piv,
+                                                          piv_stride);
+        rc = launched("k_swap_trsm");
+        if (rc != HBEM_OK || t_hi <= t_lo) return rc;
+        // rows [b1, b0 + bw) only: the row bound of the update is b0 + bw
+        rc = launch_trailing_simt(b0 + bw, batch, b0, 64, b1, t_lo, t_hi, a_re, a_im, lda, a_stride, s);
+        if (rc != HBEM_OK) return rc;
+        dim3 g2((t_hi - t_lo + kSwapCols - 1) / kSwapCols, batch);
+        k_swap_trsm<<<g2, kSwapThreads, kSwapSmem, s>>>(a_re, a_im, lda, a_stride, b1, h2, t_lo, t_hi, t_hi, 0, t_lo,
+                                                        nullptr, piv_stride);
+        return launched("k_swap_trsm");
+    };
     for (int b0 = 0; b0 < n; b0 += NB) {
         const int bw = std::min(NB, n - b0);
         // the whole block as one panel while one CTA holds it; else inner width
@@ -1975,10 +2019,7 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
             // columns; the bulk stream swaps the rest before its update
             const int lo = split ? b0 + bw : 0, hi = split ? next_end : n;
             const int ex = split ? hi : b0, exw = split ? 0 : bw;
-            dim3 grid((hi - lo - exw + kSwapCols - 1) / kSwapCols, batch);
-            k_swap_trsm<<<grid, kSwapThreads, kSwapSmem, cs>>>(a_re, a_im, lda, a_stride, b0, bw, lo, hi, ex, exw,
-                                                               b0 + bw, piv, piv_stride);
-            int rc = launched("k_swap_trsm");
+            int rc = swap_trsm(b0, bw, lo, hi, ex, exw, b0 + bw, hi, cs);
             if (rc != HBEM_OK) return finish(rc);
         }
         if (b0 + bw < n) {
@@ -1988,14 +2029,8 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
                 if (rc == HBEM_OK) rc = stream_call(cudaEventRecord(la->split[parity], cs), "look-ahead fork");
                 if (rc == HBEM_OK)
                     rc = stream_call(cudaStreamWaitEvent(la->bulk, la->split[parity], 0), "look-ahead fork");
-                if (rc == HBEM_OK) {
-                    // columns [0, b0) and [next_end, n): swaps, and the TRSM on those right of the block
-                    dim3 grid((n - (next_end - b0) + kSwapCols - 1) / kSwapCols, batch);
-                    k_swap_trsm<<<grid, kSwapThreads, kSwapSmem, la->bulk>>>(a_re, a_im, lda, a_stride, b0, bw, 0, n,
-                                                                             b0, next_end - b0, b0 + bw, piv,
-                                                                             piv_stride);
-                    rc = launched("k_swap_trsm");
-                }
+                if (rc == HBEM_OK)   // columns [0, b0) and [next_end, n): swaps, and the TRSM right of the block
+                    rc = swap_trsm(b0, bw, 0, n, b0, next_end - b0, next_end, n, la->bulk);
                 if (rc == HBEM_OK)
                     rc = tc ? launch_trailing_tc(tc, n, batch, b0, b0 + bw, next_end, n, a_re, a_im, lda, a_stride,
                                                  status, la->bulk, tc_reserve)
@@ -2058,7 +2093,8 @@ int wave_fault_check(cudaStream_t st) {
     const int zero = 0;
     cudaMemcpyToSymbolAsync(g_wave_fault, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, st);
     cudaStreamSynchronize(st);
-    return fail(HBEM_ERR_STATE, "triangular solve: a wait for an earlier block timed out (its results are NaN)");
+    return fail(HBEM_ERR_STATE, "a bounded device wait timed out: a triangular solve's wait for an earlier block (its "
+                                "results are NaN) or a captured factorisation's tensor-core update");
 }
 
 int lu_solve_single(int n, int nrhs, int batch, const float *lu_re, const float *lu_im, long long lda,

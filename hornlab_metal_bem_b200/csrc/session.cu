@@ -368,6 +368,10 @@ extern "C" int hbem_set_tuning(int key, int value) {
         case HBEM_TUNE_LU_UPDATE:
             if (value < 0 || value > 2) return fail(HBEM_ERR_ARG, "HBEM_TUNE_LU_UPDATE: 0, 1 or 2");
             break;
+        case HBEM_TUNE_LU_BLOCK:
+            if (value != 0 && value != 64 && value != 128)
+                return fail(HBEM_ERR_ARG, "HBEM_TUNE_LU_BLOCK: 0, 64 or 128");
+            break;
         default:
             return fail(HBEM_ERR_ARG, "hbem_set_tuning: unknown key " + std::to_string(key));
     }

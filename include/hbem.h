@@ -125,6 +125,9 @@ long long hbem_launch_count(void);
  *                            (1: CUDA cores, exact FP32 products; 2 and the
  *                            built-in 0: tensor cores, TF32x3 split
  *                            products, FP32-class)
+ *   HBEM_TUNE_LU_BLOCK:      column block of the mixed (BF16x3) LU and the K
+ *                            of its tensor-core update (64 or 128; 0: the
+ *                            built-in 128 for n > 256, else 64)
  */
 #define HBEM_TUNE_ASM_MINBLOCKS 0
 #define HBEM_TUNE_LU_PANEL 1
@@ -135,7 +138,8 @@ long long hbem_launch_count(void);
 #define HBEM_TUNE_LU_RESERVE 6
 #define HBEM_TUNE_WAVE_SPIN 7
 #define HBEM_TUNE_LU_UPDATE 8
-#define HBEM_TUNE_COUNT 9
+#define HBEM_TUNE_LU_BLOCK 9
+#define HBEM_TUNE_COUNT 10
 int hbem_set_tuning(int key, int value);
 int hbem_get_tuning(int key);
 
@@ -219,7 +223,10 @@ int hbem_assemble_multi(hbem_session *s, int n_freq, const float *k_re, const fl
  * Replaces: cgesv_/cgetrf_ in solveDenseAccelerateCgesvMulti
  *   (main.swift:7834-7941, 8015-8020).
  * info: device int per matrix; 0 or the 1-based index of the first zero pivot.
- * Returns HBEM_OK even when a pivot is zero (read info).
+ * Returns HBEM_OK even when a pivot is zero (read info).  With tensor-core
+ * updates (mixed precision, or the plain LU's TF32x3 bulk) it synchronises
+ * `stream` to report a timed-out barrier wait (HBEM_ERR_STATE); inside a CUDA
+ * graph capture it does not synchronise, and hbem_solve_status reports it.
  */
 int hbem_lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long long a_stride,
                    int *piv, long long piv_stride, int *info, int precision, void *stream);
@@ -236,7 +243,8 @@ int hbem_lu_solve(int n, int nrhs, int batch, const float *lu_re, const float *l
 /*
  * Synchronise `stream` and report the device-side status of the asynchronous
  * solves issued before it: HBEM_ERR_STATE when a wavefront triangular-solve
- * wait timed out since the last report (that solve's unfinished x is NaN),
+ * wait timed out since the last report (that solve's unfinished x is NaN), or
+ * the tensor-core update of a factorisation captured in a CUDA graph did,
  * else HBEM_OK.  Clears the status.  hbem_refine, hbem_lu_rcond and
  * hbem_solve_batch report it themselves.  No counterpart in the reference,
  * whose LAPACK solves are synchronous.

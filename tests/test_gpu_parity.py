@@ -547,6 +547,38 @@ def test_mixed_precision_lu_with_refinement(n):
         assert rel(x[m], ref) < 1e-5           # refined
 
 
+@pytest.mark.parametrize("n,batch", [(1043, 4), (3300, 1)])
+def test_mixed_lu_two_block_update_matches_one_block(n, batch):
+    """The mixed LU's 128-column blocks (two-half swaps and TRSM, one K = 128 tensor-core update per block)
+    against its 64-column blocks (K = 64): the same pivots where the FP32 panels see the same data up to
+    BF16x3 rounding, residuals of the same size, and both refined to 1e-6 against LAPACK."""
+    lib = load_library()
+    A, b = _lu_case(n, batch, 300 + n)
+    out = {}
+    for blk in (64, 128):
+        A0r, A0i = _dev(A)
+        LUr, LUi = A0r.clone(), A0i.clone()
+        assert lib.hbem_set_tuning(9, blk) == 0
+        try:
+            piv, info = _factor(LUr, LUi, n, batch, precision=1)
+        finally:
+            lib.hbem_set_tuning(9, 0)
+        assert int(info.abs().sum()) == 0
+        Xr, Xi = _dev(b[:, :, None])
+        _solve(LUr, LUi, piv, Xr, Xi, n, 1, batch)
+        x0 = _host(Xr, Xi)[:, :, 0]
+        Br, Bi = _dev(b)
+        Xr2, Xi2 = Xr[:, :, 0].contiguous(), Xi[:, :, 0].contiguous()
+        iters, resid = _refine(A0r, A0i, LUr, LUi, piv, Br, Bi, Xr2, Xi2, n, batch, 1e-6, 10)
+        out[blk] = (x0, _host(Xr2, Xi2), resid)
+    for m in range(batch):
+        ref = np.linalg.solve(A[m].astype(np.complex128), b[m].astype(np.complex128))
+        e64, e128 = rel(out[64][0][m], ref), rel(out[128][0][m], ref)
+        assert e128 < 1e-3 and e128 < 4 * e64 + 1e-6   # unrefined BF16x3 factors, either blocking
+        assert out[128][2][m] <= 1e-6
+        assert rel(out[128][1][m], ref) < 1e-5
+
+
 def test_wavefront_wait_that_runs_out_reports_state_error_and_nan():
     """A wavefront-solve wait bounded to one poll (HBEM_TUNE_WAVE_SPIN = 1) gives up before the earlier block's
     x arrives: the launch aborts, the unfinished x is NaN, and hbem_solve_status reports HBEM_ERR_STATE once (the
