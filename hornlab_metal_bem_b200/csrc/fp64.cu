@@ -990,7 +990,350 @@ Geo64 geo64(const Session &s) {
     return g;
 }
 
+// ---------------------------------------------------------------------------
+// CHIEF least squares (reference main.swift:1897-2036, 7186-7409).
+//
+// Interior point x_c gives one collocation row of the exterior representation,
+// which vanishes inside the body: C p = d with
+//   C[c][dof] = sum_tri sum_images int D(x_c, y) phi_dof - (int G) (i k beta) / 3,
+//   d[c]      = sum_tri (int G) g_tri,
+// D and G at the real wavenumber (the field kernels), i k of the Robin fold at
+// the complex one; no jump term, no row weight.  The system [A; s C] p =
+// [b; s d], s = weight ||A||_inf / ||C||_inf, is solved in the least-squares
+// sense in complex128 by Householder QR (LAPACK zgeqrf / zunmqr / ztrtrs, the
+// reference's zgels): per column one reflector H = I - tau v v^H (zlarfg), then
+// H^H applied to the remaining columns, the right-hand sides included as extra
+// columns; then back substitution with R.
+// ---------------------------------------------------------------------------
+constexpr int kMaxChiefSrc = 8;
+
+struct ChiefArgs {
+    Geo64 g;
+    const float *pts;                 // (3, m)
+    const float *q_re, *q_im;         // (S, F, T) Neumann data
+    long long q_stride, q_src_stride;
+    const float *beta_re, *beta_im;   // (T) admittances or NULL
+    double *c_re, *c_im;              // (F, m, n)
+    double *d_re, *d_im;              // (S, F, m)
+    int m, n, n_src, nf;
+    double kr[kMaxF64], ki[kMaxF64];
+};
+
+// Grid: x = triangle blocks of 256, y = CHIEF point, z = wavenumber.
+__global__ void __launch_bounds__(256) k64_chief_rows(const __grid_constant__ ChiefArgs p) {
+    const Geo64 &g = p.g;
+    const int ci = blockIdx.y, f = blockIdx.z;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const double ox = p.pts[ci], oy = p.pts[p.m + ci], oz = p.pts[2 * p.m + ci];
+    const double kr = p.kr[f], ki = p.ki[f];
+    double gs_re = 0.0, gs_im = 0.0;
+    if (t < g.T) {
+        const double nx = g.nrm[4 * t], ny = g.nrm[4 * t + 1], nz = g.nrm[4 * t + 2];
+        const double jac = 2.0 * g.nrm[4 * t + 3];
+        double dc_re[3] = {0.0, 0.0, 0.0}, dc_im[3] = {0.0, 0.0, 0.0};
+        for (int a = 0; a < 6; ++a) {
+            double yx, yy, yz;
+            point_on(g.tv, t, c64_qx[a], c64_qy[a], yx, yy, yz);
+            const double w = c64_qw[a] * jac;
+            const double b[3] = {1.0 - c64_qx[a] - c64_qy[a], c64_qx[a], c64_qy[a]};
+            for (int im = -1; im < g.n_masks; ++im) {
+                double px = yx, py = yy, pz = yz, mx = nx, my = ny, mz = nz;
+                if (im >= 0) {
+                    mirror3(px, py, pz, g.masks[im]);
+                    mirror3(mx, my, mz, g.masks[im]);
+                }
+                double gre = 0.0, gim = 0.0, dre = 0.0, dim = 0.0;
+                green_dlp(px - ox, py - oy, pz - oz, mx, my, mz, kr, 0.0, gre, gim, dre, dim);
+#pragma unroll
+                for (int l = 0; l < 3; ++l) {
+                    dc_re[l] += dre * b[l] * w;
+                    dc_im[l] += dim * b[l] * w;
+                }
+                gs_re += gre * w;
+                gs_im += gim * w;
+            }
+        }
+        double rob_re = 0.0, rob_im = 0.0;
+        if (p.beta_re && (p.beta_re[t] != 0.f || p.beta_im[t] != 0.f)) {
+            // (int G) (i k beta) / 3 with i k = -ki + i kr
+            const double br = p.beta_re[t], bi = p.beta_im[t];
+            const double ikb_re = -ki * br - kr * bi, ikb_im = -ki * bi + kr * br;
+            rob_re = (gs_re * ikb_re - gs_im * ikb_im) / 3.0;
+            rob_im = (gs_re * ikb_im + gs_im * ikb_re) / 3.0;
+        }
+        double *cr = p.c_re + ((size_t)f * p.m + ci) * p.n, *cim = p.c_im + ((size_t)f * p.m + ci) * p.n;
+#pragma unroll
+        for (int l = 0; l < 3; ++l) {
+            const int d = g.l2g[3 * t + l];
+            atomicAdd(cr + d, dc_re[l] - rob_re);
+            atomicAdd(cim + d, dc_im[l] - rob_im);
+        }
+    }
+    // d[s][f][ci] += sum over this block's triangles of (int G) g_tri
+    __shared__ double s_part[8][2];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int sv = 0; sv < p.n_src; ++sv) {
+        double vr = 0.0, vi = 0.0;
+        if (t < g.T && p.q_re) {
+            const size_t o = (size_t)sv * p.q_src_stride + (size_t)f * p.q_stride + t;
+            const double qr = p.q_re[o], qi = p.q_im[o];
+            vr = gs_re * qr - gs_im * qi;
+            vi = gs_re * qi + gs_im * qr;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            vr += __shfl_xor_sync(0xffffffffu, vr, o);
+            vi += __shfl_xor_sync(0xffffffffu, vi, o);
+        }
+        __syncthreads();
+        if (lane == 0) { s_part[warp][0] = vr; s_part[warp][1] = vi; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double ar = 0.0, ai = 0.0;
+            for (int w2 = 0; w2 < (int)(blockDim.x >> 5); ++w2) { ar += s_part[w2][0]; ai += s_part[w2][1]; }
+            const size_t o = ((size_t)sv * p.nf + f) * p.m + ci;
+            atomicAdd(p.d_re + o, ar);
+            atomicAdd(p.d_im + o, ai);
+        }
+    }
+}
+
+// ||X_f||_inf = max_i sum_j |x_ij| of row-major (rows, cols) matrices, one warp
+// per row; out[f] (as the bits of a non-negative double) by atomicMax.
+template <typename T>
+__global__ void k64_inf_norm(int rows, int cols, const T *xr, const T *xi, long long ld, long long stride,
+                             unsigned long long *out) {
+    const int f = blockIdx.y;
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (row >= rows) return;
+    const T *r = xr + (size_t)f * stride + (size_t)row * ld, *i = xi + (size_t)f * stride + (size_t)row * ld;
+    double sum = 0.0;
+    for (int c = lane; c < cols; c += 32) sum += hypot((double)r[c], (double)i[c]);
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (lane == 0) atomicMax(out + f, (unsigned long long)__double_as_longlong(sum));
+}
+
+// M_f = [A_f | B_f; s C_f | s D_f] (rows n + m, ldm >= n + S; B_f, D_f hold the
+// S right-hand sides as columns), s_f = weight ||A_f|| / ||C_f|| (weight when
+// ||C_f|| = 0).  Grid: x over the elements of one matrix, y = wavenumber.
+struct ChiefBuildArgs {
+    const float *a_re, *a_im;
+    long long lda, a_stride;
+    const float *b_re, *b_im;
+    long long b_stride, b_src_stride;
+    const double *c_re, *c_im, *d_re, *d_im;
+    const unsigned long long *anorm, *cnorm;
+    double *m_re, *m_im;
+    long long ldm, m_stride;
+    double *scale;
+    double weight;
+    int n, m, n_src, nf;
+};
+
+__global__ void k64_chief_build(const __grid_constant__ ChiefBuildArgs p) {
+    const int f = blockIdx.y;
+    const double an = __longlong_as_double((long long)p.anorm[f]), cn = __longlong_as_double((long long)p.cnorm[f]);
+    const double sc = p.weight * (cn > 0.0 ? an / cn : 1.0);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && p.scale) p.scale[f] = sc;
+    const int cols = p.n + p.n_src, rows = p.n + p.m;
+    double *mr = p.m_re + (size_t)f * p.m_stride, *mi = p.m_im + (size_t)f * p.m_stride;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < (long long)rows * cols;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(e / cols), c = (int)(e - (long long)r * cols);
+        double vr, vi;
+        if (r < p.n) {
+            if (c < p.n) {
+                const size_t o = (size_t)f * p.a_stride + (size_t)r * p.lda + c;
+                vr = p.a_re[o];
+                vi = p.a_im[o];
+            } else {
+                const size_t o = (size_t)(c - p.n) * p.b_src_stride + (size_t)f * p.b_stride + r;
+                vr = p.b_re[o];
+                vi = p.b_im[o];
+            }
+        } else {
+            const int ci = r - p.n;
+            if (c < p.n) {
+                const size_t o = ((size_t)f * p.m + ci) * p.n + c;
+                vr = sc * p.c_re[o];
+                vi = sc * p.c_im[o];
+            } else {
+                const size_t o = ((size_t)(c - p.n) * p.nf + f) * p.m + ci;
+                vr = sc * p.d_re[o];
+                vi = sc * p.d_im[o];
+            }
+        }
+        mr[(size_t)r * p.ldm + c] = vr;
+        mi[(size_t)r * p.ldm + c] = vi;
+    }
+}
+
+// Block sum of a double (all threads get it); blockDim.x a multiple of 32, <= 1024.
+__device__ __forceinline__ double block_sum(double v, double *s_w) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if (lane == 0) s_w[warp] = v;
+    __syncthreads();
+    double t = 0.0;
+    for (int w = 0; w < nw; ++w) t += s_w[w];
+    return t;
+}
+
+// Householder reflector of column j (LAPACK zlarfg): alpha = M[j][j],
+// x = M[j+1:rows][j]; beta = -sign(Re alpha) |(alpha, x)|, tau =
+// ((beta - Re alpha) / beta, -Im alpha / beta), v = x / (alpha - beta) stored
+// over x, M[j][j] = beta; tau = 0 when x = 0 and alpha is real.  Also clears u,
+// the accumulator of v^H M for the columns after j.  One CTA per matrix.
+__global__ void __launch_bounds__(256) k64_hh_reflector(int rows, int cols, int j, double *m_re, double *m_im,
+                                                        long long ldm, long long m_stride, double *tau, double *u) {
+    __shared__ double s_w[8];
+    __shared__ double s_scale[2];
+    const int f = blockIdx.x;
+    double *mr = m_re + (size_t)f * m_stride, *mi = m_im + (size_t)f * m_stride;
+    double acc = 0.0;
+    for (int r = j + 1 + threadIdx.x; r < rows; r += blockDim.x) {
+        const double a = mr[(size_t)r * ldm + j], b = mi[(size_t)r * ldm + j];
+        acc += a * a + b * b;
+    }
+    const double xn2 = block_sum(acc, s_w);
+    double *tf = tau + (size_t)f * 2 * cols + 2 * j;
+    if (threadIdx.x == 0) {
+        const double ar = mr[(size_t)j * ldm + j], ai = mi[(size_t)j * ldm + j];
+        if (xn2 == 0.0 && ai == 0.0) {
+            tf[0] = 0.0;
+            tf[1] = 0.0;
+            s_scale[0] = 1.0;
+            s_scale[1] = 0.0;
+        } else {
+            const double beta = -copysign(sqrt(ar * ar + ai * ai + xn2), ar);
+            tf[0] = (beta - ar) / beta;
+            tf[1] = -ai / beta;
+            // 1 / (alpha - beta)
+            const double dr = ar - beta, di = ai, den = dr * dr + di * di;
+            s_scale[0] = dr / den;
+            s_scale[1] = -di / den;
+            mr[(size_t)j * ldm + j] = beta;
+            mi[(size_t)j * ldm + j] = 0.0;
+        }
+    }
+    __syncthreads();
+    const double sr = s_scale[0], si = s_scale[1];
+    for (int r = j + 1 + threadIdx.x; r < rows; r += blockDim.x) {
+        const double a = mr[(size_t)r * ldm + j], b = mi[(size_t)r * ldm + j];
+        mr[(size_t)r * ldm + j] = a * sr - b * si;
+        mi[(size_t)r * ldm + j] = a * si + b * sr;
+    }
+    for (int c = threadIdx.x; c < 2 * cols; c += blockDim.x) u[(size_t)f * 2 * cols + c] = 0.0;
+}
+
+constexpr int kHhRows = 64;   // rows per CTA of the reflector application
+
+// u[c] += sum_r conj(v_r) M[r][c] over this CTA's rows (v_j = 1), c > j.
+// Grid: x = column blocks of 256, y = row blocks of kHhRows from j, z = matrix.
+__global__ void __launch_bounds__(256) k64_hh_dot(int rows, int cols, int j, const double *m_re, const double *m_im,
+                                                  long long ldm, long long m_stride, double *u) {
+    const int f = blockIdx.z;
+    const int c = j + 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cols) return;
+    const double *mr = m_re + (size_t)f * m_stride, *mi = m_im + (size_t)f * m_stride;
+    const int r0 = j + blockIdx.y * kHhRows, r1 = min(rows, r0 + kHhRows);
+    double ar = 0.0, ai = 0.0;
+    for (int r = r0; r < r1; ++r) {
+        const double vr = r == j ? 1.0 : mr[(size_t)r * ldm + j], vi = r == j ? 0.0 : mi[(size_t)r * ldm + j];
+        const double xr = mr[(size_t)r * ldm + c], xi = mi[(size_t)r * ldm + c];
+        ar += vr * xr + vi * xi;   // conj(v) x
+        ai += vr * xi - vi * xr;
+    }
+    atomicAdd(u + (size_t)f * 2 * cols + 2 * c, ar);
+    atomicAdd(u + (size_t)f * 2 * cols + 2 * c + 1, ai);
+}
+
+// M[r][c] -= conj(tau) v_r u_c (H^H applied from the left), same grid.
+__global__ void __launch_bounds__(256) k64_hh_update(int rows, int cols, int j, double *m_re, double *m_im,
+                                                     long long ldm, long long m_stride, const double *tau,
+                                                     const double *u) {
+    const int f = blockIdx.z;
+    const int c = j + 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cols) return;
+    double *mr = m_re + (size_t)f * m_stride, *mi = m_im + (size_t)f * m_stride;
+    const double tr = tau[(size_t)f * 2 * cols + 2 * j], ti = -tau[(size_t)f * 2 * cols + 2 * j + 1];
+    if (tr == 0.0 && ti == 0.0) return;
+    const double ur = u[(size_t)f * 2 * cols + 2 * c], ui = u[(size_t)f * 2 * cols + 2 * c + 1];
+    const double wr = tr * ur - ti * ui, wi = tr * ui + ti * ur;   // conj(tau) u_c
+    const int r0 = j + blockIdx.y * kHhRows, r1 = min(rows, r0 + kHhRows);
+    for (int r = r0; r < r1; ++r) {
+        const double vr = r == j ? 1.0 : mr[(size_t)r * ldm + j], vi = r == j ? 0.0 : mi[(size_t)r * ldm + j];
+        mr[(size_t)r * ldm + c] -= vr * wr - vi * wi;
+        mi[(size_t)r * ldm + c] -= vr * wi + vi * wr;
+    }
+}
+
+// R p = y by back substitution, R = the upper triangle of M[0:n][0:n], y =
+// M[0:n][n + s]; p_i = (y_i - sum_{j > i} R_ij p_j) / R_ii.  One CTA per
+// (right-hand side s, matrix); p (F, S, n) complex in global memory.
+__global__ void __launch_bounds__(256) k64_upper_solve(int n, int n_src, const double *m_re, const double *m_im,
+                                                       long long ldm, long long m_stride, double *p) {
+    __shared__ double s_w[8], s_w2[8];
+    const int sv = blockIdx.x, f = blockIdx.y;
+    const double *mr = m_re + (size_t)f * m_stride, *mi = m_im + (size_t)f * m_stride;
+    double *pv = p + ((size_t)f * n_src + sv) * 2 * n;
+    for (int i = n - 1; i >= 0; --i) {
+        const double *rr = mr + (size_t)i * ldm, *ri = mi + (size_t)i * ldm;
+        double ar = 0.0, ai = 0.0;
+        for (int c = i + 1 + threadIdx.x; c < n; c += blockDim.x) {
+            const double xr = pv[2 * c], xi = pv[2 * c + 1];
+            ar += rr[c] * xr - ri[c] * xi;
+            ai += rr[c] * xi + ri[c] * xr;
+        }
+        const double sr = block_sum(ar, s_w), si = block_sum(ai, s_w2);
+        if (threadIdx.x == 0) {
+            const double yr = rr[n + sv] - sr, yi = ri[n + sv] - si;
+            const double dr = rr[i], di = ri[i], den = dr * dr + di * di;
+            pv[2 * i] = den > 0.0 ? (yr * dr + yi * di) / den : 0.0;
+            pv[2 * i + 1] = den > 0.0 ? (yi * dr - yr * di) / den : 0.0;
+        }
+        __syncthreads();
+    }
+}
+
+// x = (float) p; resid = ||s (C p - d)|| / ||b|| per (source, matrix).  One CTA
+// per (source, matrix).
+__global__ void __launch_bounds__(256) k64_chief_finish(int n, int m, int n_src, int nf, const double *p,
+                                                        const double *c_re, const double *c_im, const double *d_re,
+                                                        const double *d_im, const double *scale, const float *b_re,
+                                                        const float *b_im, long long b_stride, long long b_src_stride,
+                                                        float *x_re, float *x_im, long long x_stride,
+                                                        long long x_src_stride, double *resid, long long r_stride) {
+    __shared__ double s_w[8], s_w2[8];
+    const int sv = blockIdx.x, f = blockIdx.y;
+    const double *pv = p + ((size_t)f * n_src + sv) * 2 * n;
+    double bb = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const size_t o = (size_t)sv * x_src_stride + (size_t)f * x_stride + i;
+        x_re[o] = (float)pv[2 * i];
+        x_im[o] = (float)pv[2 * i + 1];
+        const size_t ob = (size_t)sv * b_src_stride + (size_t)f * b_stride + i;
+        bb += (double)b_re[ob] * b_re[ob] + (double)b_im[ob] * b_im[ob];
+    }
+    const double bn2 = block_sum(bb, s_w);
+    double rs = 0.0;
+    for (int ci = 0; ci < m; ++ci) {
+        const double *cr = c_re + ((size_t)f * m + ci) * n, *cim = c_im + ((size_t)f * m + ci) * n;
+        double ar = 0.0, ai = 0.0;
+        for (int c = threadIdx.x; c < n; c += blockDim.x) {
+            ar += cr[c] * pv[2 * c] - cim[c] * pv[2 * c + 1];
+            ai += cr[c] * pv[2 * c + 1] + cim[c] * pv[2 * c];
+        }
+        const double sr = block_sum(ar, s_w), si = block_sum(ai, s_w2);
+        const size_t od = ((size_t)sv * nf + f) * m + ci;
+        const double er = scale[f] * (sr - d_re[od]), ei = scale[f] * (si - d_im[od]);
+        rs += er * er + ei * ei;
+    }
+    if (threadIdx.x == 0 && resid) resid[(size_t)sv * r_stride + f] = bn2 > 0.0 ? sqrt(rs / bn2) : sqrt(rs);
+}
+
 }  // namespace
+
 
 // Duffy rule records (test xi, eta, trial xi, eta, weight) in double: the same
 // Gauss-Legendre 4-point nodes per Duffy coordinate and the same sub-region maps
@@ -1397,4 +1740,132 @@ extern "C" int hbem_coupled_ib_field_f64(hbem_session *h, int n_freq, const doub
         HBEM_LAUNCH_CHECK("k64_rayleigh");
     }
     return HBEM_OK;
+}
+
+// CHIEF least squares for n_freq assembled systems and n_src right-hand sides
+// (see k64_chief_rows): frequencies in chunks of at most 32 whose complex128
+// working copies fit a quarter of the free device memory.
+extern "C" int hbem_chief_lstsq(hbem_session *h, int n_freq, int n_src, const float *k_re, const float *k_im,
+                                const float *q_re, const float *q_im, long long q_stride, long long q_src_stride,
+                                const float *beta_re, const float *beta_im, const float *a_re, const float *a_im,
+                                long long lda, long long a_stride, const float *b_re, const float *b_im,
+                                long long b_stride, long long b_src_stride, const float *chief_3xm, int m,
+                                double weight, float *x_re, float *x_im, long long x_stride, long long x_src_stride,
+                                double *resid, double *scale_out, void *stream) {
+    Session *s = reinterpret_cast<Session *>(h);
+    if (!s) return fail(HBEM_ERR_ARG, "hbem_chief_lstsq: NULL session");
+    if (n_freq <= 0) return HBEM_OK;
+    if (n_src < 1 || n_src > kMaxChiefSrc) return fail(HBEM_ERR_ARG, "hbem_chief_lstsq: 1 .. 8 sources");
+    if (!k_re || !a_re || !a_im || !b_re || !b_im || !x_re || !x_im || !chief_3xm || !q_re || !q_im)
+        return fail(HBEM_ERR_ARG, "hbem_chief_lstsq: NULL pointer");
+    if ((beta_re == nullptr) != (beta_im == nullptr)) return fail(HBEM_ERR_ARG, "hbem_chief_lstsq: beta_re/beta_im");
+    const int n = s->n_dof, T = s->n_triangles;
+    if (m < 1) return fail(HBEM_ERR_ARG, "hbem_chief_lstsq: at least one CHIEF point");
+    if (!(weight > 0.0) || !std::isfinite(weight)) return fail(HBEM_ERR_ARG, "hbem_chief_lstsq: weight must be finite and positive");
+    if (lda < n || a_stride < lda * (long long)n || b_stride < n || x_stride < n || q_stride < T ||
+        (n_src > 1 && (b_src_stride < b_stride * n_freq || x_src_stride < x_stride * n_freq ||
+                       q_src_stride < q_stride * n_freq)))
+        return fail(HBEM_ERR_ARG, "hbem_chief_lstsq: strides too small");
+    for (int i = 0; i < 3 * m; ++i)
+        if (!std::isfinite(chief_3xm[i])) return fail(HBEM_ERR_ARG, "hbem_chief_lstsq: CHIEF points must be finite");
+    for (int f = 0; f < n_freq; ++f)
+        if (!std::isfinite(k_re[f]) || (k_im && !std::isfinite(k_im[f])))
+            return fail(HBEM_ERR_ARG, "hbem_chief_lstsq: wavenumbers must be finite");
+    HBEM_CUDA(cudaSetDevice(s->device));
+    int rc = ensure_geo64(*s);
+    if (rc != HBEM_OK) return rc;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const int rows = n + m, cols = n + n_src;
+    const long long ldm = cols, m_stride = (long long)rows * ldm;
+    size_t free_b = 0, total_b = 0;
+    HBEM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t per_f = (size_t)m_stride * 16 + (size_t)m * n * 16 + (size_t)n_src * (m + 2 * n) * 16 + 64 * (size_t)cols;
+    int chunk = (int)std::min<size_t>((size_t)kMaxF64, std::max<size_t>(1, free_b / 4 / per_f));
+    const int fc_max = std::min(chunk, n_freq);
+    // scratch of one chunk
+    const size_t nC = (size_t)fc_max * m * n, nD = (size_t)n_src * fc_max * m, nM = (size_t)fc_max * m_stride;
+    const size_t nT = (size_t)fc_max * 2 * cols, nP = (size_t)fc_max * n_src * 2 * n;
+    const size_t bytes = sizeof(double) * (2 * nC + 2 * nD + 2 * nM + 2 * nT + nP + fc_max) +
+                         sizeof(unsigned long long) * 2 * fc_max + sizeof(float) * 3 * m + 256;
+    unsigned char *mem = nullptr;
+    HBEM_CUDA(cudaMallocAsync((void **)&mem, bytes, st));
+    double *c_re = reinterpret_cast<double *>(mem), *c_im = c_re + nC;
+    double *d_re = c_im + nC, *d_im = d_re + nD;
+    double *m_re = d_im + nD, *m_im = m_re + nM;
+    double *tau = m_im + nM, *u = tau + nT, *pv = u + nT, *sc = pv + nP;
+    unsigned long long *anorm = reinterpret_cast<unsigned long long *>(sc + fc_max), *cnorm = anorm + fc_max;
+    float *pts = reinterpret_cast<float *>(cnorm + fc_max);
+    auto done = [&](int r) {
+        cudaFreeAsync(mem, st);
+        return r;
+    };
+    auto launched = [&](const char *what) -> int {
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(e, what);
+        count_launch();
+        ++s->launches;
+        return HBEM_OK;
+    };
+    if (cudaMemcpyAsync(pts, chief_3xm, sizeof(float) * 3 * m, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return done(cuda_fail(cudaGetLastError(), "hbem_chief_lstsq: points"));
+    for (int f0 = 0; f0 < n_freq; f0 += fc_max) {
+        const int fc = std::min(fc_max, n_freq - f0);
+        cudaError_t e = cudaMemsetAsync(c_re, 0, sizeof(double) * (2 * nC + 2 * nD), st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(anorm, 0, sizeof(unsigned long long) * 2 * fc_max, st);
+        if (e != cudaSuccess) return done(cuda_fail(e, "hbem_chief_lstsq: memset"));
+        ChiefArgs ca{};
+        ca.g = geo64(*s);
+        ca.pts = pts;
+        ca.q_re = q_re + (size_t)f0 * q_stride;
+        ca.q_im = q_im + (size_t)f0 * q_stride;
+        ca.q_stride = q_stride;
+        ca.q_src_stride = q_src_stride;
+        ca.beta_re = beta_re;
+        ca.beta_im = beta_im;
+        ca.c_re = c_re; ca.c_im = c_im; ca.d_re = d_re; ca.d_im = d_im;
+        ca.m = m; ca.n = n; ca.n_src = n_src; ca.nf = fc;
+        for (int f = 0; f < fc; ++f) {
+            ca.kr[f] = k_re[f0 + f];
+            ca.ki[f] = k_im ? k_im[f0 + f] : 0.0;
+        }
+        k64_chief_rows<<<dim3((T + 255) / 256, m, fc), 256, 0, st>>>(ca);
+        if ((rc = launched("k64_chief_rows")) != HBEM_OK) return done(rc);
+        k64_inf_norm<float><<<dim3((n + 7) / 8, fc), 256, 0, st>>>(n, n, a_re + (size_t)f0 * a_stride,
+                                                                  a_im + (size_t)f0 * a_stride, lda, a_stride, anorm);
+        if ((rc = launched("k64_inf_norm")) != HBEM_OK) return done(rc);
+        k64_inf_norm<double><<<dim3((m + 7) / 8, fc), 256, 0, st>>>(m, n, c_re, c_im, n, (long long)m * n, cnorm);
+        if ((rc = launched("k64_inf_norm")) != HBEM_OK) return done(rc);
+        ChiefBuildArgs ba{};
+        ba.a_re = a_re + (size_t)f0 * a_stride; ba.a_im = a_im + (size_t)f0 * a_stride;
+        ba.lda = lda; ba.a_stride = a_stride;
+        ba.b_re = b_re + (size_t)f0 * b_stride; ba.b_im = b_im + (size_t)f0 * b_stride;
+        ba.b_stride = b_stride; ba.b_src_stride = b_src_stride;
+        ba.c_re = c_re; ba.c_im = c_im; ba.d_re = d_re; ba.d_im = d_im;
+        ba.anorm = anorm; ba.cnorm = cnorm;
+        ba.m_re = m_re; ba.m_im = m_im; ba.ldm = ldm; ba.m_stride = m_stride;
+        ba.scale = sc; ba.weight = weight;
+        ba.n = n; ba.m = m; ba.n_src = n_src; ba.nf = fc;
+        const long long elems = (long long)rows * cols;
+        k64_chief_build<<<dim3((unsigned)std::min<long long>((elems + 255) / 256, 4096), fc), 256, 0, st>>>(ba);
+        if ((rc = launched("k64_chief_build")) != HBEM_OK) return done(rc);
+        for (int j = 0; j < n; ++j) {
+            k64_hh_reflector<<<fc, 256, 0, st>>>(rows, cols, j, m_re, m_im, ldm, m_stride, tau, u);
+            if ((rc = launched("k64_hh_reflector")) != HBEM_OK) return done(rc);
+            const dim3 g((cols - j - 1 + 255) / 256, (rows - j + kHhRows - 1) / kHhRows, fc);
+            k64_hh_dot<<<g, 256, 0, st>>>(rows, cols, j, m_re, m_im, ldm, m_stride, u);
+            if ((rc = launched("k64_hh_dot")) != HBEM_OK) return done(rc);
+            k64_hh_update<<<g, 256, 0, st>>>(rows, cols, j, m_re, m_im, ldm, m_stride, tau, u);
+            if ((rc = launched("k64_hh_update")) != HBEM_OK) return done(rc);
+        }
+        k64_upper_solve<<<dim3(n_src, fc), 256, 0, st>>>(n, n_src, m_re, m_im, ldm, m_stride, pv);
+        if ((rc = launched("k64_upper_solve")) != HBEM_OK) return done(rc);
+        k64_chief_finish<<<dim3(n_src, fc), 256, 0, st>>>(
+            n, m, n_src, fc, pv, c_re, c_im, d_re, d_im, sc, b_re + (size_t)f0 * b_stride, b_im + (size_t)f0 * b_stride,
+            b_stride, b_src_stride, x_re + (size_t)f0 * x_stride, x_im + (size_t)f0 * x_stride, x_stride,
+            x_src_stride, resid ? resid + f0 : nullptr, n_freq);
+        if ((rc = launched("k64_chief_finish")) != HBEM_OK) return done(rc);
+        if (scale_out && cudaMemcpyAsync(scale_out + f0, sc, sizeof(double) * fc, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+            return done(cuda_fail(cudaGetLastError(), "hbem_chief_lstsq: scale"));
+    }
+    return done(HBEM_OK);
 }

@@ -1830,13 +1830,15 @@ static int lookahead_streams(cudaStream_t key, LookaheadStreams **out) {
     return HBEM_OK;
 }
 
-// The plain LU's look-ahead bulk update on the tensor cores (TF32x3) unless
-// exact FP32 products are asked for: measured on one B200, n = 1043 x 40
+// The plain LU's look-ahead bulk update on the tensor cores (TF32x3) when
+// asked for (HBEM_TUNE_LU_UPDATE = 2).  Measured on one B200: n = 1043 x 40
 // factors in 6.7 instead of 7.3 ms, 4096 x 4 in 28.2 instead of 29.6 ms and
-// 18 749 x 2 in 701 instead of 1130 ms, with residuals of 6e-7 to 1e-6
-// against 4e-7 to 9e-7 for the CUDA-core update.
+// 18 749 x 2 in 701 instead of 1130 ms; but the split products keep 22 of
+// FP32's 24 significand bits, and on a BEM matrix (the 1952-dof quarter horn)
+// the unrefined solution is 5.5e-5 from LAPACK instead of the FP32 LU's
+// < 1e-5, so the default stays the exact-FP32 CUDA-core update (cgesv).
 static bool plain_update_on_tensor_cores() {
-    return tuning(HBEM_TUNE_LU_UPDATE) != 1;
+    return tuning(HBEM_TUNE_LU_UPDATE) == 2;
 }
 
 int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long long a_stride, int *piv,
@@ -1854,7 +1856,17 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
     // column, wait for it.  The tensor-core workspace and status word are
     // only used on the bulk stream (and on the chain after it has joined).
     const size_t smem_cap = 200 * 1024;
-    const int NB = (precision == HBEM_PREC_MIXED && n > 256 && tuning(HBEM_TUNE_LU_BLOCK) != 64) ? 128 : 64;
+    // 128-column blocks (one K = 128 update per block, half the C stream of
+    // K = 64) pay where few large matrices leave the update bound by that
+    // stream: 18 749 x 2 factors in 417 instead of 498 ms; with more
+    // matrices or smaller ones the longer chain of the 128-wide panels costs
+    // more (10 000 x 2: 98 vs 83 ms; 4096 x 4: 25 vs 21 ms; the 20 systems of
+    // 18 749 of the coupled-baffle sweep: 3.7 vs 3.1 s)
+    const int blk_want = tuning(HBEM_TUNE_LU_BLOCK);
+    const int NB = (precision == HBEM_PREC_MIXED && n > 256 &&
+                    (blk_want == 128 || (blk_want == 0 && n > 16000 && batch <= 4)))
+                       ? 128
+                       : 64;
     HBEM_CUDA(cudaMemsetAsync(info, 0, sizeof(int) * batch, st));
     // K = 64 block updates on the tensor cores: BF16x3 (mixed precision), or
     // TF32x3 for the plain LU's look-ahead bulk when selected; their barrier

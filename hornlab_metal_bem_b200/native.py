@@ -74,6 +74,8 @@ _SIGNATURES = {
                      _c_ll, _c_d, _c_int, _vp, _vp, _vp], _c_int),
     "hbem_refine_noalloc": ([_c_int, _c_int, _vp, _vp, _c_ll, _c_ll, _vp, _vp, _c_ll, _vp, _c_ll, _vp, _vp, _c_ll, _vp,
                              _vp, _c_ll, _c_d, _c_int, _vp, _vp, _vp], _c_int),
+    "hbem_chief_lstsq": ([_vp, _c_int, _c_int, _vp, _vp, _vp, _vp, _c_ll, _c_ll, _vp, _vp, _vp, _vp, _c_ll, _c_ll,
+                          _vp, _vp, _c_ll, _c_ll, _vp, _c_int, _c_d, _vp, _vp, _c_ll, _c_ll, _vp, _vp, _vp], _c_int),
     "hbem_refine_async": ([_c_int, _c_int, _vp, _vp, _c_ll, _c_ll, _vp, _vp, _c_ll, _vp, _c_ll, _vp, _vp, _c_ll, _vp,
                            _vp, _c_ll, _c_d, _c_int, _vp, _vp, _vp], _c_int),
     "hbem_field": ([_vp, _c_int, _vp, _vp, _vp, _c_ll, _vp, _vp, _c_ll, _vp, _c_int, _vp, _vp, _c_ll, _vp], _c_int),
@@ -270,6 +272,7 @@ class ExtraSourceResult:
     surface_pressure: np.ndarray | None
     refine_iterations: int = 0
     refine_residual_rel: float | None = None
+    chief_residual_rel: float | None = None   # CHIEF solves: ||s (C p - d)|| / ||b|| of this source
 
 
 MAX_SOURCES_PER_PASS = 8
@@ -575,6 +578,8 @@ class NativeSession:
         impedance_sources=None,
         extra_neumann_dp0=None,
         extra_impedance_source_tags=None,
+        chief_points=None,
+        chief_weight: float = 1.0,
         **_ignored,
     ) -> list[CaseResult]:
         """Assemble, factor, solve and evaluate every frequency in one native call.
@@ -592,6 +597,11 @@ class NativeSession:
         plain LU solution as cgesv gives it.  ``compute_rcond`` adds the
         1-norm condition estimate of each matrix (``dense_solve_rcond``), as the
         reference computes with cgecon for every case.
+
+        ``chief_points`` (3, m) interior points switch every case to the CHIEF least-squares solve
+        (``hbem_chief_lstsq``: the boundary system stacked on the interior collocation rows, weighted by
+        ``chief_weight``, solved in complex128; the reference's zgels path, ``main.swift:1897-2036,
+        7186-7409``); each result's diagnostics carry ``chief_residual_rel``.
 
         ``extra_neumann_dp0`` (n_extra, F, T) adds velocity sources that share
         each frequency's assembled and factored matrix (the reference's
@@ -620,6 +630,32 @@ class NativeSession:
                 raise ValueError("extra_impedance_source_tags must name one tag (or None) per extra source")
         elif extra_impedance_source_tags is not None:
             raise ValueError("extra_impedance_source_tags requires extra_neumann_dp0")
+        if chief_points is not None:
+            pts = np.asarray(chief_points, dtype=np.float32)
+            if pts.ndim != 2 or pts.shape[0] != 3:
+                raise ValueError("chief_points must have shape (3, m)")
+            if pts.shape[1] == 0:
+                raise ValueError("chief_points must be non-empty when set")
+            if not np.all(np.isfinite(pts)):
+                raise ValueError("chief_points must be finite")
+            if not (np.isfinite(chief_weight) and float(chief_weight) > 0):
+                raise ValueError("chief_weight must be finite and positive")
+            per = None
+            if impedance_sources:
+                per = impedance_sources if isinstance(impedance_sources, list) else [impedance_sources] * F
+                if len(per) != F:
+                    raise ValueError(f"impedance_sources list must have one dict per frequency ({F}), got {len(per)}")
+                if not any(per):
+                    per = None
+            q = np.asarray(neumann_dp0)
+            if q.shape != (F, self.n_triangles) or not np.all(np.isfinite(q)):
+                raise ValueError(f"neumann_dp0 must be finite with shape {(F, self.n_triangles)}")
+            qs = q[None] if extra is None else np.concatenate([q[None], extra], axis=0)
+            return self._chief_batch(freqs, k_re, k_imag_f32, qs, observation_points, per, pts, float(chief_weight),
+                                     source_tags=source_tags, impedance_source_tag=impedance_source_tag,
+                                     extra_tags=(list(extra_impedance_source_tags) if extra_impedance_source_tags
+                                                 else [None] * (qs.shape[0] - 1)),
+                                     write_surface_pressure=write_surface_pressure, timings_out=timings_out)
         if impedance_sources:
             per = impedance_sources if isinstance(impedance_sources, list) else [impedance_sources] * F
             if len(per) != F:
@@ -743,6 +779,147 @@ class NativeSession:
             ))
         return results
 
+
+    # -- CHIEF least squares ----------------------------------------------------
+    def _chief_batch(self, freqs, k_re, k_imag_f32, qs, observation_points, per_freq, chief_pts, chief_weight, *,
+                     source_tags, impedance_source_tag, extra_tags, write_surface_pressure, timings_out):
+        """CHIEF sweep: the FP32 corrected assembly of every source's right-hand side (with Robin admittances
+        when ``per_freq`` gives them, frequencies with equal sets sharing one launch), then
+        ``hbem_chief_lstsq`` (interior collocation rows, complex128 Householder least squares of the stacked
+        system), and the field and tag averages of its solution; the field's Neumann data carry the Robin
+        term q + i k beta p_avg (``main.swift:1646-1674``)."""
+        torch = require_cuda()
+        dev = torch.device("cuda", self.device)
+        st = _stream_ptr()
+        F, n, T = freqs.shape[0], self.n_dof, self.n_triangles
+        S = qs.shape[0]
+        if S > MAX_SOURCES_PER_PASS:
+            raise ValueError(f"CHIEF solves take at most {MAX_SOURCES_PER_PASS} sources per call")
+        k_im = (np.zeros(F, np.float32) if k_imag_f32 is None
+                else np.ascontiguousarray(np.atleast_1d(k_imag_f32), dtype=np.float32))
+        obs = np.asarray(observation_points, dtype=np.float64)
+        if obs.shape[0] != 3:
+            obs = obs.T
+        obs_t = torch.tensor(np.ascontiguousarray(obs, dtype=np.float32), device=dev)
+        N = obs_t.shape[1]
+        pts = np.ascontiguousarray(chief_pts, dtype=np.float32)
+        m = pts.shape[1]
+        tags_tri = np.asarray(self.buffers.physical_tags_i32)
+        l2g = torch.as_tensor(np.asarray(self.buffers.p1_local2global_i32, dtype=np.int64), device=dev)
+        tags = list(source_tags or [])
+        want = list(tags)
+        for t in [impedance_source_tag] + list(extra_tags):
+            if t is not None and t not in want:
+                want.append(t)
+        out_field = np.zeros((S, F, N), np.complex64)
+        out_p = np.zeros((S, F, n), np.complex64)
+        out_tavg = np.zeros((S, F, max(1, len(want))), np.complex128)
+        out_res = np.zeros((S, F))
+        out_scale = np.zeros(F)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        t_asm = t_solve = t_field = 0.0
+        groups, start = [], 0
+        for f in range(1, F + 1):
+            if f == F or (per_freq is not None and per_freq[f] != per_freq[start]):
+                groups.append((start, f))
+                start = f
+        for g0, g1 in groups:
+            Fg = g1 - g0
+            sl = slice(g0, g1)
+            b_re = b_im = None
+            if per_freq is not None and per_freq[g0]:
+                beta = np.zeros(T, np.complex64)
+                for tag, bv in per_freq[g0].items():
+                    beta[tags_tri == int(tag)] = complex(bv)
+                b_re = torch.tensor(np.ascontiguousarray(beta.real), device=dev)
+                b_im = torch.tensor(np.ascontiguousarray(beta.imag), device=dev)
+            qg = qs[:, sl]
+            qr = torch.tensor(np.ascontiguousarray(qg.real, dtype=np.float32), device=dev)
+            qi = torch.tensor(np.ascontiguousarray(qg.imag, dtype=np.float32), device=dev)
+            Ar = torch.empty((Fg, n, n), dtype=torch.float32, device=dev)
+            Ai = torch.empty_like(Ar)
+            br = torch.empty((S, Fg, n), dtype=torch.float32, device=dev)
+            bi = torch.empty_like(br)
+            kr_g, ki_g = np.ascontiguousarray(k_re[sl]), np.ascontiguousarray(k_im[sl])
+            ev[0].record()
+            check(self.lib.hbem_assemble_multi(
+                self.handle, Fg, _np_ptr(kr_g), _np_ptr(ki_g), S, _t_ptr(qr), _t_ptr(qi), T, Fg * T, _t_ptr(b_re),
+                _t_ptr(b_im), _t_ptr(Ar), _t_ptr(Ai), n, n * n, _t_ptr(br), _t_ptr(bi), n, Fg * n,
+                HBEM_ASM_CORRECTED | HBEM_ASM_ZERO, st), "hbem_assemble_multi", self.lib)
+            ev[1].record()
+            xr = torch.empty((S, Fg, n), dtype=torch.float32, device=dev)
+            xi = torch.empty_like(xr)
+            res = torch.zeros((S, Fg), dtype=torch.float64, device=dev)
+            scl = torch.zeros(Fg, dtype=torch.float64, device=dev)
+            check(self.lib.hbem_chief_lstsq(
+                self.handle, Fg, S, _np_ptr(kr_g), _np_ptr(ki_g), _t_ptr(qr), _t_ptr(qi), T, Fg * T, _t_ptr(b_re),
+                _t_ptr(b_im), _t_ptr(Ar), _t_ptr(Ai), n, n * n, _t_ptr(br), _t_ptr(bi), n, Fg * n, _np_ptr(pts), m,
+                chief_weight, _t_ptr(xr), _t_ptr(xi), n, Fg * n, _t_ptr(res), _t_ptr(scl), st),
+                "hbem_chief_lstsq", self.lib)
+            del Ar, Ai
+            ev[2].record()
+            for s_ in range(S):
+                xs_r, xs_i = xr[s_].contiguous(), xi[s_].contiguous()
+                qtr, qti = qr[s_].contiguous(), qi[s_].contiguous()
+                if b_re is not None:
+                    p_c = torch.complex(xs_r, xs_i)
+                    p_avg = (p_c[:, l2g[:, 0]] + p_c[:, l2g[:, 1]] + p_c[:, l2g[:, 2]]) / 3.0
+                    ik = torch.complex(torch.tensor(-ki_g, device=dev), torch.tensor(kr_g, device=dev))[:, None]
+                    q_tot = torch.complex(qtr, qti) + ik * torch.complex(b_re, b_im)[None, :] * p_avg
+                    qtr, qti = q_tot.real.contiguous(), q_tot.imag.contiguous()
+                fr = torch.empty((Fg, N), dtype=torch.float32, device=dev)
+                fi = torch.empty_like(fr)
+                check(self.lib.hbem_field(self.handle, Fg, _np_ptr(kr_g), _t_ptr(xs_r), _t_ptr(xs_i), n,
+                                          _t_ptr(qtr), _t_ptr(qti), T, _t_ptr(obs_t), N, _t_ptr(fr), _t_ptr(fi), N,
+                                          st), "hbem_field", self.lib)
+                tavg = self.tag_average(xs_r, xs_i, want).cpu().numpy() if want else None
+                out_field[s_, sl] = (fr.cpu().numpy() + 1j * fi.cpu().numpy()).astype(np.complex64)
+                out_p[s_, sl] = (xs_r.cpu().numpy() + 1j * xs_i.cpu().numpy()).astype(np.complex64)
+                if tavg is not None:
+                    out_tavg[s_, sl] = tavg[..., 0] + 1j * tavg[..., 1]
+            ev[3].record()
+            torch.cuda.synchronize()
+            t_asm += ev[0].elapsed_time(ev[1])
+            t_solve += ev[1].elapsed_time(ev[2])
+            t_field += ev[2].elapsed_time(ev[3])
+            out_res[:, sl] = res.cpu().numpy()
+            out_scale[sl] = scl.cpu().numpy()
+        if timings_out is not None:
+            timings_out.update(assembly_ms=t_asm, solve_ms=t_solve, field_ms=t_field, total_ms=t_asm + t_solve + t_field,
+                               sources=S)
+        results = []
+        for f in range(F):
+            avgs = [{int(t): complex(out_tavg[s_, f, j]) for j, t in enumerate(want)} for s_ in range(S)]
+            diag = {"dense_solve_impl": "householder_qr_lstsq_f64", "dense_solve_dtype": "float64",
+                    "precision": "plain", "refine_iterations": 0, "refine_residual_rel": None,
+                    "dense_solve_rcond": None, "assembly_mode": "corrected",
+                    "chief_points": True, "chief_point_count": int(m), "chief_weight": float(chief_weight),
+                    "chief_scale": float(out_scale[f]), "chief_residual_rel": float(out_res[0, f]),
+                    **_case_flags(float(k_re[f]), float(k_im[f]), robin=per_freq is not None and bool(per_freq[f]))}
+            if per_freq is not None and per_freq[f]:
+                diag["robin_tags"] = sorted(int(t) for t in per_freq[f])
+            if S > 1:
+                diag["multi_source"] = True
+                diag["sources_sharing_factorisation"] = S
+            if self.near_quadrature is not None:
+                diag["near_quadrature"] = dict(self.near_quadrature)
+            extras = tuple(
+                ExtraSourceResult(
+                    source_index=s_, field=out_field[s_, f],
+                    impedance=(avgs[s_].get(int(extra_tags[s_ - 1])) if extra_tags[s_ - 1] is not None else None),
+                    surface_pressure_avg={int(t): avgs[s_][int(t)] for t in tags} if tags else None,
+                    surface_pressure=out_p[s_, f] if write_surface_pressure else None,
+                    refine_iterations=0, refine_residual_rel=None, chief_residual_rel=float(out_res[s_, f]),
+                ) for s_ in range(1, S))
+            results.append(CaseResult(
+                frequency_hz=float(freqs[f]), field=out_field[0, f],
+                impedance=avgs[0].get(int(impedance_source_tag)) if impedance_source_tag is not None else None,
+                surface_pressure_avg={int(t): avgs[0][int(t)] for t in tags} if tags else None,
+                surface_pressure=out_p[0, f] if write_surface_pressure else None,
+                assembly_s=t_asm * 1e-3 / F, dense_solve_s=t_solve * 1e-3 / F, field_s=t_field * 1e-3 / F,
+                lapack_info=0, diagnostics=diag, extra_sources=extras,
+            ))
+        return results
 
     # -- Robin (impedance) boundaries -----------------------------------------
     def _robin_batch(self, freqs, k_re, k_imag_f32, neumann_dp0, observation_points, per_freq, *, source_tags,

@@ -40,9 +40,32 @@ def should_route_native(config: SolveConfig) -> bool:
         raise BackendUnavailable(
             "native_symmetry_plane must be None or one of " + ", ".join(repr(p) for p in NATIVE_SYMMETRY_PLANES)
         )
-    if config.chief_points is not None:
-        raise BackendUnavailable("chief_points (CHIEF least squares) is not supported by the B200 path")
+    if config.chief_points is not None and config.aperture_tag is not None:
+        raise BackendUnavailable("chief_points with the coupled infinite baffle (aperture_tag): the coupled "
+                                 "solve has no CHIEF rows")
     return True
+
+
+def warn_near_boundary_chief_points(mesh: LoadedMesh, chief_points, max_edge_m: float) -> int:
+    """Warn when CHIEF points sit within half the largest edge of the boundary (distance to the nearest
+    vertex or triangle centroid): their constraint rows are exact only strictly inside the body, and a
+    near-wall row biases the least squares with no error signal (the reference's check,
+    ``sweep.py:342-380``).  Returns the number of such points."""
+    vertices = np.asarray(mesh.grid.vertices, dtype=np.float64).T
+    elements = np.asarray(mesh.grid.elements, dtype=np.int64).T
+    if elements.size == 0 or max_edge_m <= 0.0:
+        return 0
+    anchors = np.vstack([vertices, vertices[elements].mean(axis=1)])
+    pts = np.asarray(chief_points, dtype=np.float64).reshape(-1, 3)
+    d2 = ((pts[:, None, :] - anchors[None, :, :]) ** 2).sum(axis=2)
+    min_d = np.sqrt(d2.min(axis=1))
+    near = np.nonzero(min_d < 0.5 * float(max_edge_m))[0]
+    if near.size:
+        worst = int(near[np.argmin(min_d[near])])
+        logger.warning("%d of %d chief_points sit within 0.5*max_edge (%.4g m) of the boundary mesh (closest: "
+                       "point %d at %.4g m); CHIEF points must be strictly interior", int(near.size),
+                       int(pts.shape[0]), 0.5 * float(max_edge_m), worst, float(min_d[worst]))
+    return int(near.size)
 
 
 def impedance_sources_for_frequencies(physical_tags, frequencies, config: SolveConfig):
@@ -220,6 +243,10 @@ def _run_sweep_sources(mesh: LoadedMesh, frequencies, frame: ObservationFrame, c
         qs.append(neumann_rows(buffers.n_triangles, mesh.physical_tags, freqs, c, scale, robin))
     q = qs[0]
     extra = np.stack(qs[1:], axis=0) if n_src > 1 else None
+    chief = None
+    if config.chief_points is not None:
+        chief = np.ascontiguousarray(np.asarray(config.chief_points, dtype=np.float64).T, dtype=np.float32)
+        warn_near_boundary_chief_points(mesh, config.chief_points, max_edge)
 
     own = session is None
     if own:
@@ -239,6 +266,8 @@ def _run_sweep_sources(mesh: LoadedMesh, frequencies, frame: ObservationFrame, c
             kw = {}
             if extra is not None:
                 kw = dict(extra_neumann_dp0=extra[:, sl], extra_impedance_source_tags=imp_tags[1:])
+            if chief is not None:
+                kw.update(chief_points=chief, chief_weight=config.chief_weight)
             results = batch_fn(
                 freqs[sl], k_re[sl], q[sl], pts, k_imag_f32=k_im[sl], source_tags=source_tags,
                 impedance_source_tag=imp_tags[0], write_surface_pressure=config.return_surface_pressure,

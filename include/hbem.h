@@ -45,8 +45,8 @@ extern "C" {
 #define HBEM_ASM_CORRECTED (HBEM_ASM_REGULAR | HBEM_ASM_DUFFY | HBEM_ASM_ZERO)
 
 /* LU precision */
-#define HBEM_PREC_PLAIN 0      /* FP32-class LU (complex64 cgesv): inner updates FP32 on CUDA cores, the
-                                  look-ahead bulk TF32x3 on the tensor cores (HBEM_TUNE_LU_UPDATE) */
+#define HBEM_PREC_PLAIN 0      /* FP32 LU (complex64 cgesv semantics); HBEM_TUNE_LU_UPDATE = 2 moves its
+                                  look-ahead bulk update to the tensor cores (TF32x3) */
 #define HBEM_PREC_MIXED 1      /* BF16x3 tensor-core trailing updates; pair with hbem_refine */
 #define HBEM_PREC_FP64 2       /* hbem_solve_batch only: complex128 LU of the widened FP32 system (zgesv semantics) */
 
@@ -122,12 +122,13 @@ long long hbem_launch_count(void);
  *                            synchronising entry points as HBEM_ERR_STATE
  *   HBEM_TUNE_LU_UPDATE:     the K = 64 trailing update of the plain
  *                            (FP32) LU beside the factorisation chain
- *                            (1: CUDA cores, exact FP32 products; 2 and the
- *                            built-in 0: tensor cores, TF32x3 split
- *                            products, FP32-class)
+ *                            (1 and the built-in 0: CUDA cores, exact FP32
+ *                            products; 2: tensor cores, TF32x3 split
+ *                            products, 22 significand bits per operand)
  *   HBEM_TUNE_LU_BLOCK:      column block of the mixed (BF16x3) LU and the K
  *                            of its tensor-core update (64 or 128; 0: the
- *                            built-in 128 for n > 256, else 64)
+ *                            built-in 128 for n > 16000 with at most four
+ *                            matrices, else 64)
  */
 #define HBEM_TUNE_ASM_MINBLOCKS 0
 #define HBEM_TUNE_LU_PANEL 1
@@ -282,6 +283,30 @@ int hbem_refine_async(int n, int batch, const float *a_re, const float *a_im, lo
                       const float *b_re, const float *b_im, long long b_stride,
                       float *x_re, float *x_im, long long x_stride,
                       double tol, int max_iter, int *iters, double *resid, void *stream);
+
+/*
+ * CHIEF least squares (reference assembleChiefRows + solveDenseLeastSquaresZgels,
+ * main.swift:1897-2036, 7186-7409): for each of n_freq assembled systems
+ * A x = b (FP32, as hbem_assemble leaves them, n_src right-hand sides) and m
+ * interior points, the collocation rows C p = d of the vanishing exterior
+ * representation (D, G at the real wavenumber, images, the Robin fold
+ * -(int G) (i k beta) / 3 per P1 column with the complex one; d = sum (int G) g)
+ * are built in FP64 and  min || [A; s C] p - [b; s d] ||_2,  s = weight *
+ * ||A||_inf / ||C||_inf, is solved in complex128 by Householder QR; x =
+ * (float) p.  q (device, (n_src, n_freq, T)): the driving Neumann data g;
+ * beta (device, (T,)) or NULL; k_re/k_im host (k_im may be NULL);
+ * chief_3xm host (3, m) float.  resid (device (n_src, n_freq), optional):
+ * ||s (C p - d)||_2 / ||b||_2 (the reference's chief_residual_rel); scale_out
+ * (device (n_freq,), optional): s.  Asynchronous on `stream`.
+ */
+int hbem_chief_lstsq(hbem_session *s, int n_freq, int n_src, const float *k_re, const float *k_im,
+                     const float *q_re, const float *q_im, long long q_stride, long long q_src_stride,
+                     const float *beta_re, const float *beta_im,
+                     const float *a_re, const float *a_im, long long lda, long long a_stride,
+                     const float *b_re, const float *b_im, long long b_stride, long long b_src_stride,
+                     const float *chief_3xm, int m, double weight,
+                     float *x_re, float *x_im, long long x_stride, long long x_src_stride,
+                     double *resid, double *scale_out, void *stream);
 
 /*
  * 1-norm condition estimate, as LAPACK cgecon (norm '1') on the factors.

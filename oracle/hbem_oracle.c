@@ -20,6 +20,7 @@
  *   - singular / regular / subdivided pair blocks        main.swift:2701-2973
  *   - CPU Duffy correction with FP64 triplet sums        main.swift:2974-3070
  *   - tag-average surface pressure                       main.swift:807-841
+ *   - CHIEF interior collocation rows                    main.swift:1897-2036
  *
  * REAL is float (oracle "f32": same arithmetic type as the reference) or
  * double (oracle "f64": the accuracy oracle).  GREAL, the type of the
@@ -883,6 +884,72 @@ int OGP(field)(const og_geom *g, REAL kr, const REAL *p_re, const REAL *p_im,
         out_im[o] = acc.im;
     }
     return 0;
+}
+
+/* ---- CHIEF rows (main.swift:1897-2036) --------------------------------
+ * Interior point x_c: one collocation row of the exterior representation,
+ * which vanishes inside the body:
+ *   sum_tri sum_images int D(x_c, y) p(y) - G(x_c, y) q(y) dy = 0,
+ *   q = g + i k beta Pi p  (Robin: Pi p = the triangle's P1 mean).
+ * Hence C p = d with C[c][dof] = sum int D phi_dof - (int G) (i k beta) / 3
+ * and d[c] = sum_tri (int G) g_tri.  D and G take the real wavenumber (the
+ * field kernels); i k of the Robin fold takes the complex one (kr + i ki);
+ * no jump term, no symmetry row weight.  C is row-major (m, n_dof).
+ * Returns ||C||_inf, the largest row sum of |c|. */
+double OGP(chief_rows)(const og_geom *g, const float *pts3xM, int m, REAL kr, REAL ki, const REAL *beta_re,
+                       const REAL *beta_im, const REAL *q_re, const REAL *q_im, REAL *c_re, REAL *c_im,
+                       REAL *d_re, REAL *d_im) {
+    int T = g->n_triangles, n = g->n_dof;
+    int masks[3];
+    int nm = mirror_masks(g->sym, masks);
+    double cnorm = 0;
+#pragma omp parallel for schedule(static) reduction(max : cnorm)
+    for (int ci = 0; ci < m; ++ci) {
+        REAL ox = pts3xM[ci], oy = pts3xM[m + ci], oz = pts3xM[2 * m + ci];
+        REAL *cr = c_re + (size_t)ci * n, *cim = c_im + (size_t)ci * n;
+        for (int j = 0; j < n; ++j) cr[j] = cim[j] = 0;
+        cplx dsum = {0, 0};
+        for (int tri = 0; tri < T; ++tri) {
+            REAL nn[3] = {g->normals[tri], g->normals[T + tri], g->normals[2 * T + tri]};
+            REAL jac = (REAL)2 * (REAL)g->areas[tri];
+            cplx dc[3] = {{0, 0}, {0, 0}, {0, 0}}, gs = {0, 0};
+            for (int a = 0; a < 6; ++a) {
+                REAL sp[3], b[3];
+                point_on(g, tri, (REAL)QX[a], (REAL)QY[a], sp);
+                basis((REAL)QX[a], (REAL)QY[a], b);
+                REAL w = (REAL)QW[a] * jac;
+                for (int im = -1; im < nm; ++im) {
+                    REAL ip[3] = {sp[0], sp[1], sp[2]}, in[3] = {nn[0], nn[1], nn[2]};
+                    if (im >= 0) {
+                        mirror(ip, masks[im]);
+                        mirror(in, masks[im]);
+                    }
+                    cplx D = dlp(ip[0] - ox, ip[1] - oy, ip[2] - oz, in[0], in[1], in[2], kr, 0);
+                    cplx G = green(ip[0] - ox, ip[1] - oy, ip[2] - oz, kr, 0);
+                    for (int l = 0; l < 3; ++l) dc[l] = cadd(dc[l], cscale(D, b[l] * w));
+                    gs = cadd(gs, cscale(G, w));
+                }
+            }
+            cplx qv = {q_re ? q_re[tri] : 0, q_im ? q_im[tri] : 0};
+            dsum = cadd(dsum, cmul(gs, qv));
+            cplx rob = {0, 0};
+            if (beta_re && (beta_re[tri] != 0 || beta_im[tri] != 0)) {
+                cplx ik = {-ki, kr}, bt = {beta_re[tri], beta_im[tri]};
+                rob = cscale(cmul(gs, cmul(ik, bt)), (REAL)1 / 3);
+            }
+            for (int l = 0; l < 3; ++l) {
+                int d = dof(g, tri, l);
+                cr[d] += dc[l].re - rob.re;
+                cim[d] += dc[l].im - rob.im;
+            }
+        }
+        d_re[ci] = dsum.re;
+        d_im[ci] = dsum.im;
+        double row = 0;
+        for (int j = 0; j < n; ++j) row += hypot((double)cr[j], (double)cim[j]);
+        if (row > cnorm) cnorm = row;
+    }
+    return cnorm;
 }
 
 /* ---- tag reduction (main.swift:807-841), FP64 sums -------------------- */

@@ -198,6 +198,27 @@ class Oracle:
         )
         return ore + 1j * oim
 
+    def chief_rows(self, pts_3xm, k: float, q=None, k_imag: float = 0.0, beta=None):
+        """CHIEF collocation rows at interior points (main.swift:1897-2036): (C (m, n), d (m,), ||C||_inf)
+        with C p = d the vanishing exterior representation, Robin folded in as in the boundary rows."""
+        pts = np.ascontiguousarray(pts_3xm, dtype=np.float32)
+        m, n = pts.shape[1], self.n
+        cre = np.zeros((m, n), self.real); cim = np.zeros((m, n), self.real)
+        dre = np.zeros(m, self.real); dim = np.zeros(m, self.real)
+        qre, qim = (None, None)
+        if q is not None:
+            qz = np.asarray(q, dtype=np.complex128).reshape(self.T)
+            qre, qim = np.ascontiguousarray(qz.real, self.real), np.ascontiguousarray(qz.imag, self.real)
+        brr = bri = None
+        if beta is not None:
+            bz = np.asarray(beta, dtype=np.complex128).reshape(self.T)
+            brr, bri = np.ascontiguousarray(bz.real, self.real), np.ascontiguousarray(bz.imag, self.real)
+        fn = self._fn("chief_rows")
+        fn.restype = ctypes.c_double
+        cn = fn(ctypes.byref(self.geom), _ptr(pts), ctypes.c_int(m), self._ct(k), self._ct(k_imag), _ptr(brr),
+                _ptr(bri), _ptr(qre), _ptr(qim), _ptr(cre), _ptr(cim), _ptr(dre), _ptr(dim))
+        return cre + 1j * cim, dre + 1j * dim, float(cn)
+
     def tag_average(self, p, tag: int) -> complex:
         p = np.asarray(p).reshape(self.n)
         pre = np.ascontiguousarray(p.real, self.real); pim = np.ascontiguousarray(p.imag, self.real)
@@ -266,6 +287,30 @@ def dense_solve(A, b, precision: str = "f32"):
     if info != 0:
         raise RuntimeError(f"LAPACK gesv info={info}")
     return x
+
+
+def chief_lstsq(A, b, C, d, weight: float = 1.0):
+    """The reference's CHIEF least squares (main.swift:7186-7409): minimise ||[A; s C] p - [b; s d]||_2 in
+    complex128 (LAPACK zgels), s = weight ||A||_inf / ||C||_inf (largest row sums of |a|, |c|).  b and d may
+    hold several right-hand sides as columns.  Returns (p, s, per-column ||s (C p - d)|| / ||b||)."""
+    from scipy.linalg import lapack
+
+    A = np.asarray(A, np.complex128); C = np.asarray(C, np.complex128)
+    b = np.asarray(b, np.complex128); d = np.asarray(d, np.complex128)
+    one = b.ndim == 1
+    B, D = (b[:, None], d[:, None]) if one else (b, d)
+    an = float(np.abs(A).sum(axis=1).max())
+    cn = float(np.abs(C).sum(axis=1).max())
+    s = weight * (an / cn if cn > 0 else 1.0)
+    M = np.vstack([A, s * C])
+    R = np.vstack([B, s * D])
+    _, x, info = lapack.zgels(M, R)
+    if info != 0:
+        raise RuntimeError(f"LAPACK zgels info={info}")
+    p = x[:A.shape[1]]
+    res = np.linalg.norm(s * (C @ p - D), axis=0) / np.where(np.linalg.norm(B, axis=0) > 0,
+                                                            np.linalg.norm(B, axis=0), 1.0)
+    return (p[:, 0] if one else p), s, (float(res[0]) if one else res)
 
 
 def solve_case(oracle: Oracle, k: float, q, obs_3xn, precision: str = "f32"):

@@ -262,3 +262,72 @@ def test_near_pairs_exclude_touching_and_far_pairs():
     assert small and small < large
     touching = {tuple(r[:4]) for r in o.duffy_pairs()[0].tolist()}
     assert not (large & touching)
+
+
+CHIEF_PTS = np.array([[0.013, -0.021, 0.017], [-0.03, 0.02, -0.01], [0.025, 0.031, -0.028],
+                      [-0.012, -0.034, 0.03]]).T   # (3, 4) inside the 0.1 m sphere
+
+
+def _sphere_case(ka: float):
+    from hornlab_metal_bem_b200 import generators as G
+    from hornlab_metal_bem_b200.geometry import build_geometry_buffers
+    from hornlab_metal_bem_b200.mesh import make_pure_function_spaces
+
+    m = G.icosphere(2, 0.1)
+    p1, dp0 = make_pure_function_spaces(m.grid)
+    buf = build_geometry_buffers(m.grid, m.physical_tags, p1, dp0)
+    rho, c, a = 1.205, 343.0, 0.1
+    k = float(np.float32(ka / a))
+    q = np.full(buf.n_triangles, 1j * rho * k * c, np.complex64)
+    return buf, k, q, rho * c * (1j * k * a) / (1j * k * a - 1)
+
+
+@pytest.mark.parametrize("ka", [2.5, 3.18])
+def test_chief_cures_the_sphere_fictitious_frequency(ka):
+    """The Kirchhoff (D - I/2) formulation of the exterior Neumann problem is not unique at the interior
+    Dirichlet eigenvalues (sphere: j0(ka) = 0, ka = pi; the discrete ico2 sphere's near-singular point is
+    ka = 3.18, cond 443).  There the plain solve's surface pressure is 18 % off the analytic pulsating
+    sphere, while the oracle's CHIEF rows (main.swift:1897-2036) and zgels least squares (main.swift:
+    7186-7409) stay at the discretisation error (0.42 %), which is what both give at ka = 2.5."""
+    from oracle.oracle import chief_lstsq
+
+    buf, k, q, pa = _sphere_case(ka)
+    o = Oracle(buf, 0, "f64")
+    A, b = o.corrected(k, q)
+    p = dense_solve(A, b, "f64")
+    C, d, cn = o.chief_rows(CHIEF_PTS, k, q)
+    assert C.shape == (4, buf.p1_dof_count) and cn > 0
+    assert abs(cn - np.abs(C).sum(axis=1).max()) <= 1e-12 * cn
+    pc, s, res = chief_lstsq(A, b, C, d, 1.0)
+    assert abs(s - np.abs(A).sum(axis=1).max() / cn) <= 1e-12 * s
+    err_plain = abs(np.mean(p) - pa) / abs(pa)
+    err_chief = abs(np.mean(pc) - pa) / abs(pa)
+    assert err_chief < 6e-3
+    if ka > 3:
+        assert err_plain > 0.1
+    else:
+        assert err_plain < 6e-3
+    # the interior null field: the exact solution nearly satisfies the CHIEF rows
+    assert np.linalg.norm(C @ pc - d) <= np.linalg.norm(d) * 2e-2
+
+
+def test_chief_rows_images_equal_the_full_mesh():
+    """CHIEF rows of a yz+xz quarter (points and triangles reduced, images summed) equal the full mesh's
+    rows with the four image copies of each quarter dof's columns summed (the even-orbit reduction)."""
+    bq, bf = golden_buffers("yzxz_quarter"), golden_buffers("yzxz_full")
+    oq, of = Oracle(bq, 3, "f64"), Oracle(bf, 0, "f64")
+    k = 9.0
+    pts = np.array([[0.011, 0.017, 0.02], [0.004, 0.009, 0.05]]).T
+    Cq, dq, _ = oq.chief_rows(pts, k, np.ones(bq.triangles_3xm_i32.shape[1]))
+    Cf, df, _ = of.chief_rows(pts, k, np.ones(bf.triangles_3xm_i32.shape[1]))
+    vq = np.asarray(bq.vertices_3xn_f32, np.float64).T
+    vf = np.asarray(bf.vertices_3xn_f32, np.float64).T
+    # each quarter dof gathers the full dofs at its four mirror positions
+    Cr = np.zeros_like(Cq)
+    key = {tuple(np.round(v, 7)): i for i, v in enumerate(vq)}
+    for j, v in enumerate(vf):
+        i = key.get((round(abs(v[0]), 7), round(abs(v[1]), 7), round(v[2], 7)))
+        assert i is not None
+        Cr[:, i] += Cf[:, j]
+    assert np.linalg.norm(Cr - Cq) <= 1e-9 * np.linalg.norm(Cq)
+    assert np.linalg.norm(df - dq) <= 1e-9 * np.linalg.norm(dq)
