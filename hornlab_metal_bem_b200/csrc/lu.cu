@@ -1857,14 +1857,14 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
     // only used on the bulk stream (and on the chain after it has joined).
     const size_t smem_cap = 200 * 1024;
     // 128-column blocks (one K = 128 update per block, half the C stream of
-    // K = 64) pay where few large matrices leave the update bound by that
-    // stream: 18 749 x 2 factors in 417 instead of 498 ms; with more
-    // matrices or smaller ones the longer chain of the 128-wide panels costs
-    // more (10 000 x 2: 98 vs 83 ms; 4096 x 4: 25 vs 21 ms; the 20 systems of
-    // 18 749 of the coupled-baffle sweep: 3.7 vs 3.1 s)
+    // K = 64) pay for large matrices: 18 749 x 2 factors in 417 instead of
+    // 498 ms, 18 749 x 8 in 1460 instead of 1867 ms.  Below that the K = 128
+    // update, whose 128 KB resident A leaves its B ring one 32-column tile
+    // deep, runs at 23 % of HBM where K = 64 reaches 57 % (n = 8192: 2.0 ms
+    // per launch against 0.8 ms for half the K), so 8192 x 4 takes 112 vs
+    // 85 ms and 10 000 x 2 98 vs 83 ms.
     const int blk_want = tuning(HBEM_TUNE_LU_BLOCK);
-    const int NB = (precision == HBEM_PREC_MIXED && n > 256 &&
-                    (blk_want == 128 || (blk_want == 0 && n > 16000 && batch <= 4)))
+    const int NB = (precision == HBEM_PREC_MIXED && n > 256 && (blk_want == 128 || (blk_want == 0 && n > 16000)))
                        ? 128
                        : 64;
     HBEM_CUDA(cudaMemsetAsync(info, 0, sizeof(int) * batch, st));

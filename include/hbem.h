@@ -127,8 +127,7 @@ long long hbem_launch_count(void);
  *                            products, 22 significand bits per operand)
  *   HBEM_TUNE_LU_BLOCK:      column block of the mixed (BF16x3) LU and the K
  *                            of its tensor-core update (64 or 128; 0: the
- *                            built-in 128 for n > 16000 with at most four
- *                            matrices, else 64)
+ *                            built-in 128 for n > 16000, else 64)
  */
 #define HBEM_TUNE_ASM_MINBLOCKS 0
 #define HBEM_TUNE_LU_PANEL 1
