@@ -58,6 +58,10 @@ def parse():
     ap.add_argument("--batch", type=int, default=2, help="lu: matrices per launch")
     ap.add_argument("--streams", type=int, default=4, help="c3: concurrent streams")
     ap.add_argument("--precision", choices=["plain", "mixed"], default="plain")
+    ap.add_argument("--lu-block", type=int, choices=[0, 64, 128], default=0,
+                    help="lu: column block of the mixed LU (HBEM_TUNE_LU_BLOCK; 0 = built-in)")
+    ap.add_argument("--lu-update", type=int, choices=[0, 1, 2], default=0,
+                    help="lu: plain LU bulk update (HBEM_TUNE_LU_UPDATE; 2 = TF32x3 tensor cores)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="c2: skip the brief C3 / C4 / C5 form measurements")
     return ap.parse_args()
@@ -763,6 +767,8 @@ def run_lu(args):
     lib = load_library()
     n, F = args.n, args.batch
     prec = 1 if args.precision == "mixed" else 0
+    check(lib.hbem_set_tuning(9, args.lu_block), "hbem_set_tuning", lib)    # HBEM_TUNE_LU_BLOCK
+    check(lib.hbem_set_tuning(8, args.lu_update), "hbem_set_tuning", lib)   # HBEM_TUNE_LU_UPDATE
     g = torch.Generator(device="cuda").manual_seed(0)
     A0r = torch.randn((F, n, n), device="cuda", generator=g)
     A0r += 2 * n ** 0.5 * torch.eye(n, device="cuda")
@@ -797,7 +803,8 @@ def run_lu(args):
     resid = float(torch.linalg.norm(A @ x - b) / torch.linalg.norm(b))
     flops = F * (8.0 / 3.0) * n ** 3
     print(json.dumps({"metric": "complex LU factor TFLOP/s (8/3 n^3 per matrix)", "value": flops / (fac * 1e-3) / 1e12,
-                      "unit": "TFLOP/s", "n": n, "batch": F, "precision": args.precision, "factor_ms": fac,
+                      "unit": "TFLOP/s", "n": n, "batch": F, "precision": args.precision,
+                      "lu_block": args.lu_block, "lu_update": args.lu_update, "factor_ms": fac,
                       "solve_ms": sol, "steps": args.steps, "warmup": args.warmup, "residual_rel": resid,
                       "info": int(info.abs().sum())}), flush=True)
 

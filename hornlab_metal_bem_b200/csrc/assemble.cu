@@ -148,6 +148,38 @@ __device__ __forceinline__ void sample_nf_w(float dx, float dy, float dz, float 
     }
 }
 
+// sample_nf_w for two wavenumbers held in the two halves of packed FP32
+// pairs (k2 = (k0, k1)): sm_100 issues two FP32 multiplies / adds / FMAs of a
+// pair as one instruction (FMUL2 / FADD2 / FFMA2), each with the rounding of
+// its scalar twin.  nk2 = -k2.
+template <bool CK>
+__device__ __forceinline__ void sample2_w(float dx, float dy, float dz, float nx, float ny, float nz, float2 k2,
+                                          float2 nk2, float2 ki2, float wgt, float2 &dre, float2 &dim, float2 &gre,
+                                          float2 &gim) {
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    float u = rsqrtf(r2);
+    u = r2 > 1.0e-14f ? u : 0.0f;
+    const float r = r2 * u;
+    const float dn = fmaf(dx, nx, fmaf(dy, ny, dz * nz));
+    const float h = dn * (u * u) * wgt, uw = u * wgt;
+    const float2 ph = __fmul2_rn(make_float2(r, r), k2);
+    float2 sn, cs;
+    __sincosf(ph.x, &sn.x, &cs.x);
+    __sincosf(ph.y, &sn.y, &cs.y);
+    float2 nh = make_float2(-h, -h), uu = make_float2(uw, uw), fre = make_float2(u, u);
+    if (CK) {
+        const float2 damp = make_float2(__expf(-ki2.x * r), __expf(-ki2.y * r));
+        nh = __fmul2_rn(nh, damp);
+        uu = __fmul2_rn(uu, damp);
+        fre = __fadd2_rn(fre, ki2);
+    }
+    // D = hh (c + i s)(-fre + i k): re = -hh (c fre + s k), im = -hh (s fre - c k)
+    dre = __fmul2_rn(nh, __ffma2_rn(cs, fre, __fmul2_rn(sn, k2)));
+    dim = __fmul2_rn(nh, __ffma2_rn(sn, fre, __fmul2_rn(cs, nk2)));
+    gre = __fmul2_rn(uu, cs);
+    gim = __fmul2_rn(uu, sn);
+}
+
 template <int SYM, int NF, bool CK, bool NEED_G>
 __device__ __forceinline__ void pair_block(const float4 *__restrict__ tq, const float4 *__restrict__ sp, float nx,
                                            float ny, float nz, bool self, const float (&k)[NF],
@@ -902,6 +934,11 @@ __global__ void __launch_bounds__(256, MINB) k_duffy(const __grid_constant__ Duf
     // = sum D t_a s_b; turned into the P1 entries (tb = 1 - t1 - t2, t1, t2)
     // in FP64 before the warp reduction.
     float acc[NF][24];
+    // NF = 2: the two wavenumbers' moments as packed pairs (x: the first, y:
+    // the second), one FFMA2 per moment and point
+    float2 acc2[24];
+    const float2 k2 = make_float2(k[0], k[NF - 1]), nk2 = make_float2(-k[0], -k[NF - 1]);
+    const float2 ki2 = make_float2(ki[0], ki[NF - 1]);
     // (txi, teta), (sxi, seta): the point's base-local barycentrics (t1, t2),
     // (s1, s2) on the test and trial triangles
     auto accumulate = [&](float txi, float teta, float sxi, float seta, float w) {
@@ -911,6 +948,35 @@ __global__ void __launch_bounds__(256, MINB) k_duffy(const __grid_constant__ Duf
             const float x = fmaf(teta, P[2][c], fmaf(txi, P[1][c], P[0][c]));
             const float y = fmaf(seta, S[2][c], fmaf(sxi, S[1][c], S[0][c]));
             d[c] = y - x;
+        }
+        if constexpr (NF == 2) {
+            float2 dre, dim, gre, gim;
+            sample2_w<CK>(d[0], d[1], d[2], nx, ny, nz, k2, nk2, ki2, w, dre, dim, gre, gim);
+            const float2 t1 = make_float2(txi, txi), t2 = make_float2(teta, teta);
+            const float2 s1 = make_float2(sxi, sxi), s2 = make_float2(seta, seta);
+            const float2 tw[3] = {make_float2(1.f, 1.f), t1, t2}, sw[3] = {make_float2(1.f, 1.f), s1, s2};
+            const float2 ts[2][2] = {{__fmul2_rn(t1, s1), __fmul2_rn(t1, s2)}, {__fmul2_rn(t2, s1), __fmul2_rn(t2, s2)}};
+            acc2[0] = __fadd2_rn(acc2[0], gre);
+            acc2[1] = __fadd2_rn(acc2[1], gim);
+            acc2[2] = __ffma2_rn(gre, t1, acc2[2]);
+            acc2[3] = __ffma2_rn(gim, t1, acc2[3]);
+            acc2[4] = __ffma2_rn(gre, t2, acc2[4]);
+            acc2[5] = __ffma2_rn(gim, t2, acc2[5]);
+#pragma unroll
+            for (int aa = 0; aa < 3; ++aa)
+#pragma unroll
+                for (int bb = 0; bb < 3; ++bb) {
+                    const int e = 6 + 2 * (3 * aa + bb);
+                    if (aa == 0 && bb == 0) {
+                        acc2[e] = __fadd2_rn(acc2[e], dre);
+                        acc2[e + 1] = __fadd2_rn(acc2[e + 1], dim);
+                    } else {
+                        const float2 wt = aa == 0 ? sw[bb] : (bb == 0 ? tw[aa] : ts[aa - 1][bb - 1]);
+                        acc2[e] = __ffma2_rn(dre, wt, acc2[e]);
+                        acc2[e + 1] = __ffma2_rn(dim, wt, acc2[e + 1]);
+                    }
+                }
+            return;
         }
         const float ts[2][2] = {{txi * sxi, txi * seta}, {teta * sxi, teta * seta}};
         const float tw[3] = {1.f, txi, teta}, sw[3] = {1.f, sxi, seta};
@@ -958,6 +1024,8 @@ __global__ void __launch_bounds__(256, MINB) k_duffy(const __grid_constant__ Duf
     for (int f = 0; f < NF; ++f)
 #pragma unroll
         for (int e = 0; e < 24; ++e) acc[f][e] = 0.f;
+#pragma unroll
+    for (int e = 0; e < 24; ++e) acc2[e] = make_float2(0.f, 0.f);
     // singular (Duffy) points, then the regular 6x6 rule with negated weights
     // (the correction is singular - regular; the coincident self-point is
     // excluded by index exactly as in the regular assembly,
@@ -1005,6 +1073,13 @@ __global__ void __launch_bounds__(256, MINB) k_duffy(const __grid_constant__ Duf
             skip = self_pair && a == b;
         }
         if (!skip) accumulate(t1, t2, s1, s2, w);
+    }
+    if constexpr (NF == 2) {
+#pragma unroll
+        for (int e = 0; e < 24; ++e) {
+            acc[0][e] = acc2[e].x;
+            acc[NF - 1][e] = acc2[e].y;
+        }
     }
     // FP64 warp totals of the 24 NF lane partials (value v = 24 f + e): a
     // transpose-reduce leaves value v of the first set in lane v, of the
