@@ -20,7 +20,10 @@
 // basis products (inner sum over trial points first) and adds the pair block
 // into a shared-memory accumulator indexed by the tile's distinct dofs.  The
 // tile is flushed once with red.global.add, which cuts global atomics by the
-// ~25x dof sharing inside a spatially compact (Morton ordered) tile.
+// ~25x dof sharing inside a spatially compact (Morton ordered) tile.  Values
+// that come in pairs (the two orders of an unordered pair, the Duffy kernel's
+// two wavenumbers) are accumulated as packed FP32 pairs (FFMA2 / FMUL2 /
+// FADD2: half the instructions, the same rounding per element).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -79,6 +82,7 @@ __device__ __forceinline__ float bas(int q, int i) {
 __constant__ float c_wa[6][3];
 __constant__ float c_wb[6][3];   // w_b * phi_j(y_b)
 __constant__ float c_w[6];       // w_b
+__constant__ float2 c_wa2[6][3]; // (c_wa, c_wa): packed-pair operands
 
 // One geometric sample y - x shared by NF wavenumbers.  Frequency-independent
 // part once (distance, 1/r, (y-x).n / r^3); per wavenumber the phase in turns
@@ -417,10 +421,13 @@ __global__ void __launch_bounds__(kAsmThreads, MINB) k_regular(const __grid_cons
 // distinct point pair unchanged in FP32 and makes the coincident point
 // (d = 0 exactly) contribute exactly 0: its dG/dn terms carry the factor
 // d.n = 0 times a finite 1/r^2 = 1e30.
+// The two orders ride in the two halves of packed FP32 pairs: dr = (dre,
+// tre), di = (dim, tim), one FFMA2 (sm_100: two FP32 FMAs as one
+// instruction, each rounded as its scalar twin) for both orders' D or T.
 template <bool CK, bool NEED_G>
 __device__ __forceinline__ void sample_sym(float dx, float dy, float dz, float nsx, float nsy, float nsz, float ntx,
-                                           float nty, float ntz, float k, float ki, float &dre, float &dim,
-                                           float &tre, float &tim, float &gre, float &gim) {
+                                            float nty, float ntz, float k, float ki, float2 &dr, float2 &di,
+                                            float &gre, float &gim) {
     const float r2 = NEED_G ? fmaf(dx, dx, fmaf(dy, dy, dz * dz)) : fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, 1.0e-30f)));
     float u = rsqrtf(r2);
     if (NEED_G) u = r2 > 1.0e-14f ? u : 0.0f;
@@ -438,12 +445,10 @@ __device__ __forceinline__ void sample_sym(float dx, float dy, float dz, float n
         uu *= damp;
         fre += ki;
     }
-    // E = (c + i s)(-fre + i k); D = h E
     const float e_re = -fmaf(cs, fre, sn * k), e_im = fmaf(cs, k, -sn * fre);
-    dre = fmaf(hs, e_re, dre);
-    dim = fmaf(hs, e_im, dim);
-    tre = fmaf(ht, e_re, tre);
-    tim = fmaf(ht, e_im, tim);
+    const float2 h2 = make_float2(hs, ht);
+    dr = __ffma2_rn(h2, make_float2(e_re, e_re), dr);
+    di = __ffma2_rn(h2, make_float2(e_im, e_im), di);
     if (NEED_G) {
         gre = fmaf(uu, cs, gre);
         gim = fmaf(uu, sn, gim);
@@ -460,41 +465,42 @@ __device__ __forceinline__ void pair_block_sym(const float4 *__restrict__ tq, co
                                                float (&fwr)[9], float (&fwi)[9], float (&tnr)[9],
                                                float (&tni)[9], float (&sfr)[3], float (&sfi)[3], float (&str_)[3],
                                                float (&sti)[3]) {
+    float2 Fr[9], Fi[9];   // (fwd[i*3+j], trn[j*3+i])
 #pragma unroll
-    for (int i = 0; i < 9; ++i) fwr[i] = fwi[i] = tnr[i] = tni[i] = 0.0f;
+    for (int i = 0; i < 9; ++i) Fr[i] = Fi[i] = make_float2(0.f, 0.f);
 #pragma unroll
     for (int i = 0; i < 3; ++i) sfr[i] = sfi[i] = str_[i] = sti[i] = 0.0f;
 #pragma unroll 1
     for (int a = 0; a < 6; ++a) {
         const float4 x = tq[a * kTestTile];
-        float ere[3], eim[3], tre_[3], tim_[3], hre = 0.f, him = 0.f, g2r[3], g2i[3];
+        float2 er[3], ei[3];
+        float hre = 0.f, him = 0.f, g2r[3], g2i[3];
 #pragma unroll
-        for (int j = 0; j < 3; ++j) ere[j] = eim[j] = tre_[j] = tim_[j] = g2r[j] = g2i[j] = 0.f;
+        for (int j = 0; j < 3; ++j) { er[j] = ei[j] = make_float2(0.f, 0.f); g2r[j] = g2i[j] = 0.f; }
 #pragma unroll
         for (int b = 0; b < 6; ++b) {
             const float4 y = sp[b];
-            float dre = 0.f, dim = 0.f, tre = 0.f, tim = 0.f, gre = 0.f, gim = 0.f;
-            sample_sym<CK, NEED_G>(y.x - x.x, y.y - x.y, y.z - x.z, nx, ny, nz, tnx, tny, tnz, k, ki, dre,
-                                       dim, tre, tim, gre, gim);
+            float2 dr = make_float2(0.f, 0.f), di = make_float2(0.f, 0.f);
+            float gre = 0.f, gim = 0.f;
+            sample_sym<CK, NEED_G>(y.x - x.x, y.y - x.y, y.z - x.z, nx, ny, nz, tnx, tny, tnz, k, ki, dr, di, gre, gim);
             if (SYM == 1 || SYM == 3)
-                sample_sym<CK, NEED_G>(-y.x - x.x, y.y - x.y, y.z - x.z, -nx, ny, nz, tnx, tny, tnz, k, ki, dre,
-                                       dim, tre, tim, gre, gim);
+                sample_sym<CK, NEED_G>(-y.x - x.x, y.y - x.y, y.z - x.z, -nx, ny, nz, tnx, tny, tnz, k, ki,
+                                       dr, di, gre, gim);
             if (SYM == 2 || SYM == 3)
-                sample_sym<CK, NEED_G>(y.x - x.x, -y.y - x.y, y.z - x.z, nx, -ny, nz, tnx, tny, tnz, k, ki, dre,
-                                       dim, tre, tim, gre, gim);
+                sample_sym<CK, NEED_G>(y.x - x.x, -y.y - x.y, y.z - x.z, nx, -ny, nz, tnx, tny, tnz, k, ki,
+                                       dr, di, gre, gim);
             if (SYM == 3)
-                sample_sym<CK, NEED_G>(-y.x - x.x, -y.y - x.y, y.z - x.z, -nx, -ny, nz, tnx, tny, tnz, k, ki, dre,
-                                       dim, tre, tim, gre, gim);
+                sample_sym<CK, NEED_G>(-y.x - x.x, -y.y - x.y, y.z - x.z, -nx, -ny, nz, tnx, tny, tnz, k, ki,
+                                       dr, di, gre,
+                                        gim);
             if (SYM == 4)
-                sample_sym<CK, NEED_G>(y.x - x.x, y.y - x.y, -y.z - x.z, nx, ny, -nz, tnx, tny, tnz, k, ki, dre,
-                                       dim, tre, tim, gre, gim);
+                sample_sym<CK, NEED_G>(y.x - x.x, y.y - x.y, -y.z - x.z, nx, ny, -nz, tnx, tny, tnz, k, ki,
+                                       dr, di, gre, gim);
 #pragma unroll
             for (int j = 0; j < 3; ++j) {
                 const float wb = qw(b) * bas(b, j);
-                ere[j] = fmaf(dre, wb, ere[j]);
-                eim[j] = fmaf(dim, wb, eim[j]);
-                tre_[j] = fmaf(tre, wb, tre_[j]);
-                tim_[j] = fmaf(tim, wb, tim_[j]);
+                er[j] = __ffma2_rn(dr, make_float2(wb, wb), er[j]);
+                ei[j] = __ffma2_rn(di, make_float2(wb, wb), ei[j]);
                 if (NEED_G) {
                     g2r[j] = fmaf(gre, wb, g2r[j]);
                     g2i[j] = fmaf(gim, wb, g2i[j]);
@@ -507,17 +513,15 @@ __device__ __forceinline__ void pair_block_sym(const float4 *__restrict__ tq, co
         }
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
-            const float wa = c_wa[a][i];
+            const float2 wa = c_wa2[a][i];
 #pragma unroll
             for (int j = 0; j < 3; ++j) {
-                fwr[i * 3 + j] = fmaf(wa, ere[j], fwr[i * 3 + j]);
-                fwi[i * 3 + j] = fmaf(wa, eim[j], fwi[i * 3 + j]);
-                tnr[j * 3 + i] = fmaf(wa, tre_[j], tnr[j * 3 + i]);
-                tni[j * 3 + i] = fmaf(wa, tim_[j], tni[j * 3 + i]);
+                Fr[i * 3 + j] = __ffma2_rn(wa, er[j], Fr[i * 3 + j]);
+                Fi[i * 3 + j] = __ffma2_rn(wa, ei[j], Fi[i * 3 + j]);
             }
             if (NEED_G) {
-                sfr[i] = fmaf(wa, hre, sfr[i]);
-                sfi[i] = fmaf(wa, him, sfi[i]);
+                sfr[i] = fmaf(wa.x, hre, sfr[i]);
+                sfi[i] = fmaf(wa.x, him, sfi[i]);
             }
         }
         if (NEED_G) {
@@ -529,6 +533,15 @@ __device__ __forceinline__ void pair_block_sym(const float4 *__restrict__ tq, co
             }
         }
     }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            fwr[i * 3 + j] = Fr[i * 3 + j].x;
+            tnr[j * 3 + i] = Fr[i * 3 + j].y;
+            fwi[i * 3 + j] = Fi[i * 3 + j].x;
+            tni[j * 3 + i] = Fi[i * 3 + j].y;
+        }
 }
 
 // blockIdx.z = frequency.  CTAs whose test triangles all follow their trial
@@ -1212,6 +1225,10 @@ int launch_regular(Session &s, int n_freq, const float *k_re, const float *k_im,
         HBEM_CUDA(cudaMemcpyToSymbol(c_wa, wa, sizeof(wa)));
         HBEM_CUDA(cudaMemcpyToSymbol(c_wb, wa, sizeof(wa)));
         HBEM_CUDA(cudaMemcpyToSymbol(c_w, w, sizeof(w)));
+        float2 wa2[6][3];
+        for (int q = 0; q < 6; ++q)
+            for (int i = 0; i < 3; ++i) wa2[q][i] = make_float2(wa[q][i], wa[q][i]);
+        HBEM_CUDA(cudaMemcpyToSymbol(c_wa2, wa2, sizeof(wa2)));
         consts_ready[s.device] = true;
     }
     if (smem > 180 * 1024 || smem_sym > 180 * 1024)
