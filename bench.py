@@ -480,8 +480,9 @@ def run_b200(args, w):
     clk_mhz = peaks.get("sm_max_mhz", 1965.0)
     fp32_peak = N_SM * FP32_LANES_PER_SM * 2 * clk_mhz * 1e6 / 1e12
     achieved = samples * FLOPS_PER_SAMPLE / (stage["regular_ms"] * 1e-3) / 1e12
-    sfu_peak = N_SM * SFU_LANES_PER_SM * clk_mhz * 1e6 / SFU_PER_SAMPLE
-    sfu_achieved = samples / (stage["regular_ms"] * 1e-3)
+    # MUFU pipe: rsqrt, sin, cos once per unordered evaluation, i.e. 1.5 per ordered sample
+    sfu_peak = N_SM * SFU_LANES_PER_SM * clk_mhz * 1e6
+    sfu_achieved = samples * SFU_PER_SAMPLE / 2 / (stage["regular_ms"] * 1e-3)
     roofline = {
         "kernel": "k_regular_sym (regular pair assembly over unordered pairs, %d launch/step)" % ((F + 63) // 64),
         "bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
@@ -489,8 +490,10 @@ def run_b200(args, w):
         "algorithmic": f"{samples:.3e} ordered kernel samples/launch x {FLOPS_PER_SAMPLE:.0f} FP32 flops "
                        "(F T^2 36 M; the kernel evaluates each unordered pair once)",
         "peak_source": f"148 SM x 128 FP32 lanes x 2 x {clk_mhz:.0f} MHz (sm_max_mhz, {peaks['source']})",
-        "sfu": {"achieved_gsamples_s": sfu_achieved / 1e9, "peak_gsamples_s": sfu_peak / 1e9,
-                "frac": sfu_achieved / sfu_peak, "per_sample": "rsqrt + sin + cos (3 MUFU), 16 MUFU/clk/SM"},
+        "sfu": {"achieved_gops_s": sfu_achieved / 1e9, "peak_gops_s": sfu_peak / 1e9,
+                "frac": sfu_achieved / sfu_peak,
+                "per_sample": "rsqrt + sin + cos (3 MUFU) per unordered evaluation = 1.5 per ordered sample; "
+                              "16 MUFU lanes/clk/SM"},
     }
     line = {
         "metric": "freq-solves/s", "value": value, "unit": "freq-solves/s", "n_gpus": world, "steps": args.steps,
