@@ -49,15 +49,19 @@ __device__ __forceinline__ float fqy(int q) {
     return q == 0 ? HBEM_QY0 : q == 1 ? HBEM_QY1 : q == 2 ? HBEM_QY2 : q == 3 ? HBEM_QY3 : q == 4 ? HBEM_QY4 : HBEM_QY5;
 }
 
-// adds (D p - G q) for one source point y (double coordinates, exact copies of
-// the float inputs) seen from the observation point o
-__device__ __forceinline__ void fsample(double yx, double yy, double yz, double ox, double oy, double oz, float nx,
-                                        float ny, float nz, float k, double kt, float pr, float pi, float qr, float qi,
+// adds (D p - G q) for one source point y seen from the observation point o:
+// the distance for the phase from the exact double differences of the float
+// inputs (yx .. oz), the amplitude and the projection from the FP32
+// differences (fy - fo) — no double-to-float conversions on the hot path, whose
+// conversion / MUFU pipe bounds this kernel
+__device__ __forceinline__ void fsample(double yx, double yy, double yz, double ox, double oy, double oz, float fyx,
+                                        float fyy, float fyz, float fox, float foy, float foz, float nx, float ny,
+                                        float nz, float k, double kt, float pr, float pi, float qr, float qi,
                                         float &ar, float &ai) {
     const double dxd = yx - ox, dyd = yy - oy, dzd = yz - oz;
     const double r2d = fma(dxd, dxd, fma(dyd, dyd, dzd * dzd));
-    const float dx = (float)dxd, dy = (float)dyd, dz = (float)dzd;
-    const float r2 = (float)r2d;
+    const float dx = fyx - fox, dy = fyy - foy, dz = fyz - foz;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     float rinv = rsqrtf(r2);
     rinv = r2 > 1.0e-14f ? rinv : 0.0f;
     const float rf = r2 * rinv;
@@ -77,15 +81,18 @@ __device__ __forceinline__ void fsample(double yx, double yy, double yz, double 
 }
 
 template <int SYM>
-__global__ void __launch_bounds__(kFieldThreads) k_field(const __grid_constant__ FieldArgs a) {
+__global__ void __launch_bounds__(kFieldThreads, 2) k_field(const __grid_constant__ FieldArgs a) {
     __shared__ double s_obs[kObsTile][3];
+    __shared__ float s_obsf[kObsTile][3];
     __shared__ float s_red[kFieldThreads / 32][kObsTile][2];
     const int f = blockIdx.y;
     const int o0 = blockIdx.x * kObsTile;
     const int nob = min(kObsTile, a.n_obs - o0);
     if (threadIdx.x < kObsTile * 3) {
         const int o = threadIdx.x / 3, c = threadIdx.x % 3;
-        s_obs[o][c] = o < nob ? (double)a.obs[(size_t)c * a.n_obs + o0 + o] : 0.0;
+        const float v = o < nob ? a.obs[(size_t)c * a.n_obs + o0 + o] : 0.f;
+        s_obs[o][c] = v;
+        s_obsf[o][c] = v;
     }
     __syncthreads();
     const float k = a.k[f];
@@ -111,16 +118,26 @@ __global__ void __launch_bounds__(kFieldThreads) k_field(const __grid_constant__
             const float wqr = qr * w, wqi = qi * w;
 #pragma unroll
             for (int o = 0; o < kObsTile; ++o) {
-                const double ox = s_obs[o][0], oy = s_obs[o][1], oz = s_obs[o][2];
-                fsample(yx, yy, yz, ox, oy, oz, nj.x, nj.y, nj.z, k, kt, pr, pi, wqr, wqi, accr[o], acci[o]);
+                // the observation point re-read per use (volatile): kept in registers for
+                // all eight points the copies would push the kernel past 128 registers
+                const volatile double *vd = s_obs[o];
+                const double ox = vd[0], oy = vd[1], oz = vd[2];
+                const volatile float *vo = s_obsf[o];
+                const float fx = vo[0], fy = vo[1], fz = vo[2];
+                fsample(yx, yy, yz, ox, oy, oz, yf.x, yf.y, yf.z, fx, fy, fz, nj.x, nj.y, nj.z, k, kt, pr, pi, wqr, wqi,
+                        accr[o], acci[o]);
                 if (SYM == 1 || SYM == 3)
-                    fsample(-yx, yy, yz, ox, oy, oz, -nj.x, nj.y, nj.z, k, kt, pr, pi, wqr, wqi, accr[o], acci[o]);
+                    fsample(-yx, yy, yz, ox, oy, oz, -yf.x, yf.y, yf.z, fx, fy, fz, -nj.x, nj.y, nj.z, k, kt, pr, pi, wqr,
+                            wqi, accr[o], acci[o]);
                 if (SYM == 2 || SYM == 3)
-                    fsample(yx, -yy, yz, ox, oy, oz, nj.x, -nj.y, nj.z, k, kt, pr, pi, wqr, wqi, accr[o], acci[o]);
+                    fsample(yx, -yy, yz, ox, oy, oz, yf.x, -yf.y, yf.z, fx, fy, fz, nj.x, -nj.y, nj.z, k, kt, pr, pi, wqr,
+                            wqi, accr[o], acci[o]);
                 if (SYM == 3)
-                    fsample(-yx, -yy, yz, ox, oy, oz, -nj.x, -nj.y, nj.z, k, kt, pr, pi, wqr, wqi, accr[o], acci[o]);
+                    fsample(-yx, -yy, yz, ox, oy, oz, -yf.x, -yf.y, yf.z, fx, fy, fz, -nj.x, -nj.y, nj.z, k, kt, pr, pi,
+                            wqr, wqi, accr[o], acci[o]);
                 if (SYM == 4)
-                    fsample(yx, yy, -yz, ox, oy, oz, nj.x, nj.y, -nj.z, k, kt, pr, pi, wqr, wqi, accr[o], acci[o]);
+                    fsample(yx, yy, -yz, ox, oy, oz, yf.x, yf.y, -yf.z, fx, fy, fz, nj.x, nj.y, -nj.z, k, kt, pr, pi, wqr,
+                            wqi, accr[o], acci[o]);
             }
         }
     }
