@@ -27,8 +27,8 @@ from pathlib import Path
 import numpy as np
 
 from .native import (
-    HBEM_ASM_CORRECTED, HBEM_PREC_PLAIN, HBEM_TRANS_N, NativeSession, _np_ptr, _stream_ptr, _t_ptr, check,
-    load_library, require_cuda,
+    HBEM_ASM_CORRECTED, HBEM_PREC_PLAIN, HBEM_PREC_TF32X3, HBEM_TRANS_N, NativeSession, _np_ptr, _stream_ptr, _t_ptr,
+    check, load_library, require_cuda,
 )
 
 TUNE_ASM_MINBLOCKS, TUNE_LU_PANEL, TUNE_LU_SOLVE, TUNE_ASM_PAIRS, TUNE_DUFFY = 0, 1, 2, 3, 4
@@ -238,8 +238,10 @@ class _CaseRun:
             A0_re, A0_im = slot.A0_re.view(-1)[:F * n * n], slot.A0_im.view(-1)[:F * n * n]
             A0_re.copy_(A_re)
             A0_im.copy_(A_im)
+        # refined sweeps factor with the TF32x3 tensor-core bulk update (the refinement recovers FP32 accuracy)
+        prec = HBEM_PREC_TF32X3 if self.refine_max > 0 else HBEM_PREC_PLAIN
         check(lib.hbem_lu_factor(n, F, _t_ptr(A_re), _t_ptr(A_im), n, n * n, _t_ptr(piv), n, _t_ptr(self.info),
-                                 HBEM_PREC_PLAIN, st), "hbem_lu_factor", lib)
+                                 prec, st), "hbem_lu_factor", lib)
         check(lib.hbem_lu_solve(n, 1, F, _t_ptr(A_re), _t_ptr(A_im), n, n * n, _t_ptr(piv), n, _t_ptr(x_re),
                                 _t_ptr(x_im), 1, n, HBEM_TRANS_N, st), "hbem_lu_solve", lib)
         if self.refine_max > 0:

@@ -50,6 +50,26 @@ constexpr int kPanelThreads = 512;
 
 __device__ __forceinline__ float cabs1(float r, float i) { return fabsf(r) + fabsf(i); }
 
+// The panel kernels' complex arithmetic with every rounding fixed (products
+// that are not fused are __fmul_rn, the rest explicit fmaf), so the compiler
+// cannot contract a*b - c*d either way and every panel kernel computes the
+// same bits for the same element:
+//   l = x / d as x * (1 / d):  inv = conj(d) / (d.re^2 + d.im^2);
+//   x -= l * u.
+__device__ __forceinline__ void pivot_inverse(float dr, float di, float &ir, float &ii) {
+    const float den = 1.0f / fmaf(dr, dr, __fmul_rn(di, di));
+    ir = __fmul_rn(dr, den);
+    ii = __fmul_rn(-di, den);
+}
+__device__ __forceinline__ void cmul_fixed(float xr, float xi, float yr, float yi, float &zr, float &zi) {
+    zr = fmaf(xr, yr, -__fmul_rn(xi, yi));
+    zi = fmaf(xr, yi, __fmul_rn(xi, yr));
+}
+__device__ __forceinline__ void csub_mul_fixed(float &xr, float &xi, float lr, float li, float ur, float ui) {
+    xr = __fsub_rn(xr, fmaf(lr, ur, -__fmul_rn(li, ui)));
+    xi = __fsub_rn(xi, fmaf(lr, ui, __fmul_rn(li, ur)));
+}
+
 // Panel factorisation of rows k0..n-1 x nb columns (nb <= 32), worked in
 // place through L2: the fallback for panels taller than a cluster's shared
 // memory holds.  Per column j, three barrier-separated phases:
@@ -87,8 +107,7 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(float *a_re, float *a_i
             const int o = r * P;
             if (j > 0) {
                 const float xr = pre[o + j - 1], xi = pim[o + j - 1];
-                pre[o + j - 1] = xr * ir - xi * ii;
-                pim[o + j - 1] = xr * ii + xi * ir;
+                cmul_fixed(xr, xi, ir, ii, pre[o + j - 1], pim[o + j - 1]);
             }
             if (j < nb) {
                 const float c = cabs1(pre[o + j], pim[o + j]);
@@ -134,9 +153,7 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(float *a_re, float *a_i
             ir = 0.f;
             ii = 0.f;
         } else {
-            const float den = 1.0f / (dr * dr + di * di);
-            ir = dr * den;
-            ii = -di * den;
+            pivot_inverse(dr, di, ir, ii);
         }
         // ---- phase E
         const int c = j + 1 + c_off;
@@ -145,9 +162,9 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(float *a_re, float *a_i
             for (int r = j + 1 + warp * (32 / LPR) + r_sub; r < m; r += r_step) {
                 const int o = r * P;
                 const float xr = pre[o + j], xi = pim[o + j];
-                const float lr = xr * ir - xi * ii, li = xr * ii + xi * ir;
-                pre[o + c] -= lr * ur - li * ui;
-                pim[o + c] -= lr * ui + li * ur;
+                float lr, li;
+                cmul_fixed(xr, xi, ir, ii, lr, li);
+                csub_mul_fixed(pre[o + c], pim[o + c], lr, li, ur, ui);
             }
         }
         __syncthreads();
@@ -237,9 +254,7 @@ __global__ void __launch_bounds__(kPanelRowsThreads) k_panel_rows(float *a_re, f
         if (zero) {
             if (first_zero == 0) first_zero = k0 + j + 1;
         } else {
-            const float den = 1.0f / (dr * dr + di * di);
-            ir = dr * den;
-            ii = -di * den;
+            pivot_inverse(dr, di, ir, ii);
         }
         // ---- phase E
         v = -1.f;
@@ -248,16 +263,13 @@ __global__ void __launch_bounds__(kPanelRowsThreads) k_panel_rows(float *a_re, f
         for (int r = j + 1 + tid; r < m; r += blockDim.x) {
             const int o = r * P;
             const float xr = pre[o + j], xi = pim[o + j];
-            const float lr = xr * ir - xi * ii, li = xr * ii + xi * ir;
+            float lr, li;
+            cmul_fixed(xr, xi, ir, ii, lr, li);
             pre[o + j] = lr;
             pim[o + j] = li;
             if (!zero) {
 #pragma unroll 4
-                for (int c = j + 1; c < nb; ++c) {
-                    const float ur = s_pr[c], ui = s_pi[c];
-                    pre[o + c] -= lr * ur - li * ui;
-                    pim[o + c] -= lr * ui + li * ur;
-                }
+                for (int c = j + 1; c < nb; ++c) csub_mul_fixed(pre[o + c], pim[o + c], lr, li, s_pr[c], s_pi[c]);
             }
             if (next) {
                 const float a = cabs1(pre[o + j + 1], pim[o + j + 1]);
@@ -274,6 +286,200 @@ __global__ void __launch_bounds__(kPanelRowsThreads) k_panel_rows(float *a_re, f
         const int r = e / nb, j = e - r * nb;
         gre[(size_t)r * lda + j] = pre[r * P + j];
         gim[(size_t)r * lda + j] = pim[r * P + j];
+    }
+    if (tid == 0 && first_zero && info[b] == 0) info[b] = first_zero;
+}
+
+// A sub-panel of W = 16, 32 or 64 columns with its rows in registers: thread
+// t holds rows t, t + T, ... (R of them, W complex values each, as (re, im)
+// pairs) from the load to the write-back, so a column moves no row through
+// shared memory.  The column loop is rolled two columns at a time (the code
+// stays in the instruction cache); every row is rotated left by two places
+// per step, so column j sits in register j mod 2 and the trailing columns
+// follow it (after W columns the rows are back in order).  Per column j:
+//   every warp reduces the per-warp argmax candidates itself (first index on
+//   ties, as icamax); the owners of rows j and p publish those two rows (the
+//   pivot row as (re, im, im, re) quadruples); one barrier; the two rows
+//   change hands, every thread scales and updates its rows below j and takes
+//   its candidate for column j + 1; a second barrier publishes the
+//   candidates.
+// The update x -= l u is three packed FP32 instructions (FMUL2, FFMA2,
+// FADD2) whose halves round exactly as the scalar pivot_inverse /
+// cmul_fixed / csub_mul_fixed of the shared-memory kernels (negations are
+// exact), so the factors are the same bits.  Rows j < W < T live in slot 0
+// of thread j.  For m <= R * T rows; dynamic shared memory m * (2W + 1)
+// floats stages the coalesced load and store.
+template <int W, int R, int T>
+struct PanelRegs {
+    static constexpr int NW = T / 32;
+    float2 x[R][W];
+    // column j in register B; `live` trailing columns in registers B+1 .. B+live
+    template <int B>
+    __device__ __forceinline__ void column(int j, int m, int k0, int tid, int lane, int warp, float *s_v, int *s_i,
+                                           float4 *s_p, float2 *s_o, int *pv, int &first_zero) {
+        float bv = lane < NW ? s_v[lane] : -1.f;
+        int p = lane < NW ? s_i[lane] : 0x7fffffff;
+        argmax_warp(bv, p);
+        if (p >= m) p = j;  // column of NaNs: keep the diagonal, as icamax does
+        const int po = p % T, ps = p / T;
+        if (tid == j) {
+#pragma unroll
+            for (int c = 0; c < W; ++c) s_o[c] = x[0][c];
+        }
+        if (tid == po) {
+#pragma unroll
+            for (int s = 0; s < R; ++s)
+                if (s == ps) {
+#pragma unroll
+                    for (int c = 0; c < W; ++c) s_p[c] = make_float4(x[s][c].x, x[s][c].y, x[s][c].y, x[s][c].x);
+                }
+            pv[k0 + j] = k0 + p;
+        }
+        __syncthreads();
+        if (tid == j) {
+#pragma unroll
+            for (int c = 0; c < W; ++c) {
+                const float4 u = s_p[c];
+                x[0][c] = make_float2(u.x, u.y);
+            }
+        }
+        if (p != j && tid == po) {
+#pragma unroll
+            for (int s = 0; s < R; ++s)
+                if (s == ps) {
+#pragma unroll
+                    for (int c = 0; c < W; ++c) x[s][c] = s_o[c];
+                }
+        }
+        const float4 d = s_p[B];
+        const bool zero = (d.x == 0.f && d.y == 0.f);
+        float ir = 0.f, ii = 0.f;
+        if (zero) {
+            if (first_zero == 0) first_zero = k0 + j + 1;
+        } else {
+            pivot_inverse(d.x, d.y, ir, ii);
+        }
+        const int live = W - 1 - j;
+        bool act[R];
+        float2 nl[R], pl[R];   // (-l.re, -l.re) and (l.im, -l.im)
+#pragma unroll
+        for (int s = 0; s < R; ++s) {
+            const int r = tid + s * T;
+            act[s] = r > j && r < m;
+            float lr, li;
+            cmul_fixed(x[s][B].x, x[s][B].y, ir, ii, lr, li);
+            if (act[s]) x[s][B] = make_float2(lr, li);
+            nl[s] = make_float2(-lr, -lr);
+            pl[s] = make_float2(li, -li);
+        }
+        if (!zero) {
+#pragma unroll
+            for (int c = B + 1; c < W; ++c)
+                if (c - B <= live) {
+                    const float4 u = s_p[c];
+                    const float2 u1 = make_float2(u.x, u.y), u2 = make_float2(u.z, u.w);
+#pragma unroll
+                    for (int s = 0; s < R; ++s)
+                        if (act[s]) {
+                            // x - (fma(lr, ur, -li ui), fma(lr, ui, li ur)) as x + fma(-l.re, u, (li ui, -li ur))
+                            const float2 q = __ffma2_rn(nl[s], u1, __fmul2_rn(pl[s], u2));
+                            x[s][c] = __fadd2_rn(x[s][c], q);
+                        }
+                }
+        }
+        float v = -1.f;
+        int idx = 0x7fffffff;
+        if (B + 1 < W && live > 0) {
+#pragma unroll
+            for (int s = 0; s < R; ++s)
+                if (act[s]) {
+                    const float a = cabs1(x[s][B + 1].x, x[s][B + 1].y);
+                    if (a > v) { v = a; idx = tid + s * T; }
+                }
+        }
+        if (live > 0) {
+            argmax_warp(v, idx);
+            if (lane == 0) { s_v[warp] = v; s_i[warp] = idx; }
+        }
+        __syncthreads();
+    }
+};
+
+template <int W, int R, int T>
+__global__ void __launch_bounds__(T, 1) k_panel_reg(float *a_re, float *a_im, long long lda, long long a_stride,
+                                                    int n, int k0, int *piv, long long piv_stride, int *info) {
+    constexpr int NW = T / 32, SP = 2 * W + 1;
+    static_assert(T % 32 == 0 && NW <= 32 && T > W && (W == 16 || W == 32 || W == 64), "layout");
+    __shared__ float s_v[NW];
+    __shared__ int s_i[NW];
+    __shared__ float4 s_p[W];   // pivot row (the new row j) as (re, im, im, re), rotated as the rows are
+    __shared__ float2 s_o[W];   // old row j (the new row p)
+    extern __shared__ float s_stage[];
+    const int b = blockIdx.x;
+    int *pv = piv + (size_t)b * piv_stride;
+    const int m = n - k0;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    float *gre = a_re + (size_t)b * a_stride + (size_t)k0 * lda + k0;
+    float *gim = a_im + (size_t)b * a_stride + (size_t)k0 * lda + k0;
+    // coalesced in and out through shared memory: a warp moves consecutive
+    // (row, part, column) elements; pitch 2W + 1 keeps a thread's own row on
+    // distinct banks from its neighbours'
+    for (int e = tid; e < m * 2 * W; e += T) {
+        const int r = e / (2 * W), k = e % (2 * W);
+        cp_async4(&s_stage[r * SP + k], (k < W ? gre + k : gim + (k - W)) + (size_t)r * lda, 4);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    PanelRegs<W, R, T> P;
+#pragma unroll
+    for (int s = 0; s < R; ++s) {
+        const int r = tid + s * T;
+#pragma unroll
+        for (int c = 0; c < W; ++c)
+            P.x[s][c] = r < m ? make_float2(s_stage[r * SP + c], s_stage[r * SP + W + c]) : make_float2(0.f, 0.f);
+    }
+    float v = -1.f;
+    int idx = 0x7fffffff;
+#pragma unroll
+    for (int s = 0; s < R; ++s) {
+        const int r = tid + s * T;
+        const float c = cabs1(P.x[s][0].x, P.x[s][0].y);
+        if (r < m && c > v) { v = c; idx = r; }
+    }
+    argmax_warp(v, idx);
+    if (lane == 0) { s_v[warp] = v; s_i[warp] = idx; }
+    __syncthreads();
+    int first_zero = 0;
+#pragma unroll 1
+    for (int j = 0; j < W; j += 2) {
+        P.template column<0>(j, m, k0, tid, lane, warp, s_v, s_i, s_p, s_o, pv, first_zero);
+        P.template column<1>(j + 1, m, k0, tid, lane, warp, s_v, s_i, s_p, s_o, pv, first_zero);
+        // rotate left by two: columns j + 2, j + 3 to registers 0, 1
+#pragma unroll
+        for (int s = 0; s < R; ++s) {
+            const float2 t0 = P.x[s][0], t1 = P.x[s][1];
+#pragma unroll
+            for (int c = 0; c + 2 < W; ++c) P.x[s][c] = P.x[s][c + 2];
+            P.x[s][W - 2] = t0;
+            P.x[s][W - 1] = t1;
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < R; ++s) {
+        const int r = tid + s * T;
+        if (r < m) {
+#pragma unroll
+            for (int c = 0; c < W; ++c) {
+                s_stage[r * SP + c] = P.x[s][c].x;
+                s_stage[r * SP + W + c] = P.x[s][c].y;
+            }
+        }
+    }
+    __syncthreads();
+    for (int e = tid; e < m * 2 * W; e += T) {
+        const int r = e / (2 * W), k = e % (2 * W);
+        (k < W ? gre + k : gim + (k - W))[(size_t)r * lda] = s_stage[r * SP + k];
     }
     if (tid == 0 && first_zero && info[b] == 0) info[b] = first_zero;
 }
@@ -396,9 +602,7 @@ __global__ void __launch_bounds__(kPanelRowsThreads)
         if (zero) {
             if (first_zero == 0) first_zero = k0 + j + 1;
         } else {
-            const float den = 1.0f / (dr * dr + di * di);
-            ir = dr * den;
-            ii = -di * den;
+            pivot_inverse(dr, di, ir, ii);
         }
         // ---- E (own rows below j)
         v = -1.f;
@@ -407,16 +611,13 @@ __global__ void __launch_bounds__(kPanelRowsThreads)
         for (int lr = max(0, j + 1 - r0) + tid; lr < nr; lr += blockDim.x) {
             const int o = lr * P;
             const float xr = pre[o + j], xi = pim[o + j];
-            const float l_r = xr * ir - xi * ii, l_i = xr * ii + xi * ir;
+            float l_r, l_i;
+            cmul_fixed(xr, xi, ir, ii, l_r, l_i);
             pre[o + j] = l_r;
             pim[o + j] = l_i;
             if (!zero) {
 #pragma unroll 4
-                for (int c = j + 1; c < nb; ++c) {
-                    const float ur = s_pr[c], ui = s_pi[c];
-                    pre[o + c] -= l_r * ur - l_i * ui;
-                    pim[o + c] -= l_r * ui + l_i * ur;
-                }
+                for (int c = j + 1; c < nb; ++c) csub_mul_fixed(pre[o + c], pim[o + c], l_r, l_i, s_pr[c], s_pi[c]);
             }
             if (next) {
                 const float a = cabs1(pre[o + j + 1], pim[o + j + 1]);
@@ -1135,8 +1336,8 @@ struct WaveCtl {
 
 static __device__ int g_wave_fault;
 
-// A non-zero status word of a captured factorisation's tensor-core update
-// raises the fault word as well.
+// A non-zero status word of a factorisation's tensor-core update raises the
+// fault word as well.
 __global__ void k_fold_status(const int *status) {
     if (*status) atomicExch(&g_wave_fault, 1);
 }
@@ -1830,15 +2031,18 @@ static int lookahead_streams(cudaStream_t key, LookaheadStreams **out) {
     return HBEM_OK;
 }
 
-// The plain LU's look-ahead bulk update on the tensor cores (TF32x3) when
-// asked for (HBEM_TUNE_LU_UPDATE = 2).  Measured on one B200: n = 1043 x 40
-// factors in 6.7 instead of 7.3 ms, 4096 x 4 in 28.2 instead of 29.6 ms and
-// 18 749 x 2 in 701 instead of 1130 ms; but the split products keep 22 of
-// FP32's 24 significand bits, and on a BEM matrix (the 1952-dof quarter horn)
-// the unrefined solution is 5.5e-5 from LAPACK instead of the FP32 LU's
-// < 1e-5, so the default stays the exact-FP32 CUDA-core update (cgesv).
-static bool plain_update_on_tensor_cores() {
-    return tuning(HBEM_TUNE_LU_UPDATE) == 2;
+// The FP32 LU's look-ahead bulk update on the tensor cores (TF32x3): the
+// built-in choice of HBEM_PREC_TF32X3, or HBEM_TUNE_LU_UPDATE = 2.  Measured
+// on one B200: n = 1043 x 40 factors in 6.5 instead of 7.4 ms, 4096 x 4 in
+// 28.2 instead of 29.6 ms and 18 749 x 2 in 701 instead of 1130 ms; but the
+// split products keep 22 of FP32's 24 significand bits, and on a BEM matrix
+// (the 1952-dof quarter horn) the unrefined solution is 5.5e-5 from LAPACK
+// instead of the FP32 LU's < 1e-5.  So HBEM_PREC_PLAIN (cgesv) keeps the
+// exact-FP32 CUDA-core update, and the TF32x3 bulk is for callers that refine
+// with FP64 residuals, which recover the FP32 LU's solution accuracy.
+static bool plain_update_on_tensor_cores(int precision) {
+    const int v = tuning(HBEM_TUNE_LU_UPDATE);
+    return v == 2 || (v == 0 && precision == HBEM_PREC_TF32X3);
 }
 
 int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long long a_stride, int *piv,
@@ -1873,8 +2077,8 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
     // waits report through this status word
     int *status = nullptr;
     TcWorkspace *tc = nullptr;
-    const bool tf32_bulk = precision == HBEM_PREC_PLAIN && n > 2 * NB && tuning(HBEM_TUNE_LU_LOOKAHEAD) != 1 &&
-                           plain_update_on_tensor_cores();
+    const bool tf32_bulk = precision != HBEM_PREC_MIXED && n > 2 * NB && tuning(HBEM_TUNE_LU_LOOKAHEAD) != 1 &&
+                           plain_update_on_tensor_cores(precision);
     if ((precision == HBEM_PREC_MIXED && n > 64) || tf32_bulk) {
         HBEM_CUDA(cudaMallocAsync((void **)&status, sizeof(int), st));
         HBEM_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
@@ -1904,26 +2108,17 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
             cudaStreamWaitEvent(st, la->join_bulk, 0);
         }
         tc_workspace_destroy(tc, st);
-        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-        if (status && cudaStreamIsCapturing(st, &cap) == cudaSuccess && cap != cudaStreamCaptureStatusNone) {
-            // inside a graph capture nothing may wait for the host: a timed-out
-            // wait of the tensor-core update is folded into the module fault
-            // word that hbem_solve_status reports
+        if (status) {
+            // nothing waits for the host here (the caller's next launches
+            // queue behind the factorisation, and a graph capture may be
+            // running): a timed-out wait of the tensor-core update is folded
+            // into the module fault word, which hbem_solve_status,
+            // hbem_refine and hbem_solve_batch report
             k_fold_status<<<1, 1, 0, st>>>(status);
             cudaError_t e = cudaGetLastError();
             if (e == cudaSuccess) count_launch();
             else if (rc == HBEM_OK) rc = cuda_fail(e, "k_fold_status");
             cudaFreeAsync(status, st);
-        } else if (status) {
-            int h = 0;
-            if (rc == HBEM_OK) {
-                cudaError_t e = cudaMemcpyAsync(&h, status, sizeof(int), cudaMemcpyDeviceToHost, st);
-                if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-                if (e != cudaSuccess) rc = cuda_fail(e, "lu status");
-            }
-            cudaFreeAsync(status, st);
-            if (rc == HBEM_OK && h != 0)
-                rc = fail(HBEM_ERR_STATE, "tensor-core trailing update: barrier wait timed out (status " + std::to_string(h) + ")");
         }
         return rc;
     };
@@ -1937,6 +2132,31 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
         return e == cudaSuccess ? HBEM_OK : cuda_fail(e, what);
     };
     HBEM_CUDA(cudaFuncSetAttribute(k_panel_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+    HBEM_CUDA(cudaFuncSetAttribute(k_panel_reg<64, 1, 384>, cudaFuncAttributeMaxDynamicSharedMemorySize, 384 * 129 * 4));
+    HBEM_CUDA(cudaFuncSetAttribute(k_panel_reg<32, 1, 768>, cudaFuncAttributeMaxDynamicSharedMemorySize, 768 * 65 * 4));
+    HBEM_CUDA(cudaFuncSetAttribute(k_panel_reg<16, 1, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, 1024 * 33 * 4));
+    // sub-panels held in registers, one row per thread (64 columns up to 384
+    // rows, 32 up to 768, 16 up to 1024), when asked for; false: use the
+    // shared-memory or cluster kernels.  Not the default: on one B200 the
+    // n = 1043 x 40 factorisation takes 6.69 ms with them against 6.56 ms
+    // (TF32x3 bulk; 7.50 against 7.47 ms with the CUDA-core bulk).  Either
+    // kind costs about 2.4 us per column, which is the two CTA barriers and
+    // the pivot-row exchange of every column, not the row traffic that the
+    // registers remove.
+    auto panel_in_registers = [&](int c, int w) -> bool {
+        if (tuning(HBEM_TUNE_LU_PANEL_KERNEL) != 1) return false;
+        const int m = n - c;
+        const size_t ssm = (size_t)m * (2 * w + 1) * sizeof(float);
+        if (w == 64 && m <= 384)
+            k_panel_reg<64, 1, 384><<<batch, 384, ssm, cs>>>(a_re, a_im, lda, a_stride, n, c, piv, piv_stride, info);
+        else if (w == 32 && m <= 768)
+            k_panel_reg<32, 1, 768><<<batch, 768, ssm, cs>>>(a_re, a_im, lda, a_stride, n, c, piv, piv_stride, info);
+        else if (w == 16 && m <= 1024)
+            k_panel_reg<16, 1, 1024><<<batch, 1024, ssm, cs>>>(a_re, a_im, lda, a_stride, n, c, piv, piv_stride, info);
+        else
+            return false;
+        return true;
+    };
     HBEM_CUDA(cudaFuncSetAttribute(k_swap_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSwapSmem));
     const int cmax = panel_cluster_max(smem_cap);
     // Row swaps of block [b0, b0 + bw) on the columns [lo, hi) minus
@@ -1985,7 +2205,9 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
             const int w = std::min(nbi, b0 + bw - c);
             const size_t psmem = (size_t)(n - c) * (w + 1) * 8;
             int rc = HBEM_OK;
-            if (psmem <= smem_cap) {
+            if (panel_in_registers(c, w)) {
+                rc = launched("k_panel_reg");
+            } else if (psmem <= smem_cap) {
                 k_panel_rows<<<batch, kPanelRowsThreads, psmem, cs>>>(a_re, a_im, lda, a_stride, n, c, w, piv, piv_stride,
                                                                   info);
                 rc = launched("k_panel_rows");
@@ -2020,10 +2242,11 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
         const int outside = n - bw;
         const int next_end = std::min(n, b0 + bw + NB);
         // SMs the persistent tensor-core update leaves to the chain: by
-        // default 32 for the TF32x3 bulk of small matrices (n = 1043 x 40:
-        // 6.74 -> 6.46 ms), whose chain of panels is the longer path
+        // default 32 for the TF32x3 bulk of small matrices, whose chain of
+        // panels is the longer path (n = 1043 x 40: 6.76 -> 6.47 ms; at
+        // 1542 x 40 it costs: 15.06 -> 15.62 ms)
         const int tc_reserve = tuning(HBEM_TUNE_LU_RESERVE) > 0 ? tuning(HBEM_TUNE_LU_RESERVE) - 1
-                               : (tf32_bulk && n < 2048)       ? 32
+                               : (tf32_bulk && n <= 1280)      ? 32
                                                                 : 0;
         const bool split = la && next_end < n;
         if (outside > 0) {
@@ -2106,7 +2329,7 @@ int wave_fault_check(cudaStream_t st) {
     cudaMemcpyToSymbolAsync(g_wave_fault, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, st);
     cudaStreamSynchronize(st);
     return fail(HBEM_ERR_STATE, "a bounded device wait timed out: a triangular solve's wait for an earlier block (its "
-                                "results are NaN) or a captured factorisation's tensor-core update");
+                                "results are NaN) or a factorisation's tensor-core update");
 }
 
 int lu_solve_single(int n, int nrhs, int batch, const float *lu_re, const float *lu_im, long long lda,
@@ -2452,8 +2675,8 @@ extern "C" int hbem_lu_factor(int n, int batch, float *a_re, float *a_im, long l
     if (n <= 0 || batch <= 0) return HBEM_OK;
     if (!a_re || !a_im || !piv || !info) return fail(HBEM_ERR_ARG, "hbem_lu_factor: NULL pointer");
     if (lda < n || a_stride < lda * (long long)n || piv_stride < n) return fail(HBEM_ERR_ARG, "hbem_lu_factor: bad strides");
-    if (precision != HBEM_PREC_PLAIN && precision != HBEM_PREC_MIXED)
-        return fail(HBEM_ERR_ARG, "hbem_lu_factor: precision must be HBEM_PREC_PLAIN or HBEM_PREC_MIXED");
+    if (precision != HBEM_PREC_PLAIN && precision != HBEM_PREC_MIXED && precision != HBEM_PREC_TF32X3)
+        return fail(HBEM_ERR_ARG, "hbem_lu_factor: precision must be HBEM_PREC_PLAIN, HBEM_PREC_TF32X3 or HBEM_PREC_MIXED");
     return lu_factor(n, batch, a_re, a_im, lda, a_stride, piv, piv_stride, info, precision,
                      reinterpret_cast<cudaStream_t>(stream));
 }

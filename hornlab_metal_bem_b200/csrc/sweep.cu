@@ -244,7 +244,11 @@ static int solve_batch_impl(hbem_session *h, int n_freq, int n_src, const float 
             }
             if (rc != HBEM_OK) break;
         } else {
-            rc = lu_factor((int)n, nf, ar, ai, (long long)n, nn, dpiv, (long long)n, dinfo, precision, st);
+            // with refinement on, the FP32 LU's bulk update runs on the tensor
+            // cores (TF32x3): the FP64-residual passes recover the accuracy
+            // its 22-bit split products give away
+            const int lu_prec = (precision == HBEM_PREC_PLAIN && do_refine) ? HBEM_PREC_TF32X3 : precision;
+            rc = lu_factor((int)n, nf, ar, ai, (long long)n, nn, dpiv, (long long)n, dinfo, lu_prec, st);
             if (rc != HBEM_OK) break;
             if (rcond) {
                 // condition estimate on the second stream, beside the solves (both only read the factors)

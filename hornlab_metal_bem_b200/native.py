@@ -39,6 +39,7 @@ HBEM_ASM_CORRECTED = 7
 HBEM_PREC_PLAIN = 0
 HBEM_PREC_MIXED = 1
 HBEM_PREC_FP64 = 2
+HBEM_PREC_TF32X3 = 3
 HBEM_TRANS_N, HBEM_TRANS_T, HBEM_TRANS_C = 0, 1, 2
 # aperture faces from which the coupled solve uses the augmented (m + n) system
 AUGMENTED_MIN_APERTURE = 512
@@ -175,6 +176,13 @@ def solve_mode(precision: str, dense_solve_dtype: str = "float32") -> str:
 
 
 SOLVE_IMPL = {"plain": "hbem_blocked_lu_fp32", "mixed": "hbem_blocked_lu_bf16x3", "fp64": "hbem_blocked_lu_fp64"}
+
+
+def solve_impl(mode: str, refined: bool) -> str:
+    """Diagnostics name of the dense solve: a refined plain solve factors with the TF32x3 tensor-core bulk update."""
+    if not refined:
+        return SOLVE_IMPL[mode]
+    return (SOLVE_IMPL[mode] + "_tf32x3" if mode == "plain" else SOLVE_IMPL[mode]) + "_refined"
 
 
 NEAR_QUADRATURE_ENV = "HORNLAB_METAL_BEM_NATIVE_NEAR_QUADRATURE"
@@ -737,7 +745,7 @@ class NativeSession:
             avgs = [{int(t): complex(tavg[s_, f, j, 0], tavg[s_, f, j, 1]) for j, t in enumerate(want)}
                     for s_ in range(S)]
             diag = {
-                "dense_solve_impl": SOLVE_IMPL[mode] + ("_refined" if max_it > 0 else ""),
+                "dense_solve_impl": solve_impl(mode, max_it > 0),
                 "dense_solve_dtype": dense_solve_dtype,
                 "precision": precision,
                 "refine_iterations": int(iters[0, f]),
@@ -1026,8 +1034,7 @@ class NativeSession:
                 surface_pressure=out_p[f] if write_surface_pressure else None,
                 assembly_s=t_asm * 1e-3 / F, dense_solve_s=t_solve * 1e-3 / F, field_s=t_field * 1e-3 / F,
                 lapack_info=int(out_info[f]),
-                diagnostics={"dense_solve_impl": SOLVE_IMPL[mode] + ("_refined" if _refines(mode, refine_max_iterations)
-                                                                      else ""),
+                diagnostics={"dense_solve_impl": solve_impl(mode, _refines(mode, refine_max_iterations)),
                              "precision": "mixed" if mode == "mixed" else "plain",
                              "dense_solve_dtype": "float64" if mode == "fp64" else "float32",
                              "refine_iterations": int(out_iter[f]),
@@ -1124,8 +1131,7 @@ class NativeSession:
                 diagnostics={"coupled_ib": True, "ib_coupled_solve": method, "aperture_triangles": m,
                              "aperture_neumann": cat["qa"][f], "aperture_lapack_info": int(cat["info_ap"][f]),
                              "precision": precision, "dense_solve_dtype": dense_solve_dtype,
-                             "dense_solve_impl": SOLVE_IMPL[mode] + ("_refined" if _refines(mode, refine_max_iterations)
-                                                                     else ""),
+                             "dense_solve_impl": solve_impl(mode, _refines(mode, refine_max_iterations)),
                              "refine_iterations": int(cat["iters"][f]),
                              "refine_residual_rel": (float(cat["resid"][f]) if _refines(mode, refine_max_iterations)
                                                      else None),
@@ -1180,7 +1186,9 @@ class NativeSession:
         if refine:
             K0r, K0i = Kr.clone(), Ki.clone()
         xr, xi = br.clone(), bi.clone()
-        prec = HBEM_PREC_MIXED if mode == "mixed" else HBEM_PREC_PLAIN
+        # refined plain solves factor with the TF32x3 tensor-core bulk update; the FP64-residual passes
+        # recover what its 22-bit split products give away
+        prec = HBEM_PREC_MIXED if mode == "mixed" else (HBEM_PREC_TF32X3 if refine else HBEM_PREC_PLAIN)
         check(self.lib.hbem_lu_factor(N, F, _t_ptr(Kr), _t_ptr(Ki), lda, N * lda, _t_ptr(piv), N, _t_ptr(info), prec,
                                       st), "hbem_lu_factor", self.lib)
         if rcond:
@@ -1362,7 +1370,6 @@ class ResidentSweep:
         self.f_re = torch.empty((F, self.n_obs), dtype=torch.float32, device=dev)
         self.f_im = torch.empty_like(self.f_re)
         self.tag_out = torch.empty((F, max(1, self.tags.shape[0]), 2), dtype=torch.float64, device=dev)
-        self.precision = HBEM_PREC_MIXED if precision == "mixed" else HBEM_PREC_PLAIN
         self.rcond = torch.empty(F, dtype=torch.float64, device=dev) if rcond else None
         self.anorm = torch.empty(F, dtype=torch.float32, device=dev) if rcond else None
         # the condition estimate runs on a second stream beside the solves, refinement and field
@@ -1371,6 +1378,9 @@ class ResidentSweep:
         self.refine_tol = float(refine_tolerance)
         self.refine_max = max(1, int(refine_max_iterations)) if mode == "mixed" else int(refine_max_iterations)
         self.refine = _refines(mode, refine_max_iterations)
+        # as hbem_solve_batch: a refined plain sweep factors with the TF32x3 tensor-core bulk update
+        self.precision = (HBEM_PREC_MIXED if mode == "mixed" else
+                          HBEM_PREC_TF32X3 if self.refine else HBEM_PREC_PLAIN)
         # the assembled matrices kept for the FP64 residuals of the refinement
         self.A0_re = torch.empty_like(self.A_re) if self.refine else None
         self.A0_im = torch.empty_like(self.A_im) if self.refine else None

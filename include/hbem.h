@@ -49,6 +49,10 @@ extern "C" {
                                   look-ahead bulk update to the tensor cores (TF32x3) */
 #define HBEM_PREC_MIXED 1      /* BF16x3 tensor-core trailing updates; pair with hbem_refine */
 #define HBEM_PREC_FP64 2       /* hbem_solve_batch only: complex128 LU of the widened FP32 system (zgesv semantics) */
+#define HBEM_PREC_TF32X3 3     /* hbem_lu_factor only: the FP32 LU with its look-ahead bulk update on the tensor
+                                  cores as TF32x3 split products (22 significand bits per operand: backward error
+                                  a few times the FP32 LU's); for callers that refine with FP64 residuals, as
+                                  hbem_solve_batch's plain path does when refinement is on */
 
 /* Solve transposition */
 #define HBEM_TRANS_N 0
@@ -113,21 +117,27 @@ long long hbem_launch_count(void);
  *   HBEM_TUNE_LU_RESERVE:    SMs the look-ahead's persistent tensor-core
  *                            update leaves to the factorisation chain
  *                            (v >= 1: v - 1 SMs, at most half; 0: built-in,
- *                            32 for a plain LU of n < 2048, else none)
+ *                            32 for a TF32x3 bulk of n <= 1280, else none)
  *   HBEM_TUNE_WAVE_SPIN:     polls (of >= 32 ns) a wavefront-solve warp waits
  *                            for an earlier block before it gives up (0: the
  *                            built-in 2^22); a wait that runs out makes the
  *                            launch abort, writes NaN into the unfinished x
  *                            and is reported by hbem_solve_status and the
  *                            synchronising entry points as HBEM_ERR_STATE
- *   HBEM_TUNE_LU_UPDATE:     the K = 64 trailing update of the plain
- *                            (FP32) LU beside the factorisation chain
- *                            (1 and the built-in 0: CUDA cores, exact FP32
- *                            products; 2: tensor cores, TF32x3 split
- *                            products, 22 significand bits per operand)
+ *   HBEM_TUNE_LU_UPDATE:     the K = 64 trailing update of the FP32 LU
+ *                            beside the factorisation chain (0: built-in,
+ *                            CUDA cores for HBEM_PREC_PLAIN and tensor cores
+ *                            for HBEM_PREC_TF32X3; 1: CUDA cores, exact FP32
+ *                            products, for both; 2: tensor cores, TF32x3
+ *                            split products, for both)
  *   HBEM_TUNE_LU_BLOCK:      column block of the mixed (BF16x3) LU and the K
  *                            of its tensor-core update (64 or 128; 0: the
  *                            built-in 128 for n > 16000, else 64)
+ *   HBEM_TUNE_LU_PANEL_KERNEL: sub-panels with their rows in shared memory
+ *                            (0, built-in) or, where one row per thread fits,
+ *                            in registers (1: 64 columns up to 384 rows, 32
+ *                            up to 768, 16 up to 1024); the factors are the
+ *                            same bits
  */
 #define HBEM_TUNE_ASM_MINBLOCKS 0
 #define HBEM_TUNE_LU_PANEL 1
@@ -139,7 +149,8 @@ long long hbem_launch_count(void);
 #define HBEM_TUNE_WAVE_SPIN 7
 #define HBEM_TUNE_LU_UPDATE 8
 #define HBEM_TUNE_LU_BLOCK 9
-#define HBEM_TUNE_COUNT 10
+#define HBEM_TUNE_LU_PANEL_KERNEL 10
+#define HBEM_TUNE_COUNT 11
 int hbem_set_tuning(int key, int value);
 int hbem_get_tuning(int key);
 
@@ -223,10 +234,11 @@ int hbem_assemble_multi(hbem_session *s, int n_freq, const float *k_re, const fl
  * Replaces: cgesv_/cgetrf_ in solveDenseAccelerateCgesvMulti
  *   (main.swift:7834-7941, 8015-8020).
  * info: device int per matrix; 0 or the 1-based index of the first zero pivot.
- * Returns HBEM_OK even when a pivot is zero (read info).  With tensor-core
- * updates (mixed precision, or the plain LU's TF32x3 bulk) it synchronises
- * `stream` to report a timed-out barrier wait (HBEM_ERR_STATE); inside a CUDA
- * graph capture it does not synchronise, and hbem_solve_status reports it.
+ * precision: HBEM_PREC_PLAIN, HBEM_PREC_TF32X3 or HBEM_PREC_MIXED.
+ * Returns HBEM_OK even when a pivot is zero (read info).  Does not
+ * synchronise `stream`: a timed-out barrier wait of the tensor-core updates
+ * (mixed precision, or the FP32 LU's TF32x3 bulk) is reported as
+ * HBEM_ERR_STATE by hbem_solve_status, hbem_refine or hbem_solve_batch.
  */
 int hbem_lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long long a_stride,
                    int *piv, long long piv_stride, int *info, int precision, void *stream);
@@ -244,7 +256,7 @@ int hbem_lu_solve(int n, int nrhs, int batch, const float *lu_re, const float *l
  * Synchronise `stream` and report the device-side status of the asynchronous
  * solves issued before it: HBEM_ERR_STATE when a wavefront triangular-solve
  * wait timed out since the last report (that solve's unfinished x is NaN), or
- * the tensor-core update of a factorisation captured in a CUDA graph did,
+ * the tensor-core update of a factorisation did,
  * else HBEM_OK.  Clears the status.  hbem_refine, hbem_lu_rcond and
  * hbem_solve_batch report it themselves.  No counterpart in the reference,
  * whose LAPACK solves are synchronous.

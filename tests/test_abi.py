@@ -76,6 +76,7 @@ def test_tuning_knobs_validate_and_read_back():
         "HBEM_TUNE_WAVE_SPIN": ([0, 1, 4194304], [-1, 4194305]),
         "HBEM_TUNE_LU_UPDATE": ([0, 1, 2], [-1, 3]),
         "HBEM_TUNE_LU_BLOCK": ([0, 64, 128], [32, 256, -1]),
+        "HBEM_TUNE_LU_PANEL_KERNEL": ([0, 1], [-1, 2]),
     }
     assert set(valid) == set(keys)
     try:

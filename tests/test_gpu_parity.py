@@ -327,6 +327,59 @@ def test_lu_tall_panels_match_lapack(n):
     assert rel(X[0], ref) < (1e-5 if n < 3000 else 3e-5)
 
 
+@pytest.mark.parametrize("n,panel", [(1043, 0), (1300, 0), (700, 16), (1043, 32)])
+def test_register_panel_matches_shared_memory_panel(n, panel):
+    """Sub-panels with their rows in registers (HBEM_TUNE_LU_PANEL_KERNEL = 1: 64 columns x 384 rows,
+    32 x 768, 16 x 1024) give the same pivots and the same factors, bit for bit, as the shared-memory panel
+    kernel at the same sub-panel widths; HBEM_TUNE_LU_PANEL = 16 or 32 fixes the width in every block."""
+    lib = load_library()
+    batch = 5
+    A, _ = _lu_case(n, batch, n + 11)
+    out = {}
+    assert lib.hbem_set_tuning(1, panel) == 0
+    try:
+        for kernel in (0, 1):
+            Ar, Ai = _dev(A)
+            assert lib.hbem_set_tuning(10, kernel) == 0
+            piv, info = _factor(Ar, Ai, n, batch)
+            torch.cuda.synchronize()
+            out[kernel] = (Ar, Ai, piv, info)
+    finally:
+        lib.hbem_set_tuning(10, 0)
+        lib.hbem_set_tuning(1, 0)
+    assert int(out[0][3].abs().sum()) == 0 and int(out[1][3].abs().sum()) == 0
+    assert torch.equal(out[0][2], out[1][2])
+    assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1])
+
+
+@pytest.mark.parametrize("n,batch", [(1043, 6), (1542, 3)])
+def test_tf32x3_precision_refined_matches_lapack(n, batch):
+    """HBEM_PREC_TF32X3 (the FP32 LU with its bulk update on the tensor cores) followed by FP64-residual
+    refinement reaches the refinement tolerance and LAPACK's complex128 solution."""
+    lib = load_library()
+    A, b = _lu_case(n, batch, n + 3)
+    A0r, A0i = _dev(A)
+    Ar, Ai = A0r.clone(), A0i.clone()
+    piv, info = _factor(Ar, Ai, n, batch, precision=3)
+    assert int(info.abs().sum()) == 0
+    br, bi = _dev(b)
+    xr, xi = br.clone(), bi.clone()
+    _solve(Ar, Ai, piv, xr.view(batch, n, 1), xi.view(batch, n, 1), n, 1, batch)
+    iters = torch.zeros(batch, dtype=torch.int32, device="cuda")
+    resid = torch.zeros(batch, dtype=torch.float64, device="cuda")
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    p = ctypes.c_void_p
+    rc = lib.hbem_refine(n, batch, p(A0r.data_ptr()), p(A0i.data_ptr()), n, n * n, p(Ar.data_ptr()), p(Ai.data_ptr()),
+                         n * n, p(piv.data_ptr()), n, p(br.data_ptr()), p(bi.data_ptr()), n, p(xr.data_ptr()),
+                         p(xi.data_ptr()), n, ctypes.c_double(1e-7), 5, p(iters.data_ptr()), p(resid.data_ptr()), st)
+    assert rc == 0
+    assert float(resid.max()) <= 1e-7
+    x = _host(xr, xi)
+    for m in range(batch):
+        ref = np.linalg.solve(A[m].astype(np.complex128), b[m].astype(np.complex128))
+        assert rel(x[m], ref) < 1e-6
+
+
 @pytest.mark.parametrize("n,batch", [(300, 3), (1043, 6), (3300, 1)])
 def test_plain_lu_tensor_core_update_matches_lapack(n, batch):
     """The plain LU with its look-ahead bulk update on the tensor cores (TF32x3 split products,
