@@ -523,10 +523,11 @@ def run_b200(args, w):
         dist.destroy_process_group()
 
 
-def run_b200_c4(args, w, emit: bool = True, accuracy_picks=None):
+def run_b200_c4(args, w, emit: bool = True, accuracy_picks=None, refine_max_iterations: int = 10):
     """Coupled infinite-baffle sweep (augmented system, N = n + m unknowns) through
     ``NativeSession.coupled_ib_batch``; accuracy against an FP64 GPU solve of the
-    same assembled system on two of the frequencies."""
+    same assembled system on two of the frequencies.  ``refine_max_iterations`` = 0 with the plain
+    precision is the reference's cgesv arithmetic: an FP32 LU with exact FP32 updates, unrefined."""
     import torch
 
     world, rank, local = dist_env()
@@ -542,7 +543,8 @@ def run_b200_c4(args, w, emit: bool = True, accuracy_picks=None):
     n, m = sess.n_dof, sess.m_aperture
     N = n + m
     kw = dict(source_tags=w["tags"], impedance_source_tag=min(w["tags"]), precision=args.precision,
-              refine_tolerance=1e-6, field_k_f32=w["kf"], write_surface_pressure=True)
+              refine_tolerance=1e-6, refine_max_iterations=refine_max_iterations, field_k_f32=w["kf"],
+              write_surface_pressure=True)
     stream = torch.cuda.current_stream()
 
     def step():
@@ -929,12 +931,19 @@ def forms_summary(args) -> dict:
         for prec in ("mixed", "plain"):
             lines[prec] = run_b200_c4(sub(precision=prec, steps=1, warmup=1), w4, emit=False,
                                       accuracy_picks=[len(w4["freqs"]) - 1] if prec == "mixed" else [])
+        lines["cgesv"] = run_b200_c4(sub(precision="plain", steps=1, warmup=1), w4, emit=False, accuracy_picks=[],
+                                     refine_max_iterations=0)
         out["c4"] = {
             "workload": lines["mixed"]["config"]["workload"], "unknowns": lines["mixed"]["config"]["unknowns"],
             "mixed_freq_solves_per_s": lines["mixed"]["value"], "plain_freq_solves_per_s": lines["plain"]["value"],
+            "plain_path": "FP32 LU with the TF32x3 tensor-core bulk update + FP64-residual refinement (the default)",
             "mixed_over_plain": lines["mixed"]["value"] / lines["plain"]["value"],
+            "cgesv_freq_solves_per_s": lines["cgesv"]["value"],
+            "cgesv_path": "FP32 LU with exact FP32 CUDA-core updates, unrefined (the reference's cgesv arithmetic)",
+            "mixed_over_cgesv": lines["mixed"]["value"] / lines["cgesv"]["value"],
             "mixed_solve_ms": lines["mixed"]["stages_ms_per_step"]["solve_ms"],
             "plain_solve_ms": lines["plain"]["stages_ms_per_step"]["solve_ms"],
+            "cgesv_solve_ms": lines["cgesv"]["stages_ms_per_step"]["solve_ms"],
             "mixed_accuracy": lines["mixed"]["accuracy"], "mixed_roofline": lines["mixed"]["roofline"],
             "clocks": lines["mixed"]["clocks"]}
     except Exception as exc:   # a form that fails is reported, the headline still prints
