@@ -377,14 +377,14 @@ def run_b200(args, w):
         if ev0 is not None:
             ev0.record(stream)
         check(lib.hbem_assemble(sess.handle, F, _np_ptr(rs.k_re), _np_ptr(rs.k_im), _t_ptr(rs.q_re),
-                                _t_ptr(rs.q_im), sess.n_triangles, None, None, _t_ptr(rs.A_re), _t_ptr(rs.A_im), n,
-                                n * n, _t_ptr(rs.b_re), _t_ptr(rs.b_im), n, HBEM_ASM_REGULAR, _stream_ptr()),
+                                _t_ptr(rs.q_im), sess.n_triangles, None, None, _t_ptr(rs.A_re), _t_ptr(rs.A_im), rs.lda,
+                                n * rs.lda, _t_ptr(rs.b_re), _t_ptr(rs.b_im), n, HBEM_ASM_REGULAR, _stream_ptr()),
               "hbem_assemble", lib)
         if ev1 is not None:
             ev1.record(stream)
         check(lib.hbem_assemble(sess.handle, F, _np_ptr(rs.k_re), _np_ptr(rs.k_im), _t_ptr(rs.q_re),
-                                _t_ptr(rs.q_im), sess.n_triangles, None, None, _t_ptr(rs.A_re), _t_ptr(rs.A_im), n,
-                                n * n, _t_ptr(rs.b_re), _t_ptr(rs.b_im), n, HBEM_ASM_DUFFY, _stream_ptr()),
+                                _t_ptr(rs.q_im), sess.n_triangles, None, None, _t_ptr(rs.A_re), _t_ptr(rs.A_im), rs.lda,
+                                n * rs.lda, _t_ptr(rs.b_re), _t_ptr(rs.b_im), n, HBEM_ASM_DUFFY, _stream_ptr()),
               "hbem_assemble", lib)
 
     # the job's result: every rank's fields, gathered to all ranks (NCCL) after each sweep

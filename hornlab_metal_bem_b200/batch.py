@@ -28,7 +28,7 @@ import numpy as np
 
 from .native import (
     HBEM_ASM_CORRECTED, HBEM_PREC_PLAIN, HBEM_PREC_TF32X3, HBEM_TRANS_N, NativeSession, _np_ptr, _stream_ptr, _t_ptr,
-    check, load_library, require_cuda,
+    check, load_library, matrix_ld, require_cuda,
 )
 
 TUNE_ASM_MINBLOCKS, TUNE_LU_PANEL, TUNE_LU_SOLVE, TUNE_ASM_PAIRS, TUNE_DUFFY = 0, 1, 2, 3, 4
@@ -181,7 +181,7 @@ class _Slot:
 
     def __init__(self, torch, dev, n_max: int, F_max: int, refine: bool):
         self.stream = torch.cuda.Stream(device=dev)
-        self.A_re = torch.empty((F_max, n_max, n_max), dtype=torch.float32, device=dev)
+        self.A_re = torch.empty((F_max, n_max, matrix_ld(n_max)), dtype=torch.float32, device=dev)
         self.A_im = torch.empty_like(self.A_re)
         # the assembled matrices, kept for the FP64 residuals of the refinement
         self.A0_re = torch.empty_like(self.A_re) if refine else None
@@ -225,28 +225,29 @@ class _CaseRun:
     def launch(self, slot: _Slot):
         """The sweep's launches on the current stream (captured or eager)."""
         n, F, st, lib, s = self.n, self.F, _stream_ptr(), self.lib, self.s
-        A_re, A_im = slot.A_re.view(-1)[:F * n * n], slot.A_im.view(-1)[:F * n * n]
+        ld = matrix_ld(n)   # rows on 16-byte boundaries
+        A_re, A_im = slot.A_re.view(-1)[:F * n * ld], slot.A_im.view(-1)[:F * n * ld]
         b_re, b_im = slot.b_re.view(-1)[:F * n], slot.b_im.view(-1)[:F * n]
         x_re, x_im = slot.x_re.view(-1)[:F * n], slot.x_im.view(-1)[:F * n]
         piv = slot.piv.view(-1)[:F * n]
         check(lib.hbem_assemble(s.handle, F, _np_ptr(self.k_re), _np_ptr(self.k_im), _t_ptr(self.q_re),
-                                _t_ptr(self.q_im), s.n_triangles, None, None, _t_ptr(A_re), _t_ptr(A_im), n, n * n,
+                                _t_ptr(self.q_im), s.n_triangles, None, None, _t_ptr(A_re), _t_ptr(A_im), ld, n * ld,
                                 _t_ptr(b_re), _t_ptr(b_im), n, HBEM_ASM_CORRECTED | 4, st), "hbem_assemble", lib)
         x_re.copy_(b_re)
         x_im.copy_(b_im)
         if self.refine_max > 0:
-            A0_re, A0_im = slot.A0_re.view(-1)[:F * n * n], slot.A0_im.view(-1)[:F * n * n]
+            A0_re, A0_im = slot.A0_re.view(-1)[:F * n * ld], slot.A0_im.view(-1)[:F * n * ld]
             A0_re.copy_(A_re)
             A0_im.copy_(A_im)
         # refined sweeps factor with the TF32x3 tensor-core bulk update (the refinement recovers FP32 accuracy)
         prec = HBEM_PREC_TF32X3 if self.refine_max > 0 else HBEM_PREC_PLAIN
-        check(lib.hbem_lu_factor(n, F, _t_ptr(A_re), _t_ptr(A_im), n, n * n, _t_ptr(piv), n, _t_ptr(self.info),
+        check(lib.hbem_lu_factor(n, F, _t_ptr(A_re), _t_ptr(A_im), ld, n * ld, _t_ptr(piv), n, _t_ptr(self.info),
                                  prec, st), "hbem_lu_factor", lib)
-        check(lib.hbem_lu_solve(n, 1, F, _t_ptr(A_re), _t_ptr(A_im), n, n * n, _t_ptr(piv), n, _t_ptr(x_re),
+        check(lib.hbem_lu_solve(n, 1, F, _t_ptr(A_re), _t_ptr(A_im), ld, n * ld, _t_ptr(piv), n, _t_ptr(x_re),
                                 _t_ptr(x_im), 1, n, HBEM_TRANS_N, st), "hbem_lu_solve", lib)
         if self.refine_max > 0:
-            check(lib.hbem_refine_async(n, F, _t_ptr(A0_re), _t_ptr(A0_im), n, n * n, _t_ptr(A_re), _t_ptr(A_im),
-                                        n * n, _t_ptr(piv), n, _t_ptr(b_re), _t_ptr(b_im), n, _t_ptr(x_re),
+            check(lib.hbem_refine_async(n, F, _t_ptr(A0_re), _t_ptr(A0_im), ld, n * ld, _t_ptr(A_re), _t_ptr(A_im),
+                                        n * ld, _t_ptr(piv), n, _t_ptr(b_re), _t_ptr(b_im), n, _t_ptr(x_re),
                                         _t_ptr(x_im), n, self.refine_tol, self.refine_max, _t_ptr(self.iters),
                                         _t_ptr(self.resid), st), "hbem_refine_async", lib)
         check(lib.hbem_field(s.handle, F, _np_ptr(self.k_re), _t_ptr(x_re), _t_ptr(x_im), n, _t_ptr(self.q_re),

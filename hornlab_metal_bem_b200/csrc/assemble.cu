@@ -1353,7 +1353,7 @@ extern "C" int hbem_assemble_multi(hbem_session *h, int n_freq, const float *k_r
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     HBEM_CUDA(cudaSetDevice(s->device));
     if (flags & HBEM_ASM_ZERO) {
-        if (lda == s->n_dof && a_stride == lda * s->n_dof) {
+        if (a_stride == lda * s->n_dof) {   // one slab (a padded leading dimension is zeroed with it)
             HBEM_CUDA(cudaMemsetAsync(a_re, 0, sizeof(float) * (size_t)a_stride * n_freq, st));
             HBEM_CUDA(cudaMemsetAsync(a_im, 0, sizeof(float) * (size_t)a_stride * n_freq, st));
         } else {

@@ -53,14 +53,21 @@ struct Layout {
     size_t q, a, a0, a64, x64, x, b, piv, info, obs, fld, tag, want, iters, resid, anorm, rcond, total;
 };
 
+// Leading dimension of the dense FP32 matrices: n rounded up to a multiple of
+// 4 floats, so every row starts on a 16-byte boundary and the trailing
+// updates read and write C as float4 (an odd n = 1043 made three rows in four
+// take the scalar path: the 1043 x 40 LU 7.4 -> 6.5 ms with the exact-FP32
+// update, 6.5 -> 6.2 ms with the TF32x3 one, measured at n = 1044).
+size_t matrix_ld(size_t n) { return (n + 3) & ~(size_t)3; }
+
 Layout layout(const Session &s, int nf, int n_src, int n_obs, int n_tags, bool keep_a, bool fp64) {
-    const size_t n = s.n_dof, T = s.n_triangles, ns = (size_t)n_src;
+    const size_t n = s.n_dof, T = s.n_triangles, ns = (size_t)n_src, ld = matrix_ld(n);
     Layout L{};
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t o = off; off += align_up(bytes); return o; };
     L.q = take(2 * sizeof(float) * ns * nf * T);
-    L.a = take(2 * sizeof(float) * nf * n * n);
-    L.a0 = keep_a ? take(2 * sizeof(float) * nf * n * n) : 0;
+    L.a = take(2 * sizeof(float) * nf * n * ld);
+    L.a0 = keep_a ? take(2 * sizeof(float) * nf * n * ld) : 0;
     L.a64 = fp64 ? take(2 * sizeof(double) * nf * n * n) : 0;
     L.x64 = fp64 ? take(2 * sizeof(double) * ns * nf * n) : 0;
     L.x = take(2 * sizeof(float) * ns * nf * n);
@@ -126,7 +133,7 @@ static int solve_batch_impl(hbem_session *h, int n_freq, int n_src, const float 
     const bool do_refine = !fp64 && ((precision == HBEM_PREC_MIXED) || refine_max_iter > 0);
     const int max_iter = precision == HBEM_PREC_MIXED ? std::max(1, refine_max_iter) : refine_max_iter;
     const double tol = refine_tol > 0 ? refine_tol : 1e-6;
-    const size_t n = s->n_dof, T = s->n_triangles, ns = (size_t)n_src;
+    const size_t n = s->n_dof, T = s->n_triangles, ns = (size_t)n_src, ld = matrix_ld(n);
 
     // chunk size: dense matrices within ~60 % of free memory
     size_t free_b = 0, total_b = 0;
@@ -192,13 +199,13 @@ static int solve_batch_impl(hbem_session *h, int n_freq, int n_src, const float 
             ok(cudaMemcpyAsync(qr + sv * qs, q_re + ho, sizeof(float) * qs, cudaMemcpyHostToDevice, st), "q");
             ok(cudaMemcpyAsync(qi + sv * qs, q_im + ho, sizeof(float) * qs, cudaMemcpyHostToDevice, st), "q");
         }
-        float *ar = da, *ai = da + (size_t)nf * n * n;
+        float *ar = da, *ai = da + (size_t)nf * n * ld;
         float *br = db, *bi = db + ns * xs;
         float *xr = dx, *xi = dx + ns * xs;
         ok(cudaEventRecord(ev[0], st), "cudaEventRecord");
         if (rc != HBEM_OK) break;
         rc = hbem_assemble_multi(h, nf, k_re + f0, k_im ? k_im + f0 : nullptr, n_src, qr, qi, (long long)T,
-                                 (long long)qs, nullptr, nullptr, ar, ai, (long long)n, (long long)(n * n), br, bi,
+                                 (long long)qs, nullptr, nullptr, ar, ai, (long long)ld, (long long)(n * ld), br, bi,
                                  (long long)n, (long long)xs, HBEM_ASM_CORRECTED, st);
         if (rc != HBEM_OK) break;
         ok(cudaEventRecord(ev[1], st), "cudaEventRecord");
@@ -207,22 +214,22 @@ static int solve_batch_impl(hbem_session *h, int n_freq, int n_src, const float 
         float *a0r = nullptr, *a0i = nullptr;
         if (do_refine) {
             a0r = da0;
-            a0i = da0 + (size_t)nf * n * n;
-            ok(cudaMemcpyAsync(a0r, ar, sizeof(float) * nf * n * n, cudaMemcpyDeviceToDevice, st), "A copy");
-            ok(cudaMemcpyAsync(a0i, ai, sizeof(float) * nf * n * n, cudaMemcpyDeviceToDevice, st), "A copy");
+            a0i = da0 + (size_t)nf * n * ld;
+            ok(cudaMemcpyAsync(a0r, ar, sizeof(float) * nf * n * ld, cudaMemcpyDeviceToDevice, st), "A copy");
+            ok(cudaMemcpyAsync(a0i, ai, sizeof(float) * nf * n * ld, cudaMemcpyDeviceToDevice, st), "A copy");
         }
         if (rc != HBEM_OK) break;
         if (rcond) {
-            rc = matrix_norm1((int)n, nf, ar, ai, (long long)n, (long long)(n * n), danorm, st);
+            rc = matrix_norm1((int)n, nf, ar, ai, (long long)ld, (long long)(n * ld), danorm, st);
             if (rc != HBEM_OK) break;
         }
-        const long long nn = (long long)(n * n);
+        const long long nn = (long long)(n * n), na = (long long)(n * ld), lda = (long long)ld;
         if (fp64) {
             // the reference's float64 dense solve: widen the FP32 system to
             // complex128, factor and solve in FP64, narrow the solution
             double *a64r = da64, *a64i = da64 + (size_t)nf * n * n;
             double *x64r = dx64, *x64i = dx64 + ns * xs;
-            rc = widen_f64((int)n, (int)n, nf, ar, ai, (long long)n, nn, a64r, a64i, (long long)n, nn, st);
+            rc = widen_f64((int)n, (int)n, nf, ar, ai, lda, na, a64r, a64i, (long long)n, nn, st);
             if (rc == HBEM_OK)
                 rc = widen_f64(1, (int)n, n_src * nf, br, bi, (long long)n, (long long)n, x64r, x64i, (long long)n,
                                (long long)n, st);
@@ -236,10 +243,10 @@ static int solve_batch_impl(hbem_session *h, int n_freq, int n_src, const float 
                                 (long long)n, st);
             if (rc == HBEM_OK && rcond) {
                 // condition estimate from the FP64 factors narrowed to FP32, on the second stream
-                rc = narrow_f64((int)n, (int)n, nf, a64r, a64i, (long long)n, nn, ar, ai, (long long)n, nn, st);
+                rc = narrow_f64((int)n, (int)n, nf, a64r, a64i, (long long)n, nn, ar, ai, lda, na, st);
                 if (rc == HBEM_OK && ok(cudaEventRecord(s->aux_fork, st), "fork") &&
                     ok(cudaStreamWaitEvent(s->aux, s->aux_fork, 0), "fork"))
-                    rc = lu_rcond((int)n, nf, ar, ai, (long long)n, nn, danorm, drcond, s->aux);
+                    rc = lu_rcond((int)n, nf, ar, ai, lda, na, danorm, drcond, s->aux);
                 if (rc == HBEM_OK) ok(cudaEventRecord(s->aux_join, s->aux), "join");
             }
             if (rc != HBEM_OK) break;
@@ -248,23 +255,23 @@ static int solve_batch_impl(hbem_session *h, int n_freq, int n_src, const float 
             // cores (TF32x3): the FP64-residual passes recover the accuracy
             // its 22-bit split products give away
             const int lu_prec = (precision == HBEM_PREC_PLAIN && do_refine) ? HBEM_PREC_TF32X3 : precision;
-            rc = lu_factor((int)n, nf, ar, ai, (long long)n, nn, dpiv, (long long)n, dinfo, lu_prec, st);
+            rc = lu_factor((int)n, nf, ar, ai, lda, na, dpiv, (long long)n, dinfo, lu_prec, st);
             if (rc != HBEM_OK) break;
             if (rcond) {
                 // condition estimate on the second stream, beside the solves (both only read the factors)
                 if (ok(cudaEventRecord(s->aux_fork, st), "fork") && ok(cudaStreamWaitEvent(s->aux, s->aux_fork, 0), "fork"))
-                    rc = lu_rcond((int)n, nf, ar, ai, (long long)n, nn, danorm, drcond, s->aux);
+                    rc = lu_rcond((int)n, nf, ar, ai, lda, na, danorm, drcond, s->aux);
                 if (rc == HBEM_OK) ok(cudaEventRecord(s->aux_join, s->aux), "join");
                 if (rc != HBEM_OK) break;
             }
             for (int sv = 0; sv < n_src && rc == HBEM_OK; ++sv)
-                rc = lu_solve((int)n, 1, nf, ar, ai, (long long)n, nn, dpiv, (long long)n, xr + sv * xs, xi + sv * xs,
+                rc = lu_solve((int)n, 1, nf, ar, ai, lda, na, dpiv, (long long)n, xr + sv * xs, xi + sv * xs,
                               1, (long long)n, HBEM_TRANS_N, st);
             if (rc != HBEM_OK) break;
         }
         if (do_refine) {
             for (int sv = 0; sv < n_src && rc == HBEM_OK; ++sv)
-                rc = refine((int)n, nf, a0r, a0i, (long long)n, nn, ar, ai, nn, dpiv, (long long)n, br + sv * xs,
+                rc = refine((int)n, nf, a0r, a0i, lda, na, ar, ai, na, dpiv, (long long)n, br + sv * xs,
                             bi + sv * xs, (long long)n, xr + sv * xs, xi + sv * xs, (long long)n, tol, max_iter,
                             diters + (size_t)sv * nf, dres + (size_t)sv * nf, st);
             if (rc != HBEM_OK) break;

@@ -178,6 +178,12 @@ def solve_mode(precision: str, dense_solve_dtype: str = "float32") -> str:
 SOLVE_IMPL = {"plain": "hbem_blocked_lu_fp32", "mixed": "hbem_blocked_lu_bf16x3", "fp64": "hbem_blocked_lu_fp64"}
 
 
+def matrix_ld(n: int) -> int:
+    """Leading dimension of the dense FP32 matrices: ``n`` rounded up to 4 floats, so rows start on 16-byte
+    boundaries and the LU's trailing updates move C as float4 (as ``hbem_solve_batch`` lays them out)."""
+    return (int(n) + 3) & ~3
+
+
 def solve_impl(mode: str, refined: bool) -> str:
     """Diagnostics name of the dense solve: a refined plain solve factors with the TF32x3 tensor-core bulk update."""
     if not refined:
@@ -980,14 +986,15 @@ class NativeSession:
             b_re = torch.tensor(np.ascontiguousarray(beta.real), device=dev)
             b_im = torch.tensor(np.ascontiguousarray(beta.imag), device=dev)
             qr, qi = self._split_device(q[sl], (Fg, T), dev)
-            Ar = torch.empty((Fg, n, n), dtype=torch.float32, device=dev)
+            ld = matrix_ld(n)
+            Ar = torch.empty((Fg, n, ld), dtype=torch.float32, device=dev)
             Ai = torch.empty_like(Ar)
             br = torch.empty((Fg, n), dtype=torch.float32, device=dev)
             bi = torch.empty_like(br)
             kr_g, ki_g = np.ascontiguousarray(k_re[sl]), np.ascontiguousarray(k_im[sl])
             ev[0].record()
             check(self.lib.hbem_assemble(self.handle, Fg, _np_ptr(kr_g), _np_ptr(ki_g), _t_ptr(qr), _t_ptr(qi), T,
-                                         _t_ptr(b_re), _t_ptr(b_im), _t_ptr(Ar), _t_ptr(Ai), n, n * n, _t_ptr(br),
+                                         _t_ptr(b_re), _t_ptr(b_im), _t_ptr(Ar), _t_ptr(Ai), ld, n * ld, _t_ptr(br),
                                          _t_ptr(bi), n, HBEM_ASM_CORRECTED | HBEM_ASM_ZERO, st),
                   "hbem_assemble", self.lib)
             ev[1].record()
@@ -1355,11 +1362,12 @@ class ResidentSweep:
         self.k_im = None if k_im is None else np.ascontiguousarray(np.atleast_1d(k_im), dtype=np.float32)
         F, n, T = self.k_re.shape[0], session.n_dof, session.n_triangles
         self.F, self.n = F, n
+        self.lda = ld = matrix_ld(n)
         self.q_re, self.q_im = NativeSession._split_device(q, (F, T), dev)
         self.obs = torch.as_tensor(np.ascontiguousarray(obs_3xn, dtype=np.float32), device=dev)
         self.n_obs = int(self.obs.shape[1])
         self.tags = np.ascontiguousarray(tags, dtype=np.int32)
-        self.A_re = torch.empty((F, n, n), dtype=torch.float32, device=dev)
+        self.A_re = torch.empty((F, n, ld), dtype=torch.float32, device=dev)
         self.A_im = torch.empty_like(self.A_re)
         self.b_re = torch.empty((F, n), dtype=torch.float32, device=dev)
         self.b_im = torch.empty_like(self.b_re)
@@ -1388,38 +1396,39 @@ class ResidentSweep:
         self.resid = torch.zeros(F, dtype=torch.float64, device=dev)
 
     def assemble(self, stream=None):
-        n = self.n
+        n, ld = self.n, self.lda
         check(self.lib.hbem_assemble(
             self.s.handle, self.F, _np_ptr(self.k_re), _np_ptr(self.k_im), _t_ptr(self.q_re), _t_ptr(self.q_im),
-            self.s.n_triangles, None, None, _t_ptr(self.A_re), _t_ptr(self.A_im), n, n * n, _t_ptr(self.b_re),
+            self.s.n_triangles, None, None, _t_ptr(self.A_re), _t_ptr(self.A_im), ld, n * ld, _t_ptr(self.b_re),
             _t_ptr(self.b_im), n, HBEM_ASM_CORRECTED, _stream_ptr(stream)), "hbem_assemble", self.lib)
 
     def factor_solve(self, stream=None):
-        n, st = self.n, _stream_ptr(stream)
+        n, ld, st = self.n, self.lda, _stream_ptr(stream)
         self.x_re.copy_(self.b_re)
         self.x_im.copy_(self.b_im)
         if self.refine:
             self.A0_re.copy_(self.A_re)
             self.A0_im.copy_(self.A_im)
         if self.rcond is not None:
-            check(self.lib.hbem_matrix_norm1(n, self.F, _t_ptr(self.A_re), _t_ptr(self.A_im), n, n * n,
+            check(self.lib.hbem_matrix_norm1(n, self.F, _t_ptr(self.A_re), _t_ptr(self.A_im), ld, n * ld,
                                              _t_ptr(self.anorm), st), "hbem_matrix_norm1", self.lib)
-        check(self.lib.hbem_lu_factor(n, self.F, _t_ptr(self.A_re), _t_ptr(self.A_im), n, n * n, _t_ptr(self.piv), n,
+        check(self.lib.hbem_lu_factor(n, self.F, _t_ptr(self.A_re), _t_ptr(self.A_im), ld, n * ld, _t_ptr(self.piv), n,
                                       _t_ptr(self.info), self.precision, st), "hbem_lu_factor", self.lib)
         if self.rcond is not None:
             import torch
 
             main = torch.cuda.current_stream() if stream is None else stream
             self.aux.wait_stream(main)
-            check(self.lib.hbem_lu_rcond(n, self.F, _t_ptr(self.A_re), _t_ptr(self.A_im), n, n * n, _t_ptr(self.anorm),
-                                         _t_ptr(self.rcond), _stream_ptr(self.aux)), "hbem_lu_rcond", self.lib)
-        check(self.lib.hbem_lu_solve(n, 1, self.F, _t_ptr(self.A_re), _t_ptr(self.A_im), n, n * n, _t_ptr(self.piv), n,
-                                     _t_ptr(self.x_re), _t_ptr(self.x_im), 1, n, HBEM_TRANS_N, st), "hbem_lu_solve",
-              self.lib)
+            check(self.lib.hbem_lu_rcond(n, self.F, _t_ptr(self.A_re), _t_ptr(self.A_im), ld, n * ld,
+                                         _t_ptr(self.anorm), _t_ptr(self.rcond), _stream_ptr(self.aux)),
+                  "hbem_lu_rcond", self.lib)
+        check(self.lib.hbem_lu_solve(n, 1, self.F, _t_ptr(self.A_re), _t_ptr(self.A_im), ld, n * ld, _t_ptr(self.piv),
+                                     n, _t_ptr(self.x_re), _t_ptr(self.x_im), 1, n, HBEM_TRANS_N, st),
+              "hbem_lu_solve", self.lib)
         if self.refine:
             check(self.lib.hbem_refine(
-                n, self.F, _t_ptr(self.A0_re), _t_ptr(self.A0_im), n, n * n, _t_ptr(self.A_re), _t_ptr(self.A_im),
-                n * n, _t_ptr(self.piv), n, _t_ptr(self.b_re), _t_ptr(self.b_im), n, _t_ptr(self.x_re),
+                n, self.F, _t_ptr(self.A0_re), _t_ptr(self.A0_im), ld, n * ld, _t_ptr(self.A_re), _t_ptr(self.A_im),
+                n * ld, _t_ptr(self.piv), n, _t_ptr(self.b_re), _t_ptr(self.b_im), n, _t_ptr(self.x_re),
                 _t_ptr(self.x_im), n, self.refine_tol, self.refine_max, _t_ptr(self.iters), _t_ptr(self.resid), st),
                 "hbem_refine", self.lib)
 

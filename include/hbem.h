@@ -41,7 +41,8 @@ extern "C" {
 /* Assembly flags */
 #define HBEM_ASM_REGULAR 1     /* 6x6 Dunavant regular quadrature, all pairs */
 #define HBEM_ASM_DUFFY 2       /* Duffy singular corrections (coincident/edge/vertex pairs) */
-#define HBEM_ASM_ZERO 4        /* zero A and b before accumulating */
+#define HBEM_ASM_ZERO 4        /* zero A (a whole slab, padding columns included, when a_stride = lda * n)
+                                  and b before accumulating */
 #define HBEM_ASM_CORRECTED (HBEM_ASM_REGULAR | HBEM_ASM_DUFFY | HBEM_ASM_ZERO)
 
 /* LU precision */
