@@ -168,8 +168,9 @@ int launch_trailing_update(int n, int batch, int k0, int kw, int start, int col_
 // of shared memory):
 //   BF16x3: tiles of 64 complex rows x 64 columns, A2 64 KB (4 K-blocks of
 //           128 bytes per row), ring of 6 x 16 KB, two 32 KB C tiles;
-//   TF32x3: tiles of 64 complex rows x 32 columns, A2 128 KB (8 K-blocks),
-//           ring of 8 x 8 KB, two 16 KB C tiles.
+//   TF32x3 (and BF16x3 with K = 128): tiles of 64 complex rows x 32 columns,
+//           A2 128 KB (8 K-blocks), ring of 6 x 8 KB, three 16 KB C tiles
+//           (C prefetched two tiles ahead).
 // Every mbarrier wait is bounded; a timeout sets the status word and the CTA
 // returns after releasing its TMEM.
 // ===========================================================================
@@ -194,10 +195,15 @@ struct TcCfg {
     static constexpr int ABytes = 2 * KBH * kTcABlk;   // resident A2 of a row block
     static constexpr int BBlk = N * 128;               // one B K-block
     static constexpr int StageBytes = 2 * BBlk;        // ring stage: Bh and Bl of one K-block
-    static constexpr int Stages = KBH == 4 ? 8 : 6;    // B ring: two (K-block 4) / three tiles ahead
+    // B ring: one and a half 32-column tiles (K-block 4) / three 64-column tiles ahead
+    static constexpr int Stages = 6;
     static constexpr int CBytes = kTcM * N * 4;        // one C tile staged in shared memory
+    // C buffers: the 32-column tiles prefetch C two tiles ahead (one tile's
+    // time is shorter than the HBM latency of its C), the 64-column ones one
+    static constexpr int CBufs = N == 32 ? 3 : 2;
     static constexpr int Fmt = TF32 ? 2 : 1;           // instruction-descriptor operand format
-    static constexpr size_t Smem = (size_t)ABytes + (size_t)Stages * StageBytes + 2 * (size_t)CBytes + 1024;
+    static constexpr size_t Smem =
+        (size_t)ABytes + (size_t)Stages * StageBytes + (size_t)CBufs * CBytes + 1024;
     static_assert(Smem <= 227 * 1024, "tensor-core trailing update: shared memory");
 };
 
@@ -548,19 +554,22 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
             }
             asm volatile("cp.async.commit_group;" ::: "memory");
         };
+        constexpr int CB = Cfg::CBufs;
         TcWalk cur(blockIdx.x, tiles_m, tiles_n, n_chunks, chunk, n_units, G);
         TcWalk nxt = cur;
-        if (nxt.valid) {
-            prefetch(nxt.tile(), sC0);
+        for (int k = 0; k + 1 < CB && nxt.valid; ++k) {
+            prefetch(nxt.tile(), sC0 + (size_t)k * (kTcM * kTcN));
             nxt.advance();
         }
         for (int i = 0; cur.valid; ++i) {
             const int b = i & 1;
-            float *sC = sC0 + (size_t)b * (kTcM * kTcN);
+            float *sC = sC0 + (size_t)(i % CB) * (kTcM * kTcN);
             if (nxt.valid) {
-                prefetch(nxt.tile(), sC0 + (size_t)(b ^ 1) * (kTcM * kTcN));
+                // tile i + CB - 1 into the buffer tile i - 1 has written back
+                prefetch(nxt.tile(), sC0 + (size_t)((i + CB - 1) % CB) * (kTcM * kTcN));
                 nxt.advance();
-                asm volatile("cp.async.wait_group 1;" ::: "memory");
+                if constexpr (CB == 3) asm volatile("cp.async.wait_group 2;" ::: "memory");
+                else asm volatile("cp.async.wait_group 1;" ::: "memory");
             } else {
                 asm volatile("cp.async.wait_group 0;" ::: "memory");
             }
@@ -638,7 +647,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_trailing_tc(const __grid_cons
                     }
                 }
             }
-            epi_bar();   // buffer b may be refilled by the prefetch of tile i + 2
+            epi_bar();   // this buffer may be refilled by the next iteration's prefetch
             cur.advance();
         }
         asm volatile("cp.async.wait_all;" ::: "memory");
