@@ -135,13 +135,17 @@ static int solve_batch_impl(hbem_session *h, int n_freq, int n_src, const float 
     const double tol = refine_tol > 0 ? refine_tol : 1e-6;
     const size_t n = s->n_dof, T = s->n_triangles, ns = (size_t)n_src, ld = matrix_ld(n);
 
-    // chunk size: dense matrices within ~60 % of free memory
-    size_t free_b = 0, total_b = 0;
-    HBEM_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    free_b += s->ws_bytes;
+    // chunk size: the whole sweep when the session's workspace already holds
+    // it (no device query on repeated calls), else dense matrices within
+    // ~60 % of free memory
     int chunk = n_freq;
-    while (chunk > 1 && layout(*s, chunk, n_src, n_obs, n_tags, do_refine, fp64).total > free_b * 6 / 10)
-        chunk = (chunk + 1) / 2;
+    if (layout(*s, chunk, n_src, n_obs, n_tags, do_refine, fp64).total > s->ws_bytes) {
+        size_t free_b = 0, total_b = 0;
+        HBEM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        free_b += s->ws_bytes;
+        while (chunk > 1 && layout(*s, chunk, n_src, n_obs, n_tags, do_refine, fp64).total > free_b * 6 / 10)
+            chunk = (chunk + 1) / 2;
+    }
     const Layout L = layout(*s, chunk, n_src, n_obs, n_tags, do_refine, fp64);
     int rc = ensure_ws(*s, L.total);
     if (rc != HBEM_OK) return rc;
