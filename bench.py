@@ -58,8 +58,9 @@ def parse():
     ap.add_argument("--batch", type=int, default=2, help="lu: matrices per launch")
     ap.add_argument("--streams", type=int, default=4, help="c3: concurrent streams")
     ap.add_argument("--precision", choices=["plain", "mixed"], default="plain")
-    ap.add_argument("--lu-block", type=int, choices=[0, 64, 128], default=0,
-                    help="lu: column block of the mixed LU (HBEM_TUNE_LU_BLOCK; 0 = built-in)")
+    ap.add_argument("--lu-block", type=int, choices=[0, 32, 64, 128], default=0,
+                    help="lu: column block of the mixed LU, or the K of a TF32x3 bulk pass (HBEM_TUNE_LU_BLOCK; "
+                         "0 = built-in)")
     ap.add_argument("--lu-update", type=int, choices=[0, 1, 2], default=0,
                     help="lu: plain LU bulk update (HBEM_TUNE_LU_UPDATE; 2 = TF32x3 tensor cores)")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -168,9 +168,12 @@ int launch_trailing_update(int n, int batch, int k0, int kw, int start, int col_
 // of shared memory):
 //   BF16x3: tiles of 64 complex rows x 64 columns, A2 64 KB (4 K-blocks of
 //           128 bytes per row), ring of 6 x 16 KB, two 32 KB C tiles;
-//   TF32x3 (and BF16x3 with K = 128): tiles of 64 complex rows x 32 columns,
-//           A2 128 KB (8 K-blocks), ring of 6 x 8 KB, three 16 KB C tiles
-//           (C prefetched two tiles ahead).
+//   TF32x3 with K = 64 (and BF16x3 with K = 128): tiles of 64 complex rows x
+//           32 columns, A2 128 KB (8 K-blocks), ring of 6 x 8 KB, three
+//           16 KB C tiles (C prefetched two tiles ahead);
+//   TF32x3 with K = 32 (two passes per 64-column LU block): the BF16x3
+//           K = 64 shape (A2 64 KB, 64-column tiles, 6 x 16 KB ring, two
+//           32 KB C tiles).
 // Every mbarrier wait is bounded; a timeout sets the status word and the CTA
 // returns after releasing its TMEM.
 // ===========================================================================
@@ -186,7 +189,8 @@ constexpr long long kSpinLimit = 1LL << 24;
 // of one update (64: one LU block; 128: two blocks, BF16x3 only).
 template <bool TF32, int KC>
 struct TcCfg {
-    static_assert(KC == 64 || (KC == 128 && !TF32), "tensor-core update: K = 64, or 128 with BF16x3");
+    static_assert(KC == 64 || (KC == 128 && !TF32) || (KC == 32 && TF32),
+                  "tensor-core update: K = 64, 128 with BF16x3, or 32 with TF32x3");
     static constexpr int ES = TF32 ? 4 : 2;            // operand bytes
     static constexpr int EPB = 128 / ES;               // operand elements per 128-byte K-block
     static constexpr int K2 = 4 * KC;                  // packed elements per row: hi (real K = 2 KC), lo
@@ -726,32 +730,34 @@ template <bool TF32, int KC>
 __global__ void __launch_bounds__(256) k_pack_b(const float *a_re, const float *a_im, long long lda,
                                                 long long a_stride, int start, int col_end, int k0, int cols_pad,
                                                 int cols_used, typename TcSplit<TF32>::T *B2) {
-    // 64 columns per CTA, 64 rows of U12 at a time: the 64 x 64 block is read
-    // along its rows (coalesced), transposed in shared memory and written
-    // into the packed K-major rows (consecutive threads, consecutive pairs)
+    // 64 columns per CTA, CH = min(KC, 64) rows of U12 at a time: the CH x 64
+    // block is read along its rows (coalesced), transposed in shared memory
+    // and written into the packed K-major rows (consecutive threads,
+    // consecutive pairs)
     using S = TcSplit<TF32>;
     using T = typename S::T;
     constexpr int K2 = TcCfg<TF32, KC>::K2;
-    __shared__ float s_ur[64][65], s_ui[64][65];
+    constexpr int CH = KC < 64 ? KC : 64, PAIRS = 2 * CH, JSTEP = 256 / PAIRS;
+    __shared__ float s_ur[CH][65], s_ui[CH][65];
     const int mat = blockIdx.z;
     const int j0 = blockIdx.x * 64;
     const int tid = threadIdx.x;
-    // pair p of a chunk covers its entries 2p, 2p + 1 of [hi Ur, hi Ui, lo Ur, lo Ui] (64 each)
-    const int p = tid & 127;
+    // pair p of a chunk covers its entries 2p, 2p + 1 of [hi Ur, hi Ui, lo Ur, lo Ui] (CH each)
+    const int p = tid % PAIRS;
     const int kk = 2 * p;
-    const int part = kk >> 6, k = kk & 63;   // part: 0 hi Ur, 1 hi Ui, 2 lo Ur, 3 lo Ui
-    for (int kc = 0; kc < KC; kc += 64) {
+    const int part = kk / CH, k = kk % CH;   // part: 0 hi Ur, 1 hi Ui, 2 lo Ur, 3 lo Ui
+    for (int kc = 0; kc < KC; kc += CH) {
         const float *ure = a_re + (size_t)mat * a_stride + (size_t)(k0 + kc) * lda + start;
         const float *uim = a_im + (size_t)mat * a_stride + (size_t)(k0 + kc) * lda + start;
         if (kc) __syncthreads();   // the previous chunk's reads of s_ur / s_ui are done
-        for (int e = tid; e < 64 * 64; e += 256) {
+        for (int e = tid; e < CH * 64; e += 256) {
             const int kr = e >> 6, jj = e & 63, j = j0 + jj;
             const bool in = start + j < col_end;
             s_ur[kr][jj] = in ? ure[(size_t)kr * lda + j] : 0.f;
             s_ui[kr][jj] = in ? uim[(size_t)kr * lda + j] : 0.f;
         }
         __syncthreads();
-        for (int jj = tid >> 7; jj < 64; jj += 2) {
+        for (int jj = tid / PAIRS; jj < 64; jj += JSTEP) {
             const int j = j0 + jj;
             if (j >= cols_used) break;
             const float x0 = (part & 1) ? s_ui[k][jj] : s_ur[k][jj];
@@ -805,7 +811,8 @@ int make_map(CUtensorMap *map, void *ptr, long long rows, int box_rows, int es, 
 // Packed-operand workspace and tensor maps for one factorisation: sized for
 // the first (largest) trailing update and reused by the later, smaller ones.
 // tf32: TF32x3 operands (plain LU) instead of BF16x3 (mixed LU); kc: the
-// complex K of one update (64, or 128 for BF16x3).
+// complex K of one update (64; 128 for BF16x3; 32 for TF32x3, two passes per
+// 64-column block).
 struct TcWorkspace {
     void *A2 = nullptr, *B2 = nullptr;
     int rows3 = 0, cols_pad = 0, batch = 0, kc = 64;
@@ -815,9 +822,11 @@ struct TcWorkspace {
 
 int tc_workspace_create(int n, int batch, bool tf32, int kc, TcWorkspace **out, cudaStream_t st) {
     *out = nullptr;
-    if (kc != 64 && (kc != 128 || tf32)) return fail(HBEM_ERR_ARG, "tensor-core update: K = 64, or 128 with BF16x3");
+    if (!(kc == 64 || (kc == 128 && !tf32) || (kc == 32 && tf32)))
+        return fail(HBEM_ERR_ARG, "tensor-core update: K = 64, 128 with BF16x3, or 32 with TF32x3");
     auto *w = new TcWorkspace();
-    const int tn = (tf32 || kc == 128) ? 32 : 64, es = tf32 ? 4 : 2, k2 = 4 * kc;
+    const int es = tf32 ? 4 : 2, k2 = 4 * kc;
+    const int tn = 2 * kc * es / 128 == 4 ? 32 : 64;   // the configuration's tile width (TcCfg::N)
     w->tf32 = tf32;
     w->kc = kc;
     w->rows3 = ((n + 63) / 64) * kTcM;
@@ -912,6 +921,15 @@ int launch_trailing_tc(TcWorkspace *w, int n, int batch, int k0, int start, int 
                        float *a_im, long long lda, long long a_stride, int *status, cudaStream_t st,
                        int reserve_sms) {
     if (n - start <= 0 || col_end - col_start <= 0) return HBEM_OK;
+    if (w->tf32 && w->kc == 32) {
+        // the 64 columns of an LU block as two K = 32 passes (C read and
+        // written twice, each pass in the 64 KB-A, 64-column-tile shape)
+        int rc = launch_trailing_tc_t<true, 32>(w, n, batch, k0, start, col_start, col_end, a_re, a_im, lda,
+                                                a_stride, status, st, reserve_sms);
+        if (rc != HBEM_OK) return rc;
+        return launch_trailing_tc_t<true, 32>(w, n, batch, k0 + 32, start, col_start, col_end, a_re, a_im, lda,
+                                              a_stride, status, st, reserve_sms);
+    }
     if (w->tf32)
         return launch_trailing_tc_t<true, 64>(w, n, batch, k0, start, col_start, col_end, a_re, a_im, lda, a_stride,
                                               status, st, reserve_sms);

@@ -2082,7 +2082,14 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
     if ((precision == HBEM_PREC_MIXED && n > 64) || tf32_bulk) {
         HBEM_CUDA(cudaMallocAsync((void **)&status, sizeof(int), st));
         HBEM_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
-        int rc = tc_workspace_create(n, batch, tf32_bulk, tf32_bulk ? 64 : NB, &tc, st);
+        // TF32x3: below n = 12 000 each 64-column block as two K = 32 passes
+        // in the 64 KB-A, 64-column-tile shape (the K = 64 shape's 128 KB A
+        // leaves too short a B ring: 15 % tensor-pipe and 17 % HBM activity;
+        // 1044 x 40 6.2 -> 6.0 ms, 2976 x 40 71 -> 62 ms, 4096 x 8 43 -> 36 ms,
+        // 10 000 x 2 137 -> 116 ms); above, one K = 64 pass, whose single
+        // read-modify-write of C wins at 18 749 x 2 (701 ms against 831 ms)
+        const int tf32_kc = blk_want == 32 ? 32 : blk_want == 64 ? 64 : (n < 12000 ? 32 : 64);
+        int rc = tc_workspace_create(n, batch, tf32_bulk, tf32_bulk ? tf32_kc : NB, &tc, st);
         if (rc != HBEM_OK) {
             cudaFreeAsync(status, st);
             return rc;

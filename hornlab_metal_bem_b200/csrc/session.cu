@@ -369,8 +369,8 @@ extern "C" int hbem_set_tuning(int key, int value) {
             if (value < 0 || value > 2) return fail(HBEM_ERR_ARG, "HBEM_TUNE_LU_UPDATE: 0, 1 or 2");
             break;
         case HBEM_TUNE_LU_BLOCK:
-            if (value != 0 && value != 64 && value != 128)
-                return fail(HBEM_ERR_ARG, "HBEM_TUNE_LU_BLOCK: 0, 64 or 128");
+            if (value != 0 && value != 32 && value != 64 && value != 128)
+                return fail(HBEM_ERR_ARG, "HBEM_TUNE_LU_BLOCK: 0, 32, 64 or 128");
             break;
         case HBEM_TUNE_LU_PANEL_KERNEL:
             if (value < 0 || value > 1) return fail(HBEM_ERR_ARG, "HBEM_TUNE_LU_PANEL_KERNEL: 0 or 1");

@@ -133,7 +133,10 @@ long long hbem_launch_count(void);
  *                            split products, for both)
  *   HBEM_TUNE_LU_BLOCK:      column block of the mixed (BF16x3) LU and the K
  *                            of its tensor-core update (64 or 128; 0: the
- *                            built-in 128 for n > 16000, else 64)
+ *                            built-in 128 for n > 16000, else 64); for the
+ *                            FP32 LU's TF32x3 bulk, the K of one tensor-core
+ *                            pass over a 64-column block (32: two passes, 64:
+ *                            one; 0: the built-in 32 for n < 12000, else 64)
  *   HBEM_TUNE_LU_PANEL_KERNEL: sub-panels with their rows in shared memory
  *                            (0, built-in) or, where one row per thread fits,
  *                            in registers (1: 64 columns up to 384 rows, 32

@@ -75,7 +75,7 @@ def test_tuning_knobs_validate_and_read_back():
         "HBEM_TUNE_LU_RESERVE": ([0, 1, 17, 1024], [-1, 1025]),
         "HBEM_TUNE_WAVE_SPIN": ([0, 1, 4194304], [-1, 4194305]),
         "HBEM_TUNE_LU_UPDATE": ([0, 1, 2], [-1, 3]),
-        "HBEM_TUNE_LU_BLOCK": ([0, 64, 128], [32, 256, -1]),
+        "HBEM_TUNE_LU_BLOCK": ([0, 32, 64, 128], [16, 256, -1]),
         "HBEM_TUNE_LU_PANEL_KERNEL": ([0, 1], [-1, 2]),
     }
     assert set(valid) == set(keys)

@@ -380,20 +380,24 @@ def test_tf32x3_precision_refined_matches_lapack(n, batch):
         assert rel(x[m], ref) < 1e-6
 
 
-@pytest.mark.parametrize("n,batch", [(300, 3), (1043, 6), (3300, 1)])
-def test_plain_lu_tensor_core_update_matches_lapack(n, batch):
+@pytest.mark.parametrize("n,batch,kpass", [(300, 3, 0), (1043, 6, 0), (3300, 1, 0), (1043, 6, 64), (3300, 1, 64)])
+def test_plain_lu_tensor_core_update_matches_lapack(n, batch, kpass):
     """The plain LU with its look-ahead bulk update on the tensor cores (TF32x3 split products,
-    HBEM_TUNE_LU_UPDATE = 2) against LAPACK and against the CUDA-core (exact FP32 product) update."""
+    HBEM_TUNE_LU_UPDATE = 2) against LAPACK and against the CUDA-core (exact FP32 product) update; the
+    bulk in two K = 32 passes per 64-column block (built in below n = 12000) and in one K = 64 pass
+    (HBEM_TUNE_LU_BLOCK = 64)."""
     lib = load_library()
     A, b = _lu_case(n, batch, n + 7)
     xs = {}
     for mode in (1, 2):
         Ar, Ai = _dev(A)
         assert lib.hbem_set_tuning(8, mode) == 0
+        assert lib.hbem_set_tuning(9, kpass) == 0
         try:
             piv, info = _factor(Ar, Ai, n, batch)
         finally:
             lib.hbem_set_tuning(8, 0)
+            lib.hbem_set_tuning(9, 0)
         assert int(info.abs().sum()) == 0
         Br, Bi = _dev(b[:, :, None])
         _solve(Ar, Ai, piv, Br, Bi, n, 1, batch)
