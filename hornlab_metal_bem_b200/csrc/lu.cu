@@ -2248,13 +2248,11 @@ int lu_factor(int n, int batch, float *a_re, float *a_im, long long lda, long lo
         }
         const int outside = n - bw;
         const int next_end = std::min(n, b0 + bw + NB);
-        // SMs the persistent tensor-core update leaves to the chain: by
-        // default 32 for the TF32x3 bulk of small matrices, whose chain of
-        // panels is the longer path (n = 1043 x 40: 6.76 -> 6.47 ms; at
-        // 1542 x 40 it costs: 15.06 -> 15.62 ms)
-        const int tc_reserve = tuning(HBEM_TUNE_LU_RESERVE) > 0 ? tuning(HBEM_TUNE_LU_RESERVE) - 1
-                               : (tf32_bulk && n <= 1280)      ? 32
-                                                                : 0;
+        // SMs the persistent tensor-core update leaves to the chain (by
+        // default none: with the TF32x3 bulk in K = 32 passes, leaving 32 SMs
+        // gave n = 1044 x 40 5.98 against 5.87 ms and 1542 x 40 16.4 against
+        // 15.3 ms)
+        const int tc_reserve = tuning(HBEM_TUNE_LU_RESERVE) > 0 ? tuning(HBEM_TUNE_LU_RESERVE) - 1 : 0;
         const bool split = la && next_end < n;
         if (outside > 0) {
             // with look-ahead the chain swaps (and solves) only the next block's

@@ -118,7 +118,7 @@ long long hbem_launch_count(void);
  *   HBEM_TUNE_LU_RESERVE:    SMs the look-ahead's persistent tensor-core
  *                            update leaves to the factorisation chain
  *                            (v >= 1: v - 1 SMs, at most half; 0: built-in,
- *                            32 for a TF32x3 bulk of n <= 1280, else none)
+ *                            none)
  *   HBEM_TUNE_WAVE_SPIN:     polls (of >= 32 ns) a wavefront-solve warp waits
  *                            for an earlier block before it gives up (0: the
  *                            built-in 2^22); a wait that runs out makes the
