@@ -858,7 +858,9 @@ void tc_workspace_destroy(TcWorkspace *w, cudaStream_t st) {
     delete w;
 }
 
-int tc_workspace_k(const TcWorkspace *w) { return w ? w->kc : 0; }
+// The K one launch_trailing_tc call consumes: the workspace's K, or 64 for
+// the TF32x3 K = 32 workspace, which runs two passes per call.
+int tc_workspace_k(const TcWorkspace *w) { return w ? (w->tf32 && w->kc == 32 ? 64 : w->kc) : 0; }
 
 namespace {
 
