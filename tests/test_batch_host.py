@@ -56,3 +56,15 @@ def test_autotuner_picks_fastest_per_bucket_and_caches(tmp_path):
     t3.tune(cases)
     assert len(calls) == 2 * len(CANDIDATES)
     assert set(json.loads(cache.read_text())) == {"gpu-x|1", "gpu-y|1"}
+
+
+def test_matrix_pitch_and_solve_names():
+    """The sweep paths' dense row pitch is n rounded up to 4 floats (16-byte rows), and a refined plain
+    solve is reported as the FP32 LU with the TF32x3 tensor-core bulk."""
+    from hornlab_metal_bem_b200.native import matrix_ld, solve_impl
+
+    assert [matrix_ld(n) for n in (1, 4, 1043, 1044, 18749)] == [4, 4, 1044, 1044, 18752]
+    assert solve_impl("plain", False) == "hbem_blocked_lu_fp32"
+    assert solve_impl("plain", True) == "hbem_blocked_lu_fp32_tf32x3_refined"
+    assert solve_impl("mixed", True) == "hbem_blocked_lu_bf16x3_refined"
+    assert solve_impl("fp64", False) == "hbem_blocked_lu_fp64"
